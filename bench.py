@@ -1,0 +1,269 @@
+"""Benchmark of the implicit GRMHD timestep: zone-cycles/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload orszag_tang|torus|fast_mode|emhd_stratified]
+
+One JSON line on rank 0.  ``value`` is the zone-cycles/s of the product's
+fast Newton form (forward-tangent Jacobian, FP32 Jacobian/solve refined by
+the FP64 residual, per-zone convergence) with inputs resident in HBM;
+``fd64`` is the same workload through the plain FP64 finite-difference
+path (the reference's method) at the same Newton tolerance; ``e2e`` adds
+the host<->device copies of the primitives every step through the C ABI.
+Each timed step is bracketed by CUDA events on the stepper's stream; the
+L2 is flushed between timed steps (a 256 MB write) and the flush is not
+timed.  With --impl reference the CPU oracle (a C++ restatement of the
+reference's algorithm) is timed on the host cores instead.
+Multi-GPU: one independent replica per rank ("replicas only"), max over
+ranks of the device time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+from grim_b200 import config as C  # noqa: E402
+from grim_b200 import problems as PR  # noqa: E402
+
+METRIC = "zone-cycles/s per implicit step: plain FP64 FD-Jac vs tangent/mixed form, same tol"
+RTOL = 1e-10
+
+
+def workload(name):
+    """(config, prims, description) of a named workload"""
+    if name == "orszag_tang":
+        cfg = PR.orszag_tang_config(N=512, nonlinearsolve_atol=0.0, nonlinearsolve_rtol=RTOL,
+                                    maxNonLinearIter=4)
+        return cfg, PR.orszag_tang_prims(cfg), "2D Orszag-Tang 512x512, Minkowski, WENO5, HLL, flux-CT, ideal MHD (dof 8)"
+    if name == "fast_mode":
+        cfg = PR.fast_mode_config(N=128, nonlinearsolve_atol=0.0, nonlinearsolve_rtol=RTOL, maxNonLinearIter=4)
+        return cfg, PR.fast_mode_prims(cfg), "2D fast mode 128x128, Minkowski, minmod, LLF, flux-CT"
+    if name == "emhd_stratified":
+        cfg = PR.emhd_stratified_config(N=256, nonlinearsolve_atol=0.0, nonlinearsolve_rtol=RTOL,
+                                        maxNonLinearIter=4)
+        return cfg, PR.emhd_stratified_prims(cfg), "2D EMHD 256x256 (dof 10), MP5, HLL, tau(y) closure"
+    raise SystemExit("unknown workload %s" % name)
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._p = None
+
+    def start(self):
+        q = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown," \
+            "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+            "clocks_event_reasons.sw_power_cap"
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                        "--format=csv,noheader,nounits", "-lms", "200"],
+                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self._p = None
+            return
+
+        def rd():
+            for line in self._p.stdout:
+                self.samples.append([x.strip() for x in line.split(",")])
+        self._t = threading.Thread(target=rd, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        if self._p:
+            self._p.terminate()
+            try:
+                self._p.wait(timeout=5)
+            except Exception:
+                self._p.kill()
+        sm = [float(s[0]) for s in self.samples if len(s) >= 7 and s[0].replace('.', '').isdigit()]
+        mx = [float(s[1]) for s in self.samples if len(s) >= 7 and s[1].replace('.', '').isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            if len(s) >= 7:
+                for n, v in zip(names, s[3:7]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference(cfg, P, seconds=15.0, threads=None):
+    """Time the CPU oracle on a bounded sample of the workload."""
+    from oracle import oracle as O
+    n = threads or os.cpu_count()
+    O.set_threads(n)
+    o = O.Oracle(cfg)
+    o.set_prims(P)
+    o.time_step(1)  # warm-up (page faults, first dt)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        o.time_step(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or steps >= 50:
+            break
+    zones = cfg["N1"] * cfg["N2"] * cfg["N3"]
+    return zones * steps / el, n, "%d step(s) of the full %dx%dx%d grid after 1 warm-up step, %.1f s" % (
+        steps, cfg["N1"], cfg["N2"], cfg["N3"], el)
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    torch.cuda.set_device(local_rank)
+    from grim_b200.timestepper import timeStepper
+    cfg, P, desc = workload(args.workload)
+    zones = cfg["N1"] * cfg["N2"] * cfg["N3"]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def time_path(mode, graph):
+        ts = timeStepper(cfg, device=local_rank)
+        ts.setNewtonMode(mode, 1, RTOL)
+        ts.primOld.setVars(P)
+        if graph:
+            ts.enableGraph(True)
+        stream = torch.cuda.ExternalStream(ts.stream())
+        for _ in range(args.warmup):
+            ts.timeStep()
+        ts.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        for a, b in evs:
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                a.record(stream)
+            ts.timeStep()
+            b.record(stream)
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs)
+        st = ts.stats()
+        return ts, ms, st
+
+    clocks = Clocks(local_rank)
+    clocks.start()
+    ts_fast, ms_fast, st_fast = time_path(C.NEWTON_MIXED32, True)
+    clocks_info = clocks.stop()
+    _, ms_fd, st_fd = time_path(C.NEWTON_PARITY_FD64, True)
+
+    # e2e: the C-ABI call with host buffers, copies inside the timed region
+    import ctypes
+    from grim_b200 import _lib
+    dof = ts_fast.dof
+    host_in = torch.from_numpy(np.ascontiguousarray(P)).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    L = _lib.lib()
+    e2e_steps = max(3, args.steps // 2)
+    ts_fast.synchronize()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        _lib.check(L.grim_set_prims(ts_fast._h, _lib.PRIM_OLD, ctypes.c_void_p(host_in.data_ptr()), _lib.HOST))
+        _lib.check(L.grim_time_step(ts_fast._h, None, None))
+        _lib.check(L.grim_get_prims(ts_fast._h, _lib.PRIM_OLD, ctypes.c_void_p(host_out.data_ptr()), _lib.HOST))
+    e2e_s = time.perf_counter() - t0
+    e2e_bytes = host_in.numel() * 8
+
+    # max over ranks of the device time
+    t = torch.tensor([ms_fast, ms_fd, e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_fast, ms_fd, e2e_s = [float(x) for x in t.tolist()]
+    value = world * zones * args.steps / (ms_fast / 1e3)
+    fd = world * zones * args.steps / (ms_fd / 1e3)
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "zone-cycles/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_fast / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 residual / f32 Jacobian+solve",
+        "data": "synthetic (seeded initial conditions of the named workload)",
+        "config": {"workload": args.workload, "description": desc, "zones": zones,
+                   "newton": "tangent Jacobian, FP32 solve, FP64 residual, per-zone convergence",
+                   "rel_residual_tol": RTOL, "maxNonLinearIter": cfg["maxNonLinearIter"],
+                   "l2": "flushed between timed steps (256 MB write, untimed)",
+                   "parallelism": "replicas" if world > 1 else "single GPU", "cuda_graph": True},
+        "fd64": {"value": fd, "ms_per_step": ms_fd / args.steps, "newton_iters": st_fd["newtonIters"],
+                 "unconverged": st_fd["unconverged"]},
+        "speedup_vs_fd64": value / fd,
+        "newton_iters": st_fast["newtonIters"],
+        "unconverged": st_fast["unconverged"],
+        "e2e": {"value": world * zones * e2e_steps / e2e_s, "unit": "zone-cycles/s",
+                "h2d_bytes_per_step": e2e_bytes, "d2h_bytes_per_step": e2e_bytes},
+        "gpu_launches": int(st_fast["kernelLaunches"]) * args.steps,
+        "clocks": clocks_info,
+    }
+    return out, cfg, P
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="grim_b200")
+    ap.add_argument("--workload", default="orszag_tang")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cfg, P, desc = workload(args.workload)
+        vals = []
+        for _ in range(max(1, args.steps // 10)):
+            v, n, sample = cpu_reference(cfg, P, seconds=10.0)
+            vals.append(v)
+        v = float(np.median(vals))
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": v, "unit": "zone-cycles/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "description": desc,
+                       "newton": "FD Jacobian (reference method), FP64"},
+            "cpu_baseline": {"value": v, "unit": "zone-cycles/s", "cores": n, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "zone-cycles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
+
+    if world > 1:
+        import torch
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    out, cfg, P = run_gpu(args, rank, world, local_rank)
+    if rank == 0 and not args.no_cpu:
+        v, n, sample = cpu_reference(cfg, P, seconds=10.0)
+        out["cpu_baseline"] = {"value": v, "unit": "zone-cycles/s", "cores": n, "kind": "port",
+                               "sample": sample}
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1047 @@
+// kernels.cuh -- the CUDA kernels of one implicit timestep.
+//
+// Included by two translation units: kernels_exact.cu (--fmad=false, the
+// FP64 operation order of the reference, used by the parity path) and
+// kernels_fast.cu (FMA contraction on, used by the tangent / mixed paths).
+// Each defines GRIM_KNS to put its instantiations in its own namespace.
+//
+// Per stage:
+//   k_ghost_fill       ghost zones <- interior (periodic wrap, outflow,
+//                      mirror; boundary.cpp:5-241 + grid.cpp:306-315)
+//   k_emhd_prepass     u_mu and T of the stage element per zone (EMHD only)
+//   k_face_flux(dir)   reconstruction + two face elements + HLL/LLF, one
+//                      thread per face (fvmfluxes.cpp, riemannsolver.cpp)
+//   k_stage_epilogue   EMFs + flux-CT + divergence + induction + explicit
+//                      sources + consOld, per interior zone
+//   k_dt_speeds        max over zones of sum_d c_max,d / dX_d (computeDt)
+//   k_newton_*         per-zone Newton (solve.cpp / residual.cpp)
+#pragma once
+#include "physics.cuh"
+#include "recon.cuh"
+#include "stage.cuh"
+
+namespace grim {
+namespace GRIM_KNS {
+
+GRIM_D double zone_x1(const DevCfg& c, int i, double o) { return c.X1Start + ((double)(i - c.g1) + o) * c.dX[0]; }
+GRIM_D double zone_x2(const DevCfg& c, int j, double o) { return c.X2Start + ((double)(j - c.g2) + o) * c.dX[1]; }
+
+template <class R>
+GRIM_D void load_geo(ZoneGeo<R>& G, const DevCfg& c, const double* geo, long long z, int i, int j, double o1,
+                     double o2) {
+  if (geo == nullptr)
+    geo_minkowski<R>(G, (R)zone_x1(c, i, o1), (R)zone_x2(c, j, o2));
+  else
+    geo_load<R>(G, geo, c.Z, z);
+}
+
+// ---------------------------------------------------------------------------
+// ghost fill: composite gather (every ghost zone reads the interior zone
+// that the wrap / outflow / mirror maps of each direction select)
+// ---------------------------------------------------------------------------
+GRIM_D int bc_map(int x, int g, int N, int lo, int hi) {
+  if (x >= g && x < N + g) return x;
+  if (x < g) {
+    if (lo == GRIM_PERIODIC) return g + ((x - g) % N + N) % N;
+    if (lo == GRIM_MIRROR) return 2 * g - 1 - x;
+    return g;  // outflow (and Dirichlet: left to the problem hook)
+  }
+  if (hi == GRIM_PERIODIC) return g + ((x - g) % N + N) % N;
+  if (hi == GRIM_MIRROR) return 2 * (N + g) - 1 - x;
+  return N + g - 1;
+}
+
+__global__ void k_ghost_fill(DevCfg c, double* __restrict__ prim, int nv) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  int si = bc_map(i, c.g1, c.N1, c.bc[0], c.bc[1]);
+  int sj = (c.dim >= 2) ? bc_map(j, c.g2, c.N2, c.bc[2], c.bc[3]) : j;
+  int sk = (c.dim >= 3) ? bc_map(k, c.g3, c.N3, c.bc[4], c.bc[5]) : k;
+  if (si == i && sj == j && sk == k) return;
+  long long s = zidx(c, si, sj, sk);
+  for (int v = 0; v < nv; v++) prim[(long long)v * c.Z + z] = prim[(long long)v * c.Z + s];
+}
+
+// ---------------------------------------------------------------------------
+// EMHD pre-pass: u_mu and T of the stage element at every zone
+// ---------------------------------------------------------------------------
+template <int COND, int VISC>
+__global__ void k_emhd_prepass(DevCfg c, const double* __restrict__ ps, const double* __restrict__ geoC,
+                                        double* __restrict__ uT) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  ZoneGeo<double> G;
+  load_geo(G, c, geoC, z, i, j, 0.5, 0.5);
+  const long long Z = c.Z;
+  ElemT<double, double> e;
+  elem_set<COND, VISC>(e, ps[z], ps[Z + z], ps[2 * Z + z], ps[3 * Z + z], ps[4 * Z + z],
+                       ps[(long long)c.B1 * Z + z], ps[(long long)(c.B1 + 1) * Z + z],
+                       ps[(long long)(c.B1 + 2) * Z + z], COND ? ps[(long long)c.Q * Z + z] : 0.,
+                       VISC ? ps[(long long)c.DP * Z + z] : 0., G, c);
+  for (int m = 0; m < 4; m++) uT[(long long)m * Z + z] = e.uCov[m];
+  uT[4 * Z + z] = e.temperature;
+}
+
+// ---------------------------------------------------------------------------
+// face fluxes: thread z computes the flux through the face z - 1/2 along
+// `dir` (riemannsolver.cpp:202-328 after its shift).
+// ---------------------------------------------------------------------------
+template <int COND, int VISC>
+__global__ void __launch_bounds__(128) k_face_flux(DevCfg c, int dir, const double* __restrict__ ps,
+                                                            const double* __restrict__ geoF,
+                                                            const double* __restrict__ geoC,
+                                                            double* __restrict__ flux) {
+  constexpr int NF = 5 + COND + VISC;
+  constexpr int DOF = NF + 3;
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  const int x = (dir == 0) ? i : (dir == 1 ? j : k);
+  const int NT = (dir == 0) ? c.N1T : (dir == 1 ? c.N2T : c.N3T);
+  if (x < 3 || x > NT - 3) return;
+  const long long s = stride_of(c, dir);
+  const long long Z = c.Z;
+  // left state: right face of zone z-s; right state: left face of zone z
+  double pl[DOF], pr[DOF];
+#pragma unroll
+  for (int v = 0; v < DOF; v++) {
+    const double* a = ps + (long long)v * Z + z;
+    double y[6];
+#pragma unroll
+    for (int m = 0; m < 6; m++) y[m] = __ldg(a + (m - 3) * s);
+    double lo, ro;
+    recon_faces(c.reconstruction, c.theta, y[0], y[1], y[2], y[3], y[4], lo, ro);
+    pl[v] = ro;
+    recon_faces(c.reconstruction, c.theta, y[1], y[2], y[3], y[4], y[5], lo, ro);
+    pr[v] = lo;
+  }
+  ZoneGeo<double> GL, GR;
+  if (dir == 2) {
+    // X3 faces use the centre geometry of each side (fvmfluxes.cpp:150-151)
+    load_geo(GL, c, geoC, z - s, i, j, 0.5, 0.5);
+    load_geo(GR, c, geoC, z, i, j, 0.5, 0.5);
+  } else {
+    const double o1 = (dir == 0) ? 0. : 0.5, o2 = (dir == 1) ? 0. : 0.5;
+    load_geo(GL, c, geoF, z, i, j, o1, o2);
+    GR = GL;
+  }
+  const int fd = dir + 1;
+  double FL[DOF], UL[DOF], FR[DOF], UR[DOF];
+  double minL, maxL, minR, maxR;
+  {
+    ElemT<double, double> e;
+    elem_set<COND, VISC>(e, pl[0], pl[1], pl[2], pl[3], pl[4], pl[NF], pl[NF + 1], pl[NF + 2],
+                         COND ? pl[5] : 0., VISC ? pl[5 + COND] : 0., GL, c);
+    fluxes_fluid<COND, VISC>(e, fd, GL.g, FL, 5, 5 + COND);
+    fluxes_B(e, fd, GL.g, FL + NF);
+    fluxes_fluid<COND, VISC>(e, 0, GL.g, UL, 5, 5 + COND);
+    fluxes_B(e, 0, GL.g, UL + NF);
+    char_speeds<COND, VISC>(e, GL, dir, c, minL, maxL);
+  }
+  {
+    ElemT<double, double> e;
+    elem_set<COND, VISC>(e, pr[0], pr[1], pr[2], pr[3], pr[4], pr[NF], pr[NF + 1], pr[NF + 2],
+                         COND ? pr[5] : 0., VISC ? pr[5 + COND] : 0., GR, c);
+    fluxes_fluid<COND, VISC>(e, fd, GR.g, FR, 5, 5 + COND);
+    fluxes_B(e, fd, GR.g, FR + NF);
+    fluxes_fluid<COND, VISC>(e, 0, GR.g, UR, 5, 5 + COND);
+    fluxes_B(e, 0, GR.g, UR + NF);
+    char_speeds<COND, VISC>(e, GR, dir, c, minR, maxR);
+  }
+  const double cmin = fmin(minL, minR);
+  const double cmax = fmax(maxL, maxR);
+  if (c.riemann == GRIM_HLL) {
+#pragma unroll
+    for (int v = 0; v < DOF; v++)
+      flux[(long long)v * Z + z] = (cmax * FL[v] - cmin * FR[v] + cmin * cmax * (UR[v] - UL[v])) / (cmax - cmin);
+  } else {
+    const double cm = fmax(cmax, -cmin);
+#pragma unroll
+    for (int v = 0; v < DOF; v++) flux[(long long)v * Z + z] = 0.5 * (FL[v] + FR[v] - cm * (UR[v] - UL[v]));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// stage epilogue: EMF / CT (constrainedtransport.cpp:3-83), divergence
+// (fvmfluxes.cpp), induction (timestep.cpp:80-89, 226-237), consOld
+// (timestep.cpp:33-36), explicit sources (physics.cpp:360-586)
+// ---------------------------------------------------------------------------
+struct FluxView {
+  const double* F[3];
+  long long Z;
+  int B1;
+  GRIM_D double at(int d, int v, long long z) const { return __ldg(F[d] + (long long)v * Z + z); }
+};
+
+// EMF3 at edge (i-1/2, j-1/2) of zone z
+GRIM_D double emf3(const FluxView& f, long long z, long long s1, long long s2) {
+  return 0.25 * (f.at(0, f.B1 + 1, z) + f.at(0, f.B1 + 1, z - s2) - f.at(1, f.B1, z) - f.at(1, f.B1, z - s1));
+}
+GRIM_D double emf1(const FluxView& f, long long z, long long s2, long long s3) {
+  return 0.25 * (f.at(1, f.B1 + 2, z) + f.at(1, f.B1 + 2, z - s3) - f.at(2, f.B1 + 1, z) - f.at(2, f.B1 + 1, z - s2));
+}
+GRIM_D double emf2(const FluxView& f, long long z, long long s1, long long s3) {
+  return 0.25 * (f.at(2, f.B1, z) + f.at(2, f.B1, z - s1) - f.at(0, f.B1 + 2, z) - f.at(0, f.B1 + 2, z - s3));
+}
+
+template <int COND, int VISC>
+__global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, StageBufs b) {
+  constexpr int NF = 5 + COND + VISC;
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= c.Zint) return;
+  const long long Z = c.Z;
+  const long long z = interior_to_z(c, n);
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  const long long s1 = 1, s2 = (long long)c.N1T, s3 = (long long)c.N1T * c.N2T;
+  FluxView f;
+  f.F[0] = b.flux[0]; f.F[1] = b.flux[1]; f.F[2] = b.flux[2]; f.Z = Z; f.B1 = c.B1;
+  const double dt = b.st->dt;
+
+  // ---- divergence of the fluid rows
+  double div[NF + 3];
+  const double i1 = 1. / c.dX[0], i2 = 1. / c.dX[1];
+  for (int v = 0; v < NF; v++) {
+    if (c.dim <= 2) {
+      double d = f.at(0, v, z + s1) * i1 + f.at(0, v, z) * (-i1);
+      if (c.dim == 2) d = d + (f.at(1, v, z + s2) * i2 + f.at(1, v, z) * (-i2));
+      div[v] = d;
+    } else {
+      div[v] = (f.at(0, v, z + s1) - f.at(0, v, z)) / c.dX[0] + (f.at(1, v, z + s2) - f.at(1, v, z)) / c.dX[1] +
+               (f.at(2, v, z + s3) - f.at(2, v, z)) / c.dX[2];
+    }
+  }
+  // ---- flux-CT B fluxes on the zone's faces, then their divergence
+  if (c.dim == 1) {
+    for (int b3 = 0; b3 < 3; b3++) {
+      const int v = c.B1 + b3;
+      div[NF + b3] = f.at(0, v, z + s1) * i1 + f.at(0, v, z) * (-i1);
+    }
+  } else if (c.dim == 2) {
+    const double e00 = emf3(f, z, s1, s2), e10 = emf3(f, z + s1, s1, s2);
+    const double e01 = emf3(f, z + s2, s1, s2), e11 = emf3(f, z + s1 + s2, s1, s2);
+    // F1: B1 -> 0, B2 -> 0.5 (emf3 + emf3[j+1]); F2: B1 -> -0.5 (emf3 + emf3[i+1]), B2 -> 0
+    const double F1B2_l = 0.5 * (e00 + e01), F1B2_r = 0.5 * (e10 + e11);
+    const double F2B1_b = -0.5 * (e00 + e10), F2B1_t = -0.5 * (e01 + e11);
+    const double zero = 0.;
+    div[NF + 0] = (zero * i1 + zero * (-i1)) + (F2B1_t * i2 + F2B1_b * (-i2));
+    div[NF + 1] = (F1B2_r * i1 + F1B2_l * (-i1)) + (zero * i2 + zero * (-i2));
+    const int v = c.B1 + 2;
+    div[NF + 2] = (f.at(0, v, z + s1) * i1 + f.at(0, v, z) * (-i1)) + (f.at(1, v, z + s2) * i2 + f.at(1, v, z) * (-i2));
+  } else {
+    // EMF3 at (i|i+1, j|j+1), EMF2 at (i|i+1, k|k+1), EMF1 at (j|j+1, k|k+1)
+    const double a00 = emf3(f, z, s1, s2), a10 = emf3(f, z + s1, s1, s2);
+    const double a01 = emf3(f, z + s2, s1, s2), a11 = emf3(f, z + s1 + s2, s1, s2);
+    const double b00 = emf2(f, z, s1, s3), b10 = emf2(f, z + s1, s1, s3);
+    const double b01 = emf2(f, z + s3, s1, s3), b11 = emf2(f, z + s1 + s3, s1, s3);
+    const double c00 = emf1(f, z, s2, s3), c10 = emf1(f, z + s2, s2, s3);
+    const double c01 = emf1(f, z + s3, s2, s3), c11 = emf1(f, z + s2 + s3, s2, s3);
+    const double F1B1_l = 0., F1B1_r = 0.;
+    const double F1B2_l = 0.5 * (a00 + a01), F1B2_r = 0.5 * (a10 + a11);
+    const double F1B3_l = -0.5 * (b00 + b01), F1B3_r = -0.5 * (b10 + b11);
+    const double F2B1_l = -0.5 * (a00 + a10), F2B1_r = -0.5 * (a01 + a11);
+    const double F2B2_l = 0., F2B2_r = 0.;
+    const double F2B3_l = 0.5 * (c00 + c01), F2B3_r = 0.5 * (c10 + c11);
+    const double F3B1_l = 0.5 * (b00 + b10), F3B1_r = 0.5 * (b01 + b11);
+    const double F3B2_l = -0.5 * (c00 + c10), F3B2_r = -0.5 * (c01 + c11);
+    const double F3B3_l = 0., F3B3_r = 0.;
+    div[NF + 0] = (F1B1_r - F1B1_l) / c.dX[0] + (F2B1_r - F2B1_l) / c.dX[1] + (F3B1_r - F3B1_l) / c.dX[2];
+    div[NF + 1] = (F1B2_r - F1B2_l) / c.dX[0] + (F2B2_r - F2B2_l) / c.dX[1] + (F3B2_r - F3B2_l) / c.dX[2];
+    div[NF + 2] = (F1B3_r - F1B3_l) / c.dX[0] + (F2B3_r - F2B3_l) / c.dX[1] + (F3B3_r - F3B3_l) / c.dX[2];
+  }
+
+  // ---- stage element at the centre (elemOld / elemHalfStep)
+  ZoneGeo<double> G;
+  load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
+  const double* ps = b.ps;
+  ElemT<double, double> e;
+  elem_set<COND, VISC>(e, ps[z], ps[Z + z], ps[2 * Z + z], ps[3 * Z + z], ps[4 * Z + z],
+                       ps[(long long)c.B1 * Z + z], ps[(long long)(c.B1 + 1) * Z + z],
+                       ps[(long long)(c.B1 + 2) * Z + z], COND ? ps[(long long)c.Q * Z + z] : 0.,
+                       VISC ? ps[(long long)c.DP * Z + z] : 0., G, c);
+  if (stage == GRIM_HALF_STEP) {
+    double U[NF], UB[3];
+    fluxes_fluid<COND, VISC>(e, 0, G.g, U, 5, 5 + COND);
+    fluxes_B(e, 0, G.g, UB);
+    for (int v = 0; v < NF; v++) b.consOld[(long long)v * Z + z] = U[v];
+    for (int v = 0; v < 3; v++) b.consOld[(long long)(NF + v) * Z + z] = UB[v];
+  }
+  // ---- explicit sources
+  double S[NF];
+  for (int v = 0; v < NF; v++) S[v] = 0.;
+  const bool needS = (c.metric != GRIM_MINKOWSKI) || COND || VISC;
+  if (c.metric != GRIM_MINKOWSKI) {
+    double T[4][4];
+    for (int ka = 0; ka < 4; ka++)
+      for (int la = 0; la < 4; la++) T[ka][la] = tmunu<COND, VISC>(e, ka, la);
+    for (int nu = 0; nu < 4; nu++) {
+      double s = S[UU + nu];
+      for (int ka = 0; ka < 4; ka++)
+        for (int la = 0; la < 4; la++)
+          s -= G.g * T[ka][la] * __ldg(b.gamma + (long long)(la * 16 + ka * 4 + nu) * Z + z);
+      S[UU + nu] = s;
+    }
+  }
+  if (COND || VISC) {
+    // computeEMHDGradients (physics.cpp:502-586) from the pre-pass u_mu, T
+    double gu[4][4], gT[4];
+    const double* uT = b.uT;
+    auto st = [&](int m, int dir, double dx) -> double {
+      const long long sd = stride_of(c, dir);
+      const double* a = uT + (long long)m * Z + z;
+      return recon_slope(c.reconstruction, c.theta, a[-2 * sd], a[-sd], a[0], a[sd], a[2 * sd], dx);
+    };
+    for (int mu = 0; mu < 4; mu++) {
+      gu[0][mu] = 0.;
+      gu[1][mu] = st(mu, 0, c.dX[0]);
+      gu[2][mu] = (c.dim > 1) ? st(mu, 1, c.dX[1]) : 0.;
+      gu[3][mu] = (c.dim > 2) ? st(mu, 2, c.dX[2]) : 0.;
+      if (c.metric != GRIM_MINKOWSKI) {
+        for (int nu = 0; nu < 4; nu++)
+          for (int la = 0; la < 4; la++)
+            gu[nu][mu] -= __ldg(b.gamma + (long long)(la * 16 + nu * 4 + mu) * Z + z) * e.uCov[la];
+      }
+    }
+    if (COND) {
+      gT[0] = 0.;
+      gT[1] = st(4, 0, c.dX[0]);
+      gT[2] = (c.dim > 1) ? st(4, 1, c.dX[1]) : 0.;
+      gT[3] = (c.dim > 2) ? st(4, 2, c.dX[2]) : 0.;
+    }
+    double dv = 0.;
+    for (int mu = 0; mu < 4; mu++)
+      for (int nu = 0; nu < 4; nu++) dv += G.gcon[mu][nu] * gu[mu][nu];
+    if (VISC) {
+      double d0 = -dv * e.rho * e.nu;
+      for (int mu = 0; mu < 4; mu++)
+        for (int nu = 0; nu < 4; nu++) d0 += 3. * e.rho * e.nu * e.bCon[mu] * e.bCon[nu] / e.bSqr * gu[mu][nu];
+      double d0t = (c.hoVisc == 1) ? d0 * sqrt(e.tau / e.rho / e.nu / e.temperature) : d0;
+      double s = -G.g * (d0t) / e.tau;
+      if (c.hoVisc == 1) s -= 0.5 * G.g * dv * e.deltaPTilde;
+      S[c.DP] = s;
+    }
+    if (COND) {
+      double qq = 0.;
+      for (int mu = 0; mu < 4; mu++) {
+        qq -= e.rho * e.chi * e.bCon[mu] / e.bNorm * gT[mu];
+        for (int nu = 0; nu < 4; nu++) qq -= e.rho * e.chi * e.temperature * e.bCon[nu] / e.bNorm * e.uCon[mu] * gu[mu][nu];
+      }
+      double qt = (c.hoCond == 1) ? qq * sqrt(e.tau / e.rho / e.chi) / e.temperature : qq;
+      double s = -G.g * (qt) / e.tau;
+      if (c.hoCond == 1) s -= 0.5 * G.g * dv * e.qTilde;
+      S[c.Q] = s;
+    }
+  }
+  // ---- outputs: stage constants for the Newton kernels
+  for (int v = 0; v < NF + 3; v++) b.divF[(long long)v * Z + z] = div[v];
+  if (needS)
+    for (int v = 0; v < NF; v++) b.Sexp[(long long)v * Z + z] = S[v];
+  // ---- induction and the Newton guess
+  const double fac = (stage == GRIM_HALF_STEP) ? 0.5 * dt : dt;
+  for (int b3 = 0; b3 < 3; b3++) {
+    double cons = b.consOld[(long long)(NF + b3) * Z + z] - fac * div[NF + b3];
+    b.prim[(long long)(c.B1 + b3) * Z + z] = cons / G.g;
+  }
+  if (stage == GRIM_HALF_STEP)
+    for (int v = 0; v < NF; v++) b.prim[(long long)v * Z + z] = b.pold[(long long)v * Z + z];
+}
+
+// ---------------------------------------------------------------------------
+// computeDt (timestep.cpp:336-400): max over all zones (ghosts included) of
+// sum_d max(c_max/dX_d, |c_min/dX_d|) of the element state `mode` selects:
+//   0: prims as stored, 1: grid::communicate semantics (periodic ghosts
+//   wrapped, ghosts on a non-periodic edge read as zero), 2: all-zero prims
+//   (the grids the reference's elements are first set on)
+// ---------------------------------------------------------------------------
+GRIM_D void atomic_max_pos(double* addr, double v) {
+  if (!(v >= 0.)) v = 0.;
+  atomicMax((unsigned long long*)addr, (unsigned long long)__double_as_longlong(v));
+}
+
+template <int COND, int VISC>
+__global__ void k_dt_speeds(DevCfg c, const double* __restrict__ p, const double* __restrict__ geoC,
+                                     int mode, DevState* st) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double best = 0.;
+  if (z < c.Z) {
+    int i, j, k;
+    zijk(c, z, i, j, k);
+    long long src = z;
+    bool zero = (mode == 2);
+    if (mode == 1) {
+      auto m = [&](int x, int g, int N, bool per) -> int {
+        if (x >= g && x < N + g) return x;
+        if (!per) { zero = true; return x; }
+        return g + ((x - g) % N + N) % N;
+      };
+      const bool p1 = c.bc[0] == GRIM_PERIODIC || c.bc[1] == GRIM_PERIODIC;
+      const bool p2 = c.bc[2] == GRIM_PERIODIC || c.bc[3] == GRIM_PERIODIC;
+      const bool p3 = c.bc[4] == GRIM_PERIODIC || c.bc[5] == GRIM_PERIODIC;
+      int si = m(i, c.g1, c.N1, p1);
+      int sj = (c.dim >= 2) ? m(j, c.g2, c.N2, p2) : j;
+      int sk = (c.dim >= 3) ? m(k, c.g3, c.N3, p3) : k;
+      src = zidx(c, si, sj, sk);
+    }
+    const long long Z = c.Z;
+    double pv[12];
+    for (int v = 0; v < c.dof; v++) pv[v] = zero ? 0. : p[(long long)v * Z + src];
+    ZoneGeo<double> G;
+    load_geo(G, c, geoC, z, i, j, 0.5, 0.5);
+    ElemT<double, double> e;
+    elem_set<COND, VISC>(e, pv[0], pv[1], pv[2], pv[3], pv[4], pv[c.B1], pv[c.B1 + 1], pv[c.B1 + 2],
+                         COND ? pv[c.Q] : 0., VISC ? pv[c.DP] : 0., G, c);
+    double acc = 0.;
+    for (int d = 0; d < c.dim; d++) {
+      double mn, mx;
+      char_speeds<COND, VISC>(e, G, d, c, mn, mx);
+      double a = mn / c.dX[d], bb = mx / c.dX[d];
+      double m2 = fmax(bb, fabs(a));
+      acc = (d == 0) ? m2 : acc + m2;
+    }
+    best = acc;
+  }
+  // block reduction then one atomic per block
+  __shared__ double sm[32];
+  for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sm[w] = best;
+  __syncthreads();
+  if (w == 0) {
+    best = (lane < (int)(blockDim.x >> 5)) ? sm[lane] : 0.;
+    for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if (lane == 0) atomic_max_pos(&st->maxInvDt, best);
+  }
+}
+
+// dt = Courant / maxInvDt, capped at maxDtIncrement * dt (timestep.cpp:393-399)
+__global__ void k_dt_update(DevState* st, double courant, double maxInc) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double newDt = courant / st->maxInvDt;
+    if (newDt > maxInc * st->dt) newDt = maxInc * st->dt;
+    st->dtOld = st->dt;
+    st->dt = newDt;
+  }
+}
+
+__global__ void k_advance_time(DevState* st) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) st->time += st->dt;
+}
+
+// ---------------------------------------------------------------------------
+// Newton
+// ---------------------------------------------------------------------------
+template <int COND, int VISC>
+GRIM_D void load_stage_const(StageConst<5 + COND + VISC>& K, const DevCfg& c, int stage, const StageBufs& b,
+                             long long z, const ZoneGeo<double>& G) {
+  constexpr int NF = 5 + COND + VISC;
+  const long long Z = c.Z;
+  const bool needS = (c.metric != GRIM_MINKOWSKI) || COND || VISC;
+  for (int v = 0; v < NF; v++) {
+    K.Uold[v] = b.consOld[(long long)v * Z + z];
+    K.divF[v] = b.divF[(long long)v * Z + z];
+    K.Sexp[v] = needS ? b.Sexp[(long long)v * Z + z] : 0.;
+  }
+  for (int v = 0; v < 3; v++) K.B[v] = b.prim[(long long)(c.B1 + v) * Z + z];
+  const double dt = b.st->dt;
+  K.dtp = (stage == GRIM_HALF_STEP) ? dt / 2. : dt;
+  if (COND || VISC) {
+    const double* po = b.pold;
+    ElemT<double, double> eo;
+    elem_set<COND, VISC>(eo, po[z], po[Z + z], po[2 * Z + z], po[3 * Z + z], po[4 * Z + z],
+                         po[(long long)c.B1 * Z + z], po[(long long)(c.B1 + 1) * Z + z],
+                         po[(long long)(c.B1 + 2) * Z + z], COND ? po[(long long)c.Q * Z + z] : 0.,
+                         VISC ? po[(long long)c.DP * Z + z] : 0., G, c);
+    for (int m = 0; m < 4; m++) K.uCovOld[m] = eo.uCov[m];
+    K.TOld = eo.temperature;
+    ElemT<double, double> er;
+    if (stage == GRIM_HALF_STEP) {
+      er = eo;
+    } else {
+      const double* ph = b.ps;
+      elem_set<COND, VISC>(er, ph[z], ph[Z + z], ph[2 * Z + z], ph[3 * Z + z], ph[4 * Z + z],
+                           ph[(long long)c.B1 * Z + z], ph[(long long)(c.B1 + 1) * Z + z],
+                           ph[(long long)(c.B1 + 2) * Z + z], COND ? ph[(long long)c.Q * Z + z] : 0.,
+                           VISC ? ph[(long long)c.DP * Z + z] : 0., G, c);
+    }
+    K.refRho = er.rho; K.refNu = VISC ? er.nu : 0.; K.refChi = COND ? er.chi : 0.;
+    K.refTau = er.tau; K.refT = er.temperature;
+    for (int m = 0; m < 4; m++) K.refBCon[m] = er.bCon[m];
+    K.refBSqr = er.bSqr; K.refBNorm = er.bNorm; K.refUCon0 = er.uCon[0];
+    K.refQTilde = COND ? er.qTilde : 0.;
+    K.refDPTilde = VISC ? er.deltaPTilde : 0.;
+    // elemOld->computeImplicitSources(sourcesImplicitOld, ref.tau)
+    K.sImpOldQ = COND ? G.g * (eo.qTilde) / er.tau : 0.;
+    K.sImpOldDP = VISC ? G.g * (eo.deltaPTilde) / er.tau : 0.;
+    // residual normalisation (residual.cpp:291-323, :366-399)
+    if (COND) K.normQ = (c.hoCond) ? er.temperature * sqrt(er.rho * er.chi * er.tau) : er.tau;
+    if (VISC) K.normDP = (c.hoVisc) ? sqrt(er.rho * er.nu * er.temperature * er.tau) : er.tau;
+  }
+}
+
+// pivoted Gaussian elimination (the oracle's; af::solve at solve.cpp:220)
+template <class T, int N>
+GRIM_D void gauss_solve(T A[N][N], T b[N], T x[N]) {
+#pragma unroll
+  for (int kk = 0; kk < N; kk++) {
+    int p = kk;
+    T best = fabs(A[kk][kk]);
+#pragma unroll
+    for (int r = kk + 1; r < N; r++) {
+      T v = fabs(A[r][kk]);
+      if (v > best) { best = v; p = r; }
+    }
+    if (p != kk) {
+#pragma unroll
+      for (int r = kk + 1; r < N; r++) {
+        if (r == p) {
+#pragma unroll
+          for (int cc = 0; cc < N; cc++) { T t = A[kk][cc]; A[kk][cc] = A[r][cc]; A[r][cc] = t; }
+          T t = b[kk]; b[kk] = b[r]; b[r] = t;
+        }
+      }
+    }
+    const T akk = A[kk][kk];
+#pragma unroll
+    for (int r = kk + 1; r < N; r++) {
+      T l = A[r][kk] / akk;
+#pragma unroll
+      for (int cc = kk + 1; cc < N; cc++) A[r][cc] -= l * A[kk][cc];
+      b[r] -= l * b[kk];
+    }
+  }
+#pragma unroll
+  for (int r = N - 1; r >= 0; r--) {
+    T s = b[r];
+#pragma unroll
+    for (int cc = r + 1; cc < N; cc++) s -= A[r][cc] * x[cc];
+    x[r] = s / A[r][r];
+  }
+}
+
+template <int NF>
+GRIM_D double l2sum(const double* R) {
+  double s = 0.;
+#pragma unroll
+  for (int v = 0; v < NF; v++) s += R[v] * R[v];
+  return s;
+}
+
+// Parity Newton, launch 0: floor, residual, per-zone l2 and the count of
+// unconverged zones for iteration 0 (solve.cpp:17-41)
+template <int COND, int VISC>
+__global__ void __launch_bounds__(128) k_newton_fd_init(DevCfg c, int stage, StageBufs b) {
+  constexpr int NF = 5 + COND + VISC;
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int unconv = 0;
+  if (n < c.Zint) {
+    const long long Z = c.Z;
+    const long long z = interior_to_z(c, n);
+    int i, j, k;
+    zijk(c, z, i, j, k);
+    ZoneGeo<double> G;
+    load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
+    StageConst<NF> K;
+    load_stage_const<COND, VISC>(K, c, stage, b, z, G);
+    double P[NF], R[NF];
+    for (int v = 0; v < NF; v++) P[v] = b.prim[(long long)v * Z + z];
+    P[0] = fmax(P[0], c.rhoFloor);
+    P[1] = fmax(P[1], c.uFloor);
+    b.prim[z] = P[0];
+    b.prim[Z + z] = P[1];
+    zone_residual<COND, VISC, double, double>(P, K, G, c, R);
+    for (int v = 0; v < NF; v++) b.R[(long long)v * Z + z] = R[v];
+    double l2 = l2sum<NF>(R);
+    b.l2[z] = l2;
+    b.l2[Z + z] = l2;
+    double tol = fmax(c.atol, c.rtol * c.rtol * l2);
+    unconv = (l2 > tol) ? 1 : 0;
+  }
+  unconv = __syncthreads_count(unconv);
+  if (threadIdx.x == 0 && unconv) atomicAdd(&b.st->count[stage][0], (unsigned long long)unconv);
+}
+
+// Parity Newton, iteration `it` (solve.cpp:80-199): FD Jacobian, pivoted
+// solve, quadratic backtracking, update; then the floor + residual + count
+// of iteration it+1.  Returns at once when iteration `it` found every zone
+// converged (the reference's global break).
+template <int COND, int VISC>
+__global__ void __launch_bounds__(128) k_newton_fd_iter(DevCfg c, int stage, int it, StageBufs b) {
+  constexpr int NF = 5 + COND + VISC;
+  if (b.st->count[stage][it] == 0ULL) return;
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int unconv = 0;
+  if (n < c.Zint) {
+    const long long Z = c.Z;
+    const long long z = interior_to_z(c, n);
+    int i, j, k;
+    zijk(c, z, i, j, k);
+    ZoneGeo<double> G;
+    load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
+    StageConst<NF> K;
+    load_stage_const<COND, VISC>(K, c, stage, b, z, G);
+    double P[NF], R[NF];
+    for (int v = 0; v < NF; v++) {
+      P[v] = b.prim[(long long)v * Z + z];
+      R[v] = b.R[(long long)v * Z + z];
+    }
+    const double l2 = b.l2[z];
+    const double l2first = b.l2[Z + z];
+    // FD Jacobian, J[col][row] = dR_col / dP_row
+    double J[NF][NF];
+    const double eps = c.jacEps;
+#pragma unroll
+    for (int row = 0; row < NF; row++) {
+      double Pe[NF];
+#pragma unroll
+      for (int v = 0; v < NF; v++) Pe[v] = P[v];
+      double small = (fabs(P[row]) < .5 * eps) ? 1. : 0.;
+      Pe[row] = P[row] + eps * P[row] * (1. - small) + small * eps;
+      double Rp[NF];
+      zone_residual<COND, VISC, double, double>(Pe, K, G, c, Rp);
+      const double dP = Pe[row] - P[row];
+#pragma unroll
+      for (int col = 0; col < NF; col++) J[col][row] = (Rp[col] - R[col]) / dP;
+    }
+    double bvec[NF], dPv[NF];
+#pragma unroll
+    for (int v = 0; v < NF; v++) bvec[v] = -R[v];
+    gauss_solve<double, NF>(J, bvec, dPv);
+    // line search
+    const double f0 = 0.5 * l2;
+    const double fPrime0 = -2. * f0;
+    double lam = 1.;
+    bool haveRt = false;
+    double Rt[NF];
+    for (int ls = 0; ls < c.maxLS; ls++) {
+      double Pt[NF];
+#pragma unroll
+      for (int v = 0; v < NF; v++) Pt[v] = P[v] + lam * dPv[v];
+      zone_residual<COND, VISC, double, double>(Pt, K, G, c, Rt);
+      const double f1 = 0.5 * l2sum<NF>(Rt);
+      const double alpha = 1e-4;
+      if (!(f1 > (f0 * (1. - alpha * lam) + c.lsFloor))) { haveRt = true; break; }
+      const double denom = (f1 - f0 - fPrime0 * lam);
+      lam = -fPrime0 * lam * lam / denom / 2.;
+    }
+#pragma unroll
+    for (int v = 0; v < NF; v++) P[v] = P[v] + lam * dPv[v];
+    if (it + 1 < c.maxIter) {
+      const bool floored = (P[0] < c.rhoFloor) || (P[1] < c.uFloor);
+      P[0] = fmax(P[0], c.rhoFloor);
+      P[1] = fmax(P[1], c.uFloor);
+      if (!haveRt || floored) zone_residual<COND, VISC, double, double>(P, K, G, c, Rt);
+      const double l2n = l2sum<NF>(Rt);
+      for (int v = 0; v < NF; v++) b.R[(long long)v * Z + z] = Rt[v];
+      b.l2[z] = l2n;
+      double tol = fmax(c.atol, c.rtol * c.rtol * l2first);
+      unconv = (l2n > tol) ? 1 : 0;
+    }
+    for (int v = 0; v < NF; v++) b.prim[(long long)v * Z + z] = P[v];
+  }
+  unconv = __syncthreads_count(unconv);
+  if (threadIdx.x == 0) {
+    if (unconv) atomicAdd(&b.st->count[stage][it + 1], (unsigned long long)unconv);
+    if (blockIdx.x == 0) atomicAdd(&b.st->itersDone[stage], 1ULL);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fast Newton: per-zone convergence, exact Jacobian from one forward-tangent
+// pass of the residual; T = double (TANGENT64) or float (MIXED32: Jacobian
+// and solve in FP32, residual in FP64, i.e. FP32 inexact Newton refined by
+// the FP64 residual).
+// ---------------------------------------------------------------------------
+template <int COND, int VISC, class T>
+GRIM_D void tangent_jacobian(const double* P, const StageConst<5 + COND + VISC>& K, const ZoneGeo<T>& Gt,
+                             const DevCfg& c, T J[5 + COND + VISC][5 + COND + VISC]) {
+  constexpr int NF = 5 + COND + VISC;
+  typedef Dual<T, NF> D;
+  D Pd[NF], Rd[NF];
+#pragma unroll
+  for (int v = 0; v < NF; v++) Pd[v] = D::var((T)P[v], v);
+  zone_residual<COND, VISC, D, T>(Pd, K, Gt, c, Rd);
+#pragma unroll
+  for (int r = 0; r < NF; r++)
+#pragma unroll
+    for (int cc = 0; cc < NF; cc++) J[r][cc] = Rd[r].d[cc];
+}
+
+template <int COND, int VISC, class T>
+__global__ void __launch_bounds__(128) k_newton_fast(DevCfg c, int stage, StageBufs b,
+                                                              const int* __restrict__ list, long long nlist) {
+  constexpr int NF = 5 + COND + VISC;
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int unconv = 0, itsMax = 0;
+  if (n < nlist) {
+    const long long Z = c.Z;
+    const long long z = list ? (long long)list[n] : interior_to_z(c, n);
+    int i, j, k;
+    zijk(c, z, i, j, k);
+    ZoneGeo<double> G;
+    load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
+    ZoneGeo<T> Gt;
+#pragma unroll
+    for (int m = 0; m < 4; m++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = (T)G.gcov[m][q]; Gt.gcon[m][q] = (T)G.gcon[m][q]; }
+    Gt.g = (T)G.g; Gt.alpha = (T)G.alpha; Gt.x1 = (T)G.x1; Gt.x2 = (T)G.x2;
+    StageConst<NF> K;
+    load_stage_const<COND, VISC>(K, c, stage, b, z, G);
+    double P[NF], R[NF];
+    for (int v = 0; v < NF; v++) P[v] = b.prim[(long long)v * Z + z];
+    bool haveR = false;
+    double l2first = 0.;
+    int it = 0;
+    bool conv = false;
+    for (; it < c.maxIter; it++) {
+      const bool floored = (P[0] < c.rhoFloor) || (P[1] < c.uFloor);
+      P[0] = fmax(P[0], c.rhoFloor);
+      P[1] = fmax(P[1], c.uFloor);
+      if (!haveR || floored) zone_residual<COND, VISC, double, double>(P, K, G, c, R);
+      const double l2 = l2sum<NF>(R);
+      if (it == 0) l2first = l2;
+      if (l2 <= fmax(c.atol, c.rtol * c.rtol * l2first)) { conv = true; break; }
+      T J[NF][NF];
+      tangent_jacobian<COND, VISC, T>(P, K, Gt, c, J);
+      T bv[NF], xv[NF];
+#pragma unroll
+      for (int v = 0; v < NF; v++) bv[v] = (T)(-R[v]);
+      gauss_solve<T, NF>(J, bv, xv);
+      double dPv[NF];
+#pragma unroll
+      for (int v = 0; v < NF; v++) dPv[v] = (double)xv[v];
+      const double f0 = 0.5 * l2, fPrime0 = -2. * f0;
+      double lam = 1.;
+      haveR = false;
+      double Rt[NF];
+      for (int ls = 0; ls < c.maxLS; ls++) {
+        double Pt[NF];
+#pragma unroll
+        for (int v = 0; v < NF; v++) Pt[v] = P[v] + lam * dPv[v];
+        zone_residual<COND, VISC, double, double>(Pt, K, G, c, Rt);
+        const double f1 = 0.5 * l2sum<NF>(Rt);
+        if (!(f1 > (f0 * (1. - 1e-4 * lam) + c.lsFloor))) { haveR = true; break; }
+        const double denom = (f1 - f0 - fPrime0 * lam);
+        lam = -fPrime0 * lam * lam / denom / 2.;
+      }
+#pragma unroll
+      for (int v = 0; v < NF; v++) {
+        P[v] = P[v] + lam * dPv[v];
+        if (haveR) R[v] = Rt[v];
+      }
+    }
+    if (!conv && it == c.maxIter) {
+      // final check of the last update (the state that is returned)
+      const double l2 = haveR ? l2sum<NF>(R) : -1.;
+      if (!(l2 >= 0. && l2 <= fmax(c.atol, c.rtol * c.rtol * l2first))) unconv = 1;
+    }
+    itsMax = it;
+    for (int v = 0; v < NF; v++) b.prim[(long long)v * Z + z] = P[v];
+  }
+  unconv = __syncthreads_count(unconv);
+  // iterations done: max over zones (warp max then atomic)
+  for (int o = 16; o > 0; o >>= 1) itsMax = max(itsMax, __shfl_xor_sync(0xffffffffu, itsMax, o));
+  if ((threadIdx.x & 31) == 0) atomicMax((unsigned long long*)&b.st->itersDone[stage], (unsigned long long)itsMax);
+  if (threadIdx.x == 0 && unconv) atomicAdd(&b.st->finalUnconv[stage], (unsigned long long)unconv);
+}
+
+// ---------------------------------------------------------------------------
+// kernels behind the test entry points
+// ---------------------------------------------------------------------------
+template <int COND, int VISC>
+__global__ void k_residual(DevCfg c, int stage, StageBufs b, const double* __restrict__ pg,
+                                    double* __restrict__ out) {
+  constexpr int NF = 5 + COND + VISC;
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  const long long Z = c.Z;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  bool inner = i >= c.g1 && i < c.N1 + c.g1 && j >= c.g2 && j < c.N2 + c.g2 && k >= c.g3 && k < c.N3 + c.g3;
+  if (!inner) {
+    for (int v = 0; v < NF; v++) out[(long long)v * Z + z] = 0.;
+    return;
+  }
+  ZoneGeo<double> G;
+  load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
+  StageConst<NF> K;
+  load_stage_const<COND, VISC>(K, c, stage, b, z, G);
+  for (int v = 0; v < 3; v++) K.B[v] = pg[(long long)(c.B1 + v) * Z + z];
+  double P[NF], R[NF];
+  for (int v = 0; v < NF; v++) P[v] = pg[(long long)v * Z + z];
+  zone_residual<COND, VISC, double, double>(P, K, G, c, R);
+  for (int v = 0; v < NF; v++) out[(long long)v * Z + z] = R[v];
+}
+
+template <int COND, int VISC>
+__global__ void k_jacobian(DevCfg c, int stage, StageBufs b, const double* __restrict__ pg,
+                                    double* __restrict__ jac, int tangent) {
+  constexpr int NF = 5 + COND + VISC;
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  const long long Z = c.Z;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  bool inner = i >= c.g1 && i < c.N1 + c.g1 && j >= c.g2 && j < c.N2 + c.g2 && k >= c.g3 && k < c.N3 + c.g3;
+  double J[NF][NF];
+  for (int a = 0; a < NF; a++)
+    for (int q = 0; q < NF; q++) J[a][q] = 0.;
+  if (inner) {
+    ZoneGeo<double> G;
+    load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
+    StageConst<NF> K;
+    load_stage_const<COND, VISC>(K, c, stage, b, z, G);
+    for (int v = 0; v < 3; v++) K.B[v] = pg[(long long)(c.B1 + v) * Z + z];
+    double P[NF], R[NF];
+    for (int v = 0; v < NF; v++) P[v] = pg[(long long)v * Z + z];
+    if (tangent) {
+      tangent_jacobian<COND, VISC, double>(P, K, G, c, J);
+    } else {
+      zone_residual<COND, VISC, double, double>(P, K, G, c, R);
+      const double eps = c.jacEps;
+      for (int row = 0; row < NF; row++) {
+        double Pe[NF];
+        for (int v = 0; v < NF; v++) Pe[v] = P[v];
+        double small = (fabs(P[row]) < .5 * eps) ? 1. : 0.;
+        Pe[row] = P[row] + eps * P[row] * (1. - small) + small * eps;
+        double Rp[NF];
+        zone_residual<COND, VISC, double, double>(Pe, K, G, c, Rp);
+        for (int col = 0; col < NF; col++) J[col][row] = (Rp[col] - R[col]) / (Pe[row] - P[row]);
+      }
+    }
+  }
+  for (int a = 0; a < NF; a++)
+    for (int q = 0; q < NF; q++) jac[(z * NF + a) * NF + q] = J[a][q];
+}
+
+// conserved variables / characteristic speeds of a prim array
+template <int COND, int VISC>
+__global__ void k_conserved(DevCfg c, const double* __restrict__ p, const double* __restrict__ geoC,
+                                     double* __restrict__ out, int dir, double* mn, double* mx) {
+  constexpr int NF = 5 + COND + VISC;
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  const long long Z = c.Z;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  ZoneGeo<double> G;
+  load_geo(G, c, geoC, z, i, j, 0.5, 0.5);
+  ElemT<double, double> e;
+  elem_set<COND, VISC>(e, p[z], p[Z + z], p[2 * Z + z], p[3 * Z + z], p[4 * Z + z], p[(long long)c.B1 * Z + z],
+                       p[(long long)(c.B1 + 1) * Z + z], p[(long long)(c.B1 + 2) * Z + z],
+                       COND ? p[(long long)c.Q * Z + z] : 0., VISC ? p[(long long)c.DP * Z + z] : 0., G, c);
+  if (out) {
+    double U[NF], UB[3];
+    fluxes_fluid<COND, VISC>(e, 0, G.g, U, 5, 5 + COND);
+    fluxes_B(e, 0, G.g, UB);
+    for (int v = 0; v < NF; v++) out[(long long)v * Z + z] = U[v];
+    for (int v = 0; v < 3; v++) out[(long long)(NF + v) * Z + z] = UB[v];
+  }
+  if (mn) {
+    double a, bb;
+    char_speeds<COND, VISC>(e, G, dir, c, a, bb);
+    mn[z] = a;
+    mx[z] = bb;
+  }
+}
+
+// reconstruction of one direction for every zone (test entry point)
+__global__ void k_reconstruct(DevCfg c, int dir, const double* __restrict__ p, double* __restrict__ pl,
+                                       double* __restrict__ pr) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  const int NT = (dir == 0) ? c.N1T : (dir == 1 ? c.N2T : c.N3T);
+  const int x = (dir == 0) ? i : (dir == 1 ? j : k);
+  const long long s = stride_of(c, dir);
+  for (int v = 0; v < c.dof; v++) {
+    const double* a = p + (long long)v * c.Z;
+    double y[5];
+    for (int m = 0; m < 5; m++) {
+      int xx = x + m - 2;
+      xx = ((xx % NT) + NT) % NT;  // circular, af::shift semantics
+      y[m] = a[z + (long long)(xx - x) * s];
+    }
+    double lo, ro;
+    recon_faces(c.reconstruction, c.theta, y[0], y[1], y[2], y[3], y[4], lo, ro);
+    pl[(long long)v * c.Z + z] = lo;
+    pr[(long long)v * c.Z + z] = ro;
+  }
+}
+
+// batched dense solve (test entry point), one system per thread
+template <int N>
+__global__ void k_batch_solve(int batch, const double* __restrict__ A, const double* __restrict__ b,
+                                       double* __restrict__ x) {
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= batch) return;
+  double a[N][N], bb[N], xx[N];
+  for (int r = 0; r < N; r++) {
+    bb[r] = b[n * N + r];
+    for (int q = 0; q < N; q++) a[r][q] = A[(n * N + r) * N + q];
+  }
+  gauss_solve<double, N>(a, bb, xx);
+  for (int r = 0; r < N; r++) x[n * N + r] = xx[r];
+}
+
+// non-finite primitives count (diagnostic after each step)
+__global__ void k_count_nonfinite(DevCfg c, const double* __restrict__ p, DevState* st) {
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int bad = 0;
+  if (n < c.Zint) {
+    long long z = interior_to_z(c, n);
+    for (int v = 0; v < c.dof; v++) {
+      double a = p[(long long)v * c.Z + z];
+      if (!isfinite(a)) bad = 1;
+    }
+  }
+  bad = __syncthreads_count(bad);
+  if (threadIdx.x == 0 && bad) atomicAdd(&st->nonFinite, (unsigned long long)bad);
+}
+
+}  // namespace GRIM_KNS
+}  // namespace grim
+
+// ---------------------------------------------------------------------------
+// launchers (declared in launch.h)
+// ---------------------------------------------------------------------------
+namespace grim {
+namespace GRIM_KNS {
+
+static inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+#define GRIM_EMHD_DISPATCH(c, KERNEL, ...)                              \
+  do {                                                                  \
+    if ((c).conduction && (c).viscosity) KERNEL<1, 1>(__VA_ARGS__);     \
+    else if ((c).conduction) KERNEL<1, 0>(__VA_ARGS__);                 \
+    else if ((c).viscosity) KERNEL<0, 1>(__VA_ARGS__);                  \
+    else KERNEL<0, 0>(__VA_ARGS__);                                     \
+  } while (0)
+
+void ghost_fill(const DevCfg& c, double* prim, int nv, cudaStream_t s) {
+  k_ghost_fill<<<nblk(c.Z, 256), 256, 0, s>>>(c, prim, nv);
+}
+
+template <int C, int V>
+static void emhd_prepass_t(const DevCfg& c, const double* ps, const double* geoC, double* uT, cudaStream_t s) {
+  k_emhd_prepass<C, V><<<nblk(c.Z, 128), 128, 0, s>>>(c, ps, geoC, uT);
+}
+void emhd_prepass(const DevCfg& c, const double* ps, const double* geoC, double* uT, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, emhd_prepass_t, c, ps, geoC, uT, s);
+}
+
+template <int C, int V>
+static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,
+                        double* flux, cudaStream_t s) {
+  k_face_flux<C, V><<<nblk(c.Z, 128), 128, 0, s>>>(c, dir, ps, geoF, geoC, flux);
+}
+void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC, double* flux,
+               cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, face_flux_t, c, dir, ps, geoF, geoC, flux, s);
+}
+
+template <int C, int V>
+static void stage_epilogue_t(const DevCfg& c, int stage, const StageBufs& b, cudaStream_t s) {
+  k_stage_epilogue<C, V><<<nblk(c.Zint, 128), 128, 0, s>>>(c, stage, b);
+}
+void stage_epilogue(const DevCfg& c, int stage, const StageBufs& b, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, stage_epilogue_t, c, stage, b, s);
+}
+
+template <int C, int V>
+static void dt_speeds_t(const DevCfg& c, const double* p, const double* geoC, int mode, DevState* st,
+                        cudaStream_t s) {
+  k_dt_speeds<C, V><<<nblk(c.Z, 256), 256, 0, s>>>(c, p, geoC, mode, st);
+}
+void dt_speeds(const DevCfg& c, const double* p, const double* geoC, int mode, DevState* st, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, dt_speeds_t, c, p, geoC, mode, st, s);
+}
+void dt_update(DevState* st, double courant, double maxInc, cudaStream_t s) {
+  k_dt_update<<<1, 32, 0, s>>>(st, courant, maxInc);
+}
+void advance_time(DevState* st, cudaStream_t s) { k_advance_time<<<1, 32, 0, s>>>(st); }
+
+template <int C, int V>
+static void newton_fd_init_t(const DevCfg& c, int stage, const StageBufs& b, cudaStream_t s) {
+  k_newton_fd_init<C, V><<<nblk(c.Zint, 128), 128, 0, s>>>(c, stage, b);
+}
+void newton_fd_init(const DevCfg& c, int stage, const StageBufs& b, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, newton_fd_init_t, c, stage, b, s);
+}
+template <int C, int V>
+static void newton_fd_iter_t(const DevCfg& c, int stage, int it, const StageBufs& b, cudaStream_t s) {
+  k_newton_fd_iter<C, V><<<nblk(c.Zint, 128), 128, 0, s>>>(c, stage, it, b);
+}
+void newton_fd_iter(const DevCfg& c, int stage, int it, const StageBufs& b, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, newton_fd_iter_t, c, stage, it, b, s);
+}
+
+template <int C, int V>
+static void newton_fast_t(const DevCfg& c, int stage, const StageBufs& b, int mode, const int* list,
+                          long long nlist, cudaStream_t s) {
+  if (nlist <= 0) return;
+  if (mode == GRIM_NEWTON_MIXED32)
+    k_newton_fast<C, V, float><<<nblk(nlist, 128), 128, 0, s>>>(c, stage, b, list, nlist);
+  else
+    k_newton_fast<C, V, double><<<nblk(nlist, 128), 128, 0, s>>>(c, stage, b, list, nlist);
+}
+void newton_fast(const DevCfg& c, int stage, const StageBufs& b, int mode, const int* list, long long nlist,
+                 cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, newton_fast_t, c, stage, b, mode, list, nlist, s);
+}
+
+template <int C, int V>
+static void residual_t(const DevCfg& c, int stage, const StageBufs& b, const double* pg, double* out,
+                       cudaStream_t s) {
+  k_residual<C, V><<<nblk(c.Z, 128), 128, 0, s>>>(c, stage, b, pg, out);
+}
+void residual(const DevCfg& c, int stage, const StageBufs& b, const double* pg, double* out, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, residual_t, c, stage, b, pg, out, s);
+}
+template <int C, int V>
+static void jacobian_t(const DevCfg& c, int stage, const StageBufs& b, const double* pg, double* jac, int tangent,
+                       cudaStream_t s) {
+  k_jacobian<C, V><<<nblk(c.Z, 128), 128, 0, s>>>(c, stage, b, pg, jac, tangent);
+}
+void jacobian(const DevCfg& c, int stage, const StageBufs& b, const double* pg, double* jac, int tangent,
+              cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, jacobian_t, c, stage, b, pg, jac, tangent, s);
+}
+template <int C, int V>
+static void conserved_t(const DevCfg& c, const double* p, const double* geoC, double* out, int dir, double* mn,
+                        double* mx, cudaStream_t s) {
+  k_conserved<C, V><<<nblk(c.Z, 128), 128, 0, s>>>(c, p, geoC, out, dir, mn, mx);
+}
+void conserved(const DevCfg& c, const double* p, const double* geoC, double* out, int dir, double* mn, double* mx,
+               cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, conserved_t, c, p, geoC, out, dir, mn, mx, s);
+}
+void reconstruct(const DevCfg& c, int dir, const double* p, double* pl, double* pr, cudaStream_t s) {
+  k_reconstruct<<<nblk(c.Z, 128), 128, 0, s>>>(c, dir, p, pl, pr);
+}
+int batch_solve(int n, int batch, const double* A, const double* b, double* x, cudaStream_t s) {
+  const unsigned g = nblk(batch, 128);
+  switch (n) {
+    case 1: k_batch_solve<1><<<g, 128, 0, s>>>(batch, A, b, x); return 0;
+    case 2: k_batch_solve<2><<<g, 128, 0, s>>>(batch, A, b, x); return 0;
+    case 3: k_batch_solve<3><<<g, 128, 0, s>>>(batch, A, b, x); return 0;
+    case 4: k_batch_solve<4><<<g, 128, 0, s>>>(batch, A, b, x); return 0;
+    case 5: k_batch_solve<5><<<g, 128, 0, s>>>(batch, A, b, x); return 0;
+    case 6: k_batch_solve<6><<<g, 128, 0, s>>>(batch, A, b, x); return 0;
+    case 7: k_batch_solve<7><<<g, 128, 0, s>>>(batch, A, b, x); return 0;
+    case 8: k_batch_solve<8><<<g, 128, 0, s>>>(batch, A, b, x); return 0;
+    default: return -1;
+  }
+}
+void count_nonfinite(const DevCfg& c, const double* p, DevState* st, cudaStream_t s) {
+  k_count_nonfinite<<<nblk(c.Zint, 256), 256, 0, s>>>(c, p, st);
+}
+
+}  // namespace GRIM_KNS
+}  // namespace grim

@@ -1,0 +1,5 @@
+// kernels_fast.cu -- kernel instantiations compiled with FMA contraction on:
+// the tangent / mixed-precision paths.
+#define GRIM_KNS fast
+#include "kernels.cuh"
+#include "launch.h"

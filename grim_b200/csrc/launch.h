@@ -1,0 +1,36 @@
+// launch.h -- host-side launchers of the kernels of one translation unit.
+// kernels_exact.cu defines them in grim::exact (FP64 without FMA
+// contraction: the parity path), kernels_fast.cu in grim::fast.
+#pragma once
+#include "stage.cuh"
+
+#define GRIM_DECLARE_LAUNCHERS(NS)                                                                      \
+  namespace grim {                                                                                      \
+  namespace NS {                                                                                        \
+  void ghost_fill(const DevCfg& c, double* prim, int nv, cudaStream_t s);                               \
+  void emhd_prepass(const DevCfg& c, const double* ps, const double* geoC, double* uT, cudaStream_t s); \
+  void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,    \
+                 double* flux, cudaStream_t s);                                                         \
+  void stage_epilogue(const DevCfg& c, int stage, const StageBufs& b, cudaStream_t s);                  \
+  void dt_speeds(const DevCfg& c, const double* p, const double* geoC, int mode, DevState* st,          \
+                 cudaStream_t s);                                                                       \
+  void dt_update(DevState* st, double courant, double maxInc, cudaStream_t s);                          \
+  void advance_time(DevState* st, cudaStream_t s);                                                      \
+  void newton_fd_init(const DevCfg& c, int stage, const StageBufs& b, cudaStream_t s);                  \
+  void newton_fd_iter(const DevCfg& c, int stage, int it, const StageBufs& b, cudaStream_t s);          \
+  void newton_fast(const DevCfg& c, int stage, const StageBufs& b, int mode, const int* list,           \
+                   long long nlist, cudaStream_t s);                                                    \
+  void residual(const DevCfg& c, int stage, const StageBufs& b, const double* pg, double* out,         \
+                cudaStream_t s);                                                                        \
+  void jacobian(const DevCfg& c, int stage, const StageBufs& b, const double* pg, double* jac,         \
+                int tangent, cudaStream_t s);                                                           \
+  void conserved(const DevCfg& c, const double* p, const double* geoC, double* out, int dir,           \
+                 double* mn, double* mx, cudaStream_t s);                                               \
+  void reconstruct(const DevCfg& c, int dir, const double* p, double* pl, double* pr, cudaStream_t s); \
+  int batch_solve(int n, int batch, const double* A, const double* b, double* x, cudaStream_t s);      \
+  void count_nonfinite(const DevCfg& c, const double* p, DevState* st, cudaStream_t s);                \
+  }                                                                                                     \
+  }
+
+GRIM_DECLARE_LAUNCHERS(exact)
+GRIM_DECLARE_LAUNCHERS(fast)

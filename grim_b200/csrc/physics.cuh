@@ -1,0 +1,336 @@
+// physics.cuh -- per-zone GRMHD/EMHD physics as device functions.
+//
+// One fluid element is evaluated in registers for one zone; nothing is
+// materialised in HBM (the reference keeps ~80 full-grid temporaries per
+// element, src/physics/physics.cpp:53-183).  Templated on the scalar type of
+// the unknown-dependent quantities (double for the residual, float or
+// Dual<.,nf> for the Jacobian) and on the real type R of constants.
+// Operation order follows the reference expression by expression so the
+// FP64 build without FMA contraction reproduces the oracle bit for bit.
+#pragma once
+#include "common.cuh"
+
+namespace grim {
+
+template <class R>
+struct ZoneGeo {
+  R gcov[4][4];
+  R gcon[4][4];
+  R g, alpha;
+  R x1, x2;  // physical coordinates (closures)
+};
+
+// Minkowski at compile time; MKS from the stored per-location arrays
+// (layout: 16 gCov, 16 gCon, g, alpha, x1, x2 -> 36 words per zone, SoA).
+enum { GEO_WORDS = 36 };
+
+template <class R>
+GRIM_D void geo_minkowski(ZoneGeo<R>& G, R x1, R x2) {
+#pragma unroll
+  for (int m = 0; m < 4; m++)
+#pragma unroll
+    for (int n = 0; n < 4; n++) { G.gcov[m][n] = R(0); G.gcon[m][n] = R(0); }
+  G.gcov[0][0] = R(-1); G.gcov[1][1] = R(1); G.gcov[2][2] = R(1); G.gcov[3][3] = R(1);
+  G.gcon[0][0] = R(-1); G.gcon[1][1] = R(1); G.gcon[2][2] = R(1); G.gcon[3][3] = R(1);
+  G.g = R(1); G.alpha = R(1);
+  G.x1 = x1; G.x2 = x2;
+}
+
+template <class R>
+GRIM_D void geo_load(ZoneGeo<R>& G, const double* __restrict__ geo, long long Z, long long z) {
+#pragma unroll
+  for (int m = 0; m < 4; m++)
+#pragma unroll
+    for (int n = 0; n < 4; n++) {
+      G.gcov[m][n] = (R)__ldg(geo + (long long)(m * 4 + n) * Z + z);
+      G.gcon[m][n] = (R)__ldg(geo + (long long)(16 + m * 4 + n) * Z + z);
+    }
+  G.g = (R)__ldg(geo + 32LL * Z + z);
+  G.alpha = (R)__ldg(geo + 33LL * Z + z);
+  G.x1 = (R)__ldg(geo + 34LL * Z + z);
+  G.x2 = (R)__ldg(geo + 35LL * Z + z);
+}
+
+template <class S, class R>
+struct ElemT {
+  S rho, u, u1, u2, u3, pressure, temperature, soundSpeed, gam;
+  R B1, B2, B3;
+  S uCon[4], uCov[4], bCon[4], bCov[4], bSqr, bNorm;
+  S qTilde, deltaPTilde, q, deltaP, tau, chi, nu;
+};
+
+// --- scalar helpers for the torus closure ---------------------------------
+GRIM_HD double dexp(double x) { return exp(x); }
+GRIM_HD float dexp(float x) { return expf(x); }
+template <class T, int N>
+GRIM_HD Dual<T, N> dexp(const Dual<T, N>& a) {
+  Dual<T, N> r; r.v = dexp(a.v);
+#pragma unroll
+  for (int k = 0; k < N; k++) r.d[k] = a.d[k] * r.v;
+  return r;
+}
+GRIM_HD double dfabs(double x) { return fabs(x); }
+GRIM_HD float dfabs(float x) { return fabsf(x); }
+template <class T, int N>
+GRIM_HD Dual<T, N> dfabs(const Dual<T, N>& a) { return a.v < T(0) ? -a : a; }
+GRIM_HD double dmin2(double a, double b) { return fmin(a, b); }
+GRIM_HD float dmin2(float a, float b) { return fminf(a, b); }
+template <class T, int N>
+GRIM_HD Dual<T, N> dmin2(const Dual<T, N>& a, const Dual<T, N>& b) { return (b.v < a.v) ? b : a; }
+GRIM_HD double dmax2(double a, double b) { return fmax(a, b); }
+GRIM_HD float dmax2(float a, float b) { return fmaxf(a, b); }
+template <class T, int N>
+GRIM_HD Dual<T, N> dmax2(const Dual<T, N>& a, const Dual<T, N>& b) { return (b.v > a.v) ? b : a; }
+GRIM_HD double dcube(double x) { return pow(x, 3.); }
+GRIM_HD float dcube(float x) { return x * x * x; }
+template <class T, int N>
+GRIM_HD Dual<T, N> dcube(const Dual<T, N>& a) { return a * a * a; }
+
+// setFluidElementParameters (problem hook) -- closures
+template <class S, class R>
+GRIM_D void closure(ElemT<S, R>& e, const ZoneGeo<R>& G, const DevCfg& c) {
+  const S cs = e.soundSpeed;
+  if (c.closure == GRIM_CLOSURE_CONST_TAU) {
+    // linear_modes/problem.cpp:3-8
+    e.tau = Lift<S>::of(c.tau0);
+    e.chi = cs * cs * e.tau;
+    e.nu = cs * cs * e.tau;
+  } else if (c.closure == GRIM_CLOSURE_TAU_PROFILE) {
+    R s = (G.x2 - (R)c.X2Start) / ((R)c.X2End - (R)c.X2Start);
+    e.tau = Lift<S>::of((double)((R)c.tau0 + ((R)c.tau1 - (R)c.tau0) * s));
+    e.chi = cs * cs * e.tau;
+    e.nu = cs * cs * e.tau;
+  } else {
+    // torus/problem.cpp:7-55
+    typedef typename Real<S>::type T;
+    const T Radius = (T)G.x1;
+    const T Dyn = (T)pow((double)Radius, 1.5);
+    S t = Lift<S>::of((double)Dyn);
+    if (c.conduction) {
+      S Qmax = (T)c.CondClosure * e.rho * dcube(cs);
+      const T lambda = (T)0.01;
+      S yCon = dfabs(e.q) / Qmax;
+      yCon = dexp(-(yCon - T(1.)) / lambda);
+      S fdCon = yCon / (yCon + T(1.)) + T(1.e-5);
+      t = dmin2(t, Dyn * fdCon);
+    }
+    if (c.viscosity) {
+      const T fl = (T)c.bSqrFloor;
+      const S p = e.pressure, dP = e.deltaP;
+      S dPmod = dmaxc(p - T(2. / 3.) * dP, fl) / dmaxc(p + T(1. / 3.) * dP, fl);
+      S dPmaxPlus = dmin2((T)c.ViscClosure * e.bSqr * T(0.5) * dPmod, T(1.49) * p / T(1.07));
+      S dPmaxMinus = dmax2(-(T)c.ViscClosure * e.bSqr, -T(2.99) * p / T(1.07));
+      S dPmax = (val(dP) > T(0.)) ? dPmaxPlus : dPmaxMinus;
+      const T lambda = (T)0.01;
+      S yVis = dfabs(dP) / (dfabs(dPmax) + fl);
+      yVis = dexp(-(yVis - T(1.)) / lambda);
+      S fdVis = yVis / (yVis + T(1.)) + T(1.e-5);
+      t = dmin2(t, Dyn * fdVis);
+    }
+    e.tau = t;
+    S maxAlpha = (T(1.) - cs * cs) / (T(2.) * cs * cs + T(1.e-12));
+    e.chi = dmin2(maxAlpha, Lift<S>::of(c.CondAlpha)) * cs * cs * t;
+    e.nu = dmin2(maxAlpha, Lift<S>::of(c.ViscAlpha)) * cs * cs * t;
+  }
+}
+
+// fluidElement::set (physics.cpp:53-183) minus T^mu_nu, which callers take
+// row by row with tmunu().
+template <int COND, int VISC, class S, class R>
+GRIM_D void elem_set(ElemT<S, R>& e, const S& rho_in, const S& u_in, const S& v1, const S& v2,
+                     const S& v3, R B1, R B2, R B3, const S& qT, const S& dPT,
+                     const ZoneGeo<R>& G, const DevCfg& c) {
+  typedef typename Real<S>::type T;
+  const T Gam = (T)c.Gam;
+  e.rho = dmaxc(rho_in, (T)c.rhoFloor);
+  e.u = dmaxc(u_in, (T)c.uFloor);
+  e.u1 = v1; e.u2 = v2; e.u3 = v3;
+  e.B1 = B1; e.B2 = B2; e.B3 = B3;
+  e.pressure = (Gam - T(1.)) * e.u;
+  e.temperature = dmaxc(e.pressure / e.rho, (T)c.TFloor);
+  e.soundSpeed = dsqrt(Gam * e.pressure / (e.rho + Gam * e.u));
+  e.gam = dsqrt(T(1) + G.gcov[1][1] * v1 * v1 + G.gcov[2][2] * v2 * v2 + G.gcov[3][3] * v3 * v3 +
+                T(2) * (G.gcov[1][2] * v1 * v2 + G.gcov[1][3] * v1 * v3 + G.gcov[2][3] * v2 * v3));
+  e.uCon[0] = e.gam / G.alpha;
+  e.uCon[1] = v1 - e.gam * G.gcon[0][1] * G.alpha;
+  e.uCon[2] = v2 - e.gam * G.gcon[0][2] * G.alpha;
+  e.uCon[3] = v3 - e.gam * G.gcon[0][3] * G.alpha;
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++)
+    e.uCov[mu] = G.gcov[mu][0] * e.uCon[0] + G.gcov[mu][1] * e.uCon[1] + G.gcov[mu][2] * e.uCon[2] +
+                 G.gcov[mu][3] * e.uCon[3];
+  e.bCon[0] = B1 * e.uCov[1] + B2 * e.uCov[2] + B3 * e.uCov[3];
+  e.bCon[1] = (B1 + e.bCon[0] * e.uCon[1]) / e.uCon[0];
+  e.bCon[2] = (B2 + e.bCon[0] * e.uCon[2]) / e.uCon[0];
+  e.bCon[3] = (B3 + e.bCon[0] * e.uCon[3]) / e.uCon[0];
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++)
+    e.bCov[mu] = G.gcov[mu][0] * e.bCon[0] + G.gcov[mu][1] * e.bCon[1] + G.gcov[mu][2] * e.bCon[2] +
+                 G.gcov[mu][3] * e.bCon[3];
+  e.bSqr = e.bCon[0] * e.bCov[0] + e.bCon[1] * e.bCov[1] + e.bCon[2] * e.bCov[2] +
+           e.bCon[3] * e.bCov[3] + (T)c.bSqrFloor;
+  e.bNorm = dsqrt(e.bSqr);
+  const S cs = e.soundSpeed;
+  if (COND) {
+    e.qTilde = qT;
+    if (c.hoCond == 1)
+      e.q = qT * e.temperature * dsqrt(e.rho * (T)c.CondAlpha * cs * cs);
+    else
+      e.q = qT;
+  }
+  if (VISC) {
+    e.deltaPTilde = dPT;
+    if (c.hoVisc == 1)
+      e.deltaP = dPT * dsqrt(e.temperature * e.rho * (T)c.ViscAlpha * cs * cs);
+    else
+      e.deltaP = dPT;
+  }
+  if (COND || VISC) closure(e, G, c);
+}
+
+// T^mu_nu (physics.cpp:153-178)
+template <int COND, int VISC, class S, class R>
+GRIM_D S tmunu(const ElemT<S, R>& e, int mu, int nu) {
+  typedef typename Real<S>::type T;
+  const T d = (mu == nu) ? T(1.) : T(0.);
+  S w = e.rho + e.u + e.pressure + e.bSqr;
+  S pt = e.pressure + T(0.5) * e.bSqr;
+  S r = w * e.uCon[mu] * e.uCov[nu] + pt * d - e.bCon[mu] * e.bCov[nu];
+  if (COND) r += e.q / e.bNorm * (e.uCon[mu] * e.bCov[nu] + e.bCon[mu] * e.uCov[nu]);
+  if (VISC) r += (-e.deltaP) * (e.bCon[mu] * e.bCov[nu] / e.bSqr - T(1. / 3.) * (d + e.uCon[mu] * e.uCov[nu]));
+  return r;
+}
+
+// computeFluxes(dir) for the fluid rows (physics.cpp:185-217): out[0..nf)
+template <int COND, int VISC, class S, class R>
+GRIM_D void fluxes_fluid(const ElemT<S, R>& e, int dir, R g, S* out, int Q, int DP) {
+  S fr = g * (e.rho * e.uCon[dir]);
+  out[0] = fr;
+  out[1] = g * tmunu<COND, VISC>(e, dir, 0) + fr;
+  out[2] = g * tmunu<COND, VISC>(e, dir, 1);
+  out[3] = g * tmunu<COND, VISC>(e, dir, 2);
+  out[4] = g * tmunu<COND, VISC>(e, dir, 3);
+  if (COND) out[Q] = g * (e.uCon[dir] * e.qTilde);
+  if (VISC) out[DP] = g * (e.uCon[dir] * e.deltaPTilde);
+}
+// induction rows of computeFluxes
+template <class S, class R>
+GRIM_D void fluxes_B(const ElemT<S, R>& e, int dir, R g, S* out3) {
+  out3[0] = g * (e.bCon[1] * e.uCon[dir] - e.bCon[dir] * e.uCon[1]);
+  out3[1] = g * (e.bCon[2] * e.uCon[dir] - e.bCon[dir] * e.uCon[2]);
+  out3[2] = g * (e.bCon[3] * e.uCon[dir] - e.bCon[dir] * e.uCon[3]);
+}
+
+// computeMinMaxCharSpeeds (riemannsolver.cpp:54-200), dir = 0,1,2
+template <int COND, int VISC, class R>
+GRIM_D void char_speeds(const ElemT<double, R>& e, const ZoneGeo<double>& G, int dir,
+                        const DevCfg& c, double& minSpeed, double& maxSpeed) {
+  const double Gam = c.Gam;
+  double cAlvenSqr = e.bSqr / (e.rho + Gam * e.u + e.bSqr);
+  double csSqr = e.soundSpeed * e.soundSpeed;
+  double cVisSqr = 0.;
+  if (VISC) cVisSqr = 4. / 3. / (e.rho + Gam * e.u) * e.rho * e.nu / e.tau;
+  double cConSqr = 0.;
+  if (COND) cConSqr = (Gam - 1.) * e.chi / e.tau;
+  cConSqr = 0.5 * (csSqr + cConSqr + sqrt(csSqr * csSqr + cConSqr * cConSqr));
+  csSqr = cConSqr + cVisSqr;
+  csSqr = csSqr + cAlvenSqr - csSqr * cAlvenSqr;
+  if (csSqr > 1.) csSqr = 1.;
+  const int s = dir + 1;
+  const double ASqr = G.gcon[s][s];
+  const double BSqr = G.gcon[0][0];
+  const double ADotU = e.uCon[s];
+  const double BDotU = e.uCon[0];
+  const double ADotB = G.gcon[s][0];
+  double A = (BDotU * BDotU) - (BSqr + BDotU * BDotU) * csSqr;
+  double B = 2. * (ADotU * BDotU - (ADotB + ADotU * BDotU) * csSqr);
+  double C = ADotU * ADotU - (ASqr + ADotU * ADotU) * csSqr;
+  double discr = sqrt(fmax(B * B - 4. * A * C, 1.e-16));
+  double mn = -(-B + discr) / 2. / A;
+  double mx = -(-B - discr) / 2. / A;
+  if (mn > -1.e-15) mn = -1.e-15;
+  if (mx < 1.e-15) mx = 1.e-15;
+  minSpeed = mn;
+  maxSpeed = mx;
+}
+
+// ---------------------------------------------------------------------------
+// Zone residual (residual.cpp:3-180) for the Newton kernels.
+//
+// Stage constants of one zone: Uold (consOld rows), divF and the explicit
+// sources (stored by the stencil kernel), and the reference elements of the
+// stage -- elemOld (half stage) or elemHalfStep (full stage) -- recomputed
+// here from their primitives since they are pointwise.
+// ---------------------------------------------------------------------------
+template <int NF>
+struct StageConst {
+  double Uold[NF];
+  double divF[NF];
+  double Sexp[NF];
+  double B[3];
+  // EMHD: elemOld uCov / temperature, reference-element quantities
+  double uCovOld[4], TOld;
+  double refRho, refNu, refChi, refTau, refT, refBCon[4], refBSqr, refBNorm, refUCon0;
+  double refQTilde, refDPTilde;
+  double sImpOldQ, sImpOldDP;  // 0.5*(...) partner of the implicit source
+  double normQ, normDP;        // EMHD row normalisation
+  double dtp;                  // dt' (dt/2 or dt)
+};
+
+template <int COND, int VISC, class S, class R>
+GRIM_D void zone_residual(const S* P, const StageConst<5 + COND + VISC>& K, const ZoneGeo<R>& G,
+                          const DevCfg& c, S* Rout) {
+  typedef typename Real<S>::type T;
+  constexpr int NF = 5 + COND + VISC;
+  constexpr int Q = 5, DP = 5 + COND;
+  ElemT<S, R> e;
+  S qT = COND ? P[Q] : S(T(0));
+  S dPT = VISC ? P[DP] : S(T(0));
+  elem_set<COND, VISC>(e, P[0], P[1], P[2], P[3], P[4], (R)K.B[0], (R)K.B[1], (R)K.B[2], qT, dPT, G, c);
+  S U[NF];
+  fluxes_fluid<COND, VISC>(e, 0, G.g, U, Q, DP);
+  const T dtp = (T)K.dtp;
+#pragma unroll
+  for (int v = 0; v < NF; v++) {
+    S r = (U[v] - (T)K.Uold[v]) / dtp + (T)K.divF[v];
+    if (c.metric != GRIM_MINKOWSKI || COND || VISC) r = r + (T)K.Sexp[v];
+    Rout[v] = r;
+  }
+  if (COND || VISC) {
+    // time-derivative sources (physics.cpp:219-317) with `this` = the
+    // stage's reference element, elemOld / elemNew = old / trial
+    S dtuCov[4];
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) dtuCov[mu] = (e.uCov[mu] - (T)K.uCovOld[mu]) / dtp;
+    S div = S(T(0.));
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) div = div + G.gcon[0][mu] * dtuCov[mu];
+    const T rr = (T)K.refRho, rnu = (T)K.refNu, rchi = (T)K.refChi, rtau = (T)K.refTau, rT = (T)K.refT;
+    const T rbn = (T)K.refBNorm, rbs = (T)K.refBSqr;
+    if (VISC) {
+      S d0 = -div * rr * rnu;
+#pragma unroll
+      for (int mu = 0; mu < 4; mu++) d0 += T(3.) * rr * rnu * (T)K.refBCon[0] * (T)K.refBCon[mu] / rbs * dtuCov[mu];
+      if (c.hoVisc == 1) d0 = d0 * (T)sqrt((double)(rtau / rr / rnu / rT));
+      S sdt = -G.g * (d0) / rtau;
+      if (c.hoVisc == 1) sdt = sdt - T(0.5) * G.g * div * (T)K.refDPTilde;
+      // implicit source of the trial with the reference tau (physics.cpp:343)
+      S simp = G.g * (P[DP]) / rtau;
+      S r = Rout[DP] + T(0.5) * ((T)K.sImpOldDP + simp) + sdt;
+      Rout[DP] = r * (T)K.normDP;
+    }
+    if (COND) {
+      S qq = -rr * rchi * (T)K.refBCon[0] / rbn * (e.temperature - (T)K.TOld) / dtp;
+#pragma unroll
+      for (int nu = 0; nu < 4; nu++) qq -= rr * rchi * rT * (T)K.refBCon[nu] / rbn * (T)K.refUCon0 * dtuCov[nu];
+      if (c.hoCond == 1) qq = qq * ((T)sqrt((double)(rtau / rr / rchi)) / rT);
+      S sdt = -G.g * (qq) / rtau;
+      if (c.hoCond == 1) sdt = sdt - T(0.5) * G.g * div * (T)K.refQTilde;
+      S simp = G.g * (P[Q]) / rtau;
+      S r = Rout[Q] + T(0.5) * ((T)K.sImpOldQ + simp) + sdt;
+      Rout[Q] = r * (T)K.normQ;
+    }
+  }
+}
+
+}  // namespace grim

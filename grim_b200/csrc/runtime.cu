@@ -1,0 +1,740 @@
+// runtime.cu -- host runtime behind the C ABI (include/grim_b200.h):
+// handle lifecycle, device memory, the timeStep schedule on one CUDA stream,
+// optional CUDA-graph replay of a whole step, statistics.
+//
+// The schedule of grim_time_step follows timeStepper::timeStep
+// (src/timestepper/timestep.cpp:3-334):
+//   dt update
+//   half stage: ghost fill(primOld) -> [dt speeds for the next step]
+//               -> [EMHD pre-pass] -> face fluxes per direction
+//               -> stage epilogue (CT, divergence, induction, sources,
+//                  consOld, Newton guess) -> Newton -> prim copied to primHalf
+//   full stage: the same on primHalf -> prim copied to primOld -> ghost fill
+//               -> time += dt -> [dt speeds of primOld for the next step]
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "launch.h"
+
+namespace grim {
+void launch_geometry(const DevCfg& c, const grim_config& cfg, int location, double* out, double* gamma,
+                     cudaStream_t s);
+}  // namespace grim
+
+using namespace grim;
+
+static thread_local std::string g_err;
+static void set_err(const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+
+#define CK(call)                                                                    \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess) {                                                        \
+      set_err("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return GRIM_ECUDA;                                                            \
+    }                                                                               \
+  } while (0)
+
+struct grim_handle {
+  grim_config cfg;
+  DevCfg dc;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  // state grids (dof x Z each)
+  double *primOld = nullptr, *prim = nullptr, *primHalf = nullptr;
+  // stage buffers
+  double *consOld = nullptr, *divF = nullptr, *Sexp = nullptr, *R = nullptr, *l2 = nullptr, *uT = nullptr;
+  double* flux[3] = {nullptr, nullptr, nullptr};
+  double* scratch = nullptr;  // test entry points: dof x Z inputs
+  double* scratch2 = nullptr;
+  // geometry: per location 36 x Z (MKS only), centre Christoffels 64 x Z
+  double* geo[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  double* gamma = nullptr;
+  DevState* st = nullptr;
+  DevState* hst = nullptr;  // pinned mirror
+  cudaEvent_t ev[8];
+  bool graphOn = false;
+  cudaGraphExec_t graph = nullptr;
+  grim_stats stats;
+  long long launchesPerStep = 0;
+  size_t bytesZ = 0;
+  int lastStage = GRIM_HALF_STEP;
+};
+
+static void free_all(grim_handle* h) {
+  double** bufs[] = {&h->primOld, &h->prim, &h->primHalf, &h->consOld, &h->divF, &h->Sexp, &h->R,
+                     &h->l2, &h->uT, &h->flux[0], &h->flux[1], &h->flux[2], &h->scratch, &h->scratch2,
+                     &h->geo[0], &h->geo[1], &h->geo[2], &h->geo[3], &h->geo[4], &h->gamma};
+  for (double** b : bufs)
+    if (*b) { cudaFree(*b); *b = nullptr; }
+  if (h->st) { cudaFree(h->st); h->st = nullptr; }
+  if (h->hst) { cudaFreeHost(h->hst); h->hst = nullptr; }
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+}
+
+static int make_devcfg(const grim_config& c, DevCfg& d) {
+  if (c.dim < 1 || c.dim > 3) { set_err("dim must be 1, 2 or 3"); return GRIM_EINVAL; }
+  if (c.numGhost != 3) { set_err("numGhost must be 3"); return GRIM_EINVAL; }
+  if (c.N1 < 4 || (c.dim >= 2 && c.N2 < 4) || (c.dim >= 3 && c.N3 < 4)) {
+    set_err("each active dimension needs at least 4 zones"); return GRIM_EINVAL;
+  }
+  if (c.reconstruction < 0 || c.reconstruction > 3) { set_err("bad reconstruction"); return GRIM_EINVAL; }
+  if (c.maxNonLinearIter < 1 || c.maxNonLinearIter > 15) { set_err("maxNonLinearIter must be 1..15"); return GRIM_EINVAL; }
+  if (c.maxLineSearchIters < 1 || c.maxLineSearchIters > 32) { set_err("maxLineSearchIters must be 1..32"); return GRIM_EINVAL; }
+  memset(&d, 0, sizeof(d));
+  d.dim = c.dim; d.ng = c.numGhost;
+  d.N1 = c.N1; d.N2 = c.dim >= 2 ? c.N2 : 1; d.N3 = c.dim >= 3 ? c.N3 : 1;
+  d.g1 = d.ng; d.g2 = c.dim >= 2 ? d.ng : 0; d.g3 = c.dim >= 3 ? d.ng : 0;
+  d.N1T = d.N1 + 2 * d.g1; d.N2T = d.N2 + 2 * d.g2; d.N3T = d.N3 + 2 * d.g3;
+  d.Z = (long long)d.N1T * d.N2T * d.N3T;
+  d.Zint = (long long)d.N1 * d.N2 * d.N3;
+  d.conduction = c.conduction ? 1 : 0; d.viscosity = c.viscosity ? 1 : 0;
+  d.nf = 5 + d.conduction + d.viscosity; d.dof = d.nf + 3;
+  d.Q = 5; d.DP = 5 + d.conduction; d.B1 = d.nf;
+  d.hoCond = c.highOrderTermsConduction; d.hoVisc = c.highOrderTermsViscosity;
+  d.metric = c.metric; d.reconstruction = c.reconstruction; d.riemann = c.riemannSolver;
+  d.closure = c.closure; d.problem = c.problem;
+  d.maxIter = c.maxNonLinearIter; d.maxLS = c.maxLineSearchIters;
+  d.bc[0] = c.boundaryLeft; d.bc[1] = c.boundaryRight; d.bc[2] = c.boundaryBottom; d.bc[3] = c.boundaryTop;
+  d.bc[4] = c.boundaryBack; d.bc[5] = c.boundaryFront;
+  // coordinatesGrid (grid.cpp:142-146): dX from the constructor's N
+  d.dX[0] = (c.X1End - c.X1Start) / c.N1;
+  d.dX[1] = (c.X2End - c.X2Start) / c.N2;
+  d.dX[2] = (c.X3End - c.X3Start) / c.N3;
+  for (int i = 0; i < 3; i++) d.invdX[i] = 1. / d.dX[i];
+  d.X1Start = c.X1Start; d.X2Start = c.X2Start; d.X3Start = c.X3Start; d.X2End = c.X2End;
+  d.Gam = c.adiabaticIndex;
+  d.rhoFloor = c.rhoFloorInFluidElement; d.uFloor = c.uFloorInFluidElement;
+  d.bSqrFloor = c.bSqrFloorInFluidElement; d.TFloor = c.temperatureFloorInFluidElement;
+  d.CondAlpha = c.ConductionAlpha; d.ViscAlpha = c.ViscosityAlpha;
+  d.CondClosure = c.ConductionClosureFactor; d.ViscClosure = c.ViscosityClosureFactor;
+  d.theta = c.slopeLimTheta;
+  d.atol = c.nonlinearsolve_atol; d.rtol = c.nonlinearsolve_rtol;
+  d.jacEps = c.JacobianAssembleEpsilon; d.lsFloor = c.linesearchfloor;
+  d.tau0 = c.closureTau0; d.tau1 = c.closureTau1;
+  return GRIM_OK;
+}
+
+static bool use_exact(const grim_handle* h) { return h->cfg.newtonMode == GRIM_NEWTON_PARITY_FD64; }
+
+static StageBufs stage_bufs(grim_handle* h, int stage) {
+  StageBufs b;
+  memset(&b, 0, sizeof(b));
+  b.ps = (stage == GRIM_HALF_STEP) ? h->primOld : h->primHalf;
+  b.pold = h->primOld;
+  b.prim = h->prim;
+  const bool mink = h->cfg.metric == GRIM_MINKOWSKI;
+  b.geoC = mink ? nullptr : h->geo[GRIM_CENTER];
+  b.gamma = mink ? nullptr : h->gamma;
+  b.geoF[0] = mink ? nullptr : h->geo[GRIM_LEFT];
+  b.geoF[1] = mink ? nullptr : h->geo[GRIM_BOTTOM];
+  b.geoF[2] = b.geoC;
+  for (int d = 0; d < 3; d++) b.flux[d] = h->flux[d];
+  b.uT = h->uT;
+  b.consOld = h->consOld;
+  b.divF = h->divF;
+  b.Sexp = h->Sexp;
+  b.R = h->R;
+  b.l2 = h->l2;
+  b.st = h->st;
+  return b;
+}
+
+// ---------------------------------------------------------------------------
+// the step schedule (all asynchronous on h->stream)
+// ---------------------------------------------------------------------------
+#define KNS_CALL(h, fn, ...)                                           \
+  do {                                                                 \
+    if (use_exact(h)) grim::exact::fn(__VA_ARGS__);                    \
+    else grim::fast::fn(__VA_ARGS__);                                  \
+  } while (0)
+
+static long long g_launch_counter = 0;
+
+static void enqueue_stencil(grim_handle* h, int stage) {
+  const DevCfg& c = h->dc;
+  cudaStream_t s = h->stream;
+  StageBufs b = stage_bufs(h, stage);
+  if (c.conduction || c.viscosity) { KNS_CALL(h, emhd_prepass, c, b.ps, b.geoC, h->uT, s); g_launch_counter++; }
+  for (int d = 0; d < c.dim; d++) {
+    KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], s);
+    g_launch_counter++;
+  }
+  KNS_CALL(h, stage_epilogue, c, stage, b, s);
+  g_launch_counter++;
+}
+
+static void enqueue_newton(grim_handle* h, int stage) {
+  const DevCfg& c = h->dc;
+  cudaStream_t s = h->stream;
+  StageBufs b = stage_bufs(h, stage);
+  if (h->cfg.newtonMode == GRIM_NEWTON_PARITY_FD64) {
+    grim::exact::newton_fd_init(c, stage, b, s);
+    g_launch_counter++;
+    for (int it = 0; it < c.maxIter; it++) {
+      grim::exact::newton_fd_iter(c, stage, it, b, s);
+      g_launch_counter++;
+    }
+  } else {
+    grim::fast::newton_fast(c, stage, b, h->cfg.newtonMode, nullptr, c.Zint, s);
+    g_launch_counter++;
+  }
+}
+
+static void enqueue_dt_speeds(grim_handle* h, const double* p, int mode) {
+  const DevCfg& c = h->dc;
+  cudaMemsetAsync(&h->st->maxInvDt, 0, sizeof(double), h->stream);
+  const bool mink = h->cfg.metric == GRIM_MINKOWSKI;
+  KNS_CALL(h, dt_speeds, c, p, mink ? nullptr : h->geo[GRIM_CENTER], mode, h->st, h->stream);
+  g_launch_counter++;
+}
+
+static void enqueue_step(grim_handle* h, bool timed) {
+  const DevCfg& c = h->dc;
+  cudaStream_t s = h->stream;
+  const size_t bytes = (size_t)c.dof * c.Z * sizeof(double);
+  if (timed) cudaEventRecord(h->ev[0], s);
+  // computeDt (timestep.cpp:8): dt from the last elemOld state
+  KNS_CALL(h, dt_update, h->st, h->cfg.CourantFactor, h->cfg.maxDtIncrement, s);
+  g_launch_counter++;
+  cudaMemsetAsync(h->st->count, 0, sizeof(h->st->count), s);
+  cudaMemsetAsync(h->st->itersDone, 0, sizeof(h->st->itersDone), s);
+  cudaMemsetAsync(h->st->finalUnconv, 0, sizeof(h->st->finalUnconv), s);
+  cudaMemsetAsync(&h->st->nonFinite, 0, sizeof(unsigned long long), s);
+  // ---- half stage
+  KNS_CALL(h, ghost_fill, c, h->primOld, c.dof, s);
+  g_launch_counter++;
+  if (!h->cfg.elemOldFromFullStep) enqueue_dt_speeds(h, h->primOld, 0);
+  if (timed) cudaEventRecord(h->ev[1], s);
+  enqueue_stencil(h, GRIM_HALF_STEP);
+  if (timed) cudaEventRecord(h->ev[2], s);
+  enqueue_newton(h, GRIM_HALF_STEP);
+  if (timed) cudaEventRecord(h->ev[3], s);
+  cudaMemcpyAsync(h->primHalf, h->prim, bytes, cudaMemcpyDeviceToDevice, s);
+  // ---- full stage
+  KNS_CALL(h, ghost_fill, c, h->primHalf, c.dof, s);
+  g_launch_counter++;
+  if (timed) cudaEventRecord(h->ev[4], s);
+  enqueue_stencil(h, GRIM_FULL_STEP);
+  if (timed) cudaEventRecord(h->ev[5], s);
+  enqueue_newton(h, GRIM_FULL_STEP);
+  if (timed) cudaEventRecord(h->ev[6], s);
+  cudaMemcpyAsync(h->primOld, h->prim, bytes, cudaMemcpyDeviceToDevice, s);
+  KNS_CALL(h, ghost_fill, c, h->primOld, c.dof, s);
+  g_launch_counter++;
+  grim::exact::advance_time(h->st, s);
+  g_launch_counter++;
+  // fullStepDiagnostics re-setting elemOld (linear_modes/problem.cpp:287)
+  if (h->cfg.elemOldFromFullStep) enqueue_dt_speeds(h, h->primOld, 1);
+  KNS_CALL(h, count_nonfinite, c, h->primOld, h->st, s);
+  g_launch_counter++;
+  if (timed) cudaEventRecord(h->ev[7], s);
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* grim_version(void) { return "grim_b200 0.1 (sm_100a)"; }
+const char* grim_last_error(void) { return g_err.c_str(); }
+
+int grim_create(const grim_config* cfg, int device, grim_handle** out) {
+  if (!cfg || !out) { set_err("null argument"); return GRIM_EINVAL; }
+  *out = nullptr;
+  grim_handle* h = new grim_handle();
+  h->cfg = *cfg;
+  int rc = make_devcfg(*cfg, h->dc);
+  if (rc) { delete h; return rc; }
+  h->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) { set_err("cudaSetDevice(%d): %s", device, cudaGetErrorString(e)); delete h; return GRIM_ECUDA; }
+  const DevCfg& c = h->dc;
+  const size_t Zb = (size_t)c.Z * sizeof(double);
+  h->bytesZ = Zb;
+  auto alloc = [&](double** p, size_t words) -> bool {
+    if (cudaMalloc(p, words * Zb) != cudaSuccess) return false;
+    return cudaMemset(*p, 0, words * Zb) == cudaSuccess;
+  };
+  bool ok = alloc(&h->primOld, c.dof) && alloc(&h->prim, c.dof) && alloc(&h->primHalf, c.dof) &&
+            alloc(&h->consOld, c.dof) && alloc(&h->divF, c.dof) && alloc(&h->Sexp, c.nf) && alloc(&h->R, c.nf) &&
+            alloc(&h->l2, 2) && alloc(&h->scratch, c.dof) && alloc(&h->scratch2, (size_t)c.dof * 3);
+  for (int d = 0; ok && d < c.dim; d++) ok = alloc(&h->flux[d], c.dof);
+  if (ok && (c.conduction || c.viscosity)) ok = alloc(&h->uT, 5);
+  if (ok && cfg->metric != GRIM_MINKOWSKI) {
+    for (int l = 0; ok && l < 5; l++) ok = alloc(&h->geo[l], 36);
+    if (ok) ok = alloc(&h->gamma, 64);
+  }
+  if (ok) ok = cudaMalloc(&h->st, sizeof(DevState)) == cudaSuccess;
+  if (ok) ok = cudaMallocHost(&h->hst, sizeof(DevState)) == cudaSuccess;
+  if (!ok) {
+    set_err("device allocation failed (%zu MB per grid variable)", Zb >> 20);
+    free_all(h); delete h; return GRIM_ENOMEM;
+  }
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_err("stream creation failed"); free_all(h); delete h; return GRIM_ECUDA;
+  }
+  for (int i = 0; i < 8; i++) cudaEventCreate(&h->ev[i]);
+  // geometry (geometry.cpp ctor at LEFT/RIGHT/BOTTOM/TOP/CENTER, timestepper.cpp:236-283)
+  if (cfg->metric != GRIM_MINKOWSKI) {
+    for (int l = 0; l < 5; l++)
+      launch_geometry(c, *cfg, l, h->geo[l], l == GRIM_CENTER ? h->gamma : nullptr, h->stream);
+  }
+  // device scalars; the elements are first set on all-zero grids
+  // (timestepper.cpp:287-295), which is the state the first computeDt sees
+  memset(h->hst, 0, sizeof(DevState));
+  h->hst->dt = cfg->dt;
+  h->hst->time = cfg->time;
+  h->hst->first = 1;
+  cudaMemcpyAsync(h->st, h->hst, sizeof(DevState), cudaMemcpyHostToDevice, h->stream);
+  enqueue_dt_speeds(h, h->primOld, 2);
+  e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    set_err("initialisation failed: %s", cudaGetErrorString(e));
+    free_all(h); delete h; return GRIM_ECUDA;
+  }
+  memset(&h->stats, 0, sizeof(h->stats));
+  *out = h;
+  return GRIM_OK;
+}
+
+int grim_destroy(grim_handle* h) {
+  if (!h) return GRIM_OK;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_all(h);
+  for (int i = 0; i < 8; i++) cudaEventDestroy(h->ev[i]);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return GRIM_OK;
+}
+
+int grim_dims(const grim_handle* h, int* a, int* b, int* c, int* dof, int* nf) {
+  if (!h) return GRIM_EINVAL;
+  if (a) *a = h->dc.N1T;
+  if (b) *b = h->dc.N2T;
+  if (c) *c = h->dc.N3T;
+  if (dof) *dof = h->dc.dof;
+  if (nf) *nf = h->dc.nf;
+  return GRIM_OK;
+}
+
+static double* pick(grim_handle* h, int which) {
+  if (which == GRIM_PRIM_OLD) return h->primOld;
+  if (which == GRIM_PRIM) return h->prim;
+  if (which == GRIM_PRIM_HALF) return h->primHalf;
+  return nullptr;
+}
+
+int grim_set_prims(grim_handle* h, int which, const double* src, int memKind) {
+  if (!h || !src) { set_err("null argument"); return GRIM_EINVAL; }
+  double* dst = pick(h, which);
+  if (!dst) { set_err("bad state selector %d", which); return GRIM_EINVAL; }
+  CK(cudaSetDevice(h->device));
+  const size_t bytes = (size_t)h->dc.dof * h->bytesZ;
+  CK(cudaMemcpyAsync(dst, src, bytes, memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                     h->stream));
+  if (memKind != GRIM_DEVICE) CK(cudaStreamSynchronize(h->stream));
+  return GRIM_OK;
+}
+
+int grim_get_prims(grim_handle* h, int which, double* dst, int memKind) {
+  if (!h || !dst) { set_err("null argument"); return GRIM_EINVAL; }
+  double* src = pick(h, which);
+  if (!src) { set_err("bad state selector %d", which); return GRIM_EINVAL; }
+  CK(cudaSetDevice(h->device));
+  const size_t bytes = (size_t)h->dc.dof * h->bytesZ;
+  CK(cudaMemcpyAsync(dst, src, bytes, memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     h->stream));
+  if (memKind != GRIM_DEVICE) CK(cudaStreamSynchronize(h->stream));
+  return GRIM_OK;
+}
+
+static int run_steps(grim_handle* h, int nsteps) {
+  CK(cudaSetDevice(h->device));
+  for (int n = 0; n < nsteps; n++) {
+    const bool last = (n == nsteps - 1);
+    if (h->graphOn) {
+      if (!h->graph) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        long long before = g_launch_counter;
+        enqueue_step(h, false);
+        h->launchesPerStep = g_launch_counter - before;
+        CK(cudaStreamEndCapture(h->stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { set_err("graph instantiate: %s", cudaGetErrorString(e)); return GRIM_ECUDA; }
+      }
+      if (last) cudaEventRecord(h->ev[0], h->stream);
+      CK(cudaGraphLaunch(h->graph, h->stream));
+      if (last) cudaEventRecord(h->ev[7], h->stream);
+    } else {
+      long long before = g_launch_counter;
+      enqueue_step(h, last);
+      h->launchesPerStep = g_launch_counter - before;
+    }
+  }
+  CK(cudaGetLastError());
+  return GRIM_OK;
+}
+
+int grim_time_step(grim_handle* h, int* numReads, int* numWrites) {
+  if (!h) return GRIM_EINVAL;
+  int rc = run_steps(h, 1);
+  // algorithmic words per zone of one step: both stages read prims (dof)
+  // and write the new prims (dof) plus the stage constants
+  if (numReads) *numReads = 2 * h->dc.dof;
+  if (numWrites) *numWrites = 2 * h->dc.dof;
+  return rc;
+}
+
+int grim_time_steps(grim_handle* h, int nsteps) {
+  if (!h || nsteps < 0) return GRIM_EINVAL;
+  return run_steps(h, nsteps);
+}
+
+int grim_get_time(grim_handle* h, double* t, double* dt) {
+  if (!h) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(h->hst, h->st, sizeof(DevState), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (t) *t = h->hst->time;
+  if (dt) *dt = h->hst->dt;
+  return GRIM_OK;
+}
+
+int grim_set_time(grim_handle* h, double t, double dt) {
+  if (!h) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(h->hst, h->st, sizeof(DevState), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->hst->time = t;
+  h->hst->dt = dt;
+  CK(cudaMemcpyAsync(h->st, h->hst, sizeof(DevState), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return GRIM_OK;
+}
+
+int grim_compute_dt(grim_handle* h) {
+  if (!h) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  KNS_CALL(h, dt_update, h->st, h->cfg.CourantFactor, h->cfg.maxDtIncrement, h->stream);
+  CK(cudaGetLastError());
+  return GRIM_OK;
+}
+
+int grim_apply_boundaries(grim_handle* h, int which) {
+  if (!h) return GRIM_EINVAL;
+  double* p = pick(h, which);
+  if (!p) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  KNS_CALL(h, ghost_fill, h->dc, p, h->dc.dof, h->stream);
+  CK(cudaGetLastError());
+  return GRIM_OK;
+}
+
+// copy a caller array (host or device) of nv x Z words into a device buffer
+static int stage_in(grim_handle* h, double* dst, const double* src, int nv, int memKind) {
+  CK(cudaMemcpyAsync(dst, src, (size_t)nv * h->bytesZ,
+                     memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream));
+  return GRIM_OK;
+}
+static int stage_out(grim_handle* h, double* dst, const double* src, size_t bytes, int memKind) {
+  CK(cudaMemcpyAsync(dst, src, bytes, memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return GRIM_OK;
+}
+
+int grim_compute_div_fluxes(grim_handle* h, const double* prim, double* divF, double* fluxes, double* emf,
+                            int memKind) {
+  if (!h || !prim) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  const DevCfg& c = h->dc;
+  int rc = stage_in(h, h->scratch, prim, c.dof, memKind);
+  if (rc) return rc;
+  // a stencil pass on the scratch prims as a half stage with dt = 0 keeps
+  // the stored state untouched except the stage buffers
+  StageBufs b = stage_bufs(h, GRIM_HALF_STEP);
+  b.ps = h->scratch;
+  b.pold = h->scratch;
+  double* tmpPrim = h->scratch2;  // receives the guess
+  b.prim = tmpPrim;
+  if (c.conduction || c.viscosity) KNS_CALL(h, emhd_prepass, c, b.ps, b.geoC, h->uT, h->stream);
+  for (int d = 0; d < c.dim; d++) KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], h->stream);
+  // divergence of all dof rows: epilogue writes nf rows into divF and the
+  // induction into the guess; the B rows of the divergence are recovered
+  // from the guess: B_new = (consOld_B - 0.5 dt divF_B)/g with dt kept
+  KNS_CALL(h, stage_epilogue, c, GRIM_HALF_STEP, b, h->stream);
+  CK(cudaGetLastError());
+  if (divF) {
+    rc = stage_out(h, divF, h->divF, (size_t)c.dof * h->bytesZ, memKind);
+    if (rc) return rc;
+  }
+  if (fluxes) {
+    for (int d = 0; d < 3; d++) {
+      double* dst = fluxes + (size_t)d * c.dof * c.Z;
+      if (d < c.dim) {
+        rc = stage_out(h, dst, h->flux[d], (size_t)c.dof * h->bytesZ, memKind);
+        if (rc) return rc;
+      }
+    }
+  }
+  (void)emf;
+  CK(cudaStreamSynchronize(h->stream));
+  return GRIM_OK;
+}
+
+int grim_reconstruct(grim_handle* h, const double* prim, int dir, double* pl, double* pr, int memKind) {
+  if (!h || !prim || !pl || !pr || dir < 0 || dir >= h->dc.dim) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  const DevCfg& c = h->dc;
+  int rc = stage_in(h, h->scratch, prim, c.dof, memKind);
+  if (rc) return rc;
+  double* dl = h->scratch2;
+  double* dr = h->scratch2 + (size_t)c.dof * c.Z;
+  KNS_CALL(h, reconstruct, c, dir, h->scratch, dl, dr, h->stream);
+  CK(cudaGetLastError());
+  rc = stage_out(h, pl, dl, (size_t)c.dof * h->bytesZ, memKind);
+  if (rc) return rc;
+  return stage_out(h, pr, dr, (size_t)c.dof * h->bytesZ, memKind);
+}
+
+int grim_compute_divb(grim_handle* h, const double* prim, double* divB, int memKind) {
+  (void)h; (void)prim; (void)divB; (void)memKind;
+  set_err("grim_compute_divb: use the Python harness diagnostic");
+  return GRIM_ENOTSUP;
+}
+
+int grim_conserved(grim_handle* h, const double* prim, double* cons, int memKind) {
+  if (!h || !prim || !cons) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  const DevCfg& c = h->dc;
+  int rc = stage_in(h, h->scratch, prim, c.dof, memKind);
+  if (rc) return rc;
+  const bool mink = h->cfg.metric == GRIM_MINKOWSKI;
+  KNS_CALL(h, conserved, c, h->scratch, mink ? nullptr : h->geo[GRIM_CENTER], h->scratch2, 0, nullptr, nullptr,
+           h->stream);
+  CK(cudaGetLastError());
+  return stage_out(h, cons, h->scratch2, (size_t)c.dof * h->bytesZ, memKind);
+}
+
+int grim_char_speeds(grim_handle* h, const double* prim, int dir, double* mn, double* mx, int memKind) {
+  if (!h || !prim || !mn || !mx || dir < 0 || dir > 2) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  const DevCfg& c = h->dc;
+  int rc = stage_in(h, h->scratch, prim, c.dof, memKind);
+  if (rc) return rc;
+  const bool mink = h->cfg.metric == GRIM_MINKOWSKI;
+  double* a = h->scratch2;
+  double* b = h->scratch2 + c.Z;
+  KNS_CALL(h, conserved, c, h->scratch, mink ? nullptr : h->geo[GRIM_CENTER], nullptr, dir, a, b, h->stream);
+  CK(cudaGetLastError());
+  rc = stage_out(h, mn, a, h->bytesZ, memKind);
+  if (rc) return rc;
+  return stage_out(h, mx, b, h->bytesZ, memKind);
+}
+
+int grim_stage_setup(grim_handle* h, int stage) {
+  if (!h || (stage != GRIM_HALF_STEP && stage != GRIM_FULL_STEP)) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  const DevCfg& c = h->dc;
+  double* ps = (stage == GRIM_HALF_STEP) ? h->primOld : h->primHalf;
+  KNS_CALL(h, ghost_fill, c, ps, c.dof, h->stream);
+  enqueue_stencil(h, stage);
+  h->lastStage = stage;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));
+  return GRIM_OK;
+}
+
+int grim_residual(grim_handle* h, const double* pg, double* res, int memKind) {
+  if (!h || !pg || !res) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  const DevCfg& c = h->dc;
+  int rc = stage_in(h, h->scratch, pg, c.dof, memKind);
+  if (rc) return rc;
+  StageBufs b = stage_bufs(h, h->lastStage);
+  KNS_CALL(h, residual, c, h->lastStage, b, h->scratch, h->scratch2, h->stream);
+  CK(cudaGetLastError());
+  return stage_out(h, res, h->scratch2, (size_t)c.nf * h->bytesZ, memKind);
+}
+
+static int jac_common(grim_handle* h, const double* pg, double* jac, int memKind, int tangent) {
+  if (!h || !pg || !jac) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  const DevCfg& c = h->dc;
+  int rc = stage_in(h, h->scratch, pg, c.dof, memKind);
+  if (rc) return rc;
+  double* dj = nullptr;
+  const size_t bytes = (size_t)c.Z * c.nf * c.nf * sizeof(double);
+  CK(cudaMallocAsync((void**)&dj, bytes, h->stream));
+  StageBufs b = stage_bufs(h, h->lastStage);
+  if (tangent)
+    grim::fast::jacobian(c, h->lastStage, b, h->scratch, dj, 1, h->stream);
+  else
+    grim::exact::jacobian(c, h->lastStage, b, h->scratch, dj, 0, h->stream);
+  CK(cudaGetLastError());
+  rc = stage_out(h, jac, dj, bytes, memKind);
+  cudaFreeAsync(dj, h->stream);
+  cudaStreamSynchronize(h->stream);
+  return rc;
+}
+int grim_jacobian_fd(grim_handle* h, const double* pg, double* jac, int memKind) {
+  return jac_common(h, pg, jac, memKind, 0);
+}
+int grim_jacobian_tangent(grim_handle* h, const double* pg, double* jac, int memKind) {
+  return jac_common(h, pg, jac, memKind, 1);
+}
+
+int grim_newton_solve(grim_handle* h, int* iters) {
+  if (!h) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  cudaMemsetAsync(h->st->count, 0, sizeof(h->st->count), h->stream);
+  cudaMemsetAsync(h->st->itersDone, 0, sizeof(h->st->itersDone), h->stream);
+  cudaMemsetAsync(h->st->finalUnconv, 0, sizeof(h->st->finalUnconv), h->stream);
+  enqueue_newton(h, h->lastStage);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->hst, h->st, sizeof(DevState), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (iters) *iters = (int)h->hst->itersDone[h->lastStage];
+  return GRIM_OK;
+}
+
+int grim_batch_solve(int n, int batch, const double* A, const double* b, double* x, int memKind) {
+  if (n < 1 || n > 8 || batch < 0 || !A || !b || !x) return GRIM_EINVAL;
+  if (batch == 0) return GRIM_OK;
+  cudaStream_t s = 0;
+  const size_t bA = (size_t)batch * n * n * sizeof(double), bb = (size_t)batch * n * sizeof(double);
+  const double *dA = A, *db = b;
+  double* dx = x;
+  double *tA = nullptr, *tb = nullptr, *tx = nullptr;
+  if (memKind != GRIM_DEVICE) {
+    CK(cudaMalloc(&tA, bA));
+    CK(cudaMalloc(&tb, bb));
+    CK(cudaMalloc(&tx, bb));
+    CK(cudaMemcpy(tA, A, bA, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(tb, b, bb, cudaMemcpyHostToDevice));
+    dA = tA; db = tb; dx = tx;
+  }
+  grim::exact::batch_solve(n, batch, dA, db, dx, s);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && memKind != GRIM_DEVICE) e = cudaMemcpy(x, tx, bb, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (tA) cudaFree(tA);
+  if (tb) cudaFree(tb);
+  if (tx) cudaFree(tx);
+  if (e != cudaSuccess) { set_err("batch solve: %s", cudaGetErrorString(e)); return GRIM_ECUDA; }
+  return GRIM_OK;
+}
+
+int grim_get_geometry(grim_handle* h, int location, double* out, double* gamma, double* xc, int memKind) {
+  if (!h || location < 0 || location > 4) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  const DevCfg& c = h->dc;
+  if (h->cfg.metric == GRIM_MINKOWSKI) { set_err("Minkowski geometry is compile-time"); return GRIM_ENOTSUP; }
+  if (out) {
+    int rc = stage_out(h, out, h->geo[location], 34 * h->bytesZ, memKind);
+    if (rc) return rc;
+  }
+  if (xc) {
+    int rc = stage_out(h, xc, h->geo[location] + 34 * c.Z, 2 * h->bytesZ, memKind);
+    if (rc) return rc;
+  }
+  if (gamma && location == GRIM_CENTER) return stage_out(h, gamma, h->gamma, 64 * h->bytesZ, memKind);
+  return GRIM_OK;
+}
+
+int grim_set_geometry(grim_handle* h, int location, const double* in, const double* gamma, const double* xc,
+                      int memKind) {
+  if (!h || location < 0 || location > 4) return GRIM_EINVAL;
+  if (h->cfg.metric == GRIM_MINKOWSKI) { set_err("Minkowski geometry is compile-time"); return GRIM_ENOTSUP; }
+  CK(cudaSetDevice(h->device));
+  const cudaMemcpyKind k = memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (in) CK(cudaMemcpyAsync(h->geo[location], in, 34 * h->bytesZ, k, h->stream));
+  if (xc) CK(cudaMemcpyAsync(h->geo[location] + 34 * h->dc.Z, xc, 2 * h->bytesZ, k, h->stream));
+  if (gamma && location == GRIM_CENTER) CK(cudaMemcpyAsync(h->gamma, gamma, 64 * h->bytesZ, k, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  // the first computeDt depends on the geometry: redo it
+  enqueue_dt_speeds(h, h->primOld, 2);
+  CK(cudaStreamSynchronize(h->stream));
+  return GRIM_OK;
+}
+
+int grim_set_newton_mode(grim_handle* h, int mode, int perZone, double rtol) {
+  if (!h || mode < 0 || mode > 2) return GRIM_EINVAL;
+  h->cfg.newtonMode = mode;
+  h->cfg.perZoneConvergence = perZone;
+  h->cfg.nonlinearsolve_rtol = rtol;
+  h->dc.rtol = rtol;
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  return GRIM_OK;
+}
+
+int grim_get_stats(grim_handle* h, grim_stats* out) {
+  if (!h || !out) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(h->hst, h->st, sizeof(DevState), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  grim_stats s;
+  memset(&s, 0, sizeof(s));
+  for (int st = 0; st < 2; st++) {
+    s.newtonIters[st] = (int)h->hst->itersDone[st];
+    if (h->cfg.newtonMode == GRIM_NEWTON_PARITY_FD64) {
+      // zones unconverged at the last counted iteration
+      unsigned long long u = 0;
+      for (int it = 0; it <= h->dc.maxIter && it < 16; it++)
+        if (h->hst->count[st][it]) u = h->hst->count[st][it];
+      s.unconverged[st] = (long long)u;
+    } else {
+      s.unconverged[st] = (long long)h->hst->finalUnconv[st];
+    }
+  }
+  s.nonFinite = (long long)h->hst->nonFinite;
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, h->ev[0], h->ev[7]) == cudaSuccess) s.msStep = ms;
+  if (!h->graphOn) {
+    float a = 0, b = 0, c2 = 0, d = 0;
+    if (cudaEventElapsedTime(&a, h->ev[1], h->ev[2]) == cudaSuccess &&
+        cudaEventElapsedTime(&b, h->ev[4], h->ev[5]) == cudaSuccess)
+      s.msStencil = a + b;
+    if (cudaEventElapsedTime(&c2, h->ev[2], h->ev[3]) == cudaSuccess &&
+        cudaEventElapsedTime(&d, h->ev[5], h->ev[6]) == cudaSuccess)
+      s.msNewton = c2 + d;
+    s.msOther = s.msStep - s.msStencil - s.msNewton;
+  }
+  s.kernelLaunches = h->launchesPerStep;
+  *out = s;
+  return GRIM_OK;
+}
+
+int grim_enable_graph(grim_handle* h, int enable) {
+  if (!h) return GRIM_EINVAL;
+  h->graphOn = enable != 0;
+  if (!h->graphOn && h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  return GRIM_OK;
+}
+
+int grim_synchronize(grim_handle* h) {
+  if (!h) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  return GRIM_OK;
+}
+
+void* grim_stream(grim_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,37 @@
+// stage.cuh -- device state and stage buffers shared by the kernels and the
+// host runtime.
+#pragma once
+#include "common.cuh"
+
+namespace grim {
+
+// device-resident scalars of the stepper (dt, time and the Newton counters
+// live here so a captured step needs no host round trip)
+struct DevState {
+  double dt, time, maxInvDt, dtOld;
+  int first;
+  int pad;
+  unsigned long long count[2][16];   // unconverged zones per stage / iteration
+  unsigned long long itersDone[2];
+  unsigned long long nonFinite;
+  unsigned long long finalUnconv[2];
+};
+
+struct StageBufs {
+  const double* ps;       // prims the stage's fluxes are computed from
+  const double* pold;     // primOld
+  double* prim;           // Newton guess / result
+  const double* geoC;     // centre geometry (36 x Z) or null (Minkowski)
+  const double* gamma;    // centre Christoffels (64 x Z) or null
+  const double* geoF[3];  // face geometry per direction or null
+  double* flux[3];        // face fluxes per direction, dof x Z
+  double* uT;             // EMHD pre-pass: u_mu (4) + T (1), 5 x Z
+  double* consOld;        // dof x Z (fluid rows then B rows)
+  double* divF;           // dof x Z (fluid rows, then B rows)
+  double* Sexp;           // nf x Z
+  double* R;              // nf x Z  (Newton scratch)
+  double* l2;             // 2 x Z   (l2, l2first)
+  DevState* st;
+};
+
+}  // namespace grim

@@ -1,0 +1,253 @@
+"""Python mirror of the reference's timeStepperPy / gridPy interface
+(src/timestepper/timeStepperPy.pyx:20-212, src/grid/gridPy.pyx:185-221),
+implemented over the C ABI of libgrim_b200.so.
+
+    ts = timeStepper(cfg)              # or timeStepper.fromArgs(N1, N2, ...)
+    ts.primOld.setVars(P)              # numpy [var, k, j, i], ghosts included
+    ts.timeStep()                      # -> (numReads, numWrites)
+    P = ts.primOld.getVars()
+
+Grids live on the GPU; getVars/setVars copy through host memory exactly as
+gridPy does (device -> host in getVars).  Device pointers (e.g. from torch)
+can be passed with ``setVarsDevice`` / ``getVarsDevice``.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from . import config as C
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Grid:
+    """One state grid of the stepper (gridPy)."""
+
+    def __init__(self, ts, which):
+        self._ts = ts
+        self._which = which
+
+    @property
+    def shape(self):
+        return [self._ts.dof, self._ts.N3Total, self._ts.N2Total, self._ts.N1Total]
+
+    numVars = property(lambda self: self._ts.dof)
+    N1Total = property(lambda self: self._ts.N1Total)
+    N2Total = property(lambda self: self._ts.N2Total)
+    N3Total = property(lambda self: self._ts.N3Total)
+    numGhost = property(lambda self: self._ts.cfg["numGhost"])
+    dim = property(lambda self: self._ts.cfg["dim"])
+
+    def getVars(self):
+        out = np.empty(self.shape, dtype=np.float64)
+        _lib.check(_lib.lib().grim_get_prims(self._ts._h, self._which, _ptr(out), _lib.HOST), "getVars")
+        return out
+
+    def setVars(self, vars_):
+        a = np.ascontiguousarray(vars_, dtype=np.float64)
+        if list(a.shape) != self.shape:
+            raise ValueError("setVars: shape %s, expected %s" % (a.shape, self.shape))
+        _lib.check(_lib.lib().grim_set_prims(self._ts._h, self._which, _ptr(a), _lib.HOST), "setVars")
+
+    def setVarsDevice(self, dev_ptr):
+        _lib.check(_lib.lib().grim_set_prims(self._ts._h, self._which, ctypes.c_void_p(int(dev_ptr)),
+                                             _lib.DEVICE), "setVarsDevice")
+
+    def getVarsDevice(self, dev_ptr):
+        _lib.check(_lib.lib().grim_get_prims(self._ts._h, self._which, ctypes.c_void_p(int(dev_ptr)),
+                                             _lib.DEVICE), "getVarsDevice")
+
+
+class timeStepper:
+    """The reference's timeStepper (timestepper.hpp:19-132) on one B200."""
+
+    HALF_STEP, FULL_STEP = C.HALF_STEP, C.FULL_STEP
+
+    def __init__(self, cfg, device=0):
+        self.cfg = dict(cfg)
+        s = C.to_struct(self.cfg)
+        self._h = ctypes.c_void_p()
+        L = _lib.lib()
+        _lib.check(L.grim_create(ctypes.byref(s), int(device), ctypes.byref(self._h)), "grim_create")
+        a, b, c, dof, nf = (ctypes.c_int() for _ in range(5))
+        L.grim_dims(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(dof),
+                    ctypes.byref(nf))
+        self.N1Total, self.N2Total, self.N3Total = a.value, b.value, c.value
+        self.dof, self.numFluidVars = dof.value, nf.value
+        self.zshape = (self.N3Total, self.N2Total, self.N1Total)
+        self.prim = Grid(self, _lib.PRIM)
+        self.primOld = Grid(self, _lib.PRIM_OLD)
+        self.primHalfStep = Grid(self, _lib.PRIM_HALF)
+
+    @classmethod
+    def fromArgs(cls, N1, N2, N3, dim, numVars, numGhost, time, dt, boundaryLeft, boundaryRight,
+                 boundaryTop, boundaryBottom, boundaryFront, boundaryBack, metric, blackHoleSpin, hSlope,
+                 X1Start, X1End, X2Start, X2End, X3Start, X3End, **params):
+        """The reference constructor's argument list (timeStepperPy.pyx:22-50);
+        the remaining params:: values come as keywords."""
+        cfg = C.make_config(N1=N1, N2=N2, N3=N3, dim=dim, numGhost=numGhost, time=time, dt=dt,
+                            boundaryLeft=boundaryLeft, boundaryRight=boundaryRight,
+                            boundaryTop=boundaryTop, boundaryBottom=boundaryBottom,
+                            boundaryFront=boundaryFront, boundaryBack=boundaryBack, metric=metric,
+                            blackHoleSpin=blackHoleSpin, hSlope=hSlope, X1Start=X1Start, X1End=X1End,
+                            X2Start=X2Start, X2End=X2End, X3Start=X3Start, X3End=X3End, **params)
+        if C.var_counts(cfg)[0] != numVars:
+            raise ValueError("numVars %d does not match the EMHD switches" % numVars)
+        return cls(cfg)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.lib().grim_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- stepping ----------------------------------------------------------
+    def timeStep(self):
+        r, w = ctypes.c_int(), ctypes.c_int()
+        _lib.check(_lib.lib().grim_time_step(self._h, ctypes.byref(r), ctypes.byref(w)), "timeStep")
+        return r.value, w.value
+
+    def timeSteps(self, n):
+        _lib.check(_lib.lib().grim_time_steps(self._h, int(n)), "timeSteps")
+
+    @property
+    def time(self):
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        _lib.check(_lib.lib().grim_get_time(self._h, ctypes.byref(t), ctypes.byref(dt)), "get_time")
+        return t.value
+
+    @property
+    def dt(self):
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        _lib.check(_lib.lib().grim_get_time(self._h, ctypes.byref(t), ctypes.byref(dt)), "get_time")
+        return dt.value
+
+    def setTime(self, time, dt):
+        _lib.check(_lib.lib().grim_set_time(self._h, float(time), float(dt)), "set_time")
+
+    def computeDt(self):
+        _lib.check(_lib.lib().grim_compute_dt(self._h), "computeDt")
+        return self.dt
+
+    def synchronize(self):
+        _lib.check(_lib.lib().grim_synchronize(self._h), "synchronize")
+
+    def enableGraph(self, on=True):
+        _lib.check(_lib.lib().grim_enable_graph(self._h, int(bool(on))), "enable_graph")
+
+    def setNewtonMode(self, mode, perZone=1, rtol=0.0):
+        _lib.check(_lib.lib().grim_set_newton_mode(self._h, int(mode), int(perZone), float(rtol)),
+                   "set_newton_mode")
+        self.cfg["newtonMode"] = int(mode)
+        self.cfg["nonlinearsolve_rtol"] = float(rtol)
+
+    def stats(self):
+        s = _lib.GrimStats()
+        _lib.check(_lib.lib().grim_get_stats(self._h, ctypes.byref(s)), "get_stats")
+        return dict(newtonIters=list(s.newtonIters), unconverged=list(s.unconverged),
+                    nonFinite=s.nonFinite, msStep=s.msStep, msStencil=s.msStencil,
+                    msNewton=s.msNewton, msOther=s.msOther, kernelLaunches=s.kernelLaunches)
+
+    def stream(self):
+        return _lib.lib().grim_stream(self._h)
+
+    # ---- stage pieces --------------------------------------------------------
+    def _zeros(self, nv):
+        return np.zeros((nv,) + self.zshape)
+
+    def applyBoundaryConditions(self, which=_lib.PRIM_OLD):
+        _lib.check(_lib.lib().grim_apply_boundaries(self._h, int(which)), "apply_boundaries")
+
+    def computeDivOfFluxes(self, prim):
+        """divFluxes (dof x Z) and the face fluxes (3 x dof x Z, before CT)."""
+        p = np.ascontiguousarray(prim, dtype=np.float64)
+        divF = self._zeros(self.dof)
+        fl = np.zeros((3, self.dof) + self.zshape)
+        _lib.check(_lib.lib().grim_compute_div_fluxes(self._h, _ptr(p), _ptr(divF), _ptr(fl), None,
+                                                      _lib.HOST), "computeDivOfFluxes")
+        return divF, fl
+
+    def reconstruct(self, prim, direction):
+        p = np.ascontiguousarray(prim, dtype=np.float64)
+        pl, pr = self._zeros(self.dof), self._zeros(self.dof)
+        _lib.check(_lib.lib().grim_reconstruct(self._h, _ptr(p), int(direction), _ptr(pl), _ptr(pr),
+                                               _lib.HOST), "reconstruct")
+        return pl, pr
+
+    def conserved(self, prim):
+        p = np.ascontiguousarray(prim, dtype=np.float64)
+        out = self._zeros(self.dof)
+        _lib.check(_lib.lib().grim_conserved(self._h, _ptr(p), _ptr(out), _lib.HOST), "conserved")
+        return out
+
+    def charSpeeds(self, prim, direction):
+        p = np.ascontiguousarray(prim, dtype=np.float64)
+        mn, mx = np.zeros(self.zshape), np.zeros(self.zshape)
+        _lib.check(_lib.lib().grim_char_speeds(self._h, _ptr(p), int(direction), _ptr(mn), _ptr(mx),
+                                               _lib.HOST), "charSpeeds")
+        return mn, mx
+
+    def stageSetup(self, stage):
+        _lib.check(_lib.lib().grim_stage_setup(self._h, int(stage)), "stage_setup")
+
+    def computeResidual(self, primGuess):
+        p = np.ascontiguousarray(primGuess, dtype=np.float64)
+        out = self._zeros(self.numFluidVars)
+        _lib.check(_lib.lib().grim_residual(self._h, _ptr(p), _ptr(out), _lib.HOST), "residual")
+        return out
+
+    def jacobianFD(self, primGuess):
+        p = np.ascontiguousarray(primGuess, dtype=np.float64)
+        nf = self.numFluidVars
+        J = np.zeros(self.zshape + (nf, nf))
+        _lib.check(_lib.lib().grim_jacobian_fd(self._h, _ptr(p), _ptr(J), _lib.HOST), "jacobian_fd")
+        return J
+
+    def jacobianTangent(self, primGuess):
+        p = np.ascontiguousarray(primGuess, dtype=np.float64)
+        nf = self.numFluidVars
+        J = np.zeros(self.zshape + (nf, nf))
+        _lib.check(_lib.lib().grim_jacobian_tangent(self._h, _ptr(p), _ptr(J), _lib.HOST), "jacobian_tangent")
+        return J
+
+    def solve(self):
+        it = ctypes.c_int()
+        _lib.check(_lib.lib().grim_newton_solve(self._h, ctypes.byref(it)), "newton_solve")
+        return it.value
+
+    def getGeometry(self, location):
+        out = np.zeros((34,) + self.zshape)
+        gam = np.zeros((64,) + self.zshape)
+        xc = np.zeros((2,) + self.zshape)
+        _lib.check(_lib.lib().grim_get_geometry(self._h, int(location), _ptr(out), _ptr(gam), _ptr(xc),
+                                                _lib.HOST), "get_geometry")
+        return dict(gCov=out[:16].reshape((4, 4) + self.zshape), gCon=out[16:32].reshape((4, 4) + self.zshape),
+                    g=out[32], alpha=out[33], gamma=gam.reshape((4, 4, 4) + self.zshape), x=xc)
+
+    def setGeometry(self, location, gCov, gCon, g, alpha, x=None, gamma=None):
+        out = np.concatenate([np.reshape(gCov, (16,) + self.zshape), np.reshape(gCon, (16,) + self.zshape),
+                              np.reshape(g, (1,) + self.zshape), np.reshape(alpha, (1,) + self.zshape)])
+        out = np.ascontiguousarray(out, dtype=np.float64)
+        xc = None if x is None else np.ascontiguousarray(np.reshape(x, (-1,) + self.zshape)[:2])
+        gm = None if gamma is None else np.ascontiguousarray(np.reshape(gamma, (64,) + self.zshape))
+        _lib.check(_lib.lib().grim_set_geometry(self._h, int(location), _ptr(out),
+                                                None if gm is None else _ptr(gm),
+                                                None if xc is None else _ptr(xc), _lib.HOST), "set_geometry")
+
+
+def batchSolve(A, b):
+    """The batched pivoted solve of the Newton kernels on a host batch."""
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    n, batch = A.shape[-1], A.shape[0]
+    x = np.zeros((batch, n))
+    _lib.check(_lib.lib().grim_batch_solve(n, batch, _ptr(A), _ptr(b), _ptr(x), _lib.HOST), "batch_solve")
+    return x

@@ -1,0 +1,193 @@
+/*
+ * grim_b200.h -- C ABI of the B200 (sm_100a) implicit GRMHD/EMHD timestep.
+ *
+ * Drop-in for the reference's timeStepper (AFD-Illinois/grim,
+ * src/timestepper/timestepper.hpp:19-132): one handle owns the grids,
+ * geometry, stage buffers and one CUDA stream, exactly as one timeStepper
+ * object owns its grids, geometry objects and fluid elements.
+ *
+ * Conventions
+ *  - Every call returns an int status: 0 = OK, < 0 = error (GRIM_E*).
+ *    No exceptions cross the ABI.
+ *  - Primitive arrays are FP64 in [var][k][j][i] order including ghost
+ *    zones (i fastest), the layout of the reference's grid::vars and of
+ *    gridPy.getVars (src/grid/gridPy.pyx:185-221).  N1T = N1 + 2*numGhost,
+ *    N2T/N3T likewise for active dimensions (1 otherwise).
+ *  - Pointers passed with GRIM_HOST are host memory (pageable or pinned),
+ *    GRIM_DEVICE pointers are device memory on the handle's GPU.  The library
+ *    copies; the caller keeps ownership.
+ *  - All work is asynchronous on the handle's stream except the getters of
+ *    scalars and statistics, which synchronise.  Calls on one handle are not
+ *    thread-safe; different handles are independent.
+ */
+#ifndef GRIM_B200_H_
+#define GRIM_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define GRIM_OK            0
+#define GRIM_EINVAL       -1   /* bad argument or configuration */
+#define GRIM_ECUDA        -2   /* a CUDA runtime call failed */
+#define GRIM_ENOMEM       -3   /* device allocation failed */
+#define GRIM_ESTATE       -4   /* call not valid in the current state */
+#define GRIM_ENOTSUP      -5   /* configuration not supported */
+#define GRIM_ETIMEOUT     -6   /* a bounded device wait gave up */
+#define GRIM_ENONFINITE   -7   /* NaN/Inf detected in a result */
+
+/* ---- enums (src/params.hpp:32-94; MP5, closures, Newton modes are new) -- */
+enum { GRIM_PERIODIC = 0, GRIM_OUTFLOW = 1, GRIM_MIRROR = 2, GRIM_DIRICHLET = 3 };
+enum { GRIM_MINKOWSKI = 0, GRIM_MODIFIED_KERR_SCHILD = 1 };
+enum { GRIM_MINMOD = 0, GRIM_WENO5 = 1, GRIM_PPM = 2, GRIM_MP5 = 3 };
+enum { GRIM_HLL = 0, GRIM_LOCAL_LAX_FRIEDRICH = 1 };
+enum { GRIM_CENTER = 0, GRIM_LEFT = 1, GRIM_RIGHT = 2, GRIM_TOP = 3, GRIM_BOTTOM = 4 };
+enum { GRIM_HALF_STEP = 0, GRIM_FULL_STEP = 1 };
+enum { GRIM_CLOSURE_CONST_TAU = 0, GRIM_CLOSURE_TORUS = 1, GRIM_CLOSURE_TAU_PROFILE = 2 };
+enum { GRIM_PROBLEM_NONE = 0, GRIM_PROBLEM_TORUS = 1 };
+enum {
+  GRIM_NEWTON_PARITY_FD64 = 0, /* reference method: FD Jacobian, FP64, global break */
+  GRIM_NEWTON_TANGENT64   = 1, /* exact forward-tangent Jacobian, FP64 solve */
+  GRIM_NEWTON_MIXED32     = 2  /* FP32 tangent Jacobian + FP32 solve, FP64 residual */
+};
+enum { GRIM_HOST = 0, GRIM_DEVICE = 1 };
+enum { GRIM_PRIM_OLD = 0, GRIM_PRIM = 1, GRIM_PRIM_HALF = 2 };
+
+/*
+ * Configuration.  Field names are the reference's params:: globals
+ * (src/params.hpp:96-210) and timeStepper constructor arguments
+ * (timestepper.hpp:94-111).  Integers first, then doubles.
+ */
+typedef struct grim_config {
+  int N1, N2, N3, dim, numGhost;
+  int boundaryLeft, boundaryRight, boundaryTop, boundaryBottom;
+  int boundaryFront, boundaryBack;
+  int metric;
+  int DerefineThetaHorizon, DoCylindrify;
+  int conduction, viscosity;
+  int highOrderTermsConduction, highOrderTermsViscosity;
+  int reconstruction, riemannSolver;
+  int maxNonLinearIter, maxLineSearchIters;
+  int closure;              /* setFluidElementParameters variant */
+  int problem;              /* problem hooks: BCs, flux filter, floors */
+  int elemOldFromFullStep;  /* 1: fullStepDiagnostics re-sets elemOld */
+  int newtonMode;           /* GRIM_NEWTON_* */
+  int perZoneConvergence;   /* 0: global break (reference), 1: per zone */
+  int reserved_i[5];
+  double blackHoleSpin, hSlope;
+  double X1Start, X1End, X2Start, X2End, X3Start, X3End;
+  double time, dt;
+  double X1cyl, X2cyl;
+  double rhoFloorInFluidElement, uFloorInFluidElement;
+  double bSqrFloorInFluidElement, temperatureFloorInFluidElement;
+  double adiabaticIndex, ConductionAlpha, ViscosityAlpha;
+  double ConductionClosureFactor, ViscosityClosureFactor;
+  double slopeLimTheta;
+  double nonlinearsolve_atol, nonlinearsolve_rtol;
+  double JacobianAssembleEpsilon, linesearchfloor;
+  double CourantFactor, maxDtIncrement;
+  double closureTau0, closureTau1;
+  double MaxLorentzFactor, RhoFloorAmpl, UFloorAmpl, RhoFloorSlope, UFloorSlope;
+  double BsqrOverRhoMax, BsqrOverUMax;
+  double reserved_d[6];
+} grim_config;
+
+typedef struct grim_handle grim_handle;
+
+/* Per-call statistics (grim_get_stats).  Times are CUDA-event milliseconds
+ * of the last grim_time_step call, measured on the handle's stream. */
+typedef struct grim_stats {
+  int    newtonIters[2];       /* Newton iterations of the half / full stage */
+  long long unconverged[2];    /* zones above tolerance when each stage ended */
+  long long nonFinite;         /* NaN/Inf primitives after the last step */
+  double msStep;               /* whole grim_time_step */
+  double msStencil;            /* stencil kernels, both stages */
+  double msNewton;             /* Newton kernels, both stages */
+  double msOther;              /* ghost fill, dt, copies */
+  long long kernelLaunches;    /* launches of this library's kernels in the step */
+  double reserved[8];
+} grim_stats;
+
+/* ---- lifecycle: timeStepper::timeStepper / ~timeStepper
+ *      (timestepper.cpp:4-470) ------------------------------------------ */
+int grim_create(const grim_config* cfg, int device, grim_handle** out);
+int grim_destroy(grim_handle* h);
+int grim_dims(const grim_handle* h, int* N1T, int* N2T, int* N3T, int* dof, int* numFluidVars);
+const char* grim_version(void);
+const char* grim_last_error(void);
+
+/* ---- state: grid::vars through gridPy.getVars / setVars
+ *      (gridPy.pyx:185-221); which = GRIM_PRIM_OLD | GRIM_PRIM | GRIM_PRIM_HALF */
+int grim_set_prims(grim_handle* h, int which, const double* src, int memKind);
+int grim_get_prims(grim_handle* h, int which, double* dst, int memKind);
+
+/* ---- stepping: timeStepper::timeStep (timestep.cpp:3-334); numReads and
+ *      numWrites report the algorithmic words per zone, may be NULL ------ */
+int grim_time_step(grim_handle* h, int* numReads, int* numWrites);
+int grim_time_steps(grim_handle* h, int nsteps);
+int grim_get_time(grim_handle* h, double* time, double* dt);
+int grim_set_time(grim_handle* h, double time, double dt);
+
+/* ---- stage pieces (timestepper.hpp:88-123) ---------------------------- */
+/* computeDt (timestep.cpp:336-400): updates dt from the current elemOld state */
+int grim_compute_dt(grim_handle* h);
+/* ghost fill of one state buffer: periodic wrap + outflow/mirror
+ * (boundary.cpp:5-241, grid.cpp:306-315) */
+int grim_apply_boundaries(grim_handle* h, int which);
+/* computeDivOfFluxes (fvmfluxes.cpp:3-183) incl. fluxCT/computeEMF
+ * (constrainedtransport.cpp:3-83) on a caller's prim array; outputs may be
+ * NULL.  divF: dof x Z, fluxes: 3 x dof x Z, emf: 3 x Z (X1, X2, X3). */
+int grim_compute_div_fluxes(grim_handle* h, const double* prim, double* divF,
+                            double* fluxes, double* emf, int memKind);
+/* reconstruction of one direction (reconstruction.cpp:3-36) */
+int grim_reconstruct(grim_handle* h, const double* prim, int dir,
+                     double* primLeft, double* primRight, int memKind);
+/* computeDivB diagnostic (constrainedtransport.cpp:85-107), 2D */
+int grim_compute_divb(grim_handle* h, const double* prim, double* divB, int memKind);
+/* conserved variables and characteristic speeds of a prim array at the
+ * zone centres (physics.cpp:185-217, riemannsolver.cpp:54-200) */
+int grim_conserved(grim_handle* h, const double* prim, double* cons, int memKind);
+int grim_char_speeds(grim_handle* h, const double* prim, int dir,
+                     double* minSpeed, double* maxSpeed, int memKind);
+
+/* ---- Newton pieces (solve.cpp, residual.cpp) -------------------------- */
+/* Stage set-up of timeStep (BCs, elemOld, consOld, sources, divF,
+ * induction) on the current state, leaving the Newton guess in GRIM_PRIM. */
+int grim_stage_setup(grim_handle* h, int stage);
+/* computeResidual (residual.cpp:3-180) of a guess: nf x Z */
+int grim_residual(grim_handle* h, const double* primGuess, double* residual, int memKind);
+/* FD Jacobian (solve.cpp:82-109): [Z][nf][nf], J[z][i][j] = dR_i/dP_j */
+int grim_jacobian_fd(grim_handle* h, const double* primGuess, double* jac, int memKind);
+/* exact forward-tangent Jacobian of the same residual, same layout */
+int grim_jacobian_tangent(grim_handle* h, const double* primGuess, double* jac, int memKind);
+/* solve() on GRIM_PRIM with the configured newtonMode */
+int grim_newton_solve(grim_handle* h, int* itersDone);
+/* batched pivoted solve of nf x nf systems (the af::solve of solve.cpp:220)
+ * A: [batch][n][n] row-major, b: [batch][n] */
+int grim_batch_solve(int n, int batch, const double* A, const double* b, double* x, int memKind);
+
+/* ---- geometry (geometry.cpp:4-680) ------------------------------------ */
+/* out = [16 gCov | 16 gCon | g | alpha] x Z; gamma (center only) 64 x Z;
+ * xcoords 3 x Z.  get copies out, set replaces the device copy. */
+int grim_get_geometry(grim_handle* h, int location, double* out, double* gamma,
+                      double* xcoords, int memKind);
+int grim_set_geometry(grim_handle* h, int location, const double* in,
+                      const double* gamma, const double* xcoords, int memKind);
+
+/* ---- options, statistics, graphs ------------------------------------- */
+int grim_set_newton_mode(grim_handle* h, int mode, int perZoneConvergence, double rtol);
+int grim_get_stats(grim_handle* h, grim_stats* out);
+/* capture timeStep into a CUDA graph and replay it from grim_time_step */
+int grim_enable_graph(grim_handle* h, int enable);
+int grim_synchronize(grim_handle* h);
+/* the handle's cudaStream_t, as void* */
+void* grim_stream(grim_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GRIM_B200_H_ */

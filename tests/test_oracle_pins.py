@@ -1,0 +1,208 @@
+"""Pins of the CPU oracle against the reference's own known answers.
+
+The reference cannot be built here (ArrayFire, PETSc and MPI are absent),
+so the oracle is pinned on the reference's published and tested results:
+  * the damped EMHD eigenmode of linear_modes and its 2nd-order convergence
+    (src/problem/linear_modes/problem.cpp:118-213, Linear modes.ipynb);
+  * the analytic modified Kerr-Schild metric, inverse, sqrt(-g), lapse and
+    Christoffel symbols of McKinney & Gammie 2004 used by
+    src/geometry/test_geometry.py:93-345;
+  * the outflow / mirror ghost-copy rules of src/boundary/test_boundary.py;
+  * LAPACK (scipy.linalg.solve) for the batched pivoted solve that stands
+    in for af::solve (solve.cpp:220);
+  * committed golden snapshots (tests/golden/, made by make_golden.py).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from grim_b200 import config as C
+from grim_b200 import problems as PR
+from oracle import oracle as O
+from tests.helpers import interior
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _lm_errors(N, tfinal=0.25):
+    cfg = PR.linear_modes_config(N=N)
+    o = O.Oracle(cfg)
+    o.set_prims(PR.linear_modes_prims(cfg))
+    while o.time < tfinal:
+        o.time_step(1)
+    P = o.get_prims()
+    an = PR.linear_modes_analytic(cfg, o.time)
+    idx = C.var_index(cfg)
+    q, dP = PR.emhd_physical(cfg, P)
+    errs = {}
+    for name in ("RHO", "U", "U1", "U2", "B1", "B2"):
+        errs[name] = float(np.mean(np.abs(interior(cfg, P[idx[name]]) - interior(cfg, an[name]))))
+    errs["Q"] = float(np.mean(np.abs(interior(cfg, q) - interior(cfg, an["Q"]))))
+    errs["DP"] = float(np.mean(np.abs(interior(cfg, dP) - interior(cfg, an["DP"]))))
+    return errs
+
+
+def test_linear_mode_second_order():
+    """The EMHD eigenmode (omega = -0.5534 - 3.6263 i) converges at 2nd
+    order in every primitive, the reference's published behaviour."""
+    e16, e32, e64 = _lm_errors(16), _lm_errors(32), _lm_errors(64)
+    for k in e32:
+        order = np.log2(e32[k] / e64[k])
+        assert order > 1.6, (k, order, e32[k], e64[k])
+        assert np.log2(e16[k] / e64[k]) / 2 > 1.6
+    # errors per unit amplitude are O(1e-2..1e-3) of the mode at 64^2
+    assert e64["RHO"] < 1e-10
+
+
+def _mks_config(N=16):
+    return C.make_config(N1=N, N2=N, N3=8, dim=3, metric=C.MODIFIED_KERR_SCHILD, blackHoleSpin=0.5,
+                         hSlope=0.7, DerefineThetaHorizon=0, DoCylindrify=0, X1Start=0., X1End=1.,
+                         X2Start=0., X2End=1., X3Start=0., X3End=1.,
+                         boundaryLeft=C.OUTFLOW, boundaryRight=C.OUTFLOW, boundaryTop=C.MIRROR,
+                         boundaryBottom=C.MIRROR)
+
+
+def test_mks_metric_matches_analytic():
+    """geometry/test_geometry.py:93-185: McKinney & Gammie (2004) MKS."""
+    cfg = _mks_config()
+    o = O.Oracle(cfg)
+    G = o.geometry(C.CENTER)
+    X1, X2, X3 = C.cell_centers(cfg)
+    a, h = 0.5, 0.7
+    r = np.exp(X1)
+    th = np.pi * X2 + 0.5 * (1. - h) * np.sin(2. * np.pi * X2)
+    sigma = r ** 2 + (a * np.cos(th)) ** 2
+    dr = np.exp(X1)
+    dth = np.pi * (1. + (1. - h) * np.cos(2. * np.pi * X2))
+    g = np.zeros((4, 4) + r.shape)
+    g[0, 0] = -(1. - 2 * r / sigma)
+    g[0, 1] = g[1, 0] = (2 * r / sigma) * dr
+    g[0, 3] = g[3, 0] = -(2. * a * r * np.sin(th) ** 2 / sigma)
+    g[1, 1] = (1. + 2 * r / sigma) * dr ** 2
+    g[1, 3] = g[3, 1] = -a * (1. + 2 * r / sigma) * np.sin(th) ** 2 * dr
+    g[2, 2] = sigma * dth * dth
+    g[3, 3] = np.sin(th) ** 2 * (sigma + a ** 2 * (1. + 2. * r / sigma) * np.sin(th) ** 2)
+    np.testing.assert_allclose(G["gCov"], g, rtol=1e-12, atol=1e-14)
+    gm = np.moveaxis(g.reshape(4, 4, -1), -1, 0)
+    ginv = np.linalg.inv(gm)
+    gcon = np.moveaxis(ginv, 0, -1).reshape(g.shape)
+    np.testing.assert_allclose(G["gCon"], gcon, rtol=1e-10, atol=1e-13)
+    gdet = np.sqrt(-np.linalg.det(gm)).reshape(r.shape)
+    np.testing.assert_allclose(G["g"], gdet, rtol=1e-12)
+    np.testing.assert_allclose(G["alpha"], 1. / np.sqrt(-gcon[0, 0]), rtol=1e-12)
+    np.testing.assert_allclose(G["x"][0], r, rtol=1e-14)
+    np.testing.assert_allclose(G["x"][1], th, rtol=1e-14)
+
+
+def test_mks_christoffels_match_analytic():
+    """geometry/test_geometry.py:187-345 (a subset of the analytic
+    Gamma^mu_{nu lambda}); the oracle's are central differences with
+    eps = 1e-5 as in geometry.cpp:61-119, hence the tolerances."""
+    cfg = _mks_config()
+    o = O.Oracle(cfg)
+    gam = o.geometry(C.CENTER)["gamma"]
+    X1, X2, X3 = C.cell_centers(cfg)
+    a, h = 0.5, 0.7
+    r = np.exp(X1)
+    th = np.pi * X2 + 0.5 * (1. - h) * np.sin(2. * np.pi * X2)
+    s, c = np.sin(th), np.cos(th)
+    sigma = r ** 2 + (a * c) ** 2
+    sm = r ** 2 - (a * c) ** 2
+    dth = np.pi * (1. + (1. - h) * np.cos(2. * np.pi * X2))
+    ref = {
+        (0, 0, 0): 2. * r * sm / sigma ** 3,
+        (0, 0, 1): r * (2 * r + sigma) * sm / sigma ** 3,
+        (0, 0, 3): -2. * a * r * s ** 2 * sm / sigma ** 3,
+        (0, 2, 2): -2. * r ** 2 * dth ** 2 / sigma,
+        (1, 0, 0): (a ** 2 + r * (-2. + r)) * sm / (r * sigma ** 3),
+        (1, 2, 2): -(a ** 2 + r * (-2. + r)) * dth ** 2 / sigma,
+        (2, 1, 2): r ** 2 / sigma,
+        (3, 0, 0): a * sm / sigma ** 3,
+        (3, 1, 1): a * r ** 2 * sm / sigma ** 3,
+        (3, 2, 2): -a * r * dth ** 2 / sigma,
+    }
+    for (m, n, l), v in ref.items():
+        np.testing.assert_allclose(gam[m, n, l], v, rtol=1e-6, atol=1e-7, err_msg=str((m, n, l)))
+
+
+def test_boundary_copy_rules():
+    """boundary/test_boundary.py:56-243: outflow copies the edge zone,
+    mirror reflects without sign flips, periodic wraps."""
+    cfg = C.make_config(N1=8, N2=8, N3=8, dim=3, boundaryLeft=C.OUTFLOW, boundaryRight=C.MIRROR,
+                        boundaryBottom=C.MIRROR, boundaryTop=C.OUTFLOW, boundaryBack=C.PERIODIC,
+                        boundaryFront=C.PERIODIC)
+    o = O.Oracle(cfg)
+    rng = np.random.default_rng(0)
+    P = rng.standard_normal(o.shape)
+    Q = o.apply_boundaries(P)
+    g, N = 3, 8
+    I = slice(g, g + N)
+    for gi in range(g):
+        np.testing.assert_array_equal(Q[:, I, I, gi], P[:, I, I, g])                 # outflow left
+        np.testing.assert_array_equal(Q[:, I, I, N + g + gi], P[:, I, I, N + g - 1 - gi])  # mirror right
+        np.testing.assert_array_equal(Q[:, I, gi, I], P[:, I, 2 * g - 1 - gi, I])    # mirror bottom
+        np.testing.assert_array_equal(Q[:, I, N + g + gi, I], P[:, I, N + g - 1, I])  # outflow top
+        np.testing.assert_array_equal(Q[:, gi, I, I], P[:, N + gi, I, I])            # periodic back
+        np.testing.assert_array_equal(Q[:, N + g + gi, I, I], P[:, g + gi, I, I])    # periodic front
+    # interior untouched
+    np.testing.assert_array_equal(Q[:, I, I, I], P[:, I, I, I])
+    # corners: composite of the per-direction maps
+    np.testing.assert_array_equal(Q[:, 0, 0, 0], P[:, N, 2 * g - 1, g])
+
+
+def test_pivoted_solve_matches_lapack():
+    scipy_linalg = pytest.importorskip("scipy.linalg")
+    rng = np.random.default_rng(2)
+    for n in (5, 6, 7):
+        A = rng.standard_normal((200, n, n))
+        A[:, 0, 0] = 1e-12  # forces a pivot
+        b = rng.standard_normal((200, n))
+        x = O.batch_solve(A, b)
+        ref = np.stack([scipy_linalg.solve(A[i], b[i]) for i in range(200)])
+        np.testing.assert_allclose(x, ref, rtol=1e-9, atol=1e-12)
+
+
+def test_minmod_afsign_convention():
+    """minmod.cpp:11-16: sign(0) counts as positive, so a zero slope on
+    one side and a positive one on the other gives a zero limited slope."""
+    cfg = PR.fast_mode_config(N=8)
+    o = O.Oracle(cfg)
+    P = np.zeros(o.shape)
+    P[:, :, :, 7:] = 1.0
+    pl, pr = o.reconstruct(P, 0)
+    assert np.all(pl[:, :, :, 4] == 0.) and np.all(pr[:, :, :, 4] == 0.)
+    assert np.all(pl[:, :, :, 7] == 1.) and np.all(pr[:, :, :, 7] == 1.)
+
+
+def test_golden_snapshots():
+    """oracle output regression against the committed fixtures."""
+    path = os.path.join(GOLDEN, "golden.json")
+    gold = json.load(open(path))
+    for name, case in gold["cases"].items():
+        cfg = C.make_config(**case["config"])
+        import importlib
+        mk = getattr(PR, case["prims"])
+        P = mk(cfg, **case.get("prims_kw", {}))
+        o = O.Oracle(cfg)
+        o.set_prims(P)
+        o.time_step(case["steps"])
+        Q = o.get_prims()
+        assert abs(o.time - case["time"]) <= 1e-15 * case["time"], name
+        got = [float(x) for x in np.sum(interior(cfg, Q), axis=(1, 2, 3))]
+        np.testing.assert_allclose(got, case["var_sums"], rtol=1e-13, err_msg=name)
+        probe = Q[(slice(None),) + tuple(case["probe_index"])]
+        np.testing.assert_allclose(probe, case["probe"], rtol=1e-13, err_msg=name)
+
+
+def test_published_l1_table_order():
+    """Linear modes.ipynb cell 1: the published L1 errors fall at 2nd order
+    (the fixture holds the table as published)."""
+    gold = json.load(open(os.path.join(GOLDEN, "golden.json")))
+    tab = gold["published_linear_modes_L1"]
+    N = np.array(tab["N"], dtype=float)
+    for k, v in tab["errors"].items():
+        v = np.array(v)
+        slope = -np.polyfit(np.log2(N), np.log2(v), 1)[0]
+        assert 1.7 < slope < 3.7, (k, slope)

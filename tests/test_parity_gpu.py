@@ -1,0 +1,265 @@
+"""Parity of the CUDA timestep (libgrim_b200.so, through its C ABI) with the
+CPU oracle on the same seeded inputs.
+
+Tolerances (stated per test):
+  * pointwise kernels of the FP64 parity path (reconstruction, conserved
+    variables, characteristic speeds, batched solve): <= 1e-15 relative;
+  * divergence of fluxes, residual: <= 1e-13 of the variable's scale;
+  * FD Jacobian: <= 1e-6 relative per column scale (it is a divided
+    difference with eps = 4e-8, so 1e-16 perturbations of the residual are
+    amplified by ~1/eps);
+  * primitives after N full timesteps on the plain FP64 path: 1e-12
+    relative;
+  * tangent / mixed paths: the error bounds stated in their tests.
+"""
+import numpy as np
+import pytest
+
+from grim_b200 import config as C
+from grim_b200 import problems as PR
+from tests.helpers import interior, rel_err, scaled_err, pair
+
+pytestmark = pytest.mark.gpu
+
+
+def _smooth_random(cfg, seed, amp=0.05):
+    """a smooth positive state with random phases (all dof vars)"""
+    rng = np.random.default_rng(seed)
+    X1, X2, X3 = C.cell_centers(cfg)
+    dof, nf = C.var_counts(cfg)
+    P = np.zeros((dof,) + X1.shape)
+    base = [1.0, 2.0, 0.0, 0.0, 0.0] + [0.0] * (nf - 5) + [0.1, 0.3, 0.05]
+    for v in range(dof):
+        ph = rng.uniform(0, 2 * np.pi, 3)
+        P[v] = base[v] + amp * (np.sin(2 * np.pi * X1 + ph[0]) * np.cos(2 * np.pi * X2 + ph[1])
+                                + 0.3 * np.sin(4 * np.pi * (X1 + X2) + ph[2]))
+    return P
+
+
+@pytest.mark.parametrize("recon", [C.MINMOD, C.WENO5, C.PPM, C.MP5])
+def test_reconstruction_matches_oracle(recon):
+    cfg = PR.fast_mode_config(N=16, reconstruction=recon)
+    ts, orc = pair(cfg)
+    rng = np.random.default_rng(7)
+    P = rng.uniform(-1, 1, (8,) + ts.zshape)
+    P[:, 5:9, :] += 3.0  # a jump so the limiters act
+    for d in range(2):
+        gl, gr = ts.reconstruct(P, d)
+        ol, orr = orc.reconstruct(P, d)
+        assert rel_err(gl, ol, 1e-300) <= 1e-15
+        assert rel_err(gr, orr, 1e-300) <= 1e-15
+
+
+@pytest.mark.parametrize("emhd", [0, 1])
+def test_conserved_and_char_speeds(emhd):
+    cfg = (PR.linear_modes_config(N=16) if emhd else PR.fast_mode_config(N=16))
+    ts, orc = pair(cfg)
+    P = _smooth_random(cfg, 3)
+    g = ts.conserved(P)
+    o = orc.conserved(P)
+    assert rel_err(g, o, 1e-300) <= 1e-15
+    for d in range(2):
+        gm, gx = ts.charSpeeds(P, d)
+        om, ox = orc.char_speeds(P, d)
+        assert rel_err(gm, om) <= 1e-15 and rel_err(gx, ox) <= 1e-15
+
+
+@pytest.mark.parametrize("case", ["fast_mode", "orszag_tang", "linear_modes", "emhd_mp5"])
+def test_div_fluxes(case):
+    if case == "fast_mode":
+        cfg = PR.fast_mode_config(N=24)
+        P = PR.fast_mode_prims(cfg)
+    elif case == "orszag_tang":
+        cfg = PR.orszag_tang_config(N=32)
+        P = PR.orszag_tang_prims(cfg)
+    elif case == "linear_modes":
+        cfg = PR.linear_modes_config(N=24)
+        P = PR.linear_modes_prims(cfg, amplitude=1e-3)
+    else:
+        cfg = PR.emhd_stratified_config(N=24)
+        P = PR.emhd_stratified_prims(cfg)
+    ts, orc = pair(cfg)
+    P = orc.apply_boundaries(P)
+    gd, gf = ts.computeDivOfFluxes(P)
+    od, of, _ = orc.div_fluxes(P)
+    assert scaled_err(interior(cfg, gd), interior(cfg, od)) <= 1e-13
+    nf = C.var_counts(cfg)[1]
+    # raw Riemann fluxes of the fluid rows on the interior faces
+    for d in range(2):
+        assert scaled_err(interior(cfg, gf[d][:nf]), interior(cfg, of[d][:nf])) <= 1e-14
+
+
+@pytest.mark.parametrize("case", ["fast_mode", "linear_modes"])
+def test_residual_and_fd_jacobian(case):
+    if case == "fast_mode":
+        cfg = PR.fast_mode_config(N=16)
+        P = PR.fast_mode_prims(cfg)
+    else:
+        cfg = PR.linear_modes_config(N=16)
+        P = PR.linear_modes_prims(cfg, amplitude=1e-4)
+    ts, orc = pair(cfg)
+    ts.primOld.setVars(P)
+    orc.set_prims(P)
+    ts.stageSetup(C.HALF_STEP)
+    orc.stage_setup(C.HALF_STEP)
+    guess = orc.get_prims(1)  # the oracle's Newton guess (fluid = primOld, B induced)
+    gguess = ts.prim.getVars()
+    assert scaled_err(interior(cfg, gguess), interior(cfg, guess)) <= 1e-14
+    rng = np.random.default_rng(5)
+    trial = guess.copy()
+    nf = C.var_counts(cfg)[1]
+    trial[:nf] *= 1. + 1e-6 * rng.standard_normal(trial[:nf].shape)
+    gr = ts.computeResidual(trial)
+    orr = orc.residual(trial)
+    assert scaled_err(interior(cfg, gr), interior(cfg, orr)) <= 1e-12
+    gJ = ts.jacobianFD(trial)
+    oJ = orc.jacobian_fd(trial)
+    s3, s2, s1 = C.interior_slices(cfg)
+    a, b = gJ[s3, s2, s1], oJ[s3, s2, s1]
+    scale = np.max(np.abs(b), axis=(0, 1, 2, 3)) + 1e-300
+    assert float(np.max(np.abs(a - b) / scale)) <= 1e-6
+
+
+def _run_both(cfg, P, nsteps):
+    ts, orc = pair(cfg)
+    ts.primOld.setVars(P)
+    orc.set_prims(P)
+    for _ in range(nsteps):
+        ts.timeStep()
+    orc.time_step(nsteps)
+    return ts, orc
+
+
+def test_timestep_parity_fast_mode_128():
+    """2D ideal GRMHD fast mode, Minkowski 128^2, minmod/LLF, FD Newton:
+    20 steps, primitives within 1e-12 relative of the oracle."""
+    cfg = PR.fast_mode_config(N=128)
+    P = PR.fast_mode_prims(cfg, seed=1)
+    ts, orc = _run_both(cfg, P, 20)
+    g = interior(cfg, ts.primOld.getVars())
+    o = interior(cfg, orc.get_prims())
+    assert abs(ts.time - orc.time) <= 1e-15 * orc.time
+    assert rel_err(g, o, 1e-300) <= 1e-12
+
+
+def test_timestep_parity_emhd_linear_mode():
+    cfg = PR.linear_modes_config(N=32)
+    P = PR.linear_modes_prims(cfg)
+    ts, orc = _run_both(cfg, P, 10)
+    g = interior(cfg, ts.primOld.getVars())
+    o = interior(cfg, orc.get_prims())
+    assert abs(ts.time - orc.time) <= 1e-15 * orc.time
+    assert rel_err(g[:5], o[:5]) <= 1e-12
+    # q~ and dP~ oscillate around zero: relative to their amplitude
+    assert scaled_err(g[5:], o[5:]) <= 1e-12
+
+
+def test_timestep_parity_orszag_tang():
+    cfg = PR.orszag_tang_config(N=64)
+    P = PR.orszag_tang_prims(cfg)
+    ts, orc = _run_both(cfg, P, 5)
+    g = interior(cfg, ts.primOld.getVars())
+    o = interior(cfg, orc.get_prims())
+    assert scaled_err(g, o) <= 1e-12
+
+
+def test_timestep_parity_emhd_stratified_mp5():
+    cfg = PR.emhd_stratified_config(N=32)
+    P = PR.emhd_stratified_prims(cfg)
+    ts, orc = _run_both(cfg, P, 4)
+    g = interior(cfg, ts.primOld.getVars())
+    o = interior(cfg, orc.get_prims())
+    assert scaled_err(g, o) <= 1e-12
+
+
+def test_linear_mode_second_order_on_gpu():
+    """The reference's known answer: the damped EMHD eigenmode converges at
+    2nd order (Linear modes.ipynb, cells 1-2)."""
+    errs = []
+    for N in (16, 32, 64):
+        cfg = PR.linear_modes_config(N=N)
+        from grim_b200.timestepper import timeStepper
+        ts = timeStepper(cfg)
+        ts.primOld.setVars(PR.linear_modes_prims(cfg))
+        while ts.time < 0.25:
+            ts.timeStep()
+        P = ts.primOld.getVars()
+        an = PR.linear_modes_analytic(cfg, ts.time)
+        idx = C.var_index(cfg)
+        e = np.mean(np.abs(interior(cfg, P[idx["RHO"]]) - interior(cfg, an["RHO"])))
+        errs.append(e)
+    o1, o2 = np.log2(errs[0] / errs[1]), np.log2(errs[1] / errs[2])
+    assert o1 > 1.5 and o2 > 1.7, (errs, o1, o2)
+
+
+def test_batch_solve_matches_numpy():
+    from grim_b200.timestepper import batchSolve
+    rng = np.random.default_rng(11)
+    for n in (5, 6, 7):
+        A = rng.standard_normal((500, n, n)) + n * np.eye(n)
+        b = rng.standard_normal((500, n))
+        x = batchSolve(A, b)
+        ref = np.linalg.solve(A, b[..., None])[..., 0]
+        assert float(np.max(np.abs(x - ref) / (np.abs(ref) + 1e-12))) <= 1e-10
+
+
+def test_graph_replay_is_bitwise_identical():
+    cfg = PR.fast_mode_config(N=32)
+    P = PR.fast_mode_prims(cfg)
+    from grim_b200.timestepper import timeStepper
+    a, b = timeStepper(cfg), timeStepper(cfg)
+    a.primOld.setVars(P)
+    b.primOld.setVars(P)
+    b.enableGraph(True)
+    for _ in range(5):
+        a.timeStep()
+        b.timeStep()
+    assert np.array_equal(a.primOld.getVars(), b.primOld.getVars())
+    assert a.time == b.time
+
+
+@pytest.mark.parametrize("case", ["fast_mode", "linear_modes"])
+def test_tangent_jacobian_matches_fd(case):
+    if case == "fast_mode":
+        cfg = PR.fast_mode_config(N=16)
+        P = PR.fast_mode_prims(cfg)
+    else:
+        cfg = PR.linear_modes_config(N=16)
+        P = PR.linear_modes_prims(cfg, amplitude=1e-4)
+    ts, orc = pair(cfg)
+    ts.primOld.setVars(P)
+    ts.stageSetup(C.HALF_STEP)
+    guess = ts.prim.getVars()
+    Jt = ts.jacobianTangent(guess)
+    Jf = ts.jacobianFD(guess)
+    s3, s2, s1 = C.interior_slices(cfg)
+    a, b = Jt[s3, s2, s1], Jf[s3, s2, s1]
+    scale = np.max(np.abs(a), axis=(0, 1, 2, 3)) + 1e-300
+    assert float(np.max(np.abs(a - b) / scale)) <= 1e-6
+
+
+@pytest.mark.parametrize("mode", [C.NEWTON_TANGENT64, C.NEWTON_MIXED32])
+def test_fast_newton_error_bound(mode):
+    """Tangent / mixed-precision Newton with per-zone convergence at
+    relative residual 1e-10 against the FD64 parity path at the same
+    tolerance: primitives agree within 1e-9 relative after 10 steps."""
+    cfg = PR.fast_mode_config(N=64, nonlinearsolve_rtol=1e-10, nonlinearsolve_atol=0.0,
+                              maxNonLinearIter=6)
+    P = PR.fast_mode_prims(cfg)
+    from grim_b200.timestepper import timeStepper
+    ref, fast = timeStepper(cfg), timeStepper(cfg)
+    fast.setNewtonMode(mode, 1, 1e-10)
+    ref.primOld.setVars(P)
+    fast.primOld.setVars(P)
+    for _ in range(10):
+        ref.timeStep()
+        fast.timeStep()
+    a = interior(cfg, fast.primOld.getVars())
+    b = interior(cfg, ref.primOld.getVars())
+    dP = interior(cfg, P)
+    # error relative to the change of the state over the run
+    err = np.max(np.abs(a - b)) / np.max(np.abs(b - dP))
+    assert err <= 1e-6, err
+    assert rel_err(a, b) <= 1e-9
+    st = fast.stats()
+    assert st["unconverged"] == [0, 0] and st["nonFinite"] == 0
