@@ -24,7 +24,7 @@ UNITS = {
     "kernels_fast.cu": [],
     "geometry.cu": EXACT,
     "runtime.cu": [],
-    "noalloc.cu": EXACT,
+    "peaks.cu": [],
 }
 
 

@@ -51,17 +51,50 @@ GRIM_D int bc_map(int x, int g, int N, int lo, int hi) {
   return N + g - 1;
 }
 
+// boundaries::applyBoundaryConditions (boundary.cpp:5-241): outflow and
+// mirror only; periodic directions are left as they are (the reference fills
+// them in grid::communicate at the end of each stage).  Applied direction by
+// direction over full spans, its result is the gather below.
 __global__ void k_ghost_fill(DevCfg c, double* __restrict__ prim, int nv) {
   long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (z >= c.Z) return;
   int i, j, k;
   zijk(c, z, i, j, k);
-  int si = bc_map(i, c.g1, c.N1, c.bc[0], c.bc[1]);
-  int sj = (c.dim >= 2) ? bc_map(j, c.g2, c.N2, c.bc[2], c.bc[3]) : j;
-  int sk = (c.dim >= 3) ? bc_map(k, c.g3, c.N3, c.bc[4], c.bc[5]) : k;
+  const bool p1 = c.bc[0] == GRIM_PERIODIC || c.bc[1] == GRIM_PERIODIC;
+  const bool p2 = c.bc[2] == GRIM_PERIODIC || c.bc[3] == GRIM_PERIODIC;
+  const bool p3 = c.bc[4] == GRIM_PERIODIC || c.bc[5] == GRIM_PERIODIC;
+  int si = p1 ? i : bc_map(i, c.g1, c.N1, c.bc[0], c.bc[1]);
+  int sj = (c.dim >= 2 && !p2) ? bc_map(j, c.g2, c.N2, c.bc[2], c.bc[3]) : j;
+  int sk = (c.dim >= 3 && !p3) ? bc_map(k, c.g3, c.N3, c.bc[4], c.bc[5]) : k;
   if (si == i && sj == j && sk == k) return;
   long long s = zidx(c, si, sj, sk);
   for (int v = 0; v < nv; v++) prim[(long long)v * c.Z + z] = prim[(long long)v * c.Z + s];
+}
+
+// grid::communicate (grid.cpp:306-360) with PETSc DMDA semantics: periodic
+// ghost zones (corners included) take the wrapped interior value; ghost
+// zones on a non-periodic edge come back from the never-written local
+// vector, i.e. as zero.
+__global__ void k_communicate(DevCfg c, double* __restrict__ prim, int nv) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  const bool p1 = c.bc[0] == GRIM_PERIODIC || c.bc[1] == GRIM_PERIODIC;
+  const bool p2 = c.bc[2] == GRIM_PERIODIC || c.bc[3] == GRIM_PERIODIC;
+  const bool p3 = c.bc[4] == GRIM_PERIODIC || c.bc[5] == GRIM_PERIODIC;
+  bool zero = false;
+  auto m = [&](int x, int g, int N, bool per) -> int {
+    if (x >= g && x < N + g) return x;
+    if (!per) { zero = true; return x; }
+    return g + ((x - g) % N + N) % N;
+  };
+  int si = m(i, c.g1, c.N1, p1);
+  int sj = (c.dim >= 2) ? m(j, c.g2, c.N2, p2) : j;
+  int sk = (c.dim >= 3) ? m(k, c.g3, c.N3, p3) : k;
+  if (!zero && si == i && sj == j && sk == k) return;
+  long long s = zidx(c, si, sj, sk);
+  for (int v = 0; v < nv; v++) prim[(long long)v * c.Z + z] = zero ? 0. : prim[(long long)v * c.Z + s];
 }
 
 // ---------------------------------------------------------------------------
@@ -926,6 +959,9 @@ static inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) 
 
 void ghost_fill(const DevCfg& c, double* prim, int nv, cudaStream_t s) {
   k_ghost_fill<<<nblk(c.Z, 256), 256, 0, s>>>(c, prim, nv);
+}
+void communicate(const DevCfg& c, double* prim, int nv, cudaStream_t s) {
+  k_communicate<<<nblk(c.Z, 256), 256, 0, s>>>(c, prim, nv);
 }
 
 template <int C, int V>

@@ -8,6 +8,7 @@
   namespace grim {                                                                                      \
   namespace NS {                                                                                        \
   void ghost_fill(const DevCfg& c, double* prim, int nv, cudaStream_t s);                               \
+  void communicate(const DevCfg& c, double* prim, int nv, cudaStream_t s);                              \
   void emhd_prepass(const DevCfg& c, const double* ps, const double* geoC, double* uT, cudaStream_t s); \
   void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,    \
                  double* flux, cudaStream_t s);                                                         \

@@ -223,6 +223,8 @@ static void enqueue_step(grim_handle* h, bool timed) {
   enqueue_newton(h, GRIM_HALF_STEP);
   if (timed) cudaEventRecord(h->ev[3], s);
   cudaMemcpyAsync(h->primHalf, h->prim, bytes, cudaMemcpyDeviceToDevice, s);
+  KNS_CALL(h, communicate, c, h->primHalf, c.dof, s);
+  g_launch_counter++;
   // ---- full stage
   KNS_CALL(h, ghost_fill, c, h->primHalf, c.dof, s);
   g_launch_counter++;
@@ -232,12 +234,13 @@ static void enqueue_step(grim_handle* h, bool timed) {
   enqueue_newton(h, GRIM_FULL_STEP);
   if (timed) cudaEventRecord(h->ev[6], s);
   cudaMemcpyAsync(h->primOld, h->prim, bytes, cudaMemcpyDeviceToDevice, s);
-  KNS_CALL(h, ghost_fill, c, h->primOld, c.dof, s);
+  KNS_CALL(h, communicate, c, h->primOld, c.dof, s);
   g_launch_counter++;
   grim::exact::advance_time(h->st, s);
   g_launch_counter++;
   // fullStepDiagnostics re-setting elemOld (linear_modes/problem.cpp:287)
-  if (h->cfg.elemOldFromFullStep) enqueue_dt_speeds(h, h->primOld, 1);
+  // on the communicated primOld
+  if (h->cfg.elemOldFromFullStep) enqueue_dt_speeds(h, h->primOld, 0);
   KNS_CALL(h, count_nonfinite, c, h->primOld, h->st, s);
   g_launch_counter++;
   if (timed) cudaEventRecord(h->ev[7], s);
@@ -441,6 +444,7 @@ int grim_apply_boundaries(grim_handle* h, int which) {
   double* p = pick(h, which);
   if (!p) return GRIM_EINVAL;
   CK(cudaSetDevice(h->device));
+  KNS_CALL(h, communicate, h->dc, p, h->dc.dof, h->stream);
   KNS_CALL(h, ghost_fill, h->dc, p, h->dc.dof, h->stream);
   CK(cudaGetLastError());
   return GRIM_OK;

@@ -1,0 +1,243 @@
+// torus.cuh -- the torus problem's hooks on the hot path
+// (src/problem/torus/problem.cpp): floors applied after each stage
+// (applyFloor, :542-712, with the NaN reset of fullStepDiagnostics,
+// :719-746), the radial inflow check and the polar fix applied at the start
+// of each stage (setProblemSpecificBCs, :941-1241).  The flux filter
+// (:1243-1285) is applied inside the stage epilogue.  One thread per zone;
+// each is a direct restatement of the reference's array expressions.
+#pragma once
+#include "physics.cuh"
+
+namespace grim {
+namespace GRIM_KNS {
+
+struct TorusCfg {
+  double MaxLorentzFactor, RhoFloorAmpl, UFloorAmpl, RhoFloorSlope, UFloorSlope;
+  double BsqrOverRhoMax, BsqrOverUMax;
+};
+
+template <int COND, int VISC>
+GRIM_D void load_elem(ElemT<double, double>& e, const DevCfg& c, const double* p, long long z,
+                      const ZoneGeo<double>& G) {
+  const long long Z = c.Z;
+  elem_set<COND, VISC>(e, p[z], p[Z + z], p[2 * Z + z], p[3 * Z + z], p[4 * Z + z], p[(long long)c.B1 * Z + z],
+                       p[(long long)(c.B1 + 1) * Z + z], p[(long long)(c.B1 + 2) * Z + z],
+                       COND ? p[(long long)c.Q * Z + z] : 0., VISC ? p[(long long)c.DP * Z + z] : 0., G, c);
+}
+
+// applyFloor (problem.cpp:542-712) on every zone, after the NaN reset
+template <int COND, int VISC>
+__global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, const double* __restrict__ geoC,
+                              const unsigned long long* nanFlag) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  const long long Z = c.Z;
+  ZoneGeo<double> G;
+  geo_load<double>(G, geoC, Z, z);
+  double* pv[12];
+  for (int v = 0; v < c.dof; v++) pv[v] = p + (long long)v * Z + z;
+  if (nanFlag && *nanFlag) {
+    bool bad = false;
+    for (int v = 0; v < c.dof; v++) bad |= isnan(*pv[v]);
+    if (bad)
+      for (int v = 0; v < c.dof; v++) *pv[v] = 0.;
+  }
+  const double Radius = G.x1;
+  const double minRho = pow(Radius, t.RhoFloorSlope) * t.RhoFloorAmpl;
+  const double minU = pow(Radius, t.UFloorSlope) * t.UFloorAmpl;
+  const double rho_pre = *pv[RHO] * 1., u_pre = *pv[UU] * 1.;
+  bool usefloor = false;
+  {
+    bool cd = *pv[RHO] < minRho;
+    usefloor = cd;
+    if (cd) *pv[RHO] = minRho;
+    cd = *pv[UU] < minU;
+    usefloor = usefloor || cd;
+    if (cd) *pv[UU] = minU;
+  }
+  ElemT<double, double> e;
+  load_elem<COND, VISC>(e, c, p, z, G);
+  const double bSqr1 = e.bSqr;
+  {
+    bool cd = bSqr1 > t.BsqrOverRhoMax * *pv[RHO];
+    usefloor = usefloor || cd;
+    if (cd) *pv[RHO] = bSqr1 / t.BsqrOverRhoMax;
+    cd = bSqr1 > t.BsqrOverUMax * *pv[UU];
+    usefloor = usefloor || cd;
+    if (cd) *pv[UU] = bSqr1 / t.BsqrOverUMax;
+  }
+  const double rho = *pv[RHO], u = *pv[UU];
+  double trans = fmax(fmin(1., (bSqr1 - 0.1 * rho) / rho), 0.) * (usefloor ? 1. : 0.);
+  // drift-frame velocity fix
+  const double betapar = -e.bCon[0] / bSqr1 / e.uCon[0];
+  double betasqr = betapar * betapar * bSqr1;
+  const double betasqrmax = 1. - 1. / t.MaxLorentzFactor / t.MaxLorentzFactor;
+  betasqr = fmin(betasqr, betasqrmax);
+  const double gamma = 1. / sqrt(1. - betasqr);
+  double ucondr[4];
+  for (int m = 0; m < 4; m++) ucondr[m] = gamma * (e.uCon[m] + betapar * e.bCon[m]);
+  const double Bcon[4] = {0., *pv[c.B1], *pv[c.B1 + 1], *pv[c.B1 + 2]};
+  double Bcov[4];
+  for (int m = 0; m < 4; m++) {
+    double s = 0.;
+    for (int n = 0; n < 4; n++) s += G.gcov[n][m] * Bcon[n];
+    Bcov[m] = s;
+  }
+  double udotB = 0., bSqr_fl = 0.;
+  for (int n = 0; n < 4; n++) {
+    udotB += Bcov[n] * e.uCon[n];
+    bSqr_fl += Bcov[n] * Bcon[n];
+  }
+  double bNorm = fmax(sqrt(bSqr_fl), sqrt(c.bSqrFloor));
+  const double wold = rho_pre + u_pre * c.Gam;
+  const double QdotB = udotB * wold * e.uCon[0];
+  const double wnew = rho + u * c.Gam;
+  const double x = 2. * QdotB / (bNorm * wnew * ucondr[0]);
+  const double vpar = x / (ucondr[0] * (1. + sqrt(1. + x * x)));
+  const double inv_ut = 1. / ucondr[0];
+  double vcon[4];
+  vcon[0] = 0. + 1.;
+  for (int m = 1; m < 4; m++) vcon[m] = vpar * Bcon[m] / bNorm + ucondr[m] * inv_ut;
+  double vsqr = 0.;
+  for (int m = 0; m < 4; m++)
+    for (int n = 0; n < 4; n++) vsqr += G.gcov[m][n] * vcon[m] * vcon[n];
+  if (vsqr >= 0. || vsqr < 1. / G.gcon[0][0]) vsqr = 1. / G.gcon[0][0];
+  const double ut = sqrt(-1. / vsqr);
+  for (int m = 1; m < 4; m++) {
+    double utcon = ut * (vcon[m] - G.gcon[0][m] / G.gcon[0][0]);
+    *pv[UU + m] = *pv[UU + m] * (1. - trans) + trans * utcon;
+  }
+  // maximum Lorentz factor
+  load_elem<COND, VISC>(e, c, p, z, G);
+  {
+    const double lf2 = e.gam * e.gam;
+    const double gm2 = t.MaxLorentzFactor * t.MaxLorentzFactor;
+    if (lf2 > gm2) {
+      double mf = 1. / sqrt(fmax((lf2 - 1.) / (gm2 - 1.), 1.));
+      *pv[U1] *= mf;
+      *pv[U2] *= mf;
+      *pv[U3] *= mf;
+    }
+  }
+  if (COND || VISC) {
+    load_elem<COND, VISC>(e, c, p, z, G);
+    if (COND) {
+      const double cs = e.soundSpeed;
+      const double Qmax = 1.07 * c.CondClosure * *pv[RHO] * pow(cs, 3.);
+      const double lim = fmax(fabs(e.q) / Qmax, 1.);
+      *pv[c.Q] = *pv[c.Q] / lim;
+    }
+    if (VISC) {
+      const double pr = e.pressure, dP = e.deltaP, bs = e.bSqr;
+      const double dPmod = fmax(pr - 2. / 3. * dP, 0.01 * c.bSqrFloor) / fmax(pr + 1. / 3. * dP, c.bSqrFloor);
+      const double dPmaxPlus = fmin(1.07 * c.ViscClosure * bs * 0.5 * dPmod, 1.49 * pr);
+      const double dPmaxMinus = fmax(-1.07 * c.ViscClosure * bs, -2.99 * pr);
+      const double f = (dP > 0.) ? 1. / fmax(dP / dPmaxPlus, 1.) : 1. / fmax(dP / dPmaxMinus, 1.);
+      *pv[c.DP] = *pv[c.DP] * f;
+    }
+  }
+}
+
+// NaN count over the interior (fullStepDiagnostics, problem.cpp:725-733)
+__global__ void k_nan_flag(DevCfg c, const double* __restrict__ p, unsigned long long* flag) {
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int bad = 0;
+  if (n < c.Zint) {
+    long long z = interior_to_z(c, n);
+    for (int v = 0; v < c.dof; v++) bad |= isnan(p[(long long)v * c.Z + z]) ? 1 : 0;
+  }
+  bad = __syncthreads_count(bad);
+  if (threadIdx.x == 0 && bad) atomicAdd(flag, (unsigned long long)bad);
+}
+
+// inflowCheck (problem.cpp:941-1044) on the X1 ghost zones
+template <int COND, int VISC>
+__global__ void k_torus_inflow(DevCfg c, TorusCfg t, double* __restrict__ p, const double* __restrict__ geoC) {
+  // one thread per (ghost i, j, k); 2*ng columns of X1 ghosts
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long cols = (long long)2 * c.ng * c.N2T * c.N3T;
+  if (n >= cols) return;
+  const int gi = (int)(n % (2 * c.ng));
+  const long long r = n / (2 * c.ng);
+  const int j = (int)(r % c.N2T), k = (int)(r / c.N2T);
+  const bool right = gi >= c.ng;
+  const int i = right ? (c.N1 + c.ng + (gi - c.ng)) : gi;
+  const long long Z = c.Z;
+  const long long z = zidx(c, i, j, k);
+  ZoneGeo<double> G;
+  geo_load<double>(G, geoC, Z, z);
+  ElemT<double, double> e;
+  load_elem<COND, VISC>(e, c, p, z, G);
+  double* u1 = p + (long long)U1 * Z + z;
+  double* u2 = p + (long long)U2 * Z + z;
+  double* u3 = p + (long long)U3 * Z + z;
+  *u1 = *u1 / e.gam;
+  *u2 = *u2 / e.gam;
+  *u3 = *u3 / e.gam;
+  if (right) {
+    // the last active zone's g^{01} alpha, copied into the ghost columns
+    const long long ze = zidx(c, c.N1 + c.ng - 1, j, k);
+    const double minUr = __ldg(geoC + 17LL * Z + ze) * __ldg(geoC + 33LL * Z + ze);
+    *u1 = fmax(minUr, *u1);
+  } else {
+    *u1 = fmin(G.gcon[0][1] * G.alpha, *u1);
+  }
+  const double U[3] = {*u1, *u2, *u3};
+  double vSqr = 0.;
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) vSqr += G.gcov[a + 1][b + 1] * U[a] * U[b];
+  const double vSqrMax = 1. - 1. / t.MaxLorentzFactor / t.MaxLorentzFactor;
+  vSqr = fmax(fmin(vSqr, vSqrMax), 1.e-13);
+  const double lf = 1. / sqrt(1. - vSqr);
+  *u1 = *u1 * lf;
+  *u2 = *u2 * lf;
+  *u3 = *u3 * lf;
+}
+
+// fixPoles (problem.cpp:1046-1215): one thread per (i, k) column and pole
+__global__ void k_torus_poles(DevCfg c, double* __restrict__ p, const double* __restrict__ geoC) {
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long cols = (long long)c.N1T * c.N3T;
+  if (n >= 2 * cols) return;
+  const bool top = n >= cols;
+  const long long m = top ? n - cols : n;
+  const int i = (int)(m % c.N1T), k = (int)(m / c.N1T);
+  const long long Z = c.Z;
+  const int ng = c.ng;
+  auto at = [&](int v, int j) -> double& { return p[(long long)v * Z + zidx(c, i, j, k)]; };
+  auto theta = [&](int j) -> double {
+    double th = __ldg(geoC + 35LL * Z + zidx(c, i, j, k));
+    return top ? th * (-1.) + M_PI : th;
+  };
+  const int idx0 = top ? c.N2 + ng - 1 : ng;
+  const int idx1 = top ? idx0 - 1 : ng + 1;
+  const int idx2 = top ? idx0 - 2 : ng + 2;
+  const int sgnIdx[2] = {idx0, idx1};
+  for (int q = 0; q < 2; q++) {
+    const int jj = sgnIdx[q];
+    at(RHO, jj) = at(RHO, idx2);
+    at(UU, jj) = at(UU, idx2);
+    at(U1, jj) = at(U1, idx2);
+    at(U2, jj) = at(U2, idx2) * theta(jj) / theta(idx2);
+    at(U3, jj) = at(U3, idx2);
+    if (c.conduction) at(c.Q, jj) = at(c.Q, idx2) * theta(jj) / theta(idx2);
+    if (c.viscosity) at(c.DP, jj) = at(c.DP, idx2) * theta(jj) / theta(idx2);
+  }
+  for (int g = 0; g < ng; g++) {
+    const int dst = top ? c.N2 + ng + g : ng - 1 - g;
+    const int src = top ? c.N2 + ng - 1 - g : ng + g;
+    at(RHO, dst) = at(RHO, src);
+    at(UU, dst) = at(UU, src);
+    at(U1, dst) = at(U1, src);
+    at(U3, dst) = at(U3, src);
+    at(U2, dst) = at(U2, src) * (-1.0);
+    at(c.B1, dst) = at(c.B1, src);
+    at(c.B1 + 2, dst) = at(c.B1 + 2, src);
+    at(c.B1 + 1, dst) = at(c.B1 + 1, src) * (-1.0);
+    if (c.conduction) at(c.Q, dst) = at(c.Q, src) * (-1.0);
+    if (c.viscosity) at(c.DP, dst) = at(c.DP, src) * (-1.0);
+  }
+}
+
+}  // namespace GRIM_KNS
+}  // namespace grim

@@ -187,6 +187,11 @@ int grim_synchronize(grim_handle* h);
 /* the handle's cudaStream_t, as void* */
 void* grim_stream(grim_handle* h);
 
+/* ---- self-tests (extends timeStepper::bandwidthTest, timestepper.cpp:473-526):
+ *      FP64 and FP32 FMA throughput (TFLOP/s, 2 flops per FMA) and HBM copy
+ *      bandwidth (GB/s, read + write) of a device; any pointer may be NULL */
+int grim_measure_peaks(int device, double* fp64_tflops, double* fp32_tflops, double* hbm_gbs);
+
 #ifdef __cplusplus
 }
 #endif

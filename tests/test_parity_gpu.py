@@ -139,7 +139,12 @@ def test_timestep_parity_fast_mode_128():
     g = interior(cfg, ts.primOld.getVars())
     o = interior(cfg, orc.get_prims())
     assert abs(ts.time - orc.time) <= 1e-15 * orc.time
-    assert rel_err(g, o, 1e-300) <= 1e-12
+    # rho and u pointwise; the velocity and field perturbations oscillate
+    # around zero, so relative to each variable's scale
+    assert rel_err(g[:2], o[:2]) <= 1e-12
+    assert scaled_err(g, o) <= 1e-12
+    bitwise = float(np.mean(g == o))
+    assert bitwise > 0.99, bitwise
 
 
 def test_timestep_parity_emhd_linear_mode():
@@ -219,31 +224,45 @@ def test_graph_replay_is_bitwise_identical():
 
 
 @pytest.mark.parametrize("case", ["fast_mode", "linear_modes"])
-def test_tangent_jacobian_matches_fd(case):
+def test_tangent_jacobian_matches_central_fd(case):
+    """The forward-tangent Jacobian against a central difference of the FP64
+    residual with an absolute step h_j = 1e-6 max(|P_j|, 1e-2): error
+    O(h^2) + roundoff/h, i.e. <= 1e-6 of each column's scale.  (The
+    reference's one-sided FD with relative eps = 4e-8 is itself off by up to
+    ~1e-3 on columns of primitives of size 1e-5, so it is not the check.)"""
     if case == "fast_mode":
         cfg = PR.fast_mode_config(N=16)
         P = PR.fast_mode_prims(cfg)
     else:
         cfg = PR.linear_modes_config(N=16)
         P = PR.linear_modes_prims(cfg, amplitude=1e-4)
-    ts, orc = pair(cfg)
+    from grim_b200.timestepper import timeStepper
+    ts = timeStepper(cfg)
     ts.primOld.setVars(P)
     ts.stageSetup(C.HALF_STEP)
     guess = ts.prim.getVars()
     Jt = ts.jacobianTangent(guess)
-    Jf = ts.jacobianFD(guess)
+    nf = C.var_counts(cfg)[1]
     s3, s2, s1 = C.interior_slices(cfg)
-    a, b = Jt[s3, s2, s1], Jf[s3, s2, s1]
-    scale = np.max(np.abs(a), axis=(0, 1, 2, 3)) + 1e-300
-    assert float(np.max(np.abs(a - b) / scale)) <= 1e-6
+    for j in range(nf):
+        h = 1e-6 * np.maximum(np.abs(guess[j]), 1e-2)
+        gp, gm = guess.copy(), guess.copy()
+        gp[j] += h
+        gm[j] -= h
+        col = (ts.computeResidual(gp) - ts.computeResidual(gm)) / (2 * h)
+        a = Jt[s3, s2, s1][..., :, j]
+        b = np.moveaxis(col[:, s3, s2, s1], 0, -1)
+        scale = np.max(np.abs(b)) + 1e-300
+        assert float(np.max(np.abs(a - b))) <= 1e-6 * scale, (j, float(np.max(np.abs(a - b))), scale)
 
 
 @pytest.mark.parametrize("mode", [C.NEWTON_TANGENT64, C.NEWTON_MIXED32])
 def test_fast_newton_error_bound(mode):
     """Tangent / mixed-precision Newton with per-zone convergence at
-    relative residual 1e-10 against the FD64 parity path at the same
-    tolerance: primitives agree within 1e-9 relative after 10 steps."""
-    cfg = PR.fast_mode_config(N=64, nonlinearsolve_rtol=1e-10, nonlinearsolve_atol=0.0,
+    relative residual 1e-10 (absolute floor |R| <= 1e-13, the roundoff of
+    the residual here) against the FD64 parity path at the same tolerance:
+    primitives agree within 1e-9 relative after 10 steps."""
+    cfg = PR.fast_mode_config(N=64, nonlinearsolve_rtol=1e-10, nonlinearsolve_atol=1e-26,
                               maxNonLinearIter=6)
     P = PR.fast_mode_prims(cfg)
     from grim_b200.timestepper import timeStepper
