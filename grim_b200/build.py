@@ -25,6 +25,7 @@ UNITS = {
     "geometry.cu": EXACT,
     "runtime.cu": [],
     "peaks.cu": [],
+    "noalloc.cu": EXACT,
 }
 
 

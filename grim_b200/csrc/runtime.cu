@@ -742,3 +742,10 @@ int grim_synchronize(grim_handle* h) {
 void* grim_stream(grim_handle* h) { return h ? (void*)h->stream : nullptr; }
 
 }  // extern "C"
+
+// Configuration translation for entry points that live outside this file
+// (the allocation-free divergence in noalloc.cu); same checks as grim_create.
+namespace grim {
+int devcfg_from_config(const grim_config& c, DevCfg& d) { return make_devcfg(c, d); }
+void set_error_message(const char* msg) { set_err("%s", msg); }
+}  // namespace grim

@@ -192,6 +192,19 @@ void* grim_stream(grim_handle* h);
  *      bandwidth (GB/s, read + write) of a device; any pointer may be NULL */
 int grim_measure_peaks(int device, double* fp64_tflops, double* fp32_tflops, double* hbm_gbs);
 
+/* ---- allocation-free divergence.  No counterpart in the reference: for
+ *      callers that cannot call cudaMalloc (their device memory is owned by
+ *      their own pool allocator, or they call in the middle of asynchronous
+ *      work).  Same result as grim_compute_div_fluxes (interior zones of a
+ *      dof x Z divF), on device pointers, enqueued on `stream` (a
+ *      cudaStream_t, NULL = default stream) of the current device.  All
+ *      scratch lives in one static 64 MiB device array per GPU that loads the
+ *      library; grids needing more are rejected with GRIM_EINVAL.  Minkowski
+ *      metric only.  The first call on a device looks up that array's address
+ *      (make it before any stream capture); calls that overlap on the GPU
+ *      share the array and race. */
+int grim_div_fluxes_noalloc(const grim_config* cfg, const double* prim, double* divF, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
