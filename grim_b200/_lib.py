@@ -85,6 +85,9 @@ def lib():
         "grim_get_stats": [vp, P(GrimStats)],
         "grim_enable_graph": [vp, i],
         "grim_synchronize": [vp],
+        "grim_problem_init": [vp],
+        "grim_get_newton_histogram": [vp, P(ctypes.c_longlong)],
+        "grim_measure_peaks": [i, P(d), P(d), P(d)],
     }
     for name, args in sig.items():
         f = getattr(L, name)

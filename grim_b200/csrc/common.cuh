@@ -33,6 +33,8 @@ struct DevCfg {
   double theta;
   double atol, rtol, jacEps, lsFloor;
   double tau0, tau1;
+  // torus floors (problem hook)
+  double maxLF, rhoFloorAmpl, uFloorAmpl, rhoFloorSlope, uFloorSlope, bsqOverRhoMax, bsqOverUMax;
 };
 
 GRIM_HD long long zidx(const DevCfg& c, int i, int j, int k) {

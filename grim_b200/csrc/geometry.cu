@@ -2,8 +2,9 @@
 // symbols per zone and location, computed once at handle creation
 // (src/geometry/geometry.cpp:4-680, CoordinateChangeFunctionsArray.hpp).
 //
-// Stored layout per location: 36 x Z doubles, SoA:
-//   [0,16) gCov[mu][nu], [16,32) gCon[mu][nu], 32 g, 33 alpha, 34 x1, 35 x2
+// Stored layout per location: 39 x Z doubles, SoA:
+//   [0,16) gCov[mu][nu], [16,32) gCon[mu][nu], 32 g, 33 alpha, 34 x1, 35 x2,
+//   36 x1^1.5, 37 RhoFloorAmpl x1^RhoFloorSlope, 38 UFloorAmpl x1^UFloorSlope
 // and for the zone centre 64 x Z Christoffels gammaUpDownDown[mu][nu][la].
 // Compiled without FMA contraction like the parity kernels.
 #include "common.cuh"
@@ -13,6 +14,7 @@ namespace grim {
 struct GeoParams {
   int metric, derefine, cylindrify;
   double a, hSlope, X1Start, X1cyl, X2cyl;
+  double rhoFloorAmpl, rhoFloorSlope, uFloorAmpl, uFloorSlope;
 };
 
 // CoordinateChangeFunctionsArray.hpp:4-16
@@ -218,6 +220,10 @@ __global__ void k_geometry(DevCfg c, GeoParams p, double o1, double o2, double* 
   out[33LL * Z + z] = 1. / sqrt(-C[0][0]);
   out[34LL * Z + z] = x[0];
   out[35LL * Z + z] = x[1];
+  // torus/problem.cpp:7-13 (dynamical time) and :547-548 (floors)
+  out[36LL * Z + z] = pow(x[0], 1.5);
+  out[37LL * Z + z] = pow(x[0], p.rhoFloorSlope) * p.rhoFloorAmpl;
+  out[38LL * Z + z] = pow(x[0], p.uFloorSlope) * p.uFloorAmpl;
   if (gamma) {
     // computeConnectionCoeffs (geometry.cpp:61-119, 631-680), eps = 1e-5
     const double eps = 1.e-5;
@@ -256,6 +262,10 @@ void launch_geometry(const DevCfg& c, const grim_config& cfg, int location, doub
   p.X1Start = cfg.X1Start;
   p.X1cyl = cfg.X1cyl;
   p.X2cyl = cfg.X2cyl;
+  p.rhoFloorAmpl = cfg.RhoFloorAmpl;
+  p.rhoFloorSlope = cfg.RhoFloorSlope;
+  p.uFloorAmpl = cfg.UFloorAmpl;
+  p.uFloorSlope = cfg.UFloorSlope;
   double o1 = 0.5, o2 = 0.5;
   if (location == GRIM_LEFT) o1 = 0.;
   else if (location == GRIM_RIGHT) o1 = 1.;

@@ -16,12 +16,21 @@
 //   k_dt_speeds        max over zones of sum_d c_max,d / dX_d (computeDt)
 //   k_newton_*         per-zone Newton (solve.cpp / residual.cpp)
 #pragma once
+#include <algorithm>
+
 #include "physics.cuh"
 #include "recon.cuh"
 #include "stage.cuh"
+#include "torus.cuh"
 
 namespace grim {
 namespace GRIM_KNS {
+
+#ifdef GRIM_FAST_MATH
+constexpr bool kFastMath = true;   // reassociated arithmetic allowed (fast path)
+#else
+constexpr bool kFastMath = false;  // the reference's operation order (parity path)
+#endif
 
 GRIM_D double zone_x1(const DevCfg& c, int i, double o) { return c.X1Start + ((double)(i - c.g1) + o) * c.dX[0]; }
 GRIM_D double zone_x2(const DevCfg& c, int j, double o) { return c.X2Start + ((double)(j - c.g2) + o) * c.dX[1]; }
@@ -120,49 +129,34 @@ __global__ void k_emhd_prepass(DevCfg c, const double* __restrict__ ps, const do
 }
 
 // ---------------------------------------------------------------------------
-// face fluxes: thread z computes the flux through the face z - 1/2 along
-// `dir` (riemannsolver.cpp:202-328 after its shift).
+// face fluxes (riemannsolver.cpp:202-328 after its shift): the flux through
+// the face z - 1/2 along `dir` from the left state (right face value of zone
+// z - s) and the right state (left face value of zone z).  Every zone is
+// reconstructed once: X1 faces share a warp's reconstructions through
+// shuffles (31 faces per warp), X2 / X3 faces are swept by threads that
+// march along the face direction and keep the previous zone's right-face
+// state in registers.
 // ---------------------------------------------------------------------------
-template <int COND, int VISC>
-__global__ void __launch_bounds__(128) k_face_flux(DevCfg c, int dir, const double* __restrict__ ps,
-                                                            const double* __restrict__ geoF,
-                                                            const double* __restrict__ geoC,
-                                                            double* __restrict__ flux) {
-  constexpr int NF = 5 + COND + VISC;
-  constexpr int DOF = NF + 3;
-  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (z >= c.Z) return;
-  int i, j, k;
-  zijk(c, z, i, j, k);
-  const int x = (dir == 0) ? i : (dir == 1 ? j : k);
-  const int NT = (dir == 0) ? c.N1T : (dir == 1 ? c.N2T : c.N3T);
-  if (x < 3 || x > NT - 3) return;
-  const long long s = stride_of(c, dir);
-  const long long Z = c.Z;
-  // left state: right face of zone z-s; right state: left face of zone z
-  double pl[DOF], pr[DOF];
+template <int DOF>
+GRIM_D void recon_zone(const DevCfg& c, const double* __restrict__ ps, long long z, long long s, int scheme,
+                       double* lo, double* ro) {
 #pragma unroll
   for (int v = 0; v < DOF; v++) {
-    const double* a = ps + (long long)v * Z + z;
-    double y[6];
-#pragma unroll
-    for (int m = 0; m < 6; m++) y[m] = __ldg(a + (m - 3) * s);
-    double lo, ro;
-    recon_faces(c.reconstruction, c.theta, y[0], y[1], y[2], y[3], y[4], lo, ro);
-    pl[v] = ro;
-    recon_faces(c.reconstruction, c.theta, y[1], y[2], y[3], y[4], y[5], lo, ro);
-    pr[v] = lo;
+    const double* a = ps + (long long)v * c.Z + z;
+    const double y0 = __ldg(a - 2 * s), y1 = __ldg(a - s), y2 = __ldg(a), y3 = __ldg(a + s), y4 = __ldg(a + 2 * s);
+    if (kFastMath)
+      recon_faces_fast(scheme, c.theta, y0, y1, y2, y3, y4, lo[v], ro[v]);
+    else
+      recon_faces(scheme, c.theta, y0, y1, y2, y3, y4, lo[v], ro[v]);
   }
-  ZoneGeo<double> GL, GR;
-  if (dir == 2) {
-    // X3 faces use the centre geometry of each side (fvmfluxes.cpp:150-151)
-    load_geo(GL, c, geoC, z - s, i, j, 0.5, 0.5);
-    load_geo(GR, c, geoC, z, i, j, 0.5, 0.5);
-  } else {
-    const double o1 = (dir == 0) ? 0. : 0.5, o2 = (dir == 1) ? 0. : 0.5;
-    load_geo(GL, c, geoF, z, i, j, o1, o2);
-    GR = GL;
-  }
+}
+
+template <int COND, int VISC>
+GRIM_D void riemann_face(const DevCfg& c, int dir, const double* pl, const double* pr, const ZoneGeo<double>& GL,
+                         const ZoneGeo<double>& GR, double* __restrict__ flux, long long z) {
+  constexpr int NF = 5 + COND + VISC;
+  constexpr int DOF = NF + 3;
+  const long long Z = c.Z;
   const int fd = dir + 1;
   double FL[DOF], UL[DOF], FR[DOF], UR[DOF];
   double minL, maxL, minR, maxR;
@@ -196,6 +190,72 @@ __global__ void __launch_bounds__(128) k_face_flux(DevCfg c, int dir, const doub
     const double cm = fmax(cmax, -cmin);
 #pragma unroll
     for (int v = 0; v < DOF; v++) flux[(long long)v * Z + z] = 0.5 * (FL[v] + FR[v] - cm * (UR[v] - UL[v]));
+  }
+}
+
+// X1 faces: warp w of a row covers faces i0 .. i0+30; lane l reconstructs
+// zone i0 - 1 + l and, for l >= 1, computes the face between zones
+// i0 - 2 + l and i0 - 1 + l with the left state shuffled from lane l - 1.
+template <int COND, int VISC>
+__global__ void __launch_bounds__(128) k_face_flux_x1(DevCfg c, const double* __restrict__ ps,
+                                                      const double* __restrict__ geoF, double* __restrict__ flux) {
+  constexpr int DOF = 8 + COND + VISC;
+  const int lane = threadIdx.x & 31;
+  const long long wg = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nfaces = c.N1T - 5;  // faces i = 3 .. N1T-3
+  const int wpr = (nfaces + 30) / 31;
+  const long long rows = (long long)c.N2T * c.N3T;
+  if (wg >= rows * wpr) return;  // whole warps exit together
+  const long long row = wg / wpr;
+  const int i0 = 3 + (int)(wg % wpr) * 31;
+  const int iz = i0 - 1 + lane;
+  const int j = (int)(row % c.N2T), k = (int)(row / c.N2T);
+  const bool reconOK = iz >= 2 && iz <= c.N1T - 3;
+  double lo[DOF], ro[DOF];
+  const long long z = zidx(c, reconOK ? iz : 2, j, k);
+  recon_zone<DOF>(c, ps, z, 1, c.reconstruction, lo, ro);
+  double pl[DOF];
+#pragma unroll
+  for (int v = 0; v < DOF; v++) pl[v] = __shfl_up_sync(0xffffffffu, ro[v], 1);
+  if (lane == 0 || iz > c.N1T - 3) return;
+  ZoneGeo<double> G;
+  load_geo(G, c, geoF, z, iz, j, 0., 0.5);
+  riemann_face<COND, VISC>(c, 0, pl, lo, G, G, flux, z);
+}
+
+// X2 / X3 faces: thread (i, slab) marches `span` faces along dir
+template <int COND, int VISC>
+__global__ void __launch_bounds__(128) k_face_flux_march(DevCfg c, int dir, int span, const double* __restrict__ ps,
+                                                         const double* __restrict__ geoF,
+                                                         const double* __restrict__ geoC, double* __restrict__ flux) {
+  constexpr int DOF = 8 + COND + VISC;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= c.N1T) return;
+  const int NT = (dir == 1) ? c.N2T : c.N3T;
+  const int other = blockIdx.z;  // k for X2 faces, j for X3 faces
+  const int f0 = 3 + blockIdx.y * span;
+  const int f1 = min(f0 + span, NT - 2);  // faces f0 .. f1-1 (<= NT-3)
+  if (f0 >= f1) return;
+  const long long s = stride_of(c, dir);
+  auto zof = [&](int x) -> long long { return dir == 1 ? zidx(c, i, x, other) : zidx(c, i, other, x); };
+  double lo[DOF], ro[DOF], pl[DOF];
+  recon_zone<DOF>(c, ps, zof(f0 - 1), s, c.reconstruction, lo, pl);
+  for (int x = f0; x < f1; x++) {
+    const long long z = zof(x);
+    recon_zone<DOF>(c, ps, z, s, c.reconstruction, lo, ro);
+    ZoneGeo<double> GL, GR;
+    const int jj = (dir == 1) ? x : other;
+    if (dir == 2) {
+      // X3 faces use the centre geometry of each side (fvmfluxes.cpp:150-151)
+      load_geo(GL, c, geoC, z - s, i, jj, 0.5, 0.5);
+      load_geo(GR, c, geoC, z, i, jj, 0.5, 0.5);
+    } else {
+      load_geo(GL, c, geoF, z, i, jj, 0.5, 0.);
+      GR = GL;
+    }
+    riemann_face<COND, VISC>(c, dir, pl, lo, GL, GR, flux, z);
+#pragma unroll
+    for (int v = 0; v < DOF; v++) pl[v] = ro[v];
   }
 }
 
@@ -236,36 +296,29 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
   f.F[0] = b.flux[0]; f.F[1] = b.flux[1]; f.F[2] = b.flux[2]; f.Z = Z; f.B1 = c.B1;
   const double dt = b.st->dt;
 
-  // ---- divergence of the fluid rows
-  double div[NF + 3];
-  const double i1 = 1. / c.dX[0], i2 = 1. / c.dX[1];
-  for (int v = 0; v < NF; v++) {
-    if (c.dim <= 2) {
-      double d = f.at(0, v, z + s1) * i1 + f.at(0, v, z) * (-i1);
-      if (c.dim == 2) d = d + (f.at(1, v, z + s2) * i2 + f.at(1, v, z) * (-i2));
-      div[v] = d;
-    } else {
-      div[v] = (f.at(0, v, z + s1) - f.at(0, v, z)) / c.dX[0] + (f.at(1, v, z + s2) - f.at(1, v, z)) / c.dX[1] +
-               (f.at(2, v, z + s3) - f.at(2, v, z)) / c.dX[2];
-    }
-  }
-  // ---- flux-CT B fluxes on the zone's faces, then their divergence
+  // ---- fluxes on the zone's six faces: Riemann fluxes for the fluid rows,
+  // flux-CT values for the field rows (constrainedtransport.cpp:3-51)
+  constexpr int DOF = NF + 3;
+  double Fl[3][DOF], Fr[3][DOF];
+  const long long sd[3] = {s1, s2, s3};
+  for (int d = 0; d < 3; d++)
+    for (int v = 0; v < DOF; v++) { Fl[d][v] = 0.; Fr[d][v] = 0.; }
+  for (int d = 0; d < c.dim; d++)
+    for (int v = 0; v < NF; v++) { Fl[d][v] = f.at(d, v, z); Fr[d][v] = f.at(d, v, z + sd[d]); }
   if (c.dim == 1) {
-    for (int b3 = 0; b3 < 3; b3++) {
-      const int v = c.B1 + b3;
-      div[NF + b3] = f.at(0, v, z + s1) * i1 + f.at(0, v, z) * (-i1);
-    }
+    for (int b3 = 0; b3 < 3; b3++) { Fl[0][NF + b3] = f.at(0, c.B1 + b3, z); Fr[0][NF + b3] = f.at(0, c.B1 + b3, z + s1); }
   } else if (c.dim == 2) {
     const double e00 = emf3(f, z, s1, s2), e10 = emf3(f, z + s1, s1, s2);
     const double e01 = emf3(f, z + s2, s1, s2), e11 = emf3(f, z + s1 + s2, s1, s2);
     // F1: B1 -> 0, B2 -> 0.5 (emf3 + emf3[j+1]); F2: B1 -> -0.5 (emf3 + emf3[i+1]), B2 -> 0
-    const double F1B2_l = 0.5 * (e00 + e01), F1B2_r = 0.5 * (e10 + e11);
-    const double F2B1_b = -0.5 * (e00 + e10), F2B1_t = -0.5 * (e01 + e11);
-    const double zero = 0.;
-    div[NF + 0] = (zero * i1 + zero * (-i1)) + (F2B1_t * i2 + F2B1_b * (-i2));
-    div[NF + 1] = (F1B2_r * i1 + F1B2_l * (-i1)) + (zero * i2 + zero * (-i2));
-    const int v = c.B1 + 2;
-    div[NF + 2] = (f.at(0, v, z + s1) * i1 + f.at(0, v, z) * (-i1)) + (f.at(1, v, z + s2) * i2 + f.at(1, v, z) * (-i2));
+    Fl[0][NF + 1] = 0.5 * (e00 + e01);
+    Fr[0][NF + 1] = 0.5 * (e10 + e11);
+    Fl[1][NF + 0] = -0.5 * (e00 + e10);
+    Fr[1][NF + 0] = -0.5 * (e01 + e11);
+    Fl[0][NF + 2] = f.at(0, c.B1 + 2, z);
+    Fr[0][NF + 2] = f.at(0, c.B1 + 2, z + s1);
+    Fl[1][NF + 2] = f.at(1, c.B1 + 2, z);
+    Fr[1][NF + 2] = f.at(1, c.B1 + 2, z + s2);
   } else {
     // EMF3 at (i|i+1, j|j+1), EMF2 at (i|i+1, k|k+1), EMF1 at (j|j+1, k|k+1)
     const double a00 = emf3(f, z, s1, s2), a10 = emf3(f, z + s1, s1, s2);
@@ -274,18 +327,36 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
     const double b01 = emf2(f, z + s3, s1, s3), b11 = emf2(f, z + s1 + s3, s1, s3);
     const double c00 = emf1(f, z, s2, s3), c10 = emf1(f, z + s2, s2, s3);
     const double c01 = emf1(f, z + s3, s2, s3), c11 = emf1(f, z + s2 + s3, s2, s3);
-    const double F1B1_l = 0., F1B1_r = 0.;
-    const double F1B2_l = 0.5 * (a00 + a01), F1B2_r = 0.5 * (a10 + a11);
-    const double F1B3_l = -0.5 * (b00 + b01), F1B3_r = -0.5 * (b10 + b11);
-    const double F2B1_l = -0.5 * (a00 + a10), F2B1_r = -0.5 * (a01 + a11);
-    const double F2B2_l = 0., F2B2_r = 0.;
-    const double F2B3_l = 0.5 * (c00 + c01), F2B3_r = 0.5 * (c10 + c11);
-    const double F3B1_l = 0.5 * (b00 + b10), F3B1_r = 0.5 * (b01 + b11);
-    const double F3B2_l = -0.5 * (c00 + c10), F3B2_r = -0.5 * (c01 + c11);
-    const double F3B3_l = 0., F3B3_r = 0.;
-    div[NF + 0] = (F1B1_r - F1B1_l) / c.dX[0] + (F2B1_r - F2B1_l) / c.dX[1] + (F3B1_r - F3B1_l) / c.dX[2];
-    div[NF + 1] = (F1B2_r - F1B2_l) / c.dX[0] + (F2B2_r - F2B2_l) / c.dX[1] + (F3B2_r - F3B2_l) / c.dX[2];
-    div[NF + 2] = (F1B3_r - F1B3_l) / c.dX[0] + (F2B3_r - F2B3_l) / c.dX[1] + (F3B3_r - F3B3_l) / c.dX[2];
+    Fl[0][NF + 1] = 0.5 * (a00 + a01);  Fr[0][NF + 1] = 0.5 * (a10 + a11);
+    Fl[0][NF + 2] = -0.5 * (b00 + b01); Fr[0][NF + 2] = -0.5 * (b10 + b11);
+    Fl[1][NF + 0] = -0.5 * (a00 + a10); Fr[1][NF + 0] = -0.5 * (a01 + a11);
+    Fl[1][NF + 2] = 0.5 * (c00 + c01);  Fr[1][NF + 2] = 0.5 * (c10 + c11);
+    Fl[2][NF + 0] = 0.5 * (b00 + b10);  Fr[2][NF + 0] = 0.5 * (b01 + b11);
+    Fl[2][NF + 1] = -0.5 * (c00 + c10); Fr[2][NF + 1] = -0.5 * (c01 + c11);
+  }
+  if (c.problem == GRIM_PROBLEM_TORUS) {
+    // applyProblemSpecificFluxFilter (torus/problem.cpp:1243-1285)
+    if (i == c.g1) Fl[0][RHO] = fmin(Fl[0][RHO], 0.);
+    if (i == c.N1 + c.g1 - 1) Fr[0][RHO] = fmax(Fr[0][RHO], 0.);
+    if (c.dim >= 2) {
+      if (j == c.g2)
+        for (int v = 0; v < DOF; v++) Fl[1][v] = 0.;
+      if (j == c.N2 + c.g2 - 1)
+        for (int v = 0; v < DOF; v++) Fr[1][v] = 0.;
+    }
+  }
+  // ---- divergence (fvmfluxes.cpp): zero-padded convolution in 1D/2D,
+  // shifted difference in 3D
+  double div[DOF];
+  const double i1 = 1. / c.dX[0], i2 = 1. / c.dX[1];
+  for (int v = 0; v < DOF; v++) {
+    if (c.dim <= 2) {
+      double d = Fr[0][v] * i1 + Fl[0][v] * (-i1);
+      if (c.dim == 2) d = d + (Fr[1][v] * i2 + Fl[1][v] * (-i2));
+      div[v] = d;
+    } else {
+      div[v] = (Fr[0][v] - Fl[0][v]) / c.dX[0] + (Fr[1][v] - Fl[1][v]) / c.dX[1] + (Fr[2][v] - Fl[2][v]) / c.dX[2];
+    }
   }
 
   // ---- stage element at the centre (elemOld / elemHalfStep)
@@ -722,7 +793,7 @@ __global__ void __launch_bounds__(128) k_newton_fast(DevCfg c, int stage, StageB
     for (int m = 0; m < 4; m++)
 #pragma unroll
       for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = (T)G.gcov[m][q]; Gt.gcon[m][q] = (T)G.gcon[m][q]; }
-    Gt.g = (T)G.g; Gt.alpha = (T)G.alpha; Gt.x1 = (T)G.x1; Gt.x2 = (T)G.x2;
+    Gt.g = (T)G.g; Gt.alpha = (T)G.alpha; Gt.x1 = (T)G.x1; Gt.x2 = (T)G.x2; Gt.dyn = (T)G.dyn;
     StageConst<NF> K;
     load_stage_const<COND, VISC>(K, c, stage, b, z, G);
     double P[NF], R[NF];
@@ -774,6 +845,7 @@ __global__ void __launch_bounds__(128) k_newton_fast(DevCfg c, int stage, StageB
       if (!(l2 >= 0. && l2 <= fmax(c.atol, c.rtol * c.rtol * l2first))) unconv = 1;
     }
     itsMax = it;
+    atomicAdd(&b.st->itHist[stage][min(it, 15)], 1ULL);
     for (int v = 0; v < NF; v++) b.prim[(long long)v * Z + z] = P[v];
   }
   unconv = __syncthreads_count(unconv);
@@ -781,6 +853,134 @@ __global__ void __launch_bounds__(128) k_newton_fast(DevCfg c, int stage, StageB
   for (int o = 16; o > 0; o >>= 1) itsMax = max(itsMax, __shfl_xor_sync(0xffffffffu, itsMax, o));
   if ((threadIdx.x & 31) == 0) atomicMax((unsigned long long*)&b.st->itersDone[stage], (unsigned long long)itsMax);
   if (threadIdx.x == 0 && unconv) atomicAdd(&b.st->finalUnconv[stage], (unsigned long long)unconv);
+}
+
+// ---------------------------------------------------------------------------
+// Compacted fast Newton: one launch per iteration over a worklist of the
+// zones still above tolerance, so no warp carries converged lanes.  The
+// state between launches (P in prim, R, l2first) lives in HBM; worklists are
+// appended with warp-aggregated atomics.  Launch 0 floors, evaluates the
+// residual and lists the unconverged zones; launch it >= 1 does Newton
+// iteration it-1 on list[(it-1)&1] and lists the zones still unconverged.
+// ---------------------------------------------------------------------------
+GRIM_D void list_append(int* list, unsigned long long* count, int zone, bool take) {
+  const unsigned m = __ballot_sync(0xffffffffu, take);
+  if (m == 0) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(m) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(count, (unsigned long long)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (take) list[base + __popc(m & ((1u << lane) - 1))] = zone;
+}
+
+template <int COND, int VISC>
+__global__ void __launch_bounds__(128) k_newton_list_init(DevCfg c, int stage, StageBufs b) {
+  constexpr int NF = 5 + COND + VISC;
+  for (long long n0 = (long long)blockIdx.x * blockDim.x; n0 < c.Zint; n0 += (long long)gridDim.x * blockDim.x) {
+    const long long n = n0 + threadIdx.x;
+    bool take = false;
+    long long z = 0;
+    if (n < c.Zint) {
+      const long long Z = c.Z;
+      z = interior_to_z(c, n);
+      int i, j, k;
+      zijk(c, z, i, j, k);
+      ZoneGeo<double> G;
+      load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
+      StageConst<NF> K;
+      load_stage_const<COND, VISC>(K, c, stage, b, z, G);
+      double P[NF], R[NF];
+      for (int v = 0; v < NF; v++) P[v] = b.prim[(long long)v * Z + z];
+      P[0] = fmax(P[0], c.rhoFloor);
+      P[1] = fmax(P[1], c.uFloor);
+      b.prim[z] = P[0];
+      b.prim[Z + z] = P[1];
+      zone_residual<COND, VISC, double, double>(P, K, G, c, R);
+      const double l2 = l2sum<NF>(R);
+      for (int v = 0; v < NF; v++) b.R[(long long)v * Z + z] = R[v];
+      b.l2[Z + z] = l2;
+      take = l2 > fmax(c.atol, c.rtol * c.rtol * l2);
+      if (!take) atomicAdd(&b.st->itHist[stage][0], 1ULL);
+    }
+    list_append(b.list[0], &b.st->listCount[0], (int)z, take);
+  }
+}
+
+template <int COND, int VISC, class T>
+__global__ void __launch_bounds__(128) k_newton_list_iter(DevCfg c, int stage, int it, StageBufs b) {
+  constexpr int NF = 5 + COND + VISC;
+  const int in = (it - 1) & 1, out = it & 1;
+  const long long count = (long long)b.st->listCount[in];
+  const bool last = (it == c.maxIter);
+  for (long long n0 = (long long)blockIdx.x * blockDim.x; n0 < count; n0 += (long long)gridDim.x * blockDim.x) {
+    const long long n = n0 + threadIdx.x;
+    bool take = false;
+    int zone = 0;
+    if (n < count) {
+      const long long Z = c.Z;
+      zone = b.list[in][n];
+      const long long z = zone;
+      int i, j, k;
+      zijk(c, z, i, j, k);
+      ZoneGeo<double> G;
+      load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
+      ZoneGeo<T> Gt;
+      for (int m = 0; m < 4; m++)
+        for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = (T)G.gcov[m][q]; Gt.gcon[m][q] = (T)G.gcon[m][q]; }
+      Gt.g = (T)G.g; Gt.alpha = (T)G.alpha; Gt.x1 = (T)G.x1; Gt.x2 = (T)G.x2; Gt.dyn = (T)G.dyn;
+      StageConst<NF> K;
+      load_stage_const<COND, VISC>(K, c, stage, b, z, G);
+      double P[NF], R[NF];
+      for (int v = 0; v < NF; v++) {
+        P[v] = b.prim[(long long)v * Z + z];
+        R[v] = b.R[(long long)v * Z + z];
+      }
+      const double l2 = l2sum<NF>(R);
+      const double l2first = b.l2[Z + z];
+      T J[NF][NF];
+      tangent_jacobian<COND, VISC, T>(P, K, Gt, c, J);
+      T bv[NF], xv[NF];
+      for (int v = 0; v < NF; v++) bv[v] = (T)(-R[v]);
+      gauss_solve<T, NF>(J, bv, xv);
+      double dPv[NF];
+      for (int v = 0; v < NF; v++) dPv[v] = (double)xv[v];
+      const double f0 = 0.5 * l2, fPrime0 = -2. * f0;
+      double lam = 1.;
+      bool haveR = false;
+      double Rt[NF];
+      for (int ls = 0; ls < c.maxLS; ls++) {
+        double Pt[NF];
+        for (int v = 0; v < NF; v++) Pt[v] = P[v] + lam * dPv[v];
+        zone_residual<COND, VISC, double, double>(Pt, K, G, c, Rt);
+        const double f1 = 0.5 * l2sum<NF>(Rt);
+        if (!(f1 > (f0 * (1. - 1e-4 * lam) + c.lsFloor))) { haveR = true; break; }
+        const double denom = (f1 - f0 - fPrime0 * lam);
+        lam = -fPrime0 * lam * lam / denom / 2.;
+      }
+      for (int v = 0; v < NF; v++) P[v] = P[v] + lam * dPv[v];
+      const bool floored = (P[0] < c.rhoFloor) || (P[1] < c.uFloor);
+      if (!last) {
+        P[0] = fmax(P[0], c.rhoFloor);
+        P[1] = fmax(P[1], c.uFloor);
+      }
+      if (!haveR || floored) zone_residual<COND, VISC, double, double>(P, K, G, c, Rt);
+      const double l2n = l2sum<NF>(Rt);
+      const bool conv = l2n <= fmax(c.atol, c.rtol * c.rtol * l2first);
+      take = !conv && !last;
+      if (conv) atomicAdd(&b.st->itHist[stage][min(it, 15)], 1ULL);
+      else if (last) {
+        atomicAdd(&b.st->itHist[stage][min(it, 15)], 1ULL);
+        atomicAdd(&b.st->finalUnconv[stage], 1ULL);
+      }
+      for (int v = 0; v < NF; v++) {
+        b.prim[(long long)v * Z + z] = P[v];
+        b.R[(long long)v * Z + z] = Rt[v];
+      }
+    }
+    if (!last) list_append(b.list[out], &b.st->listCount[out], zone, take);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && count > 0) atomicMax(&b.st->itersDone[stage], (unsigned long long)it);
 }
 
 // ---------------------------------------------------------------------------
@@ -972,10 +1172,23 @@ void emhd_prepass(const DevCfg& c, const double* ps, const double* geoC, double*
   GRIM_EMHD_DISPATCH(c, emhd_prepass_t, c, ps, geoC, uT, s);
 }
 
+constexpr int kMarchSpan = 16;
 template <int C, int V>
 static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,
                         double* flux, cudaStream_t s) {
-  k_face_flux<C, V><<<nblk(c.Z, 128), 128, 0, s>>>(c, dir, ps, geoF, geoC, flux);
+  if (dir == 0) {
+    const long long warps = (long long)c.N2T * c.N3T * ((c.N1T - 5 + 30) / 31);
+    k_face_flux_x1<C, V><<<nblk(warps * 32, 128), 128, 0, s>>>(c, ps, geoF, flux);
+  } else {
+    const int NT = (dir == 1) ? c.N2T : c.N3T;
+    const int other = (dir == 1) ? c.N3T : c.N2T;
+    // march length: long enough to amortise the extra reconstruction, short
+    // enough to leave ~150k threads in flight
+    const long long faces = (long long)c.N1T * other * (NT - 5);
+    const int span = (int)std::max(2LL, std::min((long long)kMarchSpan, faces / (148LL * 1024)));
+    dim3 grid(nblk(c.N1T, 128), (unsigned)((NT - 5 + span - 1) / span), (unsigned)other);
+    k_face_flux_march<C, V><<<grid, 128, 0, s>>>(c, dir, span, ps, geoF, geoC, flux);
+  }
 }
 void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC, double* flux,
                cudaStream_t s) {
@@ -1032,6 +1245,34 @@ void newton_fast(const DevCfg& c, int stage, const StageBufs& b, int mode, const
   GRIM_EMHD_DISPATCH(c, newton_fast_t, c, stage, b, mode, list, nlist, s);
 }
 
+static int persistent_blocks() {
+  static int nb = 0;
+  if (!nb) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    nb = sms * 8;
+  }
+  return nb;
+}
+template <int C, int V>
+static void newton_list_t(const DevCfg& c, int stage, const StageBufs& b, int mode, cudaStream_t s) {
+  const int nb = persistent_blocks();
+  cudaMemsetAsync(b.st->listCount, 0, sizeof(b.st->listCount), s);
+  k_newton_list_init<C, V><<<nb, 128, 0, s>>>(c, stage, b);
+  for (int it = 1; it <= c.maxIter; it++) {
+    // the list this launch appends to starts empty
+    cudaMemsetAsync(&b.st->listCount[it & 1], 0, sizeof(unsigned long long), s);
+    if (mode == GRIM_NEWTON_MIXED32)
+      k_newton_list_iter<C, V, float><<<nb, 128, 0, s>>>(c, stage, it, b);
+    else
+      k_newton_list_iter<C, V, double><<<nb, 128, 0, s>>>(c, stage, it, b);
+  }
+}
+void newton_list(const DevCfg& c, int stage, const StageBufs& b, int mode, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, newton_list_t, c, stage, b, mode, s);
+}
+
 template <int C, int V>
 static void residual_t(const DevCfg& c, int stage, const StageBufs& b, const double* pg, double* out,
                        cudaStream_t s) {
@@ -1074,6 +1315,33 @@ int batch_solve(int n, int batch, const double* A, const double* b, double* x, c
     case 8: k_batch_solve<8><<<g, 128, 0, s>>>(batch, A, b, x); return 0;
     default: return -1;
   }
+}
+static TorusCfg torus_cfg(const DevCfg& c) {
+  TorusCfg t;
+  t.MaxLorentzFactor = c.maxLF; t.RhoFloorAmpl = c.rhoFloorAmpl; t.UFloorAmpl = c.uFloorAmpl;
+  t.RhoFloorSlope = c.rhoFloorSlope; t.UFloorSlope = c.uFloorSlope;
+  t.BsqrOverRhoMax = c.bsqOverRhoMax; t.BsqrOverUMax = c.bsqOverUMax;
+  return t;
+}
+template <int C, int V>
+static void torus_floor_t(const DevCfg& c, double* p, const double* geoC, const unsigned long long* flag,
+                          cudaStream_t s) {
+  k_torus_floor<C, V><<<nblk(c.Z, 128), 128, 0, s>>>(c, torus_cfg(c), p, geoC, flag);
+}
+void torus_floor(const DevCfg& c, double* p, const double* geoC, const unsigned long long* flag, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, torus_floor_t, c, p, geoC, flag, s);
+}
+void torus_nan_flag(const DevCfg& c, const double* p, unsigned long long* flag, cudaStream_t s) {
+  k_nan_flag<<<nblk(c.Zint, 256), 256, 0, s>>>(c, p, flag);
+}
+template <int C, int V>
+static void torus_bcs_t(const DevCfg& c, double* p, const double* geoC, cudaStream_t s) {
+  const long long cols = 2LL * c.ng * c.N2T * c.N3T;
+  k_torus_inflow<C, V><<<nblk(cols, 128), 128, 0, s>>>(c, torus_cfg(c), p, geoC);
+  if (c.dim >= 2) k_torus_poles<<<nblk(2LL * c.N1T * c.N3T, 128), 128, 0, s>>>(c, p, geoC);
+}
+void torus_bcs(const DevCfg& c, double* p, const double* geoC, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, torus_bcs_t, c, p, geoC, s);
 }
 void count_nonfinite(const DevCfg& c, const double* p, DevState* st, cudaStream_t s) {
   k_count_nonfinite<<<nblk(c.Zint, 256), 256, 0, s>>>(c, p, st);

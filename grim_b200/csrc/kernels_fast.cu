@@ -1,5 +1,6 @@
 // kernels_fast.cu -- kernel instantiations compiled with FMA contraction on:
 // the tangent / mixed-precision paths.
 #define GRIM_KNS fast
+#define GRIM_FAST_MATH 1
 #include "kernels.cuh"
 #include "launch.h"

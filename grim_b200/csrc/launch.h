@@ -21,6 +21,7 @@
   void newton_fd_iter(const DevCfg& c, int stage, int it, const StageBufs& b, cudaStream_t s);          \
   void newton_fast(const DevCfg& c, int stage, const StageBufs& b, int mode, const int* list,           \
                    long long nlist, cudaStream_t s);                                                    \
+  void newton_list(const DevCfg& c, int stage, const StageBufs& b, int mode, cudaStream_t s);          \
   void residual(const DevCfg& c, int stage, const StageBufs& b, const double* pg, double* out,         \
                 cudaStream_t s);                                                                        \
   void jacobian(const DevCfg& c, int stage, const StageBufs& b, const double* pg, double* jac,         \
@@ -30,6 +31,10 @@
   void reconstruct(const DevCfg& c, int dir, const double* p, double* pl, double* pr, cudaStream_t s); \
   int batch_solve(int n, int batch, const double* A, const double* b, double* x, cudaStream_t s);      \
   void count_nonfinite(const DevCfg& c, const double* p, DevState* st, cudaStream_t s);                \
+  void torus_floor(const DevCfg& c, double* p, const double* geoC, const unsigned long long* flag,     \
+                   cudaStream_t s);                                                                     \
+  void torus_nan_flag(const DevCfg& c, const double* p, unsigned long long* flag, cudaStream_t s);      \
+  void torus_bcs(const DevCfg& c, double* p, const double* geoC, cudaStream_t s);                      \
   }                                                                                                     \
   }
 

@@ -18,11 +18,15 @@ struct ZoneGeo {
   R gcon[4][4];
   R g, alpha;
   R x1, x2;  // physical coordinates (closures)
+  R dyn;     // x1^1.5 (torus closure)
 };
 
 // Minkowski at compile time; MKS from the stored per-location arrays
-// (layout: 16 gCov, 16 gCon, g, alpha, x1, x2 -> 36 words per zone, SoA).
-enum { GEO_WORDS = 36 };
+// (layout, SoA: 16 gCov, 16 gCon, g, alpha, then the auxiliary fields
+// x1, x2, x1^1.5, rhoFloor(x1), uFloor(x1) -> 39 words per zone).  The last
+// three depend on the geometry only and are evaluated once: the torus
+// closure's dynamical time r^1.5 and the radial floors of applyFloor.
+enum { GEO_WORDS = 39, GEO_AUX = 34, GEO_AUX_WORDS = 5 };
 
 template <class R>
 GRIM_D void geo_minkowski(ZoneGeo<R>& G, R x1, R x2) {
@@ -34,6 +38,7 @@ GRIM_D void geo_minkowski(ZoneGeo<R>& G, R x1, R x2) {
   G.gcon[0][0] = R(-1); G.gcon[1][1] = R(1); G.gcon[2][2] = R(1); G.gcon[3][3] = R(1);
   G.g = R(1); G.alpha = R(1);
   G.x1 = x1; G.x2 = x2;
+  G.dyn = R(0);
 }
 
 template <class R>
@@ -49,6 +54,7 @@ GRIM_D void geo_load(ZoneGeo<R>& G, const double* __restrict__ geo, long long Z,
   G.alpha = (R)__ldg(geo + 33LL * Z + z);
   G.x1 = (R)__ldg(geo + 34LL * Z + z);
   G.x2 = (R)__ldg(geo + 35LL * Z + z);
+  G.dyn = (R)__ldg(geo + 36LL * Z + z);
 }
 
 template <class S, class R>
@@ -103,8 +109,7 @@ GRIM_D void closure(ElemT<S, R>& e, const ZoneGeo<R>& G, const DevCfg& c) {
   } else {
     // torus/problem.cpp:7-55
     typedef typename Real<S>::type T;
-    const T Radius = (T)G.x1;
-    const T Dyn = (T)pow((double)Radius, 1.5);
+    const T Dyn = (T)G.dyn;
     S t = Lift<S>::of((double)Dyn);
     if (c.conduction) {
       S Qmax = (T)c.CondClosure * e.rho * dcube(cs);

@@ -108,6 +108,36 @@ GRIM_D double mp5(double vm2, double vm1, double v0, double vp1, double vp2) {
   return f + mm2(vmin - f, vmax - f);
 }
 
+// WENO5 with the same weights in fewer divisions (fast path only): the
+// normalised weights are unchanged when every weight is multiplied by
+// beta1^2 beta2^2 beta3^2, which leaves one division per face value instead
+// of four.  Equal to weno5_faces to a few ulp.
+GRIM_D void weno5_faces_fast(double y0, double y1, double y2, double y3, double y4, double& lo, double& ro) {
+  const double eps2 = 1.0e-17;
+  double beta1 = ((4.0 / 3.0) * y0 * y0 - (19.0 / 3.0) * y0 * y1 + (25.0 / 3.0) * y1 * y1 +
+                  (11.0 / 3.0) * y0 * y2 - (31.0 / 3.0) * y1 * y2 + (10.0 / 3.0) * y2 * y2) +
+                 eps2 * (1.0 + fabs(y0) + fabs(y1) + fabs(y2));
+  double beta2 = ((4.0 / 3.0) * y1 * y1 - (13.0 / 3.0) * y1 * y2 + (13.0 / 3.0) * y2 * y2 +
+                  (5.0 / 3.0) * y1 * y3 - (13.0 / 3.0) * y2 * y3 + (4.0 / 3.0) * y3 * y3) +
+                 eps2 * (1.0 + fabs(y1) + fabs(y2) + fabs(y3));
+  double beta3 = ((10.0 / 3.0) * y2 * y2 - (31.0 / 3.0) * y2 * y3 + (25.0 / 3.0) * y3 * y3 +
+                  (11.0 / 3.0) * y2 * y4 - (19.0 / 3.0) * y3 * y4 + (4.0 / 3.0) * y4 * y4) +
+                 eps2 * (1.0 + fabs(y2) + fabs(y3) + fabs(y4));
+  const double b1 = beta1 * beta1, b2 = beta2 * beta2, b3 = beta3 * beta3;
+  const double p23 = b2 * b3, p13 = b1 * b3, p12 = b1 * b2;
+  // w1 ~ 1/b1 -> p23, w2 ~ 1/b2 -> p13, w3 ~ 1/b3 -> p12
+  const double w1r = 0.0625 * p23, w2r = 0.625 * p13, w3r = 0.3125 * p12;
+  const double w1l = 0.3125 * p23, w2l = 0.625 * p13, w3l = 0.0625 * p12;
+  double u1r = 0.375 * y0 - 1.25 * y1 + 1.875 * y2;
+  double u2r = -0.125 * y1 + 0.75 * y2 + 0.375 * y3;
+  double u3r = 0.375 * y2 + 0.75 * y3 - 0.125 * y4;
+  double u1l = -0.125 * y0 + 0.75 * y1 + 0.375 * y2;
+  double u2l = 0.375 * y1 + 0.75 * y2 - 0.125 * y3;
+  double u3l = 1.875 * y2 - 1.25 * y3 + 0.375 * y4;
+  lo = (w1l * u1l + w2l * u2l + w3l * u3l) / (w1l + w2l + w3l);
+  ro = (w1r * u1r + w2r * u2r + w3r * u3r) / (w1r + w2r + w3r);
+}
+
 // face values of zone i
 GRIM_D void recon_faces(int scheme, double theta, double y0, double y1, double y2, double y3, double y4,
                         double& lo, double& ro) {
@@ -127,6 +157,15 @@ GRIM_D void recon_faces(int scheme, double theta, double y0, double y1, double y
     }
   }
 }
+GRIM_D void recon_faces_fast(int scheme, double theta, double y0, double y1, double y2, double y3, double y4,
+                             double& lo, double& ro) {
+  if (scheme == GRIM_WENO5) {
+    weno5_faces_fast(y0, y1, y2, y3, y4, lo, ro);
+    return;
+  }
+  recon_faces(scheme, theta, y0, y1, y2, y3, y4, lo, ro);
+}
+
 // the slope() used by the EMHD gradients (reconstruction.cpp:39-64); MP5
 // uses the centred 5-point derivative
 GRIM_D double recon_slope(int scheme, double theta, double y0, double y1, double y2, double y3,

@@ -57,9 +57,10 @@ struct grim_handle {
   // stage buffers
   double *consOld = nullptr, *divF = nullptr, *Sexp = nullptr, *R = nullptr, *l2 = nullptr, *uT = nullptr;
   double* flux[3] = {nullptr, nullptr, nullptr};
+  int* list[2] = {nullptr, nullptr};  // compacted Newton worklists
   double* scratch = nullptr;  // test entry points: dof x Z inputs
   double* scratch2 = nullptr;
-  // geometry: per location 36 x Z (MKS only), centre Christoffels 64 x Z
+  // geometry: per location 39 x Z (MKS only), centre Christoffels 64 x Z
   double* geo[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   double* gamma = nullptr;
   DevState* st = nullptr;
@@ -82,6 +83,8 @@ static void free_all(grim_handle* h) {
   if (h->st) { cudaFree(h->st); h->st = nullptr; }
   if (h->hst) { cudaFreeHost(h->hst); h->hst = nullptr; }
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  for (int l = 0; l < 2; l++)
+    if (h->list[l]) { cudaFree(h->list[l]); h->list[l] = nullptr; }
 }
 
 static int make_devcfg(const grim_config& c, DevCfg& d) {
@@ -124,6 +127,12 @@ static int make_devcfg(const grim_config& c, DevCfg& d) {
   d.atol = c.nonlinearsolve_atol; d.rtol = c.nonlinearsolve_rtol;
   d.jacEps = c.JacobianAssembleEpsilon; d.lsFloor = c.linesearchfloor;
   d.tau0 = c.closureTau0; d.tau1 = c.closureTau1;
+  d.maxLF = c.MaxLorentzFactor; d.rhoFloorAmpl = c.RhoFloorAmpl; d.uFloorAmpl = c.UFloorAmpl;
+  d.rhoFloorSlope = c.RhoFloorSlope; d.uFloorSlope = c.UFloorSlope;
+  d.bsqOverRhoMax = c.BsqrOverRhoMax; d.bsqOverUMax = c.BsqrOverUMax;
+  if ((c.problem == GRIM_PROBLEM_TORUS || c.closure == GRIM_CLOSURE_TORUS) && c.metric == GRIM_MINKOWSKI) {
+    set_err("the torus problem and closure need the MKS metric"); return GRIM_EINVAL;
+  }
   return GRIM_OK;
 }
 
@@ -149,6 +158,8 @@ static StageBufs stage_bufs(grim_handle* h, int stage) {
   b.R = h->R;
   b.l2 = h->l2;
   b.st = h->st;
+  b.list[0] = h->list[0];
+  b.list[1] = h->list[1];
   return b;
 }
 
@@ -187,6 +198,9 @@ static void enqueue_newton(grim_handle* h, int stage) {
       grim::exact::newton_fd_iter(c, stage, it, b, s);
       g_launch_counter++;
     }
+  } else if (h->cfg.perZoneConvergence == 2) {
+    grim::fast::newton_list(c, stage, b, h->cfg.newtonMode, s);
+    g_launch_counter += 1 + c.maxIter;
   } else {
     grim::fast::newton_fast(c, stage, b, h->cfg.newtonMode, nullptr, c.Zint, s);
     g_launch_counter++;
@@ -201,6 +215,28 @@ static void enqueue_dt_speeds(grim_handle* h, const double* p, int mode) {
   g_launch_counter++;
 }
 
+// torus: setProblemSpecificBCs (inflow check + pole fix) after the
+// stage-start boundary fill (timestep.cpp:17-22, :186-191)
+static void enqueue_problem_bcs(grim_handle* h, double* p) {
+  if (h->cfg.problem != GRIM_PROBLEM_TORUS) return;
+  KNS_CALL(h, torus_bcs, h->dc, p, h->geo[GRIM_CENTER], h->stream);
+  g_launch_counter += 2;
+}
+// halfStepDiagnostics: torus floors on primHalfStep (torus/problem.cpp:714-717)
+static void enqueue_half_diagnostics(grim_handle* h) {
+  if (h->cfg.problem != GRIM_PROBLEM_TORUS) return;
+  KNS_CALL(h, torus_floor, h->dc, h->primHalf, h->geo[GRIM_CENTER], nullptr, h->stream);
+  g_launch_counter++;
+}
+// fullStepDiagnostics: NaN reset + floors on primOld (torus/problem.cpp:719-746)
+static void enqueue_full_diagnostics(grim_handle* h) {
+  if (h->cfg.problem != GRIM_PROBLEM_TORUS) return;
+  cudaMemsetAsync(&h->st->nanFlag, 0, sizeof(unsigned long long), h->stream);
+  KNS_CALL(h, torus_nan_flag, h->dc, h->primOld, &h->st->nanFlag, h->stream);
+  KNS_CALL(h, torus_floor, h->dc, h->primOld, h->geo[GRIM_CENTER], &h->st->nanFlag, h->stream);
+  g_launch_counter += 2;
+}
+
 static void enqueue_step(grim_handle* h, bool timed) {
   const DevCfg& c = h->dc;
   cudaStream_t s = h->stream;
@@ -212,10 +248,12 @@ static void enqueue_step(grim_handle* h, bool timed) {
   cudaMemsetAsync(h->st->count, 0, sizeof(h->st->count), s);
   cudaMemsetAsync(h->st->itersDone, 0, sizeof(h->st->itersDone), s);
   cudaMemsetAsync(h->st->finalUnconv, 0, sizeof(h->st->finalUnconv), s);
+  cudaMemsetAsync(h->st->itHist, 0, sizeof(h->st->itHist), s);
   cudaMemsetAsync(&h->st->nonFinite, 0, sizeof(unsigned long long), s);
   // ---- half stage
   KNS_CALL(h, ghost_fill, c, h->primOld, c.dof, s);
   g_launch_counter++;
+  enqueue_problem_bcs(h, h->primOld);
   if (!h->cfg.elemOldFromFullStep) enqueue_dt_speeds(h, h->primOld, 0);
   if (timed) cudaEventRecord(h->ev[1], s);
   enqueue_stencil(h, GRIM_HALF_STEP);
@@ -225,9 +263,11 @@ static void enqueue_step(grim_handle* h, bool timed) {
   cudaMemcpyAsync(h->primHalf, h->prim, bytes, cudaMemcpyDeviceToDevice, s);
   KNS_CALL(h, communicate, c, h->primHalf, c.dof, s);
   g_launch_counter++;
+  enqueue_half_diagnostics(h);
   // ---- full stage
   KNS_CALL(h, ghost_fill, c, h->primHalf, c.dof, s);
   g_launch_counter++;
+  enqueue_problem_bcs(h, h->primHalf);
   if (timed) cudaEventRecord(h->ev[4], s);
   enqueue_stencil(h, GRIM_FULL_STEP);
   if (timed) cudaEventRecord(h->ev[5], s);
@@ -238,6 +278,7 @@ static void enqueue_step(grim_handle* h, bool timed) {
   g_launch_counter++;
   grim::exact::advance_time(h->st, s);
   g_launch_counter++;
+  enqueue_full_diagnostics(h);
   // fullStepDiagnostics re-setting elemOld (linear_modes/problem.cpp:287)
   // on the communicated primOld
   if (h->cfg.elemOldFromFullStep) enqueue_dt_speeds(h, h->primOld, 0);
@@ -277,9 +318,10 @@ int grim_create(const grim_config* cfg, int device, grim_handle** out) {
   for (int d = 0; ok && d < c.dim; d++) ok = alloc(&h->flux[d], c.dof);
   if (ok && (c.conduction || c.viscosity)) ok = alloc(&h->uT, 5);
   if (ok && cfg->metric != GRIM_MINKOWSKI) {
-    for (int l = 0; ok && l < 5; l++) ok = alloc(&h->geo[l], 36);
+    for (int l = 0; ok && l < 5; l++) ok = alloc(&h->geo[l], 39);
     if (ok) ok = alloc(&h->gamma, 64);
   }
+  for (int l = 0; ok && l < 2; l++) ok = cudaMalloc(&h->list[l], (size_t)c.Zint * sizeof(int)) == cudaSuccess;
   if (ok) ok = cudaMalloc(&h->st, sizeof(DevState)) == cudaSuccess;
   if (ok) ok = cudaMallocHost(&h->hst, sizeof(DevState)) == cudaSuccess;
   if (!ok) {
@@ -558,6 +600,7 @@ int grim_stage_setup(grim_handle* h, int stage) {
   const DevCfg& c = h->dc;
   double* ps = (stage == GRIM_HALF_STEP) ? h->primOld : h->primHalf;
   KNS_CALL(h, ghost_fill, c, ps, c.dof, h->stream);
+  enqueue_problem_bcs(h, ps);
   enqueue_stencil(h, stage);
   h->lastStage = stage;
   CK(cudaGetLastError());
@@ -655,7 +698,7 @@ int grim_get_geometry(grim_handle* h, int location, double* out, double* gamma, 
     if (rc) return rc;
   }
   if (xc) {
-    int rc = stage_out(h, xc, h->geo[location] + 34 * c.Z, 2 * h->bytesZ, memKind);
+    int rc = stage_out(h, xc, h->geo[location] + 34 * c.Z, 5 * h->bytesZ, memKind);
     if (rc) return rc;
   }
   if (gamma && location == GRIM_CENTER) return stage_out(h, gamma, h->gamma, 64 * h->bytesZ, memKind);
@@ -669,7 +712,7 @@ int grim_set_geometry(grim_handle* h, int location, const double* in, const doub
   CK(cudaSetDevice(h->device));
   const cudaMemcpyKind k = memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   if (in) CK(cudaMemcpyAsync(h->geo[location], in, 34 * h->bytesZ, k, h->stream));
-  if (xc) CK(cudaMemcpyAsync(h->geo[location] + 34 * h->dc.Z, xc, 2 * h->bytesZ, k, h->stream));
+  if (xc) CK(cudaMemcpyAsync(h->geo[location] + 34 * h->dc.Z, xc, 5 * h->bytesZ, k, h->stream));
   if (gamma && location == GRIM_CENTER) CK(cudaMemcpyAsync(h->gamma, gamma, 64 * h->bytesZ, k, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   // the first computeDt depends on the geometry: redo it
@@ -678,8 +721,24 @@ int grim_set_geometry(grim_handle* h, int location, const double* in, const doub
   return GRIM_OK;
 }
 
+int grim_problem_init(grim_handle* h) {
+  if (!h) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  if (h->cfg.problem == GRIM_PROBLEM_TORUS) {
+    // the tail of the torus initialConditions (problem.cpp:525-540):
+    // applyFloor, then fullStepDiagnostics (NaN reset + applyFloor); the
+    // element left set by them is what the first computeDt sees
+    KNS_CALL(h, torus_floor, h->dc, h->primOld, h->geo[GRIM_CENTER], nullptr, h->stream);
+    enqueue_full_diagnostics(h);
+    enqueue_dt_speeds(h, h->primOld, 0);
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));
+  return GRIM_OK;
+}
+
 int grim_set_newton_mode(grim_handle* h, int mode, int perZone, double rtol) {
-  if (!h || mode < 0 || mode > 2) return GRIM_EINVAL;
+  if (!h || mode < 0 || mode > 2 || perZone < 0 || perZone > 2) return GRIM_EINVAL;
   h->cfg.newtonMode = mode;
   h->cfg.perZoneConvergence = perZone;
   h->cfg.nonlinearsolve_rtol = rtol;
@@ -722,6 +781,16 @@ int grim_get_stats(grim_handle* h, grim_stats* out) {
   }
   s.kernelLaunches = h->launchesPerStep;
   *out = s;
+  return GRIM_OK;
+}
+
+int grim_get_newton_histogram(grim_handle* h, long long* out) {
+  if (!h || !out) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(h->hst, h->st, sizeof(DevState), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int st = 0; st < 2; st++)
+    for (int i = 0; i < 16; i++) out[st * 16 + i] = (long long)h->hst->itHist[st][i];
   return GRIM_OK;
 }
 

@@ -15,13 +15,16 @@ struct DevState {
   unsigned long long itersDone[2];
   unsigned long long nonFinite;
   unsigned long long finalUnconv[2];
+  unsigned long long nanFlag;
+  unsigned long long itHist[2][16];  // zones by Newton iterations used (fast path)
+  unsigned long long listCount[2];   // compacted worklists: entries per ping-pong list
 };
 
 struct StageBufs {
   const double* ps;       // prims the stage's fluxes are computed from
   const double* pold;     // primOld
   double* prim;           // Newton guess / result
-  const double* geoC;     // centre geometry (36 x Z) or null (Minkowski)
+  const double* geoC;     // centre geometry (39 x Z) or null (Minkowski)
   const double* gamma;    // centre Christoffels (64 x Z) or null
   const double* geoF[3];  // face geometry per direction or null
   double* flux[3];        // face fluxes per direction, dof x Z
@@ -32,6 +35,7 @@ struct StageBufs {
   double* R;              // nf x Z  (Newton scratch)
   double* l2;             // 2 x Z   (l2, l2first)
   DevState* st;
+  int* list[2];           // compacted Newton worklists (interior zone indices)
 };
 
 }  // namespace grim

@@ -42,9 +42,8 @@ __global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, cons
     if (bad)
       for (int v = 0; v < c.dof; v++) *pv[v] = 0.;
   }
-  const double Radius = G.x1;
-  const double minRho = pow(Radius, t.RhoFloorSlope) * t.RhoFloorAmpl;
-  const double minU = pow(Radius, t.UFloorSlope) * t.UFloorAmpl;
+  const double minRho = __ldg(geoC + 37LL * Z + z);
+  const double minU = __ldg(geoC + 38LL * Z + z);
   const double rho_pre = *pv[RHO] * 1., u_pre = *pv[UU] * 1.;
   bool usefloor = false;
   {

@@ -127,7 +127,9 @@ def torus_prims(cfg, geo, seed=4):
     idx = C.var_index(cfg)
     dof, nf = C.var_counts(cfg)
     rho, u, U = torus_fluid(cfg, geo, seed)
-    rhoMax = np.max(rho)
+    # ArrayFire's max/min reductions skip NaN (the cylindrified map is
+    # undefined in some inner ghost zones)
+    rhoMax = np.nanmax(rho)
     rho = rho / rhoMax
     u = u / rhoMax
     # vector potential from the density averaged over the 4 (6) neighbours
@@ -156,7 +158,7 @@ def torus_prims(cfg, geo, seed=4):
     # beta normalisation (SANE): min over the grid of 2(P+1e-13)/(b^2+1e-18)
     bsq, pg = b2_and_pressure(cfg, P, geo)
     beta = 2. * (pg + 1.e-13) / (bsq + 1.e-18)
-    BFactor = math.sqrt(np.min(beta) / tp["MinPlasmaBeta"])
+    BFactor = math.sqrt(np.nanmin(beta) / tp["MinPlasmaBeta"])
     for v in ("B1", "B2", "B3"):
         P[idx[v]] = P[idx[v]] * BFactor
     return P, dict(rhoMax=float(rhoMax), BFactor=BFactor)

@@ -109,6 +109,11 @@ class timeStepper:
         except Exception:
             pass
 
+    def problemInit(self):
+        """The problem's tail of initialConditions (torus: floors + the first
+        fullStepDiagnostics); call after primOld.setVars."""
+        _lib.check(_lib.lib().grim_problem_init(self._h), "problem_init")
+
     # ---- stepping ----------------------------------------------------------
     def timeStep(self):
         r, w = ctypes.c_int(), ctypes.c_int()
@@ -155,6 +160,12 @@ class timeStepper:
         return dict(newtonIters=list(s.newtonIters), unconverged=list(s.unconverged),
                     nonFinite=s.nonFinite, msStep=s.msStep, msStencil=s.msStencil,
                     msNewton=s.msNewton, msOther=s.msOther, kernelLaunches=s.kernelLaunches)
+
+    def newtonHistogram(self):
+        """[stage][iterations] -> zones, for the last step (tangent / mixed)."""
+        out = (ctypes.c_longlong * 32)()
+        _lib.check(_lib.lib().grim_get_newton_histogram(self._h, out), "newton_histogram")
+        return [list(out[0:16]), list(out[16:32])]
 
     def stream(self):
         return _lib.lib().grim_stream(self._h)
@@ -226,7 +237,7 @@ class timeStepper:
     def getGeometry(self, location):
         out = np.zeros((34,) + self.zshape)
         gam = np.zeros((64,) + self.zshape)
-        xc = np.zeros((2,) + self.zshape)
+        xc = np.zeros((5,) + self.zshape)
         _lib.check(_lib.lib().grim_get_geometry(self._h, int(location), _ptr(out), _ptr(gam), _ptr(xc),
                                                 _lib.HOST), "get_geometry")
         return dict(gCov=out[:16].reshape((4, 4) + self.zshape), gCon=out[16:32].reshape((4, 4) + self.zshape),
@@ -236,11 +247,19 @@ class timeStepper:
         out = np.concatenate([np.reshape(gCov, (16,) + self.zshape), np.reshape(gCon, (16,) + self.zshape),
                               np.reshape(g, (1,) + self.zshape), np.reshape(alpha, (1,) + self.zshape)])
         out = np.ascontiguousarray(out, dtype=np.float64)
-        xc = None if x is None else np.ascontiguousarray(np.reshape(x, (-1,) + self.zshape)[:2])
+        xc = None if x is None else np.ascontiguousarray(np.reshape(x, (-1,) + self.zshape)[:5])
         gm = None if gamma is None else np.ascontiguousarray(np.reshape(gamma, (64,) + self.zshape))
         _lib.check(_lib.lib().grim_set_geometry(self._h, int(location), _ptr(out),
                                                 None if gm is None else _ptr(gm),
                                                 None if xc is None else _ptr(xc), _lib.HOST), "set_geometry")
+
+
+def measurePeaks(device=0):
+    """(fp64 TFLOP/s, fp32 TFLOP/s, HBM GB/s) measured on ``device``."""
+    a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    _lib.check(_lib.lib().grim_measure_peaks(int(device), ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+               "measure_peaks")
+    return a.value, b.value, c.value
 
 
 def batchSolve(A, b):

@@ -76,7 +76,7 @@ typedef struct grim_config {
   int problem;              /* problem hooks: BCs, flux filter, floors */
   int elemOldFromFullStep;  /* 1: fullStepDiagnostics re-sets elemOld */
   int newtonMode;           /* GRIM_NEWTON_* */
-  int perZoneConvergence;   /* 0: global break (reference), 1: per zone */
+  int perZoneConvergence;   /* 0: global break (reference), 1: per zone, 2: compacted */
   int reserved_i[5];
   double blackHoleSpin, hSlope;
   double X1Start, X1End, X2Start, X2End, X3Start, X3End;
@@ -125,6 +125,11 @@ const char* grim_last_error(void);
 int grim_set_prims(grim_handle* h, int which, const double* src, int memKind);
 int grim_get_prims(grim_handle* h, int which, double* dst, int memKind);
 
+/* the problem's tail of timeStepper::initialConditions after the caller has
+ * set primOld: for the torus the floors and the first fullStepDiagnostics
+ * (torus/problem.cpp:525-540); nothing for the other problems */
+int grim_problem_init(grim_handle* h);
+
 /* ---- stepping: timeStepper::timeStep (timestep.cpp:3-334); numReads and
  *      numWrites report the algorithmic words per zone, may be NULL ------ */
 int grim_time_step(grim_handle* h, int* numReads, int* numWrites);
@@ -172,14 +177,23 @@ int grim_batch_solve(int n, int batch, const double* A, const double* b, double*
 
 /* ---- geometry (geometry.cpp:4-680) ------------------------------------ */
 /* out = [16 gCov | 16 gCon | g | alpha] x Z; gamma (center only) 64 x Z;
- * xcoords 3 x Z.  get copies out, set replaces the device copy. */
+ * aux 5 x Z = [x1 | x2 | x1^1.5 | RhoFloorAmpl x1^RhoFloorSlope |
+ * UFloorAmpl x1^UFloorSlope] (physical coordinates and the geometry-only
+ * fields of the torus closure and floors).  get copies out, set replaces the
+ * device copy. */
 int grim_get_geometry(grim_handle* h, int location, double* out, double* gamma,
                       double* xcoords, int memKind);
 int grim_set_geometry(grim_handle* h, int location, const double* in,
                       const double* gamma, const double* xcoords, int memKind);
 
 /* ---- options, statistics, graphs ------------------------------------- */
+/* mode: GRIM_NEWTON_*; perZoneConvergence for the tangent / mixed modes:
+ * 1 = one kernel, each thread iterates its zone to convergence; 2 = one
+ * launch per iteration over a compacted worklist of unconverged zones */
 int grim_set_newton_mode(grim_handle* h, int mode, int perZoneConvergence, double rtol);
+/* zones by Newton iterations used in the last step: out[stage*16 + iters]
+ * (tangent / mixed modes) */
+int grim_get_newton_histogram(grim_handle* h, long long* out);
 int grim_get_stats(grim_handle* h, grim_stats* out);
 /* capture timeStep into a CUDA graph and replay it from grim_time_step */
 int grim_enable_graph(grim_handle* h, int enable);

@@ -302,6 +302,7 @@ struct Geom {
   Arr gCov[4][4], gCon[4][4], g, alpha;
   Arr gamma[4][4][4]; /* gammaUpDownDown, center only */
   Arr x[3];           /* physical coordinates xCoords */
+  Arr dyn, minRho, minU; /* x1^1.5 and the radial floors (geometry only) */
   bool hasGamma = false;
   /* coordinatesGrid::setXCoords (grid.cpp:168-249) + geometry ctor
    * (geometry.cpp:4-59) + computeConnectionCoeffs (:61-119, center only) */
@@ -310,6 +311,7 @@ struct Geom {
     for (int m = 0; m < 4; m++) for (int n = 0; n < 4; n++) { gCov[m][n].assign(Z, 0.); gCon[m][n].assign(Z, 0.); }
     g.assign(Z, 0.); alpha.assign(Z, 0.);
     for (int d = 0; d < 3; d++) x[d].assign(Z, 0.);
+    dyn.assign(Z, 0.); minRho.assign(Z, 0.); minU.assign(Z, 0.);
     hasGamma = withGamma;
     if (withGamma) for (int a = 0; a < 4; a++) for (int b = 0; b < 4; b++) for (int e = 0; e < 4; e++) gamma[a][b][e].assign(Z, 0.);
     const double dX1 = (c.X1End - c.X1Start) / L.N1;
@@ -327,6 +329,10 @@ struct Geom {
       X[2] = c.X3Start + ((double)(k - L.g3) + o3) * dX3;
       double xx[3]; cm.XtoX(X, xx);
       for (int d = 0; d < 3; d++) x[d][z] = xx[d];
+      /* torus/problem.cpp:9-13 and :547-548: functions of the radius only */
+      dyn[z] = std::pow(xx[0], 1.5);
+      minRho[z] = std::pow(xx[0], c.RhoFloorSlope) * c.RhoFloorAmpl;
+      minU[z] = std::pow(xx[0], c.UFloorSlope) * c.UFloorAmpl;
       double G[4][4], C[4][4], det;
       cm.gCov(X, G);
       detAndInverse(G, det, C);
@@ -404,8 +410,7 @@ struct Elem {
       nu_emhd[z] = cs * cs * tau[z];
     } else {
       /* torus/problem.cpp:7-55 */
-      double Radius = geom->x[0][z];
-      double Dyn = std::pow(Radius, 1.5);
+      double Dyn = geom->dyn[z];
       double t = Dyn;
       if (c.conduction) {
         double Qmax = c.ConductionClosureFactor * rho[z] * std::pow(cs, 3.);
@@ -1149,8 +1154,259 @@ struct Stepper {
     }
   }
 
-  void applyProblemSpecificFluxFilter() {}
-  void setProblemSpecificBCs(Grid&) {}
+  bool torus() const { return P.c.problem == 1; }
+
+  /* torus/problem.cpp:1243-1285 */
+  void applyProblemSpecificFluxFilter() {
+    if (!torus()) return;
+    const int ng = L.ng, N1 = L.N1, N2 = L.N2;
+    for (int k = 0; k < L.N3T; k++)
+      for (int j = 0; j < L.N2T; j++) {
+        double& a = fluxesX1.v(RHO)[L.idx(ng, j, k)];
+        a = std::min(a, 0.);
+        double& b = fluxesX1.v(RHO)[L.idx(N1 + ng, j, k)];
+        b = std::max(b, 0.);
+      }
+    if (L.dim < 2) return;
+    for (int k = 0; k < L.N3T; k++)
+      for (int i = 0; i < L.N1T; i++) {
+        for (int var = 0; var < P.dof; var++) fluxesX2.v(var)[L.idx(i, ng, k)] = 0.;
+        fluxesX1.v(P.B2)[L.idx(i, ng - 1, k)] = fluxesX1.v(P.B2)[L.idx(i, ng, k)] * (-1.0);
+        for (int var = 0; var < P.dof; var++) fluxesX2.v(var)[L.idx(i, N2 + ng, k)] = 0.;
+        fluxesX1.v(P.B2)[L.idx(i, N2 + ng, k)] = fluxesX1.v(P.B2)[L.idx(i, N2 + ng - 1, k)] * (-1.0);
+      }
+  }
+
+  /* inflowCheck (torus/problem.cpp:941-1044) */
+  void inflowCheck(Grid& prim, Elem& elemBC) {
+    const int ng = L.ng, N1 = L.N1;
+    const double vSqrMax = 1. - 1. / P.c.MaxLorentzFactor / P.c.MaxLorentzFactor;
+    const double vSqrMin = 1.e-13;
+    const Geom& G = geomCenter;
+    for (int side = 0; side < 2; side++) {  // right boundary first, then left
+      const bool right = (side == 0);
+      elemBC.set(prim, G);
+      for (int k = 0; k < L.N3T; k++)
+        for (int j = 0; j < L.N2T; j++)
+          for (int gi = 0; gi < ng; gi++) {
+            const int i = right ? N1 + ng + gi : gi;
+            const long z = L.idx(i, j, k);
+            double* U[3] = {&prim.v(U1)[z], &prim.v(U2)[z], &prim.v(U3)[z]};
+            for (int a = 0; a < 3; a++) *U[a] = *U[a] / elemBC.gammaLF[z];
+            if (right) {
+              const long ze = L.idx(N1 + ng - 1, j, k);
+              const double minUr = G.gCon[0][1][ze] * G.alpha[ze];
+              *U[0] = std::max(minUr, *U[0]);
+            } else {
+              *U[0] = std::min(G.gCon[0][1][z] * G.alpha[z], *U[0]);
+            }
+            double vSqr = *U[0] * 0.;
+            for (int a = 0; a < 3; a++)
+              for (int b = 0; b < 3; b++) vSqr += G.gCov[a + 1][b + 1][z] * *U[a] * *U[b];
+            vSqr = std::max(std::min(vSqr, vSqrMax), vSqrMin);
+            const double lf = 1. / std::sqrt(1. - vSqr);
+            for (int a = 0; a < 3; a++) *U[a] = *U[a] * lf;
+          }
+      elemBC.set(prim, G);
+    }
+  }
+
+  /* fixPoles (torus/problem.cpp:1046-1215) */
+  void fixPoles(Grid& prim) {
+    const int ng = L.ng, N2 = L.N2;
+    const Geom& G = geomCenter;
+    for (int pole = 0; pole < 2; pole++) {
+      const bool top = (pole == 1);
+      const int idx0 = top ? N2 + ng - 1 : ng;
+      const int idx1 = top ? idx0 - 1 : ng + 1;
+      const int idx2 = top ? idx0 - 2 : ng + 2;
+      for (int k = 0; k < L.N3T; k++)
+        for (int i = 0; i < L.N1T; i++) {
+          auto at = [&](int v, int j) -> double& { return prim.v(v)[L.idx(i, j, k)]; };
+          auto th = [&](int j) -> double {
+            double t = G.x[1][L.idx(i, j, k)];
+            return top ? t * (-1.) + M_PI : t;
+          };
+          for (int jj : {idx0, idx1}) {
+            at(RHO, jj) = at(RHO, idx2);
+            at(UU, jj) = at(UU, idx2);
+            at(U1, jj) = at(U1, idx2);
+            at(U2, jj) = at(U2, idx2) * th(jj) / th(idx2);
+            at(U3, jj) = at(U3, idx2);
+            if (P.c.conduction) at(P.Q, jj) = at(P.Q, idx2) * th(jj) / th(idx2);
+            if (P.c.viscosity) at(P.DP, jj) = at(P.DP, idx2) * th(jj) / th(idx2);
+          }
+          for (int g = 0; g < ng; g++) {
+            const int dst = top ? N2 + ng + g : ng - 1 - g;
+            const int src = top ? N2 + ng - 1 - g : ng + g;
+            at(RHO, dst) = at(RHO, src);
+            at(UU, dst) = at(UU, src);
+            at(U1, dst) = at(U1, src);
+            at(U3, dst) = at(U3, src);
+            at(U2, dst) = at(U2, src) * (-1.0);
+            at(P.B1, dst) = at(P.B1, src);
+            at(P.B3, dst) = at(P.B3, src);
+            at(P.B2, dst) = at(P.B2, src) * (-1.0);
+            if (P.c.conduction) at(P.Q, dst) = at(P.Q, src) * (-1.0);
+            if (P.c.viscosity) at(P.DP, dst) = at(P.DP, src) * (-1.0);
+          }
+        }
+    }
+  }
+
+  /* setProblemSpecificBCs (torus/problem.cpp:1217-1241) */
+  void setProblemSpecificBCs(Grid& prim) {
+    if (!torus()) return;
+    Elem& e = (currentStep == HALF_STEP) ? elemOld : elemHalfStep;
+    inflowCheck(prim, e);
+    if (L.dim >= 2) fixPoles(prim);
+  }
+
+  /* applyFloor (torus/problem.cpp:542-712) */
+  void applyFloor(Grid& prim, Elem& elem) {
+    const orc_config& c = P.c;
+    const long Z = L.Z;
+    const Geom& G = geomCenter;
+    Arr minRho(Z), minU(Z), rho_pre(Z), u_pre(Z), usefloor(Z), bsq1(Z);
+    double* rho = prim.v(RHO);
+    double* u = prim.v(UU);
+    ZLOOP {
+      minRho[z] = G.minRho[z];
+      minU[z] = G.minU[z];
+      rho_pre[z] = rho[z] * 1.;
+      u_pre[z] = u[z] * 1.;
+      double cd = (rho[z] < minRho[z]) ? 1. : 0.;
+      usefloor[z] = cd;
+      rho[z] = cd * minRho[z] + (1. - cd) * rho[z];
+      cd = (u[z] < minU[z]) ? 1. : 0.;
+      usefloor[z] = std::max(cd, usefloor[z]);
+      u[z] = cd * minU[z] + (1. - cd) * u[z];
+    }
+    elem.set(prim, G);
+    ZLOOP {
+      const double bSqr = elem.bSqr[z];
+      bsq1[z] = bSqr;
+      double cd = (bSqr > c.BsqrOverRhoMax * rho[z]) ? 1. : 0.;
+      usefloor[z] = std::max(cd, usefloor[z]);
+      rho[z] = rho[z] * (1. - cd) + cd * bSqr / c.BsqrOverRhoMax;
+      cd = (bSqr > c.BsqrOverUMax * u[z]) ? 1. : 0.;
+      usefloor[z] = std::max(cd, usefloor[z]);
+      u[z] = u[z] * (1. - cd) + cd * bSqr / c.BsqrOverUMax;
+    }
+    ZLOOP {
+      const double bSqr = bsq1[z];
+      const double zero = usefloor[z] * 0.;
+      const double trans = std::max(std::min(zero + 1., (bSqr - 0.1 * rho[z]) / rho[z]), zero) *
+                           ((usefloor[z] > zero) ? 1. : 0.);
+      const double betapar = -elem.bCon[0][z] / bSqr / elem.uCon[0][z];
+      double betasqr = betapar * betapar * bSqr;
+      const double betasqrmax = 1. - 1. / c.MaxLorentzFactor / c.MaxLorentzFactor;
+      betasqr = std::min(betasqr, betasqrmax);
+      const double gamma = 1. / std::sqrt(1. - betasqr);
+      double ucondr[4];
+      for (int m = 0; m < 4; m++) ucondr[m] = gamma * (elem.uCon[m][z] + betapar * elem.bCon[m][z]);
+      const double Bcon[4] = {zero, prim.v(P.B1)[z], prim.v(P.B2)[z], prim.v(P.B3)[z]};
+      double Bcov[4];
+      for (int m = 0; m < 4; m++) {
+        Bcov[m] = zero;
+        for (int n = 0; n < 4; n++) Bcov[m] += G.gCov[n][m][z] * Bcon[n];
+      }
+      double udotB = zero, bSqr_fl = zero;
+      for (int n = 0; n < 4; n++) {
+        udotB += Bcov[n] * elem.uCon[n][z];
+        bSqr_fl += Bcov[n] * Bcon[n];
+      }
+      double bNorm = std::sqrt(bSqr_fl);
+      const double bMin = std::sqrt(c.bSqrFloorInFluidElement);
+      bNorm = std::max(bNorm, bMin);
+      const double wold = rho_pre[z] + u_pre[z] * c.adiabaticIndex;
+      const double QdotB = udotB * wold * elem.uCon[0][z];
+      const double wnew = rho[z] + u[z] * c.adiabaticIndex;
+      const double x = 2. * QdotB / (bNorm * wnew * ucondr[0]);
+      const double vpar = x / (ucondr[0] * (1. + std::sqrt(1. + x * x)));
+      const double inv = 1. / ucondr[0];
+      double vcon[4];
+      vcon[0] = zero + 1.;
+      for (int m = 1; m < 4; m++) vcon[m] = vpar * Bcon[m] / bNorm + ucondr[m] * inv;
+      double vsqr = zero;
+      for (int m = 0; m < 4; m++)
+        for (int n = 0; n < 4; n++) vsqr += G.gCov[m][n][z] * vcon[m] * vcon[n];
+      const double cv = (vsqr >= 0. || vsqr < 1. / G.gCon[0][0][z]) ? 1. : 0.;
+      vsqr = (1. - cv) * vsqr + cv / G.gCon[0][0][z];
+      const double ut = std::sqrt(-1. / vsqr);
+      for (int m = 1; m < 4; m++) {
+        const double utcon = ut * (vcon[m] - G.gCon[0][m][z] / G.gCon[0][0][z]);
+        prim.v(UU + m)[z] = prim.v(UU + m)[z] * (1. - trans) + trans * utcon;
+      }
+    }
+    elem.set(prim, G);
+    const double gm2 = c.MaxLorentzFactor * c.MaxLorentzFactor;
+    ZLOOP {
+      const double lf2 = elem.gammaLF[z] * elem.gammaLF[z];
+      if (lf2 > gm2) {
+        double mf = std::sqrt(std::max((lf2 - 1.) / (gm2 - 1.), 1.));
+        mf = 1. / mf;
+        prim.v(U1)[z] *= mf;
+        prim.v(U2)[z] *= mf;
+        prim.v(U3)[z] *= mf;
+      }
+    }
+    elem.set(prim, G);
+    if (c.conduction) {
+      ZLOOP {
+        const double Qmax = 1.07 * c.ConductionClosureFactor * rho[z] * std::pow(elem.soundSpeed[z], 3.);
+        const double lim = std::max(std::fabs(elem.q[z]) / Qmax, 1.);
+        prim.v(P.Q)[z] = prim.v(P.Q)[z] / lim;
+      }
+    }
+    if (c.viscosity) {
+      ZLOOP {
+        const double pr = elem.pressure[z], dP = elem.deltaP[z], bs = elem.bSqr[z];
+        const double dPmod = std::max(pr - 2. / 3. * dP, 0.01 * c.bSqrFloorInFluidElement) /
+                             std::max(pr + 1. / 3. * dP, c.bSqrFloorInFluidElement);
+        const double dPmaxPlus = std::min(1.07 * c.ViscosityClosureFactor * bs * 0.5 * dPmod, 1.49 * pr);
+        const double dPmaxMinus = std::max(-1.07 * c.ViscosityClosureFactor * bs, -2.99 * pr);
+        const double cd = (dP > 0.) ? 1. : 0.;
+        prim.v(P.DP)[z] = prim.v(P.DP)[z] * (cd / std::max(dP / dPmaxPlus, 1.) +
+                                             (1. - cd) / std::max(dP / dPmaxMinus, 1.));
+      }
+    }
+    if (c.conduction || c.viscosity) elem.set(prim, G);
+  }
+
+  /* NaN reset of fullStepDiagnostics (torus/problem.cpp:725-744) */
+  void nanReset(Grid& prim) {
+    long bad = 0;
+    for (long z = 0; z < L.Z; z++) {
+      if (!L.interior(z)) continue;
+      for (int v = 0; v < P.dof; v++) if (std::isnan(prim.v(v)[z])) { bad++; break; }
+    }
+    if (bad == 0) return;
+    for (long z = 0; z < L.Z; z++) {
+      bool isn = false;
+      for (int v = 0; v < P.dof; v++) isn |= std::isnan(prim.v(v)[z]);
+      if (isn) for (int v = 0; v < P.dof; v++) prim.v(v)[z] = 0.;
+    }
+  }
+
+  void halfStepDiagnostics() {
+    if (torus()) applyFloor(primHalfStep, elemHalfStep);
+  }
+  void fullStepDiagnostics() {
+    if (torus()) {
+      nanReset(primOld);
+      applyFloor(primOld, elemOld);
+    } else if (P.c.elemOldFromFullStep) {
+      /* linear_modes/problem.cpp:287 */
+      elemOld.set(primOld, geomCenter);
+    }
+  }
+  /* the tail of the torus initialConditions (problem.cpp:525-540) */
+  void problemInit() {
+    if (!torus()) return;
+    applyFloor(primOld, elemOld);
+    fullStepDiagnostics();
+  }
 
   /* residual.cpp:3-180 */
   void computeResidual(const Grid& primGuess, Grid& res) {
@@ -1354,14 +1610,13 @@ struct Stepper {
     lastIters[0] = solve(prim);
     copyVars(prim, primHalfStep, dof);
     communicate(primHalfStep.d.data(), dof);
-    /* halfStepDiagnostics: none for the problems the oracle models */
+    halfStepDiagnostics();
     stageSetup(FULL_STEP);
     lastIters[1] = solve(prim);
     copyVars(prim, primOld, dof);
     communicate(primOld.d.data(), dof);
     time += dt;
-    /* fullStepDiagnostics: linear_modes/problem.cpp:287 resets elemOld */
-    if (P.c.elemOldFromFullStep) elemOld.set(primOld, geomCenter);
+    fullStepDiagnostics();
   }
 };
 
@@ -1428,7 +1683,13 @@ int orc_geometry(const orc_handle* h, int location, double* out, double* gamma, 
   if (gamma && g->hasGamma)
     for (int a = 0; a < 4; a++) for (int b = 0; b < 4; b++) for (int c = 0; c < 4; c++)
       std::memcpy(gamma + (size_t)(a * 16 + b * 4 + c) * Z, g->gamma[a][b][c].data(), sizeof(double) * Z);
-  if (xc) for (int d = 0; d < 3; d++) std::memcpy(xc + (size_t)d * Z, g->x[d].data(), sizeof(double) * Z);
+  if (xc) {
+    std::memcpy(xc, g->x[0].data(), sizeof(double) * Z);
+    std::memcpy(xc + Z, g->x[1].data(), sizeof(double) * Z);
+    std::memcpy(xc + 2 * Z, g->dyn.data(), sizeof(double) * Z);
+    std::memcpy(xc + 3 * Z, g->minRho.data(), sizeof(double) * Z);
+    std::memcpy(xc + 4 * Z, g->minU.data(), sizeof(double) * Z);
+  }
   return 0;
 }
 int orc_div_fluxes(orc_handle* h, const double* prim, double* divF, double* fluxes, double* emf) {
@@ -1510,6 +1771,7 @@ int orc_batch_solve(int n, int batch, const double* A, const double* b, double* 
   return 0;
 }
 int orc_last_newton_stats(const orc_handle* h, int* a, int* b) { *a = h->s.lastIters[0]; *b = h->s.lastIters[1]; return 0; }
+int orc_problem_init(orc_handle* h) { h->s.problemInit(); return 0; }
 int orc_set_threads(int n) {
 #ifdef _OPENMP
   omp_set_num_threads(n);

@@ -77,7 +77,8 @@ int  orc_compute_dt(orc_handle* h);
 int  orc_apply_boundaries(const orc_handle* h, double* prim, int nv);
 
 /* geometry at a location (0 CENTER, 1 LEFT, 2 RIGHT, 3 TOP, 4 BOTTOM):
- * out = [16 gCov | 16 gCon | g | alpha] x Z,  gamma = 64 x Z (center only) */
+ * out = [16 gCov | 16 gCon | g | alpha] x Z,  gamma = 64 x Z (center only),
+ * xcoords = [x1 | x2 | x1^1.5 | radial rho floor | radial u floor] x Z */
 int  orc_geometry(const orc_handle* h, int location, double* out, double* gamma,
                   double* xcoords);
 
@@ -108,6 +109,9 @@ int  orc_batch_solve(int n, int batch, const double* A, const double* b, double*
 
 /* per-call statistics of the last Newton solves */
 int  orc_last_newton_stats(const orc_handle* h, int* iters_half, int* iters_full);
+
+/* the problem's tail of initialConditions (torus: floors + diagnostics) */
+int  orc_problem_init(orc_handle* h);
 
 int  orc_set_threads(int n);
 

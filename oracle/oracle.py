@@ -90,6 +90,7 @@ def lib():
         L.orc_batch_solve.argtypes = [i, i, P(d), P(d), P(d)]
         L.orc_last_newton_stats.argtypes = [vp, P(i), P(i)]
         L.orc_set_threads.argtypes = [i]
+        L.orc_problem_init.argtypes = [vp]
         _LIB = L
     return _LIB
 
@@ -196,7 +197,7 @@ class Oracle:
         Z = self.N1T * self.N2T * self.N3T
         out = np.zeros((34,) + self.zshape)
         gam = np.zeros((64,) + self.zshape)
-        xc = np.zeros((3,) + self.zshape)
+        xc = np.zeros((5,) + self.zshape)
         lib().orc_geometry(self._h, int(location), _ptr(out), _ptr(gam), _ptr(xc))
         return dict(gCov=out[:16].reshape((4, 4) + self.zshape),
                     gCon=out[16:32].reshape((4, 4) + self.zshape),
@@ -245,6 +246,9 @@ class Oracle:
         J = np.zeros((Z, self.nf, self.nf))
         lib().orc_jacobian_fd(self._h, _ptr(p), _ptr(J))
         return J.reshape(self.zshape + (self.nf, self.nf))
+
+    def problem_init(self):
+        lib().orc_problem_init(self._h)
 
     def newton(self):
         it = ctypes.c_int()

@@ -47,3 +47,21 @@ def test_oracle_struct_matches_product_struct():
 def test_version_string():
     L = _lib.lib()
     assert b"sm_100a" in L.grim_version()
+
+
+def _build_cpp_driver(tmp_path):
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "driver")
+    cmd = ["g++", "-std=c++17", "-O1", "-I", os.path.join(root, "include"),
+           os.path.join(root, "tests", "cpp", "driver.cpp"), "-L", os.path.dirname(_lib.LIB_PATH),
+           "-lgrim_b200", "-Wl,-rpath," + os.path.dirname(_lib.LIB_PATH), "-o", exe]
+    subprocess.check_call(cmd)
+    return exe
+
+
+def test_cpp_facade_compiles_and_links(tmp_path):
+    """The reference-shaped C++ facade (include/grim_b200_timestepper.hpp)
+    builds and links against the library with a plain C++ compiler."""
+    exe = _build_cpp_driver(tmp_path)
+    assert os.path.exists(exe)
