@@ -1,7 +1,7 @@
 """Benchmark of the implicit GRMHD timestep: zone-cycles/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload orszag_tang|torus|fast_mode|emhd_stratified]
+                    [--workload torus|orszag_tang|fast_mode|emhd_stratified]
 
 One JSON line on rank 0.  ``value`` is the zone-cycles/s of the product's
 fast Newton form (forward-tangent Jacobian, FP32 Jacobian/solve refined by
@@ -39,8 +39,23 @@ RTOL = 1e-10
 ATOL = 1e-24
 
 
-def workload(name):
-    """(config, prims, description) of a named workload"""
+def workload(name, grid=None):
+    """(config, prims, description) of a named workload; grid "N1xN2xN3"
+    (torus) or "N" (2D workloads) overrides the size, for small profiler
+    captures of the same set-up"""
+    dims = [int(x) for x in grid.split("x")] if grid else None
+    if dims and name != "torus":
+        n = dims[0]
+        if name == "orszag_tang":
+            cfg = PR.orszag_tang_config(N=n, nonlinearsolve_atol=ATOL, nonlinearsolve_rtol=RTOL, maxNonLinearIter=4)
+            return cfg, PR.orszag_tang_prims(cfg), "2D Orszag-Tang %dx%d" % (n, n)
+        if name == "fast_mode":
+            cfg = PR.fast_mode_config(N=n, nonlinearsolve_atol=ATOL, nonlinearsolve_rtol=RTOL, maxNonLinearIter=4)
+            return cfg, PR.fast_mode_prims(cfg), "2D fast mode %dx%d" % (n, n)
+        if name == "emhd_stratified":
+            cfg = PR.emhd_stratified_config(N=n, nonlinearsolve_atol=ATOL, nonlinearsolve_rtol=RTOL,
+                                            maxNonLinearIter=4)
+            return cfg, PR.emhd_stratified_prims(cfg), "2D EMHD %dx%d" % (n, n)
     if name == "orszag_tang":
         cfg = PR.orszag_tang_config(N=512, nonlinearsolve_atol=ATOL, nonlinearsolve_rtol=RTOL,
                                     maxNonLinearIter=4)
@@ -54,9 +69,10 @@ def workload(name):
         return cfg, PR.emhd_stratified_prims(cfg), "2D EMHD 256x256 (dof 10), MP5, HLL, tau(y) closure"
     if name == "torus":
         from grim_b200.problems import torus as T
-        cfg = T.torus_config(N1=256, N2=128, N3=64, nonlinearsolve_atol=ATOL, nonlinearsolve_rtol=RTOL)
-        return cfg, None, ("3D Fishbone-Moncrief torus in MKS, a=0.9375, r_in=6, r_max=12, 256x128x64, "
-                           "PPM, LLF, flux-CT, floors, ideal MHD (dof 8)")
+        n1, n2, n3 = dims if dims else (256, 128, 64)
+        cfg = T.torus_config(N1=n1, N2=n2, N3=n3, nonlinearsolve_atol=ATOL, nonlinearsolve_rtol=RTOL)
+        return cfg, None, ("3D Fishbone-Moncrief torus in MKS, a=0.9375, r_in=6, r_max=12, %dx%dx%d, "
+                           "PPM, LLF, flux-CT, floors, ideal MHD (dof 8)" % (n1, n2, n3))
     raise SystemExit("unknown workload %s" % name)
 
 
@@ -150,11 +166,126 @@ def cpu_reference(cfg, P, seconds=15.0, threads=None):
         steps, cfg["N1"], cfg["N2"], cfg["N3"], el)
 
 
+def profile_path(ts, steps, flush):
+    """Per kernel group device time (CUDA events on the stepper's stream
+    around each launch, graph off, L2 flushed between steps), the Newton
+    iteration histogram of every profiled step and the algorithmic flop
+    counts of one zone."""
+    import torch
+    stream = torch.cuda.ExternalStream(ts.stream())
+    tot = {}
+    hist = [[0] * 16, [0] * 16]
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(2.0)
+        p = ts.profileSteps(1)
+        for g, (ms, n) in p.items():
+            a = tot.setdefault(g, [0.0, 0])
+            a[0] += ms
+            a[1] += n
+        h = ts.newtonHistogram()
+        for st in range(2):
+            for k in range(16):
+                hist[st][k] += h[st][k]
+    return {"steps": steps, "groups": tot, "hist": hist, "flops": ts.countFlops(), "nf": ts.numFluidVars, "dof": ts.dof,
+            "maxIter": ts.cfg["maxNonLinearIter"], "mode": ts.cfg["newtonMode"]}
+
+
+def stencil_bytes_per_zone(cfg, dof, nf):
+    """Algorithmic HBM bytes of one zone's stencil (all face kernels + the
+    epilogue of one stage): the primitives in, the stage constants and the
+    new B out, and the stored geometry words the reconstruction/Riemann/
+    source terms need (22 per face location x 3, 40 Christoffels); none for
+    Minkowski, whose metric is a compile-time constant."""
+    G = 0 if cfg["metric"] == C.MINKOWSKI else 3 * 22 + 40
+    return 8 * (dof + nf + 3 + G)
+
+
+def newton_flops(prof):
+    """(fp64, fp32) algorithmic flops of the profiled steps' Newton kernels.
+    Fast form, per zone: one residual at entry, then per iteration one
+    tangent pass and pivoted solve (FP32 in the mixed form) and one
+    line-search residual, which is also the next convergence test.  FD form
+    (reference method), per zone and iteration: residual + nf FD columns
+    (nf + 1 residuals), an FP64 solve and one line-search residual."""
+    f, nf = prof["flops"], prof["nf"]
+    zone_its = sum(k * n for st in prof["hist"] for k, n in enumerate(st))
+    zones = sum(n for st in prof["hist"] for n in st)
+    if prof["mode"] == C.NEWTON_PARITY_FD64:
+        return None
+    if prof["mode"] == C.NEWTON_MIXED32:
+        f64 = zones * f["residual64"] + zone_its * f["residual64"]
+        f32 = zone_its * (f["tangent32"] + f["solve32"])
+    else:
+        f64 = zones * f["residual64"] + zone_its * (f["residual64"] + f["tangent64"] + f["solve64"])
+        f32 = 0.0
+    return f64, f32
+
+
+def rooflines(cfg, prof, prof_fd, device):
+    """The roofline object of the dominant kernel group and the same figures
+    for the other groups."""
+    from grim_b200.timestepper import measurePeaks
+    fp64_peak, fp32_peak, hbm_local = measurePeaks(device)
+    with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+        hbm_peak = float(json.load(fh)["hbm_gbs"])
+    zones = cfg["N1"] * cfg["N2"] * cfg["N3"]
+    steps = prof["steps"]
+    g = prof["groups"]
+    stencil_ms = sum(g[k][0] for k in ("faces_x1", "faces_x2", "faces_x3", "epilogue", "emhd_prepass"))
+    stencil_launches = g["epilogue"][1]  # one epilogue per stage
+    B = stencil_bytes_per_zone(cfg, prof["dof"], prof["nf"])
+    stencil_gbs = B * zones * stencil_launches / (stencil_ms * 1e-3) / 1e9 if stencil_ms > 0 else None
+    f64, f32 = newton_flops(prof)
+    newton_ms, newton_launches = g["newton"]
+    n64 = f64 / (newton_ms * 1e-3) / 1e12
+    n32 = f32 / (newton_ms * 1e-3) / 1e12
+    pipe_frac = (n64 / fp64_peak) + (n32 / fp32_peak)
+    traffic = _ncu_traffic(cfg)
+    newton = {"bound": "fp64", "achieved": n64, "peak": fp64_peak, "unit": "TFLOP/s", "frac": n64 / fp64_peak,
+              "fp32_achieved": n32, "fp32_peak": fp32_peak, "fp32_frac": n32 / fp32_peak,
+              "pipe_time_frac": pipe_frac,
+              "traffic": traffic.get("newton"),
+              "kernel": "newton (one launch per stage)", "ms_per_launch": newton_ms / newton_launches,
+              "flops_per_zone": prof["flops"],
+              "peak_source": "measured: FMA-chain self-test of this GPU (grim_measure_peaks)"}
+    stencil = {"bound": "hbm", "achieved": stencil_gbs, "peak": hbm_peak, "unit": "GB/s",
+               "frac": (stencil_gbs / hbm_peak) if stencil_gbs else None,
+               "traffic": traffic.get("stencil"),
+               "kernel": "stencil (face fluxes x%d + epilogue, per stage)" % cfg["dim"],
+               "ms_per_launch": stencil_ms / stencil_launches, "bytes_per_zone": B,
+               "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)", "hbm_selftest_gbs": hbm_local}
+    total = sum(v[0] for v in g.values())
+    shares = {k: round(v[0] / total, 4) for k, v in g.items() if v[0] > 0}
+    dominant = newton if g["newton"][0] >= stencil_ms else stencil
+    out = {"roofline": dict(dominant), "roofline_other": stencil if dominant is newton else newton,
+           "kernel_shares": shares, "profiled_ms_per_step": total / steps}
+    if prof_fd is not None:
+        gf = prof_fd["groups"]
+        tf = sum(v[0] for v in gf.values())
+        out["fd64_kernel_shares"] = {k: round(v[0] / tf, 4) for k, v in gf.items() if v[0] > 0}
+    return out
+
+
+def _ncu_traffic(cfg):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    of the workload's kernel groups from the committed ncu summary, when
+    one exists for this grid."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            table = json.load(fh)
+    except (OSError, ValueError):
+        return {}
+    key = "%dx%dx%d" % (cfg["N1"], cfg["N2"], cfg["N3"])
+    return table.get(key, {})
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     torch.cuda.set_device(local_rank)
     from grim_b200.timestepper import timeStepper
-    cfg, P, desc = workload(args.workload)
+    cfg, P, desc = workload(args.workload, args.grid)
     zones = cfg["N1"] * cfg["N2"] * cfg["N3"]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -193,7 +324,13 @@ def run_gpu(args, rank, world, local_rank):
     clocks.start()
     ts_fast, ms_fast, st_fast = time_path(C.NEWTON_MIXED32, True)
     clocks_info = clocks.stop()
-    _, ms_fd, st_fd = time_path(C.NEWTON_PARITY_FD64, True)
+    prof_fast = profile_path(ts_fast, args.steps, flush)
+    if args.no_fd:
+        ms_fd, st_fd, prof_fd = float("nan"), {"newtonIters": None, "unconverged": None}, None
+    else:
+        ts_fd, ms_fd, st_fd = time_path(C.NEWTON_PARITY_FD64, True)
+        prof_fd = profile_path(ts_fd, max(3, args.steps // 4), flush)
+        del ts_fd
 
     # e2e: the C-ABI call with host buffers, copies inside the timed region
     import ctypes
@@ -219,7 +356,7 @@ def run_gpu(args, rank, world, local_rank):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
     ms_fast, ms_fd, e2e_s = [float(x) for x in t.tolist()]
     value = world * zones * args.steps / (ms_fast / 1e3)
-    fd = world * zones * args.steps / (ms_fd / 1e3)
+    fd = world * zones * args.steps / (ms_fd / 1e3) if ms_fd == ms_fd else None
     out = {
         "metric": METRIC,
         "value": value,
@@ -240,7 +377,7 @@ def run_gpu(args, rank, world, local_rank):
                    "parallelism": "replicas" if world > 1 else "single GPU", "cuda_graph": True},
         "fd64": {"value": fd, "ms_per_step": ms_fd / args.steps, "newton_iters": st_fd["newtonIters"],
                  "unconverged": st_fd["unconverged"]},
-        "speedup_vs_fd64": value / fd,
+        "speedup_vs_fd64": value / fd if fd else None,
         "newton_iters": st_fast["newtonIters"],
         "unconverged": st_fast["unconverged"],
         "e2e": {"value": world * zones * e2e_steps / e2e_s, "unit": "zone-cycles/s",
@@ -248,6 +385,7 @@ def run_gpu(args, rank, world, local_rank):
         "gpu_launches": int(st_fast["kernelLaunches"]) * args.steps,
         "clocks": clocks_info,
     }
+    out.update(rooflines(cfg, prof_fast, prof_fd, local_rank))
     return out, cfg, state["P"]
 
 
@@ -257,8 +395,10 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="grim_b200")
-    ap.add_argument("--workload", default="orszag_tang")
+    ap.add_argument("--workload", default="torus")
+    ap.add_argument("--grid", default=None, help="override the workload size: N1xN2xN3 (torus) or N")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fd", action="store_true", help="skip the FD64 comparison path (profiler captures)")
     ap.add_argument("--per-zone", type=int, default=1,
                     help="fast Newton: 1 = per-zone loop in one kernel, 2 = compacted worklists")
     args = ap.parse_args()
@@ -269,7 +409,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        cfg, P, desc = workload(args.workload)
+        cfg, P, desc = workload(args.workload, args.grid)
         cfg = cpu_sample_config(args.workload, cfg)
         vals = []
         for _ in range(max(1, args.steps // 10)):

@@ -88,6 +88,8 @@ def lib():
         "grim_problem_init": [vp],
         "grim_get_newton_histogram": [vp, P(ctypes.c_longlong)],
         "grim_measure_peaks": [i, P(d), P(d), P(d)],
+        "grim_profile_steps": [vp, i, P(d), P(ctypes.c_longlong), i],
+        "grim_count_flops": [vp, P(d)],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -223,40 +223,57 @@ __global__ void __launch_bounds__(128) k_face_flux_x1(DevCfg c, const double* __
   riemann_face<COND, VISC>(c, 0, pl, lo, G, G, flux, z);
 }
 
-// X2 / X3 faces: thread (i, slab) marches `span` faces along dir
+// X2 / X3 faces: a 32 x 8 thread block reconstructs 8 consecutive zones
+// along dir for 32 consecutive i (each zone once, loads coalesced along i)
+// into shared memory, then 7 of its warps compute the 7 faces between them.
+constexpr int kTileRows = 8;
 template <int COND, int VISC>
-__global__ void __launch_bounds__(128) k_face_flux_march(DevCfg c, int dir, int span, const double* __restrict__ ps,
-                                                         const double* __restrict__ geoF,
-                                                         const double* __restrict__ geoC, double* __restrict__ flux) {
+__global__ void __launch_bounds__(256) k_face_flux_tile(DevCfg c, int dir, const double* __restrict__ ps,
+                                                        const double* __restrict__ geoF,
+                                                        const double* __restrict__ geoC, double* __restrict__ flux) {
   constexpr int DOF = 8 + COND + VISC;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= c.N1T) return;
+  extern __shared__ double sm_recon[];  // [row][var][lane] lo, then ro
+  double* sLo = sm_recon;
+  double* sRo = sm_recon + kTileRows * DOF * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int i = blockIdx.x * 32 + tx;
   const int NT = (dir == 1) ? c.N2T : c.N3T;
   const int other = blockIdx.z;  // k for X2 faces, j for X3 faces
-  const int f0 = 3 + blockIdx.y * span;
-  const int f1 = min(f0 + span, NT - 2);  // faces f0 .. f1-1 (<= NT-3)
-  if (f0 >= f1) return;
+  const int x0 = 3 + blockIdx.y * (kTileRows - 1);  // first face of the tile
+  const int xr = x0 - 1 + ty;                       // zone this thread reconstructs
   const long long s = stride_of(c, dir);
   auto zof = [&](int x) -> long long { return dir == 1 ? zidx(c, i, x, other) : zidx(c, i, other, x); };
-  double lo[DOF], ro[DOF], pl[DOF];
-  recon_zone<DOF>(c, ps, zof(f0 - 1), s, c.reconstruction, lo, pl);
-  for (int x = f0; x < f1; x++) {
-    const long long z = zof(x);
-    recon_zone<DOF>(c, ps, z, s, c.reconstruction, lo, ro);
-    ZoneGeo<double> GL, GR;
-    const int jj = (dir == 1) ? x : other;
-    if (dir == 2) {
-      // X3 faces use the centre geometry of each side (fvmfluxes.cpp:150-151)
-      load_geo(GL, c, geoC, z - s, i, jj, 0.5, 0.5);
-      load_geo(GR, c, geoC, z, i, jj, 0.5, 0.5);
-    } else {
-      load_geo(GL, c, geoF, z, i, jj, 0.5, 0.);
-      GR = GL;
-    }
-    riemann_face<COND, VISC>(c, dir, pl, lo, GL, GR, flux, z);
+  const bool reconOK = i < c.N1T && xr <= NT - 3;
+  if (reconOK) {
+    double lo[DOF], ro[DOF];
+    recon_zone<DOF>(c, ps, zof(xr), s, c.reconstruction, lo, ro);
 #pragma unroll
-    for (int v = 0; v < DOF; v++) pl[v] = ro[v];
+    for (int v = 0; v < DOF; v++) {
+      sLo[(ty * DOF + v) * 32 + tx] = lo[v];
+      sRo[(ty * DOF + v) * 32 + tx] = ro[v];
+    }
   }
+  __syncthreads();
+  if (ty == 0 || !reconOK) return;
+  // face xr (between zones xr-1 and xr)
+  double pl[DOF], pr[DOF];
+#pragma unroll
+  for (int v = 0; v < DOF; v++) {
+    pl[v] = sRo[((ty - 1) * DOF + v) * 32 + tx];
+    pr[v] = sLo[(ty * DOF + v) * 32 + tx];
+  }
+  const long long z = zof(xr);
+  ZoneGeo<double> GL, GR;
+  const int jj = (dir == 1) ? xr : other;
+  if (dir == 2) {
+    // X3 faces use the centre geometry of each side (fvmfluxes.cpp:150-151)
+    load_geo(GL, c, geoC, z - s, i, jj, 0.5, 0.5);
+    load_geo(GR, c, geoC, z, i, jj, 0.5, 0.5);
+  } else {
+    load_geo(GL, c, geoF, z, i, jj, 0.5, 0.);
+    GR = GL;
+  }
+  riemann_face<COND, VISC>(c, dir, pl, pr, GL, GR, flux, z);
 }
 
 // ---------------------------------------------------------------------------
@@ -627,6 +644,15 @@ GRIM_D void gauss_solve(T A[N][N], T b[N], T x[N]) {
   }
 }
 
+// histogram of per-zone iteration counts, one atomic per distinct value in
+// a warp
+GRIM_D void hist_add(unsigned long long* hist, int bin, bool active) {
+  const unsigned act = __ballot_sync(0xffffffffu, active);
+  if (!active) return;
+  const unsigned peers = __match_any_sync(act, bin);
+  if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[bin], (unsigned long long)__popc(peers));
+}
+
 template <int NF>
 GRIM_D double l2sum(const double* R) {
   double s = 0.;
@@ -845,9 +871,9 @@ __global__ void __launch_bounds__(128) k_newton_fast(DevCfg c, int stage, StageB
       if (!(l2 >= 0. && l2 <= fmax(c.atol, c.rtol * c.rtol * l2first))) unconv = 1;
     }
     itsMax = it;
-    atomicAdd(&b.st->itHist[stage][min(it, 15)], 1ULL);
     for (int v = 0; v < NF; v++) b.prim[(long long)v * Z + z] = P[v];
   }
+  hist_add(b.st->itHist[stage], min(itsMax, 15), n < nlist);
   unconv = __syncthreads_count(unconv);
   // iterations done: max over zones (warp max then atomic)
   for (int o = 16; o > 0; o >>= 1) itsMax = max(itsMax, __shfl_xor_sync(0xffffffffu, itsMax, o));
@@ -901,8 +927,8 @@ __global__ void __launch_bounds__(128) k_newton_list_init(DevCfg c, int stage, S
       for (int v = 0; v < NF; v++) b.R[(long long)v * Z + z] = R[v];
       b.l2[Z + z] = l2;
       take = l2 > fmax(c.atol, c.rtol * c.rtol * l2);
-      if (!take) atomicAdd(&b.st->itHist[stage][0], 1ULL);
     }
+    hist_add(b.st->itHist[stage], 0, n < c.Zint && !take);
     list_append(b.list[0], &b.st->listCount[0], (int)z, take);
   }
 }
@@ -968,16 +994,13 @@ __global__ void __launch_bounds__(128) k_newton_list_iter(DevCfg c, int stage, i
       const double l2n = l2sum<NF>(Rt);
       const bool conv = l2n <= fmax(c.atol, c.rtol * c.rtol * l2first);
       take = !conv && !last;
-      if (conv) atomicAdd(&b.st->itHist[stage][min(it, 15)], 1ULL);
-      else if (last) {
-        atomicAdd(&b.st->itHist[stage][min(it, 15)], 1ULL);
-        atomicAdd(&b.st->finalUnconv[stage], 1ULL);
-      }
+      if (!conv && last) atomicAdd(&b.st->finalUnconv[stage], 1ULL);
       for (int v = 0; v < NF; v++) {
         b.prim[(long long)v * Z + z] = P[v];
         b.R[(long long)v * Z + z] = Rt[v];
       }
     }
+    hist_add(b.st->itHist[stage], min(it, 15), n < count && !take);
     if (!last) list_append(b.list[out], &b.st->listCount[out], zone, take);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && count > 0) atomicMax(&b.st->itersDone[stage], (unsigned long long)it);
@@ -1172,7 +1195,6 @@ void emhd_prepass(const DevCfg& c, const double* ps, const double* geoC, double*
   GRIM_EMHD_DISPATCH(c, emhd_prepass_t, c, ps, geoC, uT, s);
 }
 
-constexpr int kMarchSpan = 16;
 template <int C, int V>
 static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,
                         double* flux, cudaStream_t s) {
@@ -1182,12 +1204,10 @@ static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double
   } else {
     const int NT = (dir == 1) ? c.N2T : c.N3T;
     const int other = (dir == 1) ? c.N3T : c.N2T;
-    // march length: long enough to amortise the extra reconstruction, short
-    // enough to leave ~150k threads in flight
-    const long long faces = (long long)c.N1T * other * (NT - 5);
-    const int span = (int)std::max(2LL, std::min((long long)kMarchSpan, faces / (148LL * 1024)));
-    dim3 grid(nblk(c.N1T, 128), (unsigned)((NT - 5 + span - 1) / span), (unsigned)other);
-    k_face_flux_march<C, V><<<grid, 128, 0, s>>>(c, dir, span, ps, geoF, geoC, flux);
+    constexpr int DOF = 8 + C + V;
+    const size_t smem = 2 * kTileRows * DOF * 32 * sizeof(double);
+    dim3 grid(nblk(c.N1T, 32), (unsigned)((NT - 5 + kTileRows - 2) / (kTileRows - 1)), (unsigned)other);
+    k_face_flux_tile<C, V><<<grid, 256, smem, s>>>(c, dir, ps, geoF, geoC, flux);
   }
 }
 void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC, double* flux,

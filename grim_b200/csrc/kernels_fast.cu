@@ -4,3 +4,4 @@
 #define GRIM_FAST_MATH 1
 #include "kernels.cuh"
 #include "launch.h"
+#include "opcount.cuh"

@@ -40,3 +40,10 @@
 
 GRIM_DECLARE_LAUNCHERS(exact)
 GRIM_DECLARE_LAUNCHERS(fast)
+
+namespace grim {
+namespace fast {
+// algorithmic flop counts of one zone's residual / tangent / solve
+void count_ops(const DevCfg& c, int stage, const StageBufs& b, long long z, double* out, cudaStream_t s);
+}  // namespace fast
+}  // namespace grim

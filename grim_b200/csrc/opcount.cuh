@@ -1,0 +1,149 @@
+// opcount.cuh -- algorithmic flop counts of the Newton kernels' building
+// blocks, taken from the code itself: the templated zone physics is
+// instantiated on a counting scalar (Cnt<double> / Cnt<float>) and run for
+// one zone by one thread.  Every add/subtract, multiply, divide, square root
+// and exponential on the counting type is tallied per precision; signs,
+// comparisons, min/max and conversions are not flops and are not counted.
+// The counts feed the FP64/FP32 pipe rooflines of the Newton kernels.
+//
+// Included by kernels_fast.cu only (one definition of the tally).
+#pragma once
+
+namespace grim {
+
+// [precision: 0 fp64, 1 fp32][op: add, mul, div, sqrt, exp]
+__device__ unsigned long long g_op_tally[2][5];
+
+template <class B>
+struct Cnt {
+  B v;
+  static constexpr int P = sizeof(B) == 8 ? 0 : 1;
+  GRIM_HD Cnt() : v(0) {}
+  GRIM_HD Cnt(double x) : v((B)x) {}
+  GRIM_HD Cnt(float x) : v((B)x) {}
+  GRIM_HD Cnt(int x) : v((B)x) {}
+  GRIM_HD explicit operator double() const { return (double)v; }
+  GRIM_HD explicit operator float() const { return (float)v; }
+  static GRIM_D void tick(int op) { g_op_tally[P][op]++; }
+
+  friend GRIM_D Cnt operator+(Cnt a, Cnt b) { tick(0); return Cnt(a.v + b.v); }
+  friend GRIM_D Cnt operator-(Cnt a, Cnt b) { tick(0); return Cnt(a.v - b.v); }
+  friend GRIM_D Cnt operator*(Cnt a, Cnt b) { tick(1); return Cnt(a.v * b.v); }
+  friend GRIM_D Cnt operator/(Cnt a, Cnt b) { tick(2); return Cnt(a.v / b.v); }
+  friend GRIM_D Cnt operator-(Cnt a) { return Cnt(-a.v); }
+  friend GRIM_D Cnt& operator+=(Cnt& a, Cnt b) { a = a + b; return a; }
+  friend GRIM_D Cnt& operator-=(Cnt& a, Cnt b) { a = a - b; return a; }
+  friend GRIM_D Cnt& operator*=(Cnt& a, Cnt b) { a = a * b; return a; }
+  friend GRIM_D Cnt& operator/=(Cnt& a, Cnt b) { a = a / b; return a; }
+  friend GRIM_D bool operator<(Cnt a, Cnt b) { return a.v < b.v; }
+  friend GRIM_D bool operator>(Cnt a, Cnt b) { return a.v > b.v; }
+  friend GRIM_D bool operator<=(Cnt a, Cnt b) { return a.v <= b.v; }
+  friend GRIM_D bool operator>=(Cnt a, Cnt b) { return a.v >= b.v; }
+  friend GRIM_D bool operator==(Cnt a, Cnt b) { return a.v == b.v; }
+  friend GRIM_D bool operator!=(Cnt a, Cnt b) { return a.v != b.v; }
+
+  // the scalar helpers the physics calls (found by argument lookup)
+  friend GRIM_D Cnt val(Cnt a) { return a; }
+  friend GRIM_D Cnt dsqrt(Cnt a) { tick(3); return Cnt(sqrt((double)a.v)); }
+  friend GRIM_D Cnt dexp(Cnt a) { tick(4); return Cnt(exp((double)a.v)); }
+  friend GRIM_D Cnt dfabs(Cnt a) { return Cnt(a.v < B(0) ? -a.v : a.v); }
+  friend GRIM_D Cnt fabs(Cnt a) { return dfabs(a); }
+  friend GRIM_D Cnt dmaxc(Cnt a, Cnt b) { return a.v >= b.v ? a : b; }
+  friend GRIM_D Cnt dmin2(Cnt a, Cnt b) { return a.v <= b.v ? a : b; }
+  friend GRIM_D Cnt dmax2(Cnt a, Cnt b) { return a.v >= b.v ? a : b; }
+  friend GRIM_D Cnt dcube(Cnt a) { return a * a * a; }
+  friend GRIM_D bool isfinite(Cnt a) { return ::isfinite((double)a.v); }
+};
+
+template <class B>
+struct Lift<Cnt<B>> {
+  GRIM_HD static Cnt<B> of(double x) { return Cnt<B>(x); }
+};
+
+namespace GRIM_KNS {
+
+// One thread, one zone z of the stage buffers b (filled by a stage set-up):
+// out = {residual fp64, tangent(fp32) fp32, tangent(fp64) fp64,
+//        solve fp32, solve fp64, residual divides, residual sqrt+exp}
+template <int COND, int VISC>
+__global__ void k_count_ops(DevCfg c, int stage, StageBufs b, long long z, double* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  constexpr int NF = 5 + COND + VISC;
+  const long long Z = c.Z;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  ZoneGeo<double> G;
+  load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
+  StageConst<NF> K;
+  load_stage_const<COND, VISC>(K, c, stage, b, z, G);
+  auto clear = [] {
+    for (int p = 0; p < 2; p++)
+      for (int o = 0; o < 5; o++) g_op_tally[p][o] = 0;
+  };
+  auto flops = [](int p) {
+    return (double)(g_op_tally[p][0] + g_op_tally[p][1] + g_op_tally[p][2] + g_op_tally[p][3] +
+                    g_op_tally[p][4]);
+  };
+  double Pd[NF];
+  for (int v = 0; v < NF; v++) Pd[v] = b.prim[(long long)v * Z + z];
+  // residual, FP64
+  {
+    typedef Cnt<double> C8;
+    ZoneGeo<C8> Gc;
+    for (int m = 0; m < 4; m++)
+      for (int q = 0; q < 4; q++) { Gc.gcov[m][q] = C8(G.gcov[m][q]); Gc.gcon[m][q] = C8(G.gcon[m][q]); }
+    Gc.g = C8(G.g); Gc.alpha = C8(G.alpha); Gc.x1 = C8(G.x1); Gc.x2 = C8(G.x2); Gc.dyn = C8(G.dyn);
+    C8 P[NF], R[NF];
+    for (int v = 0; v < NF; v++) P[v] = C8(Pd[v]);
+    clear();
+    zone_residual<COND, VISC, C8, C8>(P, K, Gc, c, R);
+    out[0] = flops(0);
+    out[5] = (double)g_op_tally[0][2];
+    out[6] = (double)(g_op_tally[0][3] + g_op_tally[0][4]);
+  }
+  // tangent pass in FP32 and in FP64
+  {
+    typedef Cnt<float> C4;
+    ZoneGeo<C4> Gt;
+    for (int m = 0; m < 4; m++)
+      for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = C4(G.gcov[m][q]); Gt.gcon[m][q] = C4(G.gcon[m][q]); }
+    Gt.g = C4(G.g); Gt.alpha = C4(G.alpha); Gt.x1 = C4(G.x1); Gt.x2 = C4(G.x2); Gt.dyn = C4(G.dyn);
+    C4 J[NF][NF];
+    clear();
+    tangent_jacobian<COND, VISC, C4>(Pd, K, Gt, c, J);
+    out[1] = flops(1);
+    C4 bv[NF], xv[NF];
+    for (int v = 0; v < NF; v++) bv[v] = C4(1.0);
+    clear();
+    gauss_solve<C4, NF>(J, bv, xv);
+    out[3] = flops(1);
+  }
+  {
+    typedef Cnt<double> C8;
+    ZoneGeo<C8> Gt;
+    for (int m = 0; m < 4; m++)
+      for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = C8(G.gcov[m][q]); Gt.gcon[m][q] = C8(G.gcon[m][q]); }
+    Gt.g = C8(G.g); Gt.alpha = C8(G.alpha); Gt.x1 = C8(G.x1); Gt.x2 = C8(G.x2); Gt.dyn = C8(G.dyn);
+    C8 J[NF][NF];
+    clear();
+    tangent_jacobian<COND, VISC, C8>(Pd, K, Gt, c, J);
+    out[2] = flops(0);
+    C8 bv[NF], xv[NF];
+    for (int v = 0; v < NF; v++) bv[v] = C8(1.0);
+    clear();
+    gauss_solve<C8, NF>(J, bv, xv);
+    out[4] = flops(0);
+  }
+}
+
+template <int C, int V>
+static void count_ops_t(const DevCfg& c, int stage, const StageBufs& b, long long z, double* out,
+                        cudaStream_t s) {
+  k_count_ops<C, V><<<1, 32, 0, s>>>(c, stage, b, z, out);
+}
+void count_ops(const DevCfg& c, int stage, const StageBufs& b, long long z, double* out, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, count_ops_t, c, stage, b, z, out, s);
+}
+
+}  // namespace GRIM_KNS
+}  // namespace grim

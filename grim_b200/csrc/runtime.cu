@@ -18,6 +18,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "launch.h"
 
@@ -72,7 +73,37 @@ struct grim_handle {
   long long launchesPerStep = 0;
   size_t bytesZ = 0;
   int lastStage = GRIM_HALF_STEP;
+  // per-kernel-group device timing (grim_profile_steps): event pairs
+  // recorded around each launch on the handle's stream
+  bool profOn = false;
+  std::vector<cudaEvent_t> profEv;
+  std::vector<int> profGroup;
+  size_t profUsed = 0;
 };
+
+// brackets one launch (or a run of launches of the same group) with events
+struct ProfScope {
+  grim_handle* h;
+  size_t slot;
+  ProfScope(grim_handle* hh, int group) : h(hh), slot(SIZE_MAX) {
+    if (!h->profOn) return;
+    if (h->profUsed * 2 + 2 > h->profEv.size()) {
+      cudaEvent_t a, b;
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      h->profEv.push_back(a);
+      h->profEv.push_back(b);
+      h->profGroup.push_back(0);
+    }
+    slot = h->profUsed++;
+    h->profGroup[slot] = group;
+    cudaEventRecord(h->profEv[2 * slot], h->stream);
+  }
+  ~ProfScope() {
+    if (slot != SIZE_MAX) cudaEventRecord(h->profEv[2 * slot + 1], h->stream);
+  }
+};
+#define PROF(group) ProfScope prof_scope_(h, group)
 
 static void free_all(grim_handle* h) {
   double** bufs[] = {&h->primOld, &h->prim, &h->primHalf, &h->consOld, &h->divF, &h->Sexp, &h->R,
@@ -85,6 +116,9 @@ static void free_all(grim_handle* h) {
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
   for (int l = 0; l < 2; l++)
     if (h->list[l]) { cudaFree(h->list[l]); h->list[l] = nullptr; }
+  for (cudaEvent_t e : h->profEv) cudaEventDestroy(e);
+  h->profEv.clear();
+  h->profGroup.clear();
 }
 
 static int make_devcfg(const grim_config& c, DevCfg& d) {
@@ -178,11 +212,17 @@ static void enqueue_stencil(grim_handle* h, int stage) {
   const DevCfg& c = h->dc;
   cudaStream_t s = h->stream;
   StageBufs b = stage_bufs(h, stage);
-  if (c.conduction || c.viscosity) { KNS_CALL(h, emhd_prepass, c, b.ps, b.geoC, h->uT, s); g_launch_counter++; }
+  if (c.conduction || c.viscosity) {
+    PROF(GRIM_PROF_EMHD_PREPASS);
+    KNS_CALL(h, emhd_prepass, c, b.ps, b.geoC, h->uT, s);
+    g_launch_counter++;
+  }
   for (int d = 0; d < c.dim; d++) {
+    PROF(GRIM_PROF_FACES_X1 + d);
     KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], s);
     g_launch_counter++;
   }
+  PROF(GRIM_PROF_EPILOGUE);
   KNS_CALL(h, stage_epilogue, c, stage, b, s);
   g_launch_counter++;
 }
@@ -191,6 +231,7 @@ static void enqueue_newton(grim_handle* h, int stage) {
   const DevCfg& c = h->dc;
   cudaStream_t s = h->stream;
   StageBufs b = stage_bufs(h, stage);
+  PROF(GRIM_PROF_NEWTON);
   if (h->cfg.newtonMode == GRIM_NEWTON_PARITY_FD64) {
     grim::exact::newton_fd_init(c, stage, b, s);
     g_launch_counter++;
@@ -209,6 +250,7 @@ static void enqueue_newton(grim_handle* h, int stage) {
 
 static void enqueue_dt_speeds(grim_handle* h, const double* p, int mode) {
   const DevCfg& c = h->dc;
+  PROF(GRIM_PROF_DT);
   cudaMemsetAsync(&h->st->maxInvDt, 0, sizeof(double), h->stream);
   const bool mink = h->cfg.metric == GRIM_MINKOWSKI;
   KNS_CALL(h, dt_speeds, c, p, mink ? nullptr : h->geo[GRIM_CENTER], mode, h->st, h->stream);
@@ -219,18 +261,21 @@ static void enqueue_dt_speeds(grim_handle* h, const double* p, int mode) {
 // stage-start boundary fill (timestep.cpp:17-22, :186-191)
 static void enqueue_problem_bcs(grim_handle* h, double* p) {
   if (h->cfg.problem != GRIM_PROBLEM_TORUS) return;
+  PROF(GRIM_PROF_BOUNDARY);
   KNS_CALL(h, torus_bcs, h->dc, p, h->geo[GRIM_CENTER], h->stream);
   g_launch_counter += 2;
 }
 // halfStepDiagnostics: torus floors on primHalfStep (torus/problem.cpp:714-717)
 static void enqueue_half_diagnostics(grim_handle* h) {
   if (h->cfg.problem != GRIM_PROBLEM_TORUS) return;
+  PROF(GRIM_PROF_DIAGNOSTICS);
   KNS_CALL(h, torus_floor, h->dc, h->primHalf, h->geo[GRIM_CENTER], nullptr, h->stream);
   g_launch_counter++;
 }
 // fullStepDiagnostics: NaN reset + floors on primOld (torus/problem.cpp:719-746)
 static void enqueue_full_diagnostics(grim_handle* h) {
   if (h->cfg.problem != GRIM_PROBLEM_TORUS) return;
+  PROF(GRIM_PROF_DIAGNOSTICS);
   cudaMemsetAsync(&h->st->nanFlag, 0, sizeof(unsigned long long), h->stream);
   KNS_CALL(h, torus_nan_flag, h->dc, h->primOld, &h->st->nanFlag, h->stream);
   KNS_CALL(h, torus_floor, h->dc, h->primOld, h->geo[GRIM_CENTER], &h->st->nanFlag, h->stream);
@@ -243,16 +288,22 @@ static void enqueue_step(grim_handle* h, bool timed) {
   const size_t bytes = (size_t)c.dof * c.Z * sizeof(double);
   if (timed) cudaEventRecord(h->ev[0], s);
   // computeDt (timestep.cpp:8): dt from the last elemOld state
-  KNS_CALL(h, dt_update, h->st, h->cfg.CourantFactor, h->cfg.maxDtIncrement, s);
-  g_launch_counter++;
+  {
+    PROF(GRIM_PROF_DT);
+    KNS_CALL(h, dt_update, h->st, h->cfg.CourantFactor, h->cfg.maxDtIncrement, s);
+    g_launch_counter++;
+  }
   cudaMemsetAsync(h->st->count, 0, sizeof(h->st->count), s);
   cudaMemsetAsync(h->st->itersDone, 0, sizeof(h->st->itersDone), s);
   cudaMemsetAsync(h->st->finalUnconv, 0, sizeof(h->st->finalUnconv), s);
   cudaMemsetAsync(h->st->itHist, 0, sizeof(h->st->itHist), s);
   cudaMemsetAsync(&h->st->nonFinite, 0, sizeof(unsigned long long), s);
   // ---- half stage
-  KNS_CALL(h, ghost_fill, c, h->primOld, c.dof, s);
-  g_launch_counter++;
+  {
+    PROF(GRIM_PROF_BOUNDARY);
+    KNS_CALL(h, ghost_fill, c, h->primOld, c.dof, s);
+    g_launch_counter++;
+  }
   enqueue_problem_bcs(h, h->primOld);
   if (!h->cfg.elemOldFromFullStep) enqueue_dt_speeds(h, h->primOld, 0);
   if (timed) cudaEventRecord(h->ev[1], s);
@@ -260,30 +311,51 @@ static void enqueue_step(grim_handle* h, bool timed) {
   if (timed) cudaEventRecord(h->ev[2], s);
   enqueue_newton(h, GRIM_HALF_STEP);
   if (timed) cudaEventRecord(h->ev[3], s);
-  cudaMemcpyAsync(h->primHalf, h->prim, bytes, cudaMemcpyDeviceToDevice, s);
-  KNS_CALL(h, communicate, c, h->primHalf, c.dof, s);
-  g_launch_counter++;
+  {
+    PROF(GRIM_PROF_COPY);
+    cudaMemcpyAsync(h->primHalf, h->prim, bytes, cudaMemcpyDeviceToDevice, s);
+  }
+  {
+    PROF(GRIM_PROF_BOUNDARY);
+    KNS_CALL(h, communicate, c, h->primHalf, c.dof, s);
+    g_launch_counter++;
+  }
   enqueue_half_diagnostics(h);
   // ---- full stage
-  KNS_CALL(h, ghost_fill, c, h->primHalf, c.dof, s);
-  g_launch_counter++;
+  {
+    PROF(GRIM_PROF_BOUNDARY);
+    KNS_CALL(h, ghost_fill, c, h->primHalf, c.dof, s);
+    g_launch_counter++;
+  }
   enqueue_problem_bcs(h, h->primHalf);
   if (timed) cudaEventRecord(h->ev[4], s);
   enqueue_stencil(h, GRIM_FULL_STEP);
   if (timed) cudaEventRecord(h->ev[5], s);
   enqueue_newton(h, GRIM_FULL_STEP);
   if (timed) cudaEventRecord(h->ev[6], s);
-  cudaMemcpyAsync(h->primOld, h->prim, bytes, cudaMemcpyDeviceToDevice, s);
-  KNS_CALL(h, communicate, c, h->primOld, c.dof, s);
-  g_launch_counter++;
-  grim::exact::advance_time(h->st, s);
-  g_launch_counter++;
+  {
+    PROF(GRIM_PROF_COPY);
+    cudaMemcpyAsync(h->primOld, h->prim, bytes, cudaMemcpyDeviceToDevice, s);
+  }
+  {
+    PROF(GRIM_PROF_BOUNDARY);
+    KNS_CALL(h, communicate, c, h->primOld, c.dof, s);
+    g_launch_counter++;
+  }
+  {
+    PROF(GRIM_PROF_DT);
+    grim::exact::advance_time(h->st, s);
+    g_launch_counter++;
+  }
   enqueue_full_diagnostics(h);
   // fullStepDiagnostics re-setting elemOld (linear_modes/problem.cpp:287)
   // on the communicated primOld
   if (h->cfg.elemOldFromFullStep) enqueue_dt_speeds(h, h->primOld, 0);
-  KNS_CALL(h, count_nonfinite, c, h->primOld, h->st, s);
-  g_launch_counter++;
+  {
+    PROF(GRIM_PROF_DIAGNOSTICS);
+    KNS_CALL(h, count_nonfinite, c, h->primOld, h->st, s);
+    g_launch_counter++;
+  }
   if (timed) cudaEventRecord(h->ev[7], s);
 }
 
@@ -791,6 +863,52 @@ int grim_get_newton_histogram(grim_handle* h, long long* out) {
   CK(cudaStreamSynchronize(h->stream));
   for (int st = 0; st < 2; st++)
     for (int i = 0; i < 16; i++) out[st * 16 + i] = (long long)h->hst->itHist[st][i];
+  return GRIM_OK;
+}
+
+int grim_profile_steps(grim_handle* h, int nsteps, double* msPerGroup, long long* launchesPerGroup,
+                       int ngroups) {
+  if (!h || nsteps < 0 || !msPerGroup || ngroups <= 0) { set_err("grim_profile_steps: bad argument"); return GRIM_EINVAL; }
+  CK(cudaSetDevice(h->device));
+  for (int g = 0; g < ngroups; g++) {
+    msPerGroup[g] = 0.;
+    if (launchesPerGroup) launchesPerGroup[g] = 0;
+  }
+  for (int n = 0; n < nsteps; n++) {
+    h->profOn = true;
+    h->profUsed = 0;
+    long long before = g_launch_counter;
+    enqueue_step(h, false);
+    h->launchesPerStep = g_launch_counter - before;
+    h->profOn = false;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    for (size_t k = 0; k < h->profUsed; k++) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, h->profEv[2 * k], h->profEv[2 * k + 1]));
+      const int g = h->profGroup[k];
+      if (g < ngroups) {
+        msPerGroup[g] += ms;
+        if (launchesPerGroup) launchesPerGroup[g]++;
+      }
+    }
+  }
+  return GRIM_OK;
+}
+
+int grim_count_flops(grim_handle* h, double* out) {
+  if (!h || !out) { set_err("grim_count_flops: null argument"); return GRIM_EINVAL; }
+  CK(cudaSetDevice(h->device));
+  double* d = nullptr;
+  CK(cudaMalloc(&d, 8 * sizeof(double)));
+  CK(cudaMemsetAsync(d, 0, 8 * sizeof(double), h->stream));
+  const long long z = interior_to_z(h->dc, h->dc.Zint / 2);
+  grim::fast::count_ops(h->dc, h->lastStage, stage_bufs(h, h->lastStage), z, d, h->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, 7 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) { set_err("grim_count_flops: %s", cudaGetErrorString(e)); return GRIM_ECUDA; }
   return GRIM_OK;
 }
 

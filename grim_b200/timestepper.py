@@ -170,6 +170,26 @@ class timeStepper:
     def stream(self):
         return _lib.lib().grim_stream(self._h)
 
+    PROF_GROUPS = ("boundary", "faces_x1", "faces_x2", "faces_x3", "epilogue", "newton", "dt",
+                   "diagnostics", "copy", "emhd_prepass")
+
+    def profileSteps(self, nsteps=1):
+        """Advance nsteps without the graph, timing every kernel group with
+        CUDA events on the stepper's stream: {group: (ms, launch runs)}."""
+        n = len(self.PROF_GROUPS)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_longlong * n)()
+        _lib.check(_lib.lib().grim_profile_steps(self._h, int(nsteps), ms, cnt, n), "profile_steps")
+        return {g: (ms[k], cnt[k]) for k, g in enumerate(self.PROF_GROUPS)}
+
+    def countFlops(self):
+        """Algorithmic flops of one zone: residual (FP64), tangent pass
+        (FP32 and FP64), pivoted solve (FP32 and FP64)."""
+        out = (ctypes.c_double * 8)()
+        _lib.check(_lib.lib().grim_count_flops(self._h, out), "count_flops")
+        keys = ("residual64", "tangent32", "tangent64", "solve32", "solve64", "residual_div", "residual_sqrt_exp")
+        return {k: out[i] for i, k in enumerate(keys)}
+
     # ---- stage pieces --------------------------------------------------------
     def _zeros(self, nv):
         return np.zeros((nv,) + self.zshape)

@@ -206,6 +206,37 @@ void* grim_stream(grim_handle* h);
  *      bandwidth (GB/s, read + write) of a device; any pointer may be NULL */
 int grim_measure_peaks(int device, double* fp64_tflops, double* fp32_tflops, double* hbm_gbs);
 
+/* ---- measurement.  The reference's own measure is the hand-counted
+ *      numReads/numWrites traffic model plus wall time of timeStep
+ *      (src/timestepper/timestepper.cpp:473-526, timestep.cpp:330-333).
+ *
+ * grim_profile_steps runs nsteps steps without the graph and returns the
+ * device time of each kernel group, measured with CUDA events recorded
+ * around its launches on the handle's stream, summed over the steps, and
+ * the number of bracketed launch runs per group. */
+enum {
+  GRIM_PROF_BOUNDARY = 0,    /* ghost fill, communicate, inflow / pole hooks */
+  GRIM_PROF_FACES_X1 = 1,    /* reconstruction + Riemann fluxes at X1 faces */
+  GRIM_PROF_FACES_X2 = 2,
+  GRIM_PROF_FACES_X3 = 3,
+  GRIM_PROF_EPILOGUE = 4,    /* CT EMFs, divergence, sources, induction, guess */
+  GRIM_PROF_NEWTON = 5,      /* every Newton kernel of a stage */
+  GRIM_PROF_DT = 6,          /* characteristic speeds, dt, time advance */
+  GRIM_PROF_DIAGNOSTICS = 7, /* floors, NaN reset, non-finite count */
+  GRIM_PROF_COPY = 8,        /* device-to-device state copies */
+  GRIM_PROF_EMHD_PREPASS = 9,
+  GRIM_PROF_GROUPS = 10
+};
+int grim_profile_steps(grim_handle* h, int nsteps, double* msPerGroup, long long* launchesPerGroup,
+                       int ngroups);
+/* Algorithmic flop counts of one zone (the middle interior zone of the
+ * last set-up stage), counted by running the kernels' templated physics on
+ * a counting scalar: out[0] residual (FP64), out[1] tangent Jacobian pass
+ * in FP32, out[2] the same in FP64, out[3] pivoted solve FP32, out[4] the
+ * same in FP64, out[5] divisions and out[6] sqrt+exp of the residual.
+ * Adds and multiplies count 1 each, as do divide, sqrt and exp. */
+int grim_count_flops(grim_handle* h, double* out);
+
 /* ---- allocation-free divergence.  No counterpart in the reference: for
  *      callers that cannot call cudaMalloc (their device memory is owned by
  *      their own pool allocator, or they call in the middle of asynchronous

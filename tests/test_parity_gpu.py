@@ -307,3 +307,36 @@ def test_cpp_driver_matches_python_binding(tmp_path):
     Q = interior(cfg, ts.primOld.getVars())
     assert t_cpp == ts.time
     assert abs(sum_cpp - float(np.sum(Q))) <= 1e-12 * abs(sum_cpp)
+
+
+def test_profile_steps_and_flop_counts():
+    """grim_profile_steps advances the state like grim_time_step (same bits)
+    and times every kernel group; grim_count_flops counts the templated
+    physics on a counting scalar: the FP32 and FP64 tangent passes do the
+    same operations, and one tangent pass (value + nf derivative lanes: a
+    product costs 1 + 3 nf flops, a sum 1 + nf) costs more than a residual
+    and less than 3 nf + 2 of them."""
+    cfg = PR.fast_mode_config(N=64, nonlinearsolve_rtol=1e-10, nonlinearsolve_atol=1e-24,
+                              maxNonLinearIter=4)
+    P = PR.fast_mode_prims(cfg)
+    from grim_b200.timestepper import timeStepper
+    a, b = timeStepper(cfg), timeStepper(cfg)
+    for ts in (a, b):
+        ts.setNewtonMode(C.NEWTON_MIXED32, 1, 1e-10)
+        ts.primOld.setVars(P)
+    prof = a.profileSteps(2)
+    b.timeStep()
+    b.timeStep()
+    assert np.array_equal(a.primOld.getVars(), b.primOld.getVars())
+    for g in ("boundary", "faces_x1", "faces_x2", "epilogue", "newton", "dt"):
+        assert prof[g][0] > 0 and prof[g][1] > 0, (g, prof[g])
+    assert prof["faces_x3"][1] == 0 and prof["emhd_prepass"][1] == 0
+    assert prof["epilogue"][1] == 4 and prof["newton"][1] == 4
+    f = a.countFlops()
+    nf = a.numFluidVars
+    assert f["residual64"] > 100
+    assert f["tangent32"] == f["tangent64"]
+    assert f["residual64"] < f["tangent32"] < (3 * nf + 2) * f["residual64"]
+    # pivoted elimination without a 1/pivot reciprocal: n^3/3 multiply-adds
+    # plus the substitution, exactly counted for n = 5
+    assert f["solve32"] == f["solve64"] and 60 <= f["solve64"] <= 200, f
