@@ -298,6 +298,7 @@ def run_gpu(args, rank, world, local_rank):
             state["P"] = torus_state(cfg, ts)
         ts.primOld.setVars(state["P"])
         ts.problemInit()
+        state.setdefault("tuned", {})[mode] = {str(d): v for d, (v, _) in ts.autotune().items()}
         if graph:
             ts.enableGraph(True)
         stream = torch.cuda.ExternalStream(ts.stream())
@@ -374,7 +375,8 @@ def run_gpu(args, rank, world, local_rank):
                    "newton": "tangent Jacobian, FP32 solve, FP64 residual, per-zone convergence",
                    "rel_residual_tol": RTOL, "abs_residual_floor": ATOL, "maxNonLinearIter": cfg["maxNonLinearIter"],
                    "l2": "flushed between timed steps (256 MB write, untimed)",
-                   "parallelism": "replicas" if world > 1 else "single GPU", "cuda_graph": True},
+                   "parallelism": "replicas" if world > 1 else "single GPU", "cuda_graph": True,
+                   "face_kernel_variants": state.get("tuned", {})},
         "fd64": {"value": fd, "ms_per_step": ms_fd / args.steps, "newton_iters": st_fd["newtonIters"],
                  "unconverged": st_fd["unconverged"]},
         "speedup_vs_fd64": value / fd if fd else None,

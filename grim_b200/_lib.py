@@ -90,6 +90,8 @@ def lib():
         "grim_measure_peaks": [i, P(d), P(d), P(d)],
         "grim_profile_steps": [vp, i, P(d), P(ctypes.c_longlong), i],
         "grim_count_flops": [vp, P(d)],
+        "grim_autotune": [vp, P(i), P(d)],
+        "grim_set_face_variant": [vp, i, i],
     }
     for name, args in sig.items():
         f = getattr(L, name)

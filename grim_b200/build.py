@@ -1,8 +1,9 @@
 """Builds libgrim_b200.so in place (nvcc, sm_100a).
 
-kernels_exact.cu and geometry.cu are compiled with --fmad=false so the FP64
-parity path keeps the reference's operation order without FMA contraction;
-kernels_fast.cu (tangent / mixed-precision Newton) keeps contraction on.
+kernels_exact.cu, faces_exact.cu and geometry.cu are compiled with
+--fmad=false so the FP64 parity path keeps the reference's operation order
+without FMA contraction; kernels_fast.cu and faces_fast.cu (tangent /
+mixed-precision Newton) keep contraction on.
 Objects are rebuilt only when a source or header is newer.
 """
 import concurrent.futures as cf
@@ -22,6 +23,8 @@ EXACT = ["--fmad=false"]
 UNITS = {
     "kernels_exact.cu": EXACT,
     "kernels_fast.cu": [],
+    "faces_exact.cu": EXACT,
+    "faces_fast.cu": [],
     "geometry.cu": EXACT,
     "runtime.cu": [],
     "peaks.cu": [],

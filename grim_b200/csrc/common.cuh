@@ -20,6 +20,7 @@ struct DevCfg {
   int g1, g2, g3;
   int N1T, N2T, N3T;
   long long Z, Zint;
+  long long GZ;  // zones of one (i, j) plane: the stride of the stored geometry
   int nf, dof, Q, DP, B1;
   int conduction, viscosity, hoCond, hoVisc;
   int metric, reconstruction, riemann, closure, problem;
@@ -54,6 +55,10 @@ GRIM_HD long long interior_to_z(const DevCfg& c, long long n) {
   int k = (int)(r / c.N2);
   return zidx(c, i + c.g1, j + c.g2, k + c.g3);
 }
+// The metrics (Minkowski, modified Kerr-Schild with derefine / cylindrify)
+// do not depend on X3, so the geometry is stored for one (i, j) plane.
+GRIM_HD long long gidx(const DevCfg& c, int i, int j) { return (long long)i + (long long)c.N1T * j; }
+GRIM_HD long long gidx(const DevCfg& c, long long z) { return z % c.GZ; }
 GRIM_HD long long stride_of(const DevCfg& c, int dir) {
   return dir == 0 ? 1LL : (dir == 1 ? (long long)c.N1T : (long long)c.N1T * c.N2T);
 }

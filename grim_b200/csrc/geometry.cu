@@ -197,11 +197,11 @@ __device__ void det_inverse(const double G[4][4], double& D, double C[4][4]) {
 // coordinatesGrid::setXCoords (grid.cpp:168-249) offsets per location
 __global__ void k_geometry(DevCfg c, GeoParams p, double o1, double o2, double* __restrict__ out,
                            double* __restrict__ gamma) {
+  // one (i, j) plane: the maps and the metric do not depend on X3
   long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (z >= c.Z) return;
-  int i, j, k;
-  zijk(c, z, i, j, k);
-  const long long Z = c.Z;
+  if (z >= c.GZ) return;
+  const int i = (int)(z % c.N1T), j = (int)(z / c.N1T), k = c.g3;
+  const long long Z = c.GZ;
   double X[3];
   X[0] = c.X1Start + ((double)(i - c.g1) + o1) * c.dX[0];
   X[1] = c.X2Start + ((double)(j - c.g2) + o2) * c.dX[1];
@@ -272,7 +272,7 @@ void launch_geometry(const DevCfg& c, const grim_config& cfg, int location, doub
   else if (location == GRIM_BOTTOM) o2 = 0.;
   else if (location == GRIM_TOP) o2 = 1.;
   const int t = 64;
-  k_geometry<<<(unsigned)((c.Z + t - 1) / t), t, 0, s>>>(c, p, o1, o2, out, gamma);
+  k_geometry<<<(unsigned)((c.GZ + t - 1) / t), t, 0, s>>>(c, p, o1, o2, out, gamma);
 }
 
 }  // namespace grim

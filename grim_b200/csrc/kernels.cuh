@@ -41,7 +41,7 @@ GRIM_D void load_geo(ZoneGeo<R>& G, const DevCfg& c, const double* geo, long lon
   if (geo == nullptr)
     geo_minkowski<R>(G, (R)zone_x1(c, i, o1), (R)zone_x2(c, j, o2));
   else
-    geo_load<R>(G, geo, c.Z, z);
+    geo_load<R>(G, geo, c.GZ, gidx(c, i, j));
 }
 
 // ---------------------------------------------------------------------------
@@ -64,7 +64,7 @@ GRIM_D int bc_map(int x, int g, int N, int lo, int hi) {
 // mirror only; periodic directions are left as they are (the reference fills
 // them in grid::communicate at the end of each stage).  Applied direction by
 // direction over full spans, its result is the gather below.
-__global__ void k_ghost_fill(DevCfg c, double* __restrict__ prim, int nv) {
+static __global__ void k_ghost_fill(DevCfg c, double* __restrict__ prim, int nv) {
   long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (z >= c.Z) return;
   int i, j, k;
@@ -84,7 +84,7 @@ __global__ void k_ghost_fill(DevCfg c, double* __restrict__ prim, int nv) {
 // ghost zones (corners included) take the wrapped interior value; ghost
 // zones on a non-periodic edge come back from the never-written local
 // vector, i.e. as zero.
-__global__ void k_communicate(DevCfg c, double* __restrict__ prim, int nv) {
+static __global__ void k_communicate(DevCfg c, double* __restrict__ prim, int nv) {
   long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (z >= c.Z) return;
   int i, j, k;
@@ -132,10 +132,9 @@ __global__ void k_emhd_prepass(DevCfg c, const double* __restrict__ ps, const do
 // face fluxes (riemannsolver.cpp:202-328 after its shift): the flux through
 // the face z - 1/2 along `dir` from the left state (right face value of zone
 // z - s) and the right state (left face value of zone z).  Every zone is
-// reconstructed once: X1 faces share a warp's reconstructions through
-// shuffles (31 faces per warp), X2 / X3 faces are swept by threads that
-// march along the face direction and keep the previous zone's right-face
-// state in registers.
+// reconstructed once per direction and handed to its neighbour by a warp
+// shuffle: X1 faces take 31 faces per warp along i, X2 / X3 faces 7 faces
+// along the direction for each of 4 consecutive i.
 // ---------------------------------------------------------------------------
 template <int DOF>
 GRIM_D void recon_zone(const DevCfg& c, const double* __restrict__ ps, long long z, long long s, int scheme,
@@ -196,8 +195,8 @@ GRIM_D void riemann_face(const DevCfg& c, int dir, const double* pl, const doubl
 // X1 faces: warp w of a row covers faces i0 .. i0+30; lane l reconstructs
 // zone i0 - 1 + l and, for l >= 1, computes the face between zones
 // i0 - 2 + l and i0 - 1 + l with the left state shuffled from lane l - 1.
-template <int COND, int VISC>
-__global__ void __launch_bounds__(128) k_face_flux_x1(DevCfg c, const double* __restrict__ ps,
+template <int COND, int VISC, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_face_flux_x1(DevCfg c, const double* __restrict__ ps,
                                                       const double* __restrict__ geoF, double* __restrict__ flux) {
   constexpr int DOF = 8 + COND + VISC;
   const int lane = threadIdx.x & 31;
@@ -223,57 +222,51 @@ __global__ void __launch_bounds__(128) k_face_flux_x1(DevCfg c, const double* __
   riemann_face<COND, VISC>(c, 0, pl, lo, G, G, flux, z);
 }
 
-// X2 / X3 faces: a 32 x 8 thread block reconstructs 8 consecutive zones
-// along dir for 32 consecutive i (each zone once, loads coalesced along i)
-// into shared memory, then 7 of its warps compute the 7 faces between them.
-constexpr int kTileRows = 8;
-template <int COND, int VISC>
-__global__ void __launch_bounds__(256) k_face_flux_tile(DevCfg c, int dir, const double* __restrict__ ps,
-                                                        const double* __restrict__ geoF,
-                                                        const double* __restrict__ geoC, double* __restrict__ flux) {
+// X2 / X3 faces: the X1 scheme turned sideways.  A warp holds QI
+// consecutive i (lane % QI) by 32/QI consecutive zones along dir
+// (lane / QI); every lane reconstructs its zone once and the right-face
+// state moves QI lanes up by shuffle, giving (32/QI - 1) x QI faces per
+// warp.  With QI = 4 each warp-wide load still covers whole 32-byte
+// sectors (4 consecutive doubles along i), as in the X1 kernel.
+template <int COND, int VISC, int QI, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_face_flux_strip(DevCfg c, int dir, const double* __restrict__ ps,
+                                                         const double* __restrict__ geoF,
+                                                         const double* __restrict__ geoC, double* __restrict__ flux) {
   constexpr int DOF = 8 + COND + VISC;
-  extern __shared__ double sm_recon[];  // [row][var][lane] lo, then ro
-  double* sLo = sm_recon;
-  double* sRo = sm_recon + kTileRows * DOF * 32;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  const int i = blockIdx.x * 32 + tx;
+  constexpr int JR = 32 / QI;       // zones along dir per warp
+  constexpr int FPW = JR - 1;       // faces along dir per warp
+  const int lane = threadIdx.x & 31;
+  const long long wg = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int NT = (dir == 1) ? c.N2T : c.N3T;
-  const int other = blockIdx.z;  // k for X2 faces, j for X3 faces
-  const int x0 = 3 + blockIdx.y * (kTileRows - 1);  // first face of the tile
-  const int xr = x0 - 1 + ty;                       // zone this thread reconstructs
+  const int nq = (c.N1T + QI - 1) / QI;
+  const int nch = (NT - 5 + FPW - 1) / FPW;  // faces 3 .. NT-3
+  const long long nother = (dir == 1) ? c.N3T : c.N2T;
+  if (wg >= (long long)nq * nch * nother) return;  // whole warps exit together
+  const int iq = (int)(wg % nq);
+  const long long r = wg / nq;
+  const int ch = (int)(r % nch);
+  const int other = (int)(r / nch);  // k for X2 faces, j for X3 faces
+  const int i = iq * QI + (lane % QI);
+  const int x = 2 + ch * FPW + lane / QI;  // zone along dir; face x sits at its left
+  const bool reconOK = i < c.N1T && x <= NT - 3;
+  const int ic = reconOK ? i : min(i, c.N1T - 1);
+  const int xc = reconOK ? x : 2;
   const long long s = stride_of(c, dir);
-  auto zof = [&](int x) -> long long { return dir == 1 ? zidx(c, i, x, other) : zidx(c, i, other, x); };
-  const bool reconOK = i < c.N1T && xr <= NT - 3;
-  if (reconOK) {
-    double lo[DOF], ro[DOF];
-    recon_zone<DOF>(c, ps, zof(xr), s, c.reconstruction, lo, ro);
+  const long long z = dir == 1 ? zidx(c, ic, xc, other) : zidx(c, ic, other, xc);
+  double lo[DOF], ro[DOF];
+  recon_zone<DOF>(c, ps, z, s, c.reconstruction, lo, ro);
+  double pl[DOF];
 #pragma unroll
-    for (int v = 0; v < DOF; v++) {
-      sLo[(ty * DOF + v) * 32 + tx] = lo[v];
-      sRo[(ty * DOF + v) * 32 + tx] = ro[v];
-    }
-  }
-  __syncthreads();
-  if (ty == 0 || !reconOK) return;
-  // face xr (between zones xr-1 and xr)
-  double pl[DOF], pr[DOF];
-#pragma unroll
-  for (int v = 0; v < DOF; v++) {
-    pl[v] = sRo[((ty - 1) * DOF + v) * 32 + tx];
-    pr[v] = sLo[(ty * DOF + v) * 32 + tx];
-  }
-  const long long z = zof(xr);
-  ZoneGeo<double> GL, GR;
-  const int jj = (dir == 1) ? xr : other;
-  if (dir == 2) {
-    // X3 faces use the centre geometry of each side (fvmfluxes.cpp:150-151)
-    load_geo(GL, c, geoC, z - s, i, jj, 0.5, 0.5);
-    load_geo(GR, c, geoC, z, i, jj, 0.5, 0.5);
-  } else {
-    load_geo(GL, c, geoF, z, i, jj, 0.5, 0.);
-    GR = GL;
-  }
-  riemann_face<COND, VISC>(c, dir, pl, pr, GL, GR, flux, z);
+  for (int v = 0; v < DOF; v++) pl[v] = __shfl_up_sync(0xffffffffu, ro[v], QI);
+  if (lane < QI || !reconOK) return;
+  ZoneGeo<double> G;
+  // X3 faces use the centre geometry of each side (fvmfluxes.cpp:150-151),
+  // which is one and the same: the metric does not depend on X3
+  if (dir == 2)
+    load_geo(G, c, geoC, z, i, other, 0.5, 0.5);
+  else
+    load_geo(G, c, geoF, z, i, x, 0.5, 0.);
+  riemann_face<COND, VISC>(c, dir, pl, lo, G, G, flux, z);
 }
 
 // ---------------------------------------------------------------------------
@@ -404,7 +397,7 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
       double s = S[UU + nu];
       for (int ka = 0; ka < 4; ka++)
         for (int la = 0; la < 4; la++)
-          s -= G.g * T[ka][la] * __ldg(b.gamma + (long long)(la * 16 + ka * 4 + nu) * Z + z);
+          s -= G.g * T[ka][la] * __ldg(b.gamma + (long long)(la * 16 + ka * 4 + nu) * c.GZ + gidx(c, i, j));
       S[UU + nu] = s;
     }
   }
@@ -425,7 +418,7 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
       if (c.metric != GRIM_MINKOWSKI) {
         for (int nu = 0; nu < 4; nu++)
           for (int la = 0; la < 4; la++)
-            gu[nu][mu] -= __ldg(b.gamma + (long long)(la * 16 + nu * 4 + mu) * Z + z) * e.uCov[la];
+            gu[nu][mu] -= __ldg(b.gamma + (long long)(la * 16 + nu * 4 + mu) * c.GZ + gidx(c, i, j)) * e.uCov[la];
       }
     }
     if (COND) {
@@ -540,7 +533,7 @@ __global__ void k_dt_speeds(DevCfg c, const double* __restrict__ p, const double
 }
 
 // dt = Courant / maxInvDt, capped at maxDtIncrement * dt (timestep.cpp:393-399)
-__global__ void k_dt_update(DevState* st, double courant, double maxInc) {
+static __global__ void k_dt_update(DevState* st, double courant, double maxInc) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     double newDt = courant / st->maxInvDt;
     if (newDt > maxInc * st->dt) newDt = maxInc * st->dt;
@@ -549,7 +542,7 @@ __global__ void k_dt_update(DevState* st, double courant, double maxInc) {
   }
 }
 
-__global__ void k_advance_time(DevState* st) {
+static __global__ void k_advance_time(DevState* st) {
   if (threadIdx.x == 0 && blockIdx.x == 0) st->time += st->dt;
 }
 
@@ -786,10 +779,15 @@ __global__ void __launch_bounds__(128) k_newton_fd_iter(DevCfg c, int stage, int
 // and solve in FP32, residual in FP64, i.e. FP32 inexact Newton refined by
 // the FP64 residual).
 // ---------------------------------------------------------------------------
-template <int COND, int VISC, class T>
+template <int COND, int VISC, class T, bool GENERIC = false>
 GRIM_D void tangent_jacobian(const double* P, const StageConst<5 + COND + VISC>& K, const ZoneGeo<T>& Gt,
                              const DevCfg& c, T J[5 + COND + VISC][5 + COND + VISC]) {
   constexpr int NF = 5 + COND + VISC;
+  if constexpr (COND == 0 && VISC == 0 && !GENERIC) {
+    // ideal MHD: the closed-form dU/dP
+    ideal_jacobian<T>(P, K, Gt, c, J);
+    return;
+  }
   typedef Dual<T, NF> D;
   D Pd[NF], Rd[NF];
 #pragma unroll
@@ -1107,7 +1105,7 @@ __global__ void k_conserved(DevCfg c, const double* __restrict__ p, const double
 }
 
 // reconstruction of one direction for every zone (test entry point)
-__global__ void k_reconstruct(DevCfg c, int dir, const double* __restrict__ p, double* __restrict__ pl,
+static __global__ void k_reconstruct(DevCfg c, int dir, const double* __restrict__ p, double* __restrict__ pl,
                                        double* __restrict__ pr) {
   long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (z >= c.Z) return;
@@ -1147,7 +1145,7 @@ __global__ void k_batch_solve(int batch, const double* __restrict__ A, const dou
 }
 
 // non-finite primitives count (diagnostic after each step)
-__global__ void k_count_nonfinite(DevCfg c, const double* __restrict__ p, DevState* st) {
+static __global__ void k_count_nonfinite(DevCfg c, const double* __restrict__ p, DevState* st) {
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int bad = 0;
   if (n < c.Zint) {
@@ -1180,6 +1178,7 @@ static inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) 
     else KERNEL<0, 0>(__VA_ARGS__);                                     \
   } while (0)
 
+#if !defined(GRIM_ONLY_FACES)
 void ghost_fill(const DevCfg& c, double* prim, int nv, cudaStream_t s) {
   k_ghost_fill<<<nblk(c.Z, 256), 256, 0, s>>>(c, prim, nv);
 }
@@ -1195,26 +1194,55 @@ void emhd_prepass(const DevCfg& c, const double* ps, const double* geoC, double*
   GRIM_EMHD_DISPATCH(c, emhd_prepass_t, c, ps, geoC, uT, s);
 }
 
+#endif  // !GRIM_ONLY_FACES
+
+#if !defined(GRIM_SKIP_FACES)
+// Launch-shape variants of the face kernels, chosen per direction by the
+// autotuner (grim_autotune): X1 faces by the register budget (3 or 4
+// resident 128-thread blocks per SM), X2 / X3 faces by that budget and by
+// the lane split QI (i per warp).  Other than ideal MHD only the default.
+template <int C, int V, int MINB>
+static void face_x1_launch(const DevCfg& c, const double* ps, const double* geoF, double* flux, cudaStream_t s) {
+  const long long warps = (long long)c.N2T * c.N3T * ((c.N1T - 5 + 30) / 31);
+  k_face_flux_x1<C, V, MINB><<<nblk(warps * 32, 128), 128, 0, s>>>(c, ps, geoF, flux);
+}
+template <int C, int V, int QI, int MINB>
+static void face_strip_launch(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,
+                              double* flux, cudaStream_t s) {
+  const int NT = (dir == 1) ? c.N2T : c.N3T;
+  const long long other = (dir == 1) ? c.N3T : c.N2T;
+  const long long warps = (long long)((c.N1T + QI - 1) / QI) * ((NT - 5 + 32 / QI - 2) / (32 / QI - 1)) * other;
+  k_face_flux_strip<C, V, QI, MINB><<<nblk(warps * 32, 128), 128, 0, s>>>(c, dir, ps, geoF, geoC, flux);
+}
 template <int C, int V>
 static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,
-                        double* flux, cudaStream_t s) {
+                        double* flux, int variant, cudaStream_t s) {
+  constexpr bool ideal = (C == 0 && V == 0);
   if (dir == 0) {
-    const long long warps = (long long)c.N2T * c.N3T * ((c.N1T - 5 + 30) / 31);
-    k_face_flux_x1<C, V><<<nblk(warps * 32, 128), 128, 0, s>>>(c, ps, geoF, flux);
-  } else {
-    const int NT = (dir == 1) ? c.N2T : c.N3T;
-    const int other = (dir == 1) ? c.N3T : c.N2T;
-    constexpr int DOF = 8 + C + V;
-    const size_t smem = 2 * kTileRows * DOF * 32 * sizeof(double);
-    dim3 grid(nblk(c.N1T, 32), (unsigned)((NT - 5 + kTileRows - 2) / (kTileRows - 1)), (unsigned)other);
-    k_face_flux_tile<C, V><<<grid, 256, smem, s>>>(c, dir, ps, geoF, geoC, flux);
+    if (ideal && variant == 1) face_x1_launch<C, V, ideal ? 4 : 3>(c, ps, geoF, flux, s);
+    else face_x1_launch<C, V, 3>(c, ps, geoF, flux, s);
+    return;
+  }
+  switch (ideal ? variant : 0) {
+    case 1: face_strip_launch<C, V, 4, 4>(c, dir, ps, geoF, geoC, flux, s); break;
+    case 2: face_strip_launch<C, V, 2, 3>(c, dir, ps, geoF, geoC, flux, s); break;
+    case 3: face_strip_launch<C, V, 2, 4>(c, dir, ps, geoF, geoC, flux, s); break;
+    case 4: face_strip_launch<C, V, 8, 3>(c, dir, ps, geoF, geoC, flux, s); break;
+    case 5: face_strip_launch<C, V, 8, 4>(c, dir, ps, geoF, geoC, flux, s); break;
+    default: face_strip_launch<C, V, 4, 3>(c, dir, ps, geoF, geoC, flux, s); break;
   }
 }
 void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC, double* flux,
-               cudaStream_t s) {
-  GRIM_EMHD_DISPATCH(c, face_flux_t, c, dir, ps, geoF, geoC, flux, s);
+               int variant, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, face_flux_t, c, dir, ps, geoF, geoC, flux, variant, s);
 }
+int face_variants(const DevCfg& c, int dir) {
+  if (c.conduction || c.viscosity) return 1;
+  return dir == 0 ? 2 : 6;
+}
+#endif  // !GRIM_SKIP_FACES
 
+#if !defined(GRIM_ONLY_FACES)
 template <int C, int V>
 static void stage_epilogue_t(const DevCfg& c, int stage, const StageBufs& b, cudaStream_t s) {
   k_stage_epilogue<C, V><<<nblk(c.Zint, 128), 128, 0, s>>>(c, stage, b);
@@ -1366,6 +1394,8 @@ void torus_bcs(const DevCfg& c, double* p, const double* geoC, cudaStream_t s) {
 void count_nonfinite(const DevCfg& c, const double* p, DevState* st, cudaStream_t s) {
   k_count_nonfinite<<<nblk(c.Zint, 256), 256, 0, s>>>(c, p, st);
 }
+
+#endif  // !GRIM_ONLY_FACES
 
 }  // namespace GRIM_KNS
 }  // namespace grim

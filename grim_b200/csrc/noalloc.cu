@@ -118,7 +118,7 @@ extern "C" int grim_div_fluxes_noalloc(const grim_config* cfg, const double* pri
   // dt = 0 for the induction part of the epilogue (its output is not used)
   if (cudaMemsetAsync(b.st, 0, sizeof(DevState), s) != cudaSuccess) return GRIM_ECUDA;
   if (emhd) exact::emhd_prepass(c, prim, nullptr, b.uT, s);
-  for (int d = 0; d < c.dim; d++) exact::face_flux(c, d, prim, nullptr, nullptr, b.flux[d], s);
+  for (int d = 0; d < c.dim; d++) exact::face_flux(c, d, prim, nullptr, nullptr, b.flux[d], 0, s);
   exact::stage_epilogue(c, GRIM_HALF_STEP, b, s);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

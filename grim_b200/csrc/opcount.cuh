@@ -63,8 +63,10 @@ struct Lift<Cnt<B>> {
 namespace GRIM_KNS {
 
 // One thread, one zone z of the stage buffers b (filled by a stage set-up):
-// out = {residual fp64, tangent(fp32) fp32, tangent(fp64) fp64,
-//        solve fp32, solve fp64, residual divides, residual sqrt+exp}
+// out = {residual fp64, Jacobian(fp32) fp32, Jacobian(fp64) fp64,
+//        solve fp32, solve fp64, residual divides, residual sqrt+exp,
+//        generic forward-tangent pass fp32}; the Jacobian is the closed
+// form for ideal MHD and the forward tangent otherwise
 template <int COND, int VISC>
 __global__ void k_count_ops(DevCfg c, int stage, StageBufs b, long long z, double* out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -109,6 +111,9 @@ __global__ void k_count_ops(DevCfg c, int stage, StageBufs b, long long z, doubl
       for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = C4(G.gcov[m][q]); Gt.gcon[m][q] = C4(G.gcon[m][q]); }
     Gt.g = C4(G.g); Gt.alpha = C4(G.alpha); Gt.x1 = C4(G.x1); Gt.x2 = C4(G.x2); Gt.dyn = C4(G.dyn);
     C4 J[NF][NF];
+    clear();
+    tangent_jacobian<COND, VISC, C4, true>(Pd, K, Gt, c, J);
+    out[7] = flops(1);  // the generic forward-tangent pass
     clear();
     tangent_jacobian<COND, VISC, C4>(Pd, K, Gt, c, J);
     out[1] = flops(1);

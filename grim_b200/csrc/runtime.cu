@@ -75,6 +75,8 @@ struct grim_handle {
   int lastStage = GRIM_HALF_STEP;
   // per-kernel-group device timing (grim_profile_steps): event pairs
   // recorded around each launch on the handle's stream
+  // face-kernel launch variants per direction, [exact unit, fast unit]
+  int faceVariant[2][3] = {{0, 0, 0}, {0, 0, 0}};
   bool profOn = false;
   std::vector<cudaEvent_t> profEv;
   std::vector<int> profGroup;
@@ -137,6 +139,7 @@ static int make_devcfg(const grim_config& c, DevCfg& d) {
   d.N1T = d.N1 + 2 * d.g1; d.N2T = d.N2 + 2 * d.g2; d.N3T = d.N3 + 2 * d.g3;
   d.Z = (long long)d.N1T * d.N2T * d.N3T;
   d.Zint = (long long)d.N1 * d.N2 * d.N3;
+  d.GZ = (long long)d.N1T * d.N2T;
   d.conduction = c.conduction ? 1 : 0; d.viscosity = c.viscosity ? 1 : 0;
   d.nf = 5 + d.conduction + d.viscosity; d.dof = d.nf + 3;
   d.Q = 5; d.DP = 5 + d.conduction; d.B1 = d.nf;
@@ -206,6 +209,12 @@ static StageBufs stage_bufs(grim_handle* h, int stage) {
     else grim::fast::fn(__VA_ARGS__);                                  \
   } while (0)
 
+#define KNS_CALL_RET(h, out, fn, ...)                                  \
+  do {                                                                 \
+    if (use_exact(h)) out = grim::exact::fn(__VA_ARGS__);              \
+    else out = grim::fast::fn(__VA_ARGS__);                            \
+  } while (0)
+
 static long long g_launch_counter = 0;
 
 static void enqueue_stencil(grim_handle* h, int stage) {
@@ -219,7 +228,7 @@ static void enqueue_stencil(grim_handle* h, int stage) {
   }
   for (int d = 0; d < c.dim; d++) {
     PROF(GRIM_PROF_FACES_X1 + d);
-    KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], s);
+    KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], h->faceVariant[use_exact(h) ? 0 : 1][d], s);
     g_launch_counter++;
   }
   PROF(GRIM_PROF_EPILOGUE);
@@ -390,8 +399,14 @@ int grim_create(const grim_config* cfg, int device, grim_handle** out) {
   for (int d = 0; ok && d < c.dim; d++) ok = alloc(&h->flux[d], c.dof);
   if (ok && (c.conduction || c.viscosity)) ok = alloc(&h->uT, 5);
   if (ok && cfg->metric != GRIM_MINKOWSKI) {
-    for (int l = 0; ok && l < 5; l++) ok = alloc(&h->geo[l], 39);
-    if (ok) ok = alloc(&h->gamma, 64);
+    // one (i, j) plane per word (the metric does not depend on X3)
+    auto allocPlane = [&](double** p, size_t words) -> bool {
+      const size_t b = words * (size_t)c.GZ * sizeof(double);
+      if (cudaMalloc(p, b) != cudaSuccess) return false;
+      return cudaMemset(*p, 0, b) == cudaSuccess;
+    };
+    for (int l = 0; ok && l < 5; l++) ok = allocPlane(&h->geo[l], 39);
+    if (ok) ok = allocPlane(&h->gamma, 64);
   }
   for (int l = 0; ok && l < 2; l++) ok = cudaMalloc(&h->list[l], (size_t)c.Zint * sizeof(int)) == cudaSuccess;
   if (ok) ok = cudaMalloc(&h->st, sizeof(DevState)) == cudaSuccess;
@@ -592,7 +607,9 @@ int grim_compute_div_fluxes(grim_handle* h, const double* prim, double* divF, do
   double* tmpPrim = h->scratch2;  // receives the guess
   b.prim = tmpPrim;
   if (c.conduction || c.viscosity) KNS_CALL(h, emhd_prepass, c, b.ps, b.geoC, h->uT, h->stream);
-  for (int d = 0; d < c.dim; d++) KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], h->stream);
+  for (int d = 0; d < c.dim; d++)
+    KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], h->faceVariant[use_exact(h) ? 0 : 1][d],
+             h->stream);
   // divergence of all dof rows: epilogue writes nf rows into divF and the
   // induction into the guess; the B rows of the divergence are recovered
   // from the guess: B_new = (consOld_B - 0.5 dt divF_B)/g with dt kept
@@ -760,20 +777,41 @@ int grim_batch_solve(int n, int batch, const double* A, const double* b, double*
   return GRIM_OK;
 }
 
+// The library keeps one (i, j) plane per geometry word (the metric does not
+// depend on X3); the ABI exchanges full [word][k][j][i] arrays.
+static int plane_to_full(grim_handle* h, double* dst, const double* src, int rows, int memKind) {
+  const DevCfg& c = h->dc;
+  const cudaMemcpyKind kind = memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  const size_t pb = (size_t)c.GZ * sizeof(double);
+  for (int w = 0; w < rows; w++)
+    for (int k = 0; k < c.N3T; k++)
+      CK(cudaMemcpyAsync(dst + (size_t)w * c.Z + (size_t)k * c.GZ, src + (size_t)w * c.GZ, pb, kind, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return GRIM_OK;
+}
+static int full_to_plane(grim_handle* h, double* dst, const double* src, int rows, int memKind) {
+  const DevCfg& c = h->dc;
+  const cudaMemcpyKind kind = memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  const size_t pb = (size_t)c.GZ * sizeof(double);
+  for (int w = 0; w < rows; w++)  // the k = 0 plane of each word
+    CK(cudaMemcpyAsync(dst + (size_t)w * c.GZ, src + (size_t)w * c.Z, pb, kind, h->stream));
+  return GRIM_OK;
+}
+
 int grim_get_geometry(grim_handle* h, int location, double* out, double* gamma, double* xc, int memKind) {
   if (!h || location < 0 || location > 4) return GRIM_EINVAL;
   CK(cudaSetDevice(h->device));
   const DevCfg& c = h->dc;
   if (h->cfg.metric == GRIM_MINKOWSKI) { set_err("Minkowski geometry is compile-time"); return GRIM_ENOTSUP; }
   if (out) {
-    int rc = stage_out(h, out, h->geo[location], 34 * h->bytesZ, memKind);
+    int rc = plane_to_full(h, out, h->geo[location], 34, memKind);
     if (rc) return rc;
   }
   if (xc) {
-    int rc = stage_out(h, xc, h->geo[location] + 34 * c.Z, 5 * h->bytesZ, memKind);
+    int rc = plane_to_full(h, xc, h->geo[location] + 34 * c.GZ, 5, memKind);
     if (rc) return rc;
   }
-  if (gamma && location == GRIM_CENTER) return stage_out(h, gamma, h->gamma, 64 * h->bytesZ, memKind);
+  if (gamma && location == GRIM_CENTER) return plane_to_full(h, gamma, h->gamma, 64, memKind);
   return GRIM_OK;
 }
 
@@ -782,10 +820,11 @@ int grim_set_geometry(grim_handle* h, int location, const double* in, const doub
   if (!h || location < 0 || location > 4) return GRIM_EINVAL;
   if (h->cfg.metric == GRIM_MINKOWSKI) { set_err("Minkowski geometry is compile-time"); return GRIM_ENOTSUP; }
   CK(cudaSetDevice(h->device));
-  const cudaMemcpyKind k = memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  if (in) CK(cudaMemcpyAsync(h->geo[location], in, 34 * h->bytesZ, k, h->stream));
-  if (xc) CK(cudaMemcpyAsync(h->geo[location] + 34 * h->dc.Z, xc, 5 * h->bytesZ, k, h->stream));
-  if (gamma && location == GRIM_CENTER) CK(cudaMemcpyAsync(h->gamma, gamma, 64 * h->bytesZ, k, h->stream));
+  int rc = GRIM_OK;
+  if (in) rc = full_to_plane(h, h->geo[location], in, 34, memKind);
+  if (!rc && xc) rc = full_to_plane(h, h->geo[location] + 34 * h->dc.GZ, xc, 5, memKind);
+  if (!rc && gamma && location == GRIM_CENTER) rc = full_to_plane(h, h->gamma, gamma, 64, memKind);
+  if (rc) return rc;
   CK(cudaStreamSynchronize(h->stream));
   // the first computeDt depends on the geometry: redo it
   enqueue_dt_speeds(h, h->primOld, 2);
@@ -896,6 +935,55 @@ int grim_profile_steps(grim_handle* h, int nsteps, double* msPerGroup, long long
   return GRIM_OK;
 }
 
+int grim_autotune(grim_handle* h, int* variants, double* msBest) {
+  if (!h) { set_err("grim_autotune: null handle"); return GRIM_EINVAL; }
+  CK(cudaSetDevice(h->device));
+  const DevCfg& c = h->dc;
+  const int unit = use_exact(h) ? 0 : 1;
+  StageBufs b = stage_bufs(h, GRIM_HALF_STEP);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  for (int d = 0; d < c.dim; d++) {
+    int nv = 1;
+    KNS_CALL_RET(h, nv, face_variants, c, d);
+    double best = 1e30;
+    int bestV = 0;
+    for (int v = 0; v < nv; v++) {
+      KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], v, h->stream);  // warm-up
+      CK(cudaEventRecord(e0, h->stream));
+      const int reps = 3;
+      for (int r = 0; r < reps; r++) KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], v, h->stream);
+      CK(cudaEventRecord(e1, h->stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms / reps < best) { best = ms / reps; bestV = v; }
+    }
+    h->faceVariant[unit][d] = bestV;
+    if (variants) variants[d] = bestV;
+    if (msBest) msBest[d] = best;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  CK(cudaGetLastError());
+  return GRIM_OK;
+}
+
+int grim_set_face_variant(grim_handle* h, int dir, int variant) {
+  if (!h || dir < 0 || dir >= h->dc.dim) { set_err("grim_set_face_variant: bad direction"); return GRIM_EINVAL; }
+  int nv = 1;
+  KNS_CALL_RET(h, nv, face_variants, h->dc, dir);
+  if (variant < 0 || variant >= nv) {
+    set_err("grim_set_face_variant: variant %d out of range [0, %d) for direction %d", variant, nv, dir);
+    return GRIM_EINVAL;
+  }
+  h->faceVariant[use_exact(h) ? 0 : 1][dir] = variant;
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  return GRIM_OK;
+}
+
 int grim_count_flops(grim_handle* h, double* out) {
   if (!h || !out) { set_err("grim_count_flops: null argument"); return GRIM_EINVAL; }
   CK(cudaSetDevice(h->device));
@@ -905,7 +993,7 @@ int grim_count_flops(grim_handle* h, double* out) {
   const long long z = interior_to_z(h->dc, h->dc.Zint / 2);
   grim::fast::count_ops(h->dc, h->lastStage, stage_bufs(h, h->lastStage), z, d, h->stream);
   cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, 7 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   cudaFree(d);
   if (e != cudaSuccess) { set_err("grim_count_flops: %s", cudaGetErrorString(e)); return GRIM_ECUDA; }

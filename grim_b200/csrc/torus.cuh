@@ -32,8 +32,9 @@ __global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, cons
   long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (z >= c.Z) return;
   const long long Z = c.Z;
+  const long long gz = gidx(c, z);
   ZoneGeo<double> G;
-  geo_load<double>(G, geoC, Z, z);
+  geo_load<double>(G, geoC, c.GZ, gz);
   double* pv[12];
   for (int v = 0; v < c.dof; v++) pv[v] = p + (long long)v * Z + z;
   if (nanFlag && *nanFlag) {
@@ -42,8 +43,8 @@ __global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, cons
     if (bad)
       for (int v = 0; v < c.dof; v++) *pv[v] = 0.;
   }
-  const double minRho = __ldg(geoC + 37LL * Z + z);
-  const double minU = __ldg(geoC + 38LL * Z + z);
+  const double minRho = __ldg(geoC + 37LL * c.GZ + gz);
+  const double minU = __ldg(geoC + 38LL * c.GZ + gz);
   const double rho_pre = *pv[RHO] * 1., u_pre = *pv[UU] * 1.;
   bool usefloor = false;
   {
@@ -138,7 +139,7 @@ __global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, cons
 }
 
 // NaN count over the interior (fullStepDiagnostics, problem.cpp:725-733)
-__global__ void k_nan_flag(DevCfg c, const double* __restrict__ p, unsigned long long* flag) {
+static __global__ void k_nan_flag(DevCfg c, const double* __restrict__ p, unsigned long long* flag) {
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int bad = 0;
   if (n < c.Zint) {
@@ -164,7 +165,7 @@ __global__ void k_torus_inflow(DevCfg c, TorusCfg t, double* __restrict__ p, con
   const long long Z = c.Z;
   const long long z = zidx(c, i, j, k);
   ZoneGeo<double> G;
-  geo_load<double>(G, geoC, Z, z);
+  geo_load<double>(G, geoC, c.GZ, gidx(c, i, j));
   ElemT<double, double> e;
   load_elem<COND, VISC>(e, c, p, z, G);
   double* u1 = p + (long long)U1 * Z + z;
@@ -175,8 +176,8 @@ __global__ void k_torus_inflow(DevCfg c, TorusCfg t, double* __restrict__ p, con
   *u3 = *u3 / e.gam;
   if (right) {
     // the last active zone's g^{01} alpha, copied into the ghost columns
-    const long long ze = zidx(c, c.N1 + c.ng - 1, j, k);
-    const double minUr = __ldg(geoC + 17LL * Z + ze) * __ldg(geoC + 33LL * Z + ze);
+    const long long ze = gidx(c, c.N1 + c.ng - 1, j);
+    const double minUr = __ldg(geoC + 17LL * c.GZ + ze) * __ldg(geoC + 33LL * c.GZ + ze);
     *u1 = fmax(minUr, *u1);
   } else {
     *u1 = fmin(G.gcon[0][1] * G.alpha, *u1);
@@ -194,7 +195,7 @@ __global__ void k_torus_inflow(DevCfg c, TorusCfg t, double* __restrict__ p, con
 }
 
 // fixPoles (problem.cpp:1046-1215): one thread per (i, k) column and pole
-__global__ void k_torus_poles(DevCfg c, double* __restrict__ p, const double* __restrict__ geoC) {
+static __global__ void k_torus_poles(DevCfg c, double* __restrict__ p, const double* __restrict__ geoC) {
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long cols = (long long)c.N1T * c.N3T;
   if (n >= 2 * cols) return;
@@ -205,7 +206,7 @@ __global__ void k_torus_poles(DevCfg c, double* __restrict__ p, const double* __
   const int ng = c.ng;
   auto at = [&](int v, int j) -> double& { return p[(long long)v * Z + zidx(c, i, j, k)]; };
   auto theta = [&](int j) -> double {
-    double th = __ldg(geoC + 35LL * Z + zidx(c, i, j, k));
+    double th = __ldg(geoC + 35LL * c.GZ + gidx(c, i, j));
     return top ? th * (-1.) + M_PI : th;
   };
   const int idx0 = top ? c.N2 + ng - 1 : ng;

@@ -182,12 +182,24 @@ class timeStepper:
         _lib.check(_lib.lib().grim_profile_steps(self._h, int(nsteps), ms, cnt, n), "profile_steps")
         return {g: (ms[k], cnt[k]) for k, g in enumerate(self.PROF_GROUPS)}
 
+    def autotune(self):
+        """Pick the fastest launch shape of each direction's face kernel on
+        the current state (for the current Newton mode): {dir: (variant, ms)}."""
+        v = (ctypes.c_int * 3)()
+        ms = (ctypes.c_double * 3)()
+        _lib.check(_lib.lib().grim_autotune(self._h, v, ms), "autotune")
+        return {d: (v[d], ms[d]) for d in range(self.cfg["dim"])}
+
+    def setFaceVariant(self, dir, variant):
+        _lib.check(_lib.lib().grim_set_face_variant(self._h, int(dir), int(variant)), "set_face_variant")
+
     def countFlops(self):
         """Algorithmic flops of one zone: residual (FP64), tangent pass
         (FP32 and FP64), pivoted solve (FP32 and FP64)."""
         out = (ctypes.c_double * 8)()
         _lib.check(_lib.lib().grim_count_flops(self._h, out), "count_flops")
-        keys = ("residual64", "tangent32", "tangent64", "solve32", "solve64", "residual_div", "residual_sqrt_exp")
+        keys = ("residual64", "tangent32", "tangent64", "solve32", "solve64", "residual_div", "residual_sqrt_exp",
+                "dual_tangent32")
         return {k: out[i] for i, k in enumerate(keys)}
 
     # ---- stage pieces --------------------------------------------------------

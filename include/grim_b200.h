@@ -180,7 +180,9 @@ int grim_batch_solve(int n, int batch, const double* A, const double* b, double*
  * aux 5 x Z = [x1 | x2 | x1^1.5 | RhoFloorAmpl x1^RhoFloorSlope |
  * UFloorAmpl x1^UFloorSlope] (physical coordinates and the geometry-only
  * fields of the torus closure and floors).  get copies out, set replaces the
- * device copy. */
+ * device copy.  The metrics do not depend on X3: the library stores one
+ * (i, j) plane per word, get repeats it over k and set takes the k = 0
+ * plane of its input. */
 int grim_get_geometry(grim_handle* h, int location, double* out, double* gamma,
                       double* xcoords, int memKind);
 int grim_set_geometry(grim_handle* h, int location, const double* in,
@@ -231,11 +233,22 @@ int grim_profile_steps(grim_handle* h, int nsteps, double* msPerGroup, long long
                        int ngroups);
 /* Algorithmic flop counts of one zone (the middle interior zone of the
  * last set-up stage), counted by running the kernels' templated physics on
- * a counting scalar: out[0] residual (FP64), out[1] tangent Jacobian pass
- * in FP32, out[2] the same in FP64, out[3] pivoted solve FP32, out[4] the
- * same in FP64, out[5] divisions and out[6] sqrt+exp of the residual.
- * Adds and multiplies count 1 each, as do divide, sqrt and exp. */
+ * a counting scalar: out[0] residual (FP64), out[1] Jacobian in FP32 (the
+ * closed form for ideal MHD, the forward tangent otherwise), out[2] the
+ * same in FP64, out[3] pivoted solve FP32, out[4] the same in FP64, out[5]
+ * divisions and out[6] sqrt+exp of the residual, out[7] the generic
+ * forward-tangent pass in FP32.  Adds and multiplies count 1 each, as do
+ * divide, sqrt and exp. */
 int grim_count_flops(grim_handle* h, double* out);
+/* Autotuner of the face-flux kernels' launch shapes (register budget per
+ * thread, lane split between i and the face direction): times every
+ * variant of each direction on the state in primOld for the handle's
+ * current Newton mode (its compilation unit) and keeps the fastest.
+ * variants[d] and msBest[d] (may be null) receive the choice and its time
+ * per launch.  Results do not depend on the variant. */
+int grim_autotune(grim_handle* h, int* variants, double* msBest);
+/* Forces one variant (for tests); GRIM_EINVAL when out of range. */
+int grim_set_face_variant(grim_handle* h, int dir, int variant);
 
 /* ---- allocation-free divergence.  No counterpart in the reference: for
  *      callers that cannot call cudaMalloc (their device memory is owned by

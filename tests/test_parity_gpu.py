@@ -312,8 +312,8 @@ def test_cpp_driver_matches_python_binding(tmp_path):
 def test_profile_steps_and_flop_counts():
     """grim_profile_steps advances the state like grim_time_step (same bits)
     and times every kernel group; grim_count_flops counts the templated
-    physics on a counting scalar: the FP32 and FP64 tangent passes do the
-    same operations, and one tangent pass (value + nf derivative lanes: a
+    physics on a counting scalar: the FP32 and FP64 Jacobians do the same
+    operations, and one forward-tangent pass (value + nf derivative lanes: a
     product costs 1 + 3 nf flops, a sum 1 + nf) costs more than a residual
     and less than 3 nf + 2 of them."""
     cfg = PR.fast_mode_config(N=64, nonlinearsolve_rtol=1e-10, nonlinearsolve_atol=1e-24,
@@ -336,7 +336,40 @@ def test_profile_steps_and_flop_counts():
     nf = a.numFluidVars
     assert f["residual64"] > 100
     assert f["tangent32"] == f["tangent64"]
-    assert f["residual64"] < f["tangent32"] < (3 * nf + 2) * f["residual64"]
+    assert f["residual64"] < f["dual_tangent32"] < (3 * nf + 2) * f["residual64"]
+    # the closed-form ideal-MHD Jacobian is cheaper than the generic tangent
+    assert f["tangent32"] < f["dual_tangent32"]
     # pivoted elimination without a 1/pivot reciprocal: n^3/3 multiply-adds
     # plus the substitution, exactly counted for n = 5
     assert f["solve32"] == f["solve64"] and 60 <= f["solve64"] <= 200, f
+
+
+@pytest.mark.parametrize("mode", [C.NEWTON_PARITY_FD64, C.NEWTON_MIXED32])
+def test_autotuned_face_kernels_give_identical_results(mode):
+    """The autotuner only changes launch shapes: a tuned stepper and one with
+    the default variants advance to the same bits."""
+    cfg = PR.orszag_tang_config(N=64, maxNonLinearIter=3)
+    P = PR.orszag_tang_prims(cfg)
+    from grim_b200.timestepper import timeStepper
+    a, b = timeStepper(cfg), timeStepper(cfg)
+    for ts in (a, b):
+        ts.setNewtonMode(mode, 1, 0.0)
+        ts.primOld.setVars(P)
+    tuned = a.autotune()
+    assert set(tuned) == {0, 1}
+    assert 0 <= tuned[0][0] < 2 and 0 <= tuned[1][0] < 6 and all(ms > 0 for _, ms in tuned.values())
+    for _ in range(3):
+        a.timeStep()
+        b.timeStep()
+    assert np.array_equal(a.primOld.getVars(), b.primOld.getVars())
+    # every variant of every direction, forced one at a time, gives the
+    # default's divergence of fluxes
+    ref_div, ref_flux = b.computeDivOfFluxes(P)
+    for d, nv in ((0, 2), (1, 6)):
+        for v in range(nv):
+            a.setFaceVariant(d, v)
+            div, flux = a.computeDivOfFluxes(P)
+            assert np.array_equal(div, ref_div) and np.array_equal(flux, ref_flux), (d, v)
+        a.setFaceVariant(d, 0)
+    with pytest.raises(Exception):
+        a.setFaceVariant(1, 6)
