@@ -150,45 +150,66 @@ GRIM_D void recon_zone(const DevCfg& c, const double* __restrict__ ps, long long
   }
 }
 
+// Shared memory holds what waits: the right face state (slot 2, put there
+// by the caller) while the left element is evaluated, then the left
+// state's fluxes (slots 0, 1) while the right element is; slot [v][thread],
+// 3 x DOF doubles per thread.  Neither holds registers across an element.
 template <int COND, int VISC>
-GRIM_D void riemann_face(const DevCfg& c, int dir, const double* pl, const double* pr, const ZoneGeo<double>& GL,
-                         const ZoneGeo<double>& GR, double* __restrict__ flux, long long z) {
+GRIM_D void riemann_face(const DevCfg& c, int dir, const double* pl, const ZoneGeo<double>& G,
+                         double* __restrict__ flux, long long z, double* __restrict__ park) {
   constexpr int NF = 5 + COND + VISC;
   constexpr int DOF = NF + 3;
   const long long Z = c.Z;
   const int fd = dir + 1;
-  double FL[DOF], UL[DOF], FR[DOF], UR[DOF];
-  double minL, maxL, minR, maxR;
+  const int nt = blockDim.x, t = threadIdx.x;
+  double minL, maxL;
   {
+    double F[DOF], U[DOF];
     ElemT<double, double> e;
     elem_set<COND, VISC>(e, pl[0], pl[1], pl[2], pl[3], pl[4], pl[NF], pl[NF + 1], pl[NF + 2],
-                         COND ? pl[5] : 0., VISC ? pl[5 + COND] : 0., GL, c);
-    fluxes_fluid<COND, VISC>(e, fd, GL.g, FL, 5, 5 + COND);
-    fluxes_B(e, fd, GL.g, FL + NF);
-    fluxes_fluid<COND, VISC>(e, 0, GL.g, UL, 5, 5 + COND);
-    fluxes_B(e, 0, GL.g, UL + NF);
-    char_speeds<COND, VISC>(e, GL, dir, c, minL, maxL);
+                         COND ? pl[5] : 0., VISC ? pl[5 + COND] : 0., G, c);
+    fluxes_fluid<COND, VISC>(e, fd, G.g, F, 5, 5 + COND);
+    fluxes_B(e, fd, G.g, F + NF);
+    fluxes_fluid<COND, VISC>(e, 0, G.g, U, 5, 5 + COND);
+    fluxes_B(e, 0, G.g, U + NF);
+    char_speeds<COND, VISC>(e, G, dir, c, minL, maxL);
+#pragma unroll
+    for (int v = 0; v < DOF; v++) {
+      park[v * nt + t] = F[v];
+      park[(DOF + v) * nt + t] = U[v];
+    }
   }
+  double F[DOF], U[DOF], minR, maxR;
   {
+    double pr[DOF];
+#pragma unroll
+    for (int v = 0; v < DOF; v++) pr[v] = park[(2 * DOF + v) * nt + t];
     ElemT<double, double> e;
     elem_set<COND, VISC>(e, pr[0], pr[1], pr[2], pr[3], pr[4], pr[NF], pr[NF + 1], pr[NF + 2],
-                         COND ? pr[5] : 0., VISC ? pr[5 + COND] : 0., GR, c);
-    fluxes_fluid<COND, VISC>(e, fd, GR.g, FR, 5, 5 + COND);
-    fluxes_B(e, fd, GR.g, FR + NF);
-    fluxes_fluid<COND, VISC>(e, 0, GR.g, UR, 5, 5 + COND);
-    fluxes_B(e, 0, GR.g, UR + NF);
-    char_speeds<COND, VISC>(e, GR, dir, c, minR, maxR);
+                         COND ? pr[5] : 0., VISC ? pr[5 + COND] : 0., G, c);
+    fluxes_fluid<COND, VISC>(e, fd, G.g, F, 5, 5 + COND);
+    fluxes_B(e, fd, G.g, F + NF);
+    fluxes_fluid<COND, VISC>(e, 0, G.g, U, 5, 5 + COND);
+    fluxes_B(e, 0, G.g, U + NF);
+    char_speeds<COND, VISC>(e, G, dir, c, minR, maxR);
   }
   const double cmin = fmin(minL, minR);
   const double cmax = fmax(maxL, maxR);
   if (c.riemann == GRIM_HLL) {
+    const double id = 1. / (cmax - cmin);
 #pragma unroll
-    for (int v = 0; v < DOF; v++)
-      flux[(long long)v * Z + z] = (cmax * FL[v] - cmin * FR[v] + cmin * cmax * (UR[v] - UL[v])) / (cmax - cmin);
+    for (int v = 0; v < DOF; v++) {
+      const double FL = park[v * nt + t], UL = park[(DOF + v) * nt + t];
+      const double num = cmax * FL - cmin * F[v] + cmin * cmax * (U[v] - UL);
+      flux[(long long)v * Z + z] = kFastMath ? num * id : num / (cmax - cmin);
+    }
   } else {
     const double cm = fmax(cmax, -cmin);
 #pragma unroll
-    for (int v = 0; v < DOF; v++) flux[(long long)v * Z + z] = 0.5 * (FL[v] + FR[v] - cm * (UR[v] - UL[v]));
+    for (int v = 0; v < DOF; v++) {
+      const double FL = park[v * nt + t], UL = park[(DOF + v) * nt + t];
+      flux[(long long)v * Z + z] = 0.5 * (FL + F[v] - cm * (U[v] - UL));
+    }
   }
 }
 
@@ -219,7 +240,10 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1(DevCfg c, const doub
   if (lane == 0 || iz > c.N1T - 3) return;
   ZoneGeo<double> G;
   load_geo(G, c, geoF, z, iz, j, 0., 0.5);
-  riemann_face<COND, VISC>(c, 0, pl, lo, G, G, flux, z);
+  extern __shared__ double park_x1[];
+#pragma unroll
+  for (int v = 0; v < DOF; v++) park_x1[(2 * DOF + v) * blockDim.x + threadIdx.x] = lo[v];
+  riemann_face<COND, VISC>(c, 0, pl, G, flux, z, park_x1);
 }
 
 // X2 / X3 faces: the X1 scheme turned sideways.  A warp holds QI
@@ -266,7 +290,10 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_strip(DevCfg c, int dir
     load_geo(G, c, geoC, z, i, other, 0.5, 0.5);
   else
     load_geo(G, c, geoF, z, i, x, 0.5, 0.);
-  riemann_face<COND, VISC>(c, dir, pl, lo, G, G, flux, z);
+  extern __shared__ double park_strip[];
+#pragma unroll
+  for (int v = 0; v < DOF; v++) park_strip[(2 * DOF + v) * blockDim.x + threadIdx.x] = lo[v];
+  riemann_face<COND, VISC>(c, dir, pl, G, flux, z, park_strip);
 }
 
 // ---------------------------------------------------------------------------
@@ -563,6 +590,9 @@ GRIM_D void load_stage_const(StageConst<5 + COND + VISC>& K, const DevCfg& c, in
   for (int v = 0; v < 3; v++) K.B[v] = b.prim[(long long)(c.B1 + v) * Z + z];
   const double dt = b.st->dt;
   K.dtp = (stage == GRIM_HALF_STEP) ? dt / 2. : dt;
+  K.idtp = 1. / K.dtp;
+#pragma unroll
+  for (int v = 0; v < NF; v++) K.Kc[v] = K.divF[v] + K.Sexp[v] - K.Uold[v] * K.idtp;
   if (COND || VISC) {
     const double* po = b.pold;
     ElemT<double, double> eo;
@@ -800,7 +830,7 @@ GRIM_D void tangent_jacobian(const double* P, const StageConst<5 + COND + VISC>&
 }
 
 template <int COND, int VISC, class T>
-__global__ void __launch_bounds__(128) k_newton_fast(DevCfg c, int stage, StageBufs b,
+__global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : 3) k_newton_fast(DevCfg c, int stage, StageBufs b,
                                                               const int* __restrict__ list, long long nlist) {
   constexpr int NF = 5 + COND + VISC;
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -812,12 +842,6 @@ __global__ void __launch_bounds__(128) k_newton_fast(DevCfg c, int stage, StageB
     zijk(c, z, i, j, k);
     ZoneGeo<double> G;
     load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
-    ZoneGeo<T> Gt;
-#pragma unroll
-    for (int m = 0; m < 4; m++)
-#pragma unroll
-      for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = (T)G.gcov[m][q]; Gt.gcon[m][q] = (T)G.gcon[m][q]; }
-    Gt.g = (T)G.g; Gt.alpha = (T)G.alpha; Gt.x1 = (T)G.x1; Gt.x2 = (T)G.x2; Gt.dyn = (T)G.dyn;
     StageConst<NF> K;
     load_stage_const<COND, VISC>(K, c, stage, b, z, G);
     double P[NF], R[NF];
@@ -835,7 +859,17 @@ __global__ void __launch_bounds__(128) k_newton_fast(DevCfg c, int stage, StageB
       if (it == 0) l2first = l2;
       if (l2 <= fmax(c.atol, c.rtol * c.rtol * l2first)) { conv = true; break; }
       T J[NF][NF];
-      tangent_jacobian<COND, VISC, T>(P, K, Gt, c, J);
+      {
+        // the Jacobian's geometry, converted where it is used rather than
+        // kept beside the FP64 copy across the iterations
+        ZoneGeo<T> Gt;
+#pragma unroll
+        for (int m = 0; m < 4; m++)
+#pragma unroll
+          for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = (T)G.gcov[m][q]; Gt.gcon[m][q] = (T)G.gcon[m][q]; }
+        Gt.g = (T)G.g; Gt.alpha = (T)G.alpha; Gt.x1 = (T)G.x1; Gt.x2 = (T)G.x2; Gt.dyn = (T)G.dyn;
+        tangent_jacobian<COND, VISC, T>(P, K, Gt, c, J);
+      }
       T bv[NF], xv[NF];
 #pragma unroll
       for (int v = 0; v < NF; v++) bv[v] = (T)(-R[v]);
@@ -872,11 +906,14 @@ __global__ void __launch_bounds__(128) k_newton_fast(DevCfg c, int stage, StageB
     for (int v = 0; v < NF; v++) b.prim[(long long)v * Z + z] = P[v];
   }
   hist_add(b.st->itHist[stage], min(itsMax, 15), n < nlist);
-  unconv = __syncthreads_count(unconv);
-  // iterations done: max over zones (warp max then atomic)
+  // warp-level tallies: no block barrier, so a warp whose zones converged
+  // early retires without waiting for the rest of its block
+  const int nUnconv = __popc(__ballot_sync(0xffffffffu, unconv != 0));
   for (int o = 16; o > 0; o >>= 1) itsMax = max(itsMax, __shfl_xor_sync(0xffffffffu, itsMax, o));
-  if ((threadIdx.x & 31) == 0) atomicMax((unsigned long long*)&b.st->itersDone[stage], (unsigned long long)itsMax);
-  if (threadIdx.x == 0 && unconv) atomicAdd(&b.st->finalUnconv[stage], (unsigned long long)unconv);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax((unsigned long long*)&b.st->itersDone[stage], (unsigned long long)itsMax);
+    if (nUnconv) atomicAdd(&b.st->finalUnconv[stage], (unsigned long long)nUnconv);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1200,11 +1237,12 @@ void emhd_prepass(const DevCfg& c, const double* ps, const double* geoC, double*
 // Launch-shape variants of the face kernels, chosen per direction by the
 // autotuner (grim_autotune): X1 faces by the register budget (3 or 4
 // resident 128-thread blocks per SM), X2 / X3 faces by that budget and by
-// the lane split QI (i per warp).  Other than ideal MHD only the default.
+// the lane split QI (i per warp).  EMHD has one shape (2 resident blocks).
 template <int C, int V, int MINB>
 static void face_x1_launch(const DevCfg& c, const double* ps, const double* geoF, double* flux, cudaStream_t s) {
   const long long warps = (long long)c.N2T * c.N3T * ((c.N1T - 5 + 30) / 31);
-  k_face_flux_x1<C, V, MINB><<<nblk(warps * 32, 128), 128, 0, s>>>(c, ps, geoF, flux);
+  const size_t park = 3 * (8 + C + V) * 128 * sizeof(double);
+  k_face_flux_x1<C, V, MINB><<<nblk(warps * 32, 128), 128, park, s>>>(c, ps, geoF, flux);
 }
 template <int C, int V, int QI, int MINB>
 static void face_strip_launch(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,
@@ -1212,24 +1250,30 @@ static void face_strip_launch(const DevCfg& c, int dir, const double* ps, const 
   const int NT = (dir == 1) ? c.N2T : c.N3T;
   const long long other = (dir == 1) ? c.N3T : c.N2T;
   const long long warps = (long long)((c.N1T + QI - 1) / QI) * ((NT - 5 + 32 / QI - 2) / (32 / QI - 1)) * other;
-  k_face_flux_strip<C, V, QI, MINB><<<nblk(warps * 32, 128), 128, 0, s>>>(c, dir, ps, geoF, geoC, flux);
+  const size_t park = 3 * (8 + C + V) * 128 * sizeof(double);
+  k_face_flux_strip<C, V, QI, MINB><<<nblk(warps * 32, 128), 128, park, s>>>(c, dir, ps, geoF, geoC, flux);
 }
 template <int C, int V>
 static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,
                         double* flux, int variant, cudaStream_t s) {
-  constexpr bool ideal = (C == 0 && V == 0);
-  if (dir == 0) {
-    if (ideal && variant == 1) face_x1_launch<C, V, ideal ? 4 : 3>(c, ps, geoF, flux, s);
-    else face_x1_launch<C, V, 3>(c, ps, geoF, flux, s);
-    return;
-  }
-  switch (ideal ? variant : 0) {
-    case 1: face_strip_launch<C, V, 4, 4>(c, dir, ps, geoF, geoC, flux, s); break;
-    case 2: face_strip_launch<C, V, 2, 3>(c, dir, ps, geoF, geoC, flux, s); break;
-    case 3: face_strip_launch<C, V, 2, 4>(c, dir, ps, geoF, geoC, flux, s); break;
-    case 4: face_strip_launch<C, V, 8, 3>(c, dir, ps, geoF, geoC, flux, s); break;
-    case 5: face_strip_launch<C, V, 8, 4>(c, dir, ps, geoF, geoC, flux, s); break;
-    default: face_strip_launch<C, V, 4, 3>(c, dir, ps, geoF, geoC, flux, s); break;
+  if constexpr (C == 0 && V == 0) {
+    if (dir == 0) {
+      if (variant == 1) face_x1_launch<C, V, 4>(c, ps, geoF, flux, s);
+      else face_x1_launch<C, V, 3>(c, ps, geoF, flux, s);
+      return;
+    }
+    switch (variant) {
+      case 1: face_strip_launch<C, V, 4, 4>(c, dir, ps, geoF, geoC, flux, s); break;
+      case 2: face_strip_launch<C, V, 2, 3>(c, dir, ps, geoF, geoC, flux, s); break;
+      case 3: face_strip_launch<C, V, 2, 4>(c, dir, ps, geoF, geoC, flux, s); break;
+      case 4: face_strip_launch<C, V, 8, 3>(c, dir, ps, geoF, geoC, flux, s); break;
+      case 5: face_strip_launch<C, V, 8, 4>(c, dir, ps, geoF, geoC, flux, s); break;
+      default: face_strip_launch<C, V, 4, 3>(c, dir, ps, geoF, geoC, flux, s); break;
+    }
+  } else {
+    // EMHD elements need more registers: two resident blocks
+    if (dir == 0) face_x1_launch<C, V, 2>(c, ps, geoF, flux, s);
+    else face_strip_launch<C, V, 4, 2>(c, dir, ps, geoF, geoC, flux, s);
   }
 }
 void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC, double* flux,

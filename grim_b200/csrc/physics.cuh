@@ -165,9 +165,18 @@ GRIM_D void elem_set(ElemT<S, R>& e, const S& rho_in, const S& u_in, const S& v1
     e.uCov[mu] = G.gcov[mu][0] * e.uCon[0] + G.gcov[mu][1] * e.uCon[1] + G.gcov[mu][2] * e.uCon[2] +
                  G.gcov[mu][3] * e.uCon[3];
   e.bCon[0] = B1 * e.uCov[1] + B2 * e.uCov[2] + B3 * e.uCov[3];
+#ifdef GRIM_FAST_MATH
+  {
+    const S iu0 = T(1) / e.uCon[0];  // one division for the three
+    e.bCon[1] = (B1 + e.bCon[0] * e.uCon[1]) * iu0;
+    e.bCon[2] = (B2 + e.bCon[0] * e.uCon[2]) * iu0;
+    e.bCon[3] = (B3 + e.bCon[0] * e.uCon[3]) * iu0;
+  }
+#else
   e.bCon[1] = (B1 + e.bCon[0] * e.uCon[1]) / e.uCon[0];
   e.bCon[2] = (B2 + e.bCon[0] * e.uCon[2]) / e.uCon[0];
   e.bCon[3] = (B3 + e.bCon[0] * e.uCon[3]) / e.uCon[0];
+#endif
 #pragma unroll
   for (int mu = 0; mu < 4; mu++)
     e.bCov[mu] = G.gcov[mu][0] * e.bCon[0] + G.gcov[mu][1] * e.bCon[1] + G.gcov[mu][2] * e.bCon[2] +
@@ -251,8 +260,14 @@ GRIM_D void char_speeds(const ElemT<double, R>& e, const ZoneGeo<double>& G, int
   double B = 2. * (ADotU * BDotU - (ADotB + ADotU * BDotU) * csSqr);
   double C = ADotU * ADotU - (ASqr + ADotU * ADotU) * csSqr;
   double discr = sqrt(fmax(B * B - 4. * A * C, 1.e-16));
+#ifdef GRIM_FAST_MATH
+  const double i2a = 0.5 / A;
+  double mn = (B - discr) * i2a;
+  double mx = (B + discr) * i2a;
+#else
   double mn = -(-B + discr) / 2. / A;
   double mx = -(-B - discr) / 2. / A;
+#endif
   if (mn > -1.e-15) mn = -1.e-15;
   if (mx < 1.e-15) mx = 1.e-15;
   minSpeed = mn;
@@ -373,6 +388,9 @@ struct StageConst {
   double sImpOldQ, sImpOldDP;  // 0.5*(...) partner of the implicit source
   double normQ, normDP;        // EMHD row normalisation
   double dtp;                  // dt' (dt/2 or dt)
+  // fast path, ideal MHD: R = U / dt' + Kc, Kc = divF + Sexp - Uold / dt'
+  double idtp;
+  double Kc[NF];
 };
 
 template <int COND, int VISC, class S, class R>
@@ -387,6 +405,15 @@ GRIM_D void zone_residual(const S* P, const StageConst<5 + COND + VISC>& K, cons
   elem_set<COND, VISC>(e, P[0], P[1], P[2], P[3], P[4], (R)K.B[0], (R)K.B[1], (R)K.B[2], qT, dPT, G, c);
   S U[NF];
   fluxes_fluid<COND, VISC>(e, 0, G.g, U, Q, DP);
+#ifdef GRIM_FAST_MATH
+  if constexpr (COND == 0 && VISC == 0) {
+    // the unknown-independent terms folded into one constant per row
+    const T idtp = (T)K.idtp;
+#pragma unroll
+    for (int v = 0; v < NF; v++) Rout[v] = U[v] * idtp + (T)K.Kc[v];
+    return;
+  }
+#endif
   const T dtp = (T)K.dtp;
 #pragma unroll
   for (int v = 0; v < NF; v++) {

@@ -47,7 +47,8 @@ def test_mks_geometry_matches_oracle():
     dtheta/dX are central differences (eps = 1e-5) of exp/acos/asin
     compositions, which turn the last-ulp differences between CUDA's and
     glibc's functions into ~1e-11 of a derivative; the Christoffels, second
-    differences, agree to 1e-5 of their component's scale."""
+    differences, agree to 1e-5 of their component's scale (at least 1e-3:
+    components that vanish analytically carry FD noise of ~1e-11)."""
     cfg, ts, orc = _pair()
     for loc in (C.CENTER, C.LEFT, C.BOTTOM):
         g = ts.getGeometry(loc)
@@ -68,7 +69,8 @@ def test_mks_geometry_matches_oracle():
             for idx in np.ndindex(4, 4, 4):
                 m = ~np.isnan(b[idx])
                 s = np.abs(b[idx][m]).max()
-                assert np.max(np.abs(a[idx][m] - b[idx][m])) <= 1e-5 * max(s, 1e-10), idx
+                # components that vanish analytically are FD noise (~1e-11)
+                assert np.max(np.abs(a[idx][m] - b[idx][m])) <= 1e-5 * max(s, 1e-3), idx
 
 
 def _load_oracle_geometry(ts, orc):
