@@ -194,10 +194,12 @@ def profile_path(ts, steps, flush):
 def stencil_bytes_per_zone(cfg, dof, nf):
     """Algorithmic HBM bytes of one zone's stencil (all face kernels + the
     epilogue of one stage): the primitives in, the stage constants and the
-    new B out, and the stored geometry words the reconstruction/Riemann/
-    source terms need (22 per face location x 3, 40 Christoffels); none for
-    Minkowski, whose metric is a compile-time constant."""
-    G = 0 if cfg["metric"] == C.MINKOWSKI else 3 * 22 + 40
+    new B out, and the geometry words the reconstruction/Riemann/source
+    terms need (22 per face location x 3, 40 Christoffels).  The geometry
+    is stored once per (i, j) plane, so its words are shared by the N3 + 2
+    ghost zones along X3; none for Minkowski, whose metric is a
+    compile-time constant."""
+    G = 0. if cfg["metric"] == C.MINKOWSKI else (3 * 22 + 40) / float(cfg["N3"] + 2 * cfg["numGhost"] * (cfg["dim"] > 2))
     return 8 * (dof + nf + 3 + G)
 
 
@@ -235,7 +237,14 @@ def rooflines(cfg, prof, prof_fd, device):
     stencil_ms = sum(g[k][0] for k in ("faces_x1", "faces_x2", "faces_x3", "epilogue", "emhd_prepass"))
     stencil_launches = g["epilogue"][1]  # one epilogue per stage
     B = stencil_bytes_per_zone(cfg, prof["dof"], prof["nf"])
-    stencil_gbs = B * zones * stencil_launches / (stencil_ms * 1e-3) / 1e9 if stencil_ms > 0 else None
+    fz = prof["flops"]
+    # counted FP64 flops of one zone's stencil stage: per direction one
+    # reconstruction and (about) one face, plus the epilogue's centre work
+    F = cfg["dim"] * (fz["recon_zone_dir"] + fz["riemann_face"]) + fz["epilogue_zone"]
+    t_st = stencil_ms * 1e-3 / stencil_launches  # s per stage
+    st_gbs = B * zones / t_st / 1e9
+    st_tf = F * zones / t_st / 1e12
+    t_hbm, t_fp = B * zones / (hbm_peak * 1e9), F * zones / (fp64_peak * 1e12)
     f64, f32 = newton_flops(prof)
     newton_ms, newton_launches = g["newton"]
     n64 = f64 / (newton_ms * 1e-3) / 1e12
@@ -249,17 +258,31 @@ def rooflines(cfg, prof, prof_fd, device):
               "kernel": "newton (one launch per stage)", "ms_per_launch": newton_ms / newton_launches,
               "flops_per_zone": prof["flops"],
               "peak_source": "measured: FMA-chain self-test of this GPU (grim_measure_peaks)"}
-    stencil = {"bound": "hbm", "achieved": stencil_gbs, "peak": hbm_peak, "unit": "GB/s",
-               "frac": (stencil_gbs / hbm_peak) if stencil_gbs else None,
-               "traffic": traffic.get("stencil"),
-               "kernel": "stencil (face fluxes x%d + epilogue, per stage)" % cfg["dim"],
-               "ms_per_launch": stencil_ms / stencil_launches, "bytes_per_zone": B,
-               "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)", "hbm_selftest_gbs": hbm_local}
+    common = {"traffic": traffic.get("stencil"),
+              "kernel": "stencil (face fluxes x%d + epilogue, per stage)" % cfg["dim"],
+              "ms_per_launch": t_st * 1e3, "bytes_per_zone": B, "flops_per_zone": F,
+              "hbm_achieved_gbs": st_gbs, "hbm_peak_gbs": hbm_peak, "hbm_frac": st_gbs / hbm_peak,
+              "fp64_achieved_tflops": st_tf, "fp64_peak_tflops": fp64_peak, "fp64_frac": st_tf / fp64_peak,
+              "peak_source": "HBM of measured (MEASURED_PEAKS.json hbm_gbs); FP64 measured (grim_measure_peaks)",
+              "hbm_selftest_gbs": hbm_local}
+    if t_fp >= t_hbm:
+        stencil = dict({"bound": "fp64", "achieved": st_tf, "peak": fp64_peak, "unit": "TFLOP/s",
+                        "frac": st_tf / fp64_peak}, **common)
+    else:
+        stencil = dict({"bound": "hbm", "achieved": st_gbs, "peak": hbm_peak, "unit": "GB/s",
+                        "frac": st_gbs / hbm_peak}, **common)
+    # whole step against sum over the stencil and Newton kernels of
+    # max(bytes / BW, flops / peak) (the other kernels are not in the bound)
+    t_newton_bound = f64 / (fp64_peak * 1e12) + f32 / (fp32_peak * 1e12)  # all profiled steps
+    t_bound = steps * 2 * max(t_hbm, t_fp) + t_newton_bound
+    step_bound = {"zone_cycles_per_s": zones * steps / t_bound,
+                  "achieved_profiled": zones * steps / (sum(v[0] for v in g.values()) * 1e-3)}
+    step_bound["frac"] = step_bound["achieved_profiled"] / step_bound["zone_cycles_per_s"]
     total = sum(v[0] for v in g.values())
     shares = {k: round(v[0] / total, 4) for k, v in g.items() if v[0] > 0}
     dominant = newton if g["newton"][0] >= stencil_ms else stencil
     out = {"roofline": dict(dominant), "roofline_other": stencil if dominant is newton else newton,
-           "kernel_shares": shares, "profiled_ms_per_step": total / steps}
+           "step_roofline": step_bound, "kernel_shares": shares, "profiled_ms_per_step": total / steps}
     if prof_fd is not None:
         gf = prof_fd["groups"]
         tf = sum(v[0] for v in gf.values())
@@ -298,7 +321,12 @@ def run_gpu(args, rank, world, local_rank):
             state["P"] = torus_state(cfg, ts)
         ts.primOld.setVars(state["P"])
         ts.problemInit()
-        state.setdefault("tuned", {})[mode] = {str(d): v for d, (v, _) in ts.autotune().items()}
+        if args.variants:
+            for d, v in enumerate(int(x) for x in args.variants.split(",")):
+                ts.setFaceVariant(d, v)
+            state.setdefault("tuned", {})[mode] = "forced " + args.variants
+        else:
+            state.setdefault("tuned", {})[mode] = {str(d): v for d, (v, _) in ts.autotune().items()}
         if graph:
             ts.enableGraph(True)
         stream = torch.cuda.ExternalStream(ts.stream())
@@ -401,6 +429,8 @@ def main():
     ap.add_argument("--grid", default=None, help="override the workload size: N1xN2xN3 (torus) or N")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fd", action="store_true", help="skip the FD64 comparison path (profiler captures)")
+    ap.add_argument("--variants", default=None,
+                    help="face-kernel launch variants per direction, e.g. 1,5,5, instead of autotuning")
     ap.add_argument("--per-zone", type=int, default=1,
                     help="fast Newton: 1 = per-zone loop in one kernel, 2 = compacted worklists")
     args = ap.parse_args()

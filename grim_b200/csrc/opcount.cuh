@@ -4,7 +4,8 @@
 // one zone by one thread.  Every add/subtract, multiply, divide, square root
 // and exponential on the counting type is tallied per precision; signs,
 // comparisons, min/max and conversions are not flops and are not counted.
-// The counts feed the FP64/FP32 pipe rooflines of the Newton kernels.
+// The counts feed the FP64/FP32 pipe rooflines of the Newton and stencil
+// kernels.
 //
 // Included by kernels_fast.cu only (one definition of the tally).
 #pragma once
@@ -52,6 +53,9 @@ struct Cnt {
   friend GRIM_D Cnt dmin2(Cnt a, Cnt b) { return a.v <= b.v ? a : b; }
   friend GRIM_D Cnt dmax2(Cnt a, Cnt b) { return a.v >= b.v ? a : b; }
   friend GRIM_D Cnt dcube(Cnt a) { return a * a * a; }
+  friend GRIM_D Cnt fmin(Cnt a, Cnt b) { return a.v <= b.v ? a : b; }
+  friend GRIM_D Cnt fmax(Cnt a, Cnt b) { return a.v >= b.v ? a : b; }
+  friend GRIM_D Cnt copysign(Cnt a, Cnt b) { return Cnt(::copysign((double)a.v, (double)b.v)); }
   friend GRIM_D bool isfinite(Cnt a) { return ::isfinite((double)a.v); }
 };
 
@@ -65,8 +69,12 @@ namespace GRIM_KNS {
 // One thread, one zone z of the stage buffers b (filled by a stage set-up):
 // out = {residual fp64, Jacobian(fp32) fp32, Jacobian(fp64) fp64,
 //        solve fp32, solve fp64, residual divides, residual sqrt+exp,
-//        generic forward-tangent pass fp32}; the Jacobian is the closed
-// form for ideal MHD and the forward tangent otherwise
+//        generic forward-tangent pass fp32, reconstruction of one zone
+//        along one direction (all dof), Riemann solve of one face,
+//        epilogue centre work of one zone (element, conserved vector,
+//        geometric source contraction; CT and divergence not counted)};
+// the Jacobian is the closed form for ideal MHD and the forward tangent
+// otherwise
 template <int COND, int VISC>
 __global__ void k_count_ops(DevCfg c, int stage, StageBufs b, long long z, double* out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -138,6 +146,75 @@ __global__ void k_count_ops(DevCfg c, int stage, StageBufs b, long long z, doubl
     clear();
     gauss_solve<C8, NF>(J, bv, xv);
     out[4] = flops(0);
+  }
+  // stencil work, FP64
+  {
+    typedef Cnt<double> C8;
+    constexpr int DOF = NF + 3;
+    ZoneGeo<C8> Gc;
+    for (int m = 0; m < 4; m++)
+      for (int q = 0; q < 4; q++) { Gc.gcov[m][q] = C8(G.gcov[m][q]); Gc.gcon[m][q] = C8(G.gcon[m][q]); }
+    Gc.g = C8(G.g); Gc.alpha = C8(G.alpha); Gc.x1 = C8(G.x1); Gc.x2 = C8(G.x2); Gc.dyn = C8(G.dyn);
+    const double* ps = b.ps;
+    // reconstruction of every dof of the zone along X1
+    clear();
+    C8 lo[DOF], ro[DOF];
+    for (int v = 0; v < DOF; v++) {
+      const double* a = ps + (long long)v * Z + z;
+      recon_faces_fast<C8>(c.reconstruction, c.theta, C8(a[-2]), C8(a[-1]), C8(a[0]), C8(a[1]), C8(a[2]), lo[v],
+                           ro[v]);
+    }
+    out[8] = flops(0);
+    // one face: both states through the element, fluxes along X1 and X0,
+    // characteristic speeds, then the HLL / LLF combination
+    clear();
+    C8 F[2][DOF], U[2][DOF], mn[2], mx[2];
+    for (int side = 0; side < 2; side++) {
+      const C8* q = side ? lo : ro;
+      ElemT<C8, C8> e;
+      elem_set<COND, VISC>(e, q[0], q[1], q[2], q[3], q[4], q[NF], q[NF + 1], q[NF + 2], COND ? q[5] : C8(0.),
+                           VISC ? q[5 + COND] : C8(0.), Gc, c);
+      fluxes_fluid<COND, VISC>(e, 1, Gc.g, F[side], 5, 5 + COND);
+      fluxes_B(e, 1, Gc.g, F[side] + NF);
+      fluxes_fluid<COND, VISC>(e, 0, Gc.g, U[side], 5, 5 + COND);
+      fluxes_B(e, 0, Gc.g, U[side] + NF);
+      char_speeds<COND, VISC>(e, Gc, 0, c, mn[side], mx[side]);
+    }
+    const C8 cmin = mn[0] <= mn[1] ? mn[0] : mn[1], cmax = mx[0] >= mx[1] ? mx[0] : mx[1];
+    C8 fl[DOF];
+    if (c.riemann == GRIM_HLL) {
+      const C8 id = C8(1.) / (cmax - cmin);
+      for (int v = 0; v < DOF; v++)
+        fl[v] = (cmax * F[0][v] - cmin * F[1][v] + cmin * cmax * (U[1][v] - U[0][v])) * id;
+    } else {
+      const C8 cm = cmax >= -cmin ? cmax : -cmin;
+      for (int v = 0; v < DOF; v++) fl[v] = C8(0.5) * (F[0][v] + F[1][v] - cm * (U[1][v] - U[0][v]));
+    }
+    out[9] = flops(0);
+    // epilogue centre: element, conserved vector, -g T^k_l Gamma^l_kn
+    clear();
+    {
+      ElemT<C8, C8> e;
+      elem_set<COND, VISC>(e, C8(ps[z]), C8(ps[Z + z]), C8(ps[2 * Z + z]), C8(ps[3 * Z + z]), C8(ps[4 * Z + z]),
+                           C8(ps[(long long)c.B1 * Z + z]), C8(ps[(long long)(c.B1 + 1) * Z + z]),
+                           C8(ps[(long long)(c.B1 + 2) * Z + z]), C8(0.), C8(0.), Gc, c);
+      C8 Uc[NF], UB[3];
+      fluxes_fluid<COND, VISC>(e, 0, Gc.g, Uc, 5, 5 + COND);
+      fluxes_B(e, 0, Gc.g, UB);
+      if (c.metric != GRIM_MINKOWSKI) {
+        C8 T[4][4];
+        for (int ka = 0; ka < 4; ka++)
+          for (int la = 0; la < 4; la++) T[ka][la] = tmunu<COND, VISC>(e, ka, la);
+        C8 S[4];
+        for (int nu = 0; nu < 4; nu++) {
+          S[nu] = C8(0.);
+          for (int ka = 0; ka < 4; ka++)
+            for (int la = 0; la < 4; la++) S[nu] = S[nu] - Gc.g * T[ka][la] * C8(1.);
+        }
+        (void)S;
+      }
+    }
+    out[10] = flops(0);
   }
 }
 

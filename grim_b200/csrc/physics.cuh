@@ -236,40 +236,41 @@ GRIM_D void fluxes_B(const ElemT<S, R>& e, int dir, R g, S* out3) {
 }
 
 // computeMinMaxCharSpeeds (riemannsolver.cpp:54-200), dir = 0,1,2
-template <int COND, int VISC, class R>
-GRIM_D void char_speeds(const ElemT<double, R>& e, const ZoneGeo<double>& G, int dir,
-                        const DevCfg& c, double& minSpeed, double& maxSpeed) {
-  const double Gam = c.Gam;
-  double cAlvenSqr = e.bSqr / (e.rho + Gam * e.u + e.bSqr);
-  double csSqr = e.soundSpeed * e.soundSpeed;
-  double cVisSqr = 0.;
-  if (VISC) cVisSqr = 4. / 3. / (e.rho + Gam * e.u) * e.rho * e.nu / e.tau;
-  double cConSqr = 0.;
-  if (COND) cConSqr = (Gam - 1.) * e.chi / e.tau;
-  cConSqr = 0.5 * (csSqr + cConSqr + sqrt(csSqr * csSqr + cConSqr * cConSqr));
+// (templated on the scalar for the op-counting build; double in the kernels)
+template <int COND, int VISC, class S, class R>
+GRIM_D void char_speeds(const ElemT<S, R>& e, const ZoneGeo<R>& G, int dir, const DevCfg& c, S& minSpeed,
+                        S& maxSpeed) {
+  const S Gam = S(c.Gam);
+  S cAlvenSqr = e.bSqr / (e.rho + Gam * e.u + e.bSqr);
+  S csSqr = e.soundSpeed * e.soundSpeed;
+  S cVisSqr = S(0.);
+  if (VISC) cVisSqr = S(4.) / S(3.) / (e.rho + Gam * e.u) * e.rho * e.nu / e.tau;
+  S cConSqr = S(0.);
+  if (COND) cConSqr = (Gam - S(1.)) * e.chi / e.tau;
+  cConSqr = S(0.5) * (csSqr + cConSqr + dsqrt(csSqr * csSqr + cConSqr * cConSqr));
   csSqr = cConSqr + cVisSqr;
   csSqr = csSqr + cAlvenSqr - csSqr * cAlvenSqr;
-  if (csSqr > 1.) csSqr = 1.;
+  if (csSqr > S(1.)) csSqr = S(1.);
   const int s = dir + 1;
-  const double ASqr = G.gcon[s][s];
-  const double BSqr = G.gcon[0][0];
-  const double ADotU = e.uCon[s];
-  const double BDotU = e.uCon[0];
-  const double ADotB = G.gcon[s][0];
-  double A = (BDotU * BDotU) - (BSqr + BDotU * BDotU) * csSqr;
-  double B = 2. * (ADotU * BDotU - (ADotB + ADotU * BDotU) * csSqr);
-  double C = ADotU * ADotU - (ASqr + ADotU * ADotU) * csSqr;
-  double discr = sqrt(fmax(B * B - 4. * A * C, 1.e-16));
+  const S ASqr = G.gcon[s][s];
+  const S BSqr = G.gcon[0][0];
+  const S ADotU = e.uCon[s];
+  const S BDotU = e.uCon[0];
+  const S ADotB = G.gcon[s][0];
+  S A = (BDotU * BDotU) - (BSqr + BDotU * BDotU) * csSqr;
+  S B = S(2.) * (ADotU * BDotU - (ADotB + ADotU * BDotU) * csSqr);
+  S C = ADotU * ADotU - (ASqr + ADotU * ADotU) * csSqr;
+  S discr = dsqrt(dmax2(B * B - S(4.) * A * C, S(1.e-16)));
 #ifdef GRIM_FAST_MATH
-  const double i2a = 0.5 / A;
-  double mn = (B - discr) * i2a;
-  double mx = (B + discr) * i2a;
+  const S i2a = S(0.5) / A;
+  S mn = (B - discr) * i2a;
+  S mx = (B + discr) * i2a;
 #else
-  double mn = -(-B + discr) / 2. / A;
-  double mx = -(-B - discr) / 2. / A;
+  S mn = -(-B + discr) / S(2.) / A;
+  S mx = -(-B - discr) / S(2.) / A;
 #endif
-  if (mn > -1.e-15) mn = -1.e-15;
-  if (mx < 1.e-15) mx = 1.e-15;
+  if (mn > S(-1.e-15)) mn = S(-1.e-15);
+  if (mx < S(1.e-15)) mx = S(1.e-15);
   minSpeed = mn;
   maxSpeed = mx;
 }

@@ -988,12 +988,12 @@ int grim_count_flops(grim_handle* h, double* out) {
   if (!h || !out) { set_err("grim_count_flops: null argument"); return GRIM_EINVAL; }
   CK(cudaSetDevice(h->device));
   double* d = nullptr;
-  CK(cudaMalloc(&d, 8 * sizeof(double)));
-  CK(cudaMemsetAsync(d, 0, 8 * sizeof(double), h->stream));
+  CK(cudaMalloc(&d, 11 * sizeof(double)));
+  CK(cudaMemsetAsync(d, 0, 11 * sizeof(double), h->stream));
   const long long z = interior_to_z(h->dc, h->dc.Zint / 2);
   grim::fast::count_ops(h->dc, h->lastStage, stage_bufs(h, h->lastStage), z, d, h->stream);
   cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, 11 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   cudaFree(d);
   if (e != cudaSuccess) { set_err("grim_count_flops: %s", cudaGetErrorString(e)); return GRIM_ECUDA; }

@@ -196,10 +196,10 @@ class timeStepper:
     def countFlops(self):
         """Algorithmic flops of one zone: residual (FP64), tangent pass
         (FP32 and FP64), pivoted solve (FP32 and FP64)."""
-        out = (ctypes.c_double * 8)()
+        out = (ctypes.c_double * 11)()
         _lib.check(_lib.lib().grim_count_flops(self._h, out), "count_flops")
         keys = ("residual64", "tangent32", "tangent64", "solve32", "solve64", "residual_div", "residual_sqrt_exp",
-                "dual_tangent32")
+                "dual_tangent32", "recon_zone_dir", "riemann_face", "epilogue_zone")
         return {k: out[i] for i, k in enumerate(keys)}
 
     # ---- stage pieces --------------------------------------------------------

@@ -237,8 +237,11 @@ int grim_profile_steps(grim_handle* h, int nsteps, double* msPerGroup, long long
  * closed form for ideal MHD, the forward tangent otherwise), out[2] the
  * same in FP64, out[3] pivoted solve FP32, out[4] the same in FP64, out[5]
  * divisions and out[6] sqrt+exp of the residual, out[7] the generic
- * forward-tangent pass in FP32.  Adds and multiplies count 1 each, as do
- * divide, sqrt and exp. */
+ * forward-tangent pass in FP32; stencil work in FP64: out[8] the
+ * reconstruction of one zone along one direction (all dof), out[9] the
+ * Riemann solve of one face, out[10] the epilogue's centre work of one zone
+ * (element, conserved vector, geometric source contraction).  Adds and
+ * multiplies count 1 each, as do divide, sqrt and exp; out holds 11. */
 int grim_count_flops(grim_handle* h, double* out);
 /* Autotuner of the face-flux kernels' launch shapes (register budget per
  * thread, lane split between i and the face direction): times every
