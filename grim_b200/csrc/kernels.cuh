@@ -107,6 +107,29 @@ static __global__ void k_communicate(DevCfg c, double* __restrict__ prim, int nv
 }
 
 // ---------------------------------------------------------------------------
+// computeDivB (constrainedtransport.cpp:85-110): corner divergence of
+// sqrt(-g) B in 2D from ArrayFire's circular shifts over the whole array,
+// ghosts included; zero in 1D and 3D, where the reference writes nothing
+// ---------------------------------------------------------------------------
+static __global__ void k_divb(DevCfg c, const double* __restrict__ p, const double* __restrict__ geoC,
+                              double* __restrict__ out) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  if (c.dim != 2) { out[z] = 0.; return; }
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  auto gB = [&](int v, int ii, int jj) -> double {
+    ii = (ii + c.N1T) % c.N1T;
+    jj = (jj + c.N2T) % c.N2T;
+    const double g = geoC ? __ldg(geoC + 32LL * c.GZ + gidx(c, ii, jj)) : 1.;
+    return g * p[(long long)(c.B1 + v) * c.Z + zidx(c, ii, jj, k)];
+  };
+  const double a = gB(0, i, j), a01 = gB(0, i, j - 1), a10 = gB(0, i - 1, j), a11 = gB(0, i - 1, j - 1);
+  const double b = gB(1, i, j), b10 = gB(1, i - 1, j), b01 = gB(1, i, j - 1), b11 = gB(1, i - 1, j - 1);
+  out[z] = (a + a01 - a10 - a11) / (2. * c.dX[0]) + (b + b10 - b01 - b11) / (2. * c.dX[1]);
+}
+
+// ---------------------------------------------------------------------------
 // EMHD pre-pass: u_mu and T of the stage element at every zone
 // ---------------------------------------------------------------------------
 template <int COND, int VISC>
@@ -1434,6 +1457,9 @@ static void torus_bcs_t(const DevCfg& c, double* p, const double* geoC, cudaStre
 }
 void torus_bcs(const DevCfg& c, double* p, const double* geoC, cudaStream_t s) {
   GRIM_EMHD_DISPATCH(c, torus_bcs_t, c, p, geoC, s);
+}
+void divb(const DevCfg& c, const double* p, const double* geoC, double* out, cudaStream_t s) {
+  k_divb<<<nblk(c.Z, 256), 256, 0, s>>>(c, p, geoC, out);
 }
 void count_nonfinite(const DevCfg& c, const double* p, DevState* st, cudaStream_t s) {
   k_count_nonfinite<<<nblk(c.Zint, 256), 256, 0, s>>>(c, p, st);

@@ -649,9 +649,15 @@ int grim_reconstruct(grim_handle* h, const double* prim, int dir, double* pl, do
 }
 
 int grim_compute_divb(grim_handle* h, const double* prim, double* divB, int memKind) {
-  (void)h; (void)prim; (void)divB; (void)memKind;
-  set_err("grim_compute_divb: use the Python harness diagnostic");
-  return GRIM_ENOTSUP;
+  if (!h || !prim || !divB) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  const DevCfg& c = h->dc;
+  int rc = stage_in(h, h->scratch, prim, c.dof, memKind);
+  if (rc) return rc;
+  const bool mink = h->cfg.metric == GRIM_MINKOWSKI;
+  grim::exact::divb(c, h->scratch, mink ? nullptr : h->geo[GRIM_CENTER], h->scratch2, h->stream);
+  CK(cudaGetLastError());
+  return stage_out(h, divB, h->scratch2, h->bytesZ, memKind);
 }
 
 int grim_conserved(grim_handle* h, const double* prim, double* cons, int memKind) {

@@ -218,6 +218,13 @@ class timeStepper:
                                                       _lib.HOST), "computeDivOfFluxes")
         return divF, fl
 
+    def computeDivB(self, prim):
+        """timeStepperPy.computeDivB: corner divergence of sqrt(-g) B (2D)."""
+        p = np.ascontiguousarray(prim, dtype=np.float64)
+        out = np.zeros(self.zshape)
+        _lib.check(_lib.lib().grim_compute_divb(self._h, _ptr(p), _ptr(out), _lib.HOST), "computeDivB")
+        return out
+
     def reconstruct(self, prim, direction):
         p = np.ascontiguousarray(prim, dtype=np.float64)
         pl, pr = self._zeros(self.dof), self._zeros(self.dof)

@@ -151,7 +151,9 @@ int grim_compute_div_fluxes(grim_handle* h, const double* prim, double* divF,
 /* reconstruction of one direction (reconstruction.cpp:3-36) */
 int grim_reconstruct(grim_handle* h, const double* prim, int dir,
                      double* primLeft, double* primRight, int memKind);
-/* computeDivB diagnostic (constrainedtransport.cpp:85-107), 2D */
+/* computeDivB diagnostic (constrainedtransport.cpp:85-110): divB (1 x Z)
+ * at the zone corners from sqrt(-g) B with circular shifts over the whole
+ * array; 2D only, zeros otherwise (the reference leaves it unwritten). */
 int grim_compute_divb(grim_handle* h, const double* prim, double* divB, int memKind);
 /* conserved variables and characteristic speeds of a prim array at the
  * zone centres (physics.cpp:185-217, riemannsolver.cpp:54-200) */

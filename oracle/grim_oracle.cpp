@@ -1728,6 +1728,27 @@ int orc_conserved(orc_handle* h, const double* prim, double* cons) {
   std::memcpy(cons, c.d.data(), sizeof(double) * c.d.size());
   return 0;
 }
+/* computeDivB (constrainedtransport.cpp:85-110), 2D */
+int orc_compute_divb(orc_handle* h, const double* prim, double* divB) {
+  Stepper& s = h->s;
+  const Layout& L = s.L;
+  const long Z = L.Z;
+  for (long z = 0; z < Z; z++) divB[z] = 0.;
+  if (L.dim != 2) return 0;
+  std::vector<double> gB1(Z), gB2(Z), a(Z), b(Z), c(Z), d(Z), e(Z), f(Z);
+  const double* B1 = prim + (long)s.P.B1 * Z;
+  const double* B2 = prim + (long)s.P.B2 * Z;
+  for (long z = 0; z < Z; z++) { gB1[z] = s.geomCenter.g[z] * B1[z]; gB2[z] = s.geomCenter.g[z] * B2[z]; }
+  shift(L, gB1.data(), 0, 1, 0, a.data());
+  shift(L, gB1.data(), 1, 0, 0, b.data());
+  shift(L, gB1.data(), 1, 1, 0, c.data());
+  shift(L, gB2.data(), 1, 0, 0, d.data());
+  shift(L, gB2.data(), 0, 1, 0, e.data());
+  shift(L, gB2.data(), 1, 1, 0, f.data());
+  for (long z = 0; z < Z; z++)
+    divB[z] = (gB1[z] + a[z] - b[z] - c[z]) / (2. * s.dX[0]) + (gB2[z] + d[z] - e[z] - f[z]) / (2. * s.dX[1]);
+  return 0;
+}
 int orc_char_speeds(orc_handle* h, const double* prim, int dir, double* mn, double* mx) {
   Stepper& s = h->s;
   const long Z = s.L.Z; const int dof = s.P.dof;

@@ -91,6 +91,7 @@ int  orc_reconstruct(orc_handle* h, const double* prim, int dir,
                      double* primLeft, double* primRight);
 /* conserved variables U = computeFluxes(0) of prim, dof x Z */
 int  orc_conserved(orc_handle* h, const double* prim, double* cons);
+int  orc_compute_divb(orc_handle* h, const double* prim, double* divB);
 /* characteristic speeds of prim at the centre in one direction */
 int  orc_char_speeds(orc_handle* h, const double* prim, int dir,
                      double* minSpeed, double* maxSpeed);

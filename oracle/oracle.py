@@ -82,6 +82,7 @@ def lib():
         L.orc_div_fluxes.argtypes = [vp, P(d), P(d), P(d), P(d)]
         L.orc_reconstruct.argtypes = [vp, P(d), i, P(d), P(d)]
         L.orc_conserved.argtypes = [vp, P(d), P(d)]
+        L.orc_compute_divb.argtypes = [vp, P(d), P(d)]
         L.orc_char_speeds.argtypes = [vp, P(d), i, P(d), P(d)]
         L.orc_stage_setup.argtypes = [vp, i]
         L.orc_residual.argtypes = [vp, P(d), P(d)]
@@ -223,6 +224,12 @@ class Oracle:
         c = self._arr()
         lib().orc_conserved(self._h, _ptr(p), _ptr(c))
         return c
+
+    def compute_divb(self, prim):
+        p = np.ascontiguousarray(prim, dtype=np.float64)
+        out = np.zeros(self.zshape)
+        lib().orc_compute_divb(self._h, _ptr(p), _ptr(out))
+        return out
 
     def char_speeds(self, prim, direction):
         p = np.ascontiguousarray(prim, dtype=np.float64)
