@@ -342,6 +342,31 @@ GRIM_D double emf2(const FluxView& f, long long z, long long s1, long long s3) {
   return 0.25 * (f.at(2, f.B1, z) + f.at(2, f.B1, z - s1) - f.at(0, f.B1 + 2, z) - f.at(0, f.B1 + 2, z - s3));
 }
 
+// computeEMF (constrainedtransport.cpp:53-83) as arrays over the whole grid,
+// neighbours by circular shift as in the reference: out = [emfX1 | emfX2 |
+// emfX3] x Z (emfX1, emfX2 only in 3D, emfX3 from 2D on; zero otherwise)
+static __global__ void k_emf(DevCfg c, const double* __restrict__ F1, const double* __restrict__ F2,
+                             const double* __restrict__ F3, double* __restrict__ out) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  const long long Z = c.Z;
+  const long long zi = zidx(c, (i - 1 + c.N1T) % c.N1T, j, k);
+  const long long zj = zidx(c, i, (j - 1 + c.N2T) % c.N2T, k);
+  const long long zk = zidx(c, i, j, (k - 1 + c.N3T) % c.N3T);
+  const long long b1 = (long long)c.B1 * Z, b2 = b1 + Z, b3 = b2 + Z;
+  double e1 = 0., e2 = 0., e3 = 0.;
+  if (c.dim >= 2) e3 = 0.25 * (F1[b2 + z] + F1[b2 + zj] - F2[b1 + z] - F2[b1 + zi]);
+  if (c.dim == 3) {
+    e1 = 0.25 * (F2[b3 + z] + F2[b3 + zk] - F3[b2 + z] - F3[b2 + zj]);
+    e2 = 0.25 * (F3[b1 + z] + F3[b1 + zi] - F1[b3 + z] - F1[b3 + zk]);
+  }
+  out[z] = e1;
+  out[Z + z] = e2;
+  out[2 * Z + z] = e3;
+}
+
 template <int COND, int VISC>
 __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, StageBufs b) {
   constexpr int NF = 5 + COND + VISC;
@@ -1457,6 +1482,10 @@ static void torus_bcs_t(const DevCfg& c, double* p, const double* geoC, cudaStre
 }
 void torus_bcs(const DevCfg& c, double* p, const double* geoC, cudaStream_t s) {
   GRIM_EMHD_DISPATCH(c, torus_bcs_t, c, p, geoC, s);
+}
+void emf(const DevCfg& c, const double* const* flux, double* out, cudaStream_t s) {
+  k_emf<<<nblk(c.Z, 256), 256, 0, s>>>(c, flux[0], c.dim >= 2 ? flux[1] : flux[0], c.dim >= 3 ? flux[2] : flux[0],
+                                         out);
 }
 void divb(const DevCfg& c, const double* p, const double* geoC, double* out, cudaStream_t s) {
   k_divb<<<nblk(c.Z, 256), 256, 0, s>>>(c, p, geoC, out);

@@ -33,6 +33,7 @@
   int batch_solve(int n, int batch, const double* A, const double* b, double* x, cudaStream_t s);      \
   void count_nonfinite(const DevCfg& c, const double* p, DevState* st, cudaStream_t s);                \
   void divb(const DevCfg& c, const double* p, const double* geoC, double* out, cudaStream_t s);        \
+  void emf(const DevCfg& c, const double* const* flux, double* out, cudaStream_t s);                   \
   void torus_floor(const DevCfg& c, double* p, const double* geoC, const unsigned long long* flag,     \
                    cudaStream_t s);                                                                     \
   void torus_nan_flag(const DevCfg& c, const double* p, unsigned long long* flag, cudaStream_t s);      \

@@ -628,7 +628,14 @@ int grim_compute_div_fluxes(grim_handle* h, const double* prim, double* divF, do
       }
     }
   }
-  (void)emf;
+  if (emf) {
+    // three rows of Z; the scratch prims are no longer needed
+    const double* fl[3] = {h->flux[0], h->flux[1], h->flux[2]};
+    grim::exact::emf(c, fl, h->scratch, h->stream);
+    CK(cudaGetLastError());
+    rc = stage_out(h, emf, h->scratch, 3 * h->bytesZ, memKind);
+    if (rc) return rc;
+  }
   CK(cudaStreamSynchronize(h->stream));
   return GRIM_OK;
 }

@@ -218,6 +218,15 @@ class timeStepper:
                                                       _lib.HOST), "computeDivOfFluxes")
         return divF, fl
 
+    def computeEMF(self, prim):
+        """timeStepperPy.computeEMF on a prim array: [emfX1, emfX2, emfX3]
+        (3 x Z) from the Riemann fluxes of prim."""
+        p = np.ascontiguousarray(prim, dtype=np.float64)
+        out = np.zeros((3,) + self.zshape)
+        _lib.check(_lib.lib().grim_compute_div_fluxes(self._h, _ptr(p), None, None, _ptr(out), _lib.HOST),
+                   "computeEMF")
+        return out
+
     def computeDivB(self, prim):
         """timeStepperPy.computeDivB: corner divergence of sqrt(-g) B (2D)."""
         p = np.ascontiguousarray(prim, dtype=np.float64)
