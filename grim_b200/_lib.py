@@ -92,6 +92,9 @@ def lib():
         "grim_count_flops": [vp, P(d)],
         "grim_autotune": [vp, P(i), P(d)],
         "grim_set_face_variant": [vp, i, i],
+        "grim_set_dt_mode": [vp, i],
+        "grim_adjoint_forward": [vp, i, i],
+        "grim_adjoint_backward": [vp, vp, vp, i],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -29,6 +29,7 @@ UNITS = {
     "runtime.cu": [],
     "peaks.cu": [],
     "noalloc.cu": EXACT,
+    "adjoint.cu": [],
 }
 
 

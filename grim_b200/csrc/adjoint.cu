@@ -1,0 +1,375 @@
+// adjoint.cu -- reverse (adjoint) sweep of whole implicit timesteps.
+//
+// The forward step (timestep.cpp:3-334) is, per stage with dt' = dt/2 then
+// dt, the implicit system R(P) = (U(P; B) - U(P0)) / dt' + divF(Ps) = 0 for
+// the fluid unknowns, with B = B0 - dt' divF_B(Ps) advanced explicitly and
+// Ps = P0 (half stage) or Ph (full stage).  Given lambda = dL/dP1 at the end
+// of a step, the adjoint of the step is (implicit-function theorem, so the
+// Newton iterations are not differentiated; they are converged):
+//
+//   full stage at P1:  mu = (dU/dPf / dt)^-T lambda_f
+//                      beta = lambda_B - (dU/dB / dt)^T mu
+//                      g_h = [-mu ; -dt beta]      (= dL/d divF(Ph))
+//   lambda_h = D(Ph)^T g_h                          (stencil VJP, ghosts folded)
+//   half stage at Ph:  mu_h, beta_h likewise with dt/2, g_0 = [-mu_h ; -dt/2 beta_h]
+//   lambda_0 = D(P0)^T g_0 + dU(P0)/dP^T (mu/dt + mu_h/(dt/2)) + [0 ; beta + beta_h]
+//
+// D^T is the transpose of the stencil: divergence (fvmfluxes.cpp:36-45),
+// flux-CT / EMF (constrainedtransport.cpp:3-83), Riemann solver
+// (riemannsolver.cpp:202-328) and reconstruction, the last two through
+// local Jacobians taken with the forward-tangent scalar on the same
+// templated physics the kernels run.  Scope: ideal MHD, Minkowski, 2D,
+// periodic in both directions, dt held fixed over the run; the runtime
+// rejects anything else.  Accumulation into zones uses double atomics, so
+// gradients agree run to run to roundoff, not bit for bit.
+#include <cuda_runtime.h>
+
+#include "launch.h"
+#include "physics.cuh"
+#include "recon.cuh"
+
+namespace grim {
+
+// ---- the forward-tangent scalar in the reconstruction's expressions:
+// comparisons on values, min / max / |.| / copysign on the selected branch
+template <class T, int N>
+GRIM_D bool operator<(const Dual<T, N>& a, const Dual<T, N>& b) { return a.v < b.v; }
+template <class T, int N>
+GRIM_D bool operator>(const Dual<T, N>& a, const Dual<T, N>& b) { return a.v > b.v; }
+template <class T, int N>
+GRIM_D bool operator<=(const Dual<T, N>& a, const Dual<T, N>& b) { return a.v <= b.v; }
+template <class T, int N>
+GRIM_D bool operator>=(const Dual<T, N>& a, const Dual<T, N>& b) { return a.v >= b.v; }
+template <class T, int N>
+GRIM_D bool operator<(const Dual<T, N>& a, T b) { return a.v < b; }
+template <class T, int N>
+GRIM_D bool operator>(const Dual<T, N>& a, T b) { return a.v > b; }
+template <class T, int N>
+GRIM_D bool operator<=(const Dual<T, N>& a, T b) { return a.v <= b; }
+template <class T, int N>
+GRIM_D bool operator>=(const Dual<T, N>& a, T b) { return a.v >= b; }
+template <class T, int N>
+GRIM_D Dual<T, N> fabs(const Dual<T, N>& a) { return a.v < T(0) ? -a : a; }
+template <class T, int N>
+GRIM_D Dual<T, N> fmin(const Dual<T, N>& a, const Dual<T, N>& b) { return (b.v < a.v) ? b : a; }
+template <class T, int N>
+GRIM_D Dual<T, N> fmax(const Dual<T, N>& a, const Dual<T, N>& b) { return (b.v > a.v) ? b : a; }
+template <class T, int N>
+GRIM_D Dual<T, N> copysign(T a, const Dual<T, N>& b) { return Dual<T, N>(::copysign(a, b.v)); }
+
+namespace adj {
+
+static inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// Gaussian elimination with partial pivoting (first largest pivot)
+GRIM_D void solve5(double A[5][5], double b[5], double x[5]) {
+  for (int kk = 0; kk < 5; kk++) {
+    int p = kk;
+    double best = ::fabs(A[kk][kk]);
+    for (int r = kk + 1; r < 5; r++)
+      if (::fabs(A[r][kk]) > best) { best = ::fabs(A[r][kk]); p = r; }
+    if (p != kk) {
+      for (int cc = 0; cc < 5; cc++) { const double t = A[kk][cc]; A[kk][cc] = A[p][cc]; A[p][cc] = t; }
+      const double t = b[kk]; b[kk] = b[p]; b[p] = t;
+    }
+    for (int r = kk + 1; r < 5; r++) {
+      const double f = A[r][kk] / A[kk][kk];
+      for (int cc = kk; cc < 5; cc++) A[r][cc] -= f * A[kk][cc];
+      b[r] -= f * b[kk];
+    }
+  }
+  for (int r = 4; r >= 0; r--) {
+    double s = b[r];
+    for (int cc = r + 1; cc < 5; cc++) s -= A[r][cc] * x[cc];
+    x[r] = s / A[r][r];
+  }
+}
+
+// conserved fluid rows U (nf = 5) of one zone and their Jacobian with
+// respect to the 8 primitives (5 fluid, then B), Minkowski
+GRIM_D void cons_jacobian(const DevCfg& c, const double* p, long long z, double J[5][8]) {
+  typedef Dual<double, 8> D;
+  const long long Z = c.Z;
+  D q[8];
+  for (int v = 0; v < 5; v++) q[v] = D::var(p[(long long)v * Z + z], v);
+  for (int v = 0; v < 3; v++) q[5 + v] = D::var(p[(long long)(c.B1 + v) * Z + z], 5 + v);
+  ZoneGeo<D> G;
+  geo_minkowski<D>(G, D(0.), D(0.));
+  ElemT<D, D> e;
+  elem_set<0, 0>(e, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], D(0.), D(0.), G, c);
+  D U[5];
+  fluxes_fluid<0, 0>(e, 0, G.g, U, 5, 5);
+  for (int r = 0; r < 5; r++)
+    for (int k = 0; k < 8; k++) J[r][k] = U[r].d[k];
+}
+
+// Stage adjoint at the stage's solution P (interior zones): lam -> g (dL/d
+// divF, dof rows), ubar (+)= mu / dt', bacc (+)= beta
+__global__ void k_stage(DevCfg c, const double* __restrict__ P, double dtp, const double* __restrict__ lam,
+                        double* __restrict__ g, double* __restrict__ ubar, double* __restrict__ bacc, int accumulate) {
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= c.Zint) return;
+  const long long Z = c.Z;
+  const long long z = interior_to_z(c, n);
+  double J[5][8];
+  cons_jacobian(c, P, z, J);
+  // (J_ff / dt')^T mu = lam_f
+  double AT[5][5], b[5], mu[5];
+  for (int r = 0; r < 5; r++) {
+    b[r] = lam[(long long)r * Z + z];
+    for (int k = 0; k < 5; k++) AT[r][k] = J[k][r] / dtp;
+  }
+  solve5(AT, b, mu);
+  for (int v = 0; v < 5; v++) {
+    g[(long long)v * Z + z] = -mu[v];
+    const double u = mu[v] / dtp;
+    ubar[(long long)v * Z + z] = accumulate ? ubar[(long long)v * Z + z] + u : u;
+  }
+  for (int k = 0; k < 3; k++) {
+    double beta = lam[(long long)(c.B1 + k) * Z + z];
+    for (int r = 0; r < 5; r++) beta -= J[r][5 + k] / dtp * mu[r];
+    g[(long long)(c.B1 + k) * Z + z] = -dtp * beta;
+    bacc[(long long)k * Z + z] = accumulate ? bacc[(long long)k * Z + z] + beta : beta;
+  }
+}
+
+// lam_out(P0) += dU/dP(P0)^T ubar + [0 ; bacc]
+__global__ void k_cons(DevCfg c, const double* __restrict__ P, const double* __restrict__ ubar,
+                       const double* __restrict__ bacc, double* __restrict__ lam) {
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= c.Zint) return;
+  const long long Z = c.Z;
+  const long long z = interior_to_z(c, n);
+  double J[5][8];
+  cons_jacobian(c, P, z, J);
+  for (int k = 0; k < 8; k++) {
+    double s = 0.;
+    for (int r = 0; r < 5; r++) s += J[r][k] * ubar[(long long)r * Z + z];
+    if (k >= 5) s += bacc[(long long)(k - 5) * Z + z];
+    const long long row = (k < 5) ? k : c.B1 + (k - 5);
+    lam[row * Z + z] += s;
+  }
+}
+
+GRIM_D bool is_interior(const DevCfg& c, int i, int j) {
+  return i >= c.g1 && i < c.N1 + c.g1 && j >= c.g2 && j < c.N2 + c.g2;
+}
+
+// divergence transpose: Ft[d][v][f] = (g[v][f - s_d] - g[v][f]) / dX_d,
+// g zero off the interior (the zero-padded convolution of fvmfluxes.cpp)
+__global__ void k_div_t(DevCfg c, const double* __restrict__ g, double* __restrict__ Ft) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  const long long Z = c.Z;
+  for (int d = 0; d < 2; d++) {
+    const int im = d == 0 ? i - 1 : i, jm = d == 0 ? j : j - 1;
+    const bool in0 = is_interior(c, i, j), in1 = is_interior(c, im, jm);
+    const long long zm = zidx(c, im < 0 ? 0 : im, jm < 0 ? 0 : jm, k);
+    const double idx = 1. / c.dX[d];
+    for (int v = 0; v < c.dof; v++) {
+      const double a = in1 ? g[(long long)v * Z + zm] : 0.;
+      const double b = in0 ? g[(long long)v * Z + z] : 0.;
+      Ft[((long long)d * c.dof + v) * Z + z] = (a - b) * idx;
+    }
+  }
+}
+
+// flux-CT transpose, step 1: the corner EMF adjoint from the CT fluxes'
+// adjoints (F1_B2[f] = (e[f] + e[f+s2]) / 2, F2_B1[f] = -(e[f] + e[f+s1]) / 2)
+__global__ void k_ct_t_emf(DevCfg c, const double* __restrict__ Ft, double* __restrict__ ebar) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  const long long Z = c.Z, s1 = 1, s2 = c.N1T;
+  const double* F1B2 = Ft + ((long long)0 * c.dof + c.B1 + 1) * Z;
+  const double* F2B1 = Ft + ((long long)1 * c.dof + c.B1) * Z;
+  double e = 0.5 * F1B2[z] - 0.5 * F2B1[z];
+  if (j >= 1) e += 0.5 * F1B2[z - s2];
+  if (i >= 1) e -= 0.5 * F2B1[z - s1];
+  ebar[z] = e;
+}
+
+// flux-CT transpose, step 2: the raw Riemann fluxes' adjoints of the B
+// rows (e[c] = (F1_B2[c] + F1_B2[c-s2] - F2_B1[c] - F2_B1[c-s1]) / 4);
+// B1 through X1 and B2 through X2 faces never reach the divergence
+__global__ void k_ct_t_raw(DevCfg c, const double* __restrict__ ebar, double* __restrict__ Ft) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  const long long Z = c.Z, s1 = 1, s2 = c.N1T;
+  const double ez = ebar[z];
+  const double ej = (j + 1 < c.N2T) ? ebar[z + s2] : 0.;
+  const double ei = (i + 1 < c.N1T) ? ebar[z + s1] : 0.;
+  Ft[((long long)0 * c.dof + c.B1) * Z + z] = 0.;
+  Ft[((long long)0 * c.dof + c.B1 + 1) * Z + z] = 0.25 * ez + 0.25 * ej;
+  Ft[((long long)1 * c.dof + c.B1) * Z + z] = -0.25 * ez - 0.25 * ei;
+  Ft[((long long)1 * c.dof + c.B1 + 1) * Z + z] = 0.;
+}
+
+// the Riemann flux of one face (riemannsolver.cpp:202-328) on any scalar
+template <class S>
+GRIM_D void riemann_flux(const DevCfg& c, int dir, const S* pl, const S* pr, S* F) {
+  ZoneGeo<S> G;
+  geo_minkowski<S>(G, S(0.), S(0.));
+  const int fd = dir + 1;
+  S FL[8], UL[8], FR[8], UR[8], mnL, mxL, mnR, mxR;
+  {
+    ElemT<S, S> e;
+    elem_set<0, 0>(e, pl[0], pl[1], pl[2], pl[3], pl[4], pl[5], pl[6], pl[7], S(0.), S(0.), G, c);
+    fluxes_fluid<0, 0>(e, fd, G.g, FL, 5, 5);
+    fluxes_B(e, fd, G.g, FL + 5);
+    fluxes_fluid<0, 0>(e, 0, G.g, UL, 5, 5);
+    fluxes_B(e, 0, G.g, UL + 5);
+    char_speeds<0, 0>(e, G, dir, c, mnL, mxL);
+  }
+  {
+    ElemT<S, S> e;
+    elem_set<0, 0>(e, pr[0], pr[1], pr[2], pr[3], pr[4], pr[5], pr[6], pr[7], S(0.), S(0.), G, c);
+    fluxes_fluid<0, 0>(e, fd, G.g, FR, 5, 5);
+    fluxes_B(e, fd, G.g, FR + 5);
+    fluxes_fluid<0, 0>(e, 0, G.g, UR, 5, 5);
+    fluxes_B(e, 0, G.g, UR + 5);
+    char_speeds<0, 0>(e, G, dir, c, mnR, mxR);
+  }
+  const S cmin = dmin2(mnL, mnR), cmax = dmax2(mxL, mxR);
+  if (c.riemann == GRIM_HLL) {
+    for (int v = 0; v < 8; v++) F[v] = (cmax * FL[v] - cmin * FR[v] + cmin * cmax * (UR[v] - UL[v])) / (cmax - cmin);
+  } else {
+    const S cm = dmax2(cmax, -cmin);
+    for (int v = 0; v < 8; v++) F[v] = S(0.5) * (FL[v] + FR[v] - cm * (UR[v] - UL[v]));
+  }
+}
+
+// Riemann + reconstruction transpose of the faces along dir: the face
+// between zones a = z - s and b = z takes Fbar (dof) and adds
+// (dF/dy)^T Fbar to the 5-point stencils of both zones in q
+__global__ void k_faces_t(DevCfg c, int dir, const double* __restrict__ P, const double* __restrict__ Ft,
+                          double* __restrict__ q) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  const int x = dir == 0 ? i : j;
+  const int NT = dir == 0 ? c.N1T : c.N2T;
+  if (x < 3 || x > NT - 3) return;
+  const long long Z = c.Z, s = stride_of(c, dir);
+  double fb[8];
+  bool any = false;
+  for (int v = 0; v < 8; v++) {
+    fb[v] = Ft[((long long)dir * c.dof + v) * Z + z];
+    any |= fb[v] != 0.;
+  }
+  if (!any) return;
+  // face states and their 5-point derivatives
+  typedef Dual<double, 5> D5;
+  double pl[8], pr[8], dro[8][5], dlo[8][5];
+  for (int v = 0; v < 8; v++) {
+    const double* a = P + (long long)v * Z;
+    D5 ya[5], yb[5];
+    for (int m = 0; m < 5; m++) {
+      ya[m] = D5::var(a[z - s + (m - 2) * s], m);
+      yb[m] = D5::var(a[z + (m - 2) * s], m);
+    }
+    D5 lo, ro, lo2, ro2;
+    recon_faces<D5>(c.reconstruction, c.theta, ya[0], ya[1], ya[2], ya[3], ya[4], lo, ro);
+    recon_faces<D5>(c.reconstruction, c.theta, yb[0], yb[1], yb[2], yb[3], yb[4], lo2, ro2);
+    pl[v] = ro.v;
+    pr[v] = lo2.v;
+    for (int m = 0; m < 5; m++) { dro[v][m] = ro.d[m]; dlo[v][m] = lo2.d[m]; }
+  }
+  // dF/dpl and dF/dpr, 8 tangent lanes each
+  typedef Dual<double, 8> D8;
+  double gl[8], gr[8];
+  for (int side = 0; side < 2; side++) {
+    D8 L[8], R[8], F[8];
+    for (int v = 0; v < 8; v++) {
+      L[v] = side == 0 ? D8::var(pl[v], v) : D8(pl[v]);
+      R[v] = side == 1 ? D8::var(pr[v], v) : D8(pr[v]);
+    }
+    riemann_flux<D8>(c, dir, L, R, F);
+    double* out = side == 0 ? gl : gr;
+    for (int k2 = 0; k2 < 8; k2++) {
+      double acc = 0.;
+      for (int r = 0; r < 8; r++) acc += fb[r] * F[r].d[k2];
+      out[k2] = acc;
+    }
+  }
+  // row index of prim variable v: fluid 0..4, B at c.B1 (= 5 for ideal)
+  for (int v = 0; v < 8; v++) {
+    double* col = q + (long long)v * Z;
+    for (int m = 0; m < 5; m++) {
+      atomicAdd(col + z - s + (m - 2) * s, gl[v] * dro[v][m]);
+      atomicAdd(col + z + (m - 2) * s, gr[v] * dlo[v][m]);
+    }
+  }
+}
+
+// ghosts are periodic images of interior zones: every interior zone
+// gathers the adjoints of itself and of its images
+__global__ void k_fold(DevCfg c, const double* __restrict__ q, double* __restrict__ out) {
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= c.Zint) return;
+  const long long Z = c.Z;
+  const long long z = interior_to_z(c, n);
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  for (int v = 0; v < c.dof; v++) {
+    double s = 0.;
+    for (int a = -1; a <= 1; a++) {
+      const int ii = i + a * c.N1;
+      if (ii < 0 || ii >= c.N1T) continue;
+      for (int b = -1; b <= 1; b++) {
+        const int jj = j + b * c.N2;
+        if (jj < 0 || jj >= c.N2T) continue;
+        s += q[(long long)v * Z + zidx(c, ii, jj, k)];
+      }
+    }
+    out[(long long)v * Z + z] = s;
+  }
+}
+
+}  // namespace adj
+
+static __global__ void k_zero_ghosts(DevCfg c, double* __restrict__ a) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  if (adj::is_interior(c, i, j)) return;
+  for (int v = 0; v < c.dof; v++) a[(long long)v * c.Z + z] = 0.;
+}
+
+// ---- host side: one step's adjoint (all buffers dof x Z unless noted)
+void adjoint_zero_ghosts(const DevCfg& c, double* a, cudaStream_t s) {
+  k_zero_ghosts<<<adj::nblk(c.Z, 256), 256, 0, s>>>(c, a);
+}
+
+void adjoint_stencil_t(const DevCfg& c, const double* P, const double* g, double* Ft, double* ebar, double* q,
+                       double* out, cudaStream_t s) {
+  using namespace adj;
+  const size_t bZ = (size_t)c.Z * sizeof(double);
+  k_div_t<<<nblk(c.Z, 128), 128, 0, s>>>(c, g, Ft);
+  k_ct_t_emf<<<nblk(c.Z, 256), 256, 0, s>>>(c, Ft, ebar);
+  k_ct_t_raw<<<nblk(c.Z, 256), 256, 0, s>>>(c, ebar, Ft);
+  cudaMemsetAsync(q, 0, (size_t)c.dof * bZ, s);
+  for (int d = 0; d < 2; d++) k_faces_t<<<nblk(c.Z, 64), 64, 0, s>>>(c, d, P, Ft, q);
+  k_fold<<<nblk(c.Zint, 128), 128, 0, s>>>(c, q, out);
+}
+
+void adjoint_step(const DevCfg& c, double dt, const double* P0, const double* Ph, const double* P1, double* lam,
+                  const AdjointBufs& w, cudaStream_t s) {
+  using namespace adj;
+  // full stage at P1
+  k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, P1, dt, lam, w.g, w.ubar, w.bacc, 0);
+  adjoint_stencil_t(c, Ph, w.g, w.Ft, w.ebar, w.q, w.lamh, s);
+  // half stage at Ph
+  k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, Ph, 0.5 * dt, w.lamh, w.g, w.ubar, w.bacc, 1);
+  adjoint_stencil_t(c, P0, w.g, w.Ft, w.ebar, w.q, lam, s);
+  k_cons<<<nblk(c.Zint, 128), 128, 0, s>>>(c, P0, w.ubar, w.bacc, lam);
+}
+
+}  // namespace grim

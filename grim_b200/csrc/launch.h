@@ -45,6 +45,23 @@ GRIM_DECLARE_LAUNCHERS(exact)
 GRIM_DECLARE_LAUNCHERS(fast)
 
 namespace grim {
+// adjoint.cu: work buffers of the reverse sweep (dof x Z unless noted)
+struct AdjointBufs {
+  double* g;     // dL/d divF of the stage
+  double* Ft;    // 2 x dof x Z: face-flux adjoints per direction
+  double* ebar;  // Z: corner EMF adjoints
+  double* q;     // stencil adjoint before the periodic fold
+  double* lamh;  // dL/dPh
+  double* ubar;  // nf x Z: dL/dU(P0)
+  double* bacc;  // 3 x Z: dL/dB0 through the induction
+};
+// lam (dL/dP1, interior) -> dL/dP0 for one step of fixed dt
+void adjoint_step(const DevCfg& c, double dt, const double* P0, const double* Ph, const double* P1, double* lam,
+                  const AdjointBufs& w, cudaStream_t s);
+void adjoint_zero_ghosts(const DevCfg& c, double* a, cudaStream_t s);
+}  // namespace grim
+
+namespace grim {
 namespace fast {
 // algorithmic flop counts of one zone's residual / tangent / solve
 void count_ops(const DevCfg& c, int stage, const StageBufs& b, long long z, double* out, cudaStream_t s);

@@ -199,7 +199,7 @@ GRIM_D void elem_set(ElemT<S, R>& e, const S& rho_in, const S& u_in, const S& v1
     else
       e.deltaP = dPT;
   }
-  if (COND || VISC) closure(e, G, c);
+  if constexpr (COND || VISC) closure(e, G, c);
 }
 
 // T^mu_nu (physics.cpp:153-178)

@@ -13,6 +13,7 @@
 //               -> time += dt -> [dt speeds of primOld for the next step]
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -77,6 +78,15 @@ struct grim_handle {
   // recorded around each launch on the handle's stream
   // face-kernel launch variants per direction, [exact unit, fast unit]
   int faceVariant[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  // dt held at its current value instead of computeDt (the adjoint's runs)
+  bool fixedDt = false;
+  // adjoint: checkpoints of primOld every adjEvery steps of the last
+  // grim_adjoint_forward, segment states and the reverse sweep's buffers
+  int adjSteps = 0, adjEvery = 0;
+  double adjT0 = 0., adjDt = 0.;
+  std::vector<double*> adjCkpt;
+  std::vector<double*> adjSeg;  // 2 * every + 1 states: S[0..every], H[0..every-1]
+  double* adjWork = nullptr;    // AdjointBufs storage
   bool profOn = false;
   std::vector<cudaEvent_t> profEv;
   std::vector<int> profGroup;
@@ -118,6 +128,11 @@ static void free_all(grim_handle* h) {
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
   for (int l = 0; l < 2; l++)
     if (h->list[l]) { cudaFree(h->list[l]); h->list[l] = nullptr; }
+  for (double* p : h->adjCkpt) cudaFree(p);
+  for (double* p : h->adjSeg) cudaFree(p);
+  h->adjCkpt.clear();
+  h->adjSeg.clear();
+  if (h->adjWork) { cudaFree(h->adjWork); h->adjWork = nullptr; }
   for (cudaEvent_t e : h->profEv) cudaEventDestroy(e);
   h->profEv.clear();
   h->profGroup.clear();
@@ -297,7 +312,7 @@ static void enqueue_step(grim_handle* h, bool timed) {
   const size_t bytes = (size_t)c.dof * c.Z * sizeof(double);
   if (timed) cudaEventRecord(h->ev[0], s);
   // computeDt (timestep.cpp:8): dt from the last elemOld state
-  {
+  if (!h->fixedDt) {
     PROF(GRIM_PROF_DT);
     KNS_CALL(h, dt_update, h->st, h->cfg.CourantFactor, h->cfg.maxDtIncrement, s);
     g_launch_counter++;
@@ -994,6 +1009,124 @@ int grim_set_face_variant(grim_handle* h, int dir, int variant) {
   }
   h->faceVariant[use_exact(h) ? 0 : 1][dir] = variant;
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  return GRIM_OK;
+}
+
+int grim_set_dt_mode(grim_handle* h, int fixed) {
+  if (!h) return GRIM_EINVAL;
+  h->fixedDt = fixed != 0;
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  return GRIM_OK;
+}
+
+static int adjoint_scope(grim_handle* h) {
+  const grim_config& c = h->cfg;
+  const bool periodic = c.boundaryLeft == GRIM_PERIODIC && c.boundaryRight == GRIM_PERIODIC &&
+                        c.boundaryBottom == GRIM_PERIODIC && c.boundaryTop == GRIM_PERIODIC;
+  if (c.dim != 2 || c.metric != GRIM_MINKOWSKI || c.conduction || c.viscosity || !periodic ||
+      c.problem != GRIM_PROBLEM_NONE) {
+    set_err("adjoint: supported for 2D ideal MHD in Minkowski with periodic boundaries only");
+    return GRIM_ENOTSUP;
+  }
+  return GRIM_OK;
+}
+
+int grim_adjoint_forward(grim_handle* h, int nsteps, int every) {
+  if (!h || nsteps <= 0 || every <= 0) { set_err("grim_adjoint_forward: bad argument"); return GRIM_EINVAL; }
+  int rc = adjoint_scope(h);
+  if (rc) return rc;
+  CK(cudaSetDevice(h->device));
+  const size_t bytes = (size_t)h->dc.dof * h->bytesZ;
+  const int nck = (nsteps + every - 1) / every;
+  while ((int)h->adjCkpt.size() < nck) {
+    double* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) { set_err("adjoint: checkpoint allocation failed"); return GRIM_ENOMEM; }
+    h->adjCkpt.push_back(p);
+  }
+  grim_set_dt_mode(h, 1);
+  double t0 = 0., dt = 0.;
+  rc = grim_get_time(h, &t0, &dt);
+  if (rc) return rc;
+  for (int n = 0; n < nsteps; n++) {
+    if (n % every == 0)
+      CK(cudaMemcpyAsync(h->adjCkpt[n / every], h->primOld, bytes, cudaMemcpyDeviceToDevice, h->stream));
+    rc = run_steps(h, 1);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  h->adjSteps = nsteps;
+  h->adjEvery = every;
+  h->adjT0 = t0;
+  h->adjDt = dt;
+  return GRIM_OK;
+}
+
+int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, int memKind) {
+  if (!h || !lambda || !grad) { set_err("grim_adjoint_backward: null argument"); return GRIM_EINVAL; }
+  if (h->adjSteps <= 0) { set_err("grim_adjoint_backward: no grim_adjoint_forward run to reverse"); return GRIM_EINVAL; }
+  CK(cudaSetDevice(h->device));
+  const DevCfg& c = h->dc;
+  const size_t bytes = (size_t)c.dof * h->bytesZ;
+  const int every = h->adjEvery;
+  // segment states and work buffers
+  while ((int)h->adjSeg.size() < 2 * every + 2) {
+    double* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) { set_err("adjoint: segment allocation failed"); return GRIM_ENOMEM; }
+    h->adjSeg.push_back(p);
+  }
+  if (!h->adjWork) {
+    // g, Ft (2 dof), ebar (1), q, lamh, ubar (nf), bacc (3), lam
+    const size_t words = (size_t)c.Z * (c.dof * 6 + 1 + c.nf + 3);
+    if (cudaMalloc(&h->adjWork, words * sizeof(double)) != cudaSuccess) {
+      set_err("adjoint: work allocation failed");
+      return GRIM_ENOMEM;
+    }
+  }
+  double* wp = h->adjWork;
+  AdjointBufs w;
+  w.g = wp; wp += (size_t)c.dof * c.Z;
+  w.Ft = wp; wp += (size_t)2 * c.dof * c.Z;
+  w.ebar = wp; wp += (size_t)c.Z;
+  w.q = wp; wp += (size_t)c.dof * c.Z;
+  w.lamh = wp; wp += (size_t)c.dof * c.Z;
+  w.ubar = wp; wp += (size_t)c.nf * c.Z;
+  w.bacc = wp; wp += (size_t)3 * c.Z;
+  double* lam = wp;
+  double* finalState = h->adjSeg[2 * every + 1];
+  CK(cudaMemcpyAsync(lam, lambda, bytes, memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                     h->stream));
+  grim::adjoint_zero_ghosts(c, lam, h->stream);
+  CK(cudaMemcpyAsync(finalState, h->primOld, bytes, cudaMemcpyDeviceToDevice, h->stream));
+  double tFinal = 0., dtNow = 0.;
+  int rc = grim_get_time(h, &tFinal, &dtNow);
+  if (rc) return rc;
+  const double dt = h->adjDt;
+  const int nseg = (h->adjSteps + every - 1) / every;
+  for (int seg = nseg - 1; seg >= 0; seg--) {
+    const int m = std::min(every, h->adjSteps - seg * every);
+    CK(cudaMemcpyAsync(h->primOld, h->adjCkpt[seg], bytes, cudaMemcpyDeviceToDevice, h->stream));
+    rc = grim_set_time(h, h->adjT0 + (double)seg * every * dt, dt);
+    if (rc) return rc;
+    // recompute the segment, keeping the states each step's adjoint needs
+    for (int t = 0; t < m; t++) {
+      CK(cudaMemcpyAsync(h->adjSeg[t], h->primOld, bytes, cudaMemcpyDeviceToDevice, h->stream));
+      rc = run_steps(h, 1);
+      if (rc) return rc;
+      CK(cudaMemcpyAsync(h->adjSeg[every + 1 + t], h->primHalf, bytes, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    CK(cudaMemcpyAsync(h->adjSeg[m], h->primOld, bytes, cudaMemcpyDeviceToDevice, h->stream));
+    for (int t = m - 1; t >= 0; t--)
+      grim::adjoint_step(c, dt, h->adjSeg[t], h->adjSeg[every + 1 + t], h->adjSeg[t + 1], lam, w, h->stream);
+    CK(cudaGetLastError());
+  }
+  grim::adjoint_zero_ghosts(c, lam, h->stream);
+  // leave the stepper where the forward run left it
+  CK(cudaMemcpyAsync(h->primOld, finalState, bytes, cudaMemcpyDeviceToDevice, h->stream));
+  rc = grim_set_time(h, tFinal, dtNow);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(grad, lam, bytes, memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
   return GRIM_OK;
 }
 

@@ -52,6 +52,11 @@ class Grid:
             raise ValueError("setVars: shape %s, expected %s" % (a.shape, self.shape))
         _lib.check(_lib.lib().grim_set_prims(self._ts._h, self._which, _ptr(a), _lib.HOST), "setVars")
 
+    def communicate(self):
+        """grid::communicate + boundaries: periodic wrap, then the physical
+        boundary fill."""
+        _lib.check(_lib.lib().grim_apply_boundaries(self._ts._h, self._which), "communicate")
+
     def setVarsDevice(self, dev_ptr):
         _lib.check(_lib.lib().grim_set_prims(self._ts._h, self._which, ctypes.c_void_p(int(dev_ptr)),
                                              _lib.DEVICE), "setVarsDevice")
@@ -192,6 +197,24 @@ class timeStepper:
 
     def setFaceVariant(self, dir, variant):
         _lib.check(_lib.lib().grim_set_face_variant(self._h, int(dir), int(variant)), "set_face_variant")
+
+    def setFixedDt(self, fixed=True):
+        """Hold dt at its current value instead of computeDt."""
+        _lib.check(_lib.lib().grim_set_dt_mode(self._h, int(bool(fixed))), "set_dt_mode")
+
+    def adjointForward(self, nsteps, every=10):
+        """Advance nsteps with dt fixed, checkpointing primOld every `every`
+        steps, for a following adjointBackward."""
+        _lib.check(_lib.lib().grim_adjoint_forward(self._h, int(nsteps), int(every)), "adjoint_forward")
+
+    def adjointBackward(self, lam):
+        """dL/d(initial primOld) from lam = dL/d(final primOld), both
+        [var][k][j][i] with ghosts (interior entries used / returned)."""
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        grad = self._zeros(self.dof)
+        _lib.check(_lib.lib().grim_adjoint_backward(self._h, _ptr(lam), _ptr(grad), _lib.HOST),
+                   "adjoint_backward")
+        return grad
 
     def countFlops(self):
         """Algorithmic flops of one zone: residual (FP64), tangent pass

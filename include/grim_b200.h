@@ -255,6 +255,29 @@ int grim_autotune(grim_handle* h, int* variants, double* msBest);
 /* Forces one variant (for tests); GRIM_EINVAL when out of range. */
 int grim_set_face_variant(grim_handle* h, int dir, int variant);
 
+/* ---- adjoint (reverse) sweep of whole timesteps.  No counterpart in the
+ *      reference, which has no derivatives; it reverses the reference's
+ *      timeStep (timestep.cpp:3-334) with the Newton solves differentiated
+ *      implicitly (converged solves; their iterations are not taped).
+ *
+ * grim_set_dt_mode(h, 1) holds dt at its current value (grim_set_time)
+ * instead of timeStepper::computeDt; 0 restores computeDt.
+ *
+ * grim_adjoint_forward advances nsteps from primOld with dt held fixed,
+ * keeping primOld every `every` steps on the device (checkpoints).  primOld
+ * must carry periodic ghost images of its interior (grim_apply_boundaries).
+ * grim_adjoint_backward takes lambda = dL/d(final primOld) (dof x Z; only
+ * interior zones are read) and returns grad = dL/d(initial primOld) for the
+ * interior zones (ghost entries zero; the ghosts are images of interior
+ * zones and their share is folded in).  Each segment between checkpoints
+ * is recomputed forward once; the stepper is left at the final state.
+ * Supported: 2D ideal MHD, Minkowski, periodic boundaries (GRIM_ENOTSUP
+ * otherwise).  Zones accumulate with double atomics, so results agree run
+ * to run to roundoff. */
+int grim_set_dt_mode(grim_handle* h, int fixed);
+int grim_adjoint_forward(grim_handle* h, int nsteps, int every);
+int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, int memKind);
+
 /* ---- allocation-free divergence.  No counterpart in the reference: for
  *      callers that cannot call cudaMalloc (their device memory is owned by
  *      their own pool allocator, or they call in the middle of asynchronous
