@@ -95,6 +95,7 @@ def lib():
         "grim_set_dt_mode": [vp, i],
         "grim_adjoint_forward": [vp, i, i],
         "grim_adjoint_backward": [vp, vp, vp, i],
+        "grim_adjoint_stencil": [vp, vp, vp, vp, i],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -59,6 +59,8 @@ struct AdjointBufs {
 void adjoint_step(const DevCfg& c, double dt, const double* P0, const double* Ph, const double* P1, double* lam,
                   const AdjointBufs& w, cudaStream_t s);
 void adjoint_zero_ghosts(const DevCfg& c, double* a, cudaStream_t s);
+void adjoint_stencil_t(const DevCfg& c, const double* P, const double* g, double* Ft, double* ebar, double* q,
+                       double* out, cudaStream_t s);
 }  // namespace grim
 
 namespace grim {

@@ -1031,6 +1031,52 @@ static int adjoint_scope(grim_handle* h) {
   return GRIM_OK;
 }
 
+// work buffers of the reverse sweep: g, Ft (2 dof), ebar (1), q, lamh,
+// ubar (nf), bacc (3), lam
+static int adjoint_work(grim_handle* h, AdjointBufs& w, double*& lam) {
+  const DevCfg& c = h->dc;
+  if (!h->adjWork) {
+    const size_t words = (size_t)c.Z * (c.dof * 6 + 1 + c.nf + 3);
+    if (cudaMalloc(&h->adjWork, words * sizeof(double)) != cudaSuccess) {
+      set_err("adjoint: work allocation failed");
+      return GRIM_ENOMEM;
+    }
+  }
+  double* wp = h->adjWork;
+  w.g = wp; wp += (size_t)c.dof * c.Z;
+  w.Ft = wp; wp += (size_t)2 * c.dof * c.Z;
+  w.ebar = wp; wp += (size_t)c.Z;
+  w.q = wp; wp += (size_t)c.dof * c.Z;
+  w.lamh = wp; wp += (size_t)c.dof * c.Z;
+  w.ubar = wp; wp += (size_t)c.nf * c.Z;
+  w.bacc = wp; wp += (size_t)3 * c.Z;
+  lam = wp;
+  return GRIM_OK;
+}
+
+int grim_adjoint_stencil(grim_handle* h, const double* prim, const double* gbar, double* out, int memKind) {
+  if (!h || !prim || !gbar || !out) { set_err("grim_adjoint_stencil: null argument"); return GRIM_EINVAL; }
+  int rc = adjoint_scope(h);
+  if (rc) return rc;
+  CK(cudaSetDevice(h->device));
+  const DevCfg& c = h->dc;
+  const size_t bytes = (size_t)c.dof * h->bytesZ;
+  AdjointBufs w;
+  double* lam = nullptr;
+  rc = adjoint_work(h, w, lam);
+  if (rc) return rc;
+  const cudaMemcpyKind in = memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  CK(cudaMemcpyAsync(h->scratch, prim, bytes, in, h->stream));
+  CK(cudaMemcpyAsync(w.g, gbar, bytes, in, h->stream));
+  CK(cudaMemsetAsync(lam, 0, bytes, h->stream));
+  grim::adjoint_stencil_t(c, h->scratch, w.g, w.Ft, w.ebar, w.q, lam, h->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, lam, bytes, memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return GRIM_OK;
+}
+
 int grim_adjoint_forward(grim_handle* h, int nsteps, int every) {
   if (!h || nsteps <= 0 || every <= 0) { set_err("grim_adjoint_forward: bad argument"); return GRIM_EINVAL; }
   int rc = adjoint_scope(h);
@@ -1074,24 +1120,10 @@ int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, in
     if (cudaMalloc(&p, bytes) != cudaSuccess) { set_err("adjoint: segment allocation failed"); return GRIM_ENOMEM; }
     h->adjSeg.push_back(p);
   }
-  if (!h->adjWork) {
-    // g, Ft (2 dof), ebar (1), q, lamh, ubar (nf), bacc (3), lam
-    const size_t words = (size_t)c.Z * (c.dof * 6 + 1 + c.nf + 3);
-    if (cudaMalloc(&h->adjWork, words * sizeof(double)) != cudaSuccess) {
-      set_err("adjoint: work allocation failed");
-      return GRIM_ENOMEM;
-    }
-  }
-  double* wp = h->adjWork;
   AdjointBufs w;
-  w.g = wp; wp += (size_t)c.dof * c.Z;
-  w.Ft = wp; wp += (size_t)2 * c.dof * c.Z;
-  w.ebar = wp; wp += (size_t)c.Z;
-  w.q = wp; wp += (size_t)c.dof * c.Z;
-  w.lamh = wp; wp += (size_t)c.dof * c.Z;
-  w.ubar = wp; wp += (size_t)c.nf * c.Z;
-  w.bacc = wp; wp += (size_t)3 * c.Z;
-  double* lam = wp;
+  double* lam = nullptr;
+  int rcw = adjoint_work(h, w, lam);
+  if (rcw) return rcw;
   double* finalState = h->adjSeg[2 * every + 1];
   CK(cudaMemcpyAsync(lam, lambda, bytes, memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                      h->stream));

@@ -216,6 +216,15 @@ class timeStepper:
                    "adjoint_backward")
         return grad
 
+    def adjointStencil(self, prim, gbar):
+        """(d divF / d prim)^T gbar on the interior (test entry point)."""
+        p = np.ascontiguousarray(prim, dtype=np.float64)
+        g = np.ascontiguousarray(gbar, dtype=np.float64)
+        out = self._zeros(self.dof)
+        _lib.check(_lib.lib().grim_adjoint_stencil(self._h, _ptr(p), _ptr(g), _ptr(out), _lib.HOST),
+                   "adjoint_stencil")
+        return out
+
     def countFlops(self):
         """Algorithmic flops of one zone: residual (FP64), tangent pass
         (FP32 and FP64), pivoted solve (FP32 and FP64)."""

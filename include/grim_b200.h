@@ -277,6 +277,10 @@ int grim_set_face_variant(grim_handle* h, int dir, int variant);
 int grim_set_dt_mode(grim_handle* h, int fixed);
 int grim_adjoint_forward(grim_handle* h, int nsteps, int every);
 int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, int memKind);
+/* the transpose of the stencil alone, for tests: out = (d divF / d prim)^T
+ * gbar for the interior zones of prim (ghosts taken as periodic images;
+ * gbar read on the interior) */
+int grim_adjoint_stencil(grim_handle* h, const double* prim, const double* gbar, double* out, int memKind);
 
 /* ---- allocation-free divergence.  No counterpart in the reference: for
  *      callers that cannot call cudaMalloc (their device memory is owned by

@@ -69,6 +69,14 @@ def _adjoint(cfg, P, nsteps, every):
 
 @pytest.mark.parametrize("recon,riemann", [(C.MINMOD, C.LOCAL_LAX_FRIEDRICH), (C.PPM, C.HLL)])
 def test_adjoint_matches_central_fd(recon, riemann):
+    """The forward map is piecewise smooth: the limiters (minmod's slope
+    choice, PPM's monotonicity corrections) and the Riemann solvers' max /
+    min of the two face states' speeds switch branch where two candidates
+    tie, and the adjoint is the derivative of the branch taken.  A central
+    difference whose bracket contains such a switch measures an average of
+    two branches, so the 1e-6 check applies where the map is smooth over the
+    bracket: the differences at h = 1e-6 and h = 1e-7 agree (to the 1e-7
+    difference's roundoff).  At least 6 of 16 random picks must qualify."""
     N, nsteps = 24, 6
     cfg = PR.fast_mode_config(N=N, reconstruction=recon, riemannSolver=riemann, maxNonLinearIter=6,
                               nonlinearsolve_atol=0.0)
@@ -79,15 +87,25 @@ def test_adjoint_matches_central_fd(recon, riemann):
     assert np.all(grad[:, 0, :g, :] == 0) and np.all(grad[:, 0, :, :g] == 0)
     scale = np.max(np.abs(gi))
     rng = np.random.default_rng(5)
-    for v in range(8):
-        j, i = rng.integers(0, N, 2)
-        h = 1e-6
+
+    def fd(v, j, i, h):
         Pp, Pm = P.copy(), P.copy()
         Pp[v, 0, j + g, i + g] += h
         Pm[v, 0, j + g, i + g] -= h
-        fd = (_loss(cfg, Pp, nsteps) - _loss(cfg, Pm, nsteps)) / (2 * h)
+        return (_loss(cfg, Pp, nsteps) - _loss(cfg, Pm, nsteps)) / (2 * h)
+
+    smooth = 0
+    for n in range(16):
+        v = n % 8
+        j, i = rng.integers(0, N, 2)
         ad = gi[v, 0, j, i]
-        assert abs(fd - ad) <= 1e-6 * max(abs(ad), 1e-3 * scale), (v, j, i, fd, ad)
+        tol = max(abs(ad), 1e-3 * scale)
+        f6, f7 = fd(v, j, i, 1e-6), fd(v, j, i, 1e-7)
+        if abs(f6 - f7) > 3e-6 * tol:
+            continue  # a branch switch inside the bracket
+        smooth += 1
+        assert abs(f6 - ad) <= 1e-6 * tol, (v, j, i, f6, f7, ad)
+    assert smooth >= 6, smooth
 
 
 def test_adjoint_checkpoint_interval_does_not_change_the_gradient():
@@ -104,3 +122,38 @@ def test_adjoint_refuses_unsupported_configurations():
     ts = timeStepper(T.torus_config(N1=32, N2=16, N3=8))
     with pytest.raises(Exception):
         ts.adjointForward(2, 1)
+
+
+def _with_images(ts, P):
+    ts.primOld.setVars(P)
+    ts.primOld.communicate()
+    return ts.primOld.getVars()
+
+
+@pytest.mark.parametrize("recon,riemann", [(C.MINMOD, C.LOCAL_LAX_FRIEDRICH), (C.PPM, C.HLL)])
+def test_stencil_transpose_matches_fd(recon, riemann):
+    """The transpose of the flux divergence (reconstruction, Riemann, flux-CT,
+    divergence; ghosts as periodic images) against central differences of
+    <gbar, divF(P)> from grim_compute_div_fluxes."""
+    cfg = PR.fast_mode_config(N=16, reconstruction=recon, riemannSolver=riemann)
+    from grim_b200.timestepper import timeStepper
+    ts = timeStepper(cfg)
+    P = _with_images(ts, _state(cfg, 2))
+    g = cfg["numGhost"]
+    rng = np.random.default_rng(1)
+    gbar = np.zeros_like(P)
+    gbar[:, :, g:g + 16, g:g + 16] = rng.standard_normal((8, 1, 16, 16))
+    vjp = ts.adjointStencil(P, gbar)
+
+    def f(Q):
+        return float(np.sum(gbar * ts.computeDivOfFluxes(Q)[0]))
+
+    h = 1e-6
+    for v in range(8):
+        j, i = rng.integers(0, 16, 2)
+        Pp, Pm = P.copy(), P.copy()
+        Pp[v, 0, j + g, i + g] += h
+        Pm[v, 0, j + g, i + g] -= h
+        fd = (f(_with_images(ts, Pp)) - f(_with_images(ts, Pm))) / (2 * h)
+        ad = vjp[v, 0, j + g, i + g]
+        assert abs(fd - ad) <= 1e-6 * max(abs(ad), 1e-3 * np.max(np.abs(vjp))), (v, j, i, fd, ad)
