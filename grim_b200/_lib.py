@@ -96,6 +96,14 @@ def lib():
         "grim_adjoint_forward": [vp, i, i],
         "grim_adjoint_backward": [vp, vp, vp, i],
         "grim_adjoint_stencil": [vp, vp, vp, vp, i],
+        "grim_batch_create": [vp, i, i, P(vp)],
+        "grim_batch_destroy": [vp],
+        "grim_batch_problem": [vp, i, P(vp)],
+        "grim_batch_set_newton_mode": [vp, i, d],
+        "grim_batch_enable_graph": [vp, i],
+        "grim_batch_time_steps": [vp, i],
+        "grim_batch_synchronize": [vp],
+        "grim_batch_size": [vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

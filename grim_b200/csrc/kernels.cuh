@@ -983,33 +983,102 @@ GRIM_D void list_append(int* list, unsigned long long* count, int zone, bool tak
   if (take) list[base + __popc(m & ((1u << lane) - 1))] = zone;
 }
 
+// Launch 0, one zone: floors, residual, stored state; true when the zone
+// is above tolerance (goes on the worklist).
+template <int COND, int VISC>
+GRIM_D bool list_init_zone(const DevCfg& c, int stage, const StageBufs& b, long long z) {
+  constexpr int NF = 5 + COND + VISC;
+  const long long Z = c.Z;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  ZoneGeo<double> G;
+  load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
+  StageConst<NF> K;
+  load_stage_const<COND, VISC>(K, c, stage, b, z, G);
+  double P[NF], R[NF];
+  for (int v = 0; v < NF; v++) P[v] = b.prim[(long long)v * Z + z];
+  P[0] = fmax(P[0], c.rhoFloor);
+  P[1] = fmax(P[1], c.uFloor);
+  b.prim[z] = P[0];
+  b.prim[Z + z] = P[1];
+  zone_residual<COND, VISC, double, double>(P, K, G, c, R);
+  const double l2 = l2sum<NF>(R);
+  for (int v = 0; v < NF; v++) b.R[(long long)v * Z + z] = R[v];
+  b.l2[Z + z] = l2;
+  return l2 > fmax(c.atol, c.rtol * c.rtol * l2);
+}
+
+// Launch it >= 1, one zone on the worklist: one Newton update from the
+// stored state; true when the zone stays above tolerance (and it is not
+// the last iteration).
+template <int COND, int VISC, class T>
+GRIM_D bool list_iter_zone(const DevCfg& c, int stage, int it, const StageBufs& b, long long z) {
+  constexpr int NF = 5 + COND + VISC;
+  const long long Z = c.Z;
+  const bool last = (it == c.maxIter);
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  ZoneGeo<double> G;
+  load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
+  ZoneGeo<T> Gt;
+  for (int m = 0; m < 4; m++)
+    for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = (T)G.gcov[m][q]; Gt.gcon[m][q] = (T)G.gcon[m][q]; }
+  Gt.g = (T)G.g; Gt.alpha = (T)G.alpha; Gt.x1 = (T)G.x1; Gt.x2 = (T)G.x2; Gt.dyn = (T)G.dyn;
+  StageConst<NF> K;
+  load_stage_const<COND, VISC>(K, c, stage, b, z, G);
+  double P[NF], R[NF];
+  for (int v = 0; v < NF; v++) {
+    P[v] = b.prim[(long long)v * Z + z];
+    R[v] = b.R[(long long)v * Z + z];
+  }
+  const double l2 = l2sum<NF>(R);
+  const double l2first = b.l2[Z + z];
+  T J[NF][NF];
+  tangent_jacobian<COND, VISC, T>(P, K, Gt, c, J);
+  T bv[NF], xv[NF];
+  for (int v = 0; v < NF; v++) bv[v] = (T)(-R[v]);
+  gauss_solve<T, NF>(J, bv, xv);
+  double dPv[NF];
+  for (int v = 0; v < NF; v++) dPv[v] = (double)xv[v];
+  const double f0 = 0.5 * l2, fPrime0 = -2. * f0;
+  double lam = 1.;
+  bool haveR = false;
+  double Rt[NF];
+  for (int ls = 0; ls < c.maxLS; ls++) {
+    double Pt[NF];
+    for (int v = 0; v < NF; v++) Pt[v] = P[v] + lam * dPv[v];
+    zone_residual<COND, VISC, double, double>(Pt, K, G, c, Rt);
+    const double f1 = 0.5 * l2sum<NF>(Rt);
+    if (!(f1 > (f0 * (1. - 1e-4 * lam) + c.lsFloor))) { haveR = true; break; }
+    const double denom = (f1 - f0 - fPrime0 * lam);
+    lam = -fPrime0 * lam * lam / denom / 2.;
+  }
+  for (int v = 0; v < NF; v++) P[v] = P[v] + lam * dPv[v];
+  const bool floored = (P[0] < c.rhoFloor) || (P[1] < c.uFloor);
+  if (!last) {
+    P[0] = fmax(P[0], c.rhoFloor);
+    P[1] = fmax(P[1], c.uFloor);
+  }
+  if (!haveR || floored) zone_residual<COND, VISC, double, double>(P, K, G, c, Rt);
+  const double l2n = l2sum<NF>(Rt);
+  const bool conv = l2n <= fmax(c.atol, c.rtol * c.rtol * l2first);
+  if (!conv && last) atomicAdd(&b.st->finalUnconv[stage], 1ULL);
+  for (int v = 0; v < NF; v++) {
+    b.prim[(long long)v * Z + z] = P[v];
+    b.R[(long long)v * Z + z] = Rt[v];
+  }
+  return !conv && !last;
+}
+
 template <int COND, int VISC>
 __global__ void __launch_bounds__(128) k_newton_list_init(DevCfg c, int stage, StageBufs b) {
-  constexpr int NF = 5 + COND + VISC;
   for (long long n0 = (long long)blockIdx.x * blockDim.x; n0 < c.Zint; n0 += (long long)gridDim.x * blockDim.x) {
     const long long n = n0 + threadIdx.x;
     bool take = false;
     long long z = 0;
     if (n < c.Zint) {
-      const long long Z = c.Z;
       z = interior_to_z(c, n);
-      int i, j, k;
-      zijk(c, z, i, j, k);
-      ZoneGeo<double> G;
-      load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
-      StageConst<NF> K;
-      load_stage_const<COND, VISC>(K, c, stage, b, z, G);
-      double P[NF], R[NF];
-      for (int v = 0; v < NF; v++) P[v] = b.prim[(long long)v * Z + z];
-      P[0] = fmax(P[0], c.rhoFloor);
-      P[1] = fmax(P[1], c.uFloor);
-      b.prim[z] = P[0];
-      b.prim[Z + z] = P[1];
-      zone_residual<COND, VISC, double, double>(P, K, G, c, R);
-      const double l2 = l2sum<NF>(R);
-      for (int v = 0; v < NF; v++) b.R[(long long)v * Z + z] = R[v];
-      b.l2[Z + z] = l2;
-      take = l2 > fmax(c.atol, c.rtol * c.rtol * l2);
+      take = list_init_zone<COND, VISC>(c, stage, b, z);
     }
     hist_add(b.st->itHist[stage], 0, n < c.Zint && !take);
     list_append(b.list[0], &b.st->listCount[0], (int)z, take);
@@ -1018,7 +1087,6 @@ __global__ void __launch_bounds__(128) k_newton_list_init(DevCfg c, int stage, S
 
 template <int COND, int VISC, class T>
 __global__ void __launch_bounds__(128) k_newton_list_iter(DevCfg c, int stage, int it, StageBufs b) {
-  constexpr int NF = 5 + COND + VISC;
   const int in = (it - 1) & 1, out = it & 1;
   const long long count = (long long)b.st->listCount[in];
   const bool last = (it == c.maxIter);
@@ -1027,66 +1095,88 @@ __global__ void __launch_bounds__(128) k_newton_list_iter(DevCfg c, int stage, i
     bool take = false;
     int zone = 0;
     if (n < count) {
-      const long long Z = c.Z;
       zone = b.list[in][n];
-      const long long z = zone;
-      int i, j, k;
-      zijk(c, z, i, j, k);
-      ZoneGeo<double> G;
-      load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
-      ZoneGeo<T> Gt;
-      for (int m = 0; m < 4; m++)
-        for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = (T)G.gcov[m][q]; Gt.gcon[m][q] = (T)G.gcon[m][q]; }
-      Gt.g = (T)G.g; Gt.alpha = (T)G.alpha; Gt.x1 = (T)G.x1; Gt.x2 = (T)G.x2; Gt.dyn = (T)G.dyn;
-      StageConst<NF> K;
-      load_stage_const<COND, VISC>(K, c, stage, b, z, G);
-      double P[NF], R[NF];
-      for (int v = 0; v < NF; v++) {
-        P[v] = b.prim[(long long)v * Z + z];
-        R[v] = b.R[(long long)v * Z + z];
-      }
-      const double l2 = l2sum<NF>(R);
-      const double l2first = b.l2[Z + z];
-      T J[NF][NF];
-      tangent_jacobian<COND, VISC, T>(P, K, Gt, c, J);
-      T bv[NF], xv[NF];
-      for (int v = 0; v < NF; v++) bv[v] = (T)(-R[v]);
-      gauss_solve<T, NF>(J, bv, xv);
-      double dPv[NF];
-      for (int v = 0; v < NF; v++) dPv[v] = (double)xv[v];
-      const double f0 = 0.5 * l2, fPrime0 = -2. * f0;
-      double lam = 1.;
-      bool haveR = false;
-      double Rt[NF];
-      for (int ls = 0; ls < c.maxLS; ls++) {
-        double Pt[NF];
-        for (int v = 0; v < NF; v++) Pt[v] = P[v] + lam * dPv[v];
-        zone_residual<COND, VISC, double, double>(Pt, K, G, c, Rt);
-        const double f1 = 0.5 * l2sum<NF>(Rt);
-        if (!(f1 > (f0 * (1. - 1e-4 * lam) + c.lsFloor))) { haveR = true; break; }
-        const double denom = (f1 - f0 - fPrime0 * lam);
-        lam = -fPrime0 * lam * lam / denom / 2.;
-      }
-      for (int v = 0; v < NF; v++) P[v] = P[v] + lam * dPv[v];
-      const bool floored = (P[0] < c.rhoFloor) || (P[1] < c.uFloor);
-      if (!last) {
-        P[0] = fmax(P[0], c.rhoFloor);
-        P[1] = fmax(P[1], c.uFloor);
-      }
-      if (!haveR || floored) zone_residual<COND, VISC, double, double>(P, K, G, c, Rt);
-      const double l2n = l2sum<NF>(Rt);
-      const bool conv = l2n <= fmax(c.atol, c.rtol * c.rtol * l2first);
-      take = !conv && !last;
-      if (!conv && last) atomicAdd(&b.st->finalUnconv[stage], 1ULL);
-      for (int v = 0; v < NF; v++) {
-        b.prim[(long long)v * Z + z] = P[v];
-        b.R[(long long)v * Z + z] = Rt[v];
-      }
+      take = list_iter_zone<COND, VISC, T>(c, stage, it, b, zone);
     }
     hist_add(b.st->itHist[stage], min(it, 15), n < count && !take);
     if (!last) list_append(b.list[out], &b.st->listCount[out], zone, take);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && count > 0) atomicMax(&b.st->itersDone[stage], (unsigned long long)it);
+}
+
+// ---------------------------------------------------------------------------
+// Ragged batch: the compacted Newton of several independent problems (grid
+// sizes may differ) in one launch per iteration.  Worklist entries are
+// global interior indices over the concatenated problems; each lane finds
+// its problem in the offset table and runs the same per-zone code with that
+// problem's configuration and buffers.
+// ---------------------------------------------------------------------------
+GRIM_D int batch_problem(const BatchEntry* tbl, int nprob, long long g) {
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tbl[mid].offset <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+// histogram add keyed by (problem, bin): one atomic per distinct key in a warp
+GRIM_D void batch_hist_add(const BatchEntry* tbl, int stage, int p, int bin, bool active) {
+  const unsigned act = __ballot_sync(0xffffffffu, active);
+  if (!active) return;
+  const unsigned peers = __match_any_sync(act, p * 16 + bin);
+  if ((threadIdx.x & 31) == __ffs(peers) - 1)
+    atomicAdd(&tbl[p].b[stage].st->itHist[stage][bin], (unsigned long long)__popc(peers));
+}
+
+template <int COND, int VISC>
+__global__ void __launch_bounds__(128) k_batch_list_init(const BatchEntry* __restrict__ tbl, int nprob,
+                                                         long long total, int stage, BatchState* bs) {
+  for (long long n0 = (long long)blockIdx.x * blockDim.x; n0 < total; n0 += (long long)gridDim.x * blockDim.x) {
+    const long long gidx_ = n0 + threadIdx.x;
+    bool take = false;
+    int p = 0;
+    if (gidx_ < total) {
+      p = batch_problem(tbl, nprob, gidx_);
+      const DevCfg& c = tbl[p].c;
+      const long long z = interior_to_z(c, gidx_ - tbl[p].offset);
+      take = list_init_zone<COND, VISC>(c, stage, tbl[p].b[stage], z);
+    }
+    batch_hist_add(tbl, stage, p, 0, gidx_ < total && !take);
+    list_append(bs->list[0], &bs->listCount[0], (int)gidx_, take);
+  }
+}
+
+template <int COND, int VISC, class T>
+__global__ void __launch_bounds__(128) k_batch_list_iter(const BatchEntry* __restrict__ tbl, int nprob, int stage,
+                                                         int it, int lastIt, BatchState* bs) {
+  const int in = (it - 1) & 1, out = it & 1;
+  const long long count = (long long)bs->listCount[in];
+  for (long long n0 = (long long)blockIdx.x * blockDim.x; n0 < count; n0 += (long long)gridDim.x * blockDim.x) {
+    const long long n = n0 + threadIdx.x;
+    bool take = false;
+    int gidx_ = 0, p = 0;
+    if (n < count) {
+      gidx_ = bs->list[in][n];
+      p = batch_problem(tbl, nprob, gidx_);
+      const DevCfg& c = tbl[p].c;
+      const long long z = interior_to_z(c, gidx_ - tbl[p].offset);
+      // a problem past its own maxIter leaves the list (its last update
+      // was counted there)
+      if (it <= c.maxIter) take = list_iter_zone<COND, VISC, T>(c, stage, it, tbl[p].b[stage], z);
+    }
+    batch_hist_add(tbl, stage, p, min(it, 15), n < count && !take);
+    {
+      // iterations done, per problem: one atomic per problem in the warp
+      const unsigned act = __ballot_sync(0xffffffffu, n < count);
+      if (n < count) {
+        const unsigned peers = __match_any_sync(act, p);
+        if ((threadIdx.x & 31) == __ffs(peers) - 1)
+          atomicMax(&tbl[p].b[stage].st->itersDone[stage], (unsigned long long)it);
+      }
+    }
+    if (it < lastIt) list_append(bs->list[out], &bs->listCount[out], gidx_, take);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1411,6 +1501,26 @@ static void newton_list_t(const DevCfg& c, int stage, const StageBufs& b, int mo
 }
 void newton_list(const DevCfg& c, int stage, const StageBufs& b, int mode, cudaStream_t s) {
   GRIM_EMHD_DISPATCH(c, newton_list_t, c, stage, b, mode, s);
+}
+
+template <int C, int V>
+static void batch_newton_t(const DevCfg& c0, const BatchEntry* tbl, int nprob, long long total, int maxIter, int stage,
+                           int mode, BatchState* bs, cudaStream_t s) {
+  (void)c0;
+  const int nb = persistent_blocks();
+  cudaMemsetAsync(bs->listCount, 0, sizeof(bs->listCount), s);
+  k_batch_list_init<C, V><<<nb, 128, 0, s>>>(tbl, nprob, total, stage, bs);
+  for (int it = 1; it <= maxIter; it++) {
+    cudaMemsetAsync(&bs->listCount[it & 1], 0, sizeof(unsigned long long), s);
+    if (mode == GRIM_NEWTON_MIXED32)
+      k_batch_list_iter<C, V, float><<<nb, 128, 0, s>>>(tbl, nprob, stage, it, maxIter, bs);
+    else
+      k_batch_list_iter<C, V, double><<<nb, 128, 0, s>>>(tbl, nprob, stage, it, maxIter, bs);
+  }
+}
+void batch_newton(const DevCfg& c0, const BatchEntry* tbl, int nprob, long long total, int maxIter, int stage,
+                  int mode, BatchState* bs, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c0, batch_newton_t, c0, tbl, nprob, total, maxIter, stage, mode, bs, s);
 }
 
 template <int C, int V>

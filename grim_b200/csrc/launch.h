@@ -65,6 +65,10 @@ void adjoint_stencil_t(const DevCfg& c, const double* P, const double* g, double
 
 namespace grim {
 namespace fast {
+// the compacted Newton of a ragged batch: one launch per iteration over
+// all problems' unconverged zones (tbl, bs in device memory)
+void batch_newton(const DevCfg& c0, const BatchEntry* tbl, int nprob, long long total, int maxIter, int stage,
+                  int mode, BatchState* bs, cudaStream_t s);
 // algorithmic flop counts of one zone's residual / tangent / solve
 void count_ops(const DevCfg& c, int stage, const StageBufs& b, long long z, double* out, cudaStream_t s);
 }  // namespace fast

@@ -306,10 +306,13 @@ static void enqueue_full_diagnostics(grim_handle* h) {
   g_launch_counter += 2;
 }
 
-static void enqueue_step(grim_handle* h, bool timed) {
+// The step in segments around the two stencil + Newton pairs, so that a
+// batch of problems can interleave its problems around one shared Newton
+// launch: pre_half -> stencil(half) -> Newton(half) -> mid -> stencil(full)
+// -> Newton(full) -> post.
+static void enqueue_pre_half(grim_handle* h, bool timed) {
   const DevCfg& c = h->dc;
   cudaStream_t s = h->stream;
-  const size_t bytes = (size_t)c.dof * c.Z * sizeof(double);
   if (timed) cudaEventRecord(h->ev[0], s);
   // computeDt (timestep.cpp:8): dt from the last elemOld state
   if (!h->fixedDt) {
@@ -331,10 +334,12 @@ static void enqueue_step(grim_handle* h, bool timed) {
   enqueue_problem_bcs(h, h->primOld);
   if (!h->cfg.elemOldFromFullStep) enqueue_dt_speeds(h, h->primOld, 0);
   if (timed) cudaEventRecord(h->ev[1], s);
-  enqueue_stencil(h, GRIM_HALF_STEP);
-  if (timed) cudaEventRecord(h->ev[2], s);
-  enqueue_newton(h, GRIM_HALF_STEP);
-  if (timed) cudaEventRecord(h->ev[3], s);
+}
+
+static void enqueue_mid(grim_handle* h) {
+  const DevCfg& c = h->dc;
+  cudaStream_t s = h->stream;
+  const size_t bytes = (size_t)c.dof * c.Z * sizeof(double);
   {
     PROF(GRIM_PROF_COPY);
     cudaMemcpyAsync(h->primHalf, h->prim, bytes, cudaMemcpyDeviceToDevice, s);
@@ -352,11 +357,12 @@ static void enqueue_step(grim_handle* h, bool timed) {
     g_launch_counter++;
   }
   enqueue_problem_bcs(h, h->primHalf);
-  if (timed) cudaEventRecord(h->ev[4], s);
-  enqueue_stencil(h, GRIM_FULL_STEP);
-  if (timed) cudaEventRecord(h->ev[5], s);
-  enqueue_newton(h, GRIM_FULL_STEP);
-  if (timed) cudaEventRecord(h->ev[6], s);
+}
+
+static void enqueue_post(grim_handle* h, bool timed) {
+  const DevCfg& c = h->dc;
+  cudaStream_t s = h->stream;
+  const size_t bytes = (size_t)c.dof * c.Z * sizeof(double);
   {
     PROF(GRIM_PROF_COPY);
     cudaMemcpyAsync(h->primOld, h->prim, bytes, cudaMemcpyDeviceToDevice, s);
@@ -381,6 +387,22 @@ static void enqueue_step(grim_handle* h, bool timed) {
     g_launch_counter++;
   }
   if (timed) cudaEventRecord(h->ev[7], s);
+}
+
+static void enqueue_step(grim_handle* h, bool timed) {
+  cudaStream_t s = h->stream;
+  enqueue_pre_half(h, timed);
+  enqueue_stencil(h, GRIM_HALF_STEP);
+  if (timed) cudaEventRecord(h->ev[2], s);
+  enqueue_newton(h, GRIM_HALF_STEP);
+  if (timed) cudaEventRecord(h->ev[3], s);
+  enqueue_mid(h);
+  if (timed) cudaEventRecord(h->ev[4], s);
+  enqueue_stencil(h, GRIM_FULL_STEP);
+  if (timed) cudaEventRecord(h->ev[5], s);
+  enqueue_newton(h, GRIM_FULL_STEP);
+  if (timed) cudaEventRecord(h->ev[6], s);
+  enqueue_post(h, timed);
 }
 
 // ---------------------------------------------------------------------------
@@ -1159,6 +1181,191 @@ int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, in
   CK(cudaMemcpyAsync(grad, lam, bytes, memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                      h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  return GRIM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// ragged batch: independent problems (grid sizes may differ) stepped
+// together on one stream; the compacted Newton of each stage is one launch
+// per iteration over all problems' unconverged zones
+// ---------------------------------------------------------------------------
+struct grim_batch {
+  int device = 0;
+  std::vector<grim_handle*> h;
+  cudaStream_t stream = nullptr;
+  BatchEntry* tbl = nullptr;   // device
+  BatchState* state = nullptr; // device
+  int* lists = nullptr;        // device, 2 x total
+  long long total = 0;
+  int maxIter = 0;
+  int mode = GRIM_NEWTON_MIXED32;
+  bool graphOn = false;
+  cudaGraphExec_t graph = nullptr;
+};
+
+static void batch_free(grim_batch* B) {
+  if (B->graph) cudaGraphExecDestroy(B->graph);
+  if (B->tbl) cudaFree(B->tbl);
+  if (B->state) cudaFree(B->state);
+  if (B->lists) cudaFree(B->lists);
+  for (grim_handle* h : B->h) {
+    if (!h) continue;
+    h->stream = nullptr;  // the batch's stream, destroyed below
+    grim_destroy(h);
+  }
+  if (B->stream) cudaStreamDestroy(B->stream);
+  delete B;
+}
+
+static int batch_upload(grim_batch* B) {
+  std::vector<BatchEntry> t(B->h.size());
+  long long off = 0;
+  B->maxIter = 0;
+  for (size_t p = 0; p < B->h.size(); p++) {
+    grim_handle* h = B->h[p];
+    t[p].c = h->dc;
+    t[p].b[GRIM_HALF_STEP] = stage_bufs(h, GRIM_HALF_STEP);
+    t[p].b[GRIM_FULL_STEP] = stage_bufs(h, GRIM_FULL_STEP);
+    t[p].offset = off;
+    off += h->dc.Zint;
+    B->maxIter = std::max(B->maxIter, h->dc.maxIter);
+  }
+  B->total = off;
+  CK(cudaMemcpyAsync(B->tbl, t.data(), sizeof(BatchEntry) * t.size(), cudaMemcpyHostToDevice, B->stream));
+  CK(cudaStreamSynchronize(B->stream));
+  if (B->graph) { cudaGraphExecDestroy(B->graph); B->graph = nullptr; }
+  return GRIM_OK;
+}
+
+int grim_batch_create(const grim_config* cfgs, int n, int device, grim_batch** out) {
+  if (!cfgs || n <= 0 || !out) { set_err("grim_batch_create: bad argument"); return GRIM_EINVAL; }
+  *out = nullptr;
+  for (int p = 1; p < n; p++)
+    if (cfgs[p].conduction != cfgs[0].conduction || cfgs[p].viscosity != cfgs[0].viscosity) {
+      set_err("grim_batch_create: the problems of a batch share conduction / viscosity flags");
+      return GRIM_EINVAL;
+    }
+  grim_batch* B = new grim_batch();
+  B->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_err("grim_batch_create: stream creation failed");
+    delete B;
+    return GRIM_ECUDA;
+  }
+  for (int p = 0; p < n; p++) {
+    grim_handle* h = nullptr;
+    int rc = grim_create(&cfgs[p], device, &h);
+    if (rc) { B->h.push_back(nullptr); batch_free(B); return rc; }
+    cudaStreamSynchronize(h->stream);
+    cudaStreamDestroy(h->stream);
+    h->stream = B->stream;
+    h->cfg.newtonMode = GRIM_NEWTON_MIXED32;
+    h->cfg.perZoneConvergence = 2;
+    B->h.push_back(h);
+  }
+  long long total = 0;
+  for (grim_handle* h : B->h) total += h->dc.Zint;
+  if (total >= (1LL << 31)) { set_err("grim_batch_create: more than 2^31 zones"); batch_free(B); return GRIM_EINVAL; }
+  if (cudaMalloc(&B->tbl, sizeof(BatchEntry) * n) != cudaSuccess ||
+      cudaMalloc(&B->state, sizeof(BatchState)) != cudaSuccess ||
+      cudaMalloc(&B->lists, sizeof(int) * 2 * (size_t)total) != cudaSuccess) {
+    set_err("grim_batch_create: device allocation failed");
+    batch_free(B);
+    return GRIM_ENOMEM;
+  }
+  BatchState hs;
+  memset(&hs, 0, sizeof(hs));
+  hs.list[0] = B->lists;
+  hs.list[1] = B->lists + total;
+  if (cudaMemcpy(B->state, &hs, sizeof(hs), cudaMemcpyHostToDevice) != cudaSuccess) {
+    set_err("grim_batch_create: state upload failed");
+    batch_free(B);
+    return GRIM_ECUDA;
+  }
+  int rc = batch_upload(B);
+  if (rc) { batch_free(B); return rc; }
+  *out = B;
+  return GRIM_OK;
+}
+
+int grim_batch_destroy(grim_batch* B) {
+  if (!B) return GRIM_OK;
+  cudaSetDevice(B->device);
+  cudaStreamSynchronize(B->stream);
+  batch_free(B);
+  return GRIM_OK;
+}
+
+int grim_batch_size(const grim_batch* B) { return B ? (int)B->h.size() : 0; }
+
+int grim_batch_problem(grim_batch* B, int p, grim_handle** h) {
+  if (!B || !h || p < 0 || p >= (int)B->h.size()) { set_err("grim_batch_problem: bad index"); return GRIM_EINVAL; }
+  *h = B->h[p];
+  return GRIM_OK;
+}
+
+int grim_batch_set_newton_mode(grim_batch* B, int mode, double rtol) {
+  if (!B || (mode != GRIM_NEWTON_MIXED32 && mode != GRIM_NEWTON_TANGENT64)) {
+    set_err("grim_batch_set_newton_mode: the batch runs the tangent or mixed compacted Newton");
+    return GRIM_EINVAL;
+  }
+  for (grim_handle* h : B->h) {
+    int rc = grim_set_newton_mode(h, mode, 2, rtol);
+    if (rc) return rc;
+  }
+  B->mode = mode;
+  return batch_upload(B);
+}
+
+static void enqueue_batch_step(grim_batch* B) {
+  const DevCfg& c0 = B->h[0]->dc;
+  for (grim_handle* h : B->h) enqueue_pre_half(h, false);
+  for (grim_handle* h : B->h) enqueue_stencil(h, GRIM_HALF_STEP);
+  grim::fast::batch_newton(c0, B->tbl, (int)B->h.size(), B->total, B->maxIter, GRIM_HALF_STEP, B->mode, B->state,
+                           B->stream);
+  for (grim_handle* h : B->h) enqueue_mid(h);
+  for (grim_handle* h : B->h) enqueue_stencil(h, GRIM_FULL_STEP);
+  grim::fast::batch_newton(c0, B->tbl, (int)B->h.size(), B->total, B->maxIter, GRIM_FULL_STEP, B->mode, B->state,
+                           B->stream);
+  for (grim_handle* h : B->h) enqueue_post(h, false);
+}
+
+int grim_batch_enable_graph(grim_batch* B, int enable) {
+  if (!B) return GRIM_EINVAL;
+  B->graphOn = enable != 0;
+  if (!B->graphOn && B->graph) { cudaGraphExecDestroy(B->graph); B->graph = nullptr; }
+  return GRIM_OK;
+}
+
+int grim_batch_time_steps(grim_batch* B, int nsteps) {
+  if (!B || nsteps < 0) return GRIM_EINVAL;
+  CK(cudaSetDevice(B->device));
+  for (grim_handle* h : B->h)
+    if (h->fixedDt != B->h[0]->fixedDt) { set_err("grim_batch_time_steps: mixed dt modes"); return GRIM_EINVAL; }
+  for (int n = 0; n < nsteps; n++) {
+    if (B->graphOn) {
+      if (!B->graph) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_batch_step(B);
+        CK(cudaStreamEndCapture(B->stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&B->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { set_err("batch graph instantiate: %s", cudaGetErrorString(e)); return GRIM_ECUDA; }
+      }
+      CK(cudaGraphLaunch(B->graph, B->stream));
+    } else {
+      enqueue_batch_step(B);
+    }
+  }
+  CK(cudaGetLastError());
+  return GRIM_OK;
+}
+
+int grim_batch_synchronize(grim_batch* B) {
+  if (!B) return GRIM_EINVAL;
+  CK(cudaSetDevice(B->device));
+  CK(cudaStreamSynchronize(B->stream));
   return GRIM_OK;
 }
 

@@ -38,4 +38,18 @@ struct StageBufs {
   int* list[2];           // compacted Newton worklists (interior zone indices)
 };
 
+// one problem of a ragged batch: its configuration, its stage buffers
+// (half, full) and the offset of its first interior zone in the batch's
+// concatenated index space
+struct BatchEntry {
+  DevCfg c;
+  StageBufs b[2];
+  long long offset;
+};
+// the batch's shared worklists (global interior indices) and their counts
+struct BatchState {
+  unsigned long long listCount[2];
+  int* list[2];
+};
+
 }  // namespace grim

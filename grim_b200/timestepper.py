@@ -71,12 +71,17 @@ class timeStepper:
 
     HALF_STEP, FULL_STEP = C.HALF_STEP, C.FULL_STEP
 
-    def __init__(self, cfg, device=0):
+    def __init__(self, cfg, device=0, _handle=None):
         self.cfg = dict(cfg)
-        s = C.to_struct(self.cfg)
-        self._h = ctypes.c_void_p()
         L = _lib.lib()
-        _lib.check(L.grim_create(ctypes.byref(s), int(device), ctypes.byref(self._h)), "grim_create")
+        if _handle is None:
+            s = C.to_struct(self.cfg)
+            self._h = ctypes.c_void_p()
+            _lib.check(L.grim_create(ctypes.byref(s), int(device), ctypes.byref(self._h)), "grim_create")
+            self._owned = True
+        else:  # a problem of a Batch: the batch owns the handle
+            self._h = ctypes.c_void_p(_handle)
+            self._owned = False
         a, b, c, dof, nf = (ctypes.c_int() for _ in range(5))
         L.grim_dims(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(dof),
                     ctypes.byref(nf))
@@ -104,9 +109,9 @@ class timeStepper:
         return cls(cfg)
 
     def close(self):
-        if getattr(self, "_h", None) and self._h.value:
+        if getattr(self, "_h", None) and self._h.value and getattr(self, "_owned", True):
             _lib.lib().grim_destroy(self._h)
-            self._h = ctypes.c_void_p()
+        self._h = ctypes.c_void_p()
 
     def __del__(self):
         try:
@@ -332,6 +337,58 @@ class timeStepper:
         _lib.check(_lib.lib().grim_set_geometry(self._h, int(location), _ptr(out),
                                                 None if gm is None else _ptr(gm),
                                                 None if xc is None else _ptr(xc), _lib.HOST), "set_geometry")
+
+
+class Batch:
+    """Independent problems stepped together (grim_batch_*): per problem the
+    stencil launches, per stage one compacted Newton launch per iteration
+    over all problems' unconverged zones.  problems[p] is a timeStepper view
+    of problem p (state, time, statistics); the batch owns it."""
+
+    def __init__(self, cfgs, device=0):
+        L = _lib.lib()
+        n = len(cfgs)
+        arr = (type(C.to_struct(cfgs[0])) * n)(*[C.to_struct(dict(c)) for c in cfgs])
+        self._b = ctypes.c_void_p()
+        _lib.check(L.grim_batch_create(ctypes.cast(arr, ctypes.c_void_p), n, int(device), ctypes.byref(self._b)),
+                   "grim_batch_create")
+        self.problems = []
+        for p, cfg in enumerate(cfgs):
+            h = ctypes.c_void_p()
+            _lib.check(L.grim_batch_problem(self._b, p, ctypes.byref(h)), "grim_batch_problem")
+            ts = timeStepper(cfg, _handle=h.value)
+            ts.cfg["newtonMode"] = C.NEWTON_MIXED32
+            self.problems.append(ts)
+
+    def setNewtonMode(self, mode, rtol=0.0):
+        _lib.check(_lib.lib().grim_batch_set_newton_mode(self._b, int(mode), float(rtol)), "batch_newton_mode")
+        for ts in self.problems:
+            ts.cfg["newtonMode"] = int(mode)
+
+    def enableGraph(self, on=True):
+        _lib.check(_lib.lib().grim_batch_enable_graph(self._b, int(bool(on))), "batch_enable_graph")
+
+    def timeSteps(self, n):
+        _lib.check(_lib.lib().grim_batch_time_steps(self._b, int(n)), "batch_time_steps")
+
+    def synchronize(self):
+        _lib.check(_lib.lib().grim_batch_synchronize(self._b), "batch_synchronize")
+
+    def stream(self):
+        return self.problems[0].stream()
+
+    def close(self):
+        if getattr(self, "_b", None) and self._b.value:
+            for ts in self.problems:
+                ts._h = ctypes.c_void_p()
+            _lib.lib().grim_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def measurePeaks(device=0):

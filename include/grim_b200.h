@@ -275,6 +275,26 @@ int grim_set_face_variant(grim_handle* h, int dir, int variant);
  * otherwise).  Zones accumulate with double atomics, so results agree run
  * to run to roundoff. */
 int grim_set_dt_mode(grim_handle* h, int fixed);
+
+/* ---- ragged batch.  No counterpart in the reference (one problem per
+ *      run).  Independent problems, grid sizes free, step together on one
+ *      stream: per problem the stencil launches of timeStep, and for each
+ *      stage ONE compacted Newton launch per iteration over the unconverged
+ *      zones of all problems (tangent or mixed mode).  The problems share
+ *      the conduction / viscosity flags; each keeps its own dt, time,
+ *      boundaries, metric and reconstruction.  grim_batch_problem returns
+ *      problem p's handle for set/get of its state and its statistics;
+ *      that handle is owned by the batch (do not destroy it) and runs on
+ *      the batch's stream. */
+typedef struct grim_batch grim_batch;
+int grim_batch_create(const grim_config* cfgs, int n, int device, grim_batch** out);
+int grim_batch_destroy(grim_batch* b);
+int grim_batch_size(const grim_batch* b);
+int grim_batch_problem(grim_batch* b, int p, grim_handle** h);
+int grim_batch_set_newton_mode(grim_batch* b, int mode, double rtol);
+int grim_batch_enable_graph(grim_batch* b, int enable);
+int grim_batch_time_steps(grim_batch* b, int nsteps);
+int grim_batch_synchronize(grim_batch* b);
 int grim_adjoint_forward(grim_handle* h, int nsteps, int every);
 int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, int memKind);
 /* the transpose of the stencil alone, for tests: out = (d divF / d prim)^T
