@@ -940,6 +940,10 @@ int grim_get_stats(grim_handle* h, grim_stats* out) {
       s.msNewton = c2 + d;
     s.msOther = s.msStep - s.msStencil - s.msNewton;
   }
+  // events a caller never recorded (a batch problem's, untimed steps) make
+  // the elapsed-time queries fail; that is handled above, so the pending
+  // error is cleared rather than left for the next checked call
+  (void)cudaGetLastError();
   s.kernelLaunches = h->launchesPerStep;
   *out = s;
   return GRIM_OK;
