@@ -1,6 +1,7 @@
 // common.cuh -- device-side configuration, grid indexing and the forward
 // tangent (dual number) scalar used by the Newton kernels.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>

@@ -269,6 +269,127 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1(DevCfg c, const doub
   riemann_face<COND, VISC>(c, 0, pl, G, flux, z, park_x1);
 }
 
+// ---------------------------------------------------------------------------
+// X1 faces with TMA-staged rows.  Persistent warps walk over the 31-face row
+// segments; while a warp computes one segment, the tensor-memory accelerator
+// copies the next segment's primitives (all dof, 40 zones along i) into the
+// warp's other shared-memory buffer, so the stencil loads come from shared
+// memory.  The tensor map covers the prim array as (i, j, k, var).  Waits
+// on the copy barrier are bounded: a wait that gives up counts in
+// DevState::waitTimeouts and the warp stops after its copy in flight lands.
+// ---------------------------------------------------------------------------
+constexpr int kX1Box = 40;  // zones per TMA row box (x rounded down to even)
+
+GRIM_D unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+GRIM_D void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+GRIM_D void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+GRIM_D void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+GRIM_D bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: false when the barrier did not complete within the limit
+GRIM_D bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+  for (int spin = 0; spin < (1 << 22); spin++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+GRIM_D void tma_load_4d(void* dst, const CUtensorMap* map, unsigned long long* bar, int x, int y, int z, int w) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(smem_u32(dst)),
+      "l"((unsigned long long)map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(bar))
+      : "memory");
+}
+
+template <int COND, int VISC, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_face_flux_x1_tma(const __grid_constant__ CUtensorMap tmap, DevCfg c,
+                                                                 const double* __restrict__ geoF,
+                                                                 double* __restrict__ flux, DevState* st) {
+  constexpr int DOF = 8 + COND + VISC;
+  constexpr int ROW = DOF * kX1Box;  // doubles per row buffer (a multiple of 128 bytes)
+  extern __shared__ __align__(128) double smem_x1[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double* rows = smem_x1 + (size_t)w * 2 * ROW;
+  double* park = smem_x1 + (size_t)nw * 2 * ROW;
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(park + 3 * DOF * blockDim.x) + 2 * w;
+  const int nfaces = c.N1T - 5;  // faces i = 3 .. N1T-3
+  const int wpr = (nfaces + 30) / 31;
+  const long long nitems = (long long)c.N2T * c.N3T * wpr;
+  const long long stride = (long long)gridDim.x * nw;
+  long long item = (long long)blockIdx.x * nw + w;
+  if (lane == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncwarp();
+  auto issue = [&](long long it, int buf) {
+    const long long row = it / wpr;
+    const int i0 = 3 + (int)(it % wpr) * 31;
+    const int j = (int)(row % c.N2T), k = (int)(row / c.N2T);
+    mbar_expect_tx(&bars[buf], ROW * (unsigned)sizeof(double));
+    tma_load_4d(rows + buf * ROW, &tmap, &bars[buf], (i0 - 3) & ~1, j, k, 0);
+  };
+  if (lane == 0 && item < nitems) issue(item, 0);
+  unsigned phase0 = 0, phase1 = 0;
+  int buf = 0;
+  for (; item < nitems; item += stride, buf ^= 1) {
+    const long long next = item + stride;
+    if (lane == 0 && next < nitems) issue(next, buf ^ 1);
+    const unsigned ph = buf ? phase1 : phase0;
+    const bool arrived = mbar_wait_bounded(&bars[buf], ph);
+    if (buf) phase1 ^= 1; else phase0 ^= 1;
+    if (!__all_sync(0xffffffffu, arrived)) {
+      // give up: count it, let the copy in flight (if any) land, stop
+      if (lane == 0) {
+        atomicAdd(&st->waitTimeouts, 1ULL);
+        if (next < nitems) mbar_wait_bounded(&bars[buf ^ 1], buf ? phase0 : phase1);
+      }
+      __syncwarp();
+      return;
+    }
+    const long long row = item / wpr;
+    const int i0 = 3 + (int)(item % wpr) * 31;
+    const int j = (int)(row % c.N2T), k = (int)(row / c.N2T);
+    const int x0 = (i0 - 3) & ~1;
+    const int iz = i0 - 1 + lane;
+    const bool reconOK = iz >= 2 && iz <= c.N1T - 3;
+    const int iu = reconOK ? iz : i0 - 1;  // a zone inside the buffer
+    const double* rb = rows + buf * ROW;
+    double lo[DOF], ro[DOF];
+#pragma unroll
+    for (int v = 0; v < DOF; v++) {
+      const double* a = rb + v * kX1Box + (iu - x0);
+      if (kFastMath)
+        recon_faces_fast(c.reconstruction, c.theta, a[-2], a[-1], a[0], a[1], a[2], lo[v], ro[v]);
+      else
+        recon_faces(c.reconstruction, c.theta, a[-2], a[-1], a[0], a[1], a[2], lo[v], ro[v]);
+    }
+    __syncwarp();  // the buffer is read; it may be refilled two items on
+    double pl[DOF];
+#pragma unroll
+    for (int v = 0; v < DOF; v++) pl[v] = __shfl_up_sync(0xffffffffu, ro[v], 1);
+    if (lane > 0 && reconOK) {
+      const long long z = zidx(c, iz, j, k);
+      ZoneGeo<double> G;
+      load_geo(G, c, geoF, z, iz, j, 0., 0.5);
+#pragma unroll
+      for (int v = 0; v < DOF; v++) park[(2 * DOF + v) * blockDim.x + threadIdx.x] = lo[v];
+      riemann_face<COND, VISC>(c, 0, pl, G, flux, z, park);
+    }
+  }
+}
+
 // X2 / X3 faces: the X1 scheme turned sideways.  A warp holds QI
 // consecutive i (lane % QI) by 32/QI consecutive zones along dir
 // (lane / QI); every lane reconstructs its zone once and the right-face
@@ -367,6 +488,26 @@ static __global__ void k_emf(DevCfg c, const double* __restrict__ F1, const doub
   out[2 * Z + z] = e3;
 }
 
+// The stage's corner EMFs (constrainedtransport.cpp:53-83), each computed
+// once per zone corner instead of four times by the zones that share it:
+// emfX3 at (i-1/2, j-1/2), and in 3D emfX1 at (j-1/2, k-1/2), emfX2 at
+// (i-1/2, k-1/2); corners whose neighbours fall off the grid are skipped
+// (no interior zone reads them).
+static __global__ void k_stage_emf(DevCfg c, StageBufs b) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  FluxView f;
+  f.F[0] = b.flux[0]; f.F[1] = b.flux[1]; f.F[2] = b.flux[2]; f.Z = c.Z; f.B1 = c.B1;
+  const long long s1 = 1, s2 = (long long)c.N1T, s3 = (long long)c.N1T * c.N2T;
+  if (i >= 1 && j >= 1) b.emf[2 * c.Z + z] = emf3(f, z, s1, s2);
+  if (c.dim == 3 && k >= 1) {
+    if (j >= 1) b.emf[z] = emf1(f, z, s2, s3);
+    if (i >= 1) b.emf[c.Z + z] = emf2(f, z, s1, s3);
+  }
+}
+
 template <int COND, int VISC>
 __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, StageBufs b) {
   constexpr int NF = 5 + COND + VISC;
@@ -393,8 +534,9 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
   if (c.dim == 1) {
     for (int b3 = 0; b3 < 3; b3++) { Fl[0][NF + b3] = f.at(0, c.B1 + b3, z); Fr[0][NF + b3] = f.at(0, c.B1 + b3, z + s1); }
   } else if (c.dim == 2) {
-    const double e00 = emf3(f, z, s1, s2), e10 = emf3(f, z + s1, s1, s2);
-    const double e01 = emf3(f, z + s2, s1, s2), e11 = emf3(f, z + s1 + s2, s1, s2);
+    const double* E3 = b.emf + 2 * Z;
+    const double e00 = E3[z], e10 = E3[z + s1];
+    const double e01 = E3[z + s2], e11 = E3[z + s1 + s2];
     // F1: B1 -> 0, B2 -> 0.5 (emf3 + emf3[j+1]); F2: B1 -> -0.5 (emf3 + emf3[i+1]), B2 -> 0
     Fl[0][NF + 1] = 0.5 * (e00 + e01);
     Fr[0][NF + 1] = 0.5 * (e10 + e11);
@@ -406,12 +548,13 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
     Fr[1][NF + 2] = f.at(1, c.B1 + 2, z + s2);
   } else {
     // EMF3 at (i|i+1, j|j+1), EMF2 at (i|i+1, k|k+1), EMF1 at (j|j+1, k|k+1)
-    const double a00 = emf3(f, z, s1, s2), a10 = emf3(f, z + s1, s1, s2);
-    const double a01 = emf3(f, z + s2, s1, s2), a11 = emf3(f, z + s1 + s2, s1, s2);
-    const double b00 = emf2(f, z, s1, s3), b10 = emf2(f, z + s1, s1, s3);
-    const double b01 = emf2(f, z + s3, s1, s3), b11 = emf2(f, z + s1 + s3, s1, s3);
-    const double c00 = emf1(f, z, s2, s3), c10 = emf1(f, z + s2, s2, s3);
-    const double c01 = emf1(f, z + s3, s2, s3), c11 = emf1(f, z + s2 + s3, s2, s3);
+    const double *E1 = b.emf, *E2 = b.emf + Z, *E3 = b.emf + 2 * Z;
+    const double a00 = E3[z], a10 = E3[z + s1];
+    const double a01 = E3[z + s2], a11 = E3[z + s1 + s2];
+    const double b00 = E2[z], b10 = E2[z + s1];
+    const double b01 = E2[z + s3], b11 = E2[z + s1 + s3];
+    const double c00 = E1[z], c10 = E1[z + s2];
+    const double c01 = E1[z + s3], c11 = E1[z + s2 + s3];
     Fl[0][NF + 1] = 0.5 * (a00 + a01);  Fr[0][NF + 1] = 0.5 * (a10 + a11);
     Fl[0][NF + 2] = -0.5 * (b00 + b01); Fr[0][NF + 2] = -0.5 * (b10 + b11);
     Fl[1][NF + 0] = -0.5 * (a00 + a10); Fr[1][NF + 0] = -0.5 * (a01 + a11);
@@ -468,12 +611,30 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
     double T[4][4];
     for (int ka = 0; ka < 4; ka++)
       for (int la = 0; la < 4; la++) T[ka][la] = tmunu<COND, VISC>(e, ka, la);
-    for (int nu = 0; nu < 4; nu++) {
-      double s = S[UU + nu];
-      for (int ka = 0; ka < 4; ka++)
-        for (int la = 0; la < 4; la++)
-          s -= G.g * T[ka][la] * __ldg(b.gamma + (long long)(la * 16 + ka * 4 + nu) * c.GZ + gidx(c, i, j));
-      S[UU + nu] = s;
+    const double* gam = b.gamma + gidx(c, i, j);
+    if constexpr (kFastMath) {
+      // Gamma^la_(ka nu) is symmetric in its lower pair: 40 loads, each
+      // used for (ka, nu) and (nu, ka)
+      double acc[4] = {S[UU], S[UU + 1], S[UU + 2], S[UU + 3]};
+#pragma unroll
+      for (int la = 0; la < 4; la++)
+#pragma unroll
+        for (int ka = 0; ka < 4; ka++)
+#pragma unroll
+          for (int nu = ka; nu < 4; nu++) {
+            const double gv = G.g * __ldg(gam + (long long)(la * 16 + ka * 4 + nu) * c.GZ);
+            acc[nu] -= T[ka][la] * gv;
+            if (nu != ka) acc[ka] -= T[nu][la] * gv;
+          }
+      for (int nu = 0; nu < 4; nu++) S[UU + nu] = acc[nu];
+    } else {
+      for (int nu = 0; nu < 4; nu++) {
+        double s = S[UU + nu];
+        for (int ka = 0; ka < 4; ka++)
+          for (int la = 0; la < 4; la++)
+            s -= G.g * T[ka][la] * __ldg(gam + (long long)(la * 16 + ka * 4 + nu) * c.GZ);
+        S[UU + nu] = s;
+      }
     }
   }
   if (COND || VISC) {
@@ -1391,13 +1552,42 @@ static void face_strip_launch(const DevCfg& c, int dir, const double* ps, const 
   const size_t park = 3 * (8 + C + V) * 128 * sizeof(double);
   k_face_flux_strip<C, V, QI, MINB><<<nblk(warps * 32, 128), 128, park, s>>>(c, dir, ps, geoF, geoC, flux);
 }
+static int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+template <int C, int V, int MINB>
+static void face_x1_tma_launch(const DevCfg& c, const CUtensorMap* tmap, const double* geoF, double* flux,
+                               DevState* st, cudaStream_t s) {
+  constexpr int DOF = 8 + C + V;
+  const int nw = 4;
+  const size_t smem = ((size_t)nw * 2 * DOF * kX1Box + 3 * DOF * 128) * sizeof(double) + 2 * nw * 8;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_face_flux_x1_tma<C, V, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  k_face_flux_x1_tma<C, V, MINB><<<sm_count() * MINB, 32 * nw, smem, s>>>(*tmap, c, geoF, flux, st);
+}
 template <int C, int V>
 static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,
-                        double* flux, int variant, cudaStream_t s) {
+                        double* flux, int variant, const CUtensorMap* tmap, DevState* st, cudaStream_t s) {
   if constexpr (C == 0 && V == 0) {
     if (dir == 0) {
-      if (variant == 1) face_x1_launch<C, V, 4>(c, ps, geoF, flux, s);
-      else face_x1_launch<C, V, 3>(c, ps, geoF, flux, s);
+      if (variant >= 2 && tmap && st) {
+        if (variant == 3) face_x1_tma_launch<C, V, 4>(c, tmap, geoF, flux, st, s);
+        else face_x1_tma_launch<C, V, 3>(c, tmap, geoF, flux, st, s);
+      } else if (variant == 1 || variant == 3) {
+        face_x1_launch<C, V, 4>(c, ps, geoF, flux, s);
+      } else {
+        face_x1_launch<C, V, 3>(c, ps, geoF, flux, s);
+      }
       return;
     }
     switch (variant) {
@@ -1410,23 +1600,28 @@ static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double
     }
   } else {
     // EMHD elements need more registers: two resident blocks
+    (void)tmap;
+    (void)st;
     if (dir == 0) face_x1_launch<C, V, 2>(c, ps, geoF, flux, s);
     else face_strip_launch<C, V, 4, 2>(c, dir, ps, geoF, geoC, flux, s);
   }
 }
 void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC, double* flux,
-               int variant, cudaStream_t s) {
-  GRIM_EMHD_DISPATCH(c, face_flux_t, c, dir, ps, geoF, geoC, flux, variant, s);
+               int variant, const CUtensorMap* tmap, DevState* st, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, face_flux_t, c, dir, ps, geoF, geoC, flux, variant, tmap, st, s);
 }
+// X1: 0, 1 = register budget 3 / 4 blocks; 2, 3 = the same with TMA-staged
+// rows (when the caller has a tensor map of the primitives)
 int face_variants(const DevCfg& c, int dir) {
   if (c.conduction || c.viscosity) return 1;
-  return dir == 0 ? 2 : 6;
+  return dir == 0 ? 4 : 6;
 }
 #endif  // !GRIM_SKIP_FACES
 
 #if !defined(GRIM_ONLY_FACES)
 template <int C, int V>
 static void stage_epilogue_t(const DevCfg& c, int stage, const StageBufs& b, cudaStream_t s) {
+  if (c.dim >= 2) k_stage_emf<<<nblk(c.Z, 256), 256, 0, s>>>(c, b);
   k_stage_epilogue<C, V><<<nblk(c.Zint, 128), 128, 0, s>>>(c, stage, b);
 }
 void stage_epilogue(const DevCfg& c, int stage, const StageBufs& b, cudaStream_t s) {

@@ -11,7 +11,7 @@
   void communicate(const DevCfg& c, double* prim, int nv, cudaStream_t s);                              \
   void emhd_prepass(const DevCfg& c, const double* ps, const double* geoC, double* uT, cudaStream_t s); \
   void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,    \
-                 double* flux, int variant, cudaStream_t s);                                            \
+                 double* flux, int variant, const CUtensorMap* tmap, DevState* st, cudaStream_t s);    \
   int face_variants(const DevCfg& c, int dir);                                                          \
   void stage_epilogue(const DevCfg& c, int stage, const StageBufs& b, cudaStream_t s);                  \
   void dt_speeds(const DevCfg& c, const double* p, const double* geoC, int mode, DevState* st,          \

@@ -82,10 +82,11 @@ extern "C" int grim_div_fluxes_noalloc(const grim_config* cfg, const double* pri
   const long long Z = c.Z;
   const bool emhd = c.conduction || c.viscosity;
   // scratch layout (words): face fluxes dim*dof*Z | consOld dof*Z | guess
-  // dof*Z | Sexp nf*Z | uT 5*Z (EMHD) | device scalars
+  // dof*Z | Sexp nf*Z | uT 5*Z (EMHD) | corner EMFs 3*Z (2D/3D) | device
+  // scalars
   const long long stateWords = (long long)((sizeof(DevState) + 255) / 256 * 256 / sizeof(double));
   const long long need = (long long)c.dim * c.dof * Z + 2LL * c.dof * Z + (long long)c.nf * Z +
-                         (emhd ? 5LL * Z : 0LL) + stateWords;
+                         (emhd ? 5LL * Z : 0LL) + (c.dim >= 2 ? 3LL * Z : 0LL) + stateWords;
   if (need > GRIM_NOALLOC_SCRATCH_WORDS) {
     char msg[256];
     snprintf(msg, sizeof(msg),
@@ -109,6 +110,7 @@ extern "C" int grim_div_fluxes_noalloc(const grim_config* cfg, const double* pri
   b.prim = w; w += (long long)c.dof * Z;
   b.Sexp = w; w += (long long)c.nf * Z;
   if (emhd) { b.uT = w; w += 5LL * Z; }
+  if (c.dim >= 2) { b.emf = w; w += 3LL * Z; }
   b.st = reinterpret_cast<DevState*>(w);
   b.ps = prim;
   b.pold = prim;
@@ -118,7 +120,7 @@ extern "C" int grim_div_fluxes_noalloc(const grim_config* cfg, const double* pri
   // dt = 0 for the induction part of the epilogue (its output is not used)
   if (cudaMemsetAsync(b.st, 0, sizeof(DevState), s) != cudaSuccess) return GRIM_ECUDA;
   if (emhd) exact::emhd_prepass(c, prim, nullptr, b.uT, s);
-  for (int d = 0; d < c.dim; d++) exact::face_flux(c, d, prim, nullptr, nullptr, b.flux[d], 0, s);
+  for (int d = 0; d < c.dim; d++) exact::face_flux(c, d, prim, nullptr, nullptr, b.flux[d], 0, nullptr, nullptr, s);
   exact::stage_epilogue(c, GRIM_HALF_STEP, b, s);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

@@ -11,6 +11,8 @@
 //                  consOld, Newton guess) -> Newton -> prim copied to primHalf
 //   full stage: the same on primHalf -> prim copied to primOld -> ghost fill
 //               -> time += dt -> [dt speeds of primOld for the next step]
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -58,6 +60,7 @@ struct grim_handle {
   double *primOld = nullptr, *prim = nullptr, *primHalf = nullptr;
   // stage buffers
   double *consOld = nullptr, *divF = nullptr, *Sexp = nullptr, *R = nullptr, *l2 = nullptr, *uT = nullptr;
+  double* emf = nullptr;  // 3 x Z stage corner EMFs
   double* flux[3] = {nullptr, nullptr, nullptr};
   int* list[2] = {nullptr, nullptr};  // compacted Newton worklists
   double* scratch = nullptr;  // test entry points: dof x Z inputs
@@ -76,6 +79,10 @@ struct grim_handle {
   int lastStage = GRIM_HALF_STEP;
   // per-kernel-group device timing (grim_profile_steps): event pairs
   // recorded around each launch on the handle's stream
+  // TMA descriptors of the arrays the X1 face kernel reads (primOld,
+  // primHalf, scratch) as (i, j, k, var); valid when haveTmap
+  bool haveTmap = false;
+  CUtensorMap tmap[3];
   // face-kernel launch variants per direction, [exact unit, fast unit]
   int faceVariant[2][3] = {{0, 0, 0}, {0, 0, 0}};
   // dt held at its current value instead of computeDt (the adjoint's runs)
@@ -119,7 +126,7 @@ struct ProfScope {
 
 static void free_all(grim_handle* h) {
   double** bufs[] = {&h->primOld, &h->prim, &h->primHalf, &h->consOld, &h->divF, &h->Sexp, &h->R,
-                     &h->l2, &h->uT, &h->flux[0], &h->flux[1], &h->flux[2], &h->scratch, &h->scratch2,
+                     &h->l2, &h->uT, &h->emf, &h->flux[0], &h->flux[1], &h->flux[2], &h->scratch, &h->scratch2,
                      &h->geo[0], &h->geo[1], &h->geo[2], &h->geo[3], &h->geo[4], &h->gamma};
   for (double** b : bufs)
     if (*b) { cudaFree(*b); *b = nullptr; }
@@ -190,6 +197,39 @@ static int make_devcfg(const grim_config& c, DevCfg& d) {
 
 static bool use_exact(const grim_handle* h) { return h->cfg.newtonMode == GRIM_NEWTON_PARITY_FD64; }
 
+// the tensor map of a prim array of this handle, or null
+static const CUtensorMap* tmap_for(const grim_handle* h, const double* p) {
+  if (!h->haveTmap) return nullptr;
+  if (p == h->primOld) return &h->tmap[0];
+  if (p == h->primHalf) return &h->tmap[1];
+  if (p == h->scratch) return &h->tmap[2];
+  return nullptr;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no
+// link-time dependency on the driver library)
+static bool encode_prim_tmap(const DevCfg& c, double* base, CUtensorMap* out) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return false;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  // rows of N1T doubles must be 16-byte strided; the 40-zone box must fit
+  if (c.N1T % 2 != 0 || c.N1T < 40 || c.dof > 256) return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)c.N1T, (cuuint64_t)c.N2T, (cuuint64_t)c.N3T, (cuuint64_t)c.dof};
+  const cuuint64_t strides[3] = {(cuuint64_t)c.N1T * 8, (cuuint64_t)c.N1T * c.N2T * 8, (cuuint64_t)c.Z * 8};
+  const cuuint32_t box[4] = {40, 1, 1, (cuuint32_t)c.dof};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUresult r = encode(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 static StageBufs stage_bufs(grim_handle* h, int stage) {
   StageBufs b;
   memset(&b, 0, sizeof(b));
@@ -210,6 +250,7 @@ static StageBufs stage_bufs(grim_handle* h, int stage) {
   b.R = h->R;
   b.l2 = h->l2;
   b.st = h->st;
+  b.emf = h->emf;
   b.list[0] = h->list[0];
   b.list[1] = h->list[1];
   return b;
@@ -243,12 +284,13 @@ static void enqueue_stencil(grim_handle* h, int stage) {
   }
   for (int d = 0; d < c.dim; d++) {
     PROF(GRIM_PROF_FACES_X1 + d);
-    KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], h->faceVariant[use_exact(h) ? 0 : 1][d], s);
+    KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], h->faceVariant[use_exact(h) ? 0 : 1][d],
+             tmap_for(h, b.ps), h->st, s);
     g_launch_counter++;
   }
   PROF(GRIM_PROF_EPILOGUE);
   KNS_CALL(h, stage_epilogue, c, stage, b, s);
-  g_launch_counter++;
+  g_launch_counter += (c.dim >= 2) ? 2 : 1;
 }
 
 static void enqueue_newton(grim_handle* h, int stage) {
@@ -434,6 +476,7 @@ int grim_create(const grim_config* cfg, int device, grim_handle** out) {
             alloc(&h->consOld, c.dof) && alloc(&h->divF, c.dof) && alloc(&h->Sexp, c.nf) && alloc(&h->R, c.nf) &&
             alloc(&h->l2, 2) && alloc(&h->scratch, c.dof) && alloc(&h->scratch2, (size_t)c.dof * 3);
   for (int d = 0; ok && d < c.dim; d++) ok = alloc(&h->flux[d], c.dof);
+  if (ok && c.dim >= 2) ok = alloc(&h->emf, 3);
   if (ok && (c.conduction || c.viscosity)) ok = alloc(&h->uT, 5);
   if (ok && cfg->metric != GRIM_MINKOWSKI) {
     // one (i, j) plane per word (the metric does not depend on X3)
@@ -456,6 +499,8 @@ int grim_create(const grim_config* cfg, int device, grim_handle** out) {
     set_err("stream creation failed"); free_all(h); delete h; return GRIM_ECUDA;
   }
   for (int i = 0; i < 8; i++) cudaEventCreate(&h->ev[i]);
+  h->haveTmap = encode_prim_tmap(c, h->primOld, &h->tmap[0]) && encode_prim_tmap(c, h->primHalf, &h->tmap[1]) &&
+                encode_prim_tmap(c, h->scratch, &h->tmap[2]);
   // geometry (geometry.cpp ctor at LEFT/RIGHT/BOTTOM/TOP/CENTER, timestepper.cpp:236-283)
   if (cfg->metric != GRIM_MINKOWSKI) {
     for (int l = 0; l < 5; l++)
@@ -646,7 +691,7 @@ int grim_compute_div_fluxes(grim_handle* h, const double* prim, double* divF, do
   if (c.conduction || c.viscosity) KNS_CALL(h, emhd_prepass, c, b.ps, b.geoC, h->uT, h->stream);
   for (int d = 0; d < c.dim; d++)
     KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], h->faceVariant[use_exact(h) ? 0 : 1][d],
-             h->stream);
+             tmap_for(h, b.ps), h->st, h->stream);
   // divergence of all dof rows: epilogue writes nf rows into divF and the
   // induction into the guess; the B rows of the divergence are recovered
   // from the guess: B_new = (consOld_B - 0.5 dt divF_B)/g with dt kept
@@ -1004,10 +1049,12 @@ int grim_autotune(grim_handle* h, int* variants, double* msBest) {
     double best = 1e30;
     int bestV = 0;
     for (int v = 0; v < nv; v++) {
-      KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], v, h->stream);  // warm-up
+      KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], v, tmap_for(h, b.ps), h->st,
+               h->stream);  // warm-up
       CK(cudaEventRecord(e0, h->stream));
       const int reps = 3;
-      for (int r = 0; r < reps; r++) KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], v, h->stream);
+      for (int r = 0; r < reps; r++)
+        KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], v, tmap_for(h, b.ps), h->st, h->stream);
       CK(cudaEventRecord(e1, h->stream));
       CK(cudaEventSynchronize(e1));
       float ms = 0.f;

@@ -18,6 +18,7 @@ struct DevState {
   unsigned long long nanFlag;
   unsigned long long itHist[2][16];  // zones by Newton iterations used (fast path)
   unsigned long long listCount[2];   // compacted worklists: entries per ping-pong list
+  unsigned long long waitTimeouts;   // bounded waits on asynchronous copies that gave up
 };
 
 struct StageBufs {
@@ -34,6 +35,7 @@ struct StageBufs {
   double* Sexp;           // nf x Z
   double* R;              // nf x Z  (Newton scratch)
   double* l2;             // 2 x Z   (l2, l2first)
+  double* emf;            // 3 x Z   corner EMFs of the stage (X1, X2, X3), dim >= 2
   DevState* st;
   int* list[2];           // compacted Newton worklists (interior zone indices)
 };
