@@ -42,19 +42,23 @@ struct DevCfg {
 GRIM_HD long long zidx(const DevCfg& c, int i, int j, int k) {
   return (long long)i + (long long)c.N1T * ((long long)j + (long long)c.N2T * k);
 }
+// Index decompositions in 32-bit unsigned arithmetic (grids are limited to
+// fewer than 2^31 zones at creation): a fraction of the instructions of
+// 64-bit division.
 GRIM_HD void zijk(const DevCfg& c, long long z, int& i, int& j, int& k) {
-  i = (int)(z % c.N1T);
-  long long r = z / c.N1T;
-  j = (int)(r % c.N2T);
-  k = (int)(r / c.N2T);
+  const unsigned zz = (unsigned)z, n1 = (unsigned)c.N1T, n2 = (unsigned)c.N2T;
+  const unsigned r = zz / n1;
+  i = (int)(zz - r * n1);
+  const unsigned q = r / n2;
+  j = (int)(r - q * n2);
+  k = (int)q;
 }
 // n-th interior zone -> full-grid index
 GRIM_HD long long interior_to_z(const DevCfg& c, long long n) {
-  int i = (int)(n % c.N1);
-  long long r = n / c.N1;
-  int j = (int)(r % c.N2);
-  int k = (int)(r / c.N2);
-  return zidx(c, i + c.g1, j + c.g2, k + c.g3);
+  const unsigned nn = (unsigned)n, n1 = (unsigned)c.N1, n2 = (unsigned)c.N2;
+  const unsigned r = nn / n1;
+  const unsigned q = r / n2;
+  return zidx(c, (int)(nn - r * n1) + c.g1, (int)(r - q * n2) + c.g2, (int)q + c.g3);
 }
 // The metrics (Minkowski, modified Kerr-Schild with derefine / cylindrify)
 // do not depend on X3, so the geometry is stored for one (i, j) plane.

@@ -249,10 +249,10 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1(DevCfg c, const doub
   const int wpr = (nfaces + 30) / 31;
   const long long rows = (long long)c.N2T * c.N3T;
   if (wg >= rows * wpr) return;  // whole warps exit together
-  const long long row = wg / wpr;
-  const int i0 = 3 + (int)(wg % wpr) * 31;
+  const unsigned wgu = (unsigned)wg, row = wgu / (unsigned)wpr;
+  const int i0 = 3 + (int)(wgu - row * (unsigned)wpr) * 31;
   const int iz = i0 - 1 + lane;
-  const int j = (int)(row % c.N2T), k = (int)(row / c.N2T);
+  const int k = (int)(row / (unsigned)c.N2T), j = (int)(row - (unsigned)k * (unsigned)c.N2T);
   const bool reconOK = iz >= 2 && iz <= c.N1T - 3;
   double lo[DOF], ro[DOF];
   const long long z = zidx(c, reconOK ? iz : 2, j, k);
@@ -333,10 +333,15 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1_tma(const __grid_con
     mbar_fence_init();
   }
   __syncwarp();
+  auto decompose = [&](long long it, int& i0, int& j, int& k) {
+    const unsigned itu = (unsigned)it, row = itu / (unsigned)wpr;
+    i0 = 3 + (int)(itu - row * (unsigned)wpr) * 31;
+    k = (int)(row / (unsigned)c.N2T);
+    j = (int)(row - (unsigned)k * (unsigned)c.N2T);
+  };
   auto issue = [&](long long it, int buf) {
-    const long long row = it / wpr;
-    const int i0 = 3 + (int)(it % wpr) * 31;
-    const int j = (int)(row % c.N2T), k = (int)(row / c.N2T);
+    int i0, j, k;
+    decompose(it, i0, j, k);
     mbar_expect_tx(&bars[buf], ROW * (unsigned)sizeof(double));
     tma_load_4d(rows + buf * ROW, &tmap, &bars[buf], (i0 - 3) & ~1, j, k, 0);
   };
@@ -358,9 +363,8 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1_tma(const __grid_con
       __syncwarp();
       return;
     }
-    const long long row = item / wpr;
-    const int i0 = 3 + (int)(item % wpr) * 31;
-    const int j = (int)(row % c.N2T), k = (int)(row / c.N2T);
+    int i0, j, k;
+    decompose(item, i0, j, k);
     const int x0 = (i0 - 3) & ~1;
     const int iz = i0 - 1 + lane;
     const bool reconOK = iz >= 2 && iz <= c.N1T - 3;
@@ -410,10 +414,11 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_strip(DevCfg c, int dir
   const int nch = (NT - 5 + FPW - 1) / FPW;  // faces 3 .. NT-3
   const long long nother = (dir == 1) ? c.N3T : c.N2T;
   if (wg >= (long long)nq * nch * nother) return;  // whole warps exit together
-  const int iq = (int)(wg % nq);
-  const long long r = wg / nq;
-  const int ch = (int)(r % nch);
-  const int other = (int)(r / nch);  // k for X2 faces, j for X3 faces
+  const unsigned wgu = (unsigned)wg, r = wgu / (unsigned)nq;
+  const int iq = (int)(wgu - r * (unsigned)nq);
+  const unsigned oth = r / (unsigned)nch;
+  const int ch = (int)(r - oth * (unsigned)nch);
+  const int other = (int)oth;  // k for X2 faces, j for X3 faces
   const int i = iq * QI + (lane % QI);
   const int x = 2 + ch * FPW + lane / QI;  // zone along dir; face x sits at its left
   const bool reconOK = i < c.N1T && x <= NT - 3;
@@ -859,12 +864,25 @@ GRIM_D void gauss_solve(T A[N][N], T b[N], T x[N]) {
       }
     }
     const T akk = A[kk][kk];
+    if constexpr (kFastMath) {
+      // one reciprocal per pivot, kept for the back substitution
+      const T ia = T(1) / akk;
+      A[kk][kk] = ia;
 #pragma unroll
-    for (int r = kk + 1; r < N; r++) {
-      T l = A[r][kk] / akk;
+      for (int r = kk + 1; r < N; r++) {
+        T l = A[r][kk] * ia;
 #pragma unroll
-      for (int cc = kk + 1; cc < N; cc++) A[r][cc] -= l * A[kk][cc];
-      b[r] -= l * b[kk];
+        for (int cc = kk + 1; cc < N; cc++) A[r][cc] -= l * A[kk][cc];
+        b[r] -= l * b[kk];
+      }
+    } else {
+#pragma unroll
+      for (int r = kk + 1; r < N; r++) {
+        T l = A[r][kk] / akk;
+#pragma unroll
+        for (int cc = kk + 1; cc < N; cc++) A[r][cc] -= l * A[kk][cc];
+        b[r] -= l * b[kk];
+      }
     }
   }
 #pragma unroll
@@ -872,7 +890,10 @@ GRIM_D void gauss_solve(T A[N][N], T b[N], T x[N]) {
     T s = b[r];
 #pragma unroll
     for (int cc = r + 1; cc < N; cc++) s -= A[r][cc] * x[cc];
-    x[r] = s / A[r][r];
+    if constexpr (kFastMath)
+      x[r] = s * A[r][r];  // the stored reciprocal
+    else
+      x[r] = s / A[r][r];
   }
 }
 

@@ -242,7 +242,13 @@ GRIM_D void char_speeds(const ElemT<S, R>& e, const ZoneGeo<R>& G, int dir, cons
                         S& maxSpeed) {
   const S Gam = S(c.Gam);
   S cAlvenSqr = e.bSqr / (e.rho + Gam * e.u + e.bSqr);
+#ifdef GRIM_FAST_MATH
+  // c_s^2 itself: without conduction or viscosity the element's c_s (a
+  // square root) is then dead code
+  S csSqr = (COND || VISC) ? e.soundSpeed * e.soundSpeed : Gam * e.pressure / (e.rho + Gam * e.u);
+#else
   S csSqr = e.soundSpeed * e.soundSpeed;
+#endif
   S cVisSqr = S(0.);
   if (VISC) cVisSqr = S(4.) / S(3.) / (e.rho + Gam * e.u) * e.rho * e.nu / e.tau;
   S cConSqr = S(0.);

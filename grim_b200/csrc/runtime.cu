@@ -162,6 +162,7 @@ static int make_devcfg(const grim_config& c, DevCfg& d) {
   d.Z = (long long)d.N1T * d.N2T * d.N3T;
   d.Zint = (long long)d.N1 * d.N2 * d.N3;
   d.GZ = (long long)d.N1T * d.N2T;
+  if (d.Z >= (1LL << 31)) return GRIM_EINVAL;  // 32-bit zone indices in the kernels
   d.conduction = c.conduction ? 1 : 0; d.viscosity = c.viscosity ? 1 : 0;
   d.nf = 5 + d.conduction + d.viscosity; d.dof = d.nf + 3;
   d.Q = 5; d.DP = 5 + d.conduction; d.B1 = d.nf;
