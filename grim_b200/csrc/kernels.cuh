@@ -236,10 +236,52 @@ GRIM_D void riemann_face(const DevCfg& c, int dir, const double* pl, const ZoneG
   }
 }
 
+// The same face flux with both states' elements evaluated side by side
+// (no shared-memory parking): twice the independent arithmetic per thread
+// for more registers, which the autotuner weighs against occupancy.
+template <int COND, int VISC>
+GRIM_D void riemann_face_pair(const DevCfg& c, int dir, const double* pl, const double* pr,
+                              const ZoneGeo<double>& G, double* __restrict__ flux, long long z) {
+  constexpr int NF = 5 + COND + VISC;
+  constexpr int DOF = NF + 3;
+  const long long Z = c.Z;
+  const int fd = dir + 1;
+  double F[2][DOF], U[2][DOF], mn[2], mx[2];
+  ElemT<double, double> e[2];
+#pragma unroll
+  for (int sd = 0; sd < 2; sd++) {
+    const double* q = sd ? pr : pl;
+    elem_set<COND, VISC>(e[sd], q[0], q[1], q[2], q[3], q[4], q[NF], q[NF + 1], q[NF + 2], COND ? q[5] : 0.,
+                         VISC ? q[5 + COND] : 0., G, c);
+  }
+#pragma unroll
+  for (int sd = 0; sd < 2; sd++) {
+    fluxes_fluid<COND, VISC>(e[sd], fd, G.g, F[sd], 5, 5 + COND);
+    fluxes_B(e[sd], fd, G.g, F[sd] + NF);
+    fluxes_fluid<COND, VISC>(e[sd], 0, G.g, U[sd], 5, 5 + COND);
+    fluxes_B(e[sd], 0, G.g, U[sd] + NF);
+    char_speeds<COND, VISC>(e[sd], G, dir, c, mn[sd], mx[sd]);
+  }
+  const double cmin = fmin(mn[0], mn[1]);
+  const double cmax = fmax(mx[0], mx[1]);
+  if (c.riemann == GRIM_HLL) {
+    const double id = 1. / (cmax - cmin);
+#pragma unroll
+    for (int v = 0; v < DOF; v++) {
+      const double num = cmax * F[0][v] - cmin * F[1][v] + cmin * cmax * (U[1][v] - U[0][v]);
+      flux[(long long)v * Z + z] = kFastMath ? num * id : num / (cmax - cmin);
+    }
+  } else {
+    const double cm = fmax(cmax, -cmin);
+#pragma unroll
+    for (int v = 0; v < DOF; v++) flux[(long long)v * Z + z] = 0.5 * (F[0][v] + F[1][v] - cm * (U[1][v] - U[0][v]));
+  }
+}
+
 // X1 faces: warp w of a row covers faces i0 .. i0+30; lane l reconstructs
 // zone i0 - 1 + l and, for l >= 1, computes the face between zones
 // i0 - 2 + l and i0 - 1 + l with the left state shuffled from lane l - 1.
-template <int COND, int VISC, int MINB>
+template <int COND, int VISC, int MINB, bool PAIR = false>
 __global__ void __launch_bounds__(128, MINB) k_face_flux_x1(DevCfg c, const double* __restrict__ ps,
                                                       const double* __restrict__ geoF, double* __restrict__ flux) {
   constexpr int DOF = 8 + COND + VISC;
@@ -263,10 +305,14 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1(DevCfg c, const doub
   if (lane == 0 || iz > c.N1T - 3) return;
   ZoneGeo<double> G;
   load_geo(G, c, geoF, z, iz, j, 0., 0.5);
-  extern __shared__ double park_x1[];
+  if constexpr (PAIR) {
+    riemann_face_pair<COND, VISC>(c, 0, pl, lo, G, flux, z);
+  } else {
+    extern __shared__ double park_x1[];
 #pragma unroll
-  for (int v = 0; v < DOF; v++) park_x1[(2 * DOF + v) * blockDim.x + threadIdx.x] = lo[v];
-  riemann_face<COND, VISC>(c, 0, pl, G, flux, z, park_x1);
+    for (int v = 0; v < DOF; v++) park_x1[(2 * DOF + v) * blockDim.x + threadIdx.x] = lo[v];
+    riemann_face<COND, VISC>(c, 0, pl, G, flux, z, park_x1);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -400,7 +446,7 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1_tma(const __grid_con
 // state moves QI lanes up by shuffle, giving (32/QI - 1) x QI faces per
 // warp.  With QI = 4 each warp-wide load still covers whole 32-byte
 // sectors (4 consecutive doubles along i), as in the X1 kernel.
-template <int COND, int VISC, int QI, int MINB>
+template <int COND, int VISC, int QI, int MINB, bool PAIR = false>
 __global__ void __launch_bounds__(128, MINB) k_face_flux_strip(DevCfg c, int dir, const double* __restrict__ ps,
                                                          const double* __restrict__ geoF,
                                                          const double* __restrict__ geoC, double* __restrict__ flux) {
@@ -439,10 +485,14 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_strip(DevCfg c, int dir
     load_geo(G, c, geoC, z, i, other, 0.5, 0.5);
   else
     load_geo(G, c, geoF, z, i, x, 0.5, 0.);
-  extern __shared__ double park_strip[];
+  if constexpr (PAIR) {
+    riemann_face_pair<COND, VISC>(c, dir, pl, lo, G, flux, z);
+  } else {
+    extern __shared__ double park_strip[];
 #pragma unroll
-  for (int v = 0; v < DOF; v++) park_strip[(2 * DOF + v) * blockDim.x + threadIdx.x] = lo[v];
-  riemann_face<COND, VISC>(c, dir, pl, G, flux, z, park_strip);
+    for (int v = 0; v < DOF; v++) park_strip[(2 * DOF + v) * blockDim.x + threadIdx.x] = lo[v];
+    riemann_face<COND, VISC>(c, dir, pl, G, flux, z, park_strip);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1558,20 +1608,20 @@ void emhd_prepass(const DevCfg& c, const double* ps, const double* geoC, double*
 // autotuner (grim_autotune): X1 faces by the register budget (3 or 4
 // resident 128-thread blocks per SM), X2 / X3 faces by that budget and by
 // the lane split QI (i per warp).  EMHD has one shape (2 resident blocks).
-template <int C, int V, int MINB>
+template <int C, int V, int MINB, bool PAIR = false>
 static void face_x1_launch(const DevCfg& c, const double* ps, const double* geoF, double* flux, cudaStream_t s) {
   const long long warps = (long long)c.N2T * c.N3T * ((c.N1T - 5 + 30) / 31);
-  const size_t park = 3 * (8 + C + V) * 128 * sizeof(double);
-  k_face_flux_x1<C, V, MINB><<<nblk(warps * 32, 128), 128, park, s>>>(c, ps, geoF, flux);
+  const size_t park = PAIR ? 0 : 3 * (8 + C + V) * 128 * sizeof(double);
+  k_face_flux_x1<C, V, MINB, PAIR><<<nblk(warps * 32, 128), 128, park, s>>>(c, ps, geoF, flux);
 }
-template <int C, int V, int QI, int MINB>
+template <int C, int V, int QI, int MINB, bool PAIR = false>
 static void face_strip_launch(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,
                               double* flux, cudaStream_t s) {
   const int NT = (dir == 1) ? c.N2T : c.N3T;
   const long long other = (dir == 1) ? c.N3T : c.N2T;
   const long long warps = (long long)((c.N1T + QI - 1) / QI) * ((NT - 5 + 32 / QI - 2) / (32 / QI - 1)) * other;
-  const size_t park = 3 * (8 + C + V) * 128 * sizeof(double);
-  k_face_flux_strip<C, V, QI, MINB><<<nblk(warps * 32, 128), 128, park, s>>>(c, dir, ps, geoF, geoC, flux);
+  const size_t park = PAIR ? 0 : 3 * (8 + C + V) * 128 * sizeof(double);
+  k_face_flux_strip<C, V, QI, MINB, PAIR><<<nblk(warps * 32, 128), 128, park, s>>>(c, dir, ps, geoF, geoC, flux);
 }
 static int sm_count() {
   static int n = 0;
@@ -1604,6 +1654,8 @@ static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double
       if (variant >= 2 && tmap && st) {
         if (variant == 3) face_x1_tma_launch<C, V, 4>(c, tmap, geoF, flux, st, s);
         else face_x1_tma_launch<C, V, 3>(c, tmap, geoF, flux, st, s);
+      } else if (variant == 4) {
+        face_x1_launch<C, V, 3, true>(c, ps, geoF, flux, s);
       } else if (variant == 1 || variant == 3) {
         face_x1_launch<C, V, 4>(c, ps, geoF, flux, s);
       } else {
@@ -1617,6 +1669,8 @@ static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double
       case 3: face_strip_launch<C, V, 2, 4>(c, dir, ps, geoF, geoC, flux, s); break;
       case 4: face_strip_launch<C, V, 8, 3>(c, dir, ps, geoF, geoC, flux, s); break;
       case 5: face_strip_launch<C, V, 8, 4>(c, dir, ps, geoF, geoC, flux, s); break;
+      case 6: face_strip_launch<C, V, 8, 3, true>(c, dir, ps, geoF, geoC, flux, s); break;
+      case 7: face_strip_launch<C, V, 4, 3, true>(c, dir, ps, geoF, geoC, flux, s); break;
       default: face_strip_launch<C, V, 4, 3>(c, dir, ps, geoF, geoC, flux, s); break;
     }
   } else {
@@ -1632,10 +1686,12 @@ void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, c
   GRIM_EMHD_DISPATCH(c, face_flux_t, c, dir, ps, geoF, geoC, flux, variant, tmap, st, s);
 }
 // X1: 0, 1 = register budget 3 / 4 blocks; 2, 3 = the same with TMA-staged
-// rows (when the caller has a tensor map of the primitives)
+// rows (when the caller has a tensor map of the primitives); 4 = both face
+// states evaluated side by side.  X2 / X3: 0-5 = lane split x register
+// budget; 6, 7 = side by side with 8 / 4 i per warp.
 int face_variants(const DevCfg& c, int dir) {
   if (c.conduction || c.viscosity) return 1;
-  return dir == 0 ? 4 : 6;
+  return dir == 0 ? 5 : 8;
 }
 #endif  // !GRIM_SKIP_FACES
 

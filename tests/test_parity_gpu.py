@@ -357,7 +357,7 @@ def test_autotuned_face_kernels_give_identical_results(mode):
         ts.primOld.setVars(P)
     tuned = a.autotune()
     assert set(tuned) == {0, 1}
-    assert 0 <= tuned[0][0] < 4 and 0 <= tuned[1][0] < 6 and all(ms > 0 for _, ms in tuned.values())
+    assert 0 <= tuned[0][0] < 5 and 0 <= tuned[1][0] < 8 and all(ms > 0 for _, ms in tuned.values())
     for _ in range(3):
         a.timeStep()
         b.timeStep()
@@ -365,14 +365,14 @@ def test_autotuned_face_kernels_give_identical_results(mode):
     # every variant of every direction, forced one at a time, gives the
     # default's divergence of fluxes
     ref_div, ref_flux = b.computeDivOfFluxes(P)
-    for d, nv in ((0, 4), (1, 6)):  # X1 variants 2, 3 stage rows with TMA
+    for d, nv in ((0, 5), (1, 8)):  # X1 variants 2, 3 stage rows with TMA
         for v in range(nv):
             a.setFaceVariant(d, v)
             div, flux = a.computeDivOfFluxes(P)
             assert np.array_equal(div, ref_div) and np.array_equal(flux, ref_flux), (d, v)
         a.setFaceVariant(d, 0)
     with pytest.raises(Exception):
-        a.setFaceVariant(1, 6)
+        a.setFaceVariant(1, 8)
 
 
 def test_divb_matches_oracle_and_stays_at_roundoff():
