@@ -563,7 +563,11 @@ static __global__ void k_stage_emf(DevCfg c, StageBufs b) {
   }
 }
 
-template <int COND, int VISC>
+// PART 0 does all of the epilogue; the split launches PART 1 (centre: the
+// stage element, consOld on the half stage, explicit sources) and then
+// PART 2 (fluxes: CT, divergence, induction, Newton guess), each with the
+// registers of its own half (the flux half is a memory stream).
+template <int COND, int VISC, int PART>
 __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, StageBufs b) {
   constexpr int NF = 5 + COND + VISC;
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -577,9 +581,11 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
   f.F[0] = b.flux[0]; f.F[1] = b.flux[1]; f.F[2] = b.flux[2]; f.Z = Z; f.B1 = c.B1;
   const double dt = b.st->dt;
 
+  constexpr int DOF = NF + 3;
+  double div[DOF];
+  if constexpr (PART != 1) {
   // ---- fluxes on the zone's six faces: Riemann fluxes for the fluid rows,
   // flux-CT values for the field rows (constrainedtransport.cpp:3-51)
-  constexpr int DOF = NF + 3;
   double Fl[3][DOF], Fr[3][DOF];
   const long long sd[3] = {s1, s2, s3};
   for (int d = 0; d < 3; d++)
@@ -630,7 +636,6 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
   }
   // ---- divergence (fvmfluxes.cpp): zero-padded convolution in 1D/2D,
   // shifted difference in 3D
-  double div[DOF];
   const double i1 = 1. / c.dX[0], i2 = 1. / c.dX[1];
   for (int v = 0; v < DOF; v++) {
     if (c.dim <= 2) {
@@ -642,9 +647,11 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
     }
   }
 
-  // ---- stage element at the centre (elemOld / elemHalfStep)
+  }  // PART != 1
   ZoneGeo<double> G;
   load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
+  if constexpr (PART != 2) {
+  // ---- stage element at the centre (elemOld / elemHalfStep)
   const double* ps = b.ps;
   ElemT<double, double> e;
   elem_set<COND, VISC>(e, ps[z], ps[Z + z], ps[2 * Z + z], ps[3 * Z + z], ps[4 * Z + z],
@@ -743,9 +750,11 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
     }
   }
   // ---- outputs: stage constants for the Newton kernels
-  for (int v = 0; v < NF + 3; v++) b.divF[(long long)v * Z + z] = div[v];
   if (needS)
     for (int v = 0; v < NF; v++) b.Sexp[(long long)v * Z + z] = S[v];
+  }  // PART != 2
+  if constexpr (PART != 1) {
+  for (int v = 0; v < NF + 3; v++) b.divF[(long long)v * Z + z] = div[v];
   // ---- induction and the Newton guess
   const double fac = (stage == GRIM_HALF_STEP) ? 0.5 * dt : dt;
   for (int b3 = 0; b3 < 3; b3++) {
@@ -754,6 +763,7 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
   }
   if (stage == GRIM_HALF_STEP)
     for (int v = 0; v < NF; v++) b.prim[(long long)v * Z + z] = b.pold[(long long)v * Z + z];
+  }  // PART != 1
 }
 
 // ---------------------------------------------------------------------------
@@ -1699,7 +1709,9 @@ int face_variants(const DevCfg& c, int dir) {
 template <int C, int V>
 static void stage_epilogue_t(const DevCfg& c, int stage, const StageBufs& b, cudaStream_t s) {
   if (c.dim >= 2) k_stage_emf<<<nblk(c.Z, 256), 256, 0, s>>>(c, b);
-  k_stage_epilogue<C, V><<<nblk(c.Zint, 128), 128, 0, s>>>(c, stage, b);
+  // centre half first: the flux half's induction reads its consOld
+  k_stage_epilogue<C, V, 1><<<nblk(c.Zint, 128), 128, 0, s>>>(c, stage, b);
+  k_stage_epilogue<C, V, 2><<<nblk(c.Zint, 128), 128, 0, s>>>(c, stage, b);
 }
 void stage_epilogue(const DevCfg& c, int stage, const StageBufs& b, cudaStream_t s) {
   GRIM_EMHD_DISPATCH(c, stage_epilogue_t, c, stage, b, s);
