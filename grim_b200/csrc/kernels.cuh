@@ -1709,9 +1709,14 @@ int face_variants(const DevCfg& c, int dir) {
 template <int C, int V>
 static void stage_epilogue_t(const DevCfg& c, int stage, const StageBufs& b, cudaStream_t s) {
   if (c.dim >= 2) k_stage_emf<<<nblk(c.Z, 256), 256, 0, s>>>(c, b);
-  // centre half first: the flux half's induction reads its consOld
-  k_stage_epilogue<C, V, 1><<<nblk(c.Zint, 128), 128, 0, s>>>(c, stage, b);
-  k_stage_epilogue<C, V, 2><<<nblk(c.Zint, 128), 128, 0, s>>>(c, stage, b);
+  if (c.metric != GRIM_MINKOWSKI || C || V) {
+    // centre half first: the flux half's induction reads its consOld
+    k_stage_epilogue<C, V, 1><<<nblk(c.Zint, 128), 128, 0, s>>>(c, stage, b);
+    k_stage_epilogue<C, V, 2><<<nblk(c.Zint, 128), 128, 0, s>>>(c, stage, b);
+  } else {
+    // no explicit sources: one kernel
+    k_stage_epilogue<C, V, 0><<<nblk(c.Zint, 128), 128, 0, s>>>(c, stage, b);
+  }
 }
 void stage_epilogue(const DevCfg& c, int stage, const StageBufs& b, cudaStream_t s) {
   GRIM_EMHD_DISPATCH(c, stage_epilogue_t, c, stage, b, s);

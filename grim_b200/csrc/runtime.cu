@@ -291,7 +291,7 @@ static void enqueue_stencil(grim_handle* h, int stage) {
   }
   PROF(GRIM_PROF_EPILOGUE);
   KNS_CALL(h, stage_epilogue, c, stage, b, s);
-  g_launch_counter += (c.dim >= 2) ? 3 : 2;
+  g_launch_counter += (c.dim >= 2 ? 1 : 0) + ((c.metric != GRIM_MINKOWSKI || c.conduction || c.viscosity) ? 2 : 1);
 }
 
 static void enqueue_newton(grim_handle* h, int stage) {
