@@ -1,7 +1,7 @@
 """Benchmark of the implicit GRMHD timestep: zone-cycles/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload torus|orszag_tang|fast_mode|emhd_stratified]
+                    [--workload torus|orszag_tang|fast_mode|emhd_stratified|batch]
 
 One JSON line on rank 0.  ``value`` is the zone-cycles/s of the product's
 fast Newton form (forward-tangent Jacobian, FP32 Jacobian/solve refined by
@@ -304,6 +304,120 @@ def _ncu_traffic(cfg):
     return table.get(key, {})
 
 
+def batch_problems(seed=5, count=16):
+    """The ragged batch: 2D ideal linear-mode problems on periodic unit
+    squares, N from 64 to 512 (seeded), wavevector 2 pi (k1, k2) with
+    k1, k2 in 1..4, amplitude 1e-4 in every primitive; minmod, LLF,
+    flux-CT, relative Newton tolerance 1e-10."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(rng.integers(4, 33)) * 16  # 64 .. 512
+        cfg = PR.fast_mode_config(N=n, nonlinearsolve_atol=ATOL, nonlinearsolve_rtol=RTOL, maxNonLinearIter=4)
+        X1, X2, _ = C.cell_centers(cfg)
+        k1, k2 = (int(x) for x in rng.integers(1, 5, 2))
+        base = [1.0, 2.0, 0.0, 0.0, 0.0, 0.1, 0.3, 0.0]
+        ph = rng.uniform(0, 2 * np.pi, 8)
+        P = np.stack([base[v] + 1e-4 * np.cos(2 * np.pi * (k1 * X1 + k2 * X2) + ph[v]) for v in range(8)])
+        out.append((cfg, P))
+    return out
+
+
+def run_batch(args, local_rank):
+    """The ragged-batch workload: value = all problems' zone-cycles/s stepped
+    as one batch (one graph per step, one compacted Newton launch per
+    iteration for all problems); beside it the same problems as separate
+    steppers (fast form and FD64 form) and the adjoint of the largest."""
+    import torch
+    from grim_b200.timestepper import Batch, timeStepper
+    torch.cuda.set_device(local_rank)
+    probs = batch_problems()
+    zones = sum(cfg["N1"] * cfg["N2"] for cfg, _ in probs)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def timed(run, sync, stream_ptr, steps):
+        stream = torch.cuda.ExternalStream(stream_ptr)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        torch.cuda.synchronize()
+        for a, b in evs:
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                a.record(stream)
+            run()
+            b.record(stream)
+        sync()
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in evs)
+
+    clocks = Clocks(local_rank)
+    B = Batch([cfg for cfg, _ in probs])
+    B.setNewtonMode(C.NEWTON_MIXED32, RTOL)
+    for (cfg, P), ts in zip(probs, B.problems):
+        ts.primOld.setVars(P)
+    B.enableGraph(True)
+    B.timeSteps(args.warmup)
+    B.synchronize()
+    clocks.start()
+    ms_b = timed(lambda: B.timeSteps(1), B.synchronize, B.stream(), args.steps)
+    clocks_info = clocks.stop()
+    unconv = sum(sum(ts.stats()["unconverged"]) for ts in B.problems)
+
+    def separate(mode):
+        sts = []
+        for cfg, P in probs:
+            ts = timeStepper(cfg)
+            ts.setNewtonMode(mode, 2, RTOL)
+            ts.primOld.setVars(P)
+            ts.enableGraph(True)
+            for _ in range(args.warmup):
+                ts.timeStep()
+            sts.append(ts)
+        for ts in sts:
+            ts.synchronize()
+        # steps issued problem after problem; each stepper has its own stream
+        ms = 0.0
+        for ts in sts:
+            ms += timed(ts.timeStep, ts.synchronize, ts.stream(), max(2, args.steps // 2)) / max(2, args.steps // 2)
+        return ms, sts
+
+    ms_sep, _ = separate(C.NEWTON_MIXED32)
+    ms_fd, _ = separate(C.NEWTON_PARITY_FD64)
+    # adjoint of the largest problem: 20 steps, checkpoints every 10
+    cfg, P = max(probs, key=lambda p: p[0]["N1"])
+    ts = timeStepper(cfg)
+    ts.setNewtonMode(C.NEWTON_TANGENT64, 1, 0.0)
+    ts.primOld.setVars(P)
+    ts.primOld.communicate()
+    ts.setFixedDt(True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ts.adjointForward(20, 10)
+    lam = ts.primOld.getVars() - np.array([1.0, 2.0, 0, 0, 0, 0.1, 0.3, 0])[:, None, None, None]
+    t1 = time.perf_counter()
+    ts.adjointBackward(lam)
+    t2 = time.perf_counter()
+    value = zones * args.steps / (ms_b / 1e3)
+    return {
+        "metric": METRIC, "value": value, "unit": "zone-cycles/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_b / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 residual / f32 Jacobian+solve",
+        "data": "synthetic (seeded linear modes)",
+        "config": {"workload": "batch", "description": "16 independent 2D ideal linear-mode problems, N = 64..512, "
+                   "minmod/LLF/flux-CT, one batch", "zones": zones,
+                   "sizes": [cfg["N1"] for cfg, _ in probs], "rel_residual_tol": RTOL,
+                   "l2": "flushed between timed steps (256 MB write, untimed)", "cuda_graph": True},
+        "unconverged": unconv,
+        "separate_fast": {"value": zones / (ms_sep / 1e3), "ms_per_step": ms_sep},
+        "fd64": {"value": zones / (ms_fd / 1e3), "ms_per_step": ms_fd},
+        "speedup_vs_fd64": value / (zones / (ms_fd / 1e3)),
+        "batch_vs_separate": value / (zones / (ms_sep / 1e3)),
+        "adjoint": {"problem": "%dx%d" % (cfg["N1"], cfg["N2"]), "steps": 20, "checkpoint_every": 10,
+                    "forward_s": t1 - t0, "backward_s": t2 - t1,
+                    "backward_zone_steps_per_s": cfg["N1"] * cfg["N2"] * 20 / (t2 - t1)},
+        "clocks": clocks_info,
+    }
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     torch.cuda.set_device(local_rank)
@@ -463,6 +577,16 @@ def main():
         import torch
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.workload == "batch":
+        out = run_batch(args, local_rank)
+        if rank == 0 and not args.no_cpu:
+            cfg, P = batch_problems()[0]
+            v, n, sample = cpu_reference(cfg, P, seconds=10.0)
+            out["cpu_baseline"] = {"value": v, "unit": "zone-cycles/s", "cores": n, "kind": "port",
+                                   "sample": sample}
+        if rank == 0:
+            print(json.dumps(out))
+        return
     out, cfg, P = run_gpu(args, rank, world, local_rank)
     if rank == 0 and not args.no_cpu:
         ccfg = cpu_sample_config(args.workload, cfg)

@@ -446,11 +446,12 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1_tma(const __grid_con
 // state moves QI lanes up by shuffle, giving (32/QI - 1) x QI faces per
 // warp.  With QI = 4 each warp-wide load still covers whole 32-byte
 // sectors (4 consecutive doubles along i), as in the X1 kernel.
-template <int COND, int VISC, int QI, int MINB, bool PAIR = false>
-__global__ void __launch_bounds__(128, MINB) k_face_flux_strip(DevCfg c, int dir, const double* __restrict__ ps,
+template <int COND, int VISC, int QI, int MINB, bool PAIR, int DIR>
+__global__ void __launch_bounds__(128, MINB) k_face_flux_strip(DevCfg c, const double* __restrict__ ps,
                                                          const double* __restrict__ geoF,
                                                          const double* __restrict__ geoC, double* __restrict__ flux) {
   constexpr int DOF = 8 + COND + VISC;
+  constexpr int dir = DIR;  // a compile-time direction keeps the element in registers
   constexpr int JR = 32 / QI;       // zones along dir per warp
   constexpr int FPW = JR - 1;       // faces along dir per warp
   const int lane = threadIdx.x & 31;
@@ -588,10 +589,17 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
   // flux-CT values for the field rows (constrainedtransport.cpp:3-51)
   double Fl[3][DOF], Fr[3][DOF];
   const long long sd[3] = {s1, s2, s3};
+#pragma unroll
   for (int d = 0; d < 3; d++)
+#pragma unroll
     for (int v = 0; v < DOF; v++) { Fl[d][v] = 0.; Fr[d][v] = 0.; }
-  for (int d = 0; d < c.dim; d++)
-    for (int v = 0; v < NF; v++) { Fl[d][v] = f.at(d, v, z); Fr[d][v] = f.at(d, v, z + sd[d]); }
+  // directions unrolled to their compile-time bound: constant indices keep
+  // Fl / Fr in registers
+#pragma unroll
+  for (int d = 0; d < 3; d++)
+    if (d < c.dim)
+#pragma unroll
+      for (int v = 0; v < NF; v++) { Fl[d][v] = f.at(d, v, z); Fr[d][v] = f.at(d, v, z + sd[d]); }
   if (c.dim == 1) {
     for (int b3 = 0; b3 < 3; b3++) { Fl[0][NF + b3] = f.at(0, c.B1 + b3, z); Fr[0][NF + b3] = f.at(0, c.B1 + b3, z + s1); }
   } else if (c.dim == 2) {
@@ -629,14 +637,17 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
     if (i == c.N1 + c.g1 - 1) Fr[0][RHO] = fmax(Fr[0][RHO], 0.);
     if (c.dim >= 2) {
       if (j == c.g2)
+#pragma unroll
         for (int v = 0; v < DOF; v++) Fl[1][v] = 0.;
       if (j == c.N2 + c.g2 - 1)
+#pragma unroll
         for (int v = 0; v < DOF; v++) Fr[1][v] = 0.;
     }
   }
   // ---- divergence (fvmfluxes.cpp): zero-padded convolution in 1D/2D,
   // shifted difference in 3D
   const double i1 = 1. / c.dX[0], i2 = 1. / c.dX[1];
+#pragma unroll
   for (int v = 0; v < DOF; v++) {
     if (c.dim <= 2) {
       double d = Fr[0][v] * i1 + Fl[0][v] * (-i1);
@@ -803,20 +814,25 @@ __global__ void k_dt_speeds(DevCfg c, const double* __restrict__ p, const double
       src = zidx(c, si, sj, sk);
     }
     const long long Z = c.Z;
-    double pv[12];
-    for (int v = 0; v < c.dof; v++) pv[v] = zero ? 0. : p[(long long)v * Z + src];
+    constexpr int NF = 5 + COND + VISC, DOF = NF + 3;
+    double pv[DOF];
+#pragma unroll
+    for (int v = 0; v < DOF; v++) pv[v] = zero ? 0. : p[(long long)v * Z + src];
     ZoneGeo<double> G;
     load_geo(G, c, geoC, z, i, j, 0.5, 0.5);
     ElemT<double, double> e;
-    elem_set<COND, VISC>(e, pv[0], pv[1], pv[2], pv[3], pv[4], pv[c.B1], pv[c.B1 + 1], pv[c.B1 + 2],
-                         COND ? pv[c.Q] : 0., VISC ? pv[c.DP] : 0., G, c);
+    elem_set<COND, VISC>(e, pv[0], pv[1], pv[2], pv[3], pv[4], pv[NF], pv[NF + 1], pv[NF + 2],
+                         COND ? pv[5] : 0., VISC ? pv[5 + COND] : 0., G, c);
     double acc = 0.;
-    for (int d = 0; d < c.dim; d++) {
-      double mn, mx;
-      char_speeds<COND, VISC>(e, G, d, c, mn, mx);
-      double a = mn / c.dX[d], bb = mx / c.dX[d];
-      double m2 = fmax(bb, fabs(a));
-      acc = (d == 0) ? m2 : acc + m2;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      if (d < c.dim) {
+        double mn, mx;
+        char_speeds<COND, VISC>(e, G, d, c, mn, mx);
+        double a = mn / c.dX[d], bb = mx / c.dX[d];
+        double m2 = fmax(bb, fabs(a));
+        acc = (d == 0) ? m2 : acc + m2;
+      }
     }
     best = acc;
   }
@@ -1631,7 +1647,10 @@ static void face_strip_launch(const DevCfg& c, int dir, const double* ps, const 
   const long long other = (dir == 1) ? c.N3T : c.N2T;
   const long long warps = (long long)((c.N1T + QI - 1) / QI) * ((NT - 5 + 32 / QI - 2) / (32 / QI - 1)) * other;
   const size_t park = PAIR ? 0 : 3 * (8 + C + V) * 128 * sizeof(double);
-  k_face_flux_strip<C, V, QI, MINB, PAIR><<<nblk(warps * 32, 128), 128, park, s>>>(c, dir, ps, geoF, geoC, flux);
+  if (dir == 1)
+    k_face_flux_strip<C, V, QI, MINB, PAIR, 1><<<nblk(warps * 32, 128), 128, park, s>>>(c, ps, geoF, geoC, flux);
+  else
+    k_face_flux_strip<C, V, QI, MINB, PAIR, 2><<<nblk(warps * 32, 128), 128, park, s>>>(c, ps, geoF, geoC, flux);
 }
 static int sm_count() {
   static int n = 0;
