@@ -250,7 +250,8 @@ int grim_count_flops(grim_handle* h, double* out);
  * variant of each direction on the state in primOld for the handle's
  * current Newton mode (its compilation unit) and keeps the fastest.
  * variants[d] and msBest[d] (may be null) receive the choice and its time
- * per launch.  Results do not depend on the variant. */
+ * per launch.  In the FP64 parity path (no FMA contraction) every variant
+ * gives the same bits; in the fast path they agree to roundoff. */
 int grim_autotune(grim_handle* h, int* variants, double* msBest);
 /* Forces one variant (for tests); GRIM_EINVAL when out of range. */
 int grim_set_face_variant(grim_handle* h, int dir, int variant);
