@@ -147,6 +147,7 @@ __global__ void k_emhd_prepass(DevCfg c, const double* __restrict__ ps, const do
                        ps[(long long)c.B1 * Z + z], ps[(long long)(c.B1 + 1) * Z + z],
                        ps[(long long)(c.B1 + 2) * Z + z], COND ? ps[(long long)c.Q * Z + z] : 0.,
                        VISC ? ps[(long long)c.DP * Z + z] : 0., G, c);
+#pragma unroll
   for (int m = 0; m < 4; m++) uT[(long long)m * Z + z] = e.uCov[m];
   uT[4 * Z + z] = e.temperature;
 }
@@ -601,6 +602,7 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
 #pragma unroll
       for (int v = 0; v < NF; v++) { Fl[d][v] = f.at(d, v, z); Fr[d][v] = f.at(d, v, z + sd[d]); }
   if (c.dim == 1) {
+#pragma unroll
     for (int b3 = 0; b3 < 3; b3++) { Fl[0][NF + b3] = f.at(0, c.B1 + b3, z); Fr[0][NF + b3] = f.at(0, c.B1 + b3, z + s1); }
   } else if (c.dim == 2) {
     const double* E3 = b.emf + 2 * Z;
@@ -673,16 +675,21 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
     double U[NF], UB[3];
     fluxes_fluid<COND, VISC>(e, 0, G.g, U, 5, 5 + COND);
     fluxes_B(e, 0, G.g, UB);
+#pragma unroll
     for (int v = 0; v < NF; v++) b.consOld[(long long)v * Z + z] = U[v];
+#pragma unroll
     for (int v = 0; v < 3; v++) b.consOld[(long long)(NF + v) * Z + z] = UB[v];
   }
   // ---- explicit sources
   double S[NF];
+#pragma unroll
   for (int v = 0; v < NF; v++) S[v] = 0.;
   const bool needS = (c.metric != GRIM_MINKOWSKI) || COND || VISC;
   if (c.metric != GRIM_MINKOWSKI) {
     double T[4][4];
+#pragma unroll
     for (int ka = 0; ka < 4; ka++)
+#pragma unroll
       for (int la = 0; la < 4; la++) T[ka][la] = tmunu<COND, VISC>(e, ka, la);
     const double* gam = b.gamma + gidx(c, i, j);
     if constexpr (kFastMath) {
@@ -699,11 +706,15 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
             acc[nu] -= T[ka][la] * gv;
             if (nu != ka) acc[ka] -= T[nu][la] * gv;
           }
+#pragma unroll
       for (int nu = 0; nu < 4; nu++) S[UU + nu] = acc[nu];
     } else {
+#pragma unroll
       for (int nu = 0; nu < 4; nu++) {
         double s = S[UU + nu];
+#pragma unroll
         for (int ka = 0; ka < 4; ka++)
+#pragma unroll
           for (int la = 0; la < 4; la++)
             s -= G.g * T[ka][la] * __ldg(gam + (long long)(la * 16 + ka * 4 + nu) * c.GZ);
         S[UU + nu] = s;
@@ -719,13 +730,16 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
       const double* a = uT + (long long)m * Z + z;
       return recon_slope(c.reconstruction, c.theta, a[-2 * sd], a[-sd], a[0], a[sd], a[2 * sd], dx);
     };
+#pragma unroll
     for (int mu = 0; mu < 4; mu++) {
       gu[0][mu] = 0.;
       gu[1][mu] = st(mu, 0, c.dX[0]);
       gu[2][mu] = (c.dim > 1) ? st(mu, 1, c.dX[1]) : 0.;
       gu[3][mu] = (c.dim > 2) ? st(mu, 2, c.dX[2]) : 0.;
       if (c.metric != GRIM_MINKOWSKI) {
+#pragma unroll
         for (int nu = 0; nu < 4; nu++)
+#pragma unroll
           for (int la = 0; la < 4; la++)
             gu[nu][mu] -= __ldg(b.gamma + (long long)(la * 16 + nu * 4 + mu) * c.GZ + gidx(c, i, j)) * e.uCov[la];
       }
@@ -737,11 +751,15 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
       gT[3] = (c.dim > 2) ? st(4, 2, c.dX[2]) : 0.;
     }
     double dv = 0.;
+#pragma unroll
     for (int mu = 0; mu < 4; mu++)
+#pragma unroll
       for (int nu = 0; nu < 4; nu++) dv += G.gcon[mu][nu] * gu[mu][nu];
     if (VISC) {
       double d0 = -dv * e.rho * e.nu;
+#pragma unroll
       for (int mu = 0; mu < 4; mu++)
+#pragma unroll
         for (int nu = 0; nu < 4; nu++) d0 += 3. * e.rho * e.nu * e.bCon[mu] * e.bCon[nu] / e.bSqr * gu[mu][nu];
       double d0t = (c.hoVisc == 1) ? d0 * sqrt(e.tau / e.rho / e.nu / e.temperature) : d0;
       double s = -G.g * (d0t) / e.tau;
@@ -750,8 +768,10 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
     }
     if (COND) {
       double qq = 0.;
+#pragma unroll
       for (int mu = 0; mu < 4; mu++) {
         qq -= e.rho * e.chi * e.bCon[mu] / e.bNorm * gT[mu];
+#pragma unroll
         for (int nu = 0; nu < 4; nu++) qq -= e.rho * e.chi * e.temperature * e.bCon[nu] / e.bNorm * e.uCon[mu] * gu[mu][nu];
       }
       double qt = (c.hoCond == 1) ? qq * sqrt(e.tau / e.rho / e.chi) / e.temperature : qq;
@@ -762,17 +782,21 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
   }
   // ---- outputs: stage constants for the Newton kernels
   if (needS)
+#pragma unroll
     for (int v = 0; v < NF; v++) b.Sexp[(long long)v * Z + z] = S[v];
   }  // PART != 2
   if constexpr (PART != 1) {
+#pragma unroll
   for (int v = 0; v < NF + 3; v++) b.divF[(long long)v * Z + z] = div[v];
   // ---- induction and the Newton guess
   const double fac = (stage == GRIM_HALF_STEP) ? 0.5 * dt : dt;
+#pragma unroll
   for (int b3 = 0; b3 < 3; b3++) {
     double cons = b.consOld[(long long)(NF + b3) * Z + z] - fac * div[NF + b3];
     b.prim[(long long)(c.B1 + b3) * Z + z] = cons / G.g;
   }
   if (stage == GRIM_HALF_STEP)
+#pragma unroll
     for (int v = 0; v < NF; v++) b.prim[(long long)v * Z + z] = b.pold[(long long)v * Z + z];
   }  // PART != 1
 }
@@ -872,11 +896,13 @@ GRIM_D void load_stage_const(StageConst<5 + COND + VISC>& K, const DevCfg& c, in
   constexpr int NF = 5 + COND + VISC;
   const long long Z = c.Z;
   const bool needS = (c.metric != GRIM_MINKOWSKI) || COND || VISC;
+#pragma unroll
   for (int v = 0; v < NF; v++) {
     K.Uold[v] = b.consOld[(long long)v * Z + z];
     K.divF[v] = b.divF[(long long)v * Z + z];
     K.Sexp[v] = needS ? b.Sexp[(long long)v * Z + z] : 0.;
   }
+#pragma unroll
   for (int v = 0; v < 3; v++) K.B[v] = b.prim[(long long)(c.B1 + v) * Z + z];
   const double dt = b.st->dt;
   K.dtp = (stage == GRIM_HALF_STEP) ? dt / 2. : dt;
@@ -890,6 +916,7 @@ GRIM_D void load_stage_const(StageConst<5 + COND + VISC>& K, const DevCfg& c, in
                          po[(long long)c.B1 * Z + z], po[(long long)(c.B1 + 1) * Z + z],
                          po[(long long)(c.B1 + 2) * Z + z], COND ? po[(long long)c.Q * Z + z] : 0.,
                          VISC ? po[(long long)c.DP * Z + z] : 0., G, c);
+#pragma unroll
     for (int m = 0; m < 4; m++) K.uCovOld[m] = eo.uCov[m];
     K.TOld = eo.temperature;
     ElemT<double, double> er;
@@ -904,6 +931,7 @@ GRIM_D void load_stage_const(StageConst<5 + COND + VISC>& K, const DevCfg& c, in
     }
     K.refRho = er.rho; K.refNu = VISC ? er.nu : 0.; K.refChi = COND ? er.chi : 0.;
     K.refTau = er.tau; K.refT = er.temperature;
+#pragma unroll
     for (int m = 0; m < 4; m++) K.refBCon[m] = er.bCon[m];
     K.refBSqr = er.bSqr; K.refBNorm = er.bNorm; K.refUCon0 = er.uCon[0];
     K.refQTilde = COND ? er.qTilde : 0.;
@@ -929,15 +957,21 @@ GRIM_D void gauss_solve(T A[N][N], T b[N], T x[N]) {
       T v = fabs(A[r][kk]);
       if (v > best) { best = v; p = r; }
     }
-    if (p != kk) {
+    // row exchange as selects over compile-time indices, so the matrix
+    // stays in registers (a conditional swap sends it to local memory);
+    // columns left of kk are not read again
 #pragma unroll
-      for (int r = kk + 1; r < N; r++) {
-        if (r == p) {
+    for (int r = kk + 1; r < N; r++) {
+      const bool sw = (r == p);
 #pragma unroll
-          for (int cc = 0; cc < N; cc++) { T t = A[kk][cc]; A[kk][cc] = A[r][cc]; A[r][cc] = t; }
-          T t = b[kk]; b[kk] = b[r]; b[r] = t;
-        }
+      for (int cc = kk; cc < N; cc++) {
+        const T a0 = A[kk][cc], a1 = A[r][cc];
+        A[kk][cc] = sw ? a1 : a0;
+        A[r][cc] = sw ? a0 : a1;
       }
+      const T b0 = b[kk], b1 = b[r];
+      b[kk] = sw ? b1 : b0;
+      b[r] = sw ? b0 : b1;
     }
     const T akk = A[kk][kk];
     if constexpr (kFastMath) {
@@ -1007,12 +1041,14 @@ __global__ void __launch_bounds__(128) k_newton_fd_init(DevCfg c, int stage, Sta
     StageConst<NF> K;
     load_stage_const<COND, VISC>(K, c, stage, b, z, G);
     double P[NF], R[NF];
+#pragma unroll
     for (int v = 0; v < NF; v++) P[v] = b.prim[(long long)v * Z + z];
     P[0] = fmax(P[0], c.rhoFloor);
     P[1] = fmax(P[1], c.uFloor);
     b.prim[z] = P[0];
     b.prim[Z + z] = P[1];
     zone_residual<COND, VISC, double, double>(P, K, G, c, R);
+#pragma unroll
     for (int v = 0; v < NF; v++) b.R[(long long)v * Z + z] = R[v];
     double l2 = l2sum<NF>(R);
     b.l2[z] = l2;
@@ -1044,6 +1080,7 @@ __global__ void __launch_bounds__(128) k_newton_fd_iter(DevCfg c, int stage, int
     StageConst<NF> K;
     load_stage_const<COND, VISC>(K, c, stage, b, z, G);
     double P[NF], R[NF];
+#pragma unroll
     for (int v = 0; v < NF; v++) {
       P[v] = b.prim[(long long)v * Z + z];
       R[v] = b.R[(long long)v * Z + z];
@@ -1095,11 +1132,13 @@ __global__ void __launch_bounds__(128) k_newton_fd_iter(DevCfg c, int stage, int
       P[1] = fmax(P[1], c.uFloor);
       if (!haveRt || floored) zone_residual<COND, VISC, double, double>(P, K, G, c, Rt);
       const double l2n = l2sum<NF>(Rt);
+#pragma unroll
       for (int v = 0; v < NF; v++) b.R[(long long)v * Z + z] = Rt[v];
       b.l2[z] = l2n;
       double tol = fmax(c.atol, c.rtol * c.rtol * l2first);
       unconv = (l2n > tol) ? 1 : 0;
     }
+#pragma unroll
     for (int v = 0; v < NF; v++) b.prim[(long long)v * Z + z] = P[v];
   }
   unconv = __syncthreads_count(unconv);
@@ -1151,6 +1190,7 @@ __global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : 3)
     StageConst<NF> K;
     load_stage_const<COND, VISC>(K, c, stage, b, z, G);
     double P[NF], R[NF];
+#pragma unroll
     for (int v = 0; v < NF; v++) P[v] = b.prim[(long long)v * Z + z];
     bool haveR = false;
     double l2first = 0.;
@@ -1209,6 +1249,7 @@ __global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : 3)
       if (!(l2 >= 0. && l2 <= fmax(c.atol, c.rtol * c.rtol * l2first))) unconv = 1;
     }
     itsMax = it;
+#pragma unroll
     for (int v = 0; v < NF; v++) b.prim[(long long)v * Z + z] = P[v];
   }
   hist_add(b.st->itHist[stage], min(itsMax, 15), n < nlist);
@@ -1254,6 +1295,7 @@ GRIM_D bool list_init_zone(const DevCfg& c, int stage, const StageBufs& b, long 
   StageConst<NF> K;
   load_stage_const<COND, VISC>(K, c, stage, b, z, G);
   double P[NF], R[NF];
+#pragma unroll
   for (int v = 0; v < NF; v++) P[v] = b.prim[(long long)v * Z + z];
   P[0] = fmax(P[0], c.rhoFloor);
   P[1] = fmax(P[1], c.uFloor);
@@ -1261,6 +1303,7 @@ GRIM_D bool list_init_zone(const DevCfg& c, int stage, const StageBufs& b, long 
   b.prim[Z + z] = P[1];
   zone_residual<COND, VISC, double, double>(P, K, G, c, R);
   const double l2 = l2sum<NF>(R);
+#pragma unroll
   for (int v = 0; v < NF; v++) b.R[(long long)v * Z + z] = R[v];
   b.l2[Z + z] = l2;
   return l2 > fmax(c.atol, c.rtol * c.rtol * l2);
@@ -1279,12 +1322,15 @@ GRIM_D bool list_iter_zone(const DevCfg& c, int stage, int it, const StageBufs& 
   ZoneGeo<double> G;
   load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
   ZoneGeo<T> Gt;
+#pragma unroll
   for (int m = 0; m < 4; m++)
+#pragma unroll
     for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = (T)G.gcov[m][q]; Gt.gcon[m][q] = (T)G.gcon[m][q]; }
   Gt.g = (T)G.g; Gt.alpha = (T)G.alpha; Gt.x1 = (T)G.x1; Gt.x2 = (T)G.x2; Gt.dyn = (T)G.dyn;
   StageConst<NF> K;
   load_stage_const<COND, VISC>(K, c, stage, b, z, G);
   double P[NF], R[NF];
+#pragma unroll
   for (int v = 0; v < NF; v++) {
     P[v] = b.prim[(long long)v * Z + z];
     R[v] = b.R[(long long)v * Z + z];
@@ -1294,9 +1340,11 @@ GRIM_D bool list_iter_zone(const DevCfg& c, int stage, int it, const StageBufs& 
   T J[NF][NF];
   tangent_jacobian<COND, VISC, T>(P, K, Gt, c, J);
   T bv[NF], xv[NF];
+#pragma unroll
   for (int v = 0; v < NF; v++) bv[v] = (T)(-R[v]);
   gauss_solve<T, NF>(J, bv, xv);
   double dPv[NF];
+#pragma unroll
   for (int v = 0; v < NF; v++) dPv[v] = (double)xv[v];
   const double f0 = 0.5 * l2, fPrime0 = -2. * f0;
   double lam = 1.;
@@ -1304,6 +1352,7 @@ GRIM_D bool list_iter_zone(const DevCfg& c, int stage, int it, const StageBufs& 
   double Rt[NF];
   for (int ls = 0; ls < c.maxLS; ls++) {
     double Pt[NF];
+#pragma unroll
     for (int v = 0; v < NF; v++) Pt[v] = P[v] + lam * dPv[v];
     zone_residual<COND, VISC, double, double>(Pt, K, G, c, Rt);
     const double f1 = 0.5 * l2sum<NF>(Rt);
@@ -1311,6 +1360,7 @@ GRIM_D bool list_iter_zone(const DevCfg& c, int stage, int it, const StageBufs& 
     const double denom = (f1 - f0 - fPrime0 * lam);
     lam = -fPrime0 * lam * lam / denom / 2.;
   }
+#pragma unroll
   for (int v = 0; v < NF; v++) P[v] = P[v] + lam * dPv[v];
   const bool floored = (P[0] < c.rhoFloor) || (P[1] < c.uFloor);
   if (!last) {
@@ -1321,6 +1371,7 @@ GRIM_D bool list_iter_zone(const DevCfg& c, int stage, int it, const StageBufs& 
   const double l2n = l2sum<NF>(Rt);
   const bool conv = l2n <= fmax(c.atol, c.rtol * c.rtol * l2first);
   if (!conv && last) atomicAdd(&b.st->finalUnconv[stage], 1ULL);
+#pragma unroll
   for (int v = 0; v < NF; v++) {
     b.prim[(long long)v * Z + z] = P[v];
     b.R[(long long)v * Z + z] = Rt[v];
@@ -1451,6 +1502,7 @@ __global__ void k_residual(DevCfg c, int stage, StageBufs b, const double* __res
   zijk(c, z, i, j, k);
   bool inner = i >= c.g1 && i < c.N1 + c.g1 && j >= c.g2 && j < c.N2 + c.g2 && k >= c.g3 && k < c.N3 + c.g3;
   if (!inner) {
+#pragma unroll
     for (int v = 0; v < NF; v++) out[(long long)v * Z + z] = 0.;
     return;
   }
@@ -1458,10 +1510,13 @@ __global__ void k_residual(DevCfg c, int stage, StageBufs b, const double* __res
   load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
   StageConst<NF> K;
   load_stage_const<COND, VISC>(K, c, stage, b, z, G);
+#pragma unroll
   for (int v = 0; v < 3; v++) K.B[v] = pg[(long long)(c.B1 + v) * Z + z];
   double P[NF], R[NF];
+#pragma unroll
   for (int v = 0; v < NF; v++) P[v] = pg[(long long)v * Z + z];
   zone_residual<COND, VISC, double, double>(P, K, G, c, R);
+#pragma unroll
   for (int v = 0; v < NF; v++) out[(long long)v * Z + z] = R[v];
 }
 
@@ -1476,33 +1531,42 @@ __global__ void k_jacobian(DevCfg c, int stage, StageBufs b, const double* __res
   zijk(c, z, i, j, k);
   bool inner = i >= c.g1 && i < c.N1 + c.g1 && j >= c.g2 && j < c.N2 + c.g2 && k >= c.g3 && k < c.N3 + c.g3;
   double J[NF][NF];
+#pragma unroll
   for (int a = 0; a < NF; a++)
+#pragma unroll
     for (int q = 0; q < NF; q++) J[a][q] = 0.;
   if (inner) {
     ZoneGeo<double> G;
     load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
     StageConst<NF> K;
     load_stage_const<COND, VISC>(K, c, stage, b, z, G);
+#pragma unroll
     for (int v = 0; v < 3; v++) K.B[v] = pg[(long long)(c.B1 + v) * Z + z];
     double P[NF], R[NF];
+#pragma unroll
     for (int v = 0; v < NF; v++) P[v] = pg[(long long)v * Z + z];
     if (tangent) {
       tangent_jacobian<COND, VISC, double>(P, K, G, c, J);
     } else {
       zone_residual<COND, VISC, double, double>(P, K, G, c, R);
       const double eps = c.jacEps;
+#pragma unroll
       for (int row = 0; row < NF; row++) {
         double Pe[NF];
+#pragma unroll
         for (int v = 0; v < NF; v++) Pe[v] = P[v];
         double small = (fabs(P[row]) < .5 * eps) ? 1. : 0.;
         Pe[row] = P[row] + eps * P[row] * (1. - small) + small * eps;
         double Rp[NF];
         zone_residual<COND, VISC, double, double>(Pe, K, G, c, Rp);
+#pragma unroll
         for (int col = 0; col < NF; col++) J[col][row] = (Rp[col] - R[col]) / (Pe[row] - P[row]);
       }
     }
   }
+#pragma unroll
   for (int a = 0; a < NF; a++)
+#pragma unroll
     for (int q = 0; q < NF; q++) jac[(z * NF + a) * NF + q] = J[a][q];
 }
 
@@ -1526,7 +1590,9 @@ __global__ void k_conserved(DevCfg c, const double* __restrict__ p, const double
     double U[NF], UB[3];
     fluxes_fluid<COND, VISC>(e, 0, G.g, U, 5, 5 + COND);
     fluxes_B(e, 0, G.g, UB);
+#pragma unroll
     for (int v = 0; v < NF; v++) out[(long long)v * Z + z] = U[v];
+#pragma unroll
     for (int v = 0; v < 3; v++) out[(long long)(NF + v) * Z + z] = UB[v];
   }
   if (mn) {
@@ -1550,6 +1616,7 @@ static __global__ void k_reconstruct(DevCfg c, int dir, const double* __restrict
   for (int v = 0; v < c.dof; v++) {
     const double* a = p + (long long)v * c.Z;
     double y[5];
+#pragma unroll
     for (int m = 0; m < 5; m++) {
       int xx = x + m - 2;
       xx = ((xx % NT) + NT) % NT;  // circular, af::shift semantics
@@ -1569,11 +1636,14 @@ __global__ void k_batch_solve(int batch, const double* __restrict__ A, const dou
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= batch) return;
   double a[N][N], bb[N], xx[N];
+#pragma unroll
   for (int r = 0; r < N; r++) {
     bb[r] = b[n * N + r];
+#pragma unroll
     for (int q = 0; q < N; q++) a[r][q] = A[(n * N + r) * N + q];
   }
   gauss_solve<double, N>(a, bb, xx);
+#pragma unroll
   for (int r = 0; r < N; r++) x[n * N + r] = xx[r];
 }
 

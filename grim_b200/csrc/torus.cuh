@@ -35,13 +35,18 @@ __global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, cons
   const long long gz = gidx(c, z);
   ZoneGeo<double> G;
   geo_load<double>(G, geoC, c.GZ, gz);
-  double* pv[12];
-  for (int v = 0; v < c.dof; v++) pv[v] = p + (long long)v * Z + z;
+  // compile-time row count and indices keep the pointer table in registers
+  constexpr int NFT = 5 + COND + VISC, DOFT = NFT + 3;
+  double* pv[DOFT];
+#pragma unroll
+  for (int v = 0; v < DOFT; v++) pv[v] = p + (long long)v * Z + z;
   if (nanFlag && *nanFlag) {
     bool bad = false;
-    for (int v = 0; v < c.dof; v++) bad |= isnan(*pv[v]);
+#pragma unroll
+    for (int v = 0; v < DOFT; v++) bad |= isnan(*pv[v]);
     if (bad)
-      for (int v = 0; v < c.dof; v++) *pv[v] = 0.;
+#pragma unroll
+      for (int v = 0; v < DOFT; v++) *pv[v] = 0.;
   }
   const double minRho = __ldg(geoC + 37LL * c.GZ + gz);
   const double minU = __ldg(geoC + 38LL * c.GZ + gz);
@@ -75,15 +80,19 @@ __global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, cons
   betasqr = fmin(betasqr, betasqrmax);
   const double gamma = 1. / sqrt(1. - betasqr);
   double ucondr[4];
+#pragma unroll
   for (int m = 0; m < 4; m++) ucondr[m] = gamma * (e.uCon[m] + betapar * e.bCon[m]);
-  const double Bcon[4] = {0., *pv[c.B1], *pv[c.B1 + 1], *pv[c.B1 + 2]};
+  const double Bcon[4] = {0., *pv[NFT], *pv[NFT + 1], *pv[NFT + 2]};
   double Bcov[4];
+#pragma unroll
   for (int m = 0; m < 4; m++) {
     double s = 0.;
+#pragma unroll
     for (int n = 0; n < 4; n++) s += G.gcov[n][m] * Bcon[n];
     Bcov[m] = s;
   }
   double udotB = 0., bSqr_fl = 0.;
+#pragma unroll
   for (int n = 0; n < 4; n++) {
     udotB += Bcov[n] * e.uCon[n];
     bSqr_fl += Bcov[n] * Bcon[n];
@@ -97,12 +106,16 @@ __global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, cons
   const double inv_ut = 1. / ucondr[0];
   double vcon[4];
   vcon[0] = 0. + 1.;
+#pragma unroll
   for (int m = 1; m < 4; m++) vcon[m] = vpar * Bcon[m] / bNorm + ucondr[m] * inv_ut;
   double vsqr = 0.;
+#pragma unroll
   for (int m = 0; m < 4; m++)
+#pragma unroll
     for (int n = 0; n < 4; n++) vsqr += G.gcov[m][n] * vcon[m] * vcon[n];
   if (vsqr >= 0. || vsqr < 1. / G.gcon[0][0]) vsqr = 1. / G.gcon[0][0];
   const double ut = sqrt(-1. / vsqr);
+#pragma unroll
   for (int m = 1; m < 4; m++) {
     double utcon = ut * (vcon[m] - G.gcon[0][m] / G.gcon[0][0]);
     *pv[UU + m] = *pv[UU + m] * (1. - trans) + trans * utcon;
@@ -125,7 +138,7 @@ __global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, cons
       const double cs = e.soundSpeed;
       const double Qmax = 1.07 * c.CondClosure * *pv[RHO] * pow(cs, 3.);
       const double lim = fmax(fabs(e.q) / Qmax, 1.);
-      *pv[c.Q] = *pv[c.Q] / lim;
+      *pv[5] = *pv[5] / lim;
     }
     if (VISC) {
       const double pr = e.pressure, dP = e.deltaP, bs = e.bSqr;
@@ -133,7 +146,7 @@ __global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, cons
       const double dPmaxPlus = fmin(1.07 * c.ViscClosure * bs * 0.5 * dPmod, 1.49 * pr);
       const double dPmaxMinus = fmax(-1.07 * c.ViscClosure * bs, -2.99 * pr);
       const double f = (dP > 0.) ? 1. / fmax(dP / dPmaxPlus, 1.) : 1. / fmax(dP / dPmaxMinus, 1.);
-      *pv[c.DP] = *pv[c.DP] * f;
+      *pv[5 + COND] = *pv[5 + COND] * f;
     }
   }
 }
@@ -184,7 +197,9 @@ __global__ void k_torus_inflow(DevCfg c, TorusCfg t, double* __restrict__ p, con
   }
   const double U[3] = {*u1, *u2, *u3};
   double vSqr = 0.;
+#pragma unroll
   for (int a = 0; a < 3; a++)
+#pragma unroll
     for (int b = 0; b < 3; b++) vSqr += G.gcov[a + 1][b + 1] * U[a] * U[b];
   const double vSqrMax = 1. - 1. / t.MaxLorentzFactor / t.MaxLorentzFactor;
   vSqr = fmax(fmin(vSqr, vSqrMax), 1.e-13);
