@@ -73,6 +73,13 @@ __global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, cons
   }
   const double rho = *pv[RHO], u = *pv[UU];
   double trans = fmax(fmin(1., (bSqr1 - 0.1 * rho) / rho), 0.) * (usefloor ? 1. : 0.);
+#ifdef GRIM_FAST_MATH
+  // the fix below blends with weight trans: with trans = 0 it returns the
+  // velocities unchanged (up to the sign of a zero), so the fast path skips it
+  if (trans != 0.) {
+#else
+  {
+#endif
   // drift-frame velocity fix
   const double betapar = -e.bCon[0] / bSqr1 / e.uCon[0];
   double betasqr = betapar * betapar * bSqr1;
@@ -120,6 +127,7 @@ __global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, cons
     double utcon = ut * (vcon[m] - G.gcon[0][m] / G.gcon[0][0]);
     *pv[UU + m] = *pv[UU + m] * (1. - trans) + trans * utcon;
   }
+  }  // drift-frame fix
   // maximum Lorentz factor
   load_elem<COND, VISC>(e, c, p, z, G);
   {
