@@ -75,7 +75,8 @@ __global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, cons
   double trans = fmax(fmin(1., (bSqr1 - 0.1 * rho) / rho), 0.) * (usefloor ? 1. : 0.);
 #ifdef GRIM_FAST_MATH
   // the fix below blends with weight trans: with trans = 0 it returns the
-  // velocities unchanged (up to the sign of a zero), so the fast path skips it
+  // velocities unchanged (up to the sign of a zero, or a non-finite
+  // correction, which it would propagate), so the fast path skips it
   if (trans != 0.) {
 #else
   {
