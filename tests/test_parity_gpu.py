@@ -349,7 +349,9 @@ def test_autotuned_face_kernels_give_identical_results(mode):
     """The autotuner only changes launch shapes.  In the FP64 parity unit
     (no FMA contraction) every variant gives the same bits; in the fast unit
     the compiler may fuse a multiply-add in one variant and not in another,
-    so the variants agree to roundoff (1e-14 of the field's scale)."""
+    so the fluxes and their divergence agree to roundoff (1e-14 / 1e-12 of
+    the field's scale), and three steps of the mixed Newton (FP32 Jacobian,
+    3 iterations) agree within its convergence band (1e-9)."""
     cfg = PR.orszag_tang_config(N=64, maxNonLinearIter=3)
     P = PR.orszag_tang_prims(cfg)
     from grim_b200.timestepper import timeStepper
@@ -371,7 +373,7 @@ def test_autotuned_face_kernels_give_identical_results(mode):
     for _ in range(3):
         a.timeStep()
         b.timeStep()
-    assert same(a.primOld.getVars(), b.primOld.getVars(), 1e-12)
+    assert same(a.primOld.getVars(), b.primOld.getVars(), 1e-9)
     # every variant of every direction, forced one at a time, gives the
     # default's divergence of fluxes
     ref_div, ref_flux = b.computeDivOfFluxes(P)
