@@ -441,6 +441,109 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1_tma(const __grid_con
   }
 }
 
+// X2 / X3 faces, TMA-staged: the strip scheme below (4 consecutive i by 8
+// zones along the direction per warp, 7 faces) with persistent warps that
+// stage each chunk's stencil -- a box of 4 i x 12 zones along DIR x all dof
+// -- in shared memory while computing the previous chunk.  The tensor map's
+// box is (4, 12, 1, dof) for X2 and (4, 1, 12, dof) for X3; x starts at 4q
+// (32-byte aligned) and the box along DIR at 7 x chunk (never negative).
+constexpr int kStripRows = 12;
+template <int COND, int VISC, int MINB, int DIR>
+__global__ void __launch_bounds__(128, MINB) k_face_flux_strip_tma(const __grid_constant__ CUtensorMap tmap, DevCfg c,
+                                                                    const double* __restrict__ geoF,
+                                                                    const double* __restrict__ geoC,
+                                                                    double* __restrict__ flux, DevState* st) {
+  constexpr int DOF = 8 + COND + VISC;
+  constexpr int QI = 4, FPW = 7;
+  constexpr int BOX = QI * kStripRows * DOF;  // doubles per buffer (a multiple of 128 bytes)
+  constexpr int dir = DIR;
+  extern __shared__ __align__(128) double smem_st[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double* bufs = smem_st + (size_t)w * 2 * BOX;
+  double* park = smem_st + (size_t)nw * 2 * BOX;
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(park + 3 * DOF * blockDim.x) + 2 * w;
+  const int NT = (DIR == 1) ? c.N2T : c.N3T;
+  const unsigned nq = (unsigned)(c.N1T + QI - 1) / QI;
+  const unsigned nch = (unsigned)(NT - 5 + FPW - 1) / FPW;  // faces 3 .. NT-3
+  const unsigned nother = (unsigned)((DIR == 1) ? c.N3T : c.N2T);
+  const long long nitems = (long long)nq * nch * nother;
+  const long long stride = (long long)gridDim.x * nw;
+  long long item = (long long)blockIdx.x * nw + w;
+  if (lane == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncwarp();
+  auto decompose = [&](long long it, int& iq, int& ch, int& other) {
+    const unsigned itu = (unsigned)it, r = itu / nq;
+    iq = (int)(itu - r * nq);
+    const unsigned o = r / nch;
+    ch = (int)(r - o * nch);
+    other = (int)o;
+  };
+  auto issue = [&](long long it, int buf) {
+    int iq, ch, other;
+    decompose(it, iq, ch, other);
+    mbar_expect_tx(&bars[buf], BOX * (unsigned)sizeof(double));
+    if (DIR == 1)
+      tma_load_4d(bufs + buf * BOX, &tmap, &bars[buf], iq * QI, ch * FPW, other, 0);
+    else
+      tma_load_4d(bufs + buf * BOX, &tmap, &bars[buf], iq * QI, other, ch * FPW, 0);
+  };
+  if (lane == 0 && item < nitems) issue(item, 0);
+  unsigned phase0 = 0, phase1 = 0;
+  int buf = 0;
+  const int ii = lane % QI, jj = lane / QI;
+  for (; item < nitems; item += stride, buf ^= 1) {
+    const long long next = item + stride;
+    if (lane == 0 && next < nitems) issue(next, buf ^ 1);
+    const unsigned ph = buf ? phase1 : phase0;
+    const bool arrived = mbar_wait_bounded(&bars[buf], ph);
+    if (buf) phase1 ^= 1; else phase0 ^= 1;
+    if (!__all_sync(0xffffffffu, arrived)) {
+      if (lane == 0) {
+        atomicAdd(&st->waitTimeouts, 1ULL);
+        if (next < nitems) mbar_wait_bounded(&bars[buf ^ 1], buf ? phase0 : phase1);
+      }
+      __syncwarp();
+      return;
+    }
+    int iq, ch, other;
+    decompose(item, iq, ch, other);
+    const int i = iq * QI + ii;
+    const int x = 2 + ch * FPW + jj;  // zone along DIR; face x sits at its left
+    const bool reconOK = i < c.N1T && x <= NT - 3;
+    const double* rb = bufs + buf * BOX;
+    double lo[DOF], ro[DOF];
+#pragma unroll
+    for (int v = 0; v < DOF; v++) {
+      const double* a = rb + (v * kStripRows + jj) * QI + ii;  // rows jj .. jj+4 hold x-2 .. x+2
+      if (kFastMath)
+        recon_faces_fast(c.reconstruction, c.theta, a[0], a[QI], a[2 * QI], a[3 * QI], a[4 * QI], lo[v], ro[v]);
+      else
+        recon_faces(c.reconstruction, c.theta, a[0], a[QI], a[2 * QI], a[3 * QI], a[4 * QI], lo[v], ro[v]);
+    }
+    __syncwarp();  // the buffer is read; it may be refilled two items on
+    double pl[DOF];
+#pragma unroll
+    for (int v = 0; v < DOF; v++) pl[v] = __shfl_up_sync(0xffffffffu, ro[v], QI);
+    if (lane >= QI && reconOK) {
+      const long long z = (DIR == 1) ? zidx(c, i, x, other) : zidx(c, i, other, x);
+      ZoneGeo<double> G;
+      // X3 faces use the centre geometry of each side (fvmfluxes.cpp:150-151),
+      // one and the same: the metric does not depend on X3
+      if (DIR == 2)
+        load_geo(G, c, geoC, z, i, other, 0.5, 0.5);
+      else
+        load_geo(G, c, geoF, z, i, x, 0.5, 0.);
+#pragma unroll
+      for (int v = 0; v < DOF; v++) park[(2 * DOF + v) * blockDim.x + threadIdx.x] = lo[v];
+      riemann_face<COND, VISC>(c, dir, pl, G, flux, z, park);
+    }
+  }
+}
+
 // X2 / X3 faces: the X1 scheme turned sideways.  A warp holds QI
 // consecutive i (lane % QI) by 32/QI consecutive zones along dir
 // (lane / QI); every lane reconstructs its zone once and the right-face
@@ -569,8 +672,12 @@ static __global__ void k_stage_emf(DevCfg c, StageBufs b) {
 // stage element, consOld on the half stage, explicit sources) and then
 // PART 2 (fluxes: CT, divergence, induction, Newton guess), each with the
 // registers of its own half (the flux half is a memory stream).
+// blocks per SM each part is compiled for: the flux half is a memory
+// stream that wants warps in flight more than registers (measured on the
+// 3D torus: 64 registers with a few spills beat 85 and 98 without)
+constexpr int kEpiMinBlocks[3] = {4, 1, 8};
 template <int COND, int VISC, int PART>
-__global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, StageBufs b) {
+__global__ void __launch_bounds__(128, kEpiMinBlocks[PART]) k_stage_epilogue(DevCfg c, int stage, StageBufs b) {
   constexpr int NF = 5 + COND + VISC;
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= c.Zint) return;
@@ -586,77 +693,83 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
   constexpr int DOF = NF + 3;
   double div[DOF];
   if constexpr (PART != 1) {
-  // ---- fluxes on the zone's six faces: Riemann fluxes for the fluid rows,
-  // flux-CT values for the field rows (constrainedtransport.cpp:3-51)
-  double Fl[3][DOF], Fr[3][DOF];
+  // ---- fluxes on the zone's two faces of each direction: Riemann fluxes
+  // for the fluid rows, flux-CT values for the field rows
+  // (constrainedtransport.cpp:3-51); the divergence (fvmfluxes.cpp) adds
+  // one direction at a time, so only that direction's faces are live:
+  // zero-padded convolution Fr*(1/dX) + Fl*(-1/dX) in 1D/2D, shifted
+  // difference (Fr - Fl)/dX in 3D, summed in direction order
   const long long sd[3] = {s1, s2, s3};
-#pragma unroll
-  for (int d = 0; d < 3; d++)
-#pragma unroll
-    for (int v = 0; v < DOF; v++) { Fl[d][v] = 0.; Fr[d][v] = 0.; }
-  // directions unrolled to their compile-time bound: constant indices keep
-  // Fl / Fr in registers
-#pragma unroll
-  for (int d = 0; d < 3; d++)
-    if (d < c.dim)
-#pragma unroll
-      for (int v = 0; v < NF; v++) { Fl[d][v] = f.at(d, v, z); Fr[d][v] = f.at(d, v, z + sd[d]); }
-  if (c.dim == 1) {
-#pragma unroll
-    for (int b3 = 0; b3 < 3; b3++) { Fl[0][NF + b3] = f.at(0, c.B1 + b3, z); Fr[0][NF + b3] = f.at(0, c.B1 + b3, z + s1); }
-  } else if (c.dim == 2) {
+  double e[12];  // corner EMFs: EMF3 (i|i+1, j|j+1), EMF2 (i|i+1, k|k+1), EMF1 (j|j+1, k|k+1)
+  if (c.dim >= 2) {
     const double* E3 = b.emf + 2 * Z;
-    const double e00 = E3[z], e10 = E3[z + s1];
-    const double e01 = E3[z + s2], e11 = E3[z + s1 + s2];
-    // F1: B1 -> 0, B2 -> 0.5 (emf3 + emf3[j+1]); F2: B1 -> -0.5 (emf3 + emf3[i+1]), B2 -> 0
-    Fl[0][NF + 1] = 0.5 * (e00 + e01);
-    Fr[0][NF + 1] = 0.5 * (e10 + e11);
-    Fl[1][NF + 0] = -0.5 * (e00 + e10);
-    Fr[1][NF + 0] = -0.5 * (e01 + e11);
-    Fl[0][NF + 2] = f.at(0, c.B1 + 2, z);
-    Fr[0][NF + 2] = f.at(0, c.B1 + 2, z + s1);
-    Fl[1][NF + 2] = f.at(1, c.B1 + 2, z);
-    Fr[1][NF + 2] = f.at(1, c.B1 + 2, z + s2);
-  } else {
-    // EMF3 at (i|i+1, j|j+1), EMF2 at (i|i+1, k|k+1), EMF1 at (j|j+1, k|k+1)
-    const double *E1 = b.emf, *E2 = b.emf + Z, *E3 = b.emf + 2 * Z;
-    const double a00 = E3[z], a10 = E3[z + s1];
-    const double a01 = E3[z + s2], a11 = E3[z + s1 + s2];
-    const double b00 = E2[z], b10 = E2[z + s1];
-    const double b01 = E2[z + s3], b11 = E2[z + s1 + s3];
-    const double c00 = E1[z], c10 = E1[z + s2];
-    const double c01 = E1[z + s3], c11 = E1[z + s2 + s3];
-    Fl[0][NF + 1] = 0.5 * (a00 + a01);  Fr[0][NF + 1] = 0.5 * (a10 + a11);
-    Fl[0][NF + 2] = -0.5 * (b00 + b01); Fr[0][NF + 2] = -0.5 * (b10 + b11);
-    Fl[1][NF + 0] = -0.5 * (a00 + a10); Fr[1][NF + 0] = -0.5 * (a01 + a11);
-    Fl[1][NF + 2] = 0.5 * (c00 + c01);  Fr[1][NF + 2] = 0.5 * (c10 + c11);
-    Fl[2][NF + 0] = 0.5 * (b00 + b10);  Fr[2][NF + 0] = 0.5 * (b01 + b11);
-    Fl[2][NF + 1] = -0.5 * (c00 + c10); Fr[2][NF + 1] = -0.5 * (c01 + c11);
+    e[0] = E3[z]; e[1] = E3[z + s1]; e[2] = E3[z + s2]; e[3] = E3[z + s1 + s2];
   }
-  if (c.problem == GRIM_PROBLEM_TORUS) {
-    // applyProblemSpecificFluxFilter (torus/problem.cpp:1243-1285)
-    if (i == c.g1) Fl[0][RHO] = fmin(Fl[0][RHO], 0.);
-    if (i == c.N1 + c.g1 - 1) Fr[0][RHO] = fmax(Fr[0][RHO], 0.);
-    if (c.dim >= 2) {
-      if (j == c.g2)
-#pragma unroll
-        for (int v = 0; v < DOF; v++) Fl[1][v] = 0.;
-      if (j == c.N2 + c.g2 - 1)
-#pragma unroll
-        for (int v = 0; v < DOF; v++) Fr[1][v] = 0.;
-    }
+  if (c.dim == 3) {
+    const double *E1 = b.emf, *E2 = b.emf + Z;
+    e[4] = E2[z]; e[5] = E2[z + s1]; e[6] = E2[z + s3]; e[7] = E2[z + s1 + s3];
+    e[8] = E1[z]; e[9] = E1[z + s2]; e[10] = E1[z + s3]; e[11] = E1[z + s2 + s3];
   }
-  // ---- divergence (fvmfluxes.cpp): zero-padded convolution in 1D/2D,
-  // shifted difference in 3D
-  const double i1 = 1. / c.dX[0], i2 = 1. / c.dX[1];
 #pragma unroll
-  for (int v = 0; v < DOF; v++) {
-    if (c.dim <= 2) {
-      double d = Fr[0][v] * i1 + Fl[0][v] * (-i1);
-      if (c.dim == 2) d = d + (Fr[1][v] * i2 + Fl[1][v] * (-i2));
-      div[v] = d;
+  for (int d = 0; d < 3; d++) {
+    if (d >= c.dim) break;
+    double Fl[DOF], Fr[DOF];
+#pragma unroll
+    for (int v = 0; v < NF; v++) { Fl[v] = f.at(d, v, z); Fr[v] = f.at(d, v, z + sd[d]); }
+#pragma unroll
+    for (int v = NF; v < DOF; v++) { Fl[v] = 0.; Fr[v] = 0.; }
+    if (c.dim == 1) {
+#pragma unroll
+      for (int b3 = 0; b3 < 3; b3++) { Fl[NF + b3] = f.at(0, c.B1 + b3, z); Fr[NF + b3] = f.at(0, c.B1 + b3, z + s1); }
+    } else if (c.dim == 2) {
+      // F1: B1 -> 0, B2 -> 0.5 (emf3 + emf3[j+1]); F2: B1 -> -0.5 (emf3 + emf3[i+1]), B2 -> 0
+      if (d == 0) {
+        Fl[NF + 1] = 0.5 * (e[0] + e[2]);
+        Fr[NF + 1] = 0.5 * (e[1] + e[3]);
+      } else {
+        Fl[NF + 0] = -0.5 * (e[0] + e[1]);
+        Fr[NF + 0] = -0.5 * (e[2] + e[3]);
+      }
+      Fl[NF + 2] = f.at(d, c.B1 + 2, z);
+      Fr[NF + 2] = f.at(d, c.B1 + 2, z + sd[d]);
+    } else if (d == 0) {
+      Fl[NF + 1] = 0.5 * (e[0] + e[2]);  Fr[NF + 1] = 0.5 * (e[1] + e[3]);
+      Fl[NF + 2] = -0.5 * (e[4] + e[6]); Fr[NF + 2] = -0.5 * (e[5] + e[7]);
+    } else if (d == 1) {
+      Fl[NF + 0] = -0.5 * (e[0] + e[1]); Fr[NF + 0] = -0.5 * (e[2] + e[3]);
+      Fl[NF + 2] = 0.5 * (e[8] + e[10]); Fr[NF + 2] = 0.5 * (e[9] + e[11]);
     } else {
-      div[v] = (Fr[0][v] - Fl[0][v]) / c.dX[0] + (Fr[1][v] - Fl[1][v]) / c.dX[1] + (Fr[2][v] - Fl[2][v]) / c.dX[2];
+      Fl[NF + 0] = 0.5 * (e[4] + e[5]);  Fr[NF + 0] = 0.5 * (e[6] + e[7]);
+      Fl[NF + 1] = -0.5 * (e[8] + e[9]); Fr[NF + 1] = -0.5 * (e[10] + e[11]);
+    }
+    if (c.problem == GRIM_PROBLEM_TORUS) {
+      // applyProblemSpecificFluxFilter (torus/problem.cpp:1243-1285)
+      if (d == 0) {
+        if (i == c.g1) Fl[RHO] = fmin(Fl[RHO], 0.);
+        if (i == c.N1 + c.g1 - 1) Fr[RHO] = fmax(Fr[RHO], 0.);
+      } else if (d == 1) {
+        if (j == c.g2)
+#pragma unroll
+          for (int v = 0; v < DOF; v++) Fl[v] = 0.;
+        if (j == c.N2 + c.g2 - 1)
+#pragma unroll
+          for (int v = 0; v < DOF; v++) Fr[v] = 0.;
+      }
+    }
+    if (c.dim <= 2) {
+      const double id = 1. / c.dX[d];
+#pragma unroll
+      for (int v = 0; v < DOF; v++) {
+        const double t = Fr[v] * id + Fl[v] * (-id);
+        div[v] = (d == 0) ? t : div[v] + t;
+      }
+    } else {
+      const double id = 1. / c.dX[d];
+#pragma unroll
+      for (int v = 0; v < DOF; v++) {
+        const double t = kFastMath ? (Fr[v] - Fl[v]) * id : (Fr[v] - Fl[v]) / c.dX[d];
+        div[v] = (d == 0) ? t : div[v] + t;
+      }
     }
   }
 
@@ -787,7 +900,10 @@ __global__ void __launch_bounds__(128) k_stage_epilogue(DevCfg c, int stage, Sta
   }  // PART != 2
   if constexpr (PART != 1) {
 #pragma unroll
-  for (int v = 0; v < NF + 3; v++) b.divF[(long long)v * Z + z] = div[v];
+  for (int v = 0; v < NF; v++) b.divF[(long long)v * Z + z] = div[v];
+  if (b.divFB)
+#pragma unroll
+    for (int v = NF; v < DOF; v++) b.divF[(long long)v * Z + z] = div[v];
   // ---- induction and the Newton guess
   const double fac = (stage == GRIM_HALF_STEP) ? 0.5 * dt : dt;
 #pragma unroll
@@ -1745,14 +1861,33 @@ static void face_x1_tma_launch(const DevCfg& c, const CUtensorMap* tmap, const d
   }
   k_face_flux_x1_tma<C, V, MINB><<<sm_count() * MINB, 32 * nw, smem, s>>>(*tmap, c, geoF, flux, st);
 }
+template <int C, int V, int MINB>
+static void face_strip_tma_launch(const DevCfg& c, int dir, const CUtensorMap* tmap, const double* geoF,
+                                  const double* geoC, double* flux, DevState* st, cudaStream_t s) {
+  constexpr int DOF = 8 + C + V;
+  const int nw = 4;
+  const size_t smem = ((size_t)nw * 2 * 4 * kStripRows * DOF + 3 * DOF * 128) * sizeof(double) + 2 * nw * 8;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_face_flux_strip_tma<C, V, MINB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    cudaFuncSetAttribute(k_face_flux_strip_tma<C, V, MINB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    attr = true;
+  }
+  if (dir == 1)
+    k_face_flux_strip_tma<C, V, MINB, 1><<<sm_count() * MINB, 32 * nw, smem, s>>>(tmap[1], c, geoF, geoC, flux, st);
+  else
+    k_face_flux_strip_tma<C, V, MINB, 2><<<sm_count() * MINB, 32 * nw, smem, s>>>(tmap[2], c, geoF, geoC, flux, st);
+}
 template <int C, int V>
 static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,
                         double* flux, int variant, const CUtensorMap* tmap, DevState* st, cudaStream_t s) {
   if constexpr (C == 0 && V == 0) {
     if (dir == 0) {
-      if (variant >= 2 && tmap && st) {
-        if (variant == 3) face_x1_tma_launch<C, V, 4>(c, tmap, geoF, flux, st, s);
-        else face_x1_tma_launch<C, V, 3>(c, tmap, geoF, flux, st, s);
+      if ((variant == 2 || variant == 3) && tmap && st) {
+        if (variant == 3) face_x1_tma_launch<C, V, 4>(c, &tmap[0], geoF, flux, st, s);
+        else face_x1_tma_launch<C, V, 3>(c, &tmap[0], geoF, flux, st, s);
       } else if (variant == 4) {
         face_x1_launch<C, V, 3, true>(c, ps, geoF, flux, s);
       } else if (variant == 1 || variant == 3) {
@@ -1762,7 +1897,14 @@ static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double
       }
       return;
     }
+    if (variant >= 8 && tmap && st) {
+      if (variant == 9) face_strip_tma_launch<C, V, 4>(c, dir, tmap, geoF, geoC, flux, st, s);
+      else face_strip_tma_launch<C, V, 3>(c, dir, tmap, geoF, geoC, flux, st, s);
+      return;
+    }
     switch (variant) {
+      case 8: face_strip_launch<C, V, 4, 3>(c, dir, ps, geoF, geoC, flux, s); break;
+      case 9: face_strip_launch<C, V, 4, 4>(c, dir, ps, geoF, geoC, flux, s); break;
       case 1: face_strip_launch<C, V, 4, 4>(c, dir, ps, geoF, geoC, flux, s); break;
       case 2: face_strip_launch<C, V, 2, 3>(c, dir, ps, geoF, geoC, flux, s); break;
       case 3: face_strip_launch<C, V, 2, 4>(c, dir, ps, geoF, geoC, flux, s); break;
@@ -1787,10 +1929,12 @@ void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, c
 // X1: 0, 1 = register budget 3 / 4 blocks; 2, 3 = the same with TMA-staged
 // rows (when the caller has a tensor map of the primitives); 4 = both face
 // states evaluated side by side.  X2 / X3: 0-5 = lane split x register
-// budget; 6, 7 = side by side with 8 / 4 i per warp.
+// budget; 6, 7 = side by side with 8 / 4 i per warp; 8, 9 = TMA-staged
+// chunks, 3 / 4 blocks per SM.  tmap points at the caller's three tensor
+// maps (X1, X2, X3 box shapes) of the prim array, or is null.
 int face_variants(const DevCfg& c, int dir) {
   if (c.conduction || c.viscosity) return 1;
-  return dir == 0 ? 5 : 8;
+  return dir == 0 ? 5 : 10;
 }
 #endif  // !GRIM_SKIP_FACES
 

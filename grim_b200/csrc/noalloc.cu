@@ -115,6 +115,7 @@ extern "C" int grim_div_fluxes_noalloc(const grim_config* cfg, const double* pri
   b.ps = prim;
   b.pold = prim;
   b.divF = divF;
+  b.divFB = 1;
   b.geoC = nullptr;
   b.gamma = nullptr;
   // dt = 0 for the induction part of the epilogue (its output is not used)

@@ -82,7 +82,8 @@ struct grim_handle {
   // TMA descriptors of the arrays the X1 face kernel reads (primOld,
   // primHalf, scratch) as (i, j, k, var); valid when haveTmap
   bool haveTmap = false;
-  CUtensorMap tmap[3];
+  CUtensorMap tmap[3][3];  // [primOld, primHalf, scratch][box for X1, X2, X3 faces]
+  bool tmapMissing[3] = {false, false, false};
   // face-kernel launch variants per direction, [exact unit, fast unit]
   int faceVariant[2][3] = {{0, 0, 0}, {0, 0, 0}};
   // dt held at its current value instead of computeDt (the adjoint's runs)
@@ -198,18 +199,19 @@ static int make_devcfg(const grim_config& c, DevCfg& d) {
 
 static bool use_exact(const grim_handle* h) { return h->cfg.newtonMode == GRIM_NEWTON_PARITY_FD64; }
 
-// the tensor map of a prim array of this handle, or null
-static const CUtensorMap* tmap_for(const grim_handle* h, const double* p) {
-  if (!h->haveTmap) return nullptr;
-  if (p == h->primOld) return &h->tmap[0];
-  if (p == h->primHalf) return &h->tmap[1];
-  if (p == h->scratch) return &h->tmap[2];
+// the three tensor maps (X1, X2, X3 box shapes) of a prim array of this
+// handle, or null when the array has none or direction dir's box does not fit
+static const CUtensorMap* tmap_for(const grim_handle* h, const double* p, int dir) {
+  if (!h->haveTmap || h->tmapMissing[dir]) return nullptr;
+  if (p == h->primOld) return h->tmap[0];
+  if (p == h->primHalf) return h->tmap[1];
+  if (p == h->scratch) return h->tmap[2];
   return nullptr;
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no
 // link-time dependency on the driver library)
-static bool encode_prim_tmap(const DevCfg& c, double* base, CUtensorMap* out) {
+static bool encode_prim_tmap(const DevCfg& c, double* base, int dir, CUtensorMap* out) {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     void* fn = nullptr;
@@ -219,11 +221,14 @@ static bool encode_prim_tmap(const DevCfg& c, double* base, CUtensorMap* out) {
       return false;
     encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   }
-  // rows of N1T doubles must be 16-byte strided; the 40-zone box must fit
+  // rows of N1T doubles must be 16-byte strided; the boxes must fit: X1
+  // faces stage 40 zones along i, X2 / X3 faces 4 i x 12 zones along j / k
   if (c.N1T % 2 != 0 || c.N1T < 40 || c.dof > 256) return false;
+  if (dir == 1 && c.N2T < 12) return false;
+  if (dir == 2 && c.N3T < 12) return false;
   const cuuint64_t dims[4] = {(cuuint64_t)c.N1T, (cuuint64_t)c.N2T, (cuuint64_t)c.N3T, (cuuint64_t)c.dof};
   const cuuint64_t strides[3] = {(cuuint64_t)c.N1T * 8, (cuuint64_t)c.N1T * c.N2T * 8, (cuuint64_t)c.Z * 8};
-  const cuuint32_t box[4] = {40, 1, 1, (cuuint32_t)c.dof};
+  const cuuint32_t box[4] = {dir == 0 ? 40u : 4u, dir == 1 ? 12u : 1u, dir == 2 ? 12u : 1u, (cuuint32_t)c.dof};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
   const CUresult r = encode(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims, strides, box, estr,
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -286,7 +291,7 @@ static void enqueue_stencil(grim_handle* h, int stage) {
   for (int d = 0; d < c.dim; d++) {
     PROF(GRIM_PROF_FACES_X1 + d);
     KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], h->faceVariant[use_exact(h) ? 0 : 1][d],
-             tmap_for(h, b.ps), h->st, s);
+             tmap_for(h, b.ps, d), h->st, s);
     g_launch_counter++;
   }
   PROF(GRIM_PROF_EPILOGUE);
@@ -500,8 +505,18 @@ int grim_create(const grim_config* cfg, int device, grim_handle** out) {
     set_err("stream creation failed"); free_all(h); delete h; return GRIM_ECUDA;
   }
   for (int i = 0; i < 8; i++) cudaEventCreate(&h->ev[i]);
-  h->haveTmap = encode_prim_tmap(c, h->primOld, &h->tmap[0]) && encode_prim_tmap(c, h->primHalf, &h->tmap[1]) &&
-                encode_prim_tmap(c, h->scratch, &h->tmap[2]);
+  {
+    // X1 maps are required; X2 / X3 maps are built when the grid has room
+    // for their boxes (a missing one leaves its direction on the plain kernel)
+    double* arrays[3] = {h->primOld, h->primHalf, h->scratch};
+    bool ok = true;
+    for (int a = 0; a < 3 && ok; a++) {
+      ok = encode_prim_tmap(c, arrays[a], 0, &h->tmap[a][0]);
+      for (int d = 1; ok && d < 3; d++)
+        if (d < c.dim && !encode_prim_tmap(c, arrays[a], d, &h->tmap[a][d])) h->tmapMissing[d] = true;
+    }
+    h->haveTmap = ok;
+  }
   // geometry (geometry.cpp ctor at LEFT/RIGHT/BOTTOM/TOP/CENTER, timestepper.cpp:236-283)
   if (cfg->metric != GRIM_MINKOWSKI) {
     for (int l = 0; l < 5; l++)
@@ -692,10 +707,9 @@ int grim_compute_div_fluxes(grim_handle* h, const double* prim, double* divF, do
   if (c.conduction || c.viscosity) KNS_CALL(h, emhd_prepass, c, b.ps, b.geoC, h->uT, h->stream);
   for (int d = 0; d < c.dim; d++)
     KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], h->faceVariant[use_exact(h) ? 0 : 1][d],
-             tmap_for(h, b.ps), h->st, h->stream);
-  // divergence of all dof rows: epilogue writes nf rows into divF and the
-  // induction into the guess; the B rows of the divergence are recovered
-  // from the guess: B_new = (consOld_B - 0.5 dt divF_B)/g with dt kept
+             tmap_for(h, b.ps, d), h->st, h->stream);
+  // divergence of all dof rows (the time step needs the fluid rows only)
+  b.divFB = 1;
   KNS_CALL(h, stage_epilogue, c, GRIM_HALF_STEP, b, h->stream);
   CK(cudaGetLastError());
   if (divF) {
@@ -1050,12 +1064,12 @@ int grim_autotune(grim_handle* h, int* variants, double* msBest) {
     double best = 1e30;
     int bestV = 0;
     for (int v = 0; v < nv; v++) {
-      KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], v, tmap_for(h, b.ps), h->st,
+      KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], v, tmap_for(h, b.ps, d), h->st,
                h->stream);  // warm-up
       CK(cudaEventRecord(e0, h->stream));
       const int reps = 3;
       for (int r = 0; r < reps; r++)
-        KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], v, tmap_for(h, b.ps), h->st, h->stream);
+        KNS_CALL(h, face_flux, c, d, b.ps, b.geoF[d], b.geoC, h->flux[d], v, tmap_for(h, b.ps, d), h->st, h->stream);
       CK(cudaEventRecord(e1, h->stream));
       CK(cudaEventSynchronize(e1));
       float ms = 0.f;

@@ -32,6 +32,7 @@ struct StageBufs {
   double* uT;             // EMHD pre-pass: u_mu (4) + T (1), 5 x Z
   double* consOld;        // dof x Z (fluid rows then B rows)
   double* divF;           // dof x Z (fluid rows, then B rows)
+  int divFB;              // the epilogue writes divF's B rows too (else the fluid rows only)
   double* Sexp;           // nf x Z
   double* R;              // nf x Z  (Newton scratch)
   double* l2;             // 2 x Z   (l2, l2first)

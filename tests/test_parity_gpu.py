@@ -369,7 +369,7 @@ def test_autotuned_face_kernels_give_identical_results(mode):
 
     tuned = a.autotune()
     assert set(tuned) == {0, 1}
-    assert 0 <= tuned[0][0] < 5 and 0 <= tuned[1][0] < 8 and all(ms > 0 for _, ms in tuned.values())
+    assert 0 <= tuned[0][0] < 5 and 0 <= tuned[1][0] < 10 and all(ms > 0 for _, ms in tuned.values())
     for _ in range(3):
         a.timeStep()
         b.timeStep()
@@ -377,14 +377,42 @@ def test_autotuned_face_kernels_give_identical_results(mode):
     # every variant of every direction, forced one at a time, gives the
     # default's divergence of fluxes
     ref_div, ref_flux = b.computeDivOfFluxes(P)
-    for d, nv in ((0, 5), (1, 8)):  # X1 variants 2, 3 stage rows with TMA
+    # (X1 variants 2, 3 and X2 variants 8, 9 stage their stencils with TMA)
+    for d, nv in ((0, 5), (1, 10)):
         for v in range(nv):
             a.setFaceVariant(d, v)
             div, flux = a.computeDivOfFluxes(P)
             assert same(div, ref_div, 1e-12) and same(flux, ref_flux, 1e-14), (d, v)
         a.setFaceVariant(d, 0)
     with pytest.raises(Exception):
-        a.setFaceVariant(1, 8)
+        a.setFaceVariant(1, 10)
+
+
+@pytest.mark.parametrize("mode", [C.NEWTON_PARITY_FD64, C.NEWTON_MIXED32])
+def test_face_variants_3d(mode):
+    """3D grid with room for every tensor-map box (N1T = 46 >= 40 zones
+    along i, N2T = N3T = 22 >= 12 along j and k): every X1, X2 and X3 face
+    variant, the TMA-staged ones included, gives the default's fluxes --
+    bit for bit in the FP64 parity unit, to roundoff (1e-14 of each
+    variable's scale) in the fast unit."""
+    cfg = PR.fast_mode_config(N=40, N3=16, dim=3)
+    P = _smooth_random(cfg, 11)
+    from grim_b200.timestepper import timeStepper
+    ts = timeStepper(cfg)
+    ts.setNewtonMode(mode, 1, 0.0)
+    exact = mode == C.NEWTON_PARITY_FD64
+    ref_div, ref_flux = ts.computeDivOfFluxes(P)
+    for d, nv in ((0, 5), (1, 10), (2, 10)):
+        for v in range(nv):
+            ts.setFaceVariant(d, v)
+            div, flux = ts.computeDivOfFluxes(P)
+            if exact:
+                assert np.array_equal(flux, ref_flux) and np.array_equal(div, ref_div), (d, v)
+            else:
+                scale = np.max(np.abs(ref_flux), axis=tuple(range(2, ref_flux.ndim)), keepdims=True) + 1e-300
+                assert np.max(np.abs(flux - ref_flux) / scale) <= 1e-14, (d, v)
+        ts.setFaceVariant(d, 0)
+    assert ts.stats()["nonFinite"] == 0
 
 
 def test_divb_matches_oracle_and_stays_at_roundoff():
