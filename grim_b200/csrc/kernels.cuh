@@ -84,25 +84,32 @@ static __global__ void k_ghost_fill(DevCfg c, double* __restrict__ prim, int nv)
 // ghost zones (corners included) take the wrapped interior value; ghost
 // zones on a non-periodic edge come back from the never-written local
 // vector, i.e. as zero.
-static __global__ void k_communicate(DevCfg c, double* __restrict__ prim, int nv) {
-  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (z >= c.Z) return;
-  int i, j, k;
-  zijk(c, z, i, j, k);
+// the zone communicate reads for zone (i, j, k): itself inside, the wrapped
+// interior zone across a periodic edge; zero is set on a non-periodic edge
+GRIM_D long long comm_source(const DevCfg& c, int i, int j, int k, bool& zero) {
   const bool p1 = c.bc[0] == GRIM_PERIODIC || c.bc[1] == GRIM_PERIODIC;
   const bool p2 = c.bc[2] == GRIM_PERIODIC || c.bc[3] == GRIM_PERIODIC;
   const bool p3 = c.bc[4] == GRIM_PERIODIC || c.bc[5] == GRIM_PERIODIC;
-  bool zero = false;
+  zero = false;
   auto m = [&](int x, int g, int N, bool per) -> int {
     if (x >= g && x < N + g) return x;
     if (!per) { zero = true; return x; }
     return g + ((x - g) % N + N) % N;
   };
-  int si = m(i, c.g1, c.N1, p1);
-  int sj = (c.dim >= 2) ? m(j, c.g2, c.N2, p2) : j;
-  int sk = (c.dim >= 3) ? m(k, c.g3, c.N3, p3) : k;
-  if (!zero && si == i && sj == j && sk == k) return;
-  long long s = zidx(c, si, sj, sk);
+  const int si = m(i, c.g1, c.N1, p1);
+  const int sj = (c.dim >= 2) ? m(j, c.g2, c.N2, p2) : j;
+  const int sk = (c.dim >= 3) ? m(k, c.g3, c.N3, p3) : k;
+  return zidx(c, si, sj, sk);
+}
+
+static __global__ void k_communicate(DevCfg c, double* __restrict__ prim, int nv) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  bool zero;
+  const long long s = comm_source(c, i, j, k, zero);
+  if (!zero && s == z) return;
   for (int v = 0; v < nv; v++) prim[(long long)v * c.Z + z] = zero ? 0. : prim[(long long)v * c.Z + s];
 }
 
@@ -358,7 +365,7 @@ GRIM_D void tma_load_4d(void* dst, const CUtensorMap* map, unsigned long long* b
       : "memory");
 }
 
-template <int COND, int VISC, int MINB>
+template <int COND, int VISC, int MINB, int RS>
 __global__ void __launch_bounds__(128, MINB) k_face_flux_x1_tma(const __grid_constant__ CUtensorMap tmap, DevCfg c,
                                                                  const double* __restrict__ geoF,
                                                                  double* __restrict__ flux, DevState* st) {
@@ -421,10 +428,7 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1_tma(const __grid_con
 #pragma unroll
     for (int v = 0; v < DOF; v++) {
       const double* a = rb + v * kX1Box + (iu - x0);
-      if (kFastMath)
-        recon_faces_fast(c.reconstruction, c.theta, a[-2], a[-1], a[0], a[1], a[2], lo[v], ro[v]);
-      else
-        recon_faces(c.reconstruction, c.theta, a[-2], a[-1], a[0], a[1], a[2], lo[v], ro[v]);
+      recon_faces_rs<RS, kFastMath>(c.reconstruction, c.theta, a[-2], a[-1], a[0], a[1], a[2], lo[v], ro[v]);
     }
     __syncwarp();  // the buffer is read; it may be refilled two items on
     double pl[DOF];
@@ -448,7 +452,7 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1_tma(const __grid_con
 // box is (4, 12, 1, dof) for X2 and (4, 1, 12, dof) for X3; x starts at 4q
 // (32-byte aligned) and the box along DIR at 7 x chunk (never negative).
 constexpr int kStripRows = 12;
-template <int COND, int VISC, int MINB, int DIR>
+template <int COND, int VISC, int MINB, int DIR, int RS>
 __global__ void __launch_bounds__(128, MINB) k_face_flux_strip_tma(const __grid_constant__ CUtensorMap tmap, DevCfg c,
                                                                     const double* __restrict__ geoF,
                                                                     const double* __restrict__ geoC,
@@ -519,10 +523,8 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_strip_tma(const __grid_
 #pragma unroll
     for (int v = 0; v < DOF; v++) {
       const double* a = rb + (v * kStripRows + jj) * QI + ii;  // rows jj .. jj+4 hold x-2 .. x+2
-      if (kFastMath)
-        recon_faces_fast(c.reconstruction, c.theta, a[0], a[QI], a[2 * QI], a[3 * QI], a[4 * QI], lo[v], ro[v]);
-      else
-        recon_faces(c.reconstruction, c.theta, a[0], a[QI], a[2 * QI], a[3 * QI], a[4 * QI], lo[v], ro[v]);
+      recon_faces_rs<RS, kFastMath>(c.reconstruction, c.theta, a[0], a[QI], a[2 * QI], a[3 * QI], a[4 * QI], lo[v],
+                                    ro[v]);
     }
     __syncwarp();  // the buffer is read; it may be refilled two items on
     double pl[DOF];
@@ -929,6 +931,40 @@ GRIM_D void atomic_max_pos(double* addr, double v) {
   atomicMax((unsigned long long*)addr, (unsigned long long)__double_as_longlong(v));
 }
 
+// one zone's sum over directions of max(c_max/dX_d, |c_min/dX_d|)
+template <int COND, int VISC>
+GRIM_D double zone_inv_dt(const DevCfg& c, const double* pv, const ZoneGeo<double>& G) {
+  ElemT<double, double> e;
+  elem_of<COND, VISC>(e, c, pv, G);
+  double acc = 0.;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    if (d < c.dim) {
+      double mn, mx;
+      char_speeds<COND, VISC>(e, G, d, c, mn, mx);
+      double a = mn / c.dX[d], bb = mx / c.dX[d];
+      double m2 = fmax(bb, fabs(a));
+      acc = (d == 0) ? m2 : acc + m2;
+    }
+  }
+  return acc;
+}
+
+// block reduction of the threads' values, then one atomic max per block
+// (every thread of the block calls it)
+GRIM_D void block_max_to(double best, double* out) {
+  __shared__ double sm[32];
+  for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sm[w] = best;
+  __syncthreads();
+  if (w == 0) {
+    best = (lane < (int)(blockDim.x >> 5)) ? sm[lane] : 0.;
+    for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if (lane == 0) atomic_max_pos(out, best);
+  }
+}
+
 template <int COND, int VISC>
 __global__ void k_dt_speeds(DevCfg c, const double* __restrict__ p, const double* __restrict__ geoC,
                                      int mode, DevState* st) {
@@ -939,20 +975,7 @@ __global__ void k_dt_speeds(DevCfg c, const double* __restrict__ p, const double
     zijk(c, z, i, j, k);
     long long src = z;
     bool zero = (mode == 2);
-    if (mode == 1) {
-      auto m = [&](int x, int g, int N, bool per) -> int {
-        if (x >= g && x < N + g) return x;
-        if (!per) { zero = true; return x; }
-        return g + ((x - g) % N + N) % N;
-      };
-      const bool p1 = c.bc[0] == GRIM_PERIODIC || c.bc[1] == GRIM_PERIODIC;
-      const bool p2 = c.bc[2] == GRIM_PERIODIC || c.bc[3] == GRIM_PERIODIC;
-      const bool p3 = c.bc[4] == GRIM_PERIODIC || c.bc[5] == GRIM_PERIODIC;
-      int si = m(i, c.g1, c.N1, p1);
-      int sj = (c.dim >= 2) ? m(j, c.g2, c.N2, p2) : j;
-      int sk = (c.dim >= 3) ? m(k, c.g3, c.N3, p3) : k;
-      src = zidx(c, si, sj, sk);
-    }
+    if (mode == 1) src = comm_source(c, i, j, k, zero);
     const long long Z = c.Z;
     constexpr int NF = 5 + COND + VISC, DOF = NF + 3;
     double pv[DOF];
@@ -960,32 +983,63 @@ __global__ void k_dt_speeds(DevCfg c, const double* __restrict__ p, const double
     for (int v = 0; v < DOF; v++) pv[v] = zero ? 0. : p[(long long)v * Z + src];
     ZoneGeo<double> G;
     load_geo(G, c, geoC, z, i, j, 0.5, 0.5);
-    ElemT<double, double> e;
-    elem_set<COND, VISC>(e, pv[0], pv[1], pv[2], pv[3], pv[4], pv[NF], pv[NF + 1], pv[NF + 2],
-                         COND ? pv[5] : 0., VISC ? pv[5 + COND] : 0., G, c);
-    double acc = 0.;
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      if (d < c.dim) {
-        double mn, mx;
-        char_speeds<COND, VISC>(e, G, d, c, mn, mx);
-        double a = mn / c.dX[d], bb = mx / c.dX[d];
-        double m2 = fmax(bb, fabs(a));
-        acc = (d == 0) ? m2 : acc + m2;
-      }
-    }
-    best = acc;
+    best = zone_inv_dt<COND, VISC>(c, pv, G);
   }
-  // block reduction then one atomic per block
-  __shared__ double sm[32];
-  for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) sm[w] = best;
-  __syncthreads();
-  if (w == 0) {
-    best = (lane < (int)(blockDim.x >> 5)) ? sm[lane] : 0.;
-    for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
-    if (lane == 0) atomic_max_pos(&st->maxInvDt, best);
+  block_max_to(best, &st->maxInvDt);
+}
+
+// The end of a stage in one pass over the grid: the Newton result src is
+// copied into the stage's array dst with grid::communicate's ghost values
+// (timestep.cpp: primHalfStep / primOld = prim, then communicate;
+// grid.cpp:306-360), then per zone
+//   FLOOR: the torus floors (halfStepDiagnostics / fullStepDiagnostics,
+//          torus/problem.cpp:714-746; with POST the NaN reset first),
+//   POST:  after the full step, the zone's term of the next computeDt from
+//          the stored result (all zones, as k_dt_speeds mode 0; when
+//          dtOn) and the non-finite count over the interior.
+// Every step of the reference's sequence acts on one zone at a time, so the
+// fused pass gives the same values (the NaN flag is counted beforehand over
+// the interior of src, which the copy leaves unchanged).
+template <int COND, int VISC, bool FLOOR, bool POST>
+__global__ void __launch_bounds__(128) k_stage_finish(DevCfg c, TorusCfg t, const double* __restrict__ src,
+                                                      double* __restrict__ dst, const double* __restrict__ geoC,
+                                                      const unsigned long long* nanFlag, int dtOn, DevState* st) {
+  constexpr int DOF = 8 + COND + VISC;
+  const long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long Z = c.Z;
+  double best = 0.;
+  int bad = 0;
+  if (z < Z) {
+    int i, j, k;
+    zijk(c, z, i, j, k);
+    bool zero;
+    const long long s = comm_source(c, i, j, k, zero);
+    double q[DOF];
+#pragma unroll
+    for (int v = 0; v < DOF; v++) q[v] = zero ? 0. : src[(long long)v * Z + s];
+    ZoneGeo<double> G;
+    load_geo(G, c, geoC, z, i, j, 0.5, 0.5);
+    if constexpr (FLOOR) {
+      const long long gz = gidx(c, i, j);
+      torus_floor_zone<COND, VISC>(c, t, q, G, __ldg(geoC + 37LL * c.GZ + gz), __ldg(geoC + 38LL * c.GZ + gz),
+                                   POST && *nanFlag != 0);
+    }
+#pragma unroll
+    for (int v = 0; v < DOF; v++) dst[(long long)v * Z + z] = q[v];
+    if constexpr (POST) {
+      if (dtOn) best = zone_inv_dt<COND, VISC>(c, q, G);
+      const bool inside = i >= c.g1 && i < c.N1 + c.g1 && j >= c.g2 && j < c.N2 + c.g2 && k >= c.g3 &&
+                          k < c.N3 + c.g3;
+      if (inside)
+#pragma unroll
+        for (int v = 0; v < DOF; v++)
+          if (!isfinite(q[v])) bad = 1;
+    }
+  }
+  if constexpr (POST) {
+    block_max_to(best, &st->maxInvDt);
+    bad = __syncthreads_count(bad);
+    if (threadIdx.x == 0 && bad) atomicAdd(&st->nonFinite, (unsigned long long)bad);
   }
 }
 
@@ -1848,37 +1902,61 @@ static int sm_count() {
   }
   return n;
 }
-template <int C, int V, int MINB>
-static void face_x1_tma_launch(const DevCfg& c, const CUtensorMap* tmap, const double* geoF, double* flux,
-                               DevState* st, cudaStream_t s) {
+template <int C, int V, int MINB, int RS>
+static void face_x1_tma_launch_rs(const DevCfg& c, const CUtensorMap* tmap, const double* geoF, double* flux,
+                                  DevState* st, cudaStream_t s) {
   constexpr int DOF = 8 + C + V;
   const int nw = 4;
   const size_t smem = ((size_t)nw * 2 * DOF * kX1Box + 3 * DOF * 128) * sizeof(double) + 2 * nw * 8;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_face_flux_x1_tma<C, V, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_face_flux_x1_tma<C, V, MINB, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr = true;
   }
-  k_face_flux_x1_tma<C, V, MINB><<<sm_count() * MINB, 32 * nw, smem, s>>>(*tmap, c, geoF, flux, st);
+  k_face_flux_x1_tma<C, V, MINB, RS><<<sm_count() * MINB, 32 * nw, smem, s>>>(*tmap, c, geoF, flux, st);
 }
+// the reconstruction scheme becomes a compile-time constant of the TMA
+// kernels: one scheme's code per kernel keeps the instruction footprint small
 template <int C, int V, int MINB>
-static void face_strip_tma_launch(const DevCfg& c, int dir, const CUtensorMap* tmap, const double* geoF,
-                                  const double* geoC, double* flux, DevState* st, cudaStream_t s) {
+static void face_x1_tma_launch(const DevCfg& c, const CUtensorMap* tmap, const double* geoF, double* flux,
+                               DevState* st, cudaStream_t s) {
+  switch (c.reconstruction) {
+    case GRIM_WENO5: face_x1_tma_launch_rs<C, V, MINB, GRIM_WENO5>(c, tmap, geoF, flux, st, s); break;
+    case GRIM_PPM: face_x1_tma_launch_rs<C, V, MINB, GRIM_PPM>(c, tmap, geoF, flux, st, s); break;
+    case GRIM_MP5: face_x1_tma_launch_rs<C, V, MINB, GRIM_MP5>(c, tmap, geoF, flux, st, s); break;
+    default: face_x1_tma_launch_rs<C, V, MINB, GRIM_MINMOD>(c, tmap, geoF, flux, st, s); break;
+  }
+}
+template <int C, int V, int MINB, int RS>
+static void face_strip_tma_launch_rs(const DevCfg& c, int dir, const CUtensorMap* tmap, const double* geoF,
+                                     const double* geoC, double* flux, DevState* st, cudaStream_t s) {
   constexpr int DOF = 8 + C + V;
   const int nw = 4;
   const size_t smem = ((size_t)nw * 2 * 4 * kStripRows * DOF + 3 * DOF * 128) * sizeof(double) + 2 * nw * 8;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_face_flux_strip_tma<C, V, MINB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_face_flux_strip_tma<C, V, MINB, 1, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    cudaFuncSetAttribute(k_face_flux_strip_tma<C, V, MINB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_face_flux_strip_tma<C, V, MINB, 2, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
     attr = true;
   }
   if (dir == 1)
-    k_face_flux_strip_tma<C, V, MINB, 1><<<sm_count() * MINB, 32 * nw, smem, s>>>(tmap[1], c, geoF, geoC, flux, st);
+    k_face_flux_strip_tma<C, V, MINB, 1, RS>
+        <<<sm_count() * MINB, 32 * nw, smem, s>>>(tmap[1], c, geoF, geoC, flux, st);
   else
-    k_face_flux_strip_tma<C, V, MINB, 2><<<sm_count() * MINB, 32 * nw, smem, s>>>(tmap[2], c, geoF, geoC, flux, st);
+    k_face_flux_strip_tma<C, V, MINB, 2, RS>
+        <<<sm_count() * MINB, 32 * nw, smem, s>>>(tmap[2], c, geoF, geoC, flux, st);
+}
+template <int C, int V, int MINB>
+static void face_strip_tma_launch(const DevCfg& c, int dir, const CUtensorMap* tmap, const double* geoF,
+                                  const double* geoC, double* flux, DevState* st, cudaStream_t s) {
+  switch (c.reconstruction) {
+    case GRIM_WENO5: face_strip_tma_launch_rs<C, V, MINB, GRIM_WENO5>(c, dir, tmap, geoF, geoC, flux, st, s); break;
+    case GRIM_PPM: face_strip_tma_launch_rs<C, V, MINB, GRIM_PPM>(c, dir, tmap, geoF, geoC, flux, st, s); break;
+    case GRIM_MP5: face_strip_tma_launch_rs<C, V, MINB, GRIM_MP5>(c, dir, tmap, geoF, geoC, flux, st, s); break;
+    default: face_strip_tma_launch_rs<C, V, MINB, GRIM_MINMOD>(c, dir, tmap, geoF, geoC, flux, st, s); break;
+  }
 }
 template <int C, int V>
 static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,
@@ -2102,6 +2180,24 @@ static void torus_floor_t(const DevCfg& c, double* p, const double* geoC, const 
 }
 void torus_floor(const DevCfg& c, double* p, const double* geoC, const unsigned long long* flag, cudaStream_t s) {
   GRIM_EMHD_DISPATCH(c, torus_floor_t, c, p, geoC, flag, s);
+}
+template <int C, int V>
+static void stage_finish_t(const DevCfg& c, const double* src, double* dst, const double* geoC, bool floors,
+                           bool post, const unsigned long long* nanFlag, int dtOn, DevState* st, cudaStream_t s) {
+  const TorusCfg t = torus_cfg(c);
+  const unsigned nb = (unsigned)nblk(c.Z, 128);
+  if (floors && post)
+    k_stage_finish<C, V, true, true><<<nb, 128, 0, s>>>(c, t, src, dst, geoC, nanFlag, dtOn, st);
+  else if (floors)
+    k_stage_finish<C, V, true, false><<<nb, 128, 0, s>>>(c, t, src, dst, geoC, nanFlag, dtOn, st);
+  else if (post)
+    k_stage_finish<C, V, false, true><<<nb, 128, 0, s>>>(c, t, src, dst, geoC, nanFlag, dtOn, st);
+  else
+    k_stage_finish<C, V, false, false><<<nb, 128, 0, s>>>(c, t, src, dst, geoC, nanFlag, dtOn, st);
+}
+void stage_finish(const DevCfg& c, const double* src, double* dst, const double* geoC, bool floors, bool post,
+                  const unsigned long long* nanFlag, int dtOn, DevState* st, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, stage_finish_t, c, src, dst, geoC, floors, post, nanFlag, dtOn, st, s);
 }
 void torus_nan_flag(const DevCfg& c, const double* p, unsigned long long* flag, cudaStream_t s) {
   k_nan_flag<<<nblk(c.Zint, 256), 256, 0, s>>>(c, p, flag);

@@ -37,6 +37,9 @@
   void torus_floor(const DevCfg& c, double* p, const double* geoC, const unsigned long long* flag,     \
                    cudaStream_t s);                                                                     \
   void torus_nan_flag(const DevCfg& c, const double* p, unsigned long long* flag, cudaStream_t s);      \
+  void stage_finish(const DevCfg& c, const double* src, double* dst, const double* geoC, bool floors,   \
+                    bool post, const unsigned long long* nanFlag, int dtOn, DevState* st,               \
+                    cudaStream_t s);                                                                    \
   void torus_bcs(const DevCfg& c, double* p, const double* geoC, cudaStream_t s);                      \
   }                                                                                                     \
   }

@@ -180,6 +180,26 @@ GRIM_D void recon_faces_fast(int scheme, double theta, S y0, S y1, S y2, S y3, S
   recon_faces(scheme, theta, y0, y1, y2, y3, y4, lo, ro);
 }
 
+// face values with the scheme fixed at compile time (RS >= 0: one scheme's
+// code in the kernel) or read at run time (RS < 0); FAST selects the
+// reassociated WENO5 weights
+template <int RS, bool FAST, class S>
+GRIM_D void recon_faces_rs(int scheme, double theta, S y0, S y1, S y2, S y3, S y4, S& lo, S& ro) {
+  if constexpr (RS < 0) {
+    if constexpr (FAST)
+      recon_faces_fast(scheme, theta, y0, y1, y2, y3, y4, lo, ro);
+    else
+      recon_faces(scheme, theta, y0, y1, y2, y3, y4, lo, ro);
+  } else if constexpr (RS == GRIM_WENO5) {
+    if constexpr (FAST)
+      weno5_faces_fast(y0, y1, y2, y3, y4, lo, ro);
+    else
+      weno5_faces(y0, y1, y2, y3, y4, lo, ro);
+  } else {
+    recon_faces(RS, theta, y0, y1, y2, y3, y4, lo, ro);  // a constant scheme folds the switch
+  }
+}
+
 // the slope() used by the EMHD gradients (reconstruction.cpp:39-64); MP5
 // uses the centred 5-point derivative
 template <class S>

@@ -337,13 +337,6 @@ static void enqueue_problem_bcs(grim_handle* h, double* p) {
   KNS_CALL(h, torus_bcs, h->dc, p, h->geo[GRIM_CENTER], h->stream);
   g_launch_counter += 2;
 }
-// halfStepDiagnostics: torus floors on primHalfStep (torus/problem.cpp:714-717)
-static void enqueue_half_diagnostics(grim_handle* h) {
-  if (h->cfg.problem != GRIM_PROBLEM_TORUS) return;
-  PROF(GRIM_PROF_DIAGNOSTICS);
-  KNS_CALL(h, torus_floor, h->dc, h->primHalf, h->geo[GRIM_CENTER], nullptr, h->stream);
-  g_launch_counter++;
-}
 // fullStepDiagnostics: NaN reset + floors on primOld (torus/problem.cpp:719-746)
 static void enqueue_full_diagnostics(grim_handle* h) {
   if (h->cfg.problem != GRIM_PROBLEM_TORUS) return;
@@ -384,20 +377,17 @@ static void enqueue_pre_half(grim_handle* h, bool timed) {
   if (timed) cudaEventRecord(h->ev[1], s);
 }
 
+// primHalfStep = prim, communicate, halfStepDiagnostics as one pass
 static void enqueue_mid(grim_handle* h) {
   const DevCfg& c = h->dc;
   cudaStream_t s = h->stream;
-  const size_t bytes = (size_t)c.dof * c.Z * sizeof(double);
   {
     PROF(GRIM_PROF_COPY);
-    cudaMemcpyAsync(h->primHalf, h->prim, bytes, cudaMemcpyDeviceToDevice, s);
-  }
-  {
-    PROF(GRIM_PROF_BOUNDARY);
-    KNS_CALL(h, communicate, c, h->primHalf, c.dof, s);
+    const bool torus = h->cfg.problem == GRIM_PROBLEM_TORUS;
+    const double* geoC = h->cfg.metric == GRIM_MINKOWSKI ? nullptr : h->geo[GRIM_CENTER];
+    KNS_CALL(h, stage_finish, c, h->prim, h->primHalf, geoC, torus, false, nullptr, 0, h->st, s);
     g_launch_counter++;
   }
-  enqueue_half_diagnostics(h);
   // ---- full stage
   {
     PROF(GRIM_PROF_BOUNDARY);
@@ -407,31 +397,33 @@ static void enqueue_mid(grim_handle* h) {
   enqueue_problem_bcs(h, h->primHalf);
 }
 
+// primOld = prim, communicate, fullStepDiagnostics (torus: NaN reset and
+// floors), the next computeDt's speeds when the element is re-set from the
+// full step (linear_modes/problem.cpp:287) and the non-finite count, as one
+// pass after the NaN count
 static void enqueue_post(grim_handle* h, bool timed) {
   const DevCfg& c = h->dc;
   cudaStream_t s = h->stream;
-  const size_t bytes = (size_t)c.dof * c.Z * sizeof(double);
-  {
-    PROF(GRIM_PROF_COPY);
-    cudaMemcpyAsync(h->primOld, h->prim, bytes, cudaMemcpyDeviceToDevice, s);
-  }
-  {
-    PROF(GRIM_PROF_BOUNDARY);
-    KNS_CALL(h, communicate, c, h->primOld, c.dof, s);
-    g_launch_counter++;
-  }
   {
     PROF(GRIM_PROF_DT);
     grim::exact::advance_time(h->st, s);
     g_launch_counter++;
   }
-  enqueue_full_diagnostics(h);
-  // fullStepDiagnostics re-setting elemOld (linear_modes/problem.cpp:287)
-  // on the communicated primOld
-  if (h->cfg.elemOldFromFullStep) enqueue_dt_speeds(h, h->primOld, 0);
+  const bool torus = h->cfg.problem == GRIM_PROBLEM_TORUS;
   {
     PROF(GRIM_PROF_DIAGNOSTICS);
-    KNS_CALL(h, count_nonfinite, c, h->primOld, h->st, s);
+    if (torus) {
+      cudaMemsetAsync(&h->st->nanFlag, 0, sizeof(unsigned long long), s);
+      KNS_CALL(h, torus_nan_flag, c, h->prim, &h->st->nanFlag, s);
+      g_launch_counter++;
+    }
+  }
+  {
+    PROF(GRIM_PROF_COPY);
+    const int dtOn = h->cfg.elemOldFromFullStep ? 1 : 0;
+    if (dtOn) cudaMemsetAsync(&h->st->maxInvDt, 0, sizeof(double), s);
+    const double* geoC = h->cfg.metric == GRIM_MINKOWSKI ? nullptr : h->geo[GRIM_CENTER];
+    KNS_CALL(h, stage_finish, c, h->prim, h->primOld, geoC, torus, true, &h->st->nanFlag, dtOn, h->st, s);
     g_launch_counter++;
   }
   if (timed) cudaEventRecord(h->ev[7], s);

@@ -25,53 +25,51 @@ GRIM_D void load_elem(ElemT<double, double>& e, const DevCfg& c, const double* p
                        COND ? p[(long long)c.Q * Z + z] : 0., VISC ? p[(long long)c.DP * Z + z] : 0., G, c);
 }
 
-// applyFloor (problem.cpp:542-712) on every zone, after the NaN reset
+// the element of one zone's primitives q (rows: fluid, then B1..B3)
 template <int COND, int VISC>
-__global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, const double* __restrict__ geoC,
-                              const unsigned long long* nanFlag) {
-  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (z >= c.Z) return;
-  const long long Z = c.Z;
-  const long long gz = gidx(c, z);
-  ZoneGeo<double> G;
-  geo_load<double>(G, geoC, c.GZ, gz);
-  // compile-time row count and indices keep the pointer table in registers
+GRIM_D void elem_of(ElemT<double, double>& e, const DevCfg& c, const double* q, const ZoneGeo<double>& G) {
+  constexpr int NFT = 5 + COND + VISC;
+  elem_set<COND, VISC>(e, q[RHO], q[UU], q[U1], q[U2], q[U3], q[NFT], q[NFT + 1], q[NFT + 2], COND ? q[5] : 0.,
+                       VISC ? q[5 + COND] : 0., G, c);
+}
+
+// applyFloor (problem.cpp:542-712) on one zone's primitives q, held in
+// registers, after the NaN reset of fullStepDiagnostics when nanReset;
+// minRho, minU are the zone's floor values (geometry words 37, 38)
+template <int COND, int VISC>
+GRIM_D void torus_floor_zone(const DevCfg& c, const TorusCfg& t, double* q, const ZoneGeo<double>& G, double minRho,
+                             double minU, bool nanReset) {
   constexpr int NFT = 5 + COND + VISC, DOFT = NFT + 3;
-  double* pv[DOFT];
-#pragma unroll
-  for (int v = 0; v < DOFT; v++) pv[v] = p + (long long)v * Z + z;
-  if (nanFlag && *nanFlag) {
+  if (nanReset) {
     bool bad = false;
 #pragma unroll
-    for (int v = 0; v < DOFT; v++) bad |= isnan(*pv[v]);
+    for (int v = 0; v < DOFT; v++) bad |= isnan(q[v]);
     if (bad)
 #pragma unroll
-      for (int v = 0; v < DOFT; v++) *pv[v] = 0.;
+      for (int v = 0; v < DOFT; v++) q[v] = 0.;
   }
-  const double minRho = __ldg(geoC + 37LL * c.GZ + gz);
-  const double minU = __ldg(geoC + 38LL * c.GZ + gz);
-  const double rho_pre = *pv[RHO] * 1., u_pre = *pv[UU] * 1.;
+  const double rho_pre = q[RHO] * 1., u_pre = q[UU] * 1.;
   bool usefloor = false;
   {
-    bool cd = *pv[RHO] < minRho;
+    bool cd = q[RHO] < minRho;
     usefloor = cd;
-    if (cd) *pv[RHO] = minRho;
-    cd = *pv[UU] < minU;
+    if (cd) q[RHO] = minRho;
+    cd = q[UU] < minU;
     usefloor = usefloor || cd;
-    if (cd) *pv[UU] = minU;
+    if (cd) q[UU] = minU;
   }
   ElemT<double, double> e;
-  load_elem<COND, VISC>(e, c, p, z, G);
+  elem_of<COND, VISC>(e, c, q, G);
   const double bSqr1 = e.bSqr;
   {
-    bool cd = bSqr1 > t.BsqrOverRhoMax * *pv[RHO];
+    bool cd = bSqr1 > t.BsqrOverRhoMax * q[RHO];
     usefloor = usefloor || cd;
-    if (cd) *pv[RHO] = bSqr1 / t.BsqrOverRhoMax;
-    cd = bSqr1 > t.BsqrOverUMax * *pv[UU];
+    if (cd) q[RHO] = bSqr1 / t.BsqrOverRhoMax;
+    cd = bSqr1 > t.BsqrOverUMax * q[UU];
     usefloor = usefloor || cd;
-    if (cd) *pv[UU] = bSqr1 / t.BsqrOverUMax;
+    if (cd) q[UU] = bSqr1 / t.BsqrOverUMax;
   }
-  const double rho = *pv[RHO], u = *pv[UU];
+  const double rho = q[RHO], u = q[UU];
   double trans = fmax(fmin(1., (bSqr1 - 0.1 * rho) / rho), 0.) * (usefloor ? 1. : 0.);
 #ifdef GRIM_FAST_MATH
   // the fix below blends with weight trans: with trans = 0 it returns the
@@ -90,7 +88,7 @@ __global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, cons
   double ucondr[4];
 #pragma unroll
   for (int m = 0; m < 4; m++) ucondr[m] = gamma * (e.uCon[m] + betapar * e.bCon[m]);
-  const double Bcon[4] = {0., *pv[NFT], *pv[NFT + 1], *pv[NFT + 2]};
+  const double Bcon[4] = {0., q[NFT], q[NFT + 1], q[NFT + 2]};
   double Bcov[4];
 #pragma unroll
   for (int m = 0; m < 4; m++) {
@@ -126,28 +124,28 @@ __global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, cons
 #pragma unroll
   for (int m = 1; m < 4; m++) {
     double utcon = ut * (vcon[m] - G.gcon[0][m] / G.gcon[0][0]);
-    *pv[UU + m] = *pv[UU + m] * (1. - trans) + trans * utcon;
+    q[UU + m] = q[UU + m] * (1. - trans) + trans * utcon;
   }
   }  // drift-frame fix
   // maximum Lorentz factor
-  load_elem<COND, VISC>(e, c, p, z, G);
+  elem_of<COND, VISC>(e, c, q, G);
   {
     const double lf2 = e.gam * e.gam;
     const double gm2 = t.MaxLorentzFactor * t.MaxLorentzFactor;
     if (lf2 > gm2) {
       double mf = 1. / sqrt(fmax((lf2 - 1.) / (gm2 - 1.), 1.));
-      *pv[U1] *= mf;
-      *pv[U2] *= mf;
-      *pv[U3] *= mf;
+      q[U1] *= mf;
+      q[U2] *= mf;
+      q[U3] *= mf;
     }
   }
   if (COND || VISC) {
-    load_elem<COND, VISC>(e, c, p, z, G);
+    elem_of<COND, VISC>(e, c, q, G);
     if (COND) {
       const double cs = e.soundSpeed;
-      const double Qmax = 1.07 * c.CondClosure * *pv[RHO] * pow(cs, 3.);
+      const double Qmax = 1.07 * c.CondClosure * q[RHO] * pow(cs, 3.);
       const double lim = fmax(fabs(e.q) / Qmax, 1.);
-      *pv[5] = *pv[5] / lim;
+      q[5] = q[5] / lim;
     }
     if (VISC) {
       const double pr = e.pressure, dP = e.deltaP, bs = e.bSqr;
@@ -155,9 +153,30 @@ __global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, cons
       const double dPmaxPlus = fmin(1.07 * c.ViscClosure * bs * 0.5 * dPmod, 1.49 * pr);
       const double dPmaxMinus = fmax(-1.07 * c.ViscClosure * bs, -2.99 * pr);
       const double f = (dP > 0.) ? 1. / fmax(dP / dPmaxPlus, 1.) : 1. / fmax(dP / dPmaxMinus, 1.);
-      *pv[5 + COND] = *pv[5 + COND] * f;
+      q[5 + COND] = q[5 + COND] * f;
     }
   }
+}
+
+// applyFloor on every zone of p in place, after the NaN reset when
+// *nanFlag is set
+template <int COND, int VISC>
+__global__ void k_torus_floor(DevCfg c, TorusCfg t, double* __restrict__ p, const double* __restrict__ geoC,
+                              const unsigned long long* nanFlag) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  const long long Z = c.Z;
+  const long long gz = gidx(c, z);
+  ZoneGeo<double> G;
+  geo_load<double>(G, geoC, c.GZ, gz);
+  constexpr int DOFT = 8 + COND + VISC;
+  double q[DOFT];
+#pragma unroll
+  for (int v = 0; v < DOFT; v++) q[v] = p[(long long)v * Z + z];
+  torus_floor_zone<COND, VISC>(c, t, q, G, __ldg(geoC + 37LL * c.GZ + gz), __ldg(geoC + 38LL * c.GZ + gz),
+                               nanFlag && *nanFlag);
+#pragma unroll
+  for (int v = 0; v < DOFT; v++) p[(long long)v * Z + z] = q[v];
 }
 
 // NaN count over the interior (fullStepDiagnostics, problem.cpp:725-733)

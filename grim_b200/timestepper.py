@@ -181,7 +181,7 @@ class timeStepper:
         return _lib.lib().grim_stream(self._h)
 
     PROF_GROUPS = ("boundary", "faces_x1", "faces_x2", "faces_x3", "epilogue", "newton", "dt",
-                   "diagnostics", "copy", "emhd_prepass")
+                   "diagnostics", "finish", "emhd_prepass")
 
     def profileSteps(self, nsteps=1):
         """Advance nsteps without the graph, timing every kernel group with

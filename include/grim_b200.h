@@ -226,8 +226,10 @@ enum {
   GRIM_PROF_EPILOGUE = 4,    /* CT EMFs, divergence, sources, induction, guess */
   GRIM_PROF_NEWTON = 5,      /* every Newton kernel of a stage */
   GRIM_PROF_DT = 6,          /* characteristic speeds, dt, time advance */
-  GRIM_PROF_DIAGNOSTICS = 7, /* floors, NaN reset, non-finite count */
-  GRIM_PROF_COPY = 8,        /* device-to-device state copies */
+  GRIM_PROF_DIAGNOSTICS = 7, /* floors, NaN reset / count (outside the stage finish) */
+  GRIM_PROF_COPY = 8,        /* stage finish: the state copy with communicate's ghosts,
+                                fused with the torus floors, the next dt's speeds and
+                                the non-finite count of the step */
   GRIM_PROF_EMHD_PREPASS = 9,
   GRIM_PROF_GROUPS = 10
 };
