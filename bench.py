@@ -524,6 +524,13 @@ def run_gpu(args, rank, world, local_rank):
         "speedup_vs_fd64": value / fd if fd else None,
         "newton_iters": st_fast["newtonIters"],
         "unconverged": st_fast["unconverged"],
+        # zones per Newton iteration count (index = updates taken), summed
+        # over the profiled steps, per stage
+        "newton_iteration_histogram": {
+            "fast": {"half": prof_fast["hist"][0][:cfg["maxNonLinearIter"] + 1],
+                     "full": prof_fast["hist"][1][:cfg["maxNonLinearIter"] + 1]},
+            "fd64": None if prof_fd is None else {"half": prof_fd["hist"][0][:cfg["maxNonLinearIter"] + 1],
+                                                  "full": prof_fd["hist"][1][:cfg["maxNonLinearIter"] + 1]}},
         "e2e": {"value": world * zones * e2e_steps / e2e_s, "unit": "zone-cycles/s",
                 "h2d_bytes_per_step": e2e_bytes, "d2h_bytes_per_step": e2e_bytes},
         "gpu_launches": int(st_fast["kernelLaunches"]) * args.steps,

@@ -677,7 +677,7 @@ static __global__ void k_stage_emf(DevCfg c, StageBufs b) {
 // blocks per SM each part is compiled for: the flux half is a memory
 // stream that wants warps in flight more than registers (measured on the
 // 3D torus: 64 registers with a few spills beat 85 and 98 without)
-constexpr int kEpiMinBlocks[3] = {4, 1, 8};
+constexpr int kEpiMinBlocks[3] = {4, 5, 8};
 template <int COND, int VISC, int PART>
 __global__ void __launch_bounds__(128, kEpiMinBlocks[PART]) k_stage_epilogue(DevCfg c, int stage, StageBufs b) {
   constexpr int NF = 5 + COND + VISC;
