@@ -71,6 +71,8 @@ def lib():
         "grim_compute_div_fluxes": [vp, vp, vp, vp, vp, i],
         "grim_reconstruct": [vp, vp, i, vp, vp, i],
         "grim_compute_divb": [vp, vp, vp, i],
+        "grim_torus_observers": [vp, P(d)],
+        "grim_get_observations": [vp, P(d), i, P(i)],
         "grim_conserved": [vp, vp, vp, i],
         "grim_char_speeds": [vp, vp, i, vp, vp, i],
         "grim_stage_setup": [vp, i],

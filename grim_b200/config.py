@@ -63,8 +63,9 @@ DOUBLE_FIELDS = [
     "closureTau0", "closureTau1",
     "MaxLorentzFactor", "RhoFloorAmpl", "UFloorAmpl", "RhoFloorSlope",
     "UFloorSlope", "BsqrOverRhoMax", "BsqrOverUMax",
+    "ObserveEveryDt",
 ]
-N_RESERVED_DOUBLE = 6
+N_RESERVED_DOUBLE = 5
 
 
 def _struct_fields():
@@ -111,6 +112,7 @@ def defaults():
         MaxLorentzFactor=10., RhoFloorAmpl=1e-3, UFloorAmpl=1e-5,
         RhoFloorSlope=-2.5, UFloorSlope=-2.5,
         BsqrOverRhoMax=10., BsqrOverUMax=500.,
+        ObserveEveryDt=0.,
     )
 
 

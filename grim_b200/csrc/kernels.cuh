@@ -1043,6 +1043,102 @@ __global__ void __launch_bounds__(128) k_stage_finish(DevCfg c, TorusCfg t, cons
   }
 }
 
+// ---------------------------------------------------------------------------
+// Torus observers (ObserversTorus.hpp:6-253, called by fullStepDiagnostics,
+// torus/problem.cpp:754-778): integrals and extrema over the interior of
+// primOld with the element of its final state at the zone centres, each
+// integrand in the reference's operation order.  Two launches: fixed-size
+// per-block partials (grid-stride over the interior, shuffle trees), then
+// one thread combines them in block order, so the sums are reproducible.
+// ---------------------------------------------------------------------------
+// ObserveData (problem.cpp:754): this step's time crossed a multiple of
+// every (every <= 0: always)
+GRIM_D bool obs_due(const DevState* st, double every) {
+  if (every <= 0.) return true;
+  return floor(st->time / every) != floor((st->time - st->dt) / every);
+}
+GRIM_D double obs_join(int v, double a, double b) {
+  return v == OBS_RHOMAX ? fmax(a, b) : (v == OBS_BETAMIN ? fmin(a, b) : a + b);
+}
+
+template <int COND, int VISC>
+__global__ void __launch_bounds__(256) k_torus_obs_partial(DevCfg c, const double* __restrict__ p,
+                                                           const double* __restrict__ geoC, double volElem,
+                                                           double every, const DevState* st,
+                                                           double* __restrict__ partials) {
+  if (!obs_due(st, every)) return;
+  constexpr int DOF = 8 + COND + VISC;
+  double acc[OBS_N];
+#pragma unroll
+  for (int v = 0; v < OBS_N; v++) acc[v] = 0.;
+  acc[OBS_RHOMAX] = -INFINITY;
+  acc[OBS_BETAMIN] = INFINITY;
+  const long long Z = c.Z;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < c.Zint;
+       n += (long long)gridDim.x * blockDim.x) {
+    const long long z = interior_to_z(c, n);
+    int i, j, k;
+    zijk(c, z, i, j, k);
+    double q[DOF];
+#pragma unroll
+    for (int v = 0; v < DOF; v++) q[v] = p[(long long)v * Z + z];
+    ZoneGeo<double> G;
+    load_geo(G, c, geoC, z, i, j, 0.5, 0.5);
+    ElemT<double, double> e;
+    elem_of<COND, VISC>(e, c, q, G);
+    const double rho = q[RHO], u = q[UU];
+    acc[OBS_MASS] += rho * volElem * G.g * e.gam / G.alpha;
+    acc[OBS_EMAG] += volElem * e.bSqr * G.g * e.gam / G.alpha;
+    acc[OBS_ETH] += volElem * u * G.g * e.gam / G.alpha;
+    acc[OBS_RHOMAX] = fmax(acc[OBS_RHOMAX], rho);
+    acc[OBS_BETAMIN] = fmin(acc[OBS_BETAMIN], 2. * (e.pressure + 1.e-13) / (e.bSqr + 1.e-18));
+    // boundary fluxes at the first and last interior X1 columns
+    const double mi = rho * volElem * G.g * e.uCon[1];
+    if (i == 3) acc[OBS_MDOT_IN] += mi;
+    if (i == c.N1 + 2) {
+      acc[OBS_MDOT_OUT] += mi;
+      const double bern = (1. + u / rho * c.Gam) * e.uCov[0];
+      const double unb = mi * ((bern < -1.) ? 1. : 0.);
+      acc[OBS_UNBOUND_OUT] += unb;
+      acc[OBS_REL_UNBOUND_OUT] += unb * ((e.gam > 2.) ? 1. : 0.);
+    }
+  }
+  __shared__ double sm[8][OBS_N];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int v = 0; v < OBS_N; v++) {
+    double a = acc[v];
+    for (int o = 16; o > 0; o >>= 1) a = obs_join(v, a, __shfl_xor_sync(0xffffffffu, a, o));
+    if (lane == 0) sm[w][v] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x < OBS_N) {
+    const int v = threadIdx.x;
+    double a = sm[0][v];
+    for (int ww = 1; ww < (int)(blockDim.x >> 5); ww++) a = obs_join(v, a, sm[ww][v]);
+    partials[(long long)blockIdx.x * OBS_N + v] = a;
+  }
+}
+
+// combines the partials in block order; writes out (OBS_N values) and, with
+// a history, appends the record {time, values} at ring slot obsCount % cap
+static __global__ void k_torus_obs_final(const double* __restrict__ partials, int nblocks, double every,
+                                         DevState* st, double* out, double* hist, int cap) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || !obs_due(st, every)) return;
+  double r[OBS_N];
+  for (int v = 0; v < OBS_N; v++) r[v] = partials[v];
+  for (int bk = 1; bk < nblocks; bk++)
+    for (int v = 0; v < OBS_N; v++) r[v] = obs_join(v, r[v], partials[(long long)bk * OBS_N + v]);
+  if (out)
+    for (int v = 0; v < OBS_N; v++) out[v] = r[v];
+  if (hist && cap > 0) {
+    double* rec = hist + (st->obsCount % (unsigned long long)cap) * (OBS_N + 1);
+    rec[0] = st->time;
+    for (int v = 0; v < OBS_N; v++) rec[1 + v] = r[v];
+    st->obsCount += 1;
+  }
+}
+
 // dt = Courant / maxInvDt, capped at maxDtIncrement * dt (timestep.cpp:393-399)
 static __global__ void k_dt_update(DevState* st, double courant, double maxInc) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -2198,6 +2294,16 @@ static void stage_finish_t(const DevCfg& c, const double* src, double* dst, cons
 void stage_finish(const DevCfg& c, const double* src, double* dst, const double* geoC, bool floors, bool post,
                   const unsigned long long* nanFlag, int dtOn, DevState* st, cudaStream_t s) {
   GRIM_EMHD_DISPATCH(c, stage_finish_t, c, src, dst, geoC, floors, post, nanFlag, dtOn, st, s);
+}
+template <int C, int V>
+static void torus_observe_t(const DevCfg& c, const double* p, const double* geoC, double volElem, double every,
+                            DevState* st, double* partials, double* out, double* hist, int cap, cudaStream_t s) {
+  k_torus_obs_partial<C, V><<<kObsBlocks, 256, 0, s>>>(c, p, geoC, volElem, every, st, partials);
+  k_torus_obs_final<<<1, 32, 0, s>>>(partials, kObsBlocks, every, st, out, hist, cap);
+}
+void torus_observe(const DevCfg& c, const double* p, const double* geoC, double volElem, double every, DevState* st,
+                   double* partials, double* out, double* hist, int cap, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, torus_observe_t, c, p, geoC, volElem, every, st, partials, out, hist, cap, s);
 }
 void torus_nan_flag(const DevCfg& c, const double* p, unsigned long long* flag, cudaStream_t s) {
   k_nan_flag<<<nblk(c.Zint, 256), 256, 0, s>>>(c, p, flag);

@@ -37,6 +37,8 @@
   void torus_floor(const DevCfg& c, double* p, const double* geoC, const unsigned long long* flag,     \
                    cudaStream_t s);                                                                     \
   void torus_nan_flag(const DevCfg& c, const double* p, unsigned long long* flag, cudaStream_t s);      \
+  void torus_observe(const DevCfg& c, const double* p, const double* geoC, double volElem, double every, \
+                     DevState* st, double* partials, double* out, double* hist, int cap, cudaStream_t s); \
   void stage_finish(const DevCfg& c, const double* src, double* dst, const double* geoC, bool floors,   \
                     bool post, const unsigned long long* nanFlag, int dtOn, DevState* st,               \
                     cudaStream_t s);                                                                    \

@@ -68,6 +68,10 @@ struct grim_handle {
   // geometry: per location 39 x Z (MKS only), centre Christoffels 64 x Z
   double* geo[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   double* gamma = nullptr;
+  // torus observers: per-block partials (kObsBlocks x OBS_N), one result
+  // (OBS_N) and the history ring (obsCap records of time + OBS_N values)
+  double* obs = nullptr;
+  int obsCap = 4096;
   DevState* st = nullptr;
   DevState* hst = nullptr;  // pinned mirror
   cudaEvent_t ev[8];
@@ -128,7 +132,7 @@ struct ProfScope {
 static void free_all(grim_handle* h) {
   double** bufs[] = {&h->primOld, &h->prim, &h->primHalf, &h->consOld, &h->divF, &h->Sexp, &h->R,
                      &h->l2, &h->uT, &h->emf, &h->flux[0], &h->flux[1], &h->flux[2], &h->scratch, &h->scratch2,
-                     &h->geo[0], &h->geo[1], &h->geo[2], &h->geo[3], &h->geo[4], &h->gamma};
+                     &h->geo[0], &h->geo[1], &h->geo[2], &h->geo[3], &h->geo[4], &h->gamma, &h->obs};
   for (double** b : bufs)
     if (*b) { cudaFree(*b); *b = nullptr; }
   if (h->st) { cudaFree(h->st); h->st = nullptr; }
@@ -397,6 +401,19 @@ static void enqueue_mid(grim_handle* h) {
   enqueue_problem_bcs(h, h->primHalf);
 }
 
+// the torus observers of primOld (ObserversTorus.hpp): into out (device,
+// OBS_N values) and / or, with toHistory, the handle's record ring
+static void enqueue_observers(grim_handle* h, double every, double* out, bool toHistory) {
+  const DevCfg& c = h->dc;
+  double volElem = c.dX[0];
+  if (c.dim > 1) volElem *= c.dX[1];
+  if (c.dim > 2) volElem *= c.dX[2];
+  const double* geoC = h->cfg.metric == GRIM_MINKOWSKI ? nullptr : h->geo[GRIM_CENTER];
+  double* hist = h->obs + (size_t)kObsBlocks * OBS_N + OBS_N;
+  grim::exact::torus_observe(c, h->primOld, geoC, volElem, every, h->st, h->obs, out,
+                             toHistory ? hist : nullptr, h->obsCap, h->stream);
+}
+
 // primOld = prim, communicate, fullStepDiagnostics (torus: NaN reset and
 // floors), the next computeDt's speeds when the element is re-set from the
 // full step (linear_modes/problem.cpp:287) and the non-finite count, as one
@@ -425,6 +442,13 @@ static void enqueue_post(grim_handle* h, bool timed) {
     const double* geoC = h->cfg.metric == GRIM_MINKOWSKI ? nullptr : h->geo[GRIM_CENTER];
     KNS_CALL(h, stage_finish, c, h->prim, h->primOld, geoC, torus, true, &h->st->nanFlag, dtOn, h->st, s);
     g_launch_counter++;
+  }
+  if (h->cfg.ObserveEveryDt > 0.) {
+    // on-the-fly observers of fullStepDiagnostics (problem.cpp:754-778): the
+    // kernels read time and dt on the device and do nothing between records
+    PROF(GRIM_PROF_DIAGNOSTICS);
+    enqueue_observers(h, h->cfg.ObserveEveryDt, nullptr, true);
+    g_launch_counter += 2;
   }
   if (timed) cudaEventRecord(h->ev[7], s);
 }
@@ -487,6 +511,11 @@ int grim_create(const grim_config* cfg, int device, grim_handle** out) {
     if (ok) ok = allocPlane(&h->gamma, 64);
   }
   for (int l = 0; ok && l < 2; l++) ok = cudaMalloc(&h->list[l], (size_t)c.Zint * sizeof(int)) == cudaSuccess;
+  if (ok) {
+    const size_t words = (size_t)kObsBlocks * OBS_N + OBS_N + (size_t)h->obsCap * (OBS_N + 1);
+    ok = cudaMalloc(&h->obs, words * sizeof(double)) == cudaSuccess &&
+         cudaMemset(h->obs, 0, words * sizeof(double)) == cudaSuccess;
+  }
   if (ok) ok = cudaMalloc(&h->st, sizeof(DevState)) == cudaSuccess;
   if (ok) ok = cudaMallocHost(&h->hst, sizeof(DevState)) == cudaSuccess;
   if (!ok) {
@@ -742,6 +771,40 @@ int grim_reconstruct(grim_handle* h, const double* prim, int dir, double* pl, do
   rc = stage_out(h, pl, dl, (size_t)c.dof * h->bytesZ, memKind);
   if (rc) return rc;
   return stage_out(h, pr, dr, (size_t)c.dof * h->bytesZ, memKind);
+}
+
+int grim_torus_observers(grim_handle* h, double* out) {
+  if (!h || !out) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  double* res = h->obs + (size_t)kObsBlocks * OBS_N;
+  enqueue_observers(h, 0., res, false);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, res, OBS_N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return GRIM_OK;
+}
+
+int grim_get_observations(grim_handle* h, double* out, int maxRecords, int* nRecords) {
+  if (!h || !nRecords || maxRecords < 0 || (maxRecords > 0 && !out)) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  unsigned long long count = 0;
+  CK(cudaMemcpyAsync(&count, &h->st->obsCount, sizeof(count), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  const unsigned long long cap = (unsigned long long)h->obsCap;
+  const unsigned long long kept = count < cap ? count : cap;
+  const unsigned long long n = kept < (unsigned long long)maxRecords ? kept : (unsigned long long)maxRecords;
+  const double* hist = h->obs + (size_t)kObsBlocks * OBS_N + OBS_N;
+  // the n most recent records, oldest first: at most two contiguous runs
+  // of the ring
+  const size_t rec = (OBS_N + 1) * sizeof(double);
+  const unsigned long long first = (count - n) % cap;
+  const unsigned long long run1 = (first + n <= cap) ? n : cap - first;
+  if (run1) CK(cudaMemcpyAsync(out, hist + first * (OBS_N + 1), run1 * rec, cudaMemcpyDeviceToHost, h->stream));
+  if (n > run1)
+    CK(cudaMemcpyAsync(out + run1 * (OBS_N + 1), hist, (n - run1) * rec, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  *nRecords = (int)n;
+  return GRIM_OK;
 }
 
 int grim_compute_divb(grim_handle* h, const double* prim, double* divB, int memKind) {

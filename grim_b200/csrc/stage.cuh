@@ -19,7 +19,15 @@ struct DevState {
   unsigned long long itHist[2][16];  // zones by Newton iterations used (fast path)
   unsigned long long listCount[2];   // compacted worklists: entries per ping-pong list
   unsigned long long waitTimeouts;   // bounded waits on asynchronous copies that gave up
+  unsigned long long obsCount;       // torus observer records written (ring index = count % capacity)
 };
+
+// the torus observers (ObserversTorus.hpp:6-253), in record order
+enum {
+  OBS_MASS = 0, OBS_EMAG, OBS_ETH, OBS_RHOMAX, OBS_BETAMIN, OBS_MDOT_IN, OBS_MDOT_OUT, OBS_UNBOUND_OUT,
+  OBS_REL_UNBOUND_OUT, OBS_N
+};
+constexpr int kObsBlocks = 296;  // fixed partial count: the sums' order does not depend on the launch
 
 struct StageBufs {
   const double* ps;       // prims the stage's fluxes are computed from

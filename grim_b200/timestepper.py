@@ -271,6 +271,29 @@ class timeStepper:
         _lib.check(_lib.lib().grim_compute_divb(self._h, _ptr(p), _ptr(out), _lib.HOST), "computeDivB")
         return out
 
+    OBSERVERS = ("BaryonMass", "EMag", "ETh", "rhoMax", "betaMin", "MdotIn", "MdotOut",
+                 "UnboundMdotOut", "RelativisticUnboundMdotOut")
+
+    def torusObservers(self):
+        """The torus observers (ComputeMinMaxVariables, ComputeEnergyIntegrals,
+        ComputeBoundaryFluxes of ObserversTorus.hpp) on primOld: {name: value}."""
+        out = (ctypes.c_double * 9)()
+        _lib.check(_lib.lib().grim_torus_observers(self._h, out), "torus_observers")
+        return dict(zip(self.OBSERVERS, list(out)))
+
+    def observations(self, maxRecords=4096):
+        """Records written by the steps when ObserveEveryDt > 0, oldest
+        first: [{"time": t, name: value, ...}]."""
+        buf = (ctypes.c_double * (10 * maxRecords))()
+        n = ctypes.c_int(0)
+        _lib.check(_lib.lib().grim_get_observations(self._h, buf, int(maxRecords), ctypes.byref(n)),
+                   "get_observations")
+        recs = []
+        for r in range(n.value):
+            row = buf[10 * r:10 * r + 10]
+            recs.append(dict(time=row[0], **dict(zip(self.OBSERVERS, row[1:]))))
+        return recs
+
     def reconstruct(self, prim, direction):
         p = np.ascontiguousarray(prim, dtype=np.float64)
         pl, pr = self._zeros(self.dof), self._zeros(self.dof)

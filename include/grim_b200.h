@@ -93,7 +93,9 @@ typedef struct grim_config {
   double closureTau0, closureTau1;
   double MaxLorentzFactor, RhoFloorAmpl, UFloorAmpl, RhoFloorSlope, UFloorSlope;
   double BsqrOverRhoMax, BsqrOverUMax;
-  double reserved_d[6];
+  double ObserveEveryDt;    /* > 0: record the torus observers whenever a step's
+                               time crosses a multiple of it (problem.cpp:754) */
+  double reserved_d[5];
 } grim_config;
 
 typedef struct grim_handle grim_handle;
@@ -136,6 +138,22 @@ int grim_time_step(grim_handle* h, int* numReads, int* numWrites);
 int grim_time_steps(grim_handle* h, int nsteps);
 int grim_get_time(grim_handle* h, double* time, double* dt);
 int grim_set_time(grim_handle* h, double time, double dt);
+
+/* ---- torus observers (ObserversTorus.hpp:6-253; fullStepDiagnostics,
+ *      torus/problem.cpp:754-778).  Nine values, in this order: baryon mass,
+ *      magnetic energy, thermal energy (integrals of rho, b^2, u times
+ *      dV sqrt(-g) gamma / alpha over the interior), rho max, plasma beta
+ *      min, mass flux through the first (MdotIn) and last (MdotOut) interior
+ *      X1 columns, and the unbound (Bernoulli < -1) and relativistic
+ *      unbound (also gamma > 2) parts of MdotOut.  The sums are combined in a
+ *      fixed order (reproducible run to run). ----------------------------- */
+/* now, on primOld; out[9] */
+int grim_torus_observers(grim_handle* h, double* out);
+/* the records written by grim_time_step when cfg.ObserveEveryDt > 0 (one per
+ * step whose time crosses a multiple of it), 10 doubles each: time, then
+ * the nine values.  The handle keeps the last 4096; out receives the most
+ * recent min(kept, maxRecords), oldest first; *nRecords their number. */
+int grim_get_observations(grim_handle* h, double* out, int maxRecords, int* nRecords);
 
 /* ---- stage pieces (timestepper.hpp:88-123) ---------------------------- */
 /* computeDt (timestep.cpp:336-400): updates dt from the current elemOld state */

@@ -1749,6 +1749,47 @@ int orc_compute_divb(orc_handle* h, const double* prim, double* divB) {
     divB[z] = (gB1[z] + a[z] - b[z] - c[z]) / (2. * s.dX[0]) + (gB2[z] + d[z] - e[z] - f[z]) / (2. * s.dX[1]);
   return 0;
 }
+/* The torus observers (ObserversTorus.hpp:6-253, called from
+ * fullStepDiagnostics, torus/problem.cpp:754-778) on primOld with its
+ * element at the zone centres; the integrands in the reference's operation
+ * order, summed zone by zone in index order.  out: baryon mass, magnetic
+ * energy, thermal energy, rho max, beta min, Mdot in (i = 3), Mdot out
+ * (i = N1 + 2), unbound and relativistic unbound Mdot out. */
+int orc_torus_observers(orc_handle* h, double* out) {
+  Stepper& s = h->s;
+  const Layout& L = s.L;
+  const long Z = L.Z;
+  const Geom& G = s.geomCenter;
+  Elem e; e.alloc(L, s.P); e.set(s.primOld, G);
+  double volElem = s.dX[0];
+  if (L.dim > 1) volElem *= s.dX[1];
+  if (L.dim > 2) volElem *= s.dX[2];
+  const double* rho = s.primOld.v(RHO);
+  const double* u = s.primOld.v(UU);
+  double mass = 0., emag = 0., eth = 0., rhoMax = -INFINITY, betaMin = INFINITY;
+  double mIn = 0., mOut = 0., unb = 0., rel = 0.;
+  for (long z = 0; z < Z; z++) {
+    if (!L.interior(z)) continue;
+    int i, j, k; L.ijk(z, i, j, k);
+    mass += rho[z] * volElem * G.g[z] * e.gammaLF[z] / G.alpha[z];
+    emag += volElem * e.bSqr[z] * G.g[z] * e.gammaLF[z] / G.alpha[z];
+    eth += volElem * u[z] * G.g[z] * e.gammaLF[z] / G.alpha[z];
+    rhoMax = std::max(rhoMax, rho[z]);
+    betaMin = std::min(betaMin, 2. * (e.pressure[z] + 1.e-13) / (e.bSqr[z] + 1.e-18));
+    const double mi = rho[z] * volElem * G.g[z] * e.uCon[1][z];
+    if (i == 3) mIn += mi;
+    if (i == L.N1 + 2) {
+      mOut += mi;
+      const double bern = (1. + u[z] / rho[z] * s.P.c.adiabaticIndex) * e.uCov[0][z];
+      const double ub = mi * ((bern < -1.) ? 1. : 0.);
+      unb += ub;
+      rel += ub * ((e.gammaLF[z] > 2.) ? 1. : 0.);
+    }
+  }
+  const double r[9] = {mass, emag, eth, rhoMax, betaMin, mIn, mOut, unb, rel};
+  for (int v = 0; v < 9; v++) out[v] = r[v];
+  return 0;
+}
 int orc_char_speeds(orc_handle* h, const double* prim, int dir, double* mn, double* mx) {
   Stepper& s = h->s;
   const long Z = s.L.Z; const int dof = s.P.dof;

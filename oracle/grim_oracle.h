@@ -51,7 +51,8 @@ typedef struct orc_config {
   double closureTau0, closureTau1;
   double MaxLorentzFactor, RhoFloorAmpl, UFloorAmpl, RhoFloorSlope, UFloorSlope;
   double BsqrOverRhoMax, BsqrOverUMax;
-  double reserved_d[6];
+  double ObserveEveryDt;
+  double reserved_d[5];
 } orc_config;
 
 typedef struct orc_handle orc_handle;
@@ -92,6 +93,9 @@ int  orc_reconstruct(orc_handle* h, const double* prim, int dir,
 /* conserved variables U = computeFluxes(0) of prim, dof x Z */
 int  orc_conserved(orc_handle* h, const double* prim, double* cons);
 int  orc_compute_divb(orc_handle* h, const double* prim, double* divB);
+/* torus observers on primOld: mass, EMag, ETh, rhoMax, betaMin, MdotIn,
+ * MdotOut, unbound and relativistic unbound MdotOut (9 values) */
+int  orc_torus_observers(orc_handle* h, double* out);
 /* characteristic speeds of prim at the centre in one direction */
 int  orc_char_speeds(orc_handle* h, const double* prim, int dir,
                      double* minSpeed, double* maxSpeed);

@@ -37,14 +37,14 @@ DOUBLE_FIELDS = [
     "nonlinearsolve_atol", "nonlinearsolve_rtol", "JacobianAssembleEpsilon",
     "linesearchfloor", "CourantFactor", "maxDtIncrement",
     "closureTau0", "closureTau1", "MaxLorentzFactor", "RhoFloorAmpl",
-    "UFloorAmpl", "RhoFloorSlope", "UFloorSlope", "BsqrOverRhoMax", "BsqrOverUMax",
+    "UFloorAmpl", "RhoFloorSlope", "UFloorSlope", "BsqrOverRhoMax", "BsqrOverUMax", "ObserveEveryDt",
 ]
 
 
 class OrcConfig(ctypes.Structure):
     _fields_ = ([(n, ctypes.c_int) for n in INT_FIELDS] + [("reserved_i", ctypes.c_int * 5)]
                 + [(n, ctypes.c_double) for n in DOUBLE_FIELDS]
-                + [("reserved_d", ctypes.c_double * 6)])
+                + [("reserved_d", ctypes.c_double * 5)])
 
 
 PRIM_OLD, PRIM, PRIM_HALF = 0, 1, 2
@@ -83,6 +83,7 @@ def lib():
         L.orc_reconstruct.argtypes = [vp, P(d), i, P(d), P(d)]
         L.orc_conserved.argtypes = [vp, P(d), P(d)]
         L.orc_compute_divb.argtypes = [vp, P(d), P(d)]
+        L.orc_torus_observers.argtypes = [vp, P(d)]
         L.orc_char_speeds.argtypes = [vp, P(d), i, P(d), P(d)]
         L.orc_stage_setup.argtypes = [vp, i]
         L.orc_residual.argtypes = [vp, P(d), P(d)]
@@ -230,6 +231,15 @@ class Oracle:
         out = np.zeros(self.zshape)
         lib().orc_compute_divb(self._h, _ptr(p), _ptr(out))
         return out
+
+    OBSERVERS = ("BaryonMass", "EMag", "ETh", "rhoMax", "betaMin", "MdotIn", "MdotOut",
+                 "UnboundMdotOut", "RelativisticUnboundMdotOut")
+
+    def torus_observers(self):
+        """ObserversTorus.hpp on primOld: {name: value}."""
+        out = np.zeros(9)
+        lib().orc_torus_observers(self._h, _ptr(out))
+        return dict(zip(self.OBSERVERS, out.tolist()))
 
     def char_speeds(self, prim, direction):
         p = np.ascontiguousarray(prim, dtype=np.float64)

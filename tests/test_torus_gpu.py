@@ -116,3 +116,57 @@ def test_torus_init_and_steps_match_oracle():
         assert scaled_err(g, o) <= 1e-12, (n, scaled_err(g, o))
     st = ts.stats()
     assert st["nonFinite"] == 0
+
+
+def test_torus_observers_match_oracle():
+    """ObserversTorus.hpp on the same primOld (the oracle's, after the
+    initial floors and two steps): the per-zone integrands are the same
+    arithmetic on both sides, so the sums agree to their summation order
+    (1e-13 of their magnitude) and the extrema exactly."""
+    cfg, ts, orc = _pair()
+    _load_oracle_geometry(ts, orc)
+    P, _ = T.torus_prims(cfg, orc.geometry(C.CENTER))
+    orc.set_prims(P)
+    orc.problem_init()
+    orc.time_step(2)
+    ts.primOld.setVars(orc.get_prims())
+    g = ts.torusObservers()
+    o = orc.torus_observers()
+    assert g["BaryonMass"] > 0 and g["ETh"] > 0 and g["EMag"] > 0
+    for k, b in o.items():
+        a = g[k]
+        if k in ("rhoMax", "betaMin"):
+            assert a == b, (k, a, b)
+        else:
+            assert abs(a - b) <= 1e-13 * max(abs(b), 1e-300), (k, a, b)
+
+
+def test_observations_recorded_by_the_steps():
+    """With ObserveEveryDt set, every step whose time crosses a multiple of
+    it (problem.cpp:754) leaves one record {time, observers}; the last one
+    equals grim_torus_observers on the state that step left."""
+    from grim_b200.timestepper import timeStepper
+    cfg = T.torus_config(**SHAPE, ObserveEveryDt=0.004)
+    ts = timeStepper(cfg)
+    from oracle.oracle import Oracle
+    orc = Oracle(cfg)
+    _load_oracle_geometry(ts, orc)
+    P, _ = T.torus_prims(cfg, orc.geometry(C.CENTER))
+    ts.primOld.setVars(P)
+    ts.problemInit()
+    E = cfg["ObserveEveryDt"]
+    due = []
+    last = None
+    for n in range(6):
+        t0 = ts.time
+        ts.timeStep()
+        t1, dt = ts.time, ts.dt
+        if np.floor(t1 / E) != np.floor((t1 - dt) / E):
+            due.append(t1)
+            last = ts.torusObservers()
+        assert abs((t1 - t0) - dt) <= 1e-15 * t1
+    recs = ts.observations()
+    assert len(due) >= 2 and len(recs) == len(due)
+    assert [r["time"] for r in recs] == due
+    for k, v in last.items():
+        assert recs[-1][k] == v, k
