@@ -72,6 +72,14 @@ def lib():
         "grim_reconstruct": [vp, vp, i, vp, vp, i],
         "grim_compute_divb": [vp, vp, vp, i],
         "grim_torus_observers": [vp, P(d)],
+        "grim_dump": [vp, i, ctypes.c_char_p],
+        "grim_load": [vp, i, ctypes.c_char_p],
+        "grim_write_restart": [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, i],
+        "grim_restart": [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p],
+        "grim_petsc_vec_write": [ctypes.c_char_p, vp, ctypes.c_longlong],
+        "grim_petsc_vec_read": [ctypes.c_char_p, vp, ctypes.c_longlong],
+        "grim_natural_from_prims": [P(GrimConfig), vp, vp],
+        "grim_prims_from_natural": [P(GrimConfig), vp, vp],
         "grim_get_observations": [vp, P(d), i, P(i)],
         "grim_conserved": [vp, vp, vp, i],
         "grim_char_speeds": [vp, vp, i, vp, vp, i],

@@ -30,6 +30,7 @@ UNITS = {
     "peaks.cu": [],
     "noalloc.cu": EXACT,
     "adjoint.cu": [],
+    "io.cu": [],
 }
 
 

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -610,6 +611,104 @@ int grim_get_prims(grim_handle* h, int which, double* dst, int memKind) {
   CK(cudaMemcpyAsync(dst, src, bytes, memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                      h->stream));
   if (memKind != GRIM_DEVICE) CK(cudaStreamSynchronize(h->stream));
+  return GRIM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// checkpoint files: grid::dump / grid::load (grid.cpp:367-381, 482-499) in
+// PETSc's binary Vec format (io.cu), the restart flow of the constructor
+// (timestepper.cpp:386-445) and CheckWallClockTermination's write
+// (torus/problem.cpp:880-907)
+// ---------------------------------------------------------------------------
+static long long natural_words(const grim_handle* h) { return h->dc.Zint * (long long)h->dc.dof; }
+
+int grim_dump(grim_handle* h, int which, const char* fileName) {
+  if (!h || !fileName) { set_err("null argument"); return GRIM_EINVAL; }
+  double* src = pick(h, which);
+  if (!src) { set_err("bad state selector %d", which); return GRIM_EINVAL; }
+  CK(cudaSetDevice(h->device));
+  std::vector<double> all((size_t)h->dc.dof * h->dc.Z), nat((size_t)natural_words(h));
+  CK(cudaMemcpyAsync(all.data(), src, all.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  int rc = grim_natural_from_prims(&h->cfg, all.data(), nat.data());
+  if (rc) return rc;
+  return grim_petsc_vec_write(fileName, nat.data(), (long long)nat.size());
+}
+
+int grim_load(grim_handle* h, int which, const char* fileName) {
+  if (!h || !fileName) { set_err("null argument"); return GRIM_EINVAL; }
+  double* dst = pick(h, which);
+  if (!dst) { set_err("bad state selector %d", which); return GRIM_EINVAL; }
+  CK(cudaSetDevice(h->device));
+  std::vector<double> nat((size_t)natural_words(h)), all((size_t)h->dc.dof * h->dc.Z, 0.);
+  int rc = grim_petsc_vec_read(fileName, nat.data(), (long long)nat.size());
+  if (rc) return rc;
+  rc = grim_prims_from_natural(&h->cfg, nat.data(), all.data());
+  if (rc) return rc;
+  // VecLoad into the global vector, then DMGlobalToLocal: the interior from
+  // the file, the ghosts as communicate leaves them
+  CK(cudaMemcpyAsync(dst, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  KNS_CALL(h, communicate, h->dc, dst, h->dc.dof, h->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));
+  return GRIM_OK;
+}
+
+int grim_write_restart(grim_handle* h, const char* restartFileName, const char* restartFileTime, char* written,
+                       int writtenCap) {
+  if (!h || !restartFileName || !restartFileTime) { set_err("null argument"); return GRIM_EINVAL; }
+  double time = 0., dt = 0.;
+  int rc = grim_get_time(h, &time, &dt);
+  if (rc) return rc;
+  // restartVarsT + the index floor(100 time) zero-padded to 8 digits
+  char name[64];
+  std::snprintf(name, sizeof(name), "restartVarsT%08lld.bin", (long long)std::floor(time * 100));
+  rc = grim_dump(h, GRIM_PRIM_OLD, name);
+  if (rc) return rc;
+  FILE* fn = std::fopen(restartFileName, "w");
+  FILE* ft = std::fopen(restartFileTime, "w");
+  bool ok = fn && ft;
+  // std::ofstream << double: 6 significant digits, as the reference writes
+  if (ok) ok = std::fprintf(fn, "%s\n", name) > 0 && std::fprintf(ft, "%g\n", time) > 0;
+  if (fn) ok = (std::fclose(fn) == 0) && ok;
+  if (ft) ok = (std::fclose(ft) == 0) && ok;
+  if (!ok) { set_err("grim_write_restart: cannot write %s / %s", restartFileName, restartFileTime); return GRIM_EINVAL; }
+  if (written && writtenCap > 0) std::snprintf(written, (size_t)writtenCap, "%s", name);
+  return GRIM_OK;
+}
+
+int grim_restart(grim_handle* h, const char* restartFileName, const char* restartFileTime, const char* restartFile) {
+  if (!h) { set_err("null argument"); return GRIM_EINVAL; }
+  CK(cudaSetDevice(h->device));
+  FILE* fn = restartFileName ? std::fopen(restartFileName, "r") : nullptr;
+  FILE* ft = restartFileTime ? std::fopen(restartFileTime, "r") : nullptr;
+  int rc = GRIM_OK;
+  if (fn && ft) {
+    double t = 0.;
+    char name[4096];
+    const bool ok = std::fscanf(ft, "%lf", &t) == 1 && std::fscanf(fn, "%4095s", name) == 1;
+    std::fclose(fn);
+    std::fclose(ft);
+    if (!ok) { set_err("grim_restart: unreadable %s / %s", restartFileName, restartFileTime); return GRIM_EINVAL; }
+    double t0 = 0., dt = 0.;
+    rc = grim_get_time(h, &t0, &dt);
+    if (!rc) rc = grim_set_time(h, t, dt);
+    if (!rc) rc = grim_load(h, GRIM_PRIM_OLD, name);
+  } else {
+    if (fn) std::fclose(fn);
+    if (ft) std::fclose(ft);
+    if (!restartFile) { set_err("grim_restart: no restart name / time files and no restart file"); return GRIM_EINVAL; }
+    rc = grim_load(h, GRIM_PRIM_OLD, restartFile);
+  }
+  if (rc) return rc;
+  // fullStepDiagnostics "to reset the time step" (timestepper.cpp:443-444):
+  // NaN reset and floors for the torus, then the element the next computeDt
+  // reads
+  enqueue_full_diagnostics(h);
+  if (h->cfg.ObserveEveryDt > 0.) enqueue_observers(h, h->cfg.ObserveEveryDt, nullptr, true);
+  enqueue_dt_speeds(h, h->primOld, 0);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));
   return GRIM_OK;
 }
 

@@ -294,6 +294,31 @@ class timeStepper:
             recs.append(dict(time=row[0], **dict(zip(self.OBSERVERS, row[1:]))))
         return recs
 
+    # ---- checkpoint files (grid::dump / grid::load, restart flow) --------
+    def dump(self, fileName, which=None):
+        """grid::dump of a state (default primOld) as a PETSc binary Vec."""
+        w = _lib.PRIM_OLD if which is None else which
+        _lib.check(_lib.lib().grim_dump(self._h, int(w), str(fileName).encode()), "dump")
+
+    def load(self, fileName, which=None):
+        """grid::load: interior from the file, ghosts as communicate sets them."""
+        w = _lib.PRIM_OLD if which is None else which
+        _lib.check(_lib.lib().grim_load(self._h, int(w), str(fileName).encode()), "load")
+
+    def writeRestart(self, restartFileName="restartFileName.txt", restartFileTime="restartFileTime.txt"):
+        """CheckWallClockTermination's write; returns the data file's name."""
+        buf = ctypes.create_string_buffer(256)
+        _lib.check(_lib.lib().grim_write_restart(self._h, str(restartFileName).encode(),
+                                                 str(restartFileTime).encode(), buf, 256), "write_restart")
+        return buf.value.decode()
+
+    def restart(self, restartFileName="restartFileName.txt", restartFileTime="restartFileTime.txt",
+                restartFile=None):
+        """The constructor's restart branch (timestepper.cpp:386-445)."""
+        _lib.check(_lib.lib().grim_restart(self._h, str(restartFileName).encode(), str(restartFileTime).encode(),
+                                           None if restartFile is None else str(restartFile).encode()),
+                   "restart")
+
     def reconstruct(self, prim, direction):
         p = np.ascontiguousarray(prim, dtype=np.float64)
         pl, pr = self._zeros(self.dof), self._zeros(self.dof)

@@ -139,6 +139,35 @@ int grim_time_steps(grim_handle* h, int nsteps);
 int grim_get_time(grim_handle* h, double* time, double* dt);
 int grim_set_time(grim_handle* h, double time, double dt);
 
+/* ---- checkpoint files (grid::dump / grid::load, grid.cpp:367-381 and
+ *      482-499).  The reference writes the DMDA global vector (interior
+ *      zones, natural order, variables interleaved: [k][j][i][var]) with
+ *      PETSc's HDF5 viewer; these files hold the same vector in PETSc's
+ *      binary Vec format (big-endian int32 class id 1211214, int32 length,
+ *      big-endian doubles), which PETSc's VecLoad reads.  HDF5 is not
+ *      linked.  A load fills the interior and leaves the ghosts as
+ *      communicate does (DMGlobalToLocal). --------------------------------- */
+int grim_dump(grim_handle* h, int which, const char* fileName);
+int grim_load(grim_handle* h, int which, const char* fileName);
+/* CheckWallClockTermination's write (torus/problem.cpp:880-907): primOld to
+ * restartVarsT<floor(100 time), 8 digits>.bin, its name into
+ * restartFileName and the time (6 significant digits, as std::ostream
+ * prints it) into restartFileTime; written (may be NULL) gets the name. */
+int grim_write_restart(grim_handle* h, const char* restartFileName, const char* restartFileTime, char* written,
+                       int writtenCap);
+/* the constructor's restart branch (timestepper.cpp:386-445): with both
+ * restartFileName and restartFileTime present, time from the one and
+ * primOld from the file the other names; else primOld from restartFile
+ * (GRIM_EINVAL when it is NULL or missing).  Then fullStepDiagnostics and
+ * the element the next computeDt reads; dt keeps its current value. */
+int grim_restart(grim_handle* h, const char* restartFileName, const char* restartFileTime, const char* restartFile);
+/* the format pieces, host only (no GPU): the PETSc binary Vec file and the
+ * reorder between [var][k][j][i] with ghosts and the natural interior */
+int grim_petsc_vec_write(const char* fileName, const double* v, long long n);
+int grim_petsc_vec_read(const char* fileName, double* v, long long n);
+int grim_natural_from_prims(const grim_config* cfg, const double* prims, double* natural);
+int grim_prims_from_natural(const grim_config* cfg, const double* natural, double* prims);
+
 /* ---- torus observers (ObserversTorus.hpp:6-253; fullStepDiagnostics,
  *      torus/problem.cpp:754-778).  Nine values, in this order: baryon mass,
  *      magnetic energy, thermal energy (integrals of rho, b^2, u times
