@@ -365,7 +365,7 @@ GRIM_D void tma_load_4d(void* dst, const CUtensorMap* map, unsigned long long* b
       : "memory");
 }
 
-template <int COND, int VISC, int MINB, int RS>
+template <int COND, int VISC, int MINB, int RS, bool PAIR>
 __global__ void __launch_bounds__(128, MINB) k_face_flux_x1_tma(const __grid_constant__ CUtensorMap tmap, DevCfg c,
                                                                  const double* __restrict__ geoF,
                                                                  double* __restrict__ flux, DevState* st) {
@@ -438,9 +438,13 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1_tma(const __grid_con
       const long long z = zidx(c, iz, j, k);
       ZoneGeo<double> G;
       load_geo(G, c, geoF, z, iz, j, 0., 0.5);
+      if constexpr (PAIR) {
+        riemann_face_pair<COND, VISC>(c, 0, pl, lo, G, flux, z);
+      } else {
 #pragma unroll
-      for (int v = 0; v < DOF; v++) park[(2 * DOF + v) * blockDim.x + threadIdx.x] = lo[v];
-      riemann_face<COND, VISC>(c, 0, pl, G, flux, z, park);
+        for (int v = 0; v < DOF; v++) park[(2 * DOF + v) * blockDim.x + threadIdx.x] = lo[v];
+        riemann_face<COND, VISC>(c, 0, pl, G, flux, z, park);
+      }
     }
   }
 }
@@ -452,7 +456,7 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1_tma(const __grid_con
 // box is (4, 12, 1, dof) for X2 and (4, 1, 12, dof) for X3; x starts at 4q
 // (32-byte aligned) and the box along DIR at 7 x chunk (never negative).
 constexpr int kStripRows = 12;
-template <int COND, int VISC, int MINB, int DIR, int RS>
+template <int COND, int VISC, int MINB, int DIR, int RS, bool PAIR>
 __global__ void __launch_bounds__(128, MINB) k_face_flux_strip_tma(const __grid_constant__ CUtensorMap tmap, DevCfg c,
                                                                     const double* __restrict__ geoF,
                                                                     const double* __restrict__ geoC,
@@ -539,9 +543,13 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_strip_tma(const __grid_
         load_geo(G, c, geoC, z, i, other, 0.5, 0.5);
       else
         load_geo(G, c, geoF, z, i, x, 0.5, 0.);
+      if constexpr (PAIR) {
+        riemann_face_pair<COND, VISC>(c, dir, pl, lo, G, flux, z);
+      } else {
 #pragma unroll
-      for (int v = 0; v < DOF; v++) park[(2 * DOF + v) * blockDim.x + threadIdx.x] = lo[v];
-      riemann_face<COND, VISC>(c, dir, pl, G, flux, z, park);
+        for (int v = 0; v < DOF; v++) park[(2 * DOF + v) * blockDim.x + threadIdx.x] = lo[v];
+        riemann_face<COND, VISC>(c, dir, pl, G, flux, z, park);
+      }
     }
   }
 }
@@ -1998,7 +2006,7 @@ static int sm_count() {
   }
   return n;
 }
-template <int C, int V, int MINB, int RS>
+template <int C, int V, int MINB, int RS, bool PAIR>
 static void face_x1_tma_launch_rs(const DevCfg& c, const CUtensorMap* tmap, const double* geoF, double* flux,
                                   DevState* st, cudaStream_t s) {
   constexpr int DOF = 8 + C + V;
@@ -2006,24 +2014,25 @@ static void face_x1_tma_launch_rs(const DevCfg& c, const CUtensorMap* tmap, cons
   const size_t smem = ((size_t)nw * 2 * DOF * kX1Box + 3 * DOF * 128) * sizeof(double) + 2 * nw * 8;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_face_flux_x1_tma<C, V, MINB, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_face_flux_x1_tma<C, V, MINB, RS, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
     attr = true;
   }
-  k_face_flux_x1_tma<C, V, MINB, RS><<<sm_count() * MINB, 32 * nw, smem, s>>>(*tmap, c, geoF, flux, st);
+  k_face_flux_x1_tma<C, V, MINB, RS, PAIR><<<sm_count() * MINB, 32 * nw, smem, s>>>(*tmap, c, geoF, flux, st);
 }
 // the reconstruction scheme becomes a compile-time constant of the TMA
 // kernels: one scheme's code per kernel keeps the instruction footprint small
-template <int C, int V, int MINB>
+template <int C, int V, int MINB, bool PAIR = false>
 static void face_x1_tma_launch(const DevCfg& c, const CUtensorMap* tmap, const double* geoF, double* flux,
                                DevState* st, cudaStream_t s) {
   switch (c.reconstruction) {
-    case GRIM_WENO5: face_x1_tma_launch_rs<C, V, MINB, GRIM_WENO5>(c, tmap, geoF, flux, st, s); break;
-    case GRIM_PPM: face_x1_tma_launch_rs<C, V, MINB, GRIM_PPM>(c, tmap, geoF, flux, st, s); break;
-    case GRIM_MP5: face_x1_tma_launch_rs<C, V, MINB, GRIM_MP5>(c, tmap, geoF, flux, st, s); break;
-    default: face_x1_tma_launch_rs<C, V, MINB, GRIM_MINMOD>(c, tmap, geoF, flux, st, s); break;
+    case GRIM_WENO5: face_x1_tma_launch_rs<C, V, MINB, GRIM_WENO5, PAIR>(c, tmap, geoF, flux, st, s); break;
+    case GRIM_PPM: face_x1_tma_launch_rs<C, V, MINB, GRIM_PPM, PAIR>(c, tmap, geoF, flux, st, s); break;
+    case GRIM_MP5: face_x1_tma_launch_rs<C, V, MINB, GRIM_MP5, PAIR>(c, tmap, geoF, flux, st, s); break;
+    default: face_x1_tma_launch_rs<C, V, MINB, GRIM_MINMOD, PAIR>(c, tmap, geoF, flux, st, s); break;
   }
 }
-template <int C, int V, int MINB, int RS>
+template <int C, int V, int MINB, int RS, bool PAIR>
 static void face_strip_tma_launch_rs(const DevCfg& c, int dir, const CUtensorMap* tmap, const double* geoF,
                                      const double* geoC, double* flux, DevState* st, cudaStream_t s) {
   constexpr int DOF = 8 + C + V;
@@ -2031,27 +2040,31 @@ static void face_strip_tma_launch_rs(const DevCfg& c, int dir, const CUtensorMap
   const size_t smem = ((size_t)nw * 2 * 4 * kStripRows * DOF + 3 * DOF * 128) * sizeof(double) + 2 * nw * 8;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_face_flux_strip_tma<C, V, MINB, 1, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_face_flux_strip_tma<C, V, MINB, 1, RS, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    cudaFuncSetAttribute(k_face_flux_strip_tma<C, V, MINB, 2, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_face_flux_strip_tma<C, V, MINB, 2, RS, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
     attr = true;
   }
   if (dir == 1)
-    k_face_flux_strip_tma<C, V, MINB, 1, RS>
+    k_face_flux_strip_tma<C, V, MINB, 1, RS, PAIR>
         <<<sm_count() * MINB, 32 * nw, smem, s>>>(tmap[1], c, geoF, geoC, flux, st);
   else
-    k_face_flux_strip_tma<C, V, MINB, 2, RS>
+    k_face_flux_strip_tma<C, V, MINB, 2, RS, PAIR>
         <<<sm_count() * MINB, 32 * nw, smem, s>>>(tmap[2], c, geoF, geoC, flux, st);
 }
-template <int C, int V, int MINB>
+template <int C, int V, int MINB, bool PAIR = false>
 static void face_strip_tma_launch(const DevCfg& c, int dir, const CUtensorMap* tmap, const double* geoF,
                                   const double* geoC, double* flux, DevState* st, cudaStream_t s) {
   switch (c.reconstruction) {
-    case GRIM_WENO5: face_strip_tma_launch_rs<C, V, MINB, GRIM_WENO5>(c, dir, tmap, geoF, geoC, flux, st, s); break;
-    case GRIM_PPM: face_strip_tma_launch_rs<C, V, MINB, GRIM_PPM>(c, dir, tmap, geoF, geoC, flux, st, s); break;
-    case GRIM_MP5: face_strip_tma_launch_rs<C, V, MINB, GRIM_MP5>(c, dir, tmap, geoF, geoC, flux, st, s); break;
-    default: face_strip_tma_launch_rs<C, V, MINB, GRIM_MINMOD>(c, dir, tmap, geoF, geoC, flux, st, s); break;
+    case GRIM_WENO5:
+      face_strip_tma_launch_rs<C, V, MINB, GRIM_WENO5, PAIR>(c, dir, tmap, geoF, geoC, flux, st, s);
+      break;
+    case GRIM_PPM: face_strip_tma_launch_rs<C, V, MINB, GRIM_PPM, PAIR>(c, dir, tmap, geoF, geoC, flux, st, s); break;
+    case GRIM_MP5: face_strip_tma_launch_rs<C, V, MINB, GRIM_MP5, PAIR>(c, dir, tmap, geoF, geoC, flux, st, s); break;
+    default:
+      face_strip_tma_launch_rs<C, V, MINB, GRIM_MINMOD, PAIR>(c, dir, tmap, geoF, geoC, flux, st, s);
+      break;
   }
 }
 template <int C, int V>
@@ -2059,10 +2072,11 @@ static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double
                         double* flux, int variant, const CUtensorMap* tmap, DevState* st, cudaStream_t s) {
   if constexpr (C == 0 && V == 0) {
     if (dir == 0) {
-      if ((variant == 2 || variant == 3) && tmap && st) {
-        if (variant == 3) face_x1_tma_launch<C, V, 4>(c, &tmap[0], geoF, flux, st, s);
+      if ((variant == 2 || variant == 3 || variant == 5) && tmap && st) {
+        if (variant == 5) face_x1_tma_launch<C, V, 3, true>(c, &tmap[0], geoF, flux, st, s);
+        else if (variant == 3) face_x1_tma_launch<C, V, 4>(c, &tmap[0], geoF, flux, st, s);
         else face_x1_tma_launch<C, V, 3>(c, &tmap[0], geoF, flux, st, s);
-      } else if (variant == 4) {
+      } else if (variant == 4 || variant == 5) {
         face_x1_launch<C, V, 3, true>(c, ps, geoF, flux, s);
       } else if (variant == 1 || variant == 3) {
         face_x1_launch<C, V, 4>(c, ps, geoF, flux, s);
@@ -2072,12 +2086,14 @@ static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double
       return;
     }
     if (variant >= 8 && tmap && st) {
-      if (variant == 9) face_strip_tma_launch<C, V, 4>(c, dir, tmap, geoF, geoC, flux, st, s);
+      if (variant == 10) face_strip_tma_launch<C, V, 3, true>(c, dir, tmap, geoF, geoC, flux, st, s);
+      else if (variant == 9) face_strip_tma_launch<C, V, 4>(c, dir, tmap, geoF, geoC, flux, st, s);
       else face_strip_tma_launch<C, V, 3>(c, dir, tmap, geoF, geoC, flux, st, s);
       return;
     }
     switch (variant) {
       case 8: face_strip_launch<C, V, 4, 3>(c, dir, ps, geoF, geoC, flux, s); break;
+      case 10: face_strip_launch<C, V, 4, 3, true>(c, dir, ps, geoF, geoC, flux, s); break;
       case 9: face_strip_launch<C, V, 4, 4>(c, dir, ps, geoF, geoC, flux, s); break;
       case 1: face_strip_launch<C, V, 4, 4>(c, dir, ps, geoF, geoC, flux, s); break;
       case 2: face_strip_launch<C, V, 2, 3>(c, dir, ps, geoF, geoC, flux, s); break;
@@ -2102,13 +2118,16 @@ void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, c
 }
 // X1: 0, 1 = register budget 3 / 4 blocks; 2, 3 = the same with TMA-staged
 // rows (when the caller has a tensor map of the primitives); 4 = both face
-// states evaluated side by side.  X2 / X3: 0-5 = lane split x register
-// budget; 6, 7 = side by side with 8 / 4 i per warp; 8, 9 = TMA-staged
-// chunks, 3 / 4 blocks per SM.  tmap points at the caller's three tensor
-// maps (X1, X2, X3 box shapes) of the prim array, or is null.
+// states evaluated side by side; 5 = TMA-staged rows with both states side
+// by side, 3 blocks per SM.  X2 / X3: 0-5 = lane split x register budget;
+// 6, 7 = side by side with 8 / 4 i per warp; 8, 9 = TMA-staged chunks, 3 / 4
+// blocks per SM; 10 = TMA-staged chunks side by side, 3 blocks per SM.
+// tmap points at the caller's three tensor maps (X1, X2, X3 box shapes) of
+// the prim array, or is null (the TMA variants then run their plain
+// counterparts).
 int face_variants(const DevCfg& c, int dir) {
   if (c.conduction || c.viscosity) return 1;
-  return dir == 0 ? 5 : 10;
+  return dir == 0 ? 6 : 11;
 }
 #endif  // !GRIM_SKIP_FACES
 
