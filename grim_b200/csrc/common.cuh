@@ -20,6 +20,9 @@ struct DevCfg {
   int N1, N2, N3, dim, ng;
   int g1, g2, g3;
   int N1T, N2T, N3T;
+  // rows of faces the interior needs (its own faces and the corner EMFs one
+  // row beyond it): j in [fj0, fj0 + nfj), k in [fk0, fk0 + nfk)
+  int fj0, nfj, fk0, nfk;
   long long Z, Zint;
   long long GZ;  // zones of one (i, j) plane: the stride of the stored geometry
   int nf, dof, Q, DP, B1;

@@ -297,12 +297,13 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1(DevCfg c, const doub
   const long long wg = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nfaces = c.N1T - 5;  // faces i = 3 .. N1T-3
   const int wpr = (nfaces + 30) / 31;
-  const long long rows = (long long)c.N2T * c.N3T;
+  const long long rows = (long long)c.nfj * c.nfk;
   if (wg >= rows * wpr) return;  // whole warps exit together
   const unsigned wgu = (unsigned)wg, row = wgu / (unsigned)wpr;
   const int i0 = 3 + (int)(wgu - row * (unsigned)wpr) * 31;
   const int iz = i0 - 1 + lane;
-  const int k = (int)(row / (unsigned)c.N2T), j = (int)(row - (unsigned)k * (unsigned)c.N2T);
+  const unsigned rk = row / (unsigned)c.nfj;
+  const int k = c.fk0 + (int)rk, j = c.fj0 + (int)(row - rk * (unsigned)c.nfj);
   const bool reconOK = iz >= 2 && iz <= c.N1T - 3;
   double lo[DOF], ro[DOF];
   const long long z = zidx(c, reconOK ? iz : 2, j, k);
@@ -378,7 +379,7 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1_tma(const __grid_con
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(park + 3 * DOF * blockDim.x) + 2 * w;
   const int nfaces = c.N1T - 5;  // faces i = 3 .. N1T-3
   const int wpr = (nfaces + 30) / 31;
-  const long long nitems = (long long)c.N2T * c.N3T * wpr;
+  const long long nitems = (long long)c.nfj * c.nfk * wpr;
   const long long stride = (long long)gridDim.x * nw;
   long long item = (long long)blockIdx.x * nw + w;
   if (lane == 0) {
@@ -390,8 +391,9 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1_tma(const __grid_con
   auto decompose = [&](long long it, int& i0, int& j, int& k) {
     const unsigned itu = (unsigned)it, row = itu / (unsigned)wpr;
     i0 = 3 + (int)(itu - row * (unsigned)wpr) * 31;
-    k = (int)(row / (unsigned)c.N2T);
-    j = (int)(row - (unsigned)k * (unsigned)c.N2T);
+    const unsigned rk = row / (unsigned)c.nfj;
+    k = c.fk0 + (int)rk;
+    j = c.fj0 + (int)(row - rk * (unsigned)c.nfj);
   };
   auto issue = [&](long long it, int buf) {
     int i0, j, k;
@@ -473,7 +475,8 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_strip_tma(const __grid_
   const int NT = (DIR == 1) ? c.N2T : c.N3T;
   const unsigned nq = (unsigned)(c.N1T + QI - 1) / QI;
   const unsigned nch = (unsigned)(NT - 5 + FPW - 1) / FPW;  // faces 3 .. NT-3
-  const unsigned nother = (unsigned)((DIR == 1) ? c.N3T : c.N2T);
+  const unsigned nother = (unsigned)((DIR == 1) ? c.nfk : c.nfj);  // rows across the direction
+  const int other0 = (DIR == 1) ? c.fk0 : c.fj0;
   const long long nitems = (long long)nq * nch * nother;
   const long long stride = (long long)gridDim.x * nw;
   long long item = (long long)blockIdx.x * nw + w;
@@ -488,7 +491,7 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_strip_tma(const __grid_
     iq = (int)(itu - r * nq);
     const unsigned o = r / nch;
     ch = (int)(r - o * nch);
-    other = (int)o;
+    other = other0 + (int)o;
   };
   auto issue = [&](long long it, int buf) {
     int iq, ch, other;
@@ -573,13 +576,13 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_strip(DevCfg c, const d
   const int NT = (dir == 1) ? c.N2T : c.N3T;
   const int nq = (c.N1T + QI - 1) / QI;
   const int nch = (NT - 5 + FPW - 1) / FPW;  // faces 3 .. NT-3
-  const long long nother = (dir == 1) ? c.N3T : c.N2T;
+  const long long nother = (dir == 1) ? c.nfk : c.nfj;  // rows across the direction
   if (wg >= (long long)nq * nch * nother) return;  // whole warps exit together
   const unsigned wgu = (unsigned)wg, r = wgu / (unsigned)nq;
   const int iq = (int)(wgu - r * (unsigned)nq);
   const unsigned oth = r / (unsigned)nch;
   const int ch = (int)(r - oth * (unsigned)nch);
-  const int other = (int)oth;  // k for X2 faces, j for X3 faces
+  const int other = ((dir == 1) ? c.fk0 : c.fj0) + (int)oth;  // k for X2 faces, j for X3 faces
   const int i = iq * QI + (lane % QI);
   const int x = 2 + ch * FPW + lane / QI;  // zone along dir; face x sits at its left
   const bool reconOK = i < c.N1T && x <= NT - 3;
@@ -1980,7 +1983,7 @@ void emhd_prepass(const DevCfg& c, const double* ps, const double* geoC, double*
 // the lane split QI (i per warp).  EMHD has one shape (2 resident blocks).
 template <int C, int V, int MINB, bool PAIR = false>
 static void face_x1_launch(const DevCfg& c, const double* ps, const double* geoF, double* flux, cudaStream_t s) {
-  const long long warps = (long long)c.N2T * c.N3T * ((c.N1T - 5 + 30) / 31);
+  const long long warps = (long long)c.nfj * c.nfk * ((c.N1T - 5 + 30) / 31);
   const size_t park = PAIR ? 0 : 3 * (8 + C + V) * 128 * sizeof(double);
   k_face_flux_x1<C, V, MINB, PAIR><<<nblk(warps * 32, 128), 128, park, s>>>(c, ps, geoF, flux);
 }
@@ -1988,7 +1991,7 @@ template <int C, int V, int QI, int MINB, bool PAIR = false>
 static void face_strip_launch(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,
                               double* flux, cudaStream_t s) {
   const int NT = (dir == 1) ? c.N2T : c.N3T;
-  const long long other = (dir == 1) ? c.N3T : c.N2T;
+  const long long other = (dir == 1) ? c.nfk : c.nfj;
   const long long warps = (long long)((c.N1T + QI - 1) / QI) * ((NT - 5 + 32 / QI - 2) / (32 / QI - 1)) * other;
   const size_t park = PAIR ? 0 : 3 * (8 + C + V) * 128 * sizeof(double);
   if (dir == 1)

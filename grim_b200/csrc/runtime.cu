@@ -165,6 +165,12 @@ static int make_devcfg(const grim_config& c, DevCfg& d) {
   d.N1 = c.N1; d.N2 = c.dim >= 2 ? c.N2 : 1; d.N3 = c.dim >= 3 ? c.N3 : 1;
   d.g1 = d.ng; d.g2 = c.dim >= 2 ? d.ng : 0; d.g3 = c.dim >= 3 ? d.ng : 0;
   d.N1T = d.N1 + 2 * d.g1; d.N2T = d.N2 + 2 * d.g2; d.N3T = d.N3 + 2 * d.g3;
+  // face rows: the interior and one row beyond it on each side (the corner
+  // EMFs of the interior's edges read one row of fluxes outside it)
+  d.fj0 = std::max(d.g2 - 1, 0);
+  d.nfj = std::min(d.N2 + d.g2, d.N2T - 1) - d.fj0 + 1;
+  d.fk0 = std::max(d.g3 - 1, 0);
+  d.nfk = std::min(d.N3 + d.g3, d.N3T - 1) - d.fk0 + 1;
   d.Z = (long long)d.N1T * d.N2T * d.N3T;
   d.Zint = (long long)d.N1 * d.N2 * d.N3;
   d.GZ = (long long)d.N1T * d.N2T;
