@@ -1451,8 +1451,9 @@ GRIM_D void tangent_jacobian(const double* P, const StageConst<5 + COND + VISC>&
     for (int cc = 0; cc < NF; cc++) J[r][cc] = Rd[r].d[cc];
 }
 
+constexpr int kNewtonMinBlocks = 3;  // blocks per SM of the ideal FP32-Jacobian Newton
 template <int COND, int VISC, class T>
-__global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : 3) k_newton_fast(DevCfg c, int stage, StageBufs b,
+__global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : kNewtonMinBlocks) k_newton_fast(DevCfg c, int stage, StageBufs b,
                                                               const int* __restrict__ list, long long nlist) {
   constexpr int NF = 5 + COND + VISC;
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
