@@ -2109,11 +2109,15 @@ static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double
       default: face_strip_launch<C, V, 4, 3>(c, dir, ps, geoF, geoC, flux, s); break;
     }
   } else {
-    // EMHD elements need more registers: two resident blocks
-    (void)tmap;
-    (void)st;
-    if (dir == 0) face_x1_launch<C, V, 2>(c, ps, geoF, flux, s);
-    else face_strip_launch<C, V, 4, 2>(c, dir, ps, geoF, geoC, flux, s);
+    // EMHD elements need more registers: two resident blocks; variant 1
+    // stages the stencils with TMA
+    if (dir == 0) {
+      if (variant == 1 && tmap && st) face_x1_tma_launch<C, V, 2>(c, &tmap[0], geoF, flux, st, s);
+      else face_x1_launch<C, V, 2>(c, ps, geoF, flux, s);
+    } else {
+      if (variant == 1 && tmap && st) face_strip_tma_launch<C, V, 2>(c, dir, tmap, geoF, geoC, flux, st, s);
+      else face_strip_launch<C, V, 4, 2>(c, dir, ps, geoF, geoC, flux, s);
+    }
   }
 }
 void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC, double* flux,
@@ -2126,11 +2130,13 @@ void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, c
 // by side, 3 blocks per SM.  X2 / X3: 0-5 = lane split x register budget;
 // 6, 7 = side by side with 8 / 4 i per warp; 8, 9 = TMA-staged chunks, 3 / 4
 // blocks per SM; 10 = TMA-staged chunks side by side, 3 blocks per SM.
+// EMHD (10 dof), every direction: 0 = plain, 1 = TMA-staged, 2 blocks per SM.
 // tmap points at the caller's three tensor maps (X1, X2, X3 box shapes) of
 // the prim array, or is null (the TMA variants then run their plain
 // counterparts).
 int face_variants(const DevCfg& c, int dir) {
-  if (c.conduction || c.viscosity) return 1;
+  (void)dir;
+  if (c.conduction || c.viscosity) return 2;  // plain / TMA-staged, 2 blocks per SM
   return dir == 0 ? 6 : 11;
 }
 #endif  // !GRIM_SKIP_FACES

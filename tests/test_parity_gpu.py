@@ -389,6 +389,30 @@ def test_autotuned_face_kernels_give_identical_results(mode):
 
 
 @pytest.mark.parametrize("mode", [C.NEWTON_PARITY_FD64, C.NEWTON_MIXED32])
+def test_face_variants_emhd(mode):
+    """EMHD (10 dof, MP5): the plain and the TMA-staged face kernels give
+    the same fluxes (bit for bit in the FP64 parity unit, roundoff in the
+    fast unit) in both directions (N1T = 70 >= 40 zones along i)."""
+    cfg = PR.emhd_stratified_config(N=64)
+    P = PR.emhd_stratified_prims(cfg)
+    from grim_b200.timestepper import timeStepper
+    ts = timeStepper(cfg)
+    ts.setNewtonMode(mode, 1, 0.0)
+    ref_div, ref_flux = ts.computeDivOfFluxes(P)
+    for d in (0, 1):
+        ts.setFaceVariant(d, 1)
+        div, flux = ts.computeDivOfFluxes(P)
+        if mode == C.NEWTON_PARITY_FD64:
+            assert np.array_equal(flux, ref_flux) and np.array_equal(div, ref_div), d
+        else:
+            scale = np.max(np.abs(ref_flux), axis=tuple(range(2, ref_flux.ndim)), keepdims=True) + 1e-300
+            assert np.max(np.abs(flux - ref_flux) / scale) <= 1e-14, d
+        ts.setFaceVariant(d, 0)
+    with pytest.raises(Exception):
+        ts.setFaceVariant(0, 2)
+
+
+@pytest.mark.parametrize("mode", [C.NEWTON_PARITY_FD64, C.NEWTON_MIXED32])
 def test_face_variants_3d(mode):
     """3D grid with room for every tensor-map box (N1T = 46 >= 40 zones
     along i, N2T = N3T = 22 >= 12 along j and k): every X1, X2 and X3 face
