@@ -167,17 +167,26 @@ __global__ void k_emhd_prepass(DevCfg c, const double* __restrict__ ps, const do
 // shuffle: X1 faces take 31 faces per warp along i, X2 / X3 faces 7 faces
 // along the direction for each of 4 consecutive i.
 // ---------------------------------------------------------------------------
-template <int DOF>
-GRIM_D void recon_zone(const DevCfg& c, const double* __restrict__ ps, long long z, long long s, int scheme,
-                       double* lo, double* ro) {
+template <int DOF, int RS>
+GRIM_D void recon_zone_rs(const DevCfg& c, const double* __restrict__ ps, long long z, long long s, double* lo,
+                          double* ro) {
 #pragma unroll
   for (int v = 0; v < DOF; v++) {
     const double* a = ps + (long long)v * c.Z + z;
     const double y0 = __ldg(a - 2 * s), y1 = __ldg(a - s), y2 = __ldg(a), y3 = __ldg(a + s), y4 = __ldg(a + 2 * s);
-    if (kFastMath)
-      recon_faces_fast(scheme, c.theta, y0, y1, y2, y3, y4, lo[v], ro[v]);
-    else
-      recon_faces(scheme, c.theta, y0, y1, y2, y3, y4, lo[v], ro[v]);
+    recon_faces_rs<RS, kFastMath>(c.reconstruction, c.theta, y0, y1, y2, y3, y4, lo[v], ro[v]);
+  }
+}
+// the scheme is chosen once, outside the loop over the variables, so the
+// path a warp executes is one scheme's contiguous code
+template <int DOF>
+GRIM_D void recon_zone(const DevCfg& c, const double* __restrict__ ps, long long z, long long s, int scheme,
+                       double* lo, double* ro) {
+  switch (scheme) {
+    case GRIM_WENO5: recon_zone_rs<DOF, GRIM_WENO5>(c, ps, z, s, lo, ro); break;
+    case GRIM_PPM: recon_zone_rs<DOF, GRIM_PPM>(c, ps, z, s, lo, ro); break;
+    case GRIM_MP5: recon_zone_rs<DOF, GRIM_MP5>(c, ps, z, s, lo, ro); break;
+    default: recon_zone_rs<DOF, GRIM_MINMOD>(c, ps, z, s, lo, ro); break;
   }
 }
 
