@@ -72,6 +72,10 @@ def lib():
         "grim_reconstruct": [vp, vp, i, vp, vp, i],
         "grim_compute_divb": [vp, vp, vp, i],
         "grim_torus_observers": [vp, P(d)],
+        "grim_step_segment": [vp, i],
+        "grim_halo_x3": [vp, i, i, i, vp],
+        "grim_scalar_get": [vp, i, vp],
+        "grim_scalar_set": [vp, i, vp],
         "grim_dump": [vp, i, ctypes.c_char_p],
         "grim_load": [vp, i, ctypes.c_char_p],
         "grim_write_restart": [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, i],

@@ -11,7 +11,7 @@ import ctypes
 import math
 
 # enums, src/params.hpp:32-94 (MP5 and the closures are additions)
-PERIODIC, OUTFLOW, MIRROR, DIRICHLET = 0, 1, 2, 3
+PERIODIC, OUTFLOW, MIRROR, DIRICHLET, EXCHANGE = 0, 1, 2, 3, 4
 MINKOWSKI, MODIFIED_KERR_SCHILD = 0, 1
 MINMOD, WENO5, PPM, MP5 = 0, 1, 2, 3
 HLL, LOCAL_LAX_FRIEDRICH = 0, 1
@@ -43,9 +43,9 @@ INT_FIELDS = [
     "reconstruction", "riemannSolver",
     "maxNonLinearIter", "maxLineSearchIters",
     "closure", "problem", "elemOldFromFullStep",
-    "newtonMode", "perZoneConvergence",
+    "newtonMode", "perZoneConvergence", "N3Global",
 ]
-N_RESERVED_INT = 5
+N_RESERVED_INT = 4
 
 DOUBLE_FIELDS = [
     "blackHoleSpin", "hSlope",
@@ -95,7 +95,7 @@ def defaults():
         reconstruction=MINMOD, riemannSolver=HLL,
         maxNonLinearIter=3, maxLineSearchIters=3,
         closure=CLOSURE_CONST_TAU, problem=PROBLEM_NONE, elemOldFromFullStep=1,
-        newtonMode=NEWTON_PARITY_FD64, perZoneConvergence=0,
+        newtonMode=NEWTON_PARITY_FD64, perZoneConvergence=0, N3Global=0,
         blackHoleSpin=0.9375, hSlope=0.3,
         X1Start=0., X1End=1., X2Start=0., X2End=1., X3Start=0., X3End=1.,
         time=0., dt=0.5 / 128,

@@ -50,6 +50,7 @@ GRIM_D void load_geo(ZoneGeo<R>& G, const DevCfg& c, const double* geo, long lon
 // ---------------------------------------------------------------------------
 GRIM_D int bc_map(int x, int g, int N, int lo, int hi) {
   if (x >= g && x < N + g) return x;
+  if ((x < g && lo == GRIM_EXCHANGE) || (x >= N + g && hi == GRIM_EXCHANGE)) return x;  // the caller's halo
   if (x < g) {
     if (lo == GRIM_PERIODIC) return g + ((x - g) % N + N) % N;
     if (lo == GRIM_MIRROR) return 2 * g - 1 - x;
@@ -85,21 +86,31 @@ static __global__ void k_ghost_fill(DevCfg c, double* __restrict__ prim, int nv)
 // zones on a non-periodic edge come back from the never-written local
 // vector, i.e. as zero.
 // the zone communicate reads for zone (i, j, k): itself inside, the wrapped
-// interior zone across a periodic edge; zero is set on a non-periodic edge
+// interior zone across a periodic edge; zero is set on a non-periodic edge.
+// A GRIM_EXCHANGE side keeps its own ghost value (the caller's halo).
 GRIM_D long long comm_source(const DevCfg& c, int i, int j, int k, bool& zero) {
   const bool p1 = c.bc[0] == GRIM_PERIODIC || c.bc[1] == GRIM_PERIODIC;
   const bool p2 = c.bc[2] == GRIM_PERIODIC || c.bc[3] == GRIM_PERIODIC;
   const bool p3 = c.bc[4] == GRIM_PERIODIC || c.bc[5] == GRIM_PERIODIC;
   zero = false;
-  auto m = [&](int x, int g, int N, bool per) -> int {
+  auto m = [&](int x, int g, int N, bool per, int lo, int hi) -> int {
     if (x >= g && x < N + g) return x;
+    if ((x < g && lo == GRIM_EXCHANGE) || (x >= N + g && hi == GRIM_EXCHANGE)) return x;
     if (!per) { zero = true; return x; }
     return g + ((x - g) % N + N) % N;
   };
-  const int si = m(i, c.g1, c.N1, p1);
-  const int sj = (c.dim >= 2) ? m(j, c.g2, c.N2, p2) : j;
-  const int sk = (c.dim >= 3) ? m(k, c.g3, c.N3, p3) : k;
+  const int si = m(i, c.g1, c.N1, p1, c.bc[0], c.bc[1]);
+  const int sj = (c.dim >= 2) ? m(j, c.g2, c.N2, p2, c.bc[2], c.bc[3]) : j;
+  const int sk = (c.dim >= 3) ? m(k, c.g3, c.N3, p3, c.bc[4], c.bc[5]) : k;
   return zidx(c, si, sj, sk);
+}
+// a ghost zone on a GRIM_EXCHANGE side: it repeats a neighbouring slab's
+// interior, which that slab's own reductions count
+GRIM_D bool in_exchange_ghost(const DevCfg& c, int i, int j, int k) {
+  const bool x1 = (i < c.g1 && c.bc[0] == GRIM_EXCHANGE) || (i >= c.N1 + c.g1 && c.bc[1] == GRIM_EXCHANGE);
+  const bool x2 = c.dim >= 2 && ((j < c.g2 && c.bc[2] == GRIM_EXCHANGE) || (j >= c.N2 + c.g2 && c.bc[3] == GRIM_EXCHANGE));
+  const bool x3 = c.dim >= 3 && ((k < c.g3 && c.bc[4] == GRIM_EXCHANGE) || (k >= c.N3 + c.g3 && c.bc[5] == GRIM_EXCHANGE));
+  return x1 || x2 || x3;
 }
 
 static __global__ void k_communicate(DevCfg c, double* __restrict__ prim, int nv) {
@@ -1003,7 +1014,7 @@ __global__ void k_dt_speeds(DevCfg c, const double* __restrict__ p, const double
     for (int v = 0; v < DOF; v++) pv[v] = zero ? 0. : p[(long long)v * Z + src];
     ZoneGeo<double> G;
     load_geo(G, c, geoC, z, i, j, 0.5, 0.5);
-    best = zone_inv_dt<COND, VISC>(c, pv, G);
+    if (!in_exchange_ghost(c, i, j, k)) best = zone_inv_dt<COND, VISC>(c, pv, G);
   }
   block_max_to(best, &st->maxInvDt);
 }
@@ -1047,7 +1058,7 @@ __global__ void __launch_bounds__(128) k_stage_finish(DevCfg c, TorusCfg t, cons
 #pragma unroll
     for (int v = 0; v < DOF; v++) dst[(long long)v * Z + z] = q[v];
     if constexpr (POST) {
-      if (dtOn) best = zone_inv_dt<COND, VISC>(c, q, G);
+      if (dtOn && !in_exchange_ghost(c, i, j, k)) best = zone_inv_dt<COND, VISC>(c, q, G);
       const bool inside = i >= c.g1 && i < c.N1 + c.g1 && j >= c.g2 && j < c.N2 + c.g2 && k >= c.g3 &&
                           k < c.N3 + c.g3;
       if (inside)

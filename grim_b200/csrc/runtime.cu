@@ -184,10 +184,16 @@ static int make_devcfg(const grim_config& c, DevCfg& d) {
   d.maxIter = c.maxNonLinearIter; d.maxLS = c.maxLineSearchIters;
   d.bc[0] = c.boundaryLeft; d.bc[1] = c.boundaryRight; d.bc[2] = c.boundaryBottom; d.bc[3] = c.boundaryTop;
   d.bc[4] = c.boundaryBack; d.bc[5] = c.boundaryFront;
+  for (int q = 0; q < 6; q++)
+    if (d.bc[q] < GRIM_PERIODIC || d.bc[q] > GRIM_EXCHANGE) { set_err("bad boundary condition %d", d.bc[q]); return GRIM_EINVAL; }
+  if (c.N3Global < 0 || (c.N3Global > 0 && (c.dim < 3 || c.N3Global < c.N3))) {
+    set_err("N3Global: a slab of a 3D grid with N3 <= N3Global"); return GRIM_EINVAL;
+  }
   // coordinatesGrid (grid.cpp:142-146): dX from the constructor's N
   d.dX[0] = (c.X1End - c.X1Start) / c.N1;
   d.dX[1] = (c.X2End - c.X2Start) / c.N2;
-  d.dX[2] = (c.X3End - c.X3Start) / c.N3;
+  // a slab: the global extent over the global plane count
+  d.dX[2] = (c.X3End - c.X3Start) / (c.N3Global > 0 ? c.N3Global : c.N3);
   for (int i = 0; i < 3; i++) d.invdX[i] = 1. / d.dX[i];
   d.X1Start = c.X1Start; d.X2Start = c.X2Start; d.X3Start = c.X3Start; d.X2End = c.X2End;
   d.Gam = c.adiabaticIndex;
@@ -389,23 +395,26 @@ static void enqueue_pre_half(grim_handle* h, bool timed) {
 }
 
 // primHalfStep = prim, communicate, halfStepDiagnostics as one pass
-static void enqueue_mid(grim_handle* h) {
+static void enqueue_mid_finish(grim_handle* h) {
   const DevCfg& c = h->dc;
-  cudaStream_t s = h->stream;
-  {
-    PROF(GRIM_PROF_COPY);
-    const bool torus = h->cfg.problem == GRIM_PROBLEM_TORUS;
-    const double* geoC = h->cfg.metric == GRIM_MINKOWSKI ? nullptr : h->geo[GRIM_CENTER];
-    KNS_CALL(h, stage_finish, c, h->prim, h->primHalf, geoC, torus, false, nullptr, 0, h->st, s);
-    g_launch_counter++;
-  }
-  // ---- full stage
+  PROF(GRIM_PROF_COPY);
+  const bool torus = h->cfg.problem == GRIM_PROBLEM_TORUS;
+  const double* geoC = h->cfg.metric == GRIM_MINKOWSKI ? nullptr : h->geo[GRIM_CENTER];
+  KNS_CALL(h, stage_finish, c, h->prim, h->primHalf, geoC, torus, false, nullptr, 0, h->st, h->stream);
+  g_launch_counter++;
+}
+// the full stage's boundaries on primHalfStep
+static void enqueue_mid_fill(grim_handle* h) {
   {
     PROF(GRIM_PROF_BOUNDARY);
-    KNS_CALL(h, ghost_fill, c, h->primHalf, c.dof, s);
+    KNS_CALL(h, ghost_fill, h->dc, h->primHalf, h->dc.dof, h->stream);
     g_launch_counter++;
   }
   enqueue_problem_bcs(h, h->primHalf);
+}
+static void enqueue_mid(grim_handle* h) {
+  enqueue_mid_finish(h);
+  enqueue_mid_fill(h);
 }
 
 // the torus observers of primOld (ObserversTorus.hpp): into out (device,
@@ -425,7 +434,9 @@ static void enqueue_observers(grim_handle* h, double every, double* out, bool to
 // floors), the next computeDt's speeds when the element is re-set from the
 // full step (linear_modes/problem.cpp:287) and the non-finite count, as one
 // pass after the NaN count
-static void enqueue_post(grim_handle* h, bool timed) {
+// time advance and the NaN count of fullStepDiagnostics (on the Newton
+// result, whose interior the finish copies unchanged)
+static void enqueue_post_count(grim_handle* h) {
   const DevCfg& c = h->dc;
   cudaStream_t s = h->stream;
   {
@@ -433,15 +444,17 @@ static void enqueue_post(grim_handle* h, bool timed) {
     grim::exact::advance_time(h->st, s);
     g_launch_counter++;
   }
-  const bool torus = h->cfg.problem == GRIM_PROBLEM_TORUS;
-  {
+  if (h->cfg.problem == GRIM_PROBLEM_TORUS) {
     PROF(GRIM_PROF_DIAGNOSTICS);
-    if (torus) {
-      cudaMemsetAsync(&h->st->nanFlag, 0, sizeof(unsigned long long), s);
-      KNS_CALL(h, torus_nan_flag, c, h->prim, &h->st->nanFlag, s);
-      g_launch_counter++;
-    }
+    cudaMemsetAsync(&h->st->nanFlag, 0, sizeof(unsigned long long), s);
+    KNS_CALL(h, torus_nan_flag, c, h->prim, &h->st->nanFlag, s);
+    g_launch_counter++;
   }
+}
+static void enqueue_post_finish(grim_handle* h, bool timed) {
+  const DevCfg& c = h->dc;
+  cudaStream_t s = h->stream;
+  const bool torus = h->cfg.problem == GRIM_PROBLEM_TORUS;
   {
     PROF(GRIM_PROF_COPY);
     const int dtOn = h->cfg.elemOldFromFullStep ? 1 : 0;
@@ -458,6 +471,29 @@ static void enqueue_post(grim_handle* h, bool timed) {
     g_launch_counter += 2;
   }
   if (timed) cudaEventRecord(h->ev[7], s);
+}
+static void enqueue_post(grim_handle* h, bool timed) {
+  enqueue_post_count(h);
+  enqueue_post_finish(h, timed);
+}
+
+// the step in the four segments of a slab-decomposed run (grim_step_segment)
+static void enqueue_segment(grim_handle* h, int seg) {
+  switch (seg) {
+    case GRIM_SEG_PRE: enqueue_pre_half(h, false); break;
+    case GRIM_SEG_HALF:
+      enqueue_stencil(h, GRIM_HALF_STEP);
+      enqueue_newton(h, GRIM_HALF_STEP);
+      enqueue_mid_finish(h);
+      break;
+    case GRIM_SEG_FULL:
+      enqueue_mid_fill(h);
+      enqueue_stencil(h, GRIM_FULL_STEP);
+      enqueue_newton(h, GRIM_FULL_STEP);
+      enqueue_post_count(h);
+      break;
+    default: enqueue_post_finish(h, false); break;
+  }
 }
 
 static void enqueue_step(grim_handle* h, bool timed) {
@@ -876,6 +912,57 @@ int grim_reconstruct(grim_handle* h, const double* prim, int dir, double* pl, do
   rc = stage_out(h, pl, dl, (size_t)c.dof * h->bytesZ, memKind);
   if (rc) return rc;
   return stage_out(h, pr, dr, (size_t)c.dof * h->bytesZ, memKind);
+}
+
+int grim_step_segment(grim_handle* h, int segment) {
+  if (!h || segment < GRIM_SEG_PRE || segment > GRIM_SEG_POST) { set_err("bad segment"); return GRIM_EINVAL; }
+  CK(cudaSetDevice(h->device));
+  enqueue_segment(h, segment);
+  CK(cudaGetLastError());
+  return GRIM_OK;
+}
+
+int grim_halo_x3(grim_handle* h, int which, int side, int unpack, void* buf) {
+  if (!h || !buf || (side != 0 && side != 1)) { set_err("bad argument"); return GRIM_EINVAL; }
+  double* p = pick(h, which);
+  if (!p) { set_err("bad state selector %d", which); return GRIM_EINVAL; }
+  const DevCfg& c = h->dc;
+  if (c.dim != 3 || c.N3 < c.g3) { set_err("grim_halo_x3: a 3D grid with at least 3 planes"); return GRIM_EINVAL; }
+  CK(cudaSetDevice(h->device));
+  const size_t plane = (size_t)c.N1T * c.N2T;
+  // the 3 planes next to the end (pack) or its 3 ghost planes (unpack)
+  const int k0 = unpack ? (side == 0 ? 0 : c.N3 + c.g3) : (side == 0 ? c.g3 : c.N3);
+  double* grid = p + (size_t)k0 * plane;
+  const size_t width = (size_t)c.g3 * plane * sizeof(double), pitch = (size_t)c.Z * sizeof(double);
+  if (unpack)
+    CK(cudaMemcpy2DAsync(grid, pitch, buf, width, width, (size_t)c.dof, cudaMemcpyDeviceToDevice, h->stream));
+  else
+    CK(cudaMemcpy2DAsync(buf, width, grid, pitch, width, (size_t)c.dof, cudaMemcpyDeviceToDevice, h->stream));
+  return GRIM_OK;
+}
+
+static void* scalar_ptr(grim_handle* h, int which, size_t* bytes) {
+  if (which == GRIM_SCALAR_MAXINVDT) { *bytes = sizeof(double); return &h->st->maxInvDt; }
+  if (which == GRIM_SCALAR_NANFLAG) { *bytes = sizeof(unsigned long long); return &h->st->nanFlag; }
+  return nullptr;
+}
+int grim_scalar_get(grim_handle* h, int which, void* devBuf) {
+  if (!h || !devBuf) { set_err("null argument"); return GRIM_EINVAL; }
+  size_t n = 0;
+  void* src = scalar_ptr(h, which, &n);
+  if (!src) { set_err("bad scalar %d", which); return GRIM_EINVAL; }
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(devBuf, src, n, cudaMemcpyDeviceToDevice, h->stream));
+  return GRIM_OK;
+}
+int grim_scalar_set(grim_handle* h, int which, const void* devBuf) {
+  if (!h || !devBuf) { set_err("null argument"); return GRIM_EINVAL; }
+  size_t n = 0;
+  void* dst = scalar_ptr(h, which, &n);
+  if (!dst) { set_err("bad scalar %d", which); return GRIM_EINVAL; }
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(dst, devBuf, n, cudaMemcpyDeviceToDevice, h->stream));
+  return GRIM_OK;
 }
 
 int grim_torus_observers(grim_handle* h, double* out) {

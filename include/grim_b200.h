@@ -41,7 +41,8 @@ extern "C" {
 #define GRIM_ENONFINITE   -7   /* NaN/Inf detected in a result */
 
 /* ---- enums (src/params.hpp:32-94; MP5, closures, Newton modes are new) -- */
-enum { GRIM_PERIODIC = 0, GRIM_OUTFLOW = 1, GRIM_MIRROR = 2, GRIM_DIRICHLET = 3 };
+enum { GRIM_PERIODIC = 0, GRIM_OUTFLOW = 1, GRIM_MIRROR = 2, GRIM_DIRICHLET = 3,
+       GRIM_EXCHANGE = 4 /* ghosts filled by the caller's halo exchange (slab of a decomposed grid) */ };
 enum { GRIM_MINKOWSKI = 0, GRIM_MODIFIED_KERR_SCHILD = 1 };
 enum { GRIM_MINMOD = 0, GRIM_WENO5 = 1, GRIM_PPM = 2, GRIM_MP5 = 3 };
 enum { GRIM_HLL = 0, GRIM_LOCAL_LAX_FRIEDRICH = 1 };
@@ -77,7 +78,9 @@ typedef struct grim_config {
   int elemOldFromFullStep;  /* 1: fullStepDiagnostics re-sets elemOld */
   int newtonMode;           /* GRIM_NEWTON_* */
   int perZoneConvergence;   /* 0: global break (reference), 1: per zone, 2: compacted */
-  int reserved_i[5];
+  int N3Global;             /* > 0: the handle holds N3 of N3Global X3 planes of a slab
+                               decomposition; X3Start / X3End are the global extent */
+  int reserved_i[4];
   double blackHoleSpin, hSlope;
   double X1Start, X1End, X2Start, X2End, X3Start, X3End;
   double time, dt;
@@ -167,6 +170,29 @@ int grim_petsc_vec_write(const char* fileName, const double* v, long long n);
 int grim_petsc_vec_read(const char* fileName, double* v, long long n);
 int grim_natural_from_prims(const grim_config* cfg, const double* prims, double* natural);
 int grim_prims_from_natural(const grim_config* cfg, const double* natural, double* prims);
+
+/* ---- slab decomposition along X3 (one handle per GPU; the caller moves
+ *      the halos and reduces the two scalars, e.g. over NCCL).  A step is
+ *      the four segments in order, with, between them:
+ *        before 0: maxInvDt <- max over ranks (the next computeDt)
+ *        after 1:  X3 halo of GRIM_PRIM_HALF (the stage-end communicate)
+ *        after 2:  nanFlag <- sum over ranks (fullStepDiagnostics)
+ *        after 3:  X3 halo of GRIM_PRIM_OLD
+ *      Ghost sides with boundary GRIM_EXCHANGE are left to the caller; the
+ *      dt reduction skips them (they repeat a neighbour's interior). ----- */
+enum { GRIM_SEG_PRE = 0, GRIM_SEG_HALF = 1, GRIM_SEG_FULL = 2, GRIM_SEG_POST = 3 };
+int grim_step_segment(grim_handle* h, int segment);
+/* halo planes of a state: side 0 = low X3 end, 1 = high; pack copies the 3
+ * interior planes next to that end into buf, unpack writes buf into the 3
+ * ghost planes of that end.  buf: device, dof x 3 x N1T x N2T doubles
+ * ([var][plane][j][i]); asynchronous on the handle's stream. */
+int grim_halo_x3(grim_handle* h, int which, int side, int unpack, void* buf);
+/* device scalars a decomposed run reduces across ranks: 0 = maxInvDt
+ * (double), 1 = nanFlag (unsigned 64-bit); devBuf is device memory;
+ * asynchronous on the handle's stream */
+enum { GRIM_SCALAR_MAXINVDT = 0, GRIM_SCALAR_NANFLAG = 1 };
+int grim_scalar_get(grim_handle* h, int which, void* devBuf);
+int grim_scalar_set(grim_handle* h, int which, const void* devBuf);
 
 /* ---- torus observers (ObserversTorus.hpp:6-253; fullStepDiagnostics,
  *      torus/problem.cpp:754-778).  Nine values, in this order: baryon mass,

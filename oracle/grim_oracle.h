@@ -34,7 +34,8 @@ typedef struct orc_config {
   int elemOldFromFullStep;
   int newtonMode;
   int perZoneConvergence;
-  int reserved_i[5];
+  int N3Global;
+  int reserved_i[4];
   /* ---- doubles ---- */
   double blackHoleSpin, hSlope;
   double X1Start, X1End, X2Start, X2End, X3Start, X3End;

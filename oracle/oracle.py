@@ -25,7 +25,7 @@ INT_FIELDS = [
     "DerefineThetaHorizon", "DoCylindrify", "conduction", "viscosity",
     "highOrderTermsConduction", "highOrderTermsViscosity",
     "reconstruction", "riemannSolver", "maxNonLinearIter", "maxLineSearchIters",
-    "closure", "problem", "elemOldFromFullStep", "newtonMode", "perZoneConvergence",
+    "closure", "problem", "elemOldFromFullStep", "newtonMode", "perZoneConvergence", "N3Global",
 ]
 DOUBLE_FIELDS = [
     "blackHoleSpin", "hSlope", "X1Start", "X1End", "X2Start", "X2End",
@@ -42,7 +42,7 @@ DOUBLE_FIELDS = [
 
 
 class OrcConfig(ctypes.Structure):
-    _fields_ = ([(n, ctypes.c_int) for n in INT_FIELDS] + [("reserved_i", ctypes.c_int * 5)]
+    _fields_ = ([(n, ctypes.c_int) for n in INT_FIELDS] + [("reserved_i", ctypes.c_int * 4)]
                 + [(n, ctypes.c_double) for n in DOUBLE_FIELDS]
                 + [("reserved_d", ctypes.c_double * 5)])
 
