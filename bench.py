@@ -418,6 +418,83 @@ def run_batch(args, local_rank):
     }
 
 
+def _free_port():
+    import socket
+    sk = socket.socket()
+    sk.bind(("127.0.0.1", 0))
+    port = sk.getsockname()[1]
+    sk.close()
+    return port
+
+
+def run_decomposed(args, rank, world, local_rank):
+    """The workload's grid split into X3 slabs over the ranks (one GPU
+    each; NCCL halos and reductions between the library's step segments):
+    total work fixed as N grows.  Fast Newton form."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    from grim_b200.slab import SlabTimeStepper
+    from grim_b200.timestepper import timeStepper
+    cfg, P, desc = workload(args.workload, args.grid)
+    cfg = dict(cfg, newtonMode=C.NEWTON_MIXED32, perZoneConvergence=args.per_zone, nonlinearsolve_rtol=RTOL)
+    if P is None:
+        P = torus_state(cfg, timeStepper(cfg, device=local_rank))
+    zones = cfg["N1"] * cfg["N2"] * cfg["N3"]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    sl = SlabTimeStepper(cfg, device=local_rank)
+    sl.setGlobalPrims(P)
+    sl.ts.problemInit()
+    tuned = {str(d): v for d, (v, _) in sl.ts.autotune().items()}
+    stream = sl.stream
+    for _ in range(args.warmup):
+        sl.timeStep()
+    sl.synchronize()
+    torch.distributed.barrier()
+    clocks = Clocks(local_rank)
+    clocks.start()
+    ms = 0.
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+        sl.timeStep()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms += a.elapsed_time(b)
+    clocks_info = clocks.stop()
+    torch.distributed.barrier()
+    # e2e: this rank's slab in from pinned host memory, the step, the slab back
+    import ctypes
+    from grim_b200 import _lib
+    host_in = torch.from_numpy(np.ascontiguousarray(sl.ts.primOld.getVars())).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    L = _lib.lib()
+    e2e_steps = max(3, args.steps // 2)
+    torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        _lib.check(L.grim_set_prims(sl.ts._h, _lib.PRIM_OLD, ctypes.c_void_p(host_in.data_ptr()), _lib.HOST))
+        sl.timeStep()
+        _lib.check(L.grim_get_prims(sl.ts._h, _lib.PRIM_OLD, ctypes.c_void_p(host_out.data_ptr()), _lib.HOST))
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([ms, e2e_s], dtype=torch.float64, device="cuda")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms, e2e_s = [float(x) for x in t.tolist()]
+    return {
+        "metric": METRIC, "value": zones * args.steps / (ms / 1e3), "unit": "zone-cycles/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64 residual / f32 Jacobian+solve",
+        "data": "synthetic (seeded initial conditions of the named workload)",
+        "config": {"workload": args.workload, "description": desc, "zones": zones,
+                   "parallelism": "X3 slabs of %d planes on %d GPUs (NCCL halos)" % (cfg["N3"] // world, world),
+                   "l2": "flushed between timed steps (256 MB write, untimed)", "face_kernel_variants": tuned},
+        "e2e": {"value": zones * e2e_steps / e2e_s, "unit": "zone-cycles/s",
+                "h2d_bytes_per_step": host_in.numel() * 8 * world, "d2h_bytes_per_step": host_in.numel() * 8 * world},
+        "gpu_launches": None, "clocks": clocks_info, "roofline": None, "cpu_baseline": None,
+    }
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     torch.cuda.set_device(local_rank)
@@ -552,6 +629,8 @@ def main():
     ap.add_argument("--no-fd", action="store_true", help="skip the FD64 comparison path (profiler captures)")
     ap.add_argument("--variants", default=None,
                     help="face-kernel launch variants per direction, e.g. 1,5,5, instead of autotuning")
+    ap.add_argument("--decomp", default=None, choices=[None, "x3"],
+                    help="x3: split the grid into X3 slabs over the GPUs (strong scaling) instead of replicas")
     ap.add_argument("--per-zone", type=int, default=1,
                     help="fast Newton: 1 = per-zone loop in one kernel, 2 = compacted worklists")
     args = ap.parse_args()
@@ -591,6 +670,19 @@ def main():
             v, n, sample = cpu_reference(cfg, P, seconds=10.0)
             out["cpu_baseline"] = {"value": v, "unit": "zone-cycles/s", "cores": n, "kind": "port",
                                    "sample": sample}
+        if rank == 0:
+            print(json.dumps(out))
+        return
+    if args.decomp == "x3":
+        if world == 1:
+            import torch
+            import datetime
+            torch.distributed.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % _free_port(),
+                                                 rank=0, world_size=1, timeout=datetime.timedelta(seconds=120))
+        out = run_decomposed(args, rank, world, local_rank)
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
         if rank == 0:
             print(json.dumps(out))
         return
