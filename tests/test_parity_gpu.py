@@ -9,7 +9,7 @@ Tolerances (stated per test):
     difference with eps = 4e-8, so 1e-16 perturbations of the residual are
     amplified by ~1/eps);
   * primitives after N full timesteps on the plain FP64 path: 1e-12
-    relative (the north-star bar);
+    relative;
   * tangent / mixed paths: the error bounds stated in their tests.
 """
 import numpy as np
