@@ -170,3 +170,35 @@ def test_observations_recorded_by_the_steps():
     assert [r["time"] for r in recs] == due
     for k, v in last.items():
         assert recs[-1][k] == v, k
+
+
+def test_torus_emhd_steps_match_oracle():
+    """The torus with conduction and viscosity (nf = 7, the torus closure of
+    problem.cpp:7-55 and the MKS EMHD gradients): initial floors and three
+    steps of the FP64 parity path against the oracle, with the oracle's
+    geometry in the handle.  The stage pieces agree bit for bit (flux
+    divergence, the half stage's residual and its Newton solution); the
+    closure's exp and pow differ from glibc's in the last ulp, and the FD
+    Jacobian (eps = 4e-8) amplifies a 1e-16 residual difference by ~1/eps,
+    so every variable is held to 1e-6 of its scale, the FD Jacobian's own
+    bar."""
+    from grim_b200.timestepper import timeStepper
+    from oracle.oracle import Oracle
+    cfg = T.torus_config(**SHAPE, emhd=True)
+    ts, orc = timeStepper(cfg), Oracle(cfg)
+    _load_oracle_geometry(ts, orc)
+    P, _ = T.torus_prims(cfg, orc.geometry(C.CENTER))
+    ts.primOld.setVars(P)
+    orc.set_prims(P)
+    ts.problemInit()
+    orc.problem_init()
+    for n in range(3):
+        ts.timeStep()
+        orc.time_step(1)
+        assert abs(ts.dt - orc.dt) <= 1e-12 * orc.dt, n
+        g = interior(cfg, ts.primOld.getVars())
+        o = interior(cfg, orc.get_prims())
+        assert not np.isnan(g).any()
+        for v in range(g.shape[0]):
+            assert scaled_err(g[v:v + 1], o[v:v + 1]) <= 1e-6, (n, v, scaled_err(g[v:v + 1], o[v:v + 1]))
+    assert np.max(np.abs(interior(cfg, ts.primOld.getVars())[5:7])) > 0
