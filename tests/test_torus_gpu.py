@@ -178,27 +178,37 @@ def test_torus_emhd_steps_match_oracle():
     steps of the FP64 parity path against the oracle, with the oracle's
     geometry in the handle.  The stage pieces agree bit for bit (flux
     divergence, the half stage's residual and its Newton solution); the
-    closure's exp and pow differ from glibc's in the last ulp, and the FD
-    Jacobian (eps = 4e-8) amplifies a 1e-16 residual difference by ~1/eps,
-    so every variable is held to 1e-6 of its scale, the FD Jacobian's own
-    bar."""
+    closure's exp and pow differ from glibc's in the last ulp, and this
+    configuration (FD Jacobian with eps = 4e-8, three iterations, global
+    break) carries such differences far: the oracle itself, started from a
+    state one ulp away, moves by up to 1e-5 of a variable's scale in three
+    steps.  Each variable must stay within 10x that sensitivity."""
     from grim_b200.timestepper import timeStepper
     from oracle.oracle import Oracle
     cfg = T.torus_config(**SHAPE, emhd=True)
-    ts, orc = timeStepper(cfg), Oracle(cfg)
+    ts, orc, orc2 = timeStepper(cfg), Oracle(cfg), Oracle(cfg)
     _load_oracle_geometry(ts, orc)
     P, _ = T.torus_prims(cfg, orc.geometry(C.CENTER))
     ts.primOld.setVars(P)
-    orc.set_prims(P)
+    for o in (orc, orc2):
+        o.set_prims(P)
+        o.problem_init()
     ts.problemInit()
-    orc.problem_init()
+    assert scaled_err(interior(cfg, ts.primOld.getVars()), interior(cfg, orc.get_prims())) == 0.
+    Q = orc2.get_prims()
+    Q[:5] = np.nextafter(Q[:5], np.inf)  # one ulp up in the fluid variables
+    orc2.set_prims(Q)
     for n in range(3):
         ts.timeStep()
         orc.time_step(1)
+        orc2.time_step(1)
         assert abs(ts.dt - orc.dt) <= 1e-12 * orc.dt, n
         g = interior(cfg, ts.primOld.getVars())
         o = interior(cfg, orc.get_prims())
+        o2 = interior(cfg, orc2.get_prims())
         assert not np.isnan(g).any()
         for v in range(g.shape[0]):
-            assert scaled_err(g[v:v + 1], o[v:v + 1]) <= 1e-6, (n, v, scaled_err(g[v:v + 1], o[v:v + 1]))
+            err = scaled_err(g[v:v + 1], o[v:v + 1])
+            sens = scaled_err(o2[v:v + 1], o[v:v + 1])
+            assert err <= 10. * sens + 1e-12, (n, v, err, sens)
     assert np.max(np.abs(interior(cfg, ts.primOld.getVars())[5:7])) > 0
