@@ -479,3 +479,35 @@ def test_emf_matches_oracle(dim):
         b = e_orc[r][(0,) * (3 - dim) + sl] if dim == 2 else e_orc[r][sl]
         assert np.array_equal(a, b), r
         assert np.max(np.abs(b)) > 0
+
+
+def test_timestep_parity_1d():
+    """1D (the reference's dim = 1: X1 faces only, the induction of B2 / B3
+    by the X1 fluxes, zero-padded divergence): a Minkowski fast mode of 256
+    zones, 10 steps.  The FP64 parity path is within 1e-12 of the oracle;
+    the mixed Newton (FP32 Jacobian, per-zone relative tolerance 1e-10)
+    agrees with it to 1e-6 of the change of the state over the run, as in
+    the 2D error-bound test."""
+    cfg = PR.fast_mode_config(N=256, dim=1, nonlinearsolve_rtol=1e-10, nonlinearsolve_atol=1e-24,
+                              maxNonLinearIter=6)
+    P = PR.fast_mode_prims(cfg, seed=2)
+    from grim_b200.timestepper import timeStepper
+    from oracle.oracle import Oracle
+    ts, fast, orc = timeStepper(cfg), timeStepper(cfg), Oracle(cfg)
+    fast.setNewtonMode(C.NEWTON_MIXED32, 1, 1e-10)
+    for x in (ts, fast):
+        x.primOld.setVars(P)
+    orc.set_prims(P)
+    for _ in range(10):
+        ts.timeStep()
+        fast.timeStep()
+    orc.time_step(10)
+    g = interior(cfg, ts.primOld.getVars())
+    o = interior(cfg, orc.get_prims())
+    f = interior(cfg, fast.primOld.getVars())
+    assert g.shape == (8, 1, 1, 256)
+    assert scaled_err(g, o) <= 1e-12, scaled_err(g, o)
+    change = np.max(np.abs(o - interior(cfg, P)))
+    assert change > 0
+    assert np.max(np.abs(f - g)) <= 1e-6 * change
+    assert fast.stats()["nonFinite"] == 0

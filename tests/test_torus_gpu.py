@@ -212,3 +212,30 @@ def test_torus_emhd_steps_match_oracle():
             sens = scaled_err(o2[v:v + 1], o[v:v + 1])
             assert err <= 10. * sens + 1e-12, (n, v, err, sens)
     assert np.max(np.abs(interior(cfg, ts.primOld.getVars())[5:7])) > 0
+
+
+def test_torus_2d_steps_match_oracle():
+    """The axisymmetric torus (dim = 2, 64x32): initial floors and three
+    steps against the oracle to 1e-12 of each variable's scale, the 2D
+    paths of the MKS stencil (flux-CT with EMF3 only, zero-padded
+    divergence, Christoffel sources)."""
+    from grim_b200.timestepper import timeStepper
+    from oracle.oracle import Oracle
+    cfg = T.torus_config(N1=64, N2=32, N3=1, dim=2)
+    ts, orc = timeStepper(cfg), Oracle(cfg)
+    _load_oracle_geometry(ts, orc)
+    P, info = T.torus_prims(cfg, orc.geometry(C.CENTER))
+    assert np.isfinite(info["BFactor"])
+    ts.primOld.setVars(P)
+    orc.set_prims(P)
+    ts.problemInit()
+    orc.problem_init()
+    assert scaled_err(interior(cfg, ts.primOld.getVars()), interior(cfg, orc.get_prims())) <= 1e-12
+    for n in range(3):
+        ts.timeStep()
+        orc.time_step(1)
+        assert abs(ts.dt - orc.dt) <= 1e-13 * orc.dt, n
+        g = interior(cfg, ts.primOld.getVars())
+        o = interior(cfg, orc.get_prims())
+        assert not np.isnan(g).any()
+        assert scaled_err(g, o) <= 1e-12, (n, scaled_err(g, o))
