@@ -2036,11 +2036,14 @@ static void face_x1_tma_launch_rs(const DevCfg& c, const CUtensorMap* tmap, cons
   constexpr int DOF = 8 + C + V;
   const int nw = 4;
   const size_t smem = ((size_t)nw * 2 * DOF * kX1Box + 3 * DOF * 128) * sizeof(double) + 2 * nw * 8;
-  static bool attr = false;
-  if (!attr) {
+  // the attribute belongs to the function on each device that launches it
+  static unsigned long long attrDevices = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !(attrDevices & (1ULL << dev))) {
     cudaFuncSetAttribute(k_face_flux_x1_tma<C, V, MINB, RS, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    attr = true;
+    attrDevices |= 1ULL << dev;
   }
   k_face_flux_x1_tma<C, V, MINB, RS, PAIR><<<sm_count() * MINB, 32 * nw, smem, s>>>(*tmap, c, geoF, flux, st);
 }
@@ -2062,13 +2065,15 @@ static void face_strip_tma_launch_rs(const DevCfg& c, int dir, const CUtensorMap
   constexpr int DOF = 8 + C + V;
   const int nw = 4;
   const size_t smem = ((size_t)nw * 2 * 4 * kStripRows * DOF + 3 * DOF * 128) * sizeof(double) + 2 * nw * 8;
-  static bool attr = false;
-  if (!attr) {
+  static unsigned long long attrDevices = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !(attrDevices & (1ULL << dev))) {
     cudaFuncSetAttribute(k_face_flux_strip_tma<C, V, MINB, 1, RS, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
     cudaFuncSetAttribute(k_face_flux_strip_tma<C, V, MINB, 2, RS, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    attr = true;
+    attrDevices |= 1ULL << dev;
   }
   if (dir == 1)
     k_face_flux_strip_tma<C, V, MINB, 1, RS, PAIR>
@@ -2100,6 +2105,8 @@ static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double
         if (variant == 5) face_x1_tma_launch<C, V, 3, true>(c, &tmap[0], geoF, flux, st, s);
         else if (variant == 3) face_x1_tma_launch<C, V, 4>(c, &tmap[0], geoF, flux, st, s);
         else face_x1_tma_launch<C, V, 3>(c, &tmap[0], geoF, flux, st, s);
+      } else if (variant == 6) {
+        face_x1_launch<C, V, 4, true>(c, ps, geoF, flux, s);
       } else if (variant == 4 || variant == 5) {
         face_x1_launch<C, V, 3, true>(c, ps, geoF, flux, s);
       } else if (variant == 1 || variant == 3) {
@@ -2110,7 +2117,8 @@ static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double
       return;
     }
     if (variant >= 8 && tmap && st) {
-      if (variant == 10) face_strip_tma_launch<C, V, 3, true>(c, dir, tmap, geoF, geoC, flux, st, s);
+      if (variant == 11) face_strip_tma_launch<C, V, 4, true>(c, dir, tmap, geoF, geoC, flux, st, s);
+      else if (variant == 10) face_strip_tma_launch<C, V, 3, true>(c, dir, tmap, geoF, geoC, flux, st, s);
       else if (variant == 9) face_strip_tma_launch<C, V, 4>(c, dir, tmap, geoF, geoC, flux, st, s);
       else face_strip_tma_launch<C, V, 3>(c, dir, tmap, geoF, geoC, flux, st, s);
       return;
@@ -2118,6 +2126,7 @@ static void face_flux_t(const DevCfg& c, int dir, const double* ps, const double
     switch (variant) {
       case 8: face_strip_launch<C, V, 4, 3>(c, dir, ps, geoF, geoC, flux, s); break;
       case 10: face_strip_launch<C, V, 4, 3, true>(c, dir, ps, geoF, geoC, flux, s); break;
+      case 11: face_strip_launch<C, V, 4, 4, true>(c, dir, ps, geoF, geoC, flux, s); break;
       case 9: face_strip_launch<C, V, 4, 4>(c, dir, ps, geoF, geoC, flux, s); break;
       case 1: face_strip_launch<C, V, 4, 4>(c, dir, ps, geoF, geoC, flux, s); break;
       case 2: face_strip_launch<C, V, 2, 3>(c, dir, ps, geoF, geoC, flux, s); break;
@@ -2147,9 +2156,11 @@ void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, c
 // X1: 0, 1 = register budget 3 / 4 blocks; 2, 3 = the same with TMA-staged
 // rows (when the caller has a tensor map of the primitives); 4 = both face
 // states evaluated side by side; 5 = TMA-staged rows with both states side
-// by side, 3 blocks per SM.  X2 / X3: 0-5 = lane split x register budget;
+// by side, 3 blocks per SM; 6 = both states side by side, 4 blocks per SM.
+// X2 / X3: 0-5 = lane split x register budget;
 // 6, 7 = side by side with 8 / 4 i per warp; 8, 9 = TMA-staged chunks, 3 / 4
-// blocks per SM; 10 = TMA-staged chunks side by side, 3 blocks per SM.
+// blocks per SM; 10, 11 = TMA-staged chunks side by side, 3 / 4 blocks per
+// SM.
 // EMHD (10 dof), every direction: 0 = plain, 1 = TMA-staged, 2 blocks per SM.
 // tmap points at the caller's three tensor maps (X1, X2, X3 box shapes) of
 // the prim array, or is null (the TMA variants then run their plain
@@ -2157,7 +2168,7 @@ void face_flux(const DevCfg& c, int dir, const double* ps, const double* geoF, c
 int face_variants(const DevCfg& c, int dir) {
   (void)dir;
   if (c.conduction || c.viscosity) return 2;  // plain / TMA-staged, 2 blocks per SM
-  return dir == 0 ? 6 : 11;
+  return dir == 0 ? 7 : 12;
 }
 #endif  // !GRIM_SKIP_FACES
 

@@ -369,7 +369,7 @@ def test_autotuned_face_kernels_give_identical_results(mode):
 
     tuned = a.autotune()
     assert set(tuned) == {0, 1}
-    assert 0 <= tuned[0][0] < 6 and 0 <= tuned[1][0] < 11 and all(ms > 0 for _, ms in tuned.values())
+    assert 0 <= tuned[0][0] < 7 and 0 <= tuned[1][0] < 12 and all(ms > 0 for _, ms in tuned.values())
     for _ in range(3):
         a.timeStep()
         b.timeStep()
@@ -378,14 +378,14 @@ def test_autotuned_face_kernels_give_identical_results(mode):
     # default's divergence of fluxes
     ref_div, ref_flux = b.computeDivOfFluxes(P)
     # (X1 variants 2, 3, 5 and X2 variants 8, 9, 10 stage their stencils with TMA)
-    for d, nv in ((0, 6), (1, 11)):
+    for d, nv in ((0, 7), (1, 12)):
         for v in range(nv):
             a.setFaceVariant(d, v)
             div, flux = a.computeDivOfFluxes(P)
             assert same(div, ref_div, 1e-12) and same(flux, ref_flux, 1e-14), (d, v)
         a.setFaceVariant(d, 0)
     with pytest.raises(Exception):
-        a.setFaceVariant(1, 11)
+        a.setFaceVariant(1, 12)
 
 
 @pytest.mark.parametrize("mode", [C.NEWTON_PARITY_FD64, C.NEWTON_MIXED32])
@@ -426,7 +426,7 @@ def test_face_variants_3d(mode):
     ts.setNewtonMode(mode, 1, 0.0)
     exact = mode == C.NEWTON_PARITY_FD64
     ref_div, ref_flux = ts.computeDivOfFluxes(P)
-    for d, nv in ((0, 6), (1, 11), (2, 11)):
+    for d, nv in ((0, 7), (1, 12), (2, 12)):
         for v in range(nv):
             ts.setFaceVariant(d, v)
             div, flux = ts.computeDivOfFluxes(P)
