@@ -43,6 +43,19 @@ GRIM_D void geo_minkowski(ZoneGeo<R>& G, R x1, R x2) {
 
 template <class R>
 GRIM_D void geo_load(ZoneGeo<R>& G, const double* __restrict__ geo, long long Z, long long z) {
+#ifdef GRIM_FAST_MATH
+  // the metric and its inverse are symmetric: the fast path loads the upper
+  // triangles (10 + 10 words) and mirrors them, which also keeps 12 fewer
+  // values in registers; the stored lower triangles can differ from them in
+  // the last bit, so the parity path reads every word as the reference does
+#pragma unroll
+  for (int m = 0; m < 4; m++)
+#pragma unroll
+    for (int n = m; n < 4; n++) {
+      G.gcov[m][n] = G.gcov[n][m] = (R)__ldg(geo + (long long)(m * 4 + n) * Z + z);
+      G.gcon[m][n] = G.gcon[n][m] = (R)__ldg(geo + (long long)(16 + m * 4 + n) * Z + z);
+    }
+#else
 #pragma unroll
   for (int m = 0; m < 4; m++)
 #pragma unroll
@@ -50,6 +63,7 @@ GRIM_D void geo_load(ZoneGeo<R>& G, const double* __restrict__ geo, long long Z,
       G.gcov[m][n] = (R)__ldg(geo + (long long)(m * 4 + n) * Z + z);
       G.gcon[m][n] = (R)__ldg(geo + (long long)(16 + m * 4 + n) * Z + z);
     }
+#endif
   G.g = (R)__ldg(geo + 32LL * Z + z);
   G.alpha = (R)__ldg(geo + 33LL * Z + z);
   G.x1 = (R)__ldg(geo + 34LL * Z + z);
