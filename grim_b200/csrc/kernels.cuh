@@ -309,7 +309,7 @@ GRIM_D void riemann_face_pair(const DevCfg& c, int dir, const double* pl, const 
 // X1 faces: warp w of a row covers faces i0 .. i0+30; lane l reconstructs
 // zone i0 - 1 + l and, for l >= 1, computes the face between zones
 // i0 - 2 + l and i0 - 1 + l with the left state shuffled from lane l - 1.
-template <int COND, int VISC, int MINB, bool PAIR = false>
+template <int COND, int VISC, int MINB, bool PAIR, int RS>
 __global__ void __launch_bounds__(128, MINB) k_face_flux_x1(DevCfg c, const double* __restrict__ ps,
                                                       const double* __restrict__ geoF, double* __restrict__ flux) {
   constexpr int DOF = 8 + COND + VISC;
@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1(DevCfg c, const doub
   const bool reconOK = iz >= 2 && iz <= c.N1T - 3;
   double lo[DOF], ro[DOF];
   const long long z = zidx(c, reconOK ? iz : 2, j, k);
-  recon_zone<DOF>(c, ps, z, 1, c.reconstruction, lo, ro);
+  recon_zone_rs<DOF, RS>(c, ps, z, 1, lo, ro);
   double pl[DOF];
 #pragma unroll
   for (int v = 0; v < DOF; v++) pl[v] = __shfl_up_sync(0xffffffffu, ro[v], 1);
@@ -2002,11 +2002,20 @@ void emhd_prepass(const DevCfg& c, const double* ps, const double* geoC, double*
 // autotuner (grim_autotune): X1 faces by the register budget (3 or 4
 // resident 128-thread blocks per SM), X2 / X3 faces by that budget and by
 // the lane split QI (i per warp).  EMHD has one shape (2 resident blocks).
+// the reconstruction scheme is a compile-time constant of the X1 kernels
+// as of the TMA ones: one scheme's code per kernel keeps the instruction
+// footprint small
 template <int C, int V, int MINB, bool PAIR = false>
 static void face_x1_launch(const DevCfg& c, const double* ps, const double* geoF, double* flux, cudaStream_t s) {
   const long long warps = (long long)c.nfj * c.nfk * ((c.N1T - 5 + 30) / 31);
   const size_t park = PAIR ? 0 : 3 * (8 + C + V) * 128 * sizeof(double);
-  k_face_flux_x1<C, V, MINB, PAIR><<<nblk(warps * 32, 128), 128, park, s>>>(c, ps, geoF, flux);
+  const unsigned nb = nblk(warps * 32, 128);
+  switch (c.reconstruction) {
+    case GRIM_WENO5: k_face_flux_x1<C, V, MINB, PAIR, GRIM_WENO5><<<nb, 128, park, s>>>(c, ps, geoF, flux); break;
+    case GRIM_PPM: k_face_flux_x1<C, V, MINB, PAIR, GRIM_PPM><<<nb, 128, park, s>>>(c, ps, geoF, flux); break;
+    case GRIM_MP5: k_face_flux_x1<C, V, MINB, PAIR, GRIM_MP5><<<nb, 128, park, s>>>(c, ps, geoF, flux); break;
+    default: k_face_flux_x1<C, V, MINB, PAIR, GRIM_MINMOD><<<nb, 128, park, s>>>(c, ps, geoF, flux); break;
+  }
 }
 template <int C, int V, int QI, int MINB, bool PAIR = false>
 static void face_strip_launch(const DevCfg& c, int dir, const double* ps, const double* geoF, const double* geoC,
