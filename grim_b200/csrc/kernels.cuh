@@ -583,7 +583,7 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_strip_tma(const __grid_
 // state moves QI lanes up by shuffle, giving (32/QI - 1) x QI faces per
 // warp.  With QI = 4 each warp-wide load still covers whole 32-byte
 // sectors (4 consecutive doubles along i), as in the X1 kernel.
-template <int COND, int VISC, int QI, int MINB, bool PAIR, int DIR>
+template <int COND, int VISC, int QI, int MINB, bool PAIR, int DIR, int RS>
 __global__ void __launch_bounds__(128, MINB) k_face_flux_strip(DevCfg c, const double* __restrict__ ps,
                                                          const double* __restrict__ geoF,
                                                          const double* __restrict__ geoC, double* __restrict__ flux) {
@@ -611,7 +611,7 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_strip(DevCfg c, const d
   const long long s = stride_of(c, dir);
   const long long z = dir == 1 ? zidx(c, ic, xc, other) : zidx(c, ic, other, xc);
   double lo[DOF], ro[DOF];
-  recon_zone<DOF>(c, ps, z, s, c.reconstruction, lo, ro);
+  recon_zone_rs<DOF, RS>(c, ps, z, s, lo, ro);
   double pl[DOF];
 #pragma unroll
   for (int v = 0; v < DOF; v++) pl[v] = __shfl_up_sync(0xffffffffu, ro[v], QI);
@@ -2024,10 +2024,20 @@ static void face_strip_launch(const DevCfg& c, int dir, const double* ps, const 
   const long long other = (dir == 1) ? c.nfk : c.nfj;
   const long long warps = (long long)((c.N1T + QI - 1) / QI) * ((NT - 5 + 32 / QI - 2) / (32 / QI - 1)) * other;
   const size_t park = PAIR ? 0 : 3 * (8 + C + V) * 128 * sizeof(double);
-  if (dir == 1)
-    k_face_flux_strip<C, V, QI, MINB, PAIR, 1><<<nblk(warps * 32, 128), 128, park, s>>>(c, ps, geoF, geoC, flux);
-  else
-    k_face_flux_strip<C, V, QI, MINB, PAIR, 2><<<nblk(warps * 32, 128), 128, park, s>>>(c, ps, geoF, geoC, flux);
+  const unsigned nb = nblk(warps * 32, 128);
+  // one kernel per reconstruction scheme, as for the X1 faces
+#define GRIM_STRIP_RS(RS)                                                                                  \
+  do {                                                                                                     \
+    if (dir == 1) k_face_flux_strip<C, V, QI, MINB, PAIR, 1, RS><<<nb, 128, park, s>>>(c, ps, geoF, geoC, flux); \
+    else k_face_flux_strip<C, V, QI, MINB, PAIR, 2, RS><<<nb, 128, park, s>>>(c, ps, geoF, geoC, flux);        \
+  } while (0)
+  switch (c.reconstruction) {
+    case GRIM_WENO5: GRIM_STRIP_RS(GRIM_WENO5); break;
+    case GRIM_PPM: GRIM_STRIP_RS(GRIM_PPM); break;
+    case GRIM_MP5: GRIM_STRIP_RS(GRIM_MP5); break;
+    default: GRIM_STRIP_RS(GRIM_MINMOD); break;
+  }
+#undef GRIM_STRIP_RS
 }
 static int sm_count() {
   static int n = 0;
