@@ -1511,7 +1511,7 @@ __global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : kN
         for (int m = 0; m < 4; m++)
 #pragma unroll
           for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = (T)G.gcov[m][q]; Gt.gcon[m][q] = (T)G.gcon[m][q]; }
-        Gt.g = (T)G.g; Gt.alpha = (T)G.alpha; Gt.x1 = (T)G.x1; Gt.x2 = (T)G.x2; Gt.dyn = (T)G.dyn;
+        Gt.g = (T)G.g; Gt.alpha = (T)G.alpha; Gt.ialpha = (T)G.ialpha; Gt.x1 = (T)G.x1; Gt.x2 = (T)G.x2; Gt.dyn = (T)G.dyn;
         tangent_jacobian<COND, VISC, T>(P, K, Gt, c, J);
       }
       T bv[NF], xv[NF];
@@ -1624,7 +1624,7 @@ GRIM_D bool list_iter_zone(const DevCfg& c, int stage, int it, const StageBufs& 
   for (int m = 0; m < 4; m++)
 #pragma unroll
     for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = (T)G.gcov[m][q]; Gt.gcon[m][q] = (T)G.gcon[m][q]; }
-  Gt.g = (T)G.g; Gt.alpha = (T)G.alpha; Gt.x1 = (T)G.x1; Gt.x2 = (T)G.x2; Gt.dyn = (T)G.dyn;
+  Gt.g = (T)G.g; Gt.alpha = (T)G.alpha; Gt.ialpha = (T)G.ialpha; Gt.x1 = (T)G.x1; Gt.x2 = (T)G.x2; Gt.dyn = (T)G.dyn;
   StageConst<NF> K;
   load_stage_const<COND, VISC>(K, c, stage, b, z, G);
   double P[NF], R[NF];

@@ -102,7 +102,7 @@ __global__ void k_count_ops(DevCfg c, int stage, StageBufs b, long long z, doubl
     ZoneGeo<C8> Gc;
     for (int m = 0; m < 4; m++)
       for (int q = 0; q < 4; q++) { Gc.gcov[m][q] = C8(G.gcov[m][q]); Gc.gcon[m][q] = C8(G.gcon[m][q]); }
-    Gc.g = C8(G.g); Gc.alpha = C8(G.alpha); Gc.x1 = C8(G.x1); Gc.x2 = C8(G.x2); Gc.dyn = C8(G.dyn);
+    Gc.g = C8(G.g); Gc.alpha = C8(G.alpha); Gc.ialpha = C8(G.ialpha); Gc.x1 = C8(G.x1); Gc.x2 = C8(G.x2); Gc.dyn = C8(G.dyn);
     C8 P[NF], R[NF];
     for (int v = 0; v < NF; v++) P[v] = C8(Pd[v]);
     clear();
@@ -117,7 +117,7 @@ __global__ void k_count_ops(DevCfg c, int stage, StageBufs b, long long z, doubl
     ZoneGeo<C4> Gt;
     for (int m = 0; m < 4; m++)
       for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = C4(G.gcov[m][q]); Gt.gcon[m][q] = C4(G.gcon[m][q]); }
-    Gt.g = C4(G.g); Gt.alpha = C4(G.alpha); Gt.x1 = C4(G.x1); Gt.x2 = C4(G.x2); Gt.dyn = C4(G.dyn);
+    Gt.g = C4(G.g); Gt.alpha = C4(G.alpha); Gt.ialpha = C4(G.ialpha); Gt.x1 = C4(G.x1); Gt.x2 = C4(G.x2); Gt.dyn = C4(G.dyn);
     C4 J[NF][NF];
     clear();
     tangent_jacobian<COND, VISC, C4, true>(Pd, K, Gt, c, J);
@@ -136,7 +136,7 @@ __global__ void k_count_ops(DevCfg c, int stage, StageBufs b, long long z, doubl
     ZoneGeo<C8> Gt;
     for (int m = 0; m < 4; m++)
       for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = C8(G.gcov[m][q]); Gt.gcon[m][q] = C8(G.gcon[m][q]); }
-    Gt.g = C8(G.g); Gt.alpha = C8(G.alpha); Gt.x1 = C8(G.x1); Gt.x2 = C8(G.x2); Gt.dyn = C8(G.dyn);
+    Gt.g = C8(G.g); Gt.alpha = C8(G.alpha); Gt.ialpha = C8(G.ialpha); Gt.x1 = C8(G.x1); Gt.x2 = C8(G.x2); Gt.dyn = C8(G.dyn);
     C8 J[NF][NF];
     clear();
     tangent_jacobian<COND, VISC, C8>(Pd, K, Gt, c, J);
@@ -154,7 +154,7 @@ __global__ void k_count_ops(DevCfg c, int stage, StageBufs b, long long z, doubl
     ZoneGeo<C8> Gc;
     for (int m = 0; m < 4; m++)
       for (int q = 0; q < 4; q++) { Gc.gcov[m][q] = C8(G.gcov[m][q]); Gc.gcon[m][q] = C8(G.gcon[m][q]); }
-    Gc.g = C8(G.g); Gc.alpha = C8(G.alpha); Gc.x1 = C8(G.x1); Gc.x2 = C8(G.x2); Gc.dyn = C8(G.dyn);
+    Gc.g = C8(G.g); Gc.alpha = C8(G.alpha); Gc.ialpha = C8(G.ialpha); Gc.x1 = C8(G.x1); Gc.x2 = C8(G.x2); Gc.dyn = C8(G.dyn);
     const double* ps = b.ps;
     // reconstruction of every dof of the zone along X1
     clear();

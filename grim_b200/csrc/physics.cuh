@@ -17,6 +17,7 @@ struct ZoneGeo {
   R gcov[4][4];
   R gcon[4][4];
   R g, alpha;
+  R ialpha;  // 1 / alpha, formed once per load (the fast path multiplies by it)
   R x1, x2;  // physical coordinates (closures)
   R dyn;     // x1^1.5 (torus closure)
 };
@@ -36,7 +37,7 @@ GRIM_D void geo_minkowski(ZoneGeo<R>& G, R x1, R x2) {
     for (int n = 0; n < 4; n++) { G.gcov[m][n] = R(0); G.gcon[m][n] = R(0); }
   G.gcov[0][0] = R(-1); G.gcov[1][1] = R(1); G.gcov[2][2] = R(1); G.gcov[3][3] = R(1);
   G.gcon[0][0] = R(-1); G.gcon[1][1] = R(1); G.gcon[2][2] = R(1); G.gcon[3][3] = R(1);
-  G.g = R(1); G.alpha = R(1);
+  G.g = R(1); G.alpha = R(1); G.ialpha = R(1);
   G.x1 = x1; G.x2 = x2;
   G.dyn = R(0);
 }
@@ -66,6 +67,7 @@ GRIM_D void geo_load(ZoneGeo<R>& G, const double* __restrict__ geo, long long Z,
 #endif
   G.g = (R)__ldg(geo + 32LL * Z + z);
   G.alpha = (R)__ldg(geo + 33LL * Z + z);
+  G.ialpha = R(1) / G.alpha;
   G.x1 = (R)__ldg(geo + 34LL * Z + z);
   G.x2 = (R)__ldg(geo + 35LL * Z + z);
   G.dyn = (R)__ldg(geo + 36LL * Z + z);
@@ -170,7 +172,11 @@ GRIM_D void elem_set(ElemT<S, R>& e, const S& rho_in, const S& u_in, const S& v1
   e.soundSpeed = dsqrt(Gam * e.pressure / (e.rho + Gam * e.u));
   e.gam = dsqrt(T(1) + G.gcov[1][1] * v1 * v1 + G.gcov[2][2] * v2 * v2 + G.gcov[3][3] * v3 * v3 +
                 T(2) * (G.gcov[1][2] * v1 * v2 + G.gcov[1][3] * v1 * v3 + G.gcov[2][3] * v2 * v3));
+#ifdef GRIM_FAST_MATH
+  e.uCon[0] = e.gam * G.ialpha;
+#else
   e.uCon[0] = e.gam / G.alpha;
+#endif
   e.uCon[1] = v1 - e.gam * G.gcon[0][1] * G.alpha;
   e.uCon[2] = v2 - e.gam * G.gcon[0][2] * G.alpha;
   e.uCon[3] = v3 - e.gam * G.gcon[0][3] * G.alpha;
@@ -255,19 +261,38 @@ template <int COND, int VISC, class S, class R>
 GRIM_D void char_speeds(const ElemT<S, R>& e, const ZoneGeo<R>& G, int dir, const DevCfg& c, S& minSpeed,
                         S& maxSpeed) {
   const S Gam = S(c.Gam);
-  S cAlvenSqr = e.bSqr / (e.rho + Gam * e.u + e.bSqr);
 #ifdef GRIM_FAST_MATH
-  // c_s^2 itself: without conduction or viscosity the element's c_s (a
-  // square root) is then dead code
-  S csSqr = (COND || VISC) ? e.soundSpeed * e.soundSpeed : Gam * e.pressure / (e.rho + Gam * e.u);
+  // without conduction or viscosity: c_s^2 itself (the element's c_s, a
+  // square root, is then dead code) and c_A^2 over one reciprocal of the
+  // product of their denominators
+  S cAlvenSqr, csSqr;
+  if constexpr (COND || VISC) {
+    cAlvenSqr = e.bSqr / (e.rho + Gam * e.u + e.bSqr);
+    csSqr = e.soundSpeed * e.soundSpeed;
+  } else {
+    const S w1 = e.rho + Gam * e.u, w2 = w1 + e.bSqr;
+    const S r = S(1.) / (w1 * w2);
+    cAlvenSqr = e.bSqr * w1 * r;
+    csSqr = Gam * e.pressure * w2 * r;
+  }
 #else
+  S cAlvenSqr = e.bSqr / (e.rho + Gam * e.u + e.bSqr);
   S csSqr = e.soundSpeed * e.soundSpeed;
 #endif
   S cVisSqr = S(0.);
   if (VISC) cVisSqr = S(4.) / S(3.) / (e.rho + Gam * e.u) * e.rho * e.nu / e.tau;
   S cConSqr = S(0.);
   if (COND) cConSqr = (Gam - S(1.)) * e.chi / e.tau;
+#ifdef GRIM_FAST_MATH
+  // with no conduction the combination is (cs^2 + |cs^2|) / 2 = cs^2
+  // (cs^2 >= 0: a square root of a square is the magnitude exactly)
+  if constexpr (COND)
+    cConSqr = S(0.5) * (csSqr + cConSqr + dsqrt(csSqr * csSqr + cConSqr * cConSqr));
+  else
+    cConSqr = csSqr;
+#else
   cConSqr = S(0.5) * (csSqr + cConSqr + dsqrt(csSqr * csSqr + cConSqr * cConSqr));
+#endif
   csSqr = cConSqr + cVisSqr;
   csSqr = csSqr + cAlvenSqr - csSqr * cAlvenSqr;
   if (csSqr > S(1.)) csSqr = S(1.);
