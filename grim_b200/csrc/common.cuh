@@ -188,6 +188,17 @@ GRIM_HD T val(const Dual<T, N>& x) { return x.v; }
 
 GRIM_HD double dsqrt(double x) { return sqrt(x); }
 GRIM_HD float dsqrt(float x) { return sqrtf(x); }
+// 1 / sqrt(x) (the fast path forms gamma and 1 / gamma from one call)
+GRIM_HD double drsqrt(double x) { return rsqrt(x); }
+GRIM_HD float drsqrt(float x) { return rsqrtf(x); }
+template <class T, int N>
+GRIM_HD Dual<T, N> drsqrt(const Dual<T, N>& a) {
+  Dual<T, N> r; r.v = drsqrt(a.v);
+  const T h = T(-0.5) * r.v * r.v * r.v;
+#pragma unroll
+  for (int k = 0; k < N; k++) r.d[k] = a.d[k] * h;
+  return r;
+}
 template <class T, int N>
 GRIM_HD Dual<T, N> dsqrt(const Dual<T, N>& a) {
   Dual<T, N> r; r.v = dsqrt(a.v);

@@ -46,6 +46,7 @@ struct Cnt {
   // the scalar helpers the physics calls (found by argument lookup)
   friend GRIM_D Cnt val(Cnt a) { return a; }
   friend GRIM_D Cnt dsqrt(Cnt a) { tick(3); return Cnt(sqrt((double)a.v)); }
+  friend GRIM_D Cnt drsqrt(Cnt a) { tick(3); return Cnt(1. / sqrt((double)a.v)); }
   friend GRIM_D Cnt dexp(Cnt a) { tick(4); return Cnt(exp((double)a.v)); }
   friend GRIM_D Cnt dfabs(Cnt a) { return Cnt(a.v < B(0) ? -a.v : a.v); }
   friend GRIM_D Cnt fabs(Cnt a) { return dfabs(a); }

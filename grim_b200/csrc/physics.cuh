@@ -170,11 +170,17 @@ GRIM_D void elem_set(ElemT<S, R>& e, const S& rho_in, const S& u_in, const S& v1
   e.pressure = (Gam - T(1.)) * e.u;
   e.temperature = dmaxc(e.pressure / e.rho, (T)c.TFloor);
   e.soundSpeed = dsqrt(Gam * e.pressure / (e.rho + Gam * e.u));
-  e.gam = dsqrt(T(1) + G.gcov[1][1] * v1 * v1 + G.gcov[2][2] * v2 * v2 + G.gcov[3][3] * v3 * v3 +
-                T(2) * (G.gcov[1][2] * v1 * v2 + G.gcov[1][3] * v1 * v3 + G.gcov[2][3] * v2 * v3));
 #ifdef GRIM_FAST_MATH
+  // gamma and 1 / gamma from one reciprocal square root: u^0 = gamma / alpha
+  // and 1 / u^0 = alpha / gamma without divisions
+  const S gsq = T(1) + G.gcov[1][1] * v1 * v1 + G.gcov[2][2] * v2 * v2 + G.gcov[3][3] * v3 * v3 +
+                T(2) * (G.gcov[1][2] * v1 * v2 + G.gcov[1][3] * v1 * v3 + G.gcov[2][3] * v2 * v3);
+  const S rgam = drsqrt(gsq);
+  e.gam = gsq * rgam;
   e.uCon[0] = e.gam * G.ialpha;
 #else
+  e.gam = dsqrt(T(1) + G.gcov[1][1] * v1 * v1 + G.gcov[2][2] * v2 * v2 + G.gcov[3][3] * v3 * v3 +
+                T(2) * (G.gcov[1][2] * v1 * v2 + G.gcov[1][3] * v1 * v3 + G.gcov[2][3] * v2 * v3));
   e.uCon[0] = e.gam / G.alpha;
 #endif
   e.uCon[1] = v1 - e.gam * G.gcon[0][1] * G.alpha;
@@ -187,7 +193,7 @@ GRIM_D void elem_set(ElemT<S, R>& e, const S& rho_in, const S& u_in, const S& v1
   e.bCon[0] = B1 * e.uCov[1] + B2 * e.uCov[2] + B3 * e.uCov[3];
 #ifdef GRIM_FAST_MATH
   {
-    const S iu0 = T(1) / e.uCon[0];  // one division for the three
+    const S iu0 = G.alpha * rgam;  // 1 / u^0
     e.bCon[1] = (B1 + e.bCon[0] * e.uCon[1]) * iu0;
     e.bCon[2] = (B2 + e.bCon[0] * e.uCon[2]) * iu0;
     e.bCon[3] = (B3 + e.bCon[0] * e.uCon[3]) * iu0;

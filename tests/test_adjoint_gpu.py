@@ -76,8 +76,11 @@ def test_adjoint_matches_central_fd(recon, riemann):
     difference whose bracket contains such a switch measures an average of
     two branches, so the 1e-6 check applies where the map is smooth over the
     bracket: the differences at h = 1e-6 and h = 1e-7 agree (to the 1e-7
-    difference's roundoff), and there the adjoint matches one of them to
-    1e-6.  At least 8 of 32 random picks must qualify."""
+    difference's roundoff) and the second differences show no slope jump at
+    the point itself (a switch within 1e-7 of the point sits in both
+    brackets); there the adjoint matches one of the central differences to
+    1e-6.  At least 10 of 64 random picks must
+    qualify."""
     N, nsteps = 24, 6
     cfg = PR.fast_mode_config(N=N, reconstruction=recon, riemannSolver=riemann, maxNonLinearIter=6,
                               nonlinearsolve_atol=0.0)
@@ -89,26 +92,36 @@ def test_adjoint_matches_central_fd(recon, riemann):
     scale = np.max(np.abs(gi))
     rng = np.random.default_rng(5)
 
-    def fd(v, j, i, h):
-        Pp, Pm = P.copy(), P.copy()
-        Pp[v, 0, j + g, i + g] += h
-        Pm[v, 0, j + g, i + g] -= h
-        return (_loss(cfg, Pp, nsteps) - _loss(cfg, Pm, nsteps)) / (2 * h)
+    L0 = _loss(cfg, P, nsteps)
+
+    def shifted(v, j, i, h):
+        Q = P.copy()
+        Q[v, 0, j + g, i + g] += h
+        return _loss(cfg, Q, nsteps)
 
     smooth = 0
-    for n in range(32):
+    for n in range(64):
         v = n % 8
         j, i = rng.integers(0, N, 2)
         ad = gi[v, 0, j, i]
         tol = max(abs(ad), 1e-3 * scale)
-        f6, f7 = fd(v, j, i, 1e-6), fd(v, j, i, 1e-7)
+        p6, m6 = shifted(v, j, i, 1e-6), shifted(v, j, i, -1e-6)
+        p7, m7 = shifted(v, j, i, 1e-7), shifted(v, j, i, -1e-7)
+        f6, f7 = (p6 - m6) / 2e-6, (p7 - m7) / 2e-7
         if abs(f6 - f7) > 3e-6 * tol:
             continue  # a branch switch inside the bracket
+        # a slope jump D at the point (a switch closer than 1e-7, inside both
+        # brackets) makes the second differences (p - 2 L0 + m) / h equal D
+        # at every h; a smooth map makes them h L''.  Their combination
+        # s7 - s6 / 10 is 0.9 D.
+        s6, s7 = (p6 - 2 * L0 + m6) / 1e-6, (p7 - 2 * L0 + m7) / 1e-7
+        if abs(s7 - s6 / 10.) > 1e-6 * tol:
+            continue  # a switch so close to the point that both brackets hold it
         smooth += 1
         # the two differences carry different errors (truncation at 1e-6,
         # roundoff at 1e-7); the adjoint must match one of them
         assert min(abs(f6 - ad), abs(f7 - ad)) <= 1e-6 * tol, (v, j, i, f6, f7, ad)
-    assert smooth >= 8, smooth
+    assert smooth >= 10, smooth
 
 
 def test_adjoint_checkpoint_interval_does_not_change_the_gradient():
