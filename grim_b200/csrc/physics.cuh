@@ -354,15 +354,18 @@ GRIM_D void ideal_jacobian(const double* P, const KC& K, const ZoneGeo<T>& G, co
   T gv[3];
 #pragma unroll
   for (int j = 0; j < 3; j++) gv[j] = G.gcov[j + 1][1] * v[0] + G.gcov[j + 1][2] * v[1] + G.gcov[j + 1][3] * v[2];
-  const T gam = dsqrt(T(1.) + v[0] * gv[0] + v[1] * gv[1] + v[2] * gv[2]);
+  // gamma and 1 / gamma from one reciprocal square root
+  const T gsq = T(1.) + v[0] * gv[0] + v[1] * gv[1] + v[2] * gv[2];
+  const T rgam = drsqrt(gsq);
+  const T gam = gsq * rgam;
   T uCon[4], uCov[4], bCon[4], bCov[4];
-  uCon[0] = gam / G.alpha;
+  uCon[0] = gam * G.ialpha;
 #pragma unroll
   for (int i = 1; i < 4; i++) uCon[i] = v[i - 1] - gam * G.gcon[0][i] * G.alpha;
 #pragma unroll
   for (int m = 0; m < 4; m++)
     uCov[m] = G.gcov[m][0] * uCon[0] + G.gcov[m][1] * uCon[1] + G.gcov[m][2] * uCon[2] + G.gcov[m][3] * uCon[3];
-  const T iu0 = T(1.) / uCon[0];
+  const T iu0 = G.alpha * rgam;  // 1 / u^0
   bCon[0] = B[0] * uCov[1] + B[1] * uCov[2] + B[2] * uCov[3];
 #pragma unroll
   for (int i = 1; i < 4; i++) bCon[i] = (B[i - 1] + bCon[0] * uCon[i]) * iu0;
@@ -391,9 +394,9 @@ GRIM_D void ideal_jacobian(const double* P, const KC& K, const ZoneGeo<T>& G, co
   // velocity columns
 #pragma unroll
   for (int j = 0; j < 3; j++) {
-    const T dg = gv[j] / gam;
+    const T dg = gv[j] * rgam;
     T du[4], duCov[4], db[4];
-    du[0] = dg / G.alpha;
+    du[0] = dg * G.ialpha;
 #pragma unroll
     for (int i = 1; i < 4; i++) du[i] = ((i == j + 1) ? T(1.) : T(0.)) - dg * G.gcon[0][i] * G.alpha;
 #pragma unroll
