@@ -65,11 +65,41 @@ GRIM_D int bc_map(int x, int g, int N, int lo, int hi) {
 // mirror only; periodic directions are left as they are (the reference fills
 // them in grid::communicate at the end of each stage).  Applied direction by
 // direction over full spans, its result is the gather below.
+// the n-th ghost zone: the X1 ghost columns (all j, k), then the X2 ghost
+// rows of the X1 interior (all k), then the X3 ghost planes of the X1 / X2
+// interior; n < Z - Zint
+GRIM_D void ghost_ijk(const DevCfg& c, long long n, int& i, int& j, int& k) {
+  const long long a = 2LL * c.g1 * c.N2T * c.N3T, b = (long long)c.N1 * 2 * c.g2 * c.N3T;
+  if (n < a) {
+    const int gi = (int)(n % (2 * c.g1));
+    const long long r = n / (2 * c.g1);
+    i = gi < c.g1 ? gi : c.N1 + gi;
+    j = (int)(r % c.N2T);
+    k = (int)(r / c.N2T);
+  } else if (n < a + b) {
+    const long long m = n - a;
+    i = c.g1 + (int)(m % c.N1);
+    const long long r = m / c.N1;
+    const int gj = (int)(r % (2 * c.g2));
+    j = gj < c.g2 ? gj : c.N2 + gj;
+    k = (int)(r / (2 * c.g2));
+  } else {
+    const long long m = n - a - b;
+    i = c.g1 + (int)(m % c.N1);
+    const long long r = m / c.N1;
+    j = c.g2 + (int)(r % c.N2);
+    const int gk = (int)(r / c.N2);
+    k = gk < c.g3 ? gk : c.N3 + gk;
+  }
+}
+
+// one thread per ghost zone
 static __global__ void k_ghost_fill(DevCfg c, double* __restrict__ prim, int nv) {
-  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (z >= c.Z) return;
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= c.Z - c.Zint) return;
   int i, j, k;
-  zijk(c, z, i, j, k);
+  ghost_ijk(c, n, i, j, k);
+  const long long z = zidx(c, i, j, k);
   const bool p1 = c.bc[0] == GRIM_PERIODIC || c.bc[1] == GRIM_PERIODIC;
   const bool p2 = c.bc[2] == GRIM_PERIODIC || c.bc[3] == GRIM_PERIODIC;
   const bool p3 = c.bc[4] == GRIM_PERIODIC || c.bc[5] == GRIM_PERIODIC;
@@ -1981,7 +2011,7 @@ static inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) 
 
 #if !defined(GRIM_ONLY_FACES)
 void ghost_fill(const DevCfg& c, double* prim, int nv, cudaStream_t s) {
-  k_ghost_fill<<<nblk(c.Z, 256), 256, 0, s>>>(c, prim, nv);
+  if (c.Z > c.Zint) k_ghost_fill<<<nblk(c.Z - c.Zint, 256), 256, 0, s>>>(c, prim, nv);
 }
 void communicate(const DevCfg& c, double* prim, int nv, cudaStream_t s) {
   k_communicate<<<nblk(c.Z, 256), 256, 0, s>>>(c, prim, nv);
