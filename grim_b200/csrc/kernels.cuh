@@ -994,9 +994,7 @@ GRIM_D void atomic_max_pos(double* addr, double v) {
 
 // one zone's sum over directions of max(c_max/dX_d, |c_min/dX_d|)
 template <int COND, int VISC>
-GRIM_D double zone_inv_dt(const DevCfg& c, const double* pv, const ZoneGeo<double>& G) {
-  ElemT<double, double> e;
-  elem_of<COND, VISC>(e, c, pv, G);
+GRIM_D double elem_inv_dt(const DevCfg& c, const ElemT<double, double>& e, const ZoneGeo<double>& G) {
   double acc = 0.;
 #pragma unroll
   for (int d = 0; d < 3; d++) {
@@ -1009,6 +1007,12 @@ GRIM_D double zone_inv_dt(const DevCfg& c, const double* pv, const ZoneGeo<doubl
     }
   }
   return acc;
+}
+template <int COND, int VISC>
+GRIM_D double zone_inv_dt(const DevCfg& c, const double* pv, const ZoneGeo<double>& G) {
+  ElemT<double, double> e;
+  elem_of<COND, VISC>(e, c, pv, G);
+  return elem_inv_dt<COND, VISC>(c, e, G);
 }
 
 // block reduction of the threads' values, then one atomic max per block
@@ -1080,15 +1084,21 @@ __global__ void __launch_bounds__(128) k_stage_finish(DevCfg c, TorusCfg t, cons
     for (int v = 0; v < DOF; v++) q[v] = zero ? 0. : src[(long long)v * Z + s];
     ZoneGeo<double> G;
     load_geo(G, c, geoC, z, i, j, 0.5, 0.5);
+    // the floors' last element, when it is that of the final state, serves
+    // the dt speeds below (the same function of the same values)
+    ElemT<double, double> ef;
+    bool haveElem = false;
     if constexpr (FLOOR) {
       const long long gz = gidx(c, i, j);
-      torus_floor_zone<COND, VISC>(c, t, q, G, __ldg(geoC + 37LL * c.GZ + gz), __ldg(geoC + 38LL * c.GZ + gz),
-                                   POST && *nanFlag != 0);
+      haveElem = torus_floor_zone<COND, VISC>(c, t, q, G, __ldg(geoC + 37LL * c.GZ + gz),
+                                              __ldg(geoC + 38LL * c.GZ + gz), POST && *nanFlag != 0,
+                                              POST ? &ef : nullptr);
     }
 #pragma unroll
     for (int v = 0; v < DOF; v++) dst[(long long)v * Z + z] = q[v];
     if constexpr (POST) {
-      if (dtOn && !in_exchange_ghost(c, i, j, k)) best = zone_inv_dt<COND, VISC>(c, q, G);
+      if (dtOn && !in_exchange_ghost(c, i, j, k))
+        best = haveElem ? elem_inv_dt<COND, VISC>(c, ef, G) : zone_inv_dt<COND, VISC>(c, q, G);
       const bool inside = i >= c.g1 && i < c.N1 + c.g1 && j >= c.g2 && j < c.N2 + c.g2 && k >= c.g3 &&
                           k < c.N3 + c.g3;
       if (inside)

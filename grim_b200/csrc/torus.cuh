@@ -36,9 +36,12 @@ GRIM_D void elem_of(ElemT<double, double>& e, const DevCfg& c, const double* q, 
 // applyFloor (problem.cpp:542-712) on one zone's primitives q, held in
 // registers, after the NaN reset of fullStepDiagnostics when nanReset;
 // minRho, minU are the zone's floor values (geometry words 37, 38)
+// Returns true when the element left in eOut (if given) is the element of
+// the final q (no change after its last evaluation), so a caller needing
+// that element can use it as is.
 template <int COND, int VISC>
-GRIM_D void torus_floor_zone(const DevCfg& c, const TorusCfg& t, double* q, const ZoneGeo<double>& G, double minRho,
-                             double minU, bool nanReset) {
+GRIM_D bool torus_floor_zone(const DevCfg& c, const TorusCfg& t, double* q, const ZoneGeo<double>& G, double minRho,
+                             double minU, bool nanReset, ElemT<double, double>* eOut = nullptr) {
   constexpr int NFT = 5 + COND + VISC, DOFT = NFT + 3;
   if (nanReset) {
     bool bad = false;
@@ -129,6 +132,7 @@ GRIM_D void torus_floor_zone(const DevCfg& c, const TorusCfg& t, double* q, cons
   }  // drift-frame fix
   // maximum Lorentz factor
   elem_of<COND, VISC>(e, c, q, G);
+  bool current = true;
   {
     const double lf2 = e.gam * e.gam;
     const double gm2 = t.MaxLorentzFactor * t.MaxLorentzFactor;
@@ -137,6 +141,7 @@ GRIM_D void torus_floor_zone(const DevCfg& c, const TorusCfg& t, double* q, cons
       q[U1] *= mf;
       q[U2] *= mf;
       q[U3] *= mf;
+      current = false;
     }
   }
   if (COND || VISC) {
@@ -155,7 +160,10 @@ GRIM_D void torus_floor_zone(const DevCfg& c, const TorusCfg& t, double* q, cons
       const double f = (dP > 0.) ? 1. / fmax(dP / dPmaxPlus, 1.) : 1. / fmax(dP / dPmaxMinus, 1.);
       q[5 + COND] = q[5 + COND] * f;
     }
+    current = false;
   }
+  if (eOut && current) *eOut = e;
+  return current;
 }
 
 // applyFloor on every zone of p in place, after the NaN reset when
