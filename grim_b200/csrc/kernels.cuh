@@ -974,7 +974,7 @@ __global__ void __launch_bounds__(128, kEpiMinBlocks[PART]) k_stage_epilogue(Dev
     double cons = b.consOld[(long long)(NF + b3) * Z + z] - fac * div[NF + b3];
     b.prim[(long long)(c.B1 + b3) * Z + z] = cons / G.g;
   }
-  if (stage == GRIM_HALF_STEP)
+  if (stage == GRIM_HALF_STEP && !b.guessOld)
 #pragma unroll
     for (int v = 0; v < NF; v++) b.prim[(long long)v * Z + z] = b.pold[(long long)v * Z + z];
   }  // PART != 1
@@ -1528,8 +1528,9 @@ __global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : kN
     StageConst<NF> K;
     load_stage_const<COND, VISC>(K, c, stage, b, z, G);
     double P[NF], R[NF];
+    const double* guess = (stage == GRIM_HALF_STEP && b.guessOld) ? b.pold : b.prim;
 #pragma unroll
-    for (int v = 0; v < NF; v++) P[v] = b.prim[(long long)v * Z + z];
+    for (int v = 0; v < NF; v++) P[v] = guess[(long long)v * Z + z];
     bool haveR = false;
     double l2first = 0.;
     int it = 0;

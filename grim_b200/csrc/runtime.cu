@@ -253,9 +253,10 @@ static bool encode_prim_tmap(const DevCfg& c, double* base, int dir, CUtensorMap
   return r == CUDA_SUCCESS;
 }
 
-static StageBufs stage_bufs(grim_handle* h, int stage) {
+static StageBufs stage_bufs(grim_handle* h, int stage, bool guessOld = false) {
   StageBufs b;
   memset(&b, 0, sizeof(b));
+  b.guessOld = guessOld ? 1 : 0;
   b.ps = (stage == GRIM_HALF_STEP) ? h->primOld : h->primHalf;
   b.pold = h->primOld;
   b.prim = h->prim;
@@ -296,10 +297,16 @@ static StageBufs stage_bufs(grim_handle* h, int stage) {
 
 static long long g_launch_counter = 0;
 
-static void enqueue_stencil(grim_handle* h, int stage) {
+// a step's per-zone fast Newton takes the half stage's guess straight from
+// primOld; the stand-alone stage pieces (grim_stage_setup and
+// grim_newton_solve) and the batch keep it in prim
+static bool step_guess_old(const grim_handle* h) {
+  return h->cfg.newtonMode != GRIM_NEWTON_PARITY_FD64 && h->cfg.perZoneConvergence != 2;
+}
+static void enqueue_stencil(grim_handle* h, int stage, bool guessOld = false) {
   const DevCfg& c = h->dc;
   cudaStream_t s = h->stream;
-  StageBufs b = stage_bufs(h, stage);
+  StageBufs b = stage_bufs(h, stage, guessOld);
   if (c.conduction || c.viscosity) {
     PROF(GRIM_PROF_EMHD_PREPASS);
     KNS_CALL(h, emhd_prepass, c, b.ps, b.geoC, h->uT, s);
@@ -316,10 +323,10 @@ static void enqueue_stencil(grim_handle* h, int stage) {
   g_launch_counter += (c.dim >= 2 ? 1 : 0) + ((c.metric != GRIM_MINKOWSKI || c.conduction || c.viscosity) ? 2 : 1);
 }
 
-static void enqueue_newton(grim_handle* h, int stage) {
+static void enqueue_newton(grim_handle* h, int stage, bool guessOld = false) {
   const DevCfg& c = h->dc;
   cudaStream_t s = h->stream;
-  StageBufs b = stage_bufs(h, stage);
+  StageBufs b = stage_bufs(h, stage, guessOld);
   PROF(GRIM_PROF_NEWTON);
   if (h->cfg.newtonMode == GRIM_NEWTON_PARITY_FD64) {
     grim::exact::newton_fd_init(c, stage, b, s);
@@ -482,8 +489,8 @@ static void enqueue_segment(grim_handle* h, int seg) {
   switch (seg) {
     case GRIM_SEG_PRE: enqueue_pre_half(h, false); break;
     case GRIM_SEG_HALF:
-      enqueue_stencil(h, GRIM_HALF_STEP);
-      enqueue_newton(h, GRIM_HALF_STEP);
+      enqueue_stencil(h, GRIM_HALF_STEP, step_guess_old(h));
+      enqueue_newton(h, GRIM_HALF_STEP, step_guess_old(h));
       enqueue_mid_finish(h);
       break;
     case GRIM_SEG_FULL:
@@ -499,9 +506,9 @@ static void enqueue_segment(grim_handle* h, int seg) {
 static void enqueue_step(grim_handle* h, bool timed) {
   cudaStream_t s = h->stream;
   enqueue_pre_half(h, timed);
-  enqueue_stencil(h, GRIM_HALF_STEP);
+  enqueue_stencil(h, GRIM_HALF_STEP, step_guess_old(h));
   if (timed) cudaEventRecord(h->ev[2], s);
-  enqueue_newton(h, GRIM_HALF_STEP);
+  enqueue_newton(h, GRIM_HALF_STEP, step_guess_old(h));
   if (timed) cudaEventRecord(h->ev[3], s);
   enqueue_mid(h);
   if (timed) cudaEventRecord(h->ev[4], s);

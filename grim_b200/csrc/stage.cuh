@@ -41,6 +41,8 @@ struct StageBufs {
   double* consOld;        // dof x Z (fluid rows then B rows)
   double* divF;           // dof x Z (fluid rows, then B rows)
   int divFB;              // the epilogue writes divF's B rows too (else the fluid rows only)
+  int guessOld;           // half stage: the per-zone Newton reads its guess's fluid rows from
+                          // pold, so the epilogue does not copy them into prim
   double* Sexp;           // nf x Z
   double* R;              // nf x Z  (Newton scratch)
   double* l2;             // 2 x Z   (l2, l2first)
