@@ -108,7 +108,7 @@ class Clocks:
             "clocks_event_reasons.sw_power_cap"
         try:
             self._p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
-                                        "--format=csv,noheader,nounits", "-lms", "200"],
+                                        "--format=csv,noheader,nounits", "-lms", "100"],
                                        stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self._p = None
@@ -119,19 +119,32 @@ class Clocks:
                 self.samples.append([x.strip() for x in line.split(",")])
         self._t = threading.Thread(target=rd, daemon=True)
         self._t.start()
+        # the sampler's first line comes before the timed region: wait for it
+        # (nvidia-smi takes a while to start) and leave it out
+        t0 = time.time()
+        while not self.samples and time.time() - t0 < 5.0 and self._p.poll() is None:
+            time.sleep(0.01)
+        self._n0 = len(self.samples)
 
     def stop(self):
+        n0 = getattr(self, "_n0", 0)
         if self._p:
+            # a timed region shorter than the sampling period: take the line
+            # that follows it
+            t0 = time.time()
+            while len(self.samples) <= n0 and time.time() - t0 < 1.0 and self._p.poll() is None:
+                time.sleep(0.005)
             self._p.terminate()
             try:
                 self._p.wait(timeout=5)
             except Exception:
                 self._p.kill()
-        sm = [float(s[0]) for s in self.samples if len(s) >= 7 and s[0].replace('.', '').isdigit()]
-        mx = [float(s[1]) for s in self.samples if len(s) >= 7 and s[1].replace('.', '').isdigit()]
+        got = self.samples[n0:]
+        sm = [float(s[0]) for s in got if len(s) >= 7 and s[0].replace('.', '').isdigit()]
+        mx = [float(s[1]) for s in got if len(s) >= 7 and s[1].replace('.', '').isdigit()]
         reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for s in self.samples:
+        for s in got:
             if len(s) >= 7:
                 for n, v in zip(names, s[3:7]):
                     if v.lower().startswith("active"):
