@@ -711,26 +711,6 @@ static __global__ void k_emf(DevCfg c, const double* __restrict__ F1, const doub
   out[2 * Z + z] = e3;
 }
 
-// The stage's corner EMFs (constrainedtransport.cpp:53-83), each computed
-// once per zone corner instead of four times by the zones that share it:
-// emfX3 at (i-1/2, j-1/2), and in 3D emfX1 at (j-1/2, k-1/2), emfX2 at
-// (i-1/2, k-1/2); corners whose neighbours fall off the grid are skipped
-// (no interior zone reads them).
-static __global__ void k_stage_emf(DevCfg c, StageBufs b) {
-  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (z >= c.Z) return;
-  int i, j, k;
-  zijk(c, z, i, j, k);
-  FluxView f;
-  f.F[0] = b.flux[0]; f.F[1] = b.flux[1]; f.F[2] = b.flux[2]; f.Z = c.Z; f.B1 = c.B1;
-  const long long s1 = 1, s2 = (long long)c.N1T, s3 = (long long)c.N1T * c.N2T;
-  if (i >= 1 && j >= 1) b.emf[2 * c.Z + z] = emf3(f, z, s1, s2);
-  if (c.dim == 3 && k >= 1) {
-    if (j >= 1) b.emf[z] = emf1(f, z, s2, s3);
-    if (i >= 1) b.emf[c.Z + z] = emf2(f, z, s1, s3);
-  }
-}
-
 // PART 0 does all of the epilogue; the split launches PART 1 (centre: the
 // stage element, consOld on the half stage, explicit sources) and then
 // PART 2 (fluxes: CT, divergence, induction, Newton guess), each with the
@@ -763,15 +743,20 @@ __global__ void __launch_bounds__(128, kEpiMinBlocks[PART]) k_stage_epilogue(Dev
   // zero-padded convolution Fr*(1/dX) + Fl*(-1/dX) in 1D/2D, shifted
   // difference (Fr - Fl)/dX in 3D, summed in direction order
   const long long sd[3] = {s1, s2, s3};
-  double e[12];  // corner EMFs: EMF3 (i|i+1, j|j+1), EMF2 (i|i+1, k|k+1), EMF1 (j|j+1, k|k+1)
+  // corner EMFs (constrainedtransport.cpp:53-83), each formed here from the
+  // face fluxes around its edge as computeEMF forms it: a corner's fluxes
+  // are L1/L2 hits shared with the neighbouring zones' threads, cheaper
+  // than a separate pass that writes the corners out and reads them back
+  double e[12];  // EMF3 (i|i+1, j|j+1), EMF2 (i|i+1, k|k+1), EMF1 (j|j+1, k|k+1)
   if (c.dim >= 2) {
-    const double* E3 = b.emf + 2 * Z;
-    e[0] = E3[z]; e[1] = E3[z + s1]; e[2] = E3[z + s2]; e[3] = E3[z + s1 + s2];
+    e[0] = emf3(f, z, s1, s2); e[1] = emf3(f, z + s1, s1, s2);
+    e[2] = emf3(f, z + s2, s1, s2); e[3] = emf3(f, z + s1 + s2, s1, s2);
   }
   if (c.dim == 3) {
-    const double *E1 = b.emf, *E2 = b.emf + Z;
-    e[4] = E2[z]; e[5] = E2[z + s1]; e[6] = E2[z + s3]; e[7] = E2[z + s1 + s3];
-    e[8] = E1[z]; e[9] = E1[z + s2]; e[10] = E1[z + s3]; e[11] = E1[z + s2 + s3];
+    e[4] = emf2(f, z, s1, s3); e[5] = emf2(f, z + s1, s1, s3);
+    e[6] = emf2(f, z + s3, s1, s3); e[7] = emf2(f, z + s1 + s3, s1, s3);
+    e[8] = emf1(f, z, s2, s3); e[9] = emf1(f, z + s2, s2, s3);
+    e[10] = emf1(f, z + s3, s2, s3); e[11] = emf1(f, z + s2 + s3, s2, s3);
   }
 #pragma unroll
   for (int d = 0; d < 3; d++) {
@@ -1518,6 +1503,7 @@ __global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : kN
   constexpr int NF = 5 + COND + VISC;
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int unconv = 0, itsMax = 0;
+  bool nanZone = false;
   if (n < nlist) {
     const long long Z = c.Z;
     const long long z = list ? (long long)list[n] : interior_to_z(c, n);
@@ -1590,15 +1576,23 @@ __global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : kN
     itsMax = it;
 #pragma unroll
     for (int v = 0; v < NF; v++) b.prim[(long long)v * Z + z] = P[v];
+    if (b.nanCount) {
+#pragma unroll
+      for (int v = 0; v < NF; v++) nanZone |= isnan(P[v]);
+#pragma unroll
+      for (int v = 0; v < 3; v++) nanZone |= isnan(K.B[v]);
+    }
   }
   hist_add(b.st->itHist[stage], min(itsMax, 15), n < nlist);
   // warp-level tallies: no block barrier, so a warp whose zones converged
   // early retires without waiting for the rest of its block
   const int nUnconv = __popc(__ballot_sync(0xffffffffu, unconv != 0));
   for (int o = 16; o > 0; o >>= 1) itsMax = max(itsMax, __shfl_xor_sync(0xffffffffu, itsMax, o));
+  const int nNan = __popc(__ballot_sync(0xffffffffu, nanZone));
   if ((threadIdx.x & 31) == 0) {
     atomicMax((unsigned long long*)&b.st->itersDone[stage], (unsigned long long)itsMax);
     if (nUnconv) atomicAdd(&b.st->finalUnconv[stage], (unsigned long long)nUnconv);
+    if (nNan) atomicAdd(b.nanCount, (unsigned long long)nNan);
   }
 }
 
@@ -2235,7 +2229,6 @@ int face_variants(const DevCfg& c, int dir) {
 #if !defined(GRIM_ONLY_FACES)
 template <int C, int V>
 static void stage_epilogue_t(const DevCfg& c, int stage, const StageBufs& b, cudaStream_t s) {
-  if (c.dim >= 2) k_stage_emf<<<nblk(c.Z, 256), 256, 0, s>>>(c, b);
   if (c.metric != GRIM_MINKOWSKI || C || V) {
     // centre half first: the flux half's induction reads its consOld
     k_stage_epilogue<C, V, 1><<<nblk(c.Zint, 128), 128, 0, s>>>(c, stage, b);

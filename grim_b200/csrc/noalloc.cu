@@ -82,11 +82,10 @@ extern "C" int grim_div_fluxes_noalloc(const grim_config* cfg, const double* pri
   const long long Z = c.Z;
   const bool emhd = c.conduction || c.viscosity;
   // scratch layout (words): face fluxes dim*dof*Z | consOld dof*Z | guess
-  // dof*Z | Sexp nf*Z | uT 5*Z (EMHD) | corner EMFs 3*Z (2D/3D) | device
-  // scalars
+  // dof*Z | Sexp nf*Z | uT 5*Z (EMHD) | device scalars
   const long long stateWords = (long long)((sizeof(DevState) + 255) / 256 * 256 / sizeof(double));
   const long long need = (long long)c.dim * c.dof * Z + 2LL * c.dof * Z + (long long)c.nf * Z +
-                         (emhd ? 5LL * Z : 0LL) + (c.dim >= 2 ? 3LL * Z : 0LL) + stateWords;
+                         (emhd ? 5LL * Z : 0LL) + stateWords;
   if (need > GRIM_NOALLOC_SCRATCH_WORDS) {
     char msg[256];
     snprintf(msg, sizeof(msg),
@@ -110,7 +109,6 @@ extern "C" int grim_div_fluxes_noalloc(const grim_config* cfg, const double* pri
   b.prim = w; w += (long long)c.dof * Z;
   b.Sexp = w; w += (long long)c.nf * Z;
   if (emhd) { b.uT = w; w += 5LL * Z; }
-  if (c.dim >= 2) { b.emf = w; w += 3LL * Z; }
   b.st = reinterpret_cast<DevState*>(w);
   b.ps = prim;
   b.pold = prim;

@@ -61,7 +61,6 @@ struct grim_handle {
   double *primOld = nullptr, *prim = nullptr, *primHalf = nullptr;
   // stage buffers
   double *consOld = nullptr, *divF = nullptr, *Sexp = nullptr, *R = nullptr, *l2 = nullptr, *uT = nullptr;
-  double* emf = nullptr;  // 3 x Z stage corner EMFs
   double* flux[3] = {nullptr, nullptr, nullptr};
   int* list[2] = {nullptr, nullptr};  // compacted Newton worklists
   double* scratch = nullptr;  // test entry points: dof x Z inputs
@@ -132,7 +131,7 @@ struct ProfScope {
 
 static void free_all(grim_handle* h) {
   double** bufs[] = {&h->primOld, &h->prim, &h->primHalf, &h->consOld, &h->divF, &h->Sexp, &h->R,
-                     &h->l2, &h->uT, &h->emf, &h->flux[0], &h->flux[1], &h->flux[2], &h->scratch, &h->scratch2,
+                     &h->l2, &h->uT, &h->flux[0], &h->flux[1], &h->flux[2], &h->scratch, &h->scratch2,
                      &h->geo[0], &h->geo[1], &h->geo[2], &h->geo[3], &h->geo[4], &h->gamma, &h->obs};
   for (double** b : bufs)
     if (*b) { cudaFree(*b); *b = nullptr; }
@@ -274,7 +273,6 @@ static StageBufs stage_bufs(grim_handle* h, int stage, bool guessOld = false) {
   b.R = h->R;
   b.l2 = h->l2;
   b.st = h->st;
-  b.emf = h->emf;
   b.list[0] = h->list[0];
   b.list[1] = h->list[1];
   return b;
@@ -323,11 +321,27 @@ static void enqueue_stencil(grim_handle* h, int stage, bool guessOld = false) {
   g_launch_counter += (c.dim >= 2 ? 1 : 0) + ((c.metric != GRIM_MINKOWSKI || c.conduction || c.viscosity) ? 2 : 1);
 }
 
-static void enqueue_newton(grim_handle* h, int stage, bool guessOld = false) {
+// the torus step's per-zone fast Newton counts, as it writes the full
+// stage's result, the zones fullStepDiagnostics would find a NaN in (so the
+// count needs no pass of its own); the other Newton forms leave the count
+// to k_nan_flag
+static bool newton_counts_nan(const grim_handle* h) {
+  return h->cfg.problem == GRIM_PROBLEM_TORUS && h->cfg.newtonMode != GRIM_NEWTON_PARITY_FD64 &&
+         h->cfg.perZoneConvergence != 2;
+}
+
+// returns whether the launch counts the NaN zones (countNan asked for it
+// and the Newton form does it)
+static bool enqueue_newton(grim_handle* h, int stage, bool guessOld = false, bool countNan = false) {
   const DevCfg& c = h->dc;
   cudaStream_t s = h->stream;
   StageBufs b = stage_bufs(h, stage, guessOld);
   PROF(GRIM_PROF_NEWTON);
+  countNan = countNan && newton_counts_nan(h);
+  if (countNan) {
+    cudaMemsetAsync(&h->st->nanFlag, 0, sizeof(unsigned long long), s);
+    b.nanCount = &h->st->nanFlag;
+  }
   if (h->cfg.newtonMode == GRIM_NEWTON_PARITY_FD64) {
     grim::exact::newton_fd_init(c, stage, b, s);
     g_launch_counter++;
@@ -342,6 +356,7 @@ static void enqueue_newton(grim_handle* h, int stage, bool guessOld = false) {
     grim::fast::newton_fast(c, stage, b, h->cfg.newtonMode, nullptr, c.Zint, s);
     g_launch_counter++;
   }
+  return countNan;
 }
 
 static void enqueue_dt_speeds(grim_handle* h, const double* p, int mode) {
@@ -442,8 +457,9 @@ static void enqueue_observers(grim_handle* h, double every, double* out, bool to
 // full step (linear_modes/problem.cpp:287) and the non-finite count, as one
 // pass after the NaN count
 // time advance and the NaN count of fullStepDiagnostics (on the Newton
-// result, whose interior the finish copies unchanged)
-static void enqueue_post_count(grim_handle* h) {
+// result, whose interior the finish copies unchanged), unless the full
+// stage's Newton counted it
+static void enqueue_post_count(grim_handle* h, bool nanCounted) {
   const DevCfg& c = h->dc;
   cudaStream_t s = h->stream;
   {
@@ -451,7 +467,7 @@ static void enqueue_post_count(grim_handle* h) {
     grim::exact::advance_time(h->st, s);
     g_launch_counter++;
   }
-  if (h->cfg.problem == GRIM_PROBLEM_TORUS) {
+  if (h->cfg.problem == GRIM_PROBLEM_TORUS && !nanCounted) {
     PROF(GRIM_PROF_DIAGNOSTICS);
     cudaMemsetAsync(&h->st->nanFlag, 0, sizeof(unsigned long long), s);
     KNS_CALL(h, torus_nan_flag, c, h->prim, &h->st->nanFlag, s);
@@ -479,8 +495,8 @@ static void enqueue_post_finish(grim_handle* h, bool timed) {
   }
   if (timed) cudaEventRecord(h->ev[7], s);
 }
-static void enqueue_post(grim_handle* h, bool timed) {
-  enqueue_post_count(h);
+static void enqueue_post(grim_handle* h, bool timed, bool nanCounted = false) {
+  enqueue_post_count(h, nanCounted);
   enqueue_post_finish(h, timed);
 }
 
@@ -496,8 +512,7 @@ static void enqueue_segment(grim_handle* h, int seg) {
     case GRIM_SEG_FULL:
       enqueue_mid_fill(h);
       enqueue_stencil(h, GRIM_FULL_STEP);
-      enqueue_newton(h, GRIM_FULL_STEP);
-      enqueue_post_count(h);
+      enqueue_post_count(h, enqueue_newton(h, GRIM_FULL_STEP, false, true));
       break;
     default: enqueue_post_finish(h, false); break;
   }
@@ -514,9 +529,9 @@ static void enqueue_step(grim_handle* h, bool timed) {
   if (timed) cudaEventRecord(h->ev[4], s);
   enqueue_stencil(h, GRIM_FULL_STEP);
   if (timed) cudaEventRecord(h->ev[5], s);
-  enqueue_newton(h, GRIM_FULL_STEP);
+  const bool nanCounted = enqueue_newton(h, GRIM_FULL_STEP, false, true);
   if (timed) cudaEventRecord(h->ev[6], s);
-  enqueue_post(h, timed);
+  enqueue_post(h, timed, nanCounted);
 }
 
 // ---------------------------------------------------------------------------
@@ -548,7 +563,6 @@ int grim_create(const grim_config* cfg, int device, grim_handle** out) {
             alloc(&h->consOld, c.dof) && alloc(&h->divF, c.dof) && alloc(&h->Sexp, c.nf) && alloc(&h->R, c.nf) &&
             alloc(&h->l2, 2) && alloc(&h->scratch, c.dof) && alloc(&h->scratch2, (size_t)c.dof * 3);
   for (int d = 0; ok && d < c.dim; d++) ok = alloc(&h->flux[d], c.dof);
-  if (ok && c.dim >= 2) ok = alloc(&h->emf, 3);
   if (ok && (c.conduction || c.viscosity)) ok = alloc(&h->uT, 5);
   if (ok && cfg->metric != GRIM_MINKOWSKI) {
     // one (i, j) plane per word (the metric does not depend on X3)

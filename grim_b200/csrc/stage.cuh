@@ -46,8 +46,9 @@ struct StageBufs {
   double* Sexp;           // nf x Z
   double* R;              // nf x Z  (Newton scratch)
   double* l2;             // 2 x Z   (l2, l2first)
-  double* emf;            // 3 x Z   corner EMFs of the stage (X1, X2, X3), dim >= 2
   DevState* st;
+  unsigned long long* nanCount;  // non-null: the per-zone Newton adds the zones whose result (fluid and field
+                                 // rows) holds a NaN (fullStepDiagnostics' count of the full stage)
   int* list[2];           // compacted Newton worklists (interior zone indices)
 };
 

@@ -245,7 +245,14 @@ __global__ void k_torus_inflow(DevCfg c, TorusCfg t, double* __restrict__ p, con
   *u3 = *u3 * lf;
 }
 
-// fixPoles (problem.cpp:1046-1215): one thread per (i, k) column and pole
+// fixPoles (problem.cpp:1046-1215): one thread per (i, k) column and pole.
+// The two rows next to the pole are rebuilt from the third (idx2) and the
+// ghost rows mirror those three rows (ghost g from row idx_g, with numGhost
+// 3 the only width make_devcfg accepts), so every value a thread writes is a
+// function of row idx2's fluid variables, the three rows' field components
+// and their theta: all of them are loaded before the first store, and a
+// thread waits on memory once instead of once per copied value.  The
+// arithmetic is the reference's, value for value.
 static __global__ void k_torus_poles(DevCfg c, double* __restrict__ p, const double* __restrict__ geoC) {
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long cols = (long long)c.N1T * c.N3T;
@@ -261,32 +268,52 @@ static __global__ void k_torus_poles(DevCfg c, double* __restrict__ p, const dou
     return top ? th * (-1.) + M_PI : th;
   };
   const int idx0 = top ? c.N2 + ng - 1 : ng;
-  const int idx1 = top ? idx0 - 1 : ng + 1;
-  const int idx2 = top ? idx0 - 2 : ng + 2;
-  const int sgnIdx[2] = {idx0, idx1};
-  for (int q = 0; q < 2; q++) {
-    const int jj = sgnIdx[q];
-    at(RHO, jj) = at(RHO, idx2);
-    at(UU, jj) = at(UU, idx2);
-    at(U1, jj) = at(U1, idx2);
-    at(U2, jj) = at(U2, idx2) * theta(jj) / theta(idx2);
-    at(U3, jj) = at(U3, idx2);
-    if (c.conduction) at(c.Q, jj) = at(c.Q, idx2) * theta(jj) / theta(idx2);
-    if (c.viscosity) at(c.DP, jj) = at(c.DP, idx2) * theta(jj) / theta(idx2);
+  const int row[3] = {idx0, top ? idx0 - 1 : ng + 1, top ? idx0 - 2 : ng + 2};
+  // ---- loads
+  double th[3], b1[3], b2[3], b3[3];
+#pragma unroll
+  for (int g = 0; g < 3; g++) {
+    th[g] = theta(row[g]);
+    b1[g] = at(c.B1, row[g]);
+    b2[g] = at(c.B1 + 1, row[g]);
+    b3[g] = at(c.B1 + 2, row[g]);
   }
-  for (int g = 0; g < ng; g++) {
+  const double rho = at(RHO, row[2]), uu = at(UU, row[2]), u1 = at(U1, row[2]), u2 = at(U2, row[2]),
+               u3 = at(U3, row[2]);
+  const double q = c.conduction ? at(c.Q, row[2]) : 0., dp = c.viscosity ? at(c.DP, row[2]) : 0.;
+  // ---- the rows next to the pole (U2, q, deltaP scaled by theta), then
+  // the ghost rows
+  double su2[3], sq[3], sdp[3];
+#pragma unroll
+  for (int g = 0; g < 3; g++) {
+    su2[g] = g < 2 ? u2 * th[g] / th[2] : u2;
+    sq[g] = g < 2 ? q * th[g] / th[2] : q;
+    sdp[g] = g < 2 ? dp * th[g] / th[2] : dp;
+  }
+#pragma unroll
+  for (int g = 0; g < 2; g++) {
+    const int jj = row[g];
+    at(RHO, jj) = rho;
+    at(UU, jj) = uu;
+    at(U1, jj) = u1;
+    at(U2, jj) = su2[g];
+    at(U3, jj) = u3;
+    if (c.conduction) at(c.Q, jj) = sq[g];
+    if (c.viscosity) at(c.DP, jj) = sdp[g];
+  }
+#pragma unroll
+  for (int g = 0; g < 3; g++) {
     const int dst = top ? c.N2 + ng + g : ng - 1 - g;
-    const int src = top ? c.N2 + ng - 1 - g : ng + g;
-    at(RHO, dst) = at(RHO, src);
-    at(UU, dst) = at(UU, src);
-    at(U1, dst) = at(U1, src);
-    at(U3, dst) = at(U3, src);
-    at(U2, dst) = at(U2, src) * (-1.0);
-    at(c.B1, dst) = at(c.B1, src);
-    at(c.B1 + 2, dst) = at(c.B1 + 2, src);
-    at(c.B1 + 1, dst) = at(c.B1 + 1, src) * (-1.0);
-    if (c.conduction) at(c.Q, dst) = at(c.Q, src) * (-1.0);
-    if (c.viscosity) at(c.DP, dst) = at(c.DP, src) * (-1.0);
+    at(RHO, dst) = rho;
+    at(UU, dst) = uu;
+    at(U1, dst) = u1;
+    at(U3, dst) = u3;
+    at(U2, dst) = su2[g] * (-1.0);
+    at(c.B1, dst) = b1[g];
+    at(c.B1 + 2, dst) = b3[g];
+    at(c.B1 + 1, dst) = b2[g] * (-1.0);
+    if (c.conduction) at(c.Q, dst) = sq[g] * (-1.0);
+    if (c.viscosity) at(c.DP, dst) = sdp[g] * (-1.0);
   }
 }
 
