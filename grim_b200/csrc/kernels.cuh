@@ -986,8 +986,15 @@ GRIM_D double elem_inv_dt(const DevCfg& c, const ElemT<double, double>& e, const
     if (d < c.dim) {
       double mn, mx;
       char_speeds<COND, VISC>(e, G, d, c, mn, mx);
-      double a = mn / c.dX[d], bb = mx / c.dX[d];
-      double m2 = fmax(bb, fabs(a));
+      double m2;
+      if constexpr (kFastMath) {
+        // one product for two divisions: scaling by 1/dX > 0 commutes with
+        // the max (rounding is monotonic)
+        m2 = fmax(mx, fabs(mn)) * c.invdX[d];
+      } else {
+        double a = mn / c.dX[d], bb = mx / c.dX[d];
+        m2 = fmax(bb, fabs(a));
+      }
       acc = (d == 0) ? m2 : acc + m2;
     }
   }

@@ -318,7 +318,7 @@ static void enqueue_stencil(grim_handle* h, int stage, bool guessOld = false) {
   }
   PROF(GRIM_PROF_EPILOGUE);
   KNS_CALL(h, stage_epilogue, c, stage, b, s);
-  g_launch_counter += (c.dim >= 2 ? 1 : 0) + ((c.metric != GRIM_MINKOWSKI || c.conduction || c.viscosity) ? 2 : 1);
+  g_launch_counter += (c.metric != GRIM_MINKOWSKI || c.conduction || c.viscosity) ? 2 : 1;
 }
 
 // the torus step's per-zone fast Newton counts, as it writes the full

@@ -131,7 +131,12 @@ GRIM_D bool torus_floor_zone(const DevCfg& c, const TorusCfg& t, double* q, cons
   }
   }  // drift-frame fix
   // maximum Lorentz factor
-  elem_of<COND, VISC>(e, c, q, G);
+#ifdef GRIM_FAST_MATH
+  // no floor applied: q is the state the element above was set from (trans
+  // is 0, so the fix was skipped) and that element stands
+  if (usefloor)
+#endif
+    elem_of<COND, VISC>(e, c, q, G);
   bool current = true;
   {
     const double lf2 = e.gam * e.gam;

@@ -239,3 +239,70 @@ def test_torus_2d_steps_match_oracle():
         o = interior(cfg, orc.get_prims())
         assert not np.isnan(g).any()
         assert scaled_err(g, o) <= 1e-12, (n, scaled_err(g, o))
+
+
+def _torus_stepper(mode, **kw):
+    from grim_b200.timestepper import timeStepper
+    cfg = dict(T.torus_config(**SHAPE), newtonMode=mode, perZoneConvergence=1, nonlinearsolve_rtol=1e-10,
+               nonlinearsolve_atol=1e-24, **kw)
+    ts = timeStepper(cfg)
+    P, _ = T.torus_prims(cfg, ts.getGeometry(C.CENTER))
+    ts.primOld.setVars(P)
+    ts.problemInit()
+    return cfg, ts
+
+
+def test_torus_fast_steps_match_parity_path():
+    """The fast form of the torus step (FP32 closed-form Jacobian, FP64
+    residual, per-zone convergence, FMA arithmetic, its fused floors / dt /
+    NaN-count passes) against the FD64 parity path at the same relative
+    tolerance and the torus's 3 Newton iterations, which leave zones above
+    tolerance in both forms (about 5x more in the parity form), so the two
+    differ by those zones' residuals, 1.5e-6 of the velocities' scale on a
+    B200: three steps agree to 1e-5 of each variable's scale, with the same
+    dt to 1e-9."""
+    _, ref = _torus_stepper(C.NEWTON_PARITY_FD64)
+    cfg, fast = _torus_stepper(C.NEWTON_MIXED32)
+    for n in range(3):
+        ref.timeStep()
+        fast.timeStep()
+        assert abs(fast.dt - ref.dt) <= 1e-9 * ref.dt, n
+    a = interior(cfg, fast.primOld.getVars())
+    b = interior(cfg, ref.primOld.getVars())
+    assert not np.isnan(a).any()
+    err = scaled_err(a, b)
+    assert err <= 1e-5, err
+    assert fast.stats()["nonFinite"] == 0
+
+
+@pytest.mark.parametrize("mode", [C.NEWTON_PARITY_FD64, C.NEWTON_MIXED32])
+def test_torus_nan_count_and_reset(mode):
+    """fullStepDiagnostics (torus/problem.cpp:719-746): the count of interior
+    zones of the full stage's Newton result that hold a NaN, then the reset
+    of those zones before the floors.  The fast per-zone Newton counts them
+    as it writes them, the parity path in a pass of its own.  A NaN planted
+    in one interior zone's velocity spreads through the two stages'
+    stencils; after the step's first three segments the count equals the
+    NaN zones of the Newton result, and the finished step leaves the
+    interior finite.  (A NaN density would not spread here: the element
+    floors rho with fmax, which returns the floor for a NaN.)"""
+    import ctypes
+    import torch
+    from grim_b200 import _lib
+    from grim_b200.slab import SCALAR_NANFLAG, SEG_FULL, SEG_HALF, SEG_POST, SEG_PRE
+    from grim_b200.timestepper import Grid
+    cfg, ts = _torus_stepper(mode)
+    P = ts.primOld.getVars()
+    P[2, 3 + SHAPE["N3"] // 2, 3 + SHAPE["N2"] // 2, 3 + SHAPE["N1"] // 3] = np.nan
+    ts.primOld.setVars(P)
+    L = _lib.lib()
+    for seg in (SEG_PRE, SEG_HALF, SEG_FULL):
+        _lib.check(L.grim_step_segment(ts._h, seg), "step_segment")
+    buf = torch.zeros(1, dtype=torch.int64, device="cuda")
+    _lib.check(L.grim_scalar_get(ts._h, SCALAR_NANFLAG, ctypes.c_void_p(buf.data_ptr())), "scalar_get")
+    ts.synchronize()
+    count = int(buf.item())
+    bad = int(np.isnan(interior(cfg, Grid(ts, _lib.PRIM).getVars())).any(axis=0).sum())
+    assert count == bad and bad > 1, (count, bad)
+    _lib.check(L.grim_step_segment(ts._h, SEG_POST), "step_segment")
+    assert not np.isnan(interior(cfg, ts.primOld.getVars())).any()
