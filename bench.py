@@ -590,6 +590,7 @@ def run_gpu(args, rank, world, local_rank):
         _lib.check(L.grim_get_prims(ts_fast._h, _lib.PRIM_OLD, ctypes.c_void_p(host_out.data_ptr()), _lib.HOST))
     e2e_s = time.perf_counter() - t0
     e2e_bytes = host_in.numel() * 8
+    side = torus_side_costs(ts_fast, cfg) if args.workload == "torus" else None
 
     # max over ranks of the device time
     t = torch.tensor([ms_fast, ms_fd, e2e_s], dtype=torch.float64, device="cuda")
@@ -634,8 +635,40 @@ def run_gpu(args, rank, world, local_rank):
         "gpu_launches": int(st_fast["kernelLaunches"]) * args.steps,
         "clocks": clocks_info,
     }
+    if side is not None:
+        out["torus_side"] = side
     out.update(rooflines(cfg, prof_fast, prof_fd, local_rank))
     return out, cfg, state["P"]
+
+
+def torus_side_costs(ts, cfg):
+    """Beside the step: one record of the torus observers (the element and
+    the integrands per interior zone, fixed-order partials; two launches and
+    a 9-value read-back per call, timed by the wall clock around the
+    synchronous call), and a checkpoint round trip of primOld (grid::dump
+    then grid::load as a PETSc binary Vec: device copy, natural-order
+    reshuffle, big-endian file I/O)."""
+    import tempfile
+    zones = cfg["N1"] * cfg["N2"] * cfg["N3"]
+    for _ in range(3):
+        ts.torusObservers()
+    n = 20
+    t0 = time.perf_counter()
+    for _ in range(n):
+        ts.torusObservers()
+    obs_s = (time.perf_counter() - t0) / n
+    obs_bytes = zones * ts.dof * 8  # the primitives each record reads
+    with tempfile.TemporaryDirectory() as d:
+        f = os.path.join(d, "primOld.bin")
+        t0 = time.perf_counter()
+        ts.dump(f)
+        t1 = time.perf_counter()
+        ts.load(f)
+        t2 = time.perf_counter()
+        size = os.path.getsize(f)
+    return {"observers": {"ms_per_record": obs_s * 1e3, "primitive_bytes": obs_bytes,
+                          "gbs": obs_bytes / obs_s / 1e9},
+            "checkpoint": {"file_bytes": size, "dump_s": t1 - t0, "load_s": t2 - t1}}
 
 
 def main():
