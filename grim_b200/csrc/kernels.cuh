@@ -1125,7 +1125,7 @@ GRIM_D double obs_join(int v, double a, double b) {
 }
 
 template <int COND, int VISC>
-__global__ void __launch_bounds__(256) k_torus_obs_partial(DevCfg c, const double* __restrict__ p,
+__global__ void __launch_bounds__(128, 5) k_torus_obs_partial(DevCfg c, const double* __restrict__ p,
                                                            const double* __restrict__ geoC, double volElem,
                                                            double every, const DevState* st,
                                                            double* __restrict__ partials) {
@@ -1187,17 +1187,28 @@ __global__ void __launch_bounds__(256) k_torus_obs_partial(DevCfg c, const doubl
 // a history, appends the record {time, values} at ring slot obsCount % cap
 static __global__ void k_torus_obs_final(const double* __restrict__ partials, int nblocks, double every,
                                          DevState* st, double* out, double* hist, int cap) {
-  if (threadIdx.x != 0 || blockIdx.x != 0 || !obs_due(st, every)) return;
-  double r[OBS_N];
-  for (int v = 0; v < OBS_N; v++) r[v] = partials[v];
-  for (int bk = 1; bk < nblocks; bk++)
-    for (int v = 0; v < OBS_N; v++) r[v] = obs_join(v, r[v], partials[(long long)bk * OBS_N + v]);
-  if (out)
-    for (int v = 0; v < OBS_N; v++) out[v] = r[v];
-  if (hist && cap > 0) {
-    double* rec = hist + (st->obsCount % (unsigned long long)cap) * (OBS_N + 1);
+  // one thread per observable folds the partials in block order; launched
+  // as one warp
+  const int v = threadIdx.x;
+  if (blockIdx.x != 0 || !obs_due(st, every)) return;
+  double* rec = (hist && cap > 0) ? hist + (st->obsCount % (unsigned long long)cap) * (OBS_N + 1) : nullptr;
+  if (v < OBS_N) {
+    // 16 loads in flight per chunk, joined in block order
+    double r = partials[v];
+    for (int b0 = 1; b0 < nblocks; b0 += 16) {
+      double t[16];
+#pragma unroll
+      for (int q = 0; q < 16; q++) t[q] = (b0 + q < nblocks) ? partials[(long long)(b0 + q) * OBS_N + v] : 0.;
+#pragma unroll
+      for (int q = 0; q < 16; q++)
+        if (b0 + q < nblocks) r = obs_join(v, r, t[q]);
+    }
+    if (out) out[v] = r;
+    if (rec) rec[1 + v] = r;
+  }
+  __syncwarp();
+  if (v == 0 && rec) {
     rec[0] = st->time;
-    for (int v = 0; v < OBS_N; v++) rec[1 + v] = r[v];
     st->obsCount += 1;
   }
 }
@@ -2418,7 +2429,7 @@ void stage_finish(const DevCfg& c, const double* src, double* dst, const double*
 template <int C, int V>
 static void torus_observe_t(const DevCfg& c, const double* p, const double* geoC, double volElem, double every,
                             DevState* st, double* partials, double* out, double* hist, int cap, cudaStream_t s) {
-  k_torus_obs_partial<C, V><<<kObsBlocks, 256, 0, s>>>(c, p, geoC, volElem, every, st, partials);
+  k_torus_obs_partial<C, V><<<kObsBlocks, 128, 0, s>>>(c, p, geoC, volElem, every, st, partials);
   k_torus_obs_final<<<1, 32, 0, s>>>(partials, kObsBlocks, every, st, out, hist, cap);
 }
 void torus_observe(const DevCfg& c, const double* p, const double* geoC, double volElem, double every, DevState* st,

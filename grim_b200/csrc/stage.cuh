@@ -27,7 +27,7 @@ enum {
   OBS_MASS = 0, OBS_EMAG, OBS_ETH, OBS_RHOMAX, OBS_BETAMIN, OBS_MDOT_IN, OBS_MDOT_OUT, OBS_UNBOUND_OUT,
   OBS_REL_UNBOUND_OUT, OBS_N
 };
-constexpr int kObsBlocks = 296;  // fixed partial count: the sums' order does not depend on the launch
+constexpr int kObsBlocks = 740;  // fixed partial count (5 blocks of 128 per SM): the sums' order does not depend on the launch
 
 struct StageBufs {
   const double* ps;       // prims the stage's fluxes are computed from
