@@ -16,6 +16,8 @@ HEADER = os.path.join(_HERE, "..", "include", "grim_b200.h")
 _LIB = None
 
 GRIM_OK = 0
+GRIM_ETIMEOUT = -6
+DEBUG_SKIP_BULK_COPIES = 1
 HOST, DEVICE = 0, 1
 PRIM_OLD, PRIM, PRIM_HALF = 0, 1, 2
 
@@ -30,12 +32,16 @@ class GrimStats(ctypes.Structure):
         ("msNewton", ctypes.c_double),
         ("msOther", ctypes.c_double),
         ("kernelLaunches", ctypes.c_longlong),
-        ("reserved", ctypes.c_double * 8),
+        ("waitTimeouts", ctypes.c_longlong),
+        ("drainTimeouts", ctypes.c_longlong),
+        ("reserved", ctypes.c_double * 6),
     ]
 
 
 class GrimError(RuntimeError):
-    pass
+    def __init__(self, msg, status=None):
+        super().__init__(msg)
+        self.status = status
 
 
 def declared_symbols():
@@ -91,6 +97,7 @@ def lib():
         "grim_residual": [vp, vp, vp, i],
         "grim_jacobian_fd": [vp, vp, vp, i],
         "grim_jacobian_tangent": [vp, vp, vp, i],
+        "grim_jacobian_form": [vp, vp, vp, i, i],
         "grim_newton_solve": [vp, P(i)],
         "grim_batch_solve": [i, i, vp, vp, vp, i],
         "grim_get_geometry": [vp, i, vp, vp, vp, i],
@@ -107,6 +114,7 @@ def lib():
         "grim_autotune": [vp, P(i), P(d)],
         "grim_set_face_variant": [vp, i, i],
         "grim_set_dt_mode": [vp, i],
+        "grim_set_debug": [vp, i, i],
         "grim_adjoint_forward": [vp, i, i],
         "grim_adjoint_backward": [vp, vp, vp, i],
         "grim_adjoint_stencil": [vp, vp, vp, vp, i],
@@ -134,4 +142,4 @@ def lib():
 def check(rc, what=""):
     if rc != GRIM_OK:
         msg = lib().grim_last_error().decode(errors="replace")
-        raise GrimError("%s failed (status %d): %s" % (what, rc, msg))
+        raise GrimError("%s failed (status %d): %s" % (what, rc, msg), rc)

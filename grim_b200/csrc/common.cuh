@@ -40,6 +40,9 @@ struct DevCfg {
   double tau0, tau1;
   // torus floors (problem hook)
   double maxLF, rhoFloorAmpl, uFloorAmpl, rhoFloorSlope, uFloorSlope, bsqOverRhoMax, bsqOverUMax;
+  // debug setting (grim_set_debug): the TMA-staged face kernels issue no
+  // copies, so their bounded waits run out
+  int dbgSkipCopies;
 };
 
 GRIM_HD long long zidx(const DevCfg& c, int i, int j, int k) {

@@ -115,7 +115,19 @@ int grim_petsc_vec_read(const char* fileName, double* v, long long n) {
     return GRIM_EINVAL;
   }
   unsigned char head[8];
-  if (std::fread(head, 1, 8, f) != 8 || get_be32(head) != kVecClassId) {
+  const size_t got = std::fread(head, 1, 8, f);
+  // HDF5 files start with the signature \x89 H D F \r \n \x1a \n (at offset 0
+  // when no user block precedes it): the reference's own restart files
+  // (PETSc's HDF5 viewer, grid.cpp:367-381) are of that kind
+  static const unsigned char kHdf5Sig[8] = {0x89, 'H', 'D', 'F', '\r', '\n', 0x1a, '\n'};
+  if (got == 8 && std::memcmp(head, kHdf5Sig, 8) == 0) {
+    std::fclose(f);
+    grim::set_error_message(
+        "grim_petsc_vec_read: this is an HDF5 file (such as the reference's restart file written with PETSc's HDF5 "
+        "viewer); HDF5 restart files are not supported: this library reads PETSc binary Vec files only");
+    return GRIM_ENOTSUP;
+  }
+  if (got != 8 || get_be32(head) != kVecClassId) {
     std::fclose(f);
     grim::set_error_message("grim_petsc_vec_read: not a PETSc binary Vec (class id 1211214)");
     return GRIM_EINVAL;

@@ -380,8 +380,10 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1(DevCfg c, const doub
 // copies the next segment's primitives (all dof, 40 zones along i) into the
 // warp's other shared-memory buffer, so the stencil loads come from shared
 // memory.  The tensor map covers the prim array as (i, j, k, var).  Waits
-// on the copy barrier are bounded: a wait that gives up counts in
-// DevState::waitTimeouts and the warp stops after its copy in flight lands.
+// on the copy barrier are bounded in time (kCopyWaitNs): a wait that gives up
+// counts in DevState::waitTimeouts, raises the handle's host-visible error
+// word, and the warp stops once every copy it issued has landed (itself a
+// bounded wait; one that gives up too counts in DevState::drainTimeouts).
 // ---------------------------------------------------------------------------
 constexpr int kX1Box = 40;  // zones per TMA row box (x rounded down to even)
 
@@ -402,11 +404,37 @@ GRIM_D bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
-// bounded wait: false when the barrier did not complete within the limit
+GRIM_D unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// A copy of one row box lands within microseconds; a wait that lasts this
+// long means the copy will not complete.
+constexpr unsigned long long kCopyWaitNs = 1000000000ull;  // 1 s
+// bounded wait: false when the barrier did not complete within kCopyWaitNs
+// (or, should the global timer not advance, 2^26 polls)
 GRIM_D bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-  for (int spin = 0; spin < (1 << 22); spin++)
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (int spin = 0; spin < (1 << 26); spin++) {
     if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > kCopyWaitNs) break;
+  }
   return false;
+}
+// The give-up path of a warp whose copy wait ran out (lane 0): count it,
+// raise the host-visible error word, then wait (bounded) for each copy the
+// warp still has in flight so none lands after the warp has stopped.
+GRIM_D void copy_wait_gave_up(DevState* st, unsigned long long* bars, const bool inflight[2],
+                              const unsigned phase[2]) {
+  atomicAdd(&st->waitTimeouts, 1ULL);
+  for (int b = 0; b < 2; b++)
+    if (inflight[b] && !mbar_wait_bounded(&bars[b], phase[b])) atomicAdd(&st->drainTimeouts, 1ULL);
+  if (st->hostError) {
+    *(volatile unsigned*)st->hostError = 1u;
+    __threadfence_system();
+  }
 }
 GRIM_D void tma_load_4d(void* dst, const CUtensorMap* map, unsigned long long* bar, int x, int y, int z, int w) {
   asm volatile(
@@ -445,30 +473,31 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_x1_tma(const __grid_con
     k = c.fk0 + (int)rk;
     j = c.fj0 + (int)(row - rk * (unsigned)c.nfj);
   };
+  // lane 0's record of the copies it issued and not yet seen land (the
+  // debug setting dbgSkipCopies issues none, so the waits run out)
+  bool inflight[2] = {false, false};
+  unsigned phase[2] = {0u, 0u};
   auto issue = [&](long long it, int buf) {
+    if (c.dbgSkipCopies) return;
     int i0, j, k;
     decompose(it, i0, j, k);
     mbar_expect_tx(&bars[buf], ROW * (unsigned)sizeof(double));
     tma_load_4d(rows + buf * ROW, &tmap, &bars[buf], (i0 - 3) & ~1, j, k, 0);
+    inflight[buf] = true;
   };
   if (lane == 0 && item < nitems) issue(item, 0);
-  unsigned phase0 = 0, phase1 = 0;
   int buf = 0;
   for (; item < nitems; item += stride, buf ^= 1) {
     const long long next = item + stride;
     if (lane == 0 && next < nitems) issue(next, buf ^ 1);
-    const unsigned ph = buf ? phase1 : phase0;
-    const bool arrived = mbar_wait_bounded(&bars[buf], ph);
-    if (buf) phase1 ^= 1; else phase0 ^= 1;
+    const bool arrived = mbar_wait_bounded(&bars[buf], phase[buf]);
     if (!__all_sync(0xffffffffu, arrived)) {
-      // give up: count it, let the copy in flight (if any) land, stop
-      if (lane == 0) {
-        atomicAdd(&st->waitTimeouts, 1ULL);
-        if (next < nitems) mbar_wait_bounded(&bars[buf ^ 1], buf ? phase0 : phase1);
-      }
+      if (lane == 0) copy_wait_gave_up(st, bars, inflight, phase);
       __syncwarp();
       return;
     }
+    phase[buf] ^= 1u;
+    inflight[buf] = false;
     int i0, j, k;
     decompose(item, i0, j, k);
     const int x0 = (i0 - 3) & ~1;
@@ -543,7 +572,10 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_strip_tma(const __grid_
     ch = (int)(r - o * nch);
     other = other0 + (int)o;
   };
+  bool inflight[2] = {false, false};  // lane 0: copies issued, not yet seen land
+  unsigned phase[2] = {0u, 0u};
   auto issue = [&](long long it, int buf) {
+    if (c.dbgSkipCopies) return;
     int iq, ch, other;
     decompose(it, iq, ch, other);
     mbar_expect_tx(&bars[buf], BOX * (unsigned)sizeof(double));
@@ -551,25 +583,22 @@ __global__ void __launch_bounds__(128, MINB) k_face_flux_strip_tma(const __grid_
       tma_load_4d(bufs + buf * BOX, &tmap, &bars[buf], iq * QI, ch * FPW, other, 0);
     else
       tma_load_4d(bufs + buf * BOX, &tmap, &bars[buf], iq * QI, other, ch * FPW, 0);
+    inflight[buf] = true;
   };
   if (lane == 0 && item < nitems) issue(item, 0);
-  unsigned phase0 = 0, phase1 = 0;
   int buf = 0;
   const int ii = lane % QI, jj = lane / QI;
   for (; item < nitems; item += stride, buf ^= 1) {
     const long long next = item + stride;
     if (lane == 0 && next < nitems) issue(next, buf ^ 1);
-    const unsigned ph = buf ? phase1 : phase0;
-    const bool arrived = mbar_wait_bounded(&bars[buf], ph);
-    if (buf) phase1 ^= 1; else phase0 ^= 1;
+    const bool arrived = mbar_wait_bounded(&bars[buf], phase[buf]);
     if (!__all_sync(0xffffffffu, arrived)) {
-      if (lane == 0) {
-        atomicAdd(&st->waitTimeouts, 1ULL);
-        if (next < nitems) mbar_wait_bounded(&bars[buf ^ 1], buf ? phase0 : phase1);
-      }
+      if (lane == 0) copy_wait_gave_up(st, bars, inflight, phase);
       __syncwarp();
       return;
     }
+    phase[buf] ^= 1u;
+    inflight[buf] = false;
     int iq, ch, other;
     decompose(item, iq, ch, other);
     const int i = iq * QI + ii;
@@ -1896,8 +1925,26 @@ __global__ void k_jacobian(DevCfg c, int stage, StageBufs b, const double* __res
     double P[NF], R[NF];
 #pragma unroll
     for (int v = 0; v < NF; v++) P[v] = pg[(long long)v * Z + z];
-    if (tangent) {
+    if (tangent == 1) {
       tangent_jacobian<COND, VISC, double>(P, K, G, c, J);
+    } else if (tangent == 2) {
+      tangent_jacobian<COND, VISC, double, true>(P, K, G, c, J);
+    } else if (tangent == 3) {
+      // the form and precision the mixed Newton uses: geometry rounded to
+      // FP32, the Jacobian in FP32
+      ZoneGeo<float> Gt;
+#pragma unroll
+      for (int m = 0; m < 4; m++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = (float)G.gcov[m][q]; Gt.gcon[m][q] = (float)G.gcon[m][q]; }
+      Gt.g = (float)G.g; Gt.alpha = (float)G.alpha; Gt.ialpha = (float)G.ialpha; Gt.x1 = (float)G.x1;
+      Gt.x2 = (float)G.x2; Gt.dyn = (float)G.dyn;
+      float Jf[NF][NF];
+      tangent_jacobian<COND, VISC, float>(P, K, Gt, c, Jf);
+#pragma unroll
+      for (int a = 0; a < NF; a++)
+#pragma unroll
+        for (int q = 0; q < NF; q++) J[a][q] = (double)Jf[a][q];
     } else {
       zone_residual<COND, VISC, double, double>(P, K, G, c, R);
       const double eps = c.jacEps;

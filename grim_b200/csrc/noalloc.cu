@@ -16,14 +16,18 @@
 //    the limit in grim_last_error()).
 //  * Host code cannot use the array's name as a device address; the first
 //    call on each device looks the address up with cudaGetSymbolAddress
-//    (with that device current) and caches it.  Make that first call before
-//    any stream capture.
+//    (with that device current) and caches it with the device's current
+//    context.  Make that first call before any stream capture.  A device
+//    reset (cudaDeviceReset) replaces the context and may move the array: a
+//    call that finds another context current looks the address up again
+//    (again, not inside a stream capture).
 //  * All calls share the array and it keeps the last call's contents.  The
 //    device scalars the kernels read are cleared at every call.  Calls that
 //    overlap on the GPU (different streams, or different host threads on
 //    one device) race on the array: serialise them.
 //  * Compiled like the parity kernels (no FMA contraction): the result is
 //    bit for bit the one of grim_compute_div_fluxes.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -44,21 +48,51 @@ void set_error_message(const char* msg);
 namespace {
 const int kMaxDevices = 64;
 double* g_scratch_ptr[kMaxDevices] = {nullptr};
+CUcontext g_scratch_ctx[kMaxDevices] = {nullptr};  // the context each cached address belongs to
 std::mutex g_scratch_mu;
 
-// device address of g_noalloc_scratch on the current device (first call on a
-// device: cudaGetSymbolAddress, checked, then cached)
+// the calling thread's current context (cuCtxGetCurrent through the
+// runtime's driver entry point: the library does not link libcuda)
+int current_context(CUcontext* ctx) {
+  typedef CUresult (*CtxGetCurrent)(CUcontext*);
+  static CtxGetCurrent fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !p)
+      return GRIM_ECUDA;
+    fn = reinterpret_cast<CtxGetCurrent>(p);
+  }
+  return fn(ctx) == CUDA_SUCCESS ? GRIM_OK : GRIM_ECUDA;
+}
+
+// device address of g_noalloc_scratch on the current device: looked up with
+// cudaGetSymbolAddress (checked) on the first call on a device, and again
+// when the device's context has changed since (a device reset); cached
 int scratch_address(int device, double** out) {
   if (device < 0 || device >= kMaxDevices) return GRIM_EINVAL;
   std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_ptr[device]) {
+  // cudaGetDevice does not create the primary context; the lookup below
+  // does, so the context is read after it on a first call
+  CUcontext ctx = nullptr;
+  if (current_context(&ctx) != GRIM_OK) {
+    grim::set_error_message("grim_div_fluxes_noalloc: cuCtxGetCurrent failed");
+    return GRIM_ECUDA;
+  }
+  if (!g_scratch_ptr[device] || ctx == nullptr || ctx != g_scratch_ctx[device]) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || p == nullptr) {
       grim::set_error_message("grim_div_fluxes_noalloc: cudaGetSymbolAddress of the scratch array failed");
       return GRIM_ECUDA;
     }
+    if (current_context(&ctx) != GRIM_OK) {
+      grim::set_error_message("grim_div_fluxes_noalloc: cuCtxGetCurrent failed");
+      return GRIM_ECUDA;
+    }
     g_scratch_ptr[device] = static_cast<double*>(p);
+    g_scratch_ctx[device] = ctx;
   }
   *out = g_scratch_ptr[device];
   return GRIM_OK;

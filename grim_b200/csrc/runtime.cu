@@ -74,6 +74,10 @@ struct grim_handle {
   int obsCap = 4096;
   DevState* st = nullptr;
   DevState* hst = nullptr;  // pinned mirror
+  // mapped pinned word a kernel whose bounded copy wait gave up sets to 1
+  // (DevState::hostError is its device alias); the next stepping or
+  // synchronising call reports it once as GRIM_ETIMEOUT
+  unsigned* hostError = nullptr;
   cudaEvent_t ev[8];
   bool graphOn = false;
   cudaGraphExec_t graph = nullptr;
@@ -137,6 +141,7 @@ static void free_all(grim_handle* h) {
     if (*b) { cudaFree(*b); *b = nullptr; }
   if (h->st) { cudaFree(h->st); h->st = nullptr; }
   if (h->hst) { cudaFreeHost(h->hst); h->hst = nullptr; }
+  if (h->hostError) { cudaFreeHost(h->hostError); h->hostError = nullptr; }
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
   for (int l = 0; l < 2; l++)
     if (h->list[l]) { cudaFree(h->list[l]); h->list[l] = nullptr; }
@@ -207,6 +212,7 @@ static int make_devcfg(const grim_config& c, DevCfg& d) {
   d.maxLF = c.MaxLorentzFactor; d.rhoFloorAmpl = c.RhoFloorAmpl; d.uFloorAmpl = c.UFloorAmpl;
   d.rhoFloorSlope = c.RhoFloorSlope; d.uFloorSlope = c.UFloorSlope;
   d.bsqOverRhoMax = c.BsqrOverRhoMax; d.bsqOverUMax = c.BsqrOverUMax;
+  d.dbgSkipCopies = 0;
   if ((c.problem == GRIM_PROBLEM_TORUS || c.closure == GRIM_CLOSURE_TORUS) && c.metric == GRIM_MINKOWSKI) {
     set_err("the torus problem and closure need the MKS metric"); return GRIM_EINVAL;
   }
@@ -582,6 +588,7 @@ int grim_create(const grim_config* cfg, int device, grim_handle** out) {
   }
   if (ok) ok = cudaMalloc(&h->st, sizeof(DevState)) == cudaSuccess;
   if (ok) ok = cudaMallocHost(&h->hst, sizeof(DevState)) == cudaSuccess;
+  if (ok) ok = cudaHostAlloc(&h->hostError, sizeof(unsigned), cudaHostAllocMapped) == cudaSuccess;
   if (!ok) {
     set_err("device allocation failed (%zu MB per grid variable)", Zb >> 20);
     free_all(h); delete h; return GRIM_ENOMEM;
@@ -610,6 +617,16 @@ int grim_create(const grim_config* cfg, int device, grim_handle** out) {
   // device scalars; the elements are first set on all-zero grids
   // (timestepper.cpp:287-295), which is the state the first computeDt sees
   memset(h->hst, 0, sizeof(DevState));
+  *(volatile unsigned*)h->hostError = 0u;
+  {
+    unsigned* alias = nullptr;
+    e = cudaHostGetDevicePointer((void**)&alias, h->hostError, 0);
+    if (e != cudaSuccess) {
+      set_err("mapping the host error word: %s", cudaGetErrorString(e));
+      free_all(h); delete h; return GRIM_ECUDA;
+    }
+    h->hst->hostError = alias;
+  }
   h->hst->dt = cfg->dt;
   h->hst->time = cfg->time;
   h->hst->first = 1;
@@ -775,7 +792,21 @@ int grim_restart(grim_handle* h, const char* restartFileName, const char* restar
   return GRIM_OK;
 }
 
+// GRIM_ETIMEOUT once per raised host error word (a bounded copy wait of an
+// earlier launch on this handle gave up); clears the word
+static int take_async_error(grim_handle* h) {
+  if (!h->hostError || *(volatile unsigned*)h->hostError == 0u) return GRIM_OK;
+  *(volatile unsigned*)h->hostError = 0u;
+  set_err("a bounded wait on an asynchronous copy gave up in an earlier launch on this handle: the face fluxes of "
+          "that stage were not computed, so the state is wrong; set the primitives again before stepping");
+  return GRIM_ETIMEOUT;
+}
+
 static int run_steps(grim_handle* h, int nsteps) {
+  {
+    const int rc = take_async_error(h);
+    if (rc) return rc;
+  }
   CK(cudaSetDevice(h->device));
   for (int n = 0; n < nsteps; n++) {
     const bool last = (n == nsteps - 1);
@@ -1098,7 +1129,7 @@ static int jac_common(grim_handle* h, const double* pg, double* jac, int memKind
   CK(cudaMallocAsync((void**)&dj, bytes, h->stream));
   StageBufs b = stage_bufs(h, h->lastStage);
   if (tangent)
-    grim::fast::jacobian(c, h->lastStage, b, h->scratch, dj, 1, h->stream);
+    grim::fast::jacobian(c, h->lastStage, b, h->scratch, dj, tangent, h->stream);
   else
     grim::exact::jacobian(c, h->lastStage, b, h->scratch, dj, 0, h->stream);
   CK(cudaGetLastError());
@@ -1112,6 +1143,13 @@ int grim_jacobian_fd(grim_handle* h, const double* pg, double* jac, int memKind)
 }
 int grim_jacobian_tangent(grim_handle* h, const double* pg, double* jac, int memKind) {
   return jac_common(h, pg, jac, memKind, 1);
+}
+int grim_jacobian_form(grim_handle* h, const double* pg, double* jac, int form, int memKind) {
+  if (form < GRIM_JAC_FD64 || form > GRIM_JAC_FAST32) {
+    set_err("grim_jacobian_form: unknown form %d", form);
+    return GRIM_EINVAL;
+  }
+  return jac_common(h, pg, jac, memKind, form);
 }
 
 int grim_newton_solve(grim_handle* h, int* iters) {
@@ -1273,6 +1311,8 @@ int grim_get_stats(grim_handle* h, grim_stats* out) {
   // error is cleared rather than left for the next checked call
   (void)cudaGetLastError();
   s.kernelLaunches = h->launchesPerStep;
+  s.waitTimeouts = (long long)h->hst->waitTimeouts;
+  s.drainTimeouts = (long long)h->hst->drainTimeouts;
   *out = s;
   return GRIM_OK;
 }
@@ -1730,6 +1770,14 @@ int grim_synchronize(grim_handle* h) {
   if (!h) return GRIM_EINVAL;
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
+  return take_async_error(h);
+}
+
+int grim_set_debug(grim_handle* h, int setting, int value) {
+  if (!h) return GRIM_EINVAL;
+  if (setting != GRIM_DEBUG_SKIP_BULK_COPIES) { set_err("grim_set_debug: unknown setting %d", setting); return GRIM_EINVAL; }
+  h->dc.dbgSkipCopies = value != 0;
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
   return GRIM_OK;
 }
 

@@ -20,6 +20,8 @@ struct DevState {
   unsigned long long listCount[2];   // compacted worklists: entries per ping-pong list
   unsigned long long waitTimeouts;   // bounded waits on asynchronous copies that gave up
   unsigned long long obsCount;       // torus observer records written (ring index = count % capacity)
+  unsigned long long drainTimeouts;  // give-up paths whose wait for their own copies in flight gave up too
+  unsigned* hostError;               // device alias of the handle's mapped host error word (null: none)
 };
 
 // the torus observers (ObserversTorus.hpp:6-253), in record order

@@ -15,7 +15,9 @@ library's four segments with, between them,
     after POST   X3 halo of primOld
 
 Every zone's arithmetic is the single-GPU step's, so a decomposed run gives
-the same primitives bit for bit.
+the same primitives bit for bit.  The torus observers are each slab's own
+sums and extrema; ``torusObservers`` and ``observations`` combine them over
+the ranks as ObserversTorus.hpp does over MPI ranks.
 """
 import ctypes
 
@@ -29,6 +31,28 @@ from .timestepper import timeStepper
 
 SEG_PRE, SEG_HALF, SEG_FULL, SEG_POST = 0, 1, 2, 3
 SCALAR_MAXINVDT, SCALAR_NANFLAG = 0, 1
+
+# How each torus observer (timeStepper.OBSERVERS order) combines over slabs,
+# as ObserversTorus.hpp:6-253 combines it over MPI ranks: the integrals and
+# boundary fluxes are summed (rank 0's value, then rank 1's, ...), rhoMax is
+# a maximum, betaMin a minimum.
+OBS_COMBINE = ("sum", "sum", "sum", "max", "min", "sum", "sum", "sum", "sum")
+
+
+def combine_observer_rows(rows):
+    """The global observers from each rank's values, ``rows`` in rank order
+    (a sequence of equal-shape arrays whose last axis is the 9 observers)."""
+    rows = [np.asarray(r, dtype=np.float64) for r in rows]
+    out = rows[0].copy()
+    for r in rows[1:]:
+        for k, how in enumerate(OBS_COMBINE):
+            if how == "sum":
+                out[..., k] = out[..., k] + r[..., k]
+            elif how == "max":
+                out[..., k] = np.maximum(out[..., k], r[..., k])
+            else:
+                out[..., k] = np.minimum(out[..., k], r[..., k])
+    return out
 
 
 def slab_config(cfg, rank, world):
@@ -51,6 +75,18 @@ def slab_config(cfg, rank, world):
     if periodic or rank < world - 1:
         local["boundaryFront"] = C.EXCHANGE
     return local
+
+
+def all_gather_rows(a, world, group=None, device=None):
+    """Every rank's float64 array ``a`` (same shape on all ranks), in rank
+    order; through ``device`` memory for NCCL, host memory when None."""
+    loc = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64))
+    if world == 1:
+        return [loc.numpy()]
+    t = loc if device is None else loc.to(device)
+    parts = [torch.empty_like(t) for _ in range(world)]
+    dist.all_gather(parts, t, group=group)
+    return [p.cpu().numpy() for p in parts]
 
 
 def neighbours(rank, world, periodic):
@@ -124,6 +160,35 @@ class SlabTimeStepper:
         w = self.ts.primOld if which is None else which
         s3, s2, s1 = C.interior_slices(self.local)
         return w.getVars()[:, s3, s2, s1]
+
+    def _all_gather_rows(self, a):
+        return all_gather_rows(a, self.world, self.group, None if self.host else self.device)
+
+    def torusObservers(self):
+        """The torus observers of the whole decomposed grid on primOld
+        (every rank gets them): each slab's, combined as OBS_COMBINE says."""
+        names = timeStepper.OBSERVERS
+        loc = self.ts.torusObservers()
+        rows = self._all_gather_rows(np.array([loc[n] for n in names]))
+        return dict(zip(names, combine_observer_rows(rows).tolist()))
+
+    def observations(self, maxRecords=4096):
+        """The records the steps wrote (ObserveEveryDt > 0), combined over
+        the slabs; every rank records at the same global times."""
+        names = timeStepper.OBSERVERS
+        recs = self.ts.observations(maxRecords)
+        n = np.array([len(recs)], dtype=np.float64)
+        counts = self._all_gather_rows(n)
+        if any(int(c[0]) != len(recs) for c in counts):
+            raise RuntimeError("slabs hold different numbers of observer records: %s"
+                               % [int(c[0]) for c in counts])
+        tab = np.array([[r["time"]] + [r[k] for k in names] for r in recs]).reshape(len(recs), 1 + len(names))
+        parts = self._all_gather_rows(tab)
+        for p in parts[1:]:
+            if not np.array_equal(p[:, 0], parts[0][:, 0]):
+                raise RuntimeError("slabs recorded their observers at different times")
+        vals = combine_observer_rows([p[:, 1:] for p in parts])
+        return [dict(time=float(parts[0][i, 0]), **dict(zip(names, vals[i].tolist()))) for i in range(len(recs))]
 
     def gatherInterior(self):
         """The global interior of primOld on every rank (all-gather)."""

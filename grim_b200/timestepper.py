@@ -169,7 +169,12 @@ class timeStepper:
         _lib.check(_lib.lib().grim_get_stats(self._h, ctypes.byref(s)), "get_stats")
         return dict(newtonIters=list(s.newtonIters), unconverged=list(s.unconverged),
                     nonFinite=s.nonFinite, msStep=s.msStep, msStencil=s.msStencil,
-                    msNewton=s.msNewton, msOther=s.msOther, kernelLaunches=s.kernelLaunches)
+                    msNewton=s.msNewton, msOther=s.msOther, kernelLaunches=s.kernelLaunches,
+                    waitTimeouts=s.waitTimeouts, drainTimeouts=s.drainTimeouts)
+
+    def setDebug(self, setting, value):
+        """Test hook (grim_set_debug), e.g. _lib.DEBUG_SKIP_BULK_COPIES."""
+        _lib.check(_lib.lib().grim_set_debug(self._h, int(setting), int(value)), "set_debug")
 
     def newtonHistogram(self):
         """[stage][iterations] -> zones, for the last step (tangent / mixed)."""
@@ -360,6 +365,16 @@ class timeStepper:
         nf = self.numFluidVars
         J = np.zeros(self.zshape + (nf, nf))
         _lib.check(_lib.lib().grim_jacobian_tangent(self._h, _ptr(p), _ptr(J), _lib.HOST), "jacobian_tangent")
+        return J
+
+    JAC_FD64, JAC_FAST64, JAC_DUAL64, JAC_FAST32 = 0, 1, 2, 3
+
+    def jacobianForm(self, primGuess, form):
+        """The Jacobian in one of the JAC_* forms (grim_jacobian_form)."""
+        p = np.ascontiguousarray(primGuess, dtype=np.float64)
+        nf = self.numFluidVars
+        J = np.zeros(self.zshape + (nf, nf))
+        _lib.check(_lib.lib().grim_jacobian_form(self._h, _ptr(p), _ptr(J), int(form), _lib.HOST), "jacobian_form")
         return J
 
     def solve(self):

@@ -114,7 +114,9 @@ typedef struct grim_stats {
   double msNewton;             /* Newton kernels, both stages */
   double msOther;              /* ghost fill, dt, copies */
   long long kernelLaunches;    /* launches of this library's kernels in the step */
-  double reserved[8];
+  long long waitTimeouts;      /* bounded waits on asynchronous copies that gave up, since creation */
+  long long drainTimeouts;     /* of those, give-ups whose copies in flight did not land either */
+  double reserved[6];
 } grim_stats;
 
 /* ---- lifecycle: timeStepper::timeStepper / ~timeStepper
@@ -165,7 +167,9 @@ int grim_write_restart(grim_handle* h, const char* restartFileName, const char* 
  * the element the next computeDt reads; dt keeps its current value. */
 int grim_restart(grim_handle* h, const char* restartFileName, const char* restartFileTime, const char* restartFile);
 /* the format pieces, host only (no GPU): the PETSc binary Vec file and the
- * reorder between [var][k][j][i] with ghosts and the natural interior */
+ * reorder between [var][k][j][i] with ghosts and the natural interior.
+ * grim_petsc_vec_read returns GRIM_ENOTSUP for an HDF5 file (the reference's
+ * own .h5 restart files), GRIM_EINVAL for anything else it cannot read. */
 int grim_petsc_vec_write(const char* fileName, const double* v, long long n);
 int grim_petsc_vec_read(const char* fileName, double* v, long long n);
 int grim_natural_from_prims(const grim_config* cfg, const double* prims, double* natural);
@@ -242,8 +246,19 @@ int grim_stage_setup(grim_handle* h, int stage);
 int grim_residual(grim_handle* h, const double* primGuess, double* residual, int memKind);
 /* FD Jacobian (solve.cpp:82-109): [Z][nf][nf], J[z][i][j] = dR_i/dP_j */
 int grim_jacobian_fd(grim_handle* h, const double* primGuess, double* jac, int memKind);
-/* exact forward-tangent Jacobian of the same residual, same layout */
+/* exact forward-tangent Jacobian of the same residual, same layout (the
+ * form the fast Newton uses, in FP64: closed-form dU/dP for ideal MHD, a
+ * forward-tangent pass of the residual with EMHD) */
 int grim_jacobian_tangent(grim_handle* h, const double* primGuess, double* jac, int memKind);
+/* the Jacobian in a chosen form, same layout; extends solve.cpp:82-109 for
+ * tests of the fast Newton's Jacobians against each other */
+enum {
+  GRIM_JAC_FD64 = 0,     /* = grim_jacobian_fd */
+  GRIM_JAC_FAST64 = 1,   /* = grim_jacobian_tangent */
+  GRIM_JAC_DUAL64 = 2,   /* forward-tangent pass of the residual, also for ideal MHD */
+  GRIM_JAC_FAST32 = 3    /* the mixed Newton's Jacobian: FAST64's form on FP32 geometry, in FP32 */
+};
+int grim_jacobian_form(grim_handle* h, const double* primGuess, double* jac, int form, int memKind);
 /* solve() on GRIM_PRIM with the configured newtonMode */
 int grim_newton_solve(grim_handle* h, int* itersDone);
 /* batched pivoted solve of nf x nf systems (the af::solve of solve.cpp:220)
@@ -275,6 +290,24 @@ int grim_get_stats(grim_handle* h, grim_stats* out);
 /* capture timeStep into a CUDA graph and replay it from grim_time_step */
 int grim_enable_graph(grim_handle* h, int enable);
 int grim_synchronize(grim_handle* h);
+
+/* Bounded waits.  The TMA-staged face kernels wait on their copies for at
+ * most 1 s.  A wait that gives up leaves that kernel's flux rows unwritten,
+ * so the stage it belongs to is wrong: it is counted in
+ * grim_stats.waitTimeouts and raises an error word in mapped host memory.
+ * The next grim_time_step, grim_time_steps or grim_synchronize on the
+ * handle that finds the word raised (grim_synchronize always does: it waits
+ * first; the stepping calls see it once the kernel has ended) clears it and
+ * returns GRIM_ETIMEOUT without stepping; the primitives must then be set
+ * again.  The give-up path waits (again bounded) for the copies its warp
+ * still has in flight; if one of those does not land either
+ * (grim_stats.drainTimeouts), destroy the handle. */
+enum {
+  GRIM_DEBUG_SKIP_BULK_COPIES = 1  /* value != 0: the TMA-staged face kernels
+                                      issue no copies, so their waits run out */
+};
+/* test hook: set a debug setting; no counterpart in the reference */
+int grim_set_debug(grim_handle* h, int setting, int value);
 /* the handle's cudaStream_t, as void* */
 void* grim_stream(grim_handle* h);
 
@@ -387,8 +420,9 @@ int grim_adjoint_stencil(grim_handle* h, const double* prim, const double* gbar,
  *      scratch lives in one static 64 MiB device array per GPU that loads the
  *      library; grids needing more are rejected with GRIM_EINVAL.  Minkowski
  *      metric only.  The first call on a device looks up that array's address
- *      (make it before any stream capture); calls that overlap on the GPU
- *      share the array and race. */
+ *      (make it before any stream capture), as does the first call after a
+ *      device reset; calls that overlap on the GPU share the array and
+ *      race. */
 int grim_div_fluxes_noalloc(const grim_config* cfg, const double* prim, double* divF, void* stream);
 
 #ifdef __cplusplus

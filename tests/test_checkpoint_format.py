@@ -13,6 +13,7 @@ from grim_b200 import config as C
 
 
 EINVAL = -1
+ENOTSUP = -5
 
 
 def _ptr(a):
@@ -63,3 +64,15 @@ def test_natural_order(dim, emhd):
     ghost = np.ones(Q.shape[1:], bool)
     ghost[s3, s2, s1] = False
     assert np.all(Q[:, ghost] == 7.)
+
+
+def test_vec_read_rejects_hdf5_restart_files(tmp_path):
+    """A restart file of the reference (PETSc's HDF5 viewer, grid.cpp:367-381)
+    starts with the HDF5 signature; it is refused with GRIM_ENOTSUP and a
+    message saying that HDF5 restart files are not supported."""
+    f = tmp_path / "restartFile.h5"
+    f.write_bytes(b"\x89HDF\r\n\x1a\n" + bytes(8) + np.arange(8.).tobytes())
+    out = np.zeros(5)
+    assert _lib.lib().grim_petsc_vec_read(str(f).encode(), _ptr(out), 5) == ENOTSUP
+    msg = _lib.lib().grim_last_error().decode()
+    assert "HDF5" in msg and "not supported" in msg

@@ -2,8 +2,10 @@
 
 The reference cannot be built here (ArrayFire, PETSc and MPI are absent),
 so the oracle is pinned on the reference's published and tested results:
-  * the damped EMHD eigenmode of linear_modes and its 2nd-order convergence
-    (src/problem/linear_modes/problem.cpp:118-213, Linear modes.ipynb);
+  * the damped EMHD eigenmode of linear_modes: the published error table of
+    Linear modes.ipynb cell 1 reproduced to its printed digits (the
+    fullStepDiagnostics errors of src/problem/linear_modes/problem.cpp:118-213
+    at t = 0.5, N = 32, 64, 128), and its 2nd-order convergence;
   * the analytic modified Kerr-Schild metric, inverse, sqrt(-g), lapse and
     Christoffel symbols of McKinney & Gammie 2004 used by
     src/geometry/test_geometry.py:93-345;
@@ -196,16 +198,57 @@ def test_golden_snapshots():
         np.testing.assert_allclose(probe, case["probe"], rtol=1e-13, err_msg=name)
 
 
-def test_published_l1_table_order():
-    """Linear modes.ipynb cell 1: the published L1 errors fall at 2nd order
-    (the fixture holds the table as published)."""
-    gold = json.load(open(os.path.join(GOLDEN, "golden.json")))
-    tab = gold["published_linear_modes_L1"]
-    N = np.array(tab["N"], dtype=float)
-    for k, v in tab["errors"].items():
-        v = np.array(v)
-        slope = -np.polyfit(np.log2(N), np.log2(v), 1)[0]
-        assert 1.7 < slope < 3.7, (k, slope)
+# fixture keys of the published table -> variable names of the diagnostic
+PUBLISHED_KEYS = dict(rho="RHO", u="U", u1="U1", u2="U2", q="Q", dP="DP", B1="B1", B2="B2")
+# The table is printed to 7 significant digits, but it is a norm of
+# differences between O(1e-8) perturbations and the analytic mode, taken on
+# O(1) backgrounds (rho = 1, u = 2, B2 = 0.3): the rounding of each step's
+# FP64 arithmetic, which differs between the reference's GPU build, the
+# oracle and the CUDA paths, reaches the 5th digit by N = 128, the 4th at
+# N = 256 (errors of 1e-15..1e-16) and the 3rd at N = 512 (1e-16..1e-17).
+# Agreement is held per N to: 1e-4 relative up to N = 128 (largest seen:
+# 2.2e-5 oracle and FP64 path, 7.2e-5 fast form), 5e-4 at N = 256 (1.6e-4
+# oracle and FP64 path, 2.5e-4 fast form), 5e-3 at N = 512 (6.0e-4 FP64 path,
+# 2.9e-3 fast form).
+PUBLISHED_RTOL = {32: 1e-4, 64: 1e-4, 128: 1e-4, 256: 5e-4, 512: 5e-3}
+
+
+def published_l1_table():
+    tab = json.load(open(os.path.join(GOLDEN, "golden.json")))["published_linear_modes_L1"]
+    return {int(N): {PUBLISHED_KEYS[k]: v[i] for k, v in tab["errors"].items()}
+            for i, N in enumerate(tab["N"])}
+
+
+def run_published_linear_mode(step_fn, N, **kw):
+    """The damped EMHD mode of linear_modes/params.cpp:4-81 (minmod theta 2,
+    HLL, CFL 0.9, conduction and viscosity with high-order terms) run as
+    grim.cpp:31-46 runs it up to the published end time; returns the
+    fullStepDiagnostics errors of the final state.  ``kw`` overrides config
+    fields that do not change the scheme (Newton tolerances)."""
+    cfg = PR.linear_modes_config(N=N, **kw)
+    P, t = step_fn(cfg, PR.LM_PUBLISHED_FINAL_TIME)
+    return PR.linear_modes_errors(cfg, P, t)
+
+
+def test_oracle_reproduces_published_l1_table():
+    """The oracle's timestep reproduces the reference's only published
+    numbers for this path, Linear modes.ipynb cell 1, at N = 32, 64 and 128
+    in all 8 variables (to 1e-4 relative, PUBLISHED_RTOL).  These are the
+    errors fullStepDiagnostics prints (problem.cpp:184-212) after the step
+    that crosses t = 0.5."""
+    table = published_l1_table()
+
+    def oracle_run(cfg, tfinal):
+        o = O.Oracle(cfg)
+        o.set_prims(PR.linear_modes_prims(cfg))
+        while o.time < tfinal:
+            o.time_step(1)
+        return o.get_prims(), o.time
+
+    for N in (32, 64, 128):
+        errs = run_published_linear_mode(oracle_run, N)
+        for k, v in table[N].items():
+            assert abs(errs[k] - v) <= PUBLISHED_RTOL[N] * v, (N, k, errs[k], v)
 
 
 def test_oracle_flux_ct_keeps_corner_divb():

@@ -197,6 +197,43 @@ def test_linear_mode_second_order_on_gpu():
     assert o1 > 1.5 and o2 > 1.7, (errs, o1, o2)
 
 
+@pytest.mark.parametrize("mode", [C.NEWTON_PARITY_FD64, C.NEWTON_MIXED32])
+def test_published_l1_table_on_gpu(mode):
+    """The reference's published numbers for this path (Linear modes.ipynb
+    cell 1: the linear_modes fullStepDiagnostics errors at N = 32 ... 512)
+    reproduced by the CUDA timestep, all 8 variables, within PUBLISHED_RTOL
+    of the printed table (1e-4 relative up to N = 128, 5e-4 at 256, 5e-3 at
+    512, where rounding reaches those digits of the tiny errors).  The FP64 parity path and the
+    fast form (FP32 tangent Jacobian and solve, FP64 residual, per-zone
+    convergence at relative residual 1e-10 with the absolute floor
+    |R| <= 1e-12 the other fast-form tests use: the reference's atol 1e-20
+    on |R|^2 is a global-break test there, and as a per-zone stopping rule
+    it would leave a Newton error near the N = 512 entries) are held to the
+    same band: the fast form's Newton error is far below the
+    discretisation error the table measures."""
+    from grim_b200.timestepper import timeStepper
+    from tests.test_oracle_pins import PUBLISHED_RTOL, published_l1_table, run_published_linear_mode
+
+    def gpu_run(cfg, tfinal):
+        ts = timeStepper(cfg)
+        if mode != C.NEWTON_PARITY_FD64:
+            ts.setNewtonMode(mode, 1, 1e-10)
+        ts.primOld.setVars(PR.linear_modes_prims(cfg))
+        while ts.time < tfinal:
+            ts.timeStep()
+        st = ts.stats()
+        assert st["nonFinite"] == 0
+        return ts.primOld.getVars(), ts.time
+
+    kw = {} if mode == C.NEWTON_PARITY_FD64 else dict(nonlinearsolve_atol=1e-24)
+    table = published_l1_table()
+    worst = {}
+    for N in sorted(table):
+        errs = run_published_linear_mode(gpu_run, N, **kw)
+        worst[N] = max(abs(errs[k] - v) / v for k, v in table[N].items())
+    assert all(worst[N] <= PUBLISHED_RTOL[N] for N in worst), worst
+
+
 def test_batch_solve_matches_numpy():
     from grim_b200.timestepper import batchSolve
     rng = np.random.default_rng(11)

@@ -72,3 +72,44 @@ def test_halo_wiring_gloo(world, periodic):
         lo, hi = out[r]
         assert lo == (10 * lower + 2 if lower is not None else -1.0), (r, lo)
         assert hi == (10 * upper + 1 if upper is not None else -1.0), (r, hi)
+
+
+def test_combine_observer_rows():
+    """Integrals and boundary fluxes add over slabs, rhoMax is the largest
+    slab maximum, betaMin the smallest slab minimum (ObserversTorus.hpp)."""
+    a = np.arange(1., 10.)
+    b = np.array([10., 20., 30., 0.5, 7., 40., 50., 60., 70.])
+    out = slab.combine_observer_rows([a, b])
+    want = a + b
+    want[3] = max(a[3], b[3])
+    want[4] = min(a[4], b[4])
+    np.testing.assert_array_equal(out, want)
+    # records (rows of 9) combine row by row
+    recs = slab.combine_observer_rows([np.stack([a, b]), np.stack([b, a])])
+    np.testing.assert_array_equal(recs[0], want)
+    np.testing.assert_array_equal(recs[1], want)
+
+
+def _obs_worker(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        mine = np.full((2, 9), float(rank + 1))
+        mine[:, 4] = 10. - rank  # betaMin: smallest on the last rank
+        rows = slab.all_gather_rows(mine, world)
+        out[rank] = slab.combine_observer_rows(rows).tolist()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_observer_rows_gathered_over_gloo():
+    """Two ranks gather each other's observer records in rank order and
+    agree on the combined values."""
+    out = mp.Manager().dict()
+    mp.start_processes(_obs_worker, args=(2, _free_port(), out), nprocs=2, start_method="spawn")
+    for r in range(2):
+        got = np.array(out[r])
+        assert got.shape == (2, 9)
+        np.testing.assert_array_equal(got[:, 0], 3.)  # 1 + 2
+        np.testing.assert_array_equal(got[:, 3], 2.)  # max
+        np.testing.assert_array_equal(got[:, 4], 9.)  # min

@@ -87,3 +87,59 @@ def test_two_rank_slabs_equal_the_plain_step(tmp_path):
     mp.start_processes(_rank, args=(2, port, C.NEWTON_PARITY_FD64, P, out), nprocs=2, start_method="spawn")
     assert not np.isnan(ref).any()
     assert np.array_equal(np.load(out), ref)
+
+
+def _obs_rank(rank, world, port, cfg, P, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import torch.distributed as dist
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from grim_b200.slab import SlabTimeStepper
+        sl = SlabTimeStepper(cfg, device=0)
+        sl.setGlobalPrims(P)
+        sl.ts.problemInit()
+        for _ in range(STEPS):
+            sl.timeStep()
+        recs = sl.observations()
+        now = sl.torusObservers()
+        if rank == 0:
+            np.save(out, np.array([[r["time"]] + [r[k] for k in OBS] for r in recs]
+                                  + [[sl.time] + [now[k] for k in OBS]]))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+OBS = ("BaryonMass", "EMag", "ETh", "rhoMax", "betaMin", "MdotIn", "MdotOut", "UnboundMdotOut",
+       "RelativisticUnboundMdotOut")
+
+
+def test_two_rank_slab_observers_equal_the_single_handle(tmp_path):
+    """The torus observers recorded by a two-slab run, combined over the
+    ranks (sums for the integrals and boundary fluxes, max rhoMax, min
+    betaMin), equal the single handle's records: sums to 1e-13 of their
+    magnitude (the partial sums are added in another order), extrema and
+    record times exactly."""
+    cfg = dict(_cfg(C.NEWTON_PARITY_FD64), ObserveEveryDt=1e-12)
+    ts, P = _initial(cfg)
+    _single(cfg, P, ts)
+    ref = [[r["time"]] + [r[k] for k in OBS] for r in ts.observations()]
+    now = ts.torusObservers()
+    ref.append([ts.time] + [now[k] for k in OBS])
+    ref = np.array(ref)
+    del ts
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    out = str(tmp_path / "obs.npy")
+    mp.start_processes(_obs_rank, args=(2, port, cfg, P, out), nprocs=2, start_method="spawn")
+    got = np.load(out)
+    assert got.shape == ref.shape and ref.shape[0] >= STEPS + 1
+    np.testing.assert_array_equal(got[:, 0], ref[:, 0])
+    for k, name in enumerate(OBS, start=1):
+        if name in ("rhoMax", "betaMin"):
+            np.testing.assert_array_equal(got[:, k], ref[:, k], err_msg=name)
+        else:
+            scale = np.max(np.abs(ref[:, k])) + 1e-300
+            assert np.max(np.abs(got[:, k] - ref[:, k])) <= 1e-13 * scale, name

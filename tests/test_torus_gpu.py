@@ -252,6 +252,53 @@ def _torus_stepper(mode, **kw):
     return cfg, ts
 
 
+def _column_err(a, b, keep):
+    """max over kept zones and columns of max_i |a[z,i,j] - b[z,i,j]| / max_i |b[z,i,j]|"""
+    scale = np.max(np.abs(b), axis=-2, keepdims=True) + 1e-300
+    return float(np.max((np.abs(a - b) / scale)[keep]))
+
+
+def test_closed_form_jacobian_on_kerr_schild():
+    """The closed-form ideal-MHD Jacobian the fast Newton uses on every torus
+    step (physics.cpp:53-217 differentiated by hand) on the 64x32x8 torus,
+    MKS with derefine and cylindrify, at the half stage's Newton guess:
+      * against the generic forward-tangent pass of the residual (dual
+        numbers, FP64): 1e-10 of each zone's column scale;
+      * against a central difference of the FP64 residual with the step
+        h_j = 1e-6 |P_j| for rho and u (the atmosphere holds them near
+        1e-12: a larger step crosses the element's floors, a kink) and
+        1e-6 max(|P_j|, 1e-2) for the velocities: 1e-6 of the column scale
+        (O(h^2) plus roundoff / h);
+      * the mixed Newton's FP32 Jacobian (the same closed form on FP32
+        geometry) against the FP64 one: 3e-5 of the column scale, the
+        stated error of the Jacobian the FP64 residual then corrects."""
+    from grim_b200.timestepper import timeStepper as TS
+    cfg, ts = _torus_stepper(C.NEWTON_PARITY_FD64)
+    ts.stageSetup(C.HALF_STEP)
+    guess = ts.prim.getVars()
+    s3, s2, s1 = C.interior_slices(cfg)
+    J64 = ts.jacobianForm(guess, TS.JAC_FAST64)
+    Jdual = ts.jacobianForm(guess, TS.JAC_DUAL64)
+    J32 = ts.jacobianForm(guess, TS.JAC_FAST32)
+    assert np.array_equal(J64, ts.jacobianTangent(guess))
+    keep = np.zeros(ts.zshape + (1, 1), bool)
+    keep[s3, s2, s1] = True
+    keep = np.broadcast_to(keep, J64.shape)
+    assert np.all(np.isfinite(J64[keep]))
+    assert _column_err(J64, Jdual, keep) <= 1e-10
+    assert _column_err(J32, J64, keep) <= 3e-5
+    nf = C.var_counts(cfg)[1]
+    Jfd = np.zeros_like(J64)
+    for j in range(nf):
+        h = 1e-6 * (np.abs(guess[j]) if j < 2 else np.maximum(np.abs(guess[j]), 1e-2))
+        h = np.where(h > 0, h, 1e-8)  # ghost zones (not compared) may hold zeros
+        gp, gm = guess.copy(), guess.copy()
+        gp[j] += h
+        gm[j] -= h
+        Jfd[..., :, j] = np.moveaxis((ts.computeResidual(gp) - ts.computeResidual(gm)) / (2 * h), 0, -1)
+    assert _column_err(J64, Jfd, keep) <= 1e-6
+
+
 def test_torus_fast_steps_match_parity_path():
     """The fast form of the torus step (FP32 closed-form Jacobian, FP64
     residual, per-zone convergence, FMA arithmetic, its fused floors / dt /

@@ -5,11 +5,13 @@ primitives and the result and keeps all of its scratch in one static 64 MiB
 device array, so it must give the same divergence as the allocating entry
 point grim_compute_div_fluxes.
 
-Two calls in a row with different workloads (ideal MHD, then EMHD, whose
-scratch layout differs) are each compared with grim_compute_div_fluxes at
-the tolerance of the other divergence tests (1e-13 of each variable's
-scale); a grid beyond the scratch limit is refused.  This file is collected
-last so a failure here leaves the rest of the suite already run.
+Calls in a row with different workloads (ideal MHD in 2D, EMHD, whose
+scratch layout differs, Orszag-Tang with WENO5/HLL, and a 3D grid with its
+three corner EMFs) are each compared with grim_compute_div_fluxes at the
+tolerance of the other divergence tests (1e-13 of each variable's scale).
+A grid whose scratch fits just under the limit is computed; the next size
+up is refused.  This file is collected last so a failure here leaves the
+rest of the suite already run.
 """
 import ctypes
 
@@ -34,13 +36,19 @@ def _noalloc(cfg, prim_dev, out_dev, stream):
 
 
 def test_noalloc_divergence_matches_allocating_entry_point():
-    import torch
-    from grim_b200.timestepper import timeStepper
-
     cases = [
         (PR.fast_mode_config(N=48), PR.fast_mode_prims),
         (PR.linear_modes_config(N=40), lambda c: PR.linear_modes_prims(c, amplitude=1e-3)),
+        (PR.orszag_tang_config(N=64), PR.orszag_tang_prims),
+        (PR.fast_mode_config(N=24, dim=3, N3=24), PR.fast_mode_prims),
+        (PR.fast_mode_config(N=48), PR.fast_mode_prims),  # the first workload again, after the others
     ]
+    _compare_cases(cases)
+
+
+def _compare_cases(cases):
+    import torch
+    from grim_b200.timestepper import timeStepper
     stream = torch.cuda.current_stream().cuda_stream
     for cfg, mk in cases:
         P = np.ascontiguousarray(mk(cfg))
@@ -55,9 +63,31 @@ def test_noalloc_divergence_matches_allocating_entry_point():
         assert scaled_err(interior(cfg, got), interior(cfg, ref)) <= 1e-13
 
 
-def test_noalloc_rejects_grids_beyond_the_scratch_limit():
+SCRATCH_WORDS = 8 * 1024 * 1024  # the documented limit: 64 MiB of doubles
+
+
+def _scratch_words(cfg):
+    """Scratch the call needs for a 2D/3D ideal-MHD grid: face fluxes per
+    direction, the stage's conserved variables and guess (dof rows each),
+    the explicit sources (nf rows), plus at most 1024 words of device
+    scalars."""
+    dof, nf = C.var_counts(cfg)
+    n1, n2, n3 = C.total_dims(cfg)
+    Z = n1 * n2 * n3
+    return cfg["dim"] * dof * Z + 2 * dof * Z + nf * Z
+
+
+def test_noalloc_at_the_scratch_limit():
+    """The largest 2D ideal-MHD grid whose scratch fits (470^2 + ghosts) is
+    computed like the allocating entry point; 471^2 is refused."""
+    fits, over = PR.fast_mode_config(N=470), PR.fast_mode_config(N=471)
+    assert _scratch_words(fits) + 1024 <= SCRATCH_WORDS < _scratch_words(over)
+    _compare_cases([(fits, PR.fast_mode_prims)])
+    _expect_refused(over)
+
+
+def _expect_refused(cfg):
     import torch
-    cfg = PR.fast_mode_config(N=1024)
     dof, _ = C.var_counts(cfg)
     n1, n2, n3 = C.total_dims(cfg)
     prim_dev = torch.zeros((dof, n3, n2, n1), dtype=torch.float64, device="cuda")
@@ -65,3 +95,7 @@ def test_noalloc_rejects_grids_beyond_the_scratch_limit():
     rc = _noalloc(cfg, prim_dev.data_ptr(), out_dev.data_ptr(), torch.cuda.current_stream().cuda_stream)
     assert rc == -1
     assert b"maximum" in _lib.lib().grim_last_error()
+
+
+def test_noalloc_rejects_grids_beyond_the_scratch_limit():
+    _expect_refused(PR.fast_mode_config(N=1024))
