@@ -31,6 +31,7 @@ PROBLEM_TORUS = 1
 NEWTON_PARITY_FD64 = 0     # the reference's method (solve.cpp:3-230)
 NEWTON_TANGENT64 = 1       # exact forward-tangent Jacobian, FP64 solve
 NEWTON_MIXED32 = 2         # FP32 tangent Jacobian + FP32 solve, FP64 residual
+NEWTON_FD64_FAST = 3       # the reference's FD Newton in the fast path's arithmetic and kernels
 
 INT_FIELDS = [
     "N1", "N2", "N3", "dim", "numGhost",
@@ -64,8 +65,9 @@ DOUBLE_FIELDS = [
     "MaxLorentzFactor", "RhoFloorAmpl", "UFloorAmpl", "RhoFloorSlope",
     "UFloorSlope", "BsqrOverRhoMax", "BsqrOverUMax",
     "ObserveEveryDt",
+    "nonlinearsolve_ulps",
 ]
-N_RESERVED_DOUBLE = 5
+N_RESERVED_DOUBLE = 4
 
 
 def _struct_fields():
@@ -112,7 +114,7 @@ def defaults():
         MaxLorentzFactor=10., RhoFloorAmpl=1e-3, UFloorAmpl=1e-5,
         RhoFloorSlope=-2.5, UFloorSlope=-2.5,
         BsqrOverRhoMax=10., BsqrOverUMax=500.,
-        ObserveEveryDt=0.,
+        ObserveEveryDt=0., nonlinearsolve_ulps=0.,
     )
 
 

@@ -37,6 +37,7 @@ struct DevCfg {
   double CondAlpha, ViscAlpha, CondClosure, ViscClosure;
   double theta;
   double atol, rtol, jacEps, lsFloor;
+  double tolUlps;  // rounding floor of the Newton test in ulps of the residual's largest term (0: none)
   double tau0, tau1;
   // torus floors (problem hook)
   double maxLF, rhoFloorAmpl, uFloorAmpl, rhoFloorSlope, uFloorSlope, bsqOverRhoMax, bsqOverUMax;

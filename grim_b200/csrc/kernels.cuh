@@ -1278,6 +1278,14 @@ GRIM_D void load_stage_const(StageConst<5 + COND + VISC>& K, const DevCfg& c, in
   K.idtp = 1. / K.dtp;
 #pragma unroll
   for (int v = 0; v < NF; v++) K.Kc[v] = K.divF[v] + K.Sexp[v] - K.Uold[v] * K.idtp;
+  K.tolFloor2 = 0.;
+  if (c.tolUlps > 0.) {
+    double s = 0.;
+#pragma unroll
+    for (int v = 0; v < 5; v++) s = fmax(s, fabs(K.Uold[v]) * K.idtp + fabs(K.divF[v]) + fabs(K.Sexp[v]));
+    const double f = c.tolUlps * 2.220446049250313e-16 * s;
+    K.tolFloor2 = f * f;
+  }
   if (COND || VISC) {
     const double* po = b.pold;
     ElemT<double, double> eo;
@@ -1422,7 +1430,7 @@ __global__ void __launch_bounds__(128) k_newton_fd_init(DevCfg c, int stage, Sta
     double l2 = l2sum<NF>(R);
     b.l2[z] = l2;
     b.l2[Z + z] = l2;
-    double tol = fmax(c.atol, c.rtol * c.rtol * l2);
+    double tol = newton_tol(c, l2, K);
     unconv = (l2 > tol) ? 1 : 0;
   }
   unconv = __syncthreads_count(unconv);
@@ -1504,7 +1512,7 @@ __global__ void __launch_bounds__(128) k_newton_fd_iter(DevCfg c, int stage, int
 #pragma unroll
       for (int v = 0; v < NF; v++) b.R[(long long)v * Z + z] = Rt[v];
       b.l2[z] = l2n;
-      double tol = fmax(c.atol, c.rtol * c.rtol * l2first);
+      double tol = newton_tol(c, l2first, K);
       unconv = (l2n > tol) ? 1 : 0;
     }
 #pragma unroll
@@ -1575,7 +1583,7 @@ __global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : kN
       if (!haveR || floored) zone_residual<COND, VISC, double, double>(P, K, G, c, R);
       const double l2 = l2sum<NF>(R);
       if (it == 0) l2first = l2;
-      if (l2 <= fmax(c.atol, c.rtol * c.rtol * l2first)) { conv = true; break; }
+      if (l2 <= newton_tol(c, l2first, K)) { conv = true; break; }
       T J[NF][NF];
       {
         // the Jacobian's geometry, converted where it is used rather than
@@ -1616,9 +1624,19 @@ __global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : kN
       }
     }
     if (!conv && it == c.maxIter) {
-      // final check of the last update (the state that is returned)
-      const double l2 = haveR ? l2sum<NF>(R) : -1.;
-      if (!(l2 >= 0. && l2 <= fmax(c.atol, c.rtol * c.rtol * l2first))) unconv = 1;
+      // final check of the last update (the state that is returned); a last
+      // step whose line search ran out was applied unevaluated: its residual
+      // is formed here, at the floored state the next iteration would see
+      if (!haveR) {
+        double Pf[NF];
+#pragma unroll
+        for (int v = 0; v < NF; v++) Pf[v] = P[v];
+        Pf[0] = fmax(Pf[0], c.rhoFloor);
+        Pf[1] = fmax(Pf[1], c.uFloor);
+        zone_residual<COND, VISC, double, double>(Pf, K, G, c, R);
+      }
+      const double l2 = l2sum<NF>(R);
+      if (!(l2 >= 0. && l2 <= newton_tol(c, l2first, K))) unconv = 1;
     }
     itsMax = it;
 #pragma unroll
@@ -1686,7 +1704,7 @@ GRIM_D bool list_init_zone(const DevCfg& c, int stage, const StageBufs& b, long 
 #pragma unroll
   for (int v = 0; v < NF; v++) b.R[(long long)v * Z + z] = R[v];
   b.l2[Z + z] = l2;
-  return l2 > fmax(c.atol, c.rtol * c.rtol * l2);
+  return l2 > newton_tol(c, l2, K);
 }
 
 // Launch it >= 1, one zone on the worklist: one Newton update from the
@@ -1749,7 +1767,7 @@ GRIM_D bool list_iter_zone(const DevCfg& c, int stage, int it, const StageBufs& 
   }
   if (!haveR || floored) zone_residual<COND, VISC, double, double>(P, K, G, c, Rt);
   const double l2n = l2sum<NF>(Rt);
-  const bool conv = l2n <= fmax(c.atol, c.rtol * c.rtol * l2first);
+  const bool conv = l2n <= newton_tol(c, l2first, K);
   if (!conv && last) atomicAdd(&b.st->finalUnconv[stage], 1ULL);
 #pragma unroll
   for (int v = 0; v < NF; v++) {

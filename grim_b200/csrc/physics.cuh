@@ -446,7 +446,17 @@ struct StageConst {
   // fast path, ideal MHD: R = U / dt' + Kc, Kc = divF + Sexp - Uold / dt'
   double idtp;
   double Kc[NF];
+  // square of the Newton test's rounding floor: (tolUlps eps max_v(|Uold_v|/dt'
+  // + |divF_v| + |Sexp_v|))^2 over the conserved rows, 0 when tolUlps = 0
+  double tolFloor2;
 };
+
+// the per-zone Newton test: converged once sum R^2 <= this (solve.cpp:36-41
+// with atol; rtol relative to the first residual; the rounding floor)
+template <class K_>
+GRIM_D double newton_tol(const DevCfg& c, double l2first, const K_& K) {
+  return fmax(fmax(c.atol, c.rtol * c.rtol * l2first), K.tolFloor2);
+}
 
 template <int COND, int VISC, class S, class R>
 GRIM_D void zone_residual(const S* P, const StageConst<5 + COND + VISC>& K, const ZoneGeo<R>& G,

@@ -207,6 +207,8 @@ static int make_devcfg(const grim_config& c, DevCfg& d) {
   d.CondClosure = c.ConductionClosureFactor; d.ViscClosure = c.ViscosityClosureFactor;
   d.theta = c.slopeLimTheta;
   d.atol = c.nonlinearsolve_atol; d.rtol = c.nonlinearsolve_rtol;
+  if (!(c.nonlinearsolve_ulps >= 0.)) { set_err("nonlinearsolve_ulps must be >= 0"); return GRIM_EINVAL; }
+  d.tolUlps = c.nonlinearsolve_ulps;
   d.jacEps = c.JacobianAssembleEpsilon; d.lsFloor = c.linesearchfloor;
   d.tau0 = c.closureTau0; d.tau1 = c.closureTau1;
   d.maxLF = c.MaxLorentzFactor; d.rhoFloorAmpl = c.RhoFloorAmpl; d.uFloorAmpl = c.UFloorAmpl;
@@ -220,6 +222,10 @@ static int make_devcfg(const grim_config& c, DevCfg& d) {
 }
 
 static bool use_exact(const grim_handle* h) { return h->cfg.newtonMode == GRIM_NEWTON_PARITY_FD64; }
+// the reference's FD-Jacobian Newton with global break, in either unit
+static bool is_fd(const grim_handle* h) {
+  return h->cfg.newtonMode == GRIM_NEWTON_PARITY_FD64 || h->cfg.newtonMode == GRIM_NEWTON_FD64_FAST;
+}
 
 // the three tensor maps (X1, X2, X3 box shapes) of a prim array of this
 // handle, or null when the array has none or direction dir's box does not fit
@@ -305,7 +311,7 @@ static long long g_launch_counter = 0;
 // primOld; the stand-alone stage pieces (grim_stage_setup and
 // grim_newton_solve) and the batch keep it in prim
 static bool step_guess_old(const grim_handle* h) {
-  return h->cfg.newtonMode != GRIM_NEWTON_PARITY_FD64 && h->cfg.perZoneConvergence != 2;
+  return !is_fd(h) && h->cfg.perZoneConvergence != 2;
 }
 static void enqueue_stencil(grim_handle* h, int stage, bool guessOld = false) {
   const DevCfg& c = h->dc;
@@ -332,8 +338,7 @@ static void enqueue_stencil(grim_handle* h, int stage, bool guessOld = false) {
 // count needs no pass of its own); the other Newton forms leave the count
 // to k_nan_flag
 static bool newton_counts_nan(const grim_handle* h) {
-  return h->cfg.problem == GRIM_PROBLEM_TORUS && h->cfg.newtonMode != GRIM_NEWTON_PARITY_FD64 &&
-         h->cfg.perZoneConvergence != 2;
+  return h->cfg.problem == GRIM_PROBLEM_TORUS && !is_fd(h) && h->cfg.perZoneConvergence != 2;
 }
 
 // returns whether the launch counts the NaN zones (countNan asked for it
@@ -353,6 +358,13 @@ static bool enqueue_newton(grim_handle* h, int stage, bool guessOld = false, boo
     g_launch_counter++;
     for (int it = 0; it < c.maxIter; it++) {
       grim::exact::newton_fd_iter(c, stage, it, b, s);
+      g_launch_counter++;
+    }
+  } else if (h->cfg.newtonMode == GRIM_NEWTON_FD64_FAST) {
+    grim::fast::newton_fd_init(c, stage, b, s);
+    g_launch_counter++;
+    for (int it = 0; it < c.maxIter; it++) {
+      grim::fast::newton_fd_iter(c, stage, it, b, s);
       g_launch_counter++;
     }
   } else if (h->cfg.perZoneConvergence == 2) {
@@ -1265,7 +1277,7 @@ int grim_problem_init(grim_handle* h) {
 }
 
 int grim_set_newton_mode(grim_handle* h, int mode, int perZone, double rtol) {
-  if (!h || mode < 0 || mode > 2 || perZone < 0 || perZone > 2) return GRIM_EINVAL;
+  if (!h || mode < 0 || mode > 3 || perZone < 0 || perZone > 2) return GRIM_EINVAL;
   h->cfg.newtonMode = mode;
   h->cfg.perZoneConvergence = perZone;
   h->cfg.nonlinearsolve_rtol = rtol;
@@ -1283,12 +1295,11 @@ int grim_get_stats(grim_handle* h, grim_stats* out) {
   memset(&s, 0, sizeof(s));
   for (int st = 0; st < 2; st++) {
     s.newtonIters[st] = (int)h->hst->itersDone[st];
-    if (h->cfg.newtonMode == GRIM_NEWTON_PARITY_FD64) {
-      // zones unconverged at the last counted iteration
-      unsigned long long u = 0;
-      for (int it = 0; it <= h->dc.maxIter && it < 16; it++)
-        if (h->hst->count[st][it]) u = h->hst->count[st][it];
-      s.unconverged[st] = (long long)u;
+    if (is_fd(h)) {
+      // zones unconverged after the last iteration performed (count[n] is
+      // the tally after n updates; the global break stops at a zero)
+      const int n = (int)std::min<unsigned long long>(h->hst->itersDone[st], 15ULL);
+      s.unconverged[st] = (long long)h->hst->count[st][n];
     } else {
       s.unconverged[st] = (long long)h->hst->finalUnconv[st];
     }

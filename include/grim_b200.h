@@ -53,7 +53,10 @@ enum { GRIM_PROBLEM_NONE = 0, GRIM_PROBLEM_TORUS = 1 };
 enum {
   GRIM_NEWTON_PARITY_FD64 = 0, /* reference method: FD Jacobian, FP64, global break */
   GRIM_NEWTON_TANGENT64   = 1, /* exact forward-tangent Jacobian, FP64 solve */
-  GRIM_NEWTON_MIXED32     = 2  /* FP32 tangent Jacobian + FP32 solve, FP64 residual */
+  GRIM_NEWTON_MIXED32     = 2, /* FP32 tangent Jacobian + FP32 solve, FP64 residual */
+  GRIM_NEWTON_FD64_FAST   = 3  /* the reference method (FD Jacobian, FP64 solve, line search,
+                                  global break) in the fast path's arithmetic and kernels: the
+                                  FD baseline the fast forms are timed against */
 };
 enum { GRIM_HOST = 0, GRIM_DEVICE = 1 };
 enum { GRIM_PRIM_OLD = 0, GRIM_PRIM = 1, GRIM_PRIM_HALF = 2 };
@@ -98,7 +101,12 @@ typedef struct grim_config {
   double BsqrOverRhoMax, BsqrOverUMax;
   double ObserveEveryDt;    /* > 0: record the torus observers whenever a step's
                                time crosses a multiple of it (problem.cpp:754) */
-  double reserved_d[5];
+  double nonlinearsolve_ulps; /* > 0: a zone also counts as converged once its
+                               residual is within this many ulps of the residual's
+                               largest term, max over the conserved rows of
+                               |U_old|/dt' + |divF| + |S| (the rounding floor of
+                               an FP64 residual); 0: the reference's test */
+  double reserved_d[4];
 } grim_config;
 
 typedef struct grim_handle grim_handle;

@@ -53,7 +53,8 @@ typedef struct orc_config {
   double MaxLorentzFactor, RhoFloorAmpl, UFloorAmpl, RhoFloorSlope, UFloorSlope;
   double BsqrOverRhoMax, BsqrOverUMax;
   double ObserveEveryDt;
-  double reserved_d[5];
+  double nonlinearsolve_ulps;  // product-only (rounding floor of the fast Newton test); the oracle ignores it
+  double reserved_d[4];
 } orc_config;
 
 typedef struct orc_handle orc_handle;

@@ -38,13 +38,14 @@ DOUBLE_FIELDS = [
     "linesearchfloor", "CourantFactor", "maxDtIncrement",
     "closureTau0", "closureTau1", "MaxLorentzFactor", "RhoFloorAmpl",
     "UFloorAmpl", "RhoFloorSlope", "UFloorSlope", "BsqrOverRhoMax", "BsqrOverUMax", "ObserveEveryDt",
+    "nonlinearsolve_ulps",
 ]
 
 
 class OrcConfig(ctypes.Structure):
     _fields_ = ([(n, ctypes.c_int) for n in INT_FIELDS] + [("reserved_i", ctypes.c_int * 4)]
                 + [(n, ctypes.c_double) for n in DOUBLE_FIELDS]
-                + [("reserved_d", ctypes.c_double * 5)])
+                + [("reserved_d", ctypes.c_double * 4)])
 
 
 PRIM_OLD, PRIM, PRIM_HALF = 0, 1, 2
