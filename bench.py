@@ -324,22 +324,10 @@ def _ncu_traffic(cfg):
 
 
 def batch_problems(seed=5, count=16):
-    """The ragged batch: 2D ideal linear-mode problems on periodic unit
-    squares, N from 64 to 512 (seeded), wavevector 2 pi (k1, k2) with
-    k1, k2 in 1..4, amplitude 1e-4 in every primitive; minmod, LLF,
-    flux-CT, relative Newton tolerance 1e-10."""
-    rng = np.random.default_rng(seed)
-    out = []
-    for _ in range(count):
-        n = int(rng.integers(4, 33)) * 16  # 64 .. 512
-        cfg = PR.fast_mode_config(N=n, nonlinearsolve_atol=ATOL, nonlinearsolve_rtol=RTOL, nonlinearsolve_ulps=ULPS, maxNonLinearIter=4)
-        X1, X2, _ = C.cell_centers(cfg)
-        k1, k2 = (int(x) for x in rng.integers(1, 5, 2))
-        base = [1.0, 2.0, 0.0, 0.0, 0.0, 0.1, 0.3, 0.0]
-        ph = rng.uniform(0, 2 * np.pi, 8)
-        P = np.stack([base[v] + 1e-4 * np.cos(2 * np.pi * (k1 * X1 + k2 * X2) + ph[v]) for v in range(8)])
-        out.append((cfg, P))
-    return out
+    """The ragged batch of the adjoint / batching workload at the bench's
+    Newton tolerances (grim_b200.problems.ragged_batch)."""
+    return PR.ragged_batch(seed=seed, count=count, nonlinearsolve_atol=ATOL, nonlinearsolve_rtol=RTOL,
+                           nonlinearsolve_ulps=ULPS, maxNonLinearIter=4)
 
 
 def run_batch(args, local_rank):

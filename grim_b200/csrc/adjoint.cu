@@ -20,8 +20,8 @@
 // local Jacobians taken with the forward-tangent scalar on the same
 // templated physics the kernels run.  Scope: ideal MHD, Minkowski, 2D,
 // periodic in both directions, dt held fixed over the run; the runtime
-// rejects anything else.  Accumulation into zones uses double atomics, so
-// gradients agree run to run to roundoff, not bit for bit.
+// rejects anything else.  Every accumulation is a gather in a fixed order
+// (no atomics), so a gradient is the same bits run to run.
 #include <cuda_runtime.h>
 
 #include "launch.h"
@@ -244,46 +244,42 @@ GRIM_D void riemann_flux(const DevCfg& c, int dir, const S* pl, const S* pr, S* 
   }
 }
 
-// Riemann + reconstruction transpose of the faces along dir: the face
-// between zones a = z - s and b = z takes Fbar (dof) and adds
-// (dF/dy)^T Fbar to the 5-point stencils of both zones in q
+// Riemann transpose of the faces along dir: the face between zones
+// a = z - s and b = z takes Fbar (dof) and forms the adjoints of its two
+// reconstructed states, gl = (dF/dpl)^T Fbar (pl: the right-face state of a)
+// and gr = (dF/dpr)^T Fbar (pr: the left-face state of b), into gface
+// (rows 0..7 gl, 8..15 gr; zero on the faces the stencil does not use)
 __global__ void k_faces_t(DevCfg c, int dir, const double* __restrict__ P, const double* __restrict__ Ft,
-                          double* __restrict__ q) {
+                          double* __restrict__ gface) {
   long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (z >= c.Z) return;
   int i, j, k;
   zijk(c, z, i, j, k);
   const int x = dir == 0 ? i : j;
   const int NT = dir == 0 ? c.N1T : c.N2T;
-  if (x < 3 || x > NT - 3) return;
   const long long Z = c.Z, s = stride_of(c, dir);
   double fb[8];
   bool any = false;
   for (int v = 0; v < 8; v++) {
-    fb[v] = Ft[((long long)dir * c.dof + v) * Z + z];
+    fb[v] = (x < 3 || x > NT - 3) ? 0. : Ft[((long long)dir * c.dof + v) * Z + z];
     any |= fb[v] != 0.;
   }
-  if (!any) return;
-  // face states and their 5-point derivatives
-  typedef Dual<double, 5> D5;
-  double pl[8], pr[8], dro[8][5], dlo[8][5];
+  if (!any) {
+    for (int v = 0; v < 16; v++) gface[(long long)v * Z + z] = 0.;
+    return;
+  }
+  // the face states
+  double pl[8], pr[8];
   for (int v = 0; v < 8; v++) {
     const double* a = P + (long long)v * Z;
-    D5 ya[5], yb[5];
-    for (int m = 0; m < 5; m++) {
-      ya[m] = D5::var(a[z - s + (m - 2) * s], m);
-      yb[m] = D5::var(a[z + (m - 2) * s], m);
-    }
-    D5 lo, ro, lo2, ro2;
-    recon_faces<D5>(c.reconstruction, c.theta, ya[0], ya[1], ya[2], ya[3], ya[4], lo, ro);
-    recon_faces<D5>(c.reconstruction, c.theta, yb[0], yb[1], yb[2], yb[3], yb[4], lo2, ro2);
-    pl[v] = ro.v;
-    pr[v] = lo2.v;
-    for (int m = 0; m < 5; m++) { dro[v][m] = ro.d[m]; dlo[v][m] = lo2.d[m]; }
+    double lo, ro, lo2, ro2;
+    recon_faces<double>(c.reconstruction, c.theta, a[z - 3 * s], a[z - 2 * s], a[z - s], a[z], a[z + s], lo, ro);
+    recon_faces<double>(c.reconstruction, c.theta, a[z - 2 * s], a[z - s], a[z], a[z + s], a[z + 2 * s], lo2, ro2);
+    pl[v] = ro;
+    pr[v] = lo2;
   }
   // dF/dpl and dF/dpr, 8 tangent lanes each
   typedef Dual<double, 8> D8;
-  double gl[8], gr[8];
   for (int side = 0; side < 2; side++) {
     D8 L[8], R[8], F[8];
     for (int v = 0; v < 8; v++) {
@@ -291,20 +287,49 @@ __global__ void k_faces_t(DevCfg c, int dir, const double* __restrict__ P, const
       R[v] = side == 1 ? D8::var(pr[v], v) : D8(pr[v]);
     }
     riemann_flux<D8>(c, dir, L, R, F);
-    double* out = side == 0 ? gl : gr;
     for (int k2 = 0; k2 < 8; k2++) {
       double acc = 0.;
       for (int r = 0; r < 8; r++) acc += fb[r] * F[r].d[k2];
-      out[k2] = acc;
+      gface[(long long)(side * 8 + k2) * Z + z] = acc;
     }
   }
-  // row index of prim variable v: fluid 0..4, B at c.B1 (= 5 for ideal)
+}
+
+// Reconstruction transpose along dir, as a gather: zone x collects, in a
+// fixed order, the adjoints of the face states of the five zones whose
+// stencils hold it (y = x - 2 .. x + 2 along dir): the right-face state of y
+// (the left state of face y + 1, adjoint gl there) and its left-face state
+// (the right state of face y, adjoint gr), each times its derivative with
+// respect to x from a forward-tangent pass of y's reconstruction.  One
+// thread per zone and direction, so the sums are the same run to run.
+__global__ void k_recon_t(DevCfg c, int dir, const double* __restrict__ P, const double* __restrict__ gface,
+                          double* __restrict__ q) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  const int x = dir == 0 ? i : j;
+  const int NT = dir == 0 ? c.N1T : c.N2T;
+  const long long Z = c.Z, s = stride_of(c, dir);
+  typedef Dual<double, 5> D5;
   for (int v = 0; v < 8; v++) {
-    double* col = q + (long long)v * Z;
-    for (int m = 0; m < 5; m++) {
-      atomicAdd(col + z - s + (m - 2) * s, gl[v] * dro[v][m]);
-      atomicAdd(col + z + (m - 2) * s, gr[v] * dlo[v][m]);
+    const double* a = P + (long long)v * Z;
+    double acc = 0.;
+    for (int m = 4; m >= 0; m--) {
+      // x is point m of the stencil of y = x + 2 - m
+      const int y = x + 2 - m;
+      if (y < 2 || y > NT - 3) continue;
+      const long long zy = z + (long long)(2 - m) * s;
+      const double gl = (y + 1 <= NT - 1) ? gface[(long long)v * Z + zy + s] : 0.;
+      const double gr = gface[(long long)(8 + v) * Z + zy];
+      if (gl == 0. && gr == 0.) continue;
+      D5 yb[5];
+      for (int mm = 0; mm < 5; mm++) yb[mm] = D5::var(a[zy + (mm - 2) * s], mm);
+      D5 lo, ro;
+      recon_faces<D5>(c.reconstruction, c.theta, yb[0], yb[1], yb[2], yb[3], yb[4], lo, ro);
+      acc += gl * ro.d[m] + gr * lo.d[m];
     }
+    q[(long long)v * Z + z] += acc;
   }
 }
 
@@ -349,14 +374,17 @@ void adjoint_zero_ghosts(const DevCfg& c, double* a, cudaStream_t s) {
 }
 
 void adjoint_stencil_t(const DevCfg& c, const double* P, const double* g, double* Ft, double* ebar, double* q,
-                       double* out, cudaStream_t s) {
+                       double* gface, double* out, cudaStream_t s) {
   using namespace adj;
   const size_t bZ = (size_t)c.Z * sizeof(double);
   k_div_t<<<nblk(c.Z, 128), 128, 0, s>>>(c, g, Ft);
   k_ct_t_emf<<<nblk(c.Z, 256), 256, 0, s>>>(c, Ft, ebar);
   k_ct_t_raw<<<nblk(c.Z, 256), 256, 0, s>>>(c, ebar, Ft);
   cudaMemsetAsync(q, 0, (size_t)c.dof * bZ, s);
-  for (int d = 0; d < 2; d++) k_faces_t<<<nblk(c.Z, 64), 64, 0, s>>>(c, d, P, Ft, q);
+  for (int d = 0; d < 2; d++) {
+    k_faces_t<<<nblk(c.Z, 64), 64, 0, s>>>(c, d, P, Ft, gface);
+    k_recon_t<<<nblk(c.Z, 64), 64, 0, s>>>(c, d, P, gface, q);
+  }
   k_fold<<<nblk(c.Zint, 128), 128, 0, s>>>(c, q, out);
 }
 
@@ -365,10 +393,10 @@ void adjoint_step(const DevCfg& c, double dt, const double* P0, const double* Ph
   using namespace adj;
   // full stage at P1
   k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, P1, dt, lam, w.g, w.ubar, w.bacc, 0);
-  adjoint_stencil_t(c, Ph, w.g, w.Ft, w.ebar, w.q, w.lamh, s);
+  adjoint_stencil_t(c, Ph, w.g, w.Ft, w.ebar, w.q, w.gface, w.lamh, s);
   // half stage at Ph
   k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, Ph, 0.5 * dt, w.lamh, w.g, w.ubar, w.bacc, 1);
-  adjoint_stencil_t(c, P0, w.g, w.Ft, w.ebar, w.q, lam, s);
+  adjoint_stencil_t(c, P0, w.g, w.Ft, w.ebar, w.q, w.gface, lam, s);
   k_cons<<<nblk(c.Zint, 128), 128, 0, s>>>(c, P0, w.ubar, w.bacc, lam);
 }
 

@@ -56,6 +56,7 @@ struct AdjointBufs {
   double* Ft;    // 2 x dof x Z: face-flux adjoints per direction
   double* ebar;  // Z: corner EMF adjoints
   double* q;     // stencil adjoint before the periodic fold
+  double* gface; // 2 x dof x Z: adjoints of the two reconstructed states of the faces along one direction
   double* lamh;  // dL/dPh
   double* ubar;  // nf x Z: dL/dU(P0)
   double* bacc;  // 3 x Z: dL/dB0 through the induction
@@ -65,7 +66,7 @@ void adjoint_step(const DevCfg& c, double dt, const double* P0, const double* Ph
                   const AdjointBufs& w, cudaStream_t s);
 void adjoint_zero_ghosts(const DevCfg& c, double* a, cudaStream_t s);
 void adjoint_stencil_t(const DevCfg& c, const double* P, const double* g, double* Ft, double* ebar, double* q,
-                       double* out, cudaStream_t s);
+                       double* gface, double* out, cudaStream_t s);
 }  // namespace grim
 
 namespace grim {

@@ -1230,7 +1230,23 @@ int grim_get_geometry(grim_handle* h, int location, double* out, double* gamma, 
   if (!h || location < 0 || location > 4) return GRIM_EINVAL;
   CK(cudaSetDevice(h->device));
   const DevCfg& c = h->dc;
-  if (h->cfg.metric == GRIM_MINKOWSKI) { set_err("Minkowski geometry is compile-time"); return GRIM_ENOTSUP; }
+  if (h->cfg.metric == GRIM_MINKOWSKI) {
+    // the stepping kernels take Minkowski as a compile-time constant and
+    // store nothing; the geometry kernel's Minkowski branch evaluates the
+    // same metric (and zero connection) for the caller, in a scratch plane
+    double* tmp = nullptr;
+    const size_t words = (size_t)(39 + 64) * (size_t)c.GZ;  // 39 words per location, 64 Christoffels
+    CK(cudaMallocAsync((void**)&tmp, words * sizeof(double), h->stream));
+    grim::launch_geometry(c, h->cfg, location, tmp, location == GRIM_CENTER ? tmp + (size_t)39 * c.GZ : nullptr,
+                          h->stream);
+    int rc = GRIM_OK;
+    if (out) rc = plane_to_full(h, out, tmp, 34, memKind);
+    if (!rc && xc) rc = plane_to_full(h, xc, tmp + 34 * c.GZ, 5, memKind);
+    if (!rc && gamma && location == GRIM_CENTER) rc = plane_to_full(h, gamma, tmp + (size_t)39 * c.GZ, 64, memKind);
+    cudaFreeAsync(tmp, h->stream);
+    CK(cudaStreamSynchronize(h->stream));
+    return rc;
+  }
   if (out) {
     int rc = plane_to_full(h, out, h->geo[location], 34, memKind);
     if (rc) return rc;
@@ -1443,7 +1459,7 @@ static int adjoint_scope(grim_handle* h) {
 static int adjoint_work(grim_handle* h, AdjointBufs& w, double*& lam) {
   const DevCfg& c = h->dc;
   if (!h->adjWork) {
-    const size_t words = (size_t)c.Z * (c.dof * 6 + 1 + c.nf + 3);
+    const size_t words = (size_t)c.Z * (c.dof * 8 + 1 + c.nf + 3);
     if (cudaMalloc(&h->adjWork, words * sizeof(double)) != cudaSuccess) {
       set_err("adjoint: work allocation failed");
       return GRIM_ENOMEM;
@@ -1454,6 +1470,7 @@ static int adjoint_work(grim_handle* h, AdjointBufs& w, double*& lam) {
   w.Ft = wp; wp += (size_t)2 * c.dof * c.Z;
   w.ebar = wp; wp += (size_t)c.Z;
   w.q = wp; wp += (size_t)c.dof * c.Z;
+  w.gface = wp; wp += (size_t)2 * c.dof * c.Z;
   w.lamh = wp; wp += (size_t)c.dof * c.Z;
   w.ubar = wp; wp += (size_t)c.nf * c.Z;
   w.bacc = wp; wp += (size_t)3 * c.Z;
@@ -1476,7 +1493,7 @@ int grim_adjoint_stencil(grim_handle* h, const double* prim, const double* gbar,
   CK(cudaMemcpyAsync(h->scratch, prim, bytes, in, h->stream));
   CK(cudaMemcpyAsync(w.g, gbar, bytes, in, h->stream));
   CK(cudaMemsetAsync(lam, 0, bytes, h->stream));
-  grim::adjoint_stencil_t(c, h->scratch, w.g, w.Ft, w.ebar, w.q, lam, h->stream);
+  grim::adjoint_stencil_t(c, h->scratch, w.g, w.Ft, w.ebar, w.q, w.gface, lam, h->stream);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, lam, bytes, memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                      h->stream));

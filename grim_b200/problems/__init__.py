@@ -16,6 +16,8 @@ Workloads:
   * ``emhd_stratified`` -- 2D EMHD 256^2, stratified density, tau(y) profile,
     MP5 reconstruction.
   * ``torus``         -- 3D Fishbone-Moncrief torus in MKS (torus/*).
+  * ``ragged_batch``  -- 16 independent 2D ideal linear-mode problems of
+    64^2 .. 512^2 (seeded), the batching and adjoint workload.
 """
 import math
 
@@ -246,3 +248,31 @@ def emhd_stratified_prims(cfg, seed=3, H=0.5, amplitude=1e-3):
     P[idx["B1"]] = EMHD_B * math.cos(th)
     P[idx["B2"]] = EMHD_B * math.sin(th)
     return P
+
+
+# --------------------------------------------------------------------------
+# ragged batch: independent 2D ideal linear-mode problems of different sizes
+# --------------------------------------------------------------------------
+LM_BACKGROUND_IDEAL = (1.0, 2.0, 0.0, 0.0, 0.0, 0.1, 0.3, 0.0)
+
+
+def ragged_batch(seed=5, count=16, amplitude=1e-4, **kw):
+    """[(config, prims)] of ``count`` problems: 2D ideal MHD, Minkowski,
+    periodic unit squares, N = 16 U{4..32} (64 .. 512, seeded PCG64), a
+    wave 2 pi (k1 x + k2 y) with k1, k2 in U{1..4} and ``amplitude`` (1e-4)
+    in every primitive (random phase per variable) on the background
+    rho = 1, u = 2, B = (0.1, 0.3, 0); minmod, LLF, flux-CT
+    (fast_mode_config); ``kw`` sets further config fields (Newton
+    tolerances, the scheme)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(rng.integers(4, 33)) * 16
+        cfg = fast_mode_config(N=n, **kw)
+        X1, X2, _ = C.cell_centers(cfg)
+        k1, k2 = (int(x) for x in rng.integers(1, 5, 2))
+        ph = rng.uniform(0, 2 * math.pi, 8)
+        P = np.stack([LM_BACKGROUND_IDEAL[v] + amplitude * np.cos(2 * math.pi * (k1 * X1 + k2 * X2) + ph[v])
+                      for v in range(8)])
+        out.append((cfg, P))
+    return out

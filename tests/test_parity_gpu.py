@@ -177,12 +177,14 @@ def test_timestep_parity_emhd_stratified_mp5():
     assert scaled_err(g, o) <= 1e-12
 
 
-def test_linear_mode_second_order_on_gpu():
+@pytest.mark.parametrize("recon", [C.MINMOD, C.MP5])
+def test_linear_mode_second_order_on_gpu(recon):
     """The reference's known answer: the damped EMHD eigenmode converges at
-    2nd order (Linear modes.ipynb, cells 1-2)."""
+    2nd order (Linear modes.ipynb, cells 1-2); with MP5 (no reference
+    counterpart, pinned by its order) on the asymptotic pairs 32-64-128."""
     errs = []
-    for N in (16, 32, 64):
-        cfg = PR.linear_modes_config(N=N)
+    for N in ((16, 32, 64) if recon == C.MINMOD else (32, 64, 128)):
+        cfg = PR.linear_modes_config(N=N, reconstruction=recon)
         from grim_b200.timestepper import timeStepper
         ts = timeStepper(cfg)
         ts.primOld.setVars(PR.linear_modes_prims(cfg))
@@ -195,6 +197,8 @@ def test_linear_mode_second_order_on_gpu():
         errs.append(e)
     o1, o2 = np.log2(errs[0] / errs[1]), np.log2(errs[1] / errs[2])
     assert o1 > 1.5 and o2 > 1.7, (errs, o1, o2)
+    if recon == C.MP5:
+        assert o2 > 1.8, (errs, o2)
 
 
 @pytest.mark.parametrize("mode", [C.NEWTON_PARITY_FD64, C.NEWTON_MIXED32])
