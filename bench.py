@@ -38,7 +38,8 @@ RTOL = 1e-10
 # of the residual for these workloads (|U|/dt' ~ 1e3, eps ~ 1e-16)
 ATOL = 1e-24
 # rounding floor of the zone test, in ulps of the residual's largest term
-# (max over the conserved rows of |U_old|/dt' + |divF| + |S|): relative 1e-10
+# (|U|/dt' at the solution: max over the conserved rows of
+# |divF + S - U_old/dt'|): relative 1e-10
 # of the first residual lies below the rounding of an FP64 residual in about
 # 0.1% of the torus zones (their first residual is 1e-6..1e-9 of |U|/dt'),
 # which then never test converged in any Newton form

@@ -1265,6 +1265,9 @@ GRIM_D void load_stage_const(StageConst<5 + COND + VISC>& K, const DevCfg& c, in
   constexpr int NF = 5 + COND + VISC;
   const long long Z = c.Z;
   const bool needS = (c.metric != GRIM_MINKOWSKI) || COND || VISC;
+  const double dt = b.st->dt;
+  K.dtp = (stage == GRIM_HALF_STEP) ? dt / 2. : dt;
+  K.idtp = 1. / K.dtp;
 #pragma unroll
   for (int v = 0; v < NF; v++) {
     K.Uold[v] = b.consOld[(long long)v * Z + z];
@@ -1272,17 +1275,16 @@ GRIM_D void load_stage_const(StageConst<5 + COND + VISC>& K, const DevCfg& c, in
     K.Sexp[v] = needS ? b.Sexp[(long long)v * Z + z] : 0.;
   }
 #pragma unroll
-  for (int v = 0; v < 3; v++) K.B[v] = b.prim[(long long)(c.B1 + v) * Z + z];
-  const double dt = b.st->dt;
-  K.dtp = (stage == GRIM_HALF_STEP) ? dt / 2. : dt;
-  K.idtp = 1. / K.dtp;
-#pragma unroll
   for (int v = 0; v < NF; v++) K.Kc[v] = K.divF[v] + K.Sexp[v] - K.Uold[v] * K.idtp;
+#pragma unroll
+  for (int v = 0; v < 3; v++) K.B[v] = b.prim[(long long)(c.B1 + v) * Z + z];
+  // the rounding floor: the residual's largest term is U / dt', which at
+  // the solution is -Kc (R = U / dt' + Kc = 0), over the conserved rows
   K.tolFloor2 = 0.;
   if (c.tolUlps > 0.) {
     double s = 0.;
 #pragma unroll
-    for (int v = 0; v < 5; v++) s = fmax(s, fabs(K.Uold[v]) * K.idtp + fabs(K.divF[v]) + fabs(K.Sexp[v]));
+    for (int v = 0; v < 5; v++) s = fmax(s, fabs(K.Kc[v]));
     const double f = c.tolUlps * 2.220446049250313e-16 * s;
     K.tolFloor2 = f * f;
   }

@@ -446,8 +446,9 @@ struct StageConst {
   // fast path, ideal MHD: R = U / dt' + Kc, Kc = divF + Sexp - Uold / dt'
   double idtp;
   double Kc[NF];
-  // square of the Newton test's rounding floor: (tolUlps eps max_v(|Uold_v|/dt'
-  // + |divF_v| + |Sexp_v|))^2 over the conserved rows, 0 when tolUlps = 0
+  // square of the Newton test's rounding floor: (tolUlps eps max_v |Kc_v|)^2
+  // over the conserved rows (|Kc_v| = |U_v| / dt' at the solution, the
+  // residual's largest term), 0 when tolUlps = 0
   double tolFloor2;
 };
 

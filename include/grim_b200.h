@@ -103,9 +103,10 @@ typedef struct grim_config {
                                time crosses a multiple of it (problem.cpp:754) */
   double nonlinearsolve_ulps; /* > 0: a zone also counts as converged once its
                                residual is within this many ulps of the residual's
-                               largest term, max over the conserved rows of
-                               |U_old|/dt' + |divF| + |S| (the rounding floor of
-                               an FP64 residual); 0: the reference's test */
+                               largest term, |U|/dt' at the solution, i.e. max over
+                               the conserved rows of |divF + S - U_old/dt'| (the
+                               rounding floor of an FP64 residual); 0: the
+                               reference's test */
   double reserved_d[4];
 } grim_config;
 
