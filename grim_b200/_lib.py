@@ -74,6 +74,7 @@ def lib():
         "grim_set_time": [vp, d, d],
         "grim_compute_dt": [vp],
         "grim_apply_boundaries": [vp, i],
+        "grim_communicate": [vp, i],
         "grim_compute_div_fluxes": [vp, vp, vp, vp, vp, i],
         "grim_reconstruct": [vp, vp, i, vp, vp, i],
         "grim_compute_divb": [vp, vp, vp, i],

@@ -903,6 +903,16 @@ int grim_apply_boundaries(grim_handle* h, int which) {
   return GRIM_OK;
 }
 
+int grim_communicate(grim_handle* h, int which) {
+  if (!h) return GRIM_EINVAL;
+  double* p = pick(h, which);
+  if (!p) return GRIM_EINVAL;
+  CK(cudaSetDevice(h->device));
+  KNS_CALL(h, communicate, h->dc, p, h->dc.dof, h->stream);
+  CK(cudaGetLastError());
+  return GRIM_OK;
+}
+
 // copy a caller array (host or device) of nv x Z words into a device buffer
 static int stage_in(grim_handle* h, double* dst, const double* src, int nv, int memKind) {
   CK(cudaMemcpyAsync(dst, src, (size_t)nv * h->bytesZ,

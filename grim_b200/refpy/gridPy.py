@@ -23,6 +23,9 @@ class gridPy:
                  periodicBoundariesX2=False, periodicBoundariesX3=False):
         self._N = (int(N1), int(N2), int(N3))
         self._dim, self._numVars, self._numGhost = int(dim), int(numVars), int(numGhost)
+        if (self._dim < 2 and self._N[1] != 1) or (self._dim < 3 and self._N[2] != 1):
+            raise ValueError("the library holds one zone along each inactive direction (dim %d: N2, N3 = %d, %d)"
+                             % (self._dim, self._N[1], self._N[2]))
         self.periodic = (bool(periodicBoundariesX1), bool(periodicBoundariesX2), bool(periodicBoundariesX3))
         self._ghost, self._total = _totals(*self._N, self._dim, self._numGhost)
         self._vars = np.zeros(self.shape)
@@ -59,6 +62,33 @@ class gridPy:
         if list(a.shape) != self.shape:
             raise ValueError("setVars: shape %s, expected %s" % (list(a.shape), self.shape))
         self._vars = a.copy()
+
+    def communicate(self):
+        """grid::communicate (grid.cpp:306-360) by the library's kernel: the
+        ghosts of the periodic directions become images of the interior,
+        the other ghosts zero; the variables pass through a library state
+        grid eight at a time."""
+        from .. import _lib
+        ts = self._handle()
+        v = self._vars
+        for v0 in range(0, self._numVars, ts.dof):
+            n = min(ts.dof, self._numVars - v0)
+            block = np.zeros([ts.dof] + self.shape[1:])
+            block[:n] = v[v0:v0 + n]
+            ts.primOld.setVars(block)
+            _lib.check(_lib.lib().grim_communicate(ts._h, _lib.PRIM_OLD), "communicate")
+            v[v0:v0 + n] = ts.primOld.getVars()[:n]
+
+    def _handle(self):
+        if getattr(self, "_ts", None) is None:
+            from ..timestepper import timeStepper
+            side = [C.PERIODIC if p else C.OUTFLOW for p in self.periodic]
+            cfg = C.make_config(N1=self._N[0], N2=self._N[1], N3=self._N[2], dim=self._dim,
+                                numGhost=self._numGhost, boundaryLeft=side[0], boundaryRight=side[0],
+                                boundaryBottom=side[1], boundaryTop=side[1], boundaryBack=side[2],
+                                boundaryFront=side[2])
+            self._ts = timeStepper(cfg)
+        return self._ts
 
 
 class coordinatesGridPy:

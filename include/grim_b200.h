@@ -229,6 +229,10 @@ int grim_compute_dt(grim_handle* h);
 /* ghost fill of one state buffer: periodic wrap + outflow/mirror
  * (boundary.cpp:5-241, grid.cpp:306-315) */
 int grim_apply_boundaries(grim_handle* h, int which);
+/* grid::communicate alone (grid.cpp:306-360): the periodic directions'
+ * ghosts become images of the interior, the physical ghosts zero (the
+ * never-written part of PETSc's local vector) */
+int grim_communicate(grim_handle* h, int which);
 /* computeDivOfFluxes (fvmfluxes.cpp:3-183) incl. fluxCT/computeEMF
  * (constrainedtransport.cpp:3-83) on a caller's prim array; outputs may be
  * NULL.  divF: dof x Z, fluxes: 3 x dof x Z, emf: 3 x Z (X1, X2, X3). */

@@ -1,6 +1,7 @@
-"""The reference's own tests of its grid boundaries and geometry
-(src/boundary/test_boundary.py:56-243, src/geometry/test_geometry.py:44-420),
-run against libgrim_b200.so through the reference-named modules gridPy,
+"""The reference's own tests of its grid boundaries, geometry and periodic
+communication (src/boundary/test_boundary.py:56-243,
+src/geometry/test_geometry.py:44-420, src/grid/test_mpi.py:1-200), run
+against libgrim_b200.so through the reference-named modules gridPy,
 geometryPy and boundaryPy (grim_b200/refpy).  Each test below restates one
 of the reference's checks with its own tolerance; the grids are the
 reference tests' set-up (unit cube, 3 ghost zones, outflow everywhere,
@@ -198,3 +199,52 @@ def test_modified_kerr_schild_connection(mks):
     for idx in np.ndindex(4, 4, 4):
         np.testing.assert_allclose(geom.gammaUpDownDown[idx], exact[idx], rtol=1e-7, atol=1e-7,
                                    err_msg="gammaUpDownDown%s" % (list(idx),))
+
+
+# ---- periodic communication (grid/test_mpi.py) --------------------------------
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_periodic_communicate(dim):
+    """grid/test_mpi.py:1-200: sin(2 pi X1) sin(2 pi X2) sin(2 pi X3) on the
+    interior of a grid periodic in every direction, gridPy.communicate, then
+    central differences over the whole array: at the first and last
+    interior planes of each direction (where the stencil reaches into the
+    ghosts) the mean error of the derivative equals the bulk's within the
+    reference's 0.1 (a missing or wrong exchange makes it ~0.6).  Here the
+    ghosts are also checked to be exact periodic images of the interior."""
+    N = 32
+    N2, N3 = (N if dim >= 2 else 1), (N if dim == 3 else 1)
+    prim = gridPy.gridPy(N, N2, N3, dim, 1, NUM_GHOST, True, True, True)
+    X = gridPy.coordinatesGridPy(N, N2, N3, dim, NUM_GHOST, 0., 1., 0., 1., 0., 1.)
+    X1, X2, X3 = X.getCoords(gridPy.CENTER)
+    g = (prim.numGhostX1, prim.numGhostX2, prim.numGhostX3)
+    bulk = tuple(slice(gg, -gg) if gg else slice(None) for gg in reversed(g))  # (k, j, i)
+    # sin(2 pi X) in each active direction (an inactive one holds one zone)
+    S = [np.sin(2 * np.pi * X1), np.sin(2 * np.pi * X2) if dim >= 2 else 1., np.sin(2 * np.pi * X3) if dim == 3 else 1.]
+    D = [2 * np.pi * np.cos(2 * np.pi * X1), 2 * np.pi * np.cos(2 * np.pi * X2), 2 * np.pi * np.cos(2 * np.pi * X3)]
+    f = S[0] * S[1] * S[2]
+    v = prim.getVars()
+    v[(0,) + bulk] = f[bulk]
+    prim.setVars(v)
+    prim.communicate()
+    v = prim.getVars()[0]
+    # the ghosts hold the periodic images
+    idx = [np.arange(n) for n in v.shape]
+    for ax, gg in zip((2, 1, 0), g):
+        if gg:
+            n = v.shape[ax] - 2 * gg
+            idx[ax] = (idx[ax] - gg) % n + gg
+    np.testing.assert_array_equal(v, v[np.ix_(*idx)])
+    # the derivatives at the interior's edge planes against the bulk
+    dX = (1. / N, 1. / N2, 1. / N3)
+    exact = [D[0] * S[1] * S[2], S[0] * D[1] * S[2], S[0] * S[1] * D[2]]
+    for d in range(dim):
+        ax = 2 - d
+        num = np.gradient(v, dX[d], axis=ax)
+        err = np.abs(num - exact[d])[bulk]
+        sl = [slice(None)] * 3
+        sl[ax] = 0
+        first = float(np.mean(err[tuple(sl)]))
+        sl[ax] = -1
+        last = float(np.mean(err[tuple(sl)]))
+        mid = float(np.mean(err))
+        assert abs(first - mid) < 0.1 and abs(last - mid) < 0.1, (d, first, last, mid)
