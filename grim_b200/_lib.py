@@ -70,6 +70,7 @@ def lib():
         "grim_get_prims": [vp, i, vp, i],
         "grim_time_step": [vp, P(i), P(i)],
         "grim_time_steps": [vp, i],
+        "grim_time_steps_host": [vp, i, vp, vp],
         "grim_get_time": [vp, P(d), P(d)],
         "grim_set_time": [vp, d, d],
         "grim_compute_dt": [vp],

@@ -103,6 +103,13 @@ struct grim_handle {
   std::vector<double*> adjCkpt;
   std::vector<double*> adjSeg;  // 2 * every + 1 states: S[0..every], H[0..every-1]
   double* adjWork = nullptr;    // AdjointBufs storage
+  // grim_time_steps_host: two staging buffers each way (dof x Z), an upload
+  // and a download stream so both directions of PCIe and the step overlap
+  double* ioIn[2] = {nullptr, nullptr};
+  double* ioOut[2] = {nullptr, nullptr};
+  cudaStream_t ioUp = nullptr, ioDown = nullptr;
+  cudaEvent_t ioEv[8];  // [0,2) upload done, [2,4) input consumed, [4,6) output staged, [6,8) download done
+  bool ioReady = false;
   bool profOn = false;
   std::vector<cudaEvent_t> profEv;
   std::vector<int> profGroup;
@@ -153,6 +160,16 @@ static void free_all(grim_handle* h) {
   for (cudaEvent_t e : h->profEv) cudaEventDestroy(e);
   h->profEv.clear();
   h->profGroup.clear();
+  for (int i = 0; i < 2; i++) {
+    if (h->ioIn[i]) { cudaFree(h->ioIn[i]); h->ioIn[i] = nullptr; }
+    if (h->ioOut[i]) { cudaFree(h->ioOut[i]); h->ioOut[i] = nullptr; }
+  }
+  if (h->ioReady) {
+    for (int i = 0; i < 8; i++) cudaEventDestroy(h->ioEv[i]);
+    cudaStreamDestroy(h->ioUp);
+    cudaStreamDestroy(h->ioDown);
+    h->ioReady = false;
+  }
 }
 
 static int make_devcfg(const grim_config& c, DevCfg& d) {
@@ -860,6 +877,72 @@ int grim_time_step(grim_handle* h, int* numReads, int* numWrites) {
 int grim_time_steps(grim_handle* h, int nsteps) {
   if (!h || nsteps < 0) return GRIM_EINVAL;
   return run_steps(h, nsteps);
+}
+
+// nsteps of (primOld <- hostIn[k]; timeStep; hostOut[k] <- primOld) with the
+// copies of one step overlapping the other steps' work: uploads on one
+// stream, downloads on another, each through two device staging buffers,
+// the step on the handle's stream between a device copy in and one out.
+int grim_time_steps_host(grim_handle* h, int nsteps, const double* const* hostIn, double* const* hostOut) {
+  if (!h || nsteps < 0) { set_err("grim_time_steps_host: bad argument"); return GRIM_EINVAL; }
+  {
+    const int rc = take_async_error(h);
+    if (rc) return rc;
+  }
+  CK(cudaSetDevice(h->device));
+  const size_t bytes = (size_t)h->dc.dof * h->bytesZ;
+  if (!h->ioReady) {
+    bool ok = true;
+    for (int i = 0; i < 2; i++) {
+      if (!h->ioIn[i]) ok = ok && cudaMalloc(&h->ioIn[i], bytes) == cudaSuccess;
+      if (!h->ioOut[i]) ok = ok && cudaMalloc(&h->ioOut[i], bytes) == cudaSuccess;
+    }
+    if (!ok) {
+      cudaGetLastError();
+      for (int i = 0; i < 2; i++) {
+        cudaFree(h->ioIn[i]);
+        cudaFree(h->ioOut[i]);
+        h->ioIn[i] = h->ioOut[i] = nullptr;
+      }
+      set_err("grim_time_steps_host: staging allocation failed (4 x %zu MB)", bytes >> 20);
+      return GRIM_ENOMEM;
+    }
+    CK(cudaStreamCreateWithFlags(&h->ioUp, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&h->ioDown, cudaStreamNonBlocking));
+    for (int i = 0; i < 8; i++) CK(cudaEventCreateWithFlags(&h->ioEv[i], cudaEventDisableTiming));
+    h->ioReady = true;
+  }
+  cudaEvent_t* upDone = h->ioEv;
+  cudaEvent_t* inFree = h->ioEv + 2;
+  cudaEvent_t* outStaged = h->ioEv + 4;
+  cudaEvent_t* outFree = h->ioEv + 6;
+  for (int k = 0; k < nsteps; k++) {
+    const int s = k & 1;
+    if (hostIn && hostIn[k]) {
+      // staging buffer s is free once the step of k - 2 has copied it in
+      CK(cudaStreamWaitEvent(h->ioUp, inFree[s], 0));
+      CK(cudaMemcpyAsync(h->ioIn[s], hostIn[k], bytes, cudaMemcpyHostToDevice, h->ioUp));
+      CK(cudaEventRecord(upDone[s], h->ioUp));
+      CK(cudaStreamWaitEvent(h->stream, upDone[s], 0));
+      CK(cudaMemcpyAsync(h->primOld, h->ioIn[s], bytes, cudaMemcpyDeviceToDevice, h->stream));
+      CK(cudaEventRecord(inFree[s], h->stream));
+    }
+    int rc = run_steps(h, 1);
+    if (rc) return rc;
+    if (hostOut && hostOut[k]) {
+      // staging buffer s is free once the download of k - 2 has finished
+      CK(cudaStreamWaitEvent(h->stream, outFree[s], 0));
+      CK(cudaMemcpyAsync(h->ioOut[s], h->primOld, bytes, cudaMemcpyDeviceToDevice, h->stream));
+      CK(cudaEventRecord(outStaged[s], h->stream));
+      CK(cudaStreamWaitEvent(h->ioDown, outStaged[s], 0));
+      CK(cudaMemcpyAsync(hostOut[k], h->ioOut[s], bytes, cudaMemcpyDeviceToHost, h->ioDown));
+      CK(cudaEventRecord(outFree[s], h->ioDown));
+    }
+  }
+  CK(cudaStreamSynchronize(h->ioUp));
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaStreamSynchronize(h->ioDown));
+  return take_async_error(h);
 }
 
 int grim_get_time(grim_handle* h, double* t, double* dt) {

@@ -150,6 +150,16 @@ int grim_problem_init(grim_handle* h);
  *      numWrites report the algorithmic words per zone, may be NULL ------ */
 int grim_time_step(grim_handle* h, int* numReads, int* numWrites);
 int grim_time_steps(grim_handle* h, int nsteps);
+/* nsteps of: primOld <- hostIn[k] (when hostIn and hostIn[k] are not NULL;
+ * the whole [var][k][j][i] array with ghosts, as grim_set_prims), one
+ * timeStep, hostOut[k] <- primOld (when hostOut and hostOut[k] are not
+ * NULL).  The same results as those calls made one after another; here the
+ * upload of step k + 1, the step k and the download of step k - 1 run at
+ * once (two device staging buffers each way, an upload and a download
+ * stream).  Host buffers must be pinned (cudaHostAlloc / cudaHostRegister)
+ * for the copies to overlap.  Returns when every step and copy is done;
+ * the first call allocates the staging buffers (4 x dof x Z doubles). */
+int grim_time_steps_host(grim_handle* h, int nsteps, const double* const* hostIn, double* const* hostOut);
 int grim_get_time(grim_handle* h, double* time, double* dt);
 int grim_set_time(grim_handle* h, double time, double dt);
 
