@@ -1553,6 +1553,86 @@ GRIM_D void tangent_jacobian(const double* P, const StageConst<5 + COND + VISC>&
     for (int cc = 0; cc < NF; cc++) J[r][cc] = Rd[r].d[cc];
 }
 
+// One zone's fast Newton from iteration `it` up to (not including) itEnd:
+// at the top of each iteration the floors, the residual where the last
+// line search did not leave one, and the per-zone test; then the Jacobian,
+// the solve and the backtracking line search (solve.cpp:80-199 per zone).
+// Returns with conv set when the test passed (`it` = the updates taken) or
+// with it == itEnd.
+template <int COND, int VISC, class T>
+GRIM_D void fast_newton_iters(const DevCfg& c, const StageConst<5 + COND + VISC>& K, const ZoneGeo<double>& G,
+                              double* P, double* R, bool& haveR, double& l2first, int& it, bool& conv,
+                              int itEnd) {
+  constexpr int NF = 5 + COND + VISC;
+  for (; it < itEnd; it++) {
+    const bool floored = (P[0] < c.rhoFloor) || (P[1] < c.uFloor);
+    P[0] = fmax(P[0], c.rhoFloor);
+    P[1] = fmax(P[1], c.uFloor);
+    if (!haveR || floored) zone_residual<COND, VISC, double, double>(P, K, G, c, R);
+    const double l2 = l2sum<NF>(R);
+    if (it == 0) l2first = l2;
+    if (l2 <= newton_tol(c, l2first, K)) { conv = true; return; }
+    T J[NF][NF];
+    {
+      // the Jacobian's geometry, converted where it is used rather than
+      // kept beside the FP64 copy across the iterations
+      ZoneGeo<T> Gt;
+#pragma unroll
+      for (int m = 0; m < 4; m++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = (T)G.gcov[m][q]; Gt.gcon[m][q] = (T)G.gcon[m][q]; }
+      Gt.g = (T)G.g; Gt.alpha = (T)G.alpha; Gt.ialpha = (T)G.ialpha; Gt.x1 = (T)G.x1; Gt.x2 = (T)G.x2; Gt.dyn = (T)G.dyn;
+      tangent_jacobian<COND, VISC, T>(P, K, Gt, c, J);
+    }
+    T bv[NF], xv[NF];
+#pragma unroll
+    for (int v = 0; v < NF; v++) bv[v] = (T)(-R[v]);
+    gauss_solve<T, NF>(J, bv, xv);
+    double dPv[NF];
+#pragma unroll
+    for (int v = 0; v < NF; v++) dPv[v] = (double)xv[v];
+    const double f0 = 0.5 * l2, fPrime0 = -2. * f0;
+    double lam = 1.;
+    haveR = false;
+    double Rt[NF];
+    for (int ls = 0; ls < c.maxLS; ls++) {
+      double Pt[NF];
+#pragma unroll
+      for (int v = 0; v < NF; v++) Pt[v] = P[v] + lam * dPv[v];
+      zone_residual<COND, VISC, double, double>(Pt, K, G, c, Rt);
+      const double f1 = 0.5 * l2sum<NF>(Rt);
+      if (!(f1 > (f0 * (1. - 1e-4 * lam) + c.lsFloor))) { haveR = true; break; }
+      const double denom = (f1 - f0 - fPrime0 * lam);
+      lam = -fPrime0 * lam * lam / denom / 2.;
+    }
+#pragma unroll
+    for (int v = 0; v < NF; v++) {
+      P[v] = P[v] + lam * dPv[v];
+      if (haveR) R[v] = Rt[v];
+    }
+  }
+}
+
+// The test of a zone that used every iteration, on the state it returns; a
+// last step whose line search ran out was applied unevaluated: its residual
+// is formed here, at the floored state the next iteration would see.
+// Returns true when the zone is above tolerance.
+template <int COND, int VISC>
+GRIM_D bool fast_newton_final(const DevCfg& c, const StageConst<5 + COND + VISC>& K, const ZoneGeo<double>& G,
+                              const double* P, double* R, bool haveR, double l2first) {
+  constexpr int NF = 5 + COND + VISC;
+  if (!haveR) {
+    double Pf[NF];
+#pragma unroll
+    for (int v = 0; v < NF; v++) Pf[v] = P[v];
+    Pf[0] = fmax(Pf[0], c.rhoFloor);
+    Pf[1] = fmax(Pf[1], c.uFloor);
+    zone_residual<COND, VISC, double, double>(Pf, K, G, c, R);
+  }
+  const double l2 = l2sum<NF>(R);
+  return !(l2 >= 0. && l2 <= newton_tol(c, l2first, K));
+}
+
 constexpr int kNewtonMinBlocks = 3;  // blocks per SM of the ideal FP32-Jacobian Newton
 template <int COND, int VISC, class T>
 __global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : kNewtonMinBlocks) k_newton_fast(DevCfg c, int stage, StageBufs b,
@@ -1574,72 +1654,11 @@ __global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : kN
     const double* guess = (stage == GRIM_HALF_STEP && b.guessOld) ? b.pold : b.prim;
 #pragma unroll
     for (int v = 0; v < NF; v++) P[v] = guess[(long long)v * Z + z];
-    bool haveR = false;
+    bool haveR = false, conv = false;
     double l2first = 0.;
     int it = 0;
-    bool conv = false;
-    for (; it < c.maxIter; it++) {
-      const bool floored = (P[0] < c.rhoFloor) || (P[1] < c.uFloor);
-      P[0] = fmax(P[0], c.rhoFloor);
-      P[1] = fmax(P[1], c.uFloor);
-      if (!haveR || floored) zone_residual<COND, VISC, double, double>(P, K, G, c, R);
-      const double l2 = l2sum<NF>(R);
-      if (it == 0) l2first = l2;
-      if (l2 <= newton_tol(c, l2first, K)) { conv = true; break; }
-      T J[NF][NF];
-      {
-        // the Jacobian's geometry, converted where it is used rather than
-        // kept beside the FP64 copy across the iterations
-        ZoneGeo<T> Gt;
-#pragma unroll
-        for (int m = 0; m < 4; m++)
-#pragma unroll
-          for (int q = 0; q < 4; q++) { Gt.gcov[m][q] = (T)G.gcov[m][q]; Gt.gcon[m][q] = (T)G.gcon[m][q]; }
-        Gt.g = (T)G.g; Gt.alpha = (T)G.alpha; Gt.ialpha = (T)G.ialpha; Gt.x1 = (T)G.x1; Gt.x2 = (T)G.x2; Gt.dyn = (T)G.dyn;
-        tangent_jacobian<COND, VISC, T>(P, K, Gt, c, J);
-      }
-      T bv[NF], xv[NF];
-#pragma unroll
-      for (int v = 0; v < NF; v++) bv[v] = (T)(-R[v]);
-      gauss_solve<T, NF>(J, bv, xv);
-      double dPv[NF];
-#pragma unroll
-      for (int v = 0; v < NF; v++) dPv[v] = (double)xv[v];
-      const double f0 = 0.5 * l2, fPrime0 = -2. * f0;
-      double lam = 1.;
-      haveR = false;
-      double Rt[NF];
-      for (int ls = 0; ls < c.maxLS; ls++) {
-        double Pt[NF];
-#pragma unroll
-        for (int v = 0; v < NF; v++) Pt[v] = P[v] + lam * dPv[v];
-        zone_residual<COND, VISC, double, double>(Pt, K, G, c, Rt);
-        const double f1 = 0.5 * l2sum<NF>(Rt);
-        if (!(f1 > (f0 * (1. - 1e-4 * lam) + c.lsFloor))) { haveR = true; break; }
-        const double denom = (f1 - f0 - fPrime0 * lam);
-        lam = -fPrime0 * lam * lam / denom / 2.;
-      }
-#pragma unroll
-      for (int v = 0; v < NF; v++) {
-        P[v] = P[v] + lam * dPv[v];
-        if (haveR) R[v] = Rt[v];
-      }
-    }
-    if (!conv && it == c.maxIter) {
-      // final check of the last update (the state that is returned); a last
-      // step whose line search ran out was applied unevaluated: its residual
-      // is formed here, at the floored state the next iteration would see
-      if (!haveR) {
-        double Pf[NF];
-#pragma unroll
-        for (int v = 0; v < NF; v++) Pf[v] = P[v];
-        Pf[0] = fmax(Pf[0], c.rhoFloor);
-        Pf[1] = fmax(Pf[1], c.uFloor);
-        zone_residual<COND, VISC, double, double>(Pf, K, G, c, R);
-      }
-      const double l2 = l2sum<NF>(R);
-      if (!(l2 >= 0. && l2 <= newton_tol(c, l2first, K))) unconv = 1;
-    }
+    fast_newton_iters<COND, VISC, T>(c, K, G, P, R, haveR, l2first, it, conv, c.maxIter);
+    if (!conv && it == c.maxIter) unconv = fast_newton_final<COND, VISC>(c, K, G, P, R, haveR, l2first) ? 1 : 0;
     itsMax = it;
 #pragma unroll
     for (int v = 0; v < NF; v++) b.prim[(long long)v * Z + z] = P[v];
@@ -1662,6 +1681,150 @@ __global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : kN
     if (nNan) atomicAdd(b.nanCount, (unsigned long long)nNan);
   }
 }
+
+#ifdef GRIM_FAST_MATH
+// ---------------------------------------------------------------------------
+// Deferred-tail fast Newton, ideal MHD: a persistent kernel whose warps take
+// batches of 32 consecutive zones and run each zone's first maxIter - 1
+// updates together; a zone still above tolerance then goes, with its state,
+// onto its warp's stash in shared memory, and whenever the stash holds 32
+// zones the warp runs their last update as one full batch.  Most zones
+// converge one update before the cap, so the per-zone kernel's warps nearly
+// all run the last update for a few lanes; here it runs on full warps
+// only.  The per-zone arithmetic is fast_newton_iters / fast_newton_final,
+// as in k_newton_fast: the results are the same bits.  The stash keeps what
+// the ideal residual and Jacobian read besides the geometry (reloaded, it
+// is the same for every stage): B, Kc, the rounding floor; dt' comes from
+// the step's dt as in load_stage_const.
+// ---------------------------------------------------------------------------
+constexpr int kDeferWarps = 4;  // warps per block
+constexpr int kDeferCap = 64;   // stash slots per warp (< 32 left + 32 pushed)
+struct DeferStash {
+  double P[5][kDeferCap];
+  double R[5][kDeferCap];
+  double Kc[5][kDeferCap];
+  double B[3][kDeferCap];
+  double l2first[kDeferCap];
+  double tolFloor2[kDeferCap];
+  int z[kDeferCap];
+  int haveR[kDeferCap];
+};
+
+template <class T>
+__global__ void __launch_bounds__(32 * kDeferWarps, kNewtonMinBlocks) k_newton_defer(DevCfg c, int stage, StageBufs b,
+                                                                                  long long nlist) {
+  constexpr int NF = 5;
+  __shared__ DeferStash stashes[kDeferWarps];
+  const int lane = threadIdx.x & 31;
+  DeferStash& S = stashes[threadIdx.x >> 5];
+  const long long Z = c.Z;
+  const int split = c.maxIter - 1;
+  const double dt = b.st->dt;
+  const double dtp = (stage == GRIM_HALF_STEP) ? dt / 2. : dt;
+  const double* guess = (stage == GRIM_HALF_STEP && b.guessOld) ? b.pold : b.prim;
+  const long long nbatch = (nlist + 31) / 32;
+  const long long stride = (long long)gridDim.x * kDeferWarps;
+  long long bt = (long long)blockIdx.x * kDeferWarps + (threadIdx.x >> 5);
+  int held = 0;                           // warp-uniform stash fill
+  int itsMax = 0, nUnconv = 0, nNan = 0;  // this lane's tallies
+  // one task per pass, the same for the whole warp: the last update of 32
+  // stashed zones when the stash holds 32, else the first maxIter - 1
+  // updates of the next batch, else the last update of what is left
+  for (;;) {
+    bool tail;
+    int from = 0, count = 32;
+    if (held >= 32) {
+      tail = true;
+      held -= 32;
+      from = held;
+    } else if (bt < nbatch) {
+      tail = false;
+    } else if (held > 0) {
+      tail = true;
+      count = held;
+      held = 0;
+    } else {
+      break;
+    }
+    const long long n = bt * 32 + lane;
+    const bool act = tail ? lane < count : n < nlist;
+    long long z = 0;
+    StageConst<NF> K;
+    double P[NF], R[NF], l2first = 0.;
+    bool haveR = false, conv = false;
+    int it = tail ? split : 0;
+    if (act) {
+      const int sl = from + lane;
+      z = tail ? (long long)S.z[sl] : interior_to_z(c, n);
+      int i, j, k;
+      zijk(c, z, i, j, k);
+      ZoneGeo<double> G;
+      load_geo(G, c, b.geoC, z, i, j, 0.5, 0.5);
+      if (tail) {
+        K.dtp = dtp;
+        K.idtp = 1. / dtp;
+#pragma unroll
+        for (int v = 0; v < NF; v++) { K.Kc[v] = S.Kc[v][sl]; P[v] = S.P[v][sl]; R[v] = S.R[v][sl]; }
+#pragma unroll
+        for (int v = 0; v < 3; v++) K.B[v] = S.B[v][sl];
+        K.tolFloor2 = S.tolFloor2[sl];
+        haveR = S.haveR[sl] != 0;
+        l2first = S.l2first[sl];
+      } else {
+        load_stage_const<0, 0>(K, c, stage, b, z, G);
+#pragma unroll
+        for (int v = 0; v < NF; v++) P[v] = guess[(long long)v * Z + z];
+      }
+      fast_newton_iters<0, 0, T>(c, K, G, P, R, haveR, l2first, it, conv, tail ? c.maxIter : split);
+      if (tail && !conv) nUnconv += fast_newton_final<0, 0>(c, K, G, P, R, haveR, l2first) ? 1 : 0;
+      if (tail || conv) {
+        itsMax = max(itsMax, it);
+#pragma unroll
+        for (int v = 0; v < NF; v++) b.prim[(long long)v * Z + z] = P[v];
+        if (b.nanCount) {
+          bool nz = false;
+#pragma unroll
+          for (int v = 0; v < NF; v++) nz |= isnan(P[v]);
+#pragma unroll
+          for (int v = 0; v < 3; v++) nz |= isnan(K.B[v]);
+          nNan += nz ? 1 : 0;
+        }
+      }
+    }
+    hist_add(b.st->itHist[stage], min(it, 15), act && (tail || conv));
+    if (!tail) {
+      // the zones of the batch still above tolerance onto the stash
+      const bool defer = act && !conv;
+      const unsigned m = __ballot_sync(0xffffffffu, defer);
+      if (defer) {
+        const int sl = held + __popc(m & ((1u << lane) - 1u));
+        S.z[sl] = (int)z;
+#pragma unroll
+        for (int v = 0; v < NF; v++) { S.P[v][sl] = P[v]; S.R[v][sl] = R[v]; S.Kc[v][sl] = K.Kc[v]; }
+#pragma unroll
+        for (int v = 0; v < 3; v++) S.B[v][sl] = K.B[v];
+        S.l2first[sl] = l2first;
+        S.tolFloor2[sl] = K.tolFloor2;
+        S.haveR[sl] = haveR ? 1 : 0;
+      }
+      held += __popc(m);
+      bt += stride;
+    }
+    __syncwarp();
+  }
+  // warp tallies
+  for (int o = 16; o > 0; o >>= 1) {
+    itsMax = max(itsMax, __shfl_xor_sync(0xffffffffu, itsMax, o));
+    nUnconv += __shfl_xor_sync(0xffffffffu, nUnconv, o);
+    nNan += __shfl_xor_sync(0xffffffffu, nNan, o);
+  }
+  if (lane == 0) {
+    atomicMax((unsigned long long*)&b.st->itersDone[stage], (unsigned long long)itsMax);
+    if (nUnconv) atomicAdd(&b.st->finalUnconv[stage], (unsigned long long)nUnconv);
+    if (nNan) atomicAdd(b.nanCount, (unsigned long long)nNan);
+  }
+}
+#endif  // GRIM_FAST_MATH
 
 // ---------------------------------------------------------------------------
 // Compacted fast Newton: one launch per iteration over a worklist of the
@@ -2368,6 +2531,23 @@ void newton_fast(const DevCfg& c, int stage, const StageBufs& b, int mode, const
                  cudaStream_t s) {
   GRIM_EMHD_DISPATCH(c, newton_fast_t, c, stage, b, mode, list, nlist, s);
 }
+
+#ifdef GRIM_FAST_MATH
+bool newton_defer(const DevCfg& c, int stage, const StageBufs& b, int mode, cudaStream_t s) {
+  if (c.conduction || c.viscosity || mode != GRIM_NEWTON_MIXED32 || c.maxIter < 2 || c.Z > 0x7fffffffLL)
+    return false;
+  static int grid = 0;
+  if (!grid) {
+    int dev = 0, sms = 148, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_newton_defer<float>, 32 * kDeferWarps, 0);
+    grid = sms * (per > 0 ? per : 1);
+  }
+  if (c.Zint > 0) k_newton_defer<float><<<grid, 32 * kDeferWarps, 0, s>>>(c, stage, b, c.Zint);
+  return true;
+}
+#endif
 
 static int persistent_blocks() {
   static int nb = 0;

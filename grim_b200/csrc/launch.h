@@ -75,6 +75,10 @@ namespace fast {
 // all problems' unconverged zones (tbl, bs in device memory)
 void batch_newton(const DevCfg& c0, const BatchEntry* tbl, int nprob, long long total, int maxIter, int stage,
                   int mode, BatchState* bs, cudaStream_t s);
+// the deferred-tail Newton (ideal MHD, mixed form, maxIter >= 2): one
+// persistent launch per stage; false when the configuration is not one it
+// runs (the caller then runs newton_fast)
+bool newton_defer(const DevCfg& c, int stage, const StageBufs& b, int mode, cudaStream_t s);
 // algorithmic flop counts of one zone's residual / tangent / solve
 void count_ops(const DevCfg& c, int stage, const StageBufs& b, long long z, double* out, cudaStream_t s);
 }  // namespace fast

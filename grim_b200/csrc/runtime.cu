@@ -387,6 +387,8 @@ static bool enqueue_newton(grim_handle* h, int stage, bool guessOld = false, boo
   } else if (h->cfg.perZoneConvergence == 2) {
     grim::fast::newton_list(c, stage, b, h->cfg.newtonMode, s);
     g_launch_counter += 1 + c.maxIter;
+  } else if (h->cfg.perZoneConvergence == 3 && grim::fast::newton_defer(c, stage, b, h->cfg.newtonMode, s)) {
+    g_launch_counter++;
   } else {
     grim::fast::newton_fast(c, stage, b, h->cfg.newtonMode, nullptr, c.Zint, s);
     g_launch_counter++;
@@ -1386,7 +1388,7 @@ int grim_problem_init(grim_handle* h) {
 }
 
 int grim_set_newton_mode(grim_handle* h, int mode, int perZone, double rtol) {
-  if (!h || mode < 0 || mode > 3 || perZone < 0 || perZone > 2) return GRIM_EINVAL;
+  if (!h || mode < 0 || mode > 3 || perZone < 0 || perZone > 3) return GRIM_EINVAL;
   h->cfg.newtonMode = mode;
   h->cfg.perZoneConvergence = perZone;
   h->cfg.nonlinearsolve_rtol = rtol;

@@ -80,7 +80,8 @@ typedef struct grim_config {
   int problem;              /* problem hooks: BCs, flux filter, floors */
   int elemOldFromFullStep;  /* 1: fullStepDiagnostics re-sets elemOld */
   int newtonMode;           /* GRIM_NEWTON_* */
-  int perZoneConvergence;   /* 0: global break (reference), 1: per zone, 2: compacted */
+  int perZoneConvergence;   /* 0: global break (reference), 1: per zone, 2: compacted,
+                               3: per zone with the last update deferred */
   int N3Global;             /* > 0: the handle holds N3 of N3Global X3 planes of a slab
                                decomposition; X3Start / X3End are the global extent */
   int reserved_i[4];
@@ -304,7 +305,12 @@ int grim_set_geometry(grim_handle* h, int location, const double* in,
 /* ---- options, statistics, graphs ------------------------------------- */
 /* mode: GRIM_NEWTON_*; perZoneConvergence for the tangent / mixed modes:
  * 1 = one kernel, each thread iterates its zone to convergence; 2 = one
- * launch per iteration over a compacted worklist of unconverged zones */
+ * launch per iteration over a compacted worklist of unconverged zones;
+ * 3 = one persistent kernel whose warps run the first maxIter - 1 updates
+ * of 32 zones together and gather the zones still unconverged, 32 at a
+ * time, for the last update (ideal MHD in the mixed mode with
+ * maxNonLinearIter >= 2; anything else runs as 1).  1 and 3 give the same
+ * bits. */
 int grim_set_newton_mode(grim_handle* h, int mode, int perZoneConvergence, double rtol);
 /* zones by Newton iterations used in the last step: out[stage*16 + iters]
  * (tangent / mixed modes) */
