@@ -9,9 +9,11 @@ the FP64 residual, per-zone convergence) with inputs resident in HBM;
 ``fd64`` is the same workload through the plain FP64 finite-difference
 path (the reference's method) at the same Newton tolerance; ``e2e`` adds
 the host<->device copies of the primitives every step through the C ABI
-(grim_time_steps_host: each step's copies overlap the neighbouring steps;
-the same steps as separate grim_set_prims / grim_time_step /
-grim_get_prims calls are reported beside it as ``sequential``).
+(grim_time_steps_host on arrays of the interior zones: each step's copies
+overlap the neighbouring steps; the same call on whole arrays with ghosts
+and the same steps as separate grim_set_prims / grim_time_step /
+grim_get_prims calls are reported beside it as ``ghosted`` and
+``sequential``).
 Each timed step is bracketed by CUDA events on the stepper's stream; the
 L2 is flushed between timed steps (a 256 MB write) and the flush is not
 timed.  With --impl reference the CPU oracle (a C++ restatement of the
@@ -595,7 +597,8 @@ def run_gpu(args, rank, world, local_rank):
     # the same steps through grim_time_steps_host: every step's state in
     # from pinned host memory and its result back, the copies of one step
     # overlapped with the neighbouring steps (one untimed call first
-    # allocates the staging buffers)
+    # allocates the staging buffers); whole arrays with ghosts, then the
+    # interior zones only (the step's boundary pass refills the ghosts)
     host_outs = [host_out, torch.empty_like(host_in).pin_memory()]
     ins = [host_in.data_ptr()] * e2e_steps
     outs = [host_outs[k & 1].data_ptr() for k in range(e2e_steps)]
@@ -603,15 +606,26 @@ def run_gpu(args, rank, world, local_rank):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     ts_fast.timeStepsHost(ins, outs)
+    e2e_ghosted_s = time.perf_counter() - t0
+    sl = (slice(None),) + tuple(C.interior_slices(cfg))
+    inner_in = torch.from_numpy(np.ascontiguousarray(state["P"][sl])).pin_memory()
+    inner_outs = [torch.empty_like(inner_in).pin_memory() for _ in range(2)]
+    ins = [inner_in.data_ptr()] * e2e_steps
+    outs = [inner_outs[k & 1].data_ptr() for k in range(e2e_steps)]
+    ts_fast.timeStepsHost(ins[:2], outs[:2], interior=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ts_fast.timeStepsHost(ins, outs, interior=True)
     e2e_s = time.perf_counter() - t0
-    e2e_bytes = host_in.numel() * 8
+    e2e_bytes = inner_in.numel() * 8
+    e2e_ghosted_bytes = host_in.numel() * 8
     side = torus_side_costs(ts_fast, cfg) if args.workload == "torus" else None
 
     # max over ranks of the device time
-    t = torch.tensor([ms_fast, ms_fd, ms_fdf, e2e_s, e2e_seq_s], dtype=torch.float64, device="cuda")
+    t = torch.tensor([ms_fast, ms_fd, ms_fdf, e2e_s, e2e_seq_s, e2e_ghosted_s], dtype=torch.float64, device="cuda")
     if world > 1:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_fast, ms_fd, ms_fdf, e2e_s, e2e_seq_s = [float(x) for x in t.tolist()]
+    ms_fast, ms_fd, ms_fdf, e2e_s, e2e_seq_s, e2e_ghosted_s = [float(x) for x in t.tolist()]
     value = world * zones * args.steps / (ms_fast / 1e3)
     fd = world * zones * args.steps / (ms_fd / 1e3) if ms_fd == ms_fd else None
     fdf = world * zones * args.steps / (ms_fdf / 1e3) if ms_fdf == ms_fdf else None
@@ -654,8 +668,12 @@ def run_gpu(args, rank, world, local_rank):
                                                   "full": prof_fd["hist"][1][:cfg["maxNonLinearIter"] + 1]}},
         "e2e": {"value": world * zones * e2e_steps / e2e_s, "unit": "zone-cycles/s",
                 "h2d_bytes_per_step": e2e_bytes, "d2h_bytes_per_step": e2e_bytes,
-                "call": "grim_time_steps_host (pinned buffers; copies overlapped with the steps)",
+                "call": "grim_time_steps_host, interior zones (pinned buffers; copies overlapped with the steps)",
+                "ghosted": {"value": world * zones * e2e_steps / e2e_ghosted_s,
+                            "h2d_bytes_per_step": e2e_ghosted_bytes, "d2h_bytes_per_step": e2e_ghosted_bytes,
+                            "call": "grim_time_steps_host, whole arrays with ghosts"},
                 "sequential": {"value": world * zones * e2e_steps / e2e_seq_s,
+                               "h2d_bytes_per_step": e2e_ghosted_bytes, "d2h_bytes_per_step": e2e_ghosted_bytes,
                                "call": "grim_set_prims, grim_time_step, grim_get_prims per step"}},
         "gpu_launches": int(st_fast["kernelLaunches"]) * args.steps,
         "clocks": clocks_info,

@@ -18,6 +18,7 @@ _LIB = None
 GRIM_OK = 0
 GRIM_ETIMEOUT = -6
 DEBUG_SKIP_BULK_COPIES = 1
+LAYOUT_GHOSTED, LAYOUT_INTERIOR = 0, 1
 HOST, DEVICE = 0, 1
 PRIM_OLD, PRIM, PRIM_HALF = 0, 1, 2
 
@@ -70,7 +71,7 @@ def lib():
         "grim_get_prims": [vp, i, vp, i],
         "grim_time_step": [vp, P(i), P(i)],
         "grim_time_steps": [vp, i],
-        "grim_time_steps_host": [vp, i, vp, vp],
+        "grim_time_steps_host": [vp, i, vp, vp, i],
         "grim_get_time": [vp, P(d), P(d)],
         "grim_set_time": [vp, d, d],
         "grim_compute_dt": [vp],

@@ -881,18 +881,45 @@ int grim_time_steps(grim_handle* h, int nsteps) {
   return run_steps(h, nsteps);
 }
 
+}  // extern "C"
+
+// interior zones, [var][k][j][i] contiguous (dof x Zint) <-> the same zones
+// of a grid array with ghosts; one row of blocks per variable
+__global__ void k_interior_copy(DevCfg c, const double* __restrict__ src, double* __restrict__ dst, int toGrid) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= c.Zint) return;
+  const long long v = blockIdx.y;
+  const long long z = v * c.Z + interior_to_z(c, n);
+  const long long t = v * c.Zint + n;
+  if (toGrid) dst[z] = src[t];
+  else dst[t] = src[z];
+}
+static void interior_copy(const DevCfg& c, const double* src, double* dst, bool toGrid, cudaStream_t s) {
+  const dim3 grid((unsigned)((c.Zint + 255) / 256), (unsigned)c.dof);
+  k_interior_copy<<<grid, 256, 0, s>>>(c, src, dst, toGrid ? 1 : 0);
+}
+
+extern "C" {
+
 // nsteps of (primOld <- hostIn[k]; timeStep; hostOut[k] <- primOld) with the
 // copies of one step overlapping the other steps' work: uploads on one
 // stream, downloads on another, each through two device staging buffers,
-// the step on the handle's stream between a device copy in and one out.
-int grim_time_steps_host(grim_handle* h, int nsteps, const double* const* hostIn, double* const* hostOut) {
-  if (!h || nsteps < 0) { set_err("grim_time_steps_host: bad argument"); return GRIM_EINVAL; }
+// the step on the handle's stream between a device copy (or an interior
+// scatter / gather) in and one out.
+int grim_time_steps_host(grim_handle* h, int nsteps, const double* const* hostIn, double* const* hostOut,
+                         int layout) {
+  if (!h || nsteps < 0 || (layout != GRIM_LAYOUT_GHOSTED && layout != GRIM_LAYOUT_INTERIOR)) {
+    set_err("grim_time_steps_host: bad argument");
+    return GRIM_EINVAL;
+  }
   {
     const int rc = take_async_error(h);
     if (rc) return rc;
   }
   CK(cudaSetDevice(h->device));
+  const bool interior = layout == GRIM_LAYOUT_INTERIOR;
   const size_t bytes = (size_t)h->dc.dof * h->bytesZ;
+  const size_t hostBytes = interior ? (size_t)h->dc.dof * h->dc.Zint * sizeof(double) : bytes;
   if (!h->ioReady) {
     bool ok = true;
     for (int i = 0; i < 2; i++) {
@@ -923,10 +950,17 @@ int grim_time_steps_host(grim_handle* h, int nsteps, const double* const* hostIn
     if (hostIn && hostIn[k]) {
       // staging buffer s is free once the step of k - 2 has copied it in
       CK(cudaStreamWaitEvent(h->ioUp, inFree[s], 0));
-      CK(cudaMemcpyAsync(h->ioIn[s], hostIn[k], bytes, cudaMemcpyHostToDevice, h->ioUp));
+      CK(cudaMemcpyAsync(h->ioIn[s], hostIn[k], hostBytes, cudaMemcpyHostToDevice, h->ioUp));
       CK(cudaEventRecord(upDone[s], h->ioUp));
       CK(cudaStreamWaitEvent(h->stream, upDone[s], 0));
-      CK(cudaMemcpyAsync(h->primOld, h->ioIn[s], bytes, cudaMemcpyDeviceToDevice, h->stream));
+      if (interior) {
+        // the periodic ghosts as grid::communicate forms them; the step's
+        // boundary pass fills the others
+        interior_copy(h->dc, h->ioIn[s], h->primOld, true, h->stream);
+        KNS_CALL(h, communicate, h->dc, h->primOld, h->dc.dof, h->stream);
+      } else {
+        CK(cudaMemcpyAsync(h->primOld, h->ioIn[s], bytes, cudaMemcpyDeviceToDevice, h->stream));
+      }
       CK(cudaEventRecord(inFree[s], h->stream));
     }
     int rc = run_steps(h, 1);
@@ -934,10 +968,11 @@ int grim_time_steps_host(grim_handle* h, int nsteps, const double* const* hostIn
     if (hostOut && hostOut[k]) {
       // staging buffer s is free once the download of k - 2 has finished
       CK(cudaStreamWaitEvent(h->stream, outFree[s], 0));
-      CK(cudaMemcpyAsync(h->ioOut[s], h->primOld, bytes, cudaMemcpyDeviceToDevice, h->stream));
+      if (interior) interior_copy(h->dc, h->primOld, h->ioOut[s], false, h->stream);
+      else CK(cudaMemcpyAsync(h->ioOut[s], h->primOld, bytes, cudaMemcpyDeviceToDevice, h->stream));
       CK(cudaEventRecord(outStaged[s], h->stream));
       CK(cudaStreamWaitEvent(h->ioDown, outStaged[s], 0));
-      CK(cudaMemcpyAsync(hostOut[k], h->ioOut[s], bytes, cudaMemcpyDeviceToHost, h->ioDown));
+      CK(cudaMemcpyAsync(hostOut[k], h->ioOut[s], hostBytes, cudaMemcpyDeviceToHost, h->ioDown));
       CK(cudaEventRecord(outFree[s], h->ioDown));
     }
   }

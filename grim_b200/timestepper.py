@@ -133,19 +133,21 @@ class timeStepper:
     def timeSteps(self, n):
         _lib.check(_lib.lib().grim_time_steps(self._h, int(n)), "timeSteps")
 
-    def timeStepsHost(self, inputs, outputs):
+    def timeStepsHost(self, inputs, outputs, interior=False):
         """grim_time_steps_host: per step, primOld from inputs[k] (a host
         address, or None to continue from the current state), one
         timeStep, primOld to outputs[k] (a host address or None); the
         copies overlap the other steps' work when the buffers are pinned.
         Addresses are ints (numpy ``a.ctypes.data``, torch
-        ``t.data_ptr()``) of float64 [var][k][j][i] arrays with ghosts."""
+        ``t.data_ptr()``) of float64 [var][k][j][i] arrays with ghosts, or
+        of the interior zones only with ``interior``."""
         n = len(inputs)
         if len(outputs) != n:
             raise ValueError("inputs and outputs differ in length")
         ins = (ctypes.c_void_p * n)(*[None if a is None else int(a) for a in inputs])
         outs = (ctypes.c_void_p * n)(*[None if a is None else int(a) for a in outputs])
-        _lib.check(_lib.lib().grim_time_steps_host(self._h, n, ins, outs), "timeStepsHost")
+        layout = _lib.LAYOUT_INTERIOR if interior else _lib.LAYOUT_GHOSTED
+        _lib.check(_lib.lib().grim_time_steps_host(self._h, n, ins, outs, layout), "timeStepsHost")
 
     @property
     def time(self):

@@ -151,16 +151,28 @@ int grim_problem_init(grim_handle* h);
  *      numWrites report the algorithmic words per zone, may be NULL ------ */
 int grim_time_step(grim_handle* h, int* numReads, int* numWrites);
 int grim_time_steps(grim_handle* h, int nsteps);
-/* nsteps of: primOld <- hostIn[k] (when hostIn and hostIn[k] are not NULL;
- * the whole [var][k][j][i] array with ghosts, as grim_set_prims), one
- * timeStep, hostOut[k] <- primOld (when hostOut and hostOut[k] are not
- * NULL).  The same results as those calls made one after another; here the
- * upload of step k + 1, the step k and the download of step k - 1 run at
- * once (two device staging buffers each way, an upload and a download
+/* nsteps of: primOld <- hostIn[k] (when hostIn and hostIn[k] are not NULL),
+ * one timeStep, hostOut[k] <- primOld (when hostOut and hostOut[k] are not
+ * NULL).  The host arrays are, by layout:
+ *   GRIM_LAYOUT_GHOSTED   the whole [var][k][j][i] array with ghosts, as
+ *                         grim_set_prims / grim_get_prims: the same results
+ *                         as those calls made one after another;
+ *   GRIM_LAYOUT_INTERIOR  [var][k][j][i] of the interior zones only
+ *                         (dof x N1 x N2 x N3): the input's ghost zones are
+ *                         formed from its interior, the periodic ones as
+ *                         grid::communicate forms them (grim_communicate),
+ *                         the others by the step's boundary pass; the
+ *                         results equal the ghosted calls given arrays whose
+ *                         ghosts were communicated (a slab's GRIM_EXCHANGE
+ *                         halo keeps its values: the caller's to fill).
+ * The upload of step k + 1, the step k and the download of step k - 1 run
+ * at once (two device staging buffers each way, an upload and a download
  * stream).  Host buffers must be pinned (cudaHostAlloc / cudaHostRegister)
  * for the copies to overlap.  Returns when every step and copy is done;
  * the first call allocates the staging buffers (4 x dof x Z doubles). */
-int grim_time_steps_host(grim_handle* h, int nsteps, const double* const* hostIn, double* const* hostOut);
+enum { GRIM_LAYOUT_GHOSTED = 0, GRIM_LAYOUT_INTERIOR = 1 };
+int grim_time_steps_host(grim_handle* h, int nsteps, const double* const* hostIn, double* const* hostOut,
+                         int layout);
 int grim_get_time(grim_handle* h, double* time, double* dt);
 int grim_set_time(grim_handle* h, double time, double dt);
 
