@@ -18,8 +18,8 @@
 // flux-CT / EMF (constrainedtransport.cpp:3-83), Riemann solver
 // (riemannsolver.cpp:202-328) and reconstruction, the last two through
 // local Jacobians taken with the forward-tangent scalar on the same
-// templated physics the kernels run.  Scope: ideal MHD, Minkowski, 2D,
-// periodic in both directions, dt held fixed over the run; the runtime
+// templated physics the kernels run.  Scope: ideal MHD, Minkowski, 2D or
+// 3D, periodic in every direction, dt held fixed over the run; the runtime
 // rejects anything else.  Every accumulation is a gather in a fixed order
 // (no atomics), so a gradient is the same bits run to run.
 #include <cuda_runtime.h>
@@ -151,22 +151,24 @@ __global__ void k_cons(DevCfg c, const double* __restrict__ P, const double* __r
   }
 }
 
-GRIM_D bool is_interior(const DevCfg& c, int i, int j) {
-  return i >= c.g1 && i < c.N1 + c.g1 && j >= c.g2 && j < c.N2 + c.g2;
+GRIM_D bool is_interior(const DevCfg& c, int i, int j, int k) {
+  return i >= c.g1 && i < c.N1 + c.g1 && j >= c.g2 && j < c.N2 + c.g2 &&
+         (c.dim < 3 || (k >= c.g3 && k < c.N3 + c.g3));
 }
 
 // divergence transpose: Ft[d][v][f] = (g[v][f - s_d] - g[v][f]) / dX_d,
-// g zero off the interior (the zero-padded convolution of fvmfluxes.cpp)
+// g zero off the interior (the zero-padded convolution of fvmfluxes.cpp in
+// 2D, the shifted difference in 3D: the same linear map)
 __global__ void k_div_t(DevCfg c, const double* __restrict__ g, double* __restrict__ Ft) {
   long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (z >= c.Z) return;
   int i, j, k;
   zijk(c, z, i, j, k);
   const long long Z = c.Z;
-  for (int d = 0; d < 2; d++) {
-    const int im = d == 0 ? i - 1 : i, jm = d == 0 ? j : j - 1;
-    const bool in0 = is_interior(c, i, j), in1 = is_interior(c, im, jm);
-    const long long zm = zidx(c, im < 0 ? 0 : im, jm < 0 ? 0 : jm, k);
+  for (int d = 0; d < c.dim; d++) {
+    const int im = d == 0 ? i - 1 : i, jm = d == 1 ? j - 1 : j, km = d == 2 ? k - 1 : k;
+    const bool in0 = is_interior(c, i, j, k), in1 = is_interior(c, im, jm, km);
+    const long long zm = zidx(c, im < 0 ? 0 : im, jm < 0 ? 0 : jm, km < 0 ? 0 : km);
     const double idx = 1. / c.dX[d];
     for (int v = 0; v < c.dof; v++) {
       const double a = in1 ? g[(long long)v * Z + zm] : 0.;
@@ -176,38 +178,71 @@ __global__ void k_div_t(DevCfg c, const double* __restrict__ g, double* __restri
   }
 }
 
-// flux-CT transpose, step 1: the corner EMF adjoint from the CT fluxes'
-// adjoints (F1_B2[f] = (e[f] + e[f+s2]) / 2, F2_B1[f] = -(e[f] + e[f+s1]) / 2)
+// flux-CT transpose, step 1: the edge EMF adjoints from the CT fluxes'
+// adjoints.  The CT fluxes of the field rows (constrainedtransport.cpp:3-51)
+// are F1_B2 = (e3 + e3[+s2]) / 2, F2_B1 = -(e3 + e3[+s1]) / 2 and, in 3D,
+// F1_B3 = -(e2 + e2[+s3]) / 2, F3_B1 = (e2 + e2[+s1]) / 2,
+// F2_B3 = (e1 + e1[+s3]) / 2, F3_B2 = -(e1 + e1[+s2]) / 2.
+// ebar rows: e3, e1, e2.
+GRIM_D const double* ft_row(const DevCfg& c, const double* Ft, int d, int b) {
+  return Ft + ((long long)d * c.dof + c.B1 + b) * c.Z;
+}
 __global__ void k_ct_t_emf(DevCfg c, const double* __restrict__ Ft, double* __restrict__ ebar) {
   long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (z >= c.Z) return;
   int i, j, k;
   zijk(c, z, i, j, k);
-  const long long Z = c.Z, s1 = 1, s2 = c.N1T;
-  const double* F1B2 = Ft + ((long long)0 * c.dof + c.B1 + 1) * Z;
-  const double* F2B1 = Ft + ((long long)1 * c.dof + c.B1) * Z;
+  const long long Z = c.Z, s1 = 1, s2 = c.N1T, s3 = (long long)c.N1T * c.N2T;
+  const double* F1B2 = ft_row(c, Ft, 0, 1);
+  const double* F2B1 = ft_row(c, Ft, 1, 0);
   double e = 0.5 * F1B2[z] - 0.5 * F2B1[z];
   if (j >= 1) e += 0.5 * F1B2[z - s2];
   if (i >= 1) e -= 0.5 * F2B1[z - s1];
   ebar[z] = e;
+  if (c.dim < 3) return;
+  const double* F2B3 = ft_row(c, Ft, 1, 2);
+  const double* F3B2 = ft_row(c, Ft, 2, 1);
+  const double* F1B3 = ft_row(c, Ft, 0, 2);
+  const double* F3B1 = ft_row(c, Ft, 2, 0);
+  double e1 = 0.5 * F2B3[z] - 0.5 * F3B2[z];
+  if (k >= 1) e1 += 0.5 * F2B3[z - s3];
+  if (j >= 1) e1 -= 0.5 * F3B2[z - s2];
+  double e2 = 0.5 * F3B1[z] - 0.5 * F1B3[z];
+  if (i >= 1) e2 += 0.5 * F3B1[z - s1];
+  if (k >= 1) e2 -= 0.5 * F1B3[z - s3];
+  ebar[Z + z] = e1;
+  ebar[2 * Z + z] = e2;
 }
 
 // flux-CT transpose, step 2: the raw Riemann fluxes' adjoints of the B
-// rows (e[c] = (F1_B2[c] + F1_B2[c-s2] - F2_B1[c] - F2_B1[c-s1]) / 4);
-// B1 through X1 and B2 through X2 faces never reach the divergence
+// rows from the edge EMFs e3 = (R1_B2 + R1_B2[-s2] - R2_B1 - R2_B1[-s1]) / 4,
+// e1 = (R2_B3 + R2_B3[-s3] - R3_B2 - R3_B2[-s2]) / 4,
+// e2 = (R3_B1 + R3_B1[-s1] - R1_B3 - R1_B3[-s3]) / 4 (constrainedtransport.cpp:
+// 53-83); a direction's own field row never reaches the divergence; in 2D
+// the B3 rows are the raw fluxes and keep their adjoints
 __global__ void k_ct_t_raw(DevCfg c, const double* __restrict__ ebar, double* __restrict__ Ft) {
   long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (z >= c.Z) return;
   int i, j, k;
   zijk(c, z, i, j, k);
-  const long long Z = c.Z, s1 = 1, s2 = c.N1T;
+  const long long Z = c.Z, s1 = 1, s2 = c.N1T, s3 = (long long)c.N1T * c.N2T;
+  auto row = [&](int d, int b) -> double& { return Ft[((long long)d * c.dof + c.B1 + b) * Z + z]; };
   const double ez = ebar[z];
   const double ej = (j + 1 < c.N2T) ? ebar[z + s2] : 0.;
   const double ei = (i + 1 < c.N1T) ? ebar[z + s1] : 0.;
-  Ft[((long long)0 * c.dof + c.B1) * Z + z] = 0.;
-  Ft[((long long)0 * c.dof + c.B1 + 1) * Z + z] = 0.25 * ez + 0.25 * ej;
-  Ft[((long long)1 * c.dof + c.B1) * Z + z] = -0.25 * ez - 0.25 * ei;
-  Ft[((long long)1 * c.dof + c.B1 + 1) * Z + z] = 0.;
+  row(0, 0) = 0.;
+  row(0, 1) = 0.25 * ez + 0.25 * ej;
+  row(1, 0) = -0.25 * ez - 0.25 * ei;
+  row(1, 1) = 0.;
+  if (c.dim < 3) return;
+  const double* e1 = ebar + Z;
+  const double* e2 = ebar + 2 * Z;
+  const bool kp = k + 1 < c.N3T, jp = j + 1 < c.N2T, ip = i + 1 < c.N1T;
+  row(0, 2) = -0.25 * e2[z] - 0.25 * (kp ? e2[z + s3] : 0.);
+  row(1, 2) = 0.25 * e1[z] + 0.25 * (kp ? e1[z + s3] : 0.);
+  row(2, 0) = 0.25 * e2[z] + 0.25 * (ip ? e2[z + s1] : 0.);
+  row(2, 1) = -0.25 * e1[z] - 0.25 * (jp ? e1[z + s2] : 0.);
+  row(2, 2) = 0.;
 }
 
 // the Riemann flux of one face (riemannsolver.cpp:202-328) on any scalar
@@ -255,8 +290,8 @@ __global__ void k_faces_t(DevCfg c, int dir, const double* __restrict__ P, const
   if (z >= c.Z) return;
   int i, j, k;
   zijk(c, z, i, j, k);
-  const int x = dir == 0 ? i : j;
-  const int NT = dir == 0 ? c.N1T : c.N2T;
+  const int x = dir == 0 ? i : (dir == 1 ? j : k);
+  const int NT = dir == 0 ? c.N1T : (dir == 1 ? c.N2T : c.N3T);
   const long long Z = c.Z, s = stride_of(c, dir);
   double fb[8];
   bool any = false;
@@ -308,8 +343,8 @@ __global__ void k_recon_t(DevCfg c, int dir, const double* __restrict__ P, const
   if (z >= c.Z) return;
   int i, j, k;
   zijk(c, z, i, j, k);
-  const int x = dir == 0 ? i : j;
-  const int NT = dir == 0 ? c.N1T : c.N2T;
+  const int x = dir == 0 ? i : (dir == 1 ? j : k);
+  const int NT = dir == 0 ? c.N1T : (dir == 1 ? c.N2T : c.N3T);
   const long long Z = c.Z, s = stride_of(c, dir);
   typedef Dual<double, 5> D5;
   for (int v = 0; v < 8; v++) {
@@ -342,6 +377,7 @@ __global__ void k_fold(DevCfg c, const double* __restrict__ q, double* __restric
   const long long z = interior_to_z(c, n);
   int i, j, k;
   zijk(c, z, i, j, k);
+  const int kr = c.dim >= 3 ? 1 : 0;
   for (int v = 0; v < c.dof; v++) {
     double s = 0.;
     for (int a = -1; a <= 1; a++) {
@@ -350,7 +386,11 @@ __global__ void k_fold(DevCfg c, const double* __restrict__ q, double* __restric
       for (int b = -1; b <= 1; b++) {
         const int jj = j + b * c.N2;
         if (jj < 0 || jj >= c.N2T) continue;
-        s += q[(long long)v * Z + zidx(c, ii, jj, k)];
+        for (int m = -kr; m <= kr; m++) {
+          const int kk = k + m * c.N3;
+          if (kk < 0 || kk >= c.N3T) continue;
+          s += q[(long long)v * Z + zidx(c, ii, jj, kk)];
+        }
       }
     }
     out[(long long)v * Z + z] = s;
@@ -364,7 +404,7 @@ static __global__ void k_zero_ghosts(DevCfg c, double* __restrict__ a) {
   if (z >= c.Z) return;
   int i, j, k;
   zijk(c, z, i, j, k);
-  if (adj::is_interior(c, i, j)) return;
+  if (adj::is_interior(c, i, j, k)) return;
   for (int v = 0; v < c.dof; v++) a[(long long)v * c.Z + z] = 0.;
 }
 
@@ -381,7 +421,7 @@ void adjoint_stencil_t(const DevCfg& c, const double* P, const double* g, double
   k_ct_t_emf<<<nblk(c.Z, 256), 256, 0, s>>>(c, Ft, ebar);
   k_ct_t_raw<<<nblk(c.Z, 256), 256, 0, s>>>(c, ebar, Ft);
   cudaMemsetAsync(q, 0, (size_t)c.dof * bZ, s);
-  for (int d = 0; d < 2; d++) {
+  for (int d = 0; d < c.dim; d++) {
     k_faces_t<<<nblk(c.Z, 64), 64, 0, s>>>(c, d, P, Ft, gface);
     k_recon_t<<<nblk(c.Z, 64), 64, 0, s>>>(c, d, P, gface, q);
   }

@@ -53,8 +53,8 @@ namespace grim {
 // adjoint.cu: work buffers of the reverse sweep (dof x Z unless noted)
 struct AdjointBufs {
   double* g;     // dL/d divF of the stage
-  double* Ft;    // 2 x dof x Z: face-flux adjoints per direction
-  double* ebar;  // Z: corner EMF adjoints
+  double* Ft;    // dim x dof x Z: face-flux adjoints per direction
+  double* ebar;  // 3 x Z: edge EMF adjoints (e3, e1, e2)
   double* q;     // stencil adjoint before the periodic fold
   double* gface; // 2 x dof x Z: adjoints of the two reconstructed states of the faces along one direction
   double* lamh;  // dL/dPh

@@ -1575,21 +1575,22 @@ int grim_set_dt_mode(grim_handle* h, int fixed) {
 static int adjoint_scope(grim_handle* h) {
   const grim_config& c = h->cfg;
   const bool periodic = c.boundaryLeft == GRIM_PERIODIC && c.boundaryRight == GRIM_PERIODIC &&
-                        c.boundaryBottom == GRIM_PERIODIC && c.boundaryTop == GRIM_PERIODIC;
-  if (c.dim != 2 || c.metric != GRIM_MINKOWSKI || c.conduction || c.viscosity || !periodic ||
-      c.problem != GRIM_PROBLEM_NONE) {
-    set_err("adjoint: supported for 2D ideal MHD in Minkowski with periodic boundaries only");
+                        c.boundaryBottom == GRIM_PERIODIC && c.boundaryTop == GRIM_PERIODIC &&
+                        (c.dim < 3 || (c.boundaryFront == GRIM_PERIODIC && c.boundaryBack == GRIM_PERIODIC));
+  if ((c.dim != 2 && c.dim != 3) || c.metric != GRIM_MINKOWSKI || c.conduction || c.viscosity || !periodic ||
+      c.problem != GRIM_PROBLEM_NONE || c.N3Global > 0) {
+    set_err("adjoint: supported for 2D and 3D ideal MHD in Minkowski with periodic boundaries only");
     return GRIM_ENOTSUP;
   }
   return GRIM_OK;
 }
 
-// work buffers of the reverse sweep: g, Ft (2 dof), ebar (1), q, lamh,
-// ubar (nf), bacc (3), lam
+// work buffers of the reverse sweep: g, Ft (dim x dof), ebar (3), q,
+// gface (2 dof), lamh, ubar (nf), bacc (3), lam
 static int adjoint_work(grim_handle* h, AdjointBufs& w, double*& lam) {
   const DevCfg& c = h->dc;
   if (!h->adjWork) {
-    const size_t words = (size_t)c.Z * (c.dof * 8 + 1 + c.nf + 3);
+    const size_t words = (size_t)c.Z * (c.dof * (6 + c.dim) + 3 + c.nf + 3);
     if (cudaMalloc(&h->adjWork, words * sizeof(double)) != cudaSuccess) {
       set_err("adjoint: work allocation failed");
       return GRIM_ENOMEM;
@@ -1597,8 +1598,8 @@ static int adjoint_work(grim_handle* h, AdjointBufs& w, double*& lam) {
   }
   double* wp = h->adjWork;
   w.g = wp; wp += (size_t)c.dof * c.Z;
-  w.Ft = wp; wp += (size_t)2 * c.dof * c.Z;
-  w.ebar = wp; wp += (size_t)c.Z;
+  w.Ft = wp; wp += (size_t)c.dim * c.dof * c.Z;
+  w.ebar = wp; wp += (size_t)3 * c.Z;
   w.q = wp; wp += (size_t)c.dof * c.Z;
   w.gface = wp; wp += (size_t)2 * c.dof * c.Z;
   w.lamh = wp; wp += (size_t)c.dof * c.Z;

@@ -79,9 +79,9 @@ class TimeSteps(torch.autograd.Function):
 
 
 def fd_check(loss_of, L0, adjoint, picks, scale, rtol=1e-6):
-    """Central differences of the scalar map ``loss_of(v, j, i, h)`` (the
-    loss after shifting interior entry (v, j, i) by h) against
-    ``adjoint[v, j, i]`` at the picked entries.  The forward map is
+    """Central differences of the scalar map ``loss_of(*pick, h)`` (the
+    loss after shifting the interior entry ``pick``, e.g. (v, j, i), by h)
+    against ``adjoint[pick]`` at the picked entries.  The forward map is
     piecewise smooth (limiter branches, the Riemann solvers' min / max of
     speeds): an entry counts only where the differences at h = 1e-6 and
     1e-7 agree and the second differences show no slope jump at the point;
@@ -92,11 +92,11 @@ def fd_check(loss_of, L0, adjoint, picks, scale, rtol=1e-6):
     by the step.  Returns (entries checked, failures)."""
     smooth, bad = 0, []
     noise = 2 * math.ulp(abs(L0))  # rounding of one loss evaluation
-    for v, j, i in picks:
-        ad = adjoint[v, j, i]
+    for pick in picks:
+        ad = adjoint[tuple(pick)]
         tol = max(abs(ad), 1e-3 * scale)
-        p6, m6 = loss_of(v, j, i, 1e-6), loss_of(v, j, i, -1e-6)
-        p7, m7 = loss_of(v, j, i, 1e-7), loss_of(v, j, i, -1e-7)
+        p6, m6 = loss_of(*pick, 1e-6), loss_of(*pick, -1e-6)
+        p7, m7 = loss_of(*pick, 1e-7), loss_of(*pick, -1e-7)
         f6, f7 = (p6 - m6) / 2e-6, (p7 - m7) / 2e-7
         if abs(f6 - f7) > 3e-6 * tol + 2 * noise / 2e-7:
             continue  # a branch switch inside the bracket
@@ -107,7 +107,7 @@ def fd_check(loss_of, L0, adjoint, picks, scale, rtol=1e-6):
         # the two differences carry different errors (truncation at 1e-6,
         # rounding at 1e-7); the adjoint must match one of them
         if min(abs(f6 - ad), abs(f7 - ad)) > rtol * tol:
-            bad.append((v, j, i, f6, f7, ad))
+            bad.append(tuple(pick) + (f6, f7, ad))
     return smooth, bad
 
 

@@ -7,7 +7,8 @@ the same forward map (dt held fixed, Newton converged to roundoff with the
 exact FP64 tangent Jacobian) at a relative tolerance of 1e-6 in FP64.
 The workload is the ideal-MHD linear-mode problem family of the batched
 adjoint configuration: 2D, Minkowski, periodic, minmod / PPM reconstruction,
-LLF / HLL fluxes, flux-CT, random smooth 1e-2 perturbations.
+LLF / HLL fluxes, flux-CT, random smooth 1e-2 perturbations; and the same
+in 3D (periodic in all three directions, the three edge EMFs of flux-CT).
 """
 import numpy as np
 import pytest
@@ -121,6 +122,8 @@ def test_adjoint_checkpoint_interval_does_not_change_the_gradient():
 
 
 def test_adjoint_refuses_unsupported_configurations():
+    """The torus (MKS, outflow / mirror boundaries, problem hooks) is outside
+    the adjoint's scope."""
     from grim_b200.problems import torus as T
     from grim_b200.timestepper import timeStepper
     ts = timeStepper(T.torus_config(N1=32, N2=16, N3=8))
@@ -161,3 +164,98 @@ def test_stencil_transpose_matches_fd(recon, riemann):
         fd = (f(_with_images(ts, Pp)) - f(_with_images(ts, Pm))) / (2 * h)
         ad = vjp[v, 0, j + g, i + g]
         assert abs(fd - ad) <= 1e-6 * max(abs(ad), 1e-3 * np.max(np.abs(vjp))), (v, j, i, fd, ad)
+
+
+# ---- 3D periodic ------------------------------------------------------------
+def _cfg3(N=12, **kw):
+    return PR.fast_mode_config(N=N, N3=N, dim=3, **kw)
+
+
+def _state3(cfg, seed, amp=1e-2):
+    rng = np.random.default_rng(seed)
+    X1, X2, X3 = C.cell_centers(cfg)
+    P = np.zeros((8,) + X1.shape)
+    for v in range(8):
+        k1, k2, k3 = rng.integers(1, 3, 3)
+        ph = rng.uniform(0, 2 * np.pi, 3)
+        P[v] = BG[v] + amp * (np.sin(2 * np.pi * k1 * X1 + ph[0]) * np.cos(2 * np.pi * k2 * X2 + ph[1])
+                              * np.cos(2 * np.pi * k3 * X3 + ph[2]))
+    return P
+
+
+def _adjoint3(cfg, P, nsteps, every):
+    ts = _stepper(cfg, P)
+    ts.adjointForward(nsteps, every)
+    Pf = ts.primOld.getVars()
+    lam = np.zeros_like(Pf)
+    sl = (slice(None),) + tuple(C.interior_slices(cfg))
+    lam[sl] = Pf[sl] - BG[:, None, None, None]
+    return ts.adjointBackward(lam)
+
+
+@pytest.mark.parametrize("recon,riemann", [(C.MINMOD, C.LOCAL_LAX_FRIEDRICH), (C.PPM, C.HLL)])
+def test_stencil_transpose_matches_fd_3d(recon, riemann):
+    """The 3D stencil transpose (three face directions, the three edge EMFs
+    of flux-CT, ghosts as periodic images in every direction) against
+    central differences of <gbar, divF(P)> (an exactly rounded sum).  The
+    map is piecewise smooth (the limiters; the Riemann solvers' min / max of
+    speeds, which tie often around a fluid at rest), so the entries are
+    screened and checked as in the whole-run test: at least 12 of 40
+    random picks must qualify, and every one that does must match."""
+    import math
+    N = 10
+    cfg = _cfg3(N, reconstruction=recon, riemannSolver=riemann)
+    from grim_b200.timestepper import timeStepper
+    ts = timeStepper(cfg)
+    P = _with_images(ts, _state3(cfg, 2))
+    g = cfg["numGhost"]
+    rng = np.random.default_rng(1)
+    gbar = np.zeros_like(P)
+    gbar[:, g:g + N, g:g + N, g:g + N] = rng.standard_normal((8, N, N, N))
+    vjp = ts.adjointStencil(P, gbar)
+
+    def f(Q):
+        return math.fsum((gbar * ts.computeDivOfFluxes(Q)[0]).ravel().tolist())
+
+    def shifted(v, k, j, i, h):
+        Q = P.copy()
+        Q[v, k + g, j + g, i + g] += h
+        return f(_with_images(ts, Q))
+
+    picks = [(n % 8,) + tuple(int(x) for x in rng.integers(0, N, 3)) for n in range(40)]
+    smooth, bad = fd_check(shifted, f(P), interior(cfg, vjp), picks, float(np.max(np.abs(vjp))))
+    assert not bad, bad
+    assert smooth >= 12, smooth
+
+
+def test_adjoint_matches_central_fd_3d():
+    """Whole checkpointed runs in 3D (12^3, 4 steps, checkpoints every 2),
+    screened and checked as the 2D runs are."""
+    N, nsteps = 12, 4
+    cfg = _cfg3(N, reconstruction=C.PPM, riemannSolver=C.HLL, maxNonLinearIter=6, nonlinearsolve_atol=0.0)
+    P = _state3(cfg, 7)
+    grad = _adjoint3(cfg, P, nsteps, every=2)
+    g = cfg["numGhost"]
+    gi = interior(cfg, grad)
+    assert np.all(grad[:, :g] == 0) and np.all(grad[:, :, :g] == 0) and np.all(grad[:, :, :, :g] == 0)
+    scale = np.max(np.abs(gi))
+    L0 = _loss(cfg, P, nsteps)
+
+    def shifted(v, k, j, i, h):
+        Q = P.copy()
+        Q[v, k + g, j + g, i + g] += h
+        return _loss(cfg, Q, nsteps)
+
+    rng = np.random.default_rng(9)
+    picks = [(n % 8,) + tuple(int(x) for x in rng.integers(0, N, 3)) for n in range(40)]
+    smooth, bad = fd_check(shifted, L0, gi, picks, scale)
+    assert not bad, bad
+    assert smooth >= 8, smooth
+
+
+def test_adjoint_checkpoint_interval_does_not_change_the_gradient_3d():
+    cfg = _cfg3(10, maxNonLinearIter=6, nonlinearsolve_atol=0.0)
+    P = _state3(cfg, 3)
+    a = _adjoint3(cfg, P, 4, every=1)
+    b = _adjoint3(cfg, P, 4, every=3)
+    assert np.array_equal(a, b)
