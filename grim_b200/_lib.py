@@ -18,7 +18,6 @@ _LIB = None
 GRIM_OK = 0
 GRIM_ETIMEOUT = -6
 DEBUG_SKIP_BULK_COPIES = 1
-DEBUG_SEPARATE_FINISH = 2
 LAYOUT_GHOSTED, LAYOUT_INTERIOR = 0, 1
 HOST, DEVICE = 0, 1
 PRIM_OLD, PRIM, PRIM_HALF = 0, 1, 2

@@ -1086,103 +1086,47 @@ __global__ void k_dt_speeds(DevCfg c, const double* __restrict__ p, const double
 // Every step of the reference's sequence acts on one zone at a time, so the
 // fused pass gives the same values (the NaN flag is counted beforehand over
 // the interior of src, which the copy leaves unchanged).
-// One zone of the stage finish: q holds the zone's copied state (rows:
-// fluid, then B); floors, the store into dst, and the POST terms (best: the
-// zone's 1/dt term, bad: a non-finite interior zone).  nanReset zeroes a
-// zone holding a NaN before the floors (fullStepDiagnostics' reset, which
-// only changes such zones).
-GRIM_HD TorusCfg torus_cfg(const DevCfg& c) {
-  TorusCfg t;
-  t.MaxLorentzFactor = c.maxLF; t.RhoFloorAmpl = c.rhoFloorAmpl; t.UFloorAmpl = c.uFloorAmpl;
-  t.RhoFloorSlope = c.rhoFloorSlope; t.UFloorSlope = c.uFloorSlope;
-  t.BsqrOverRhoMax = c.bsqOverRhoMax; t.BsqrOverUMax = c.bsqOverUMax;
-  return t;
-}
-template <int COND, int VISC, bool FLOOR, bool POST>
-GRIM_D void stage_finish_zone(const DevCfg& c, const TorusCfg& t, double* q, const ZoneGeo<double>& G,
-                              const double* geoC, int i, int j, int k, long long z, bool nanReset, int dtOn,
-                              double* __restrict__ dst, double& best, int& bad) {
-  constexpr int DOF = 8 + COND + VISC;
-  const long long Z = c.Z;
-  // the floors' last element, when it is that of the final state, serves
-  // the dt speeds below (the same function of the same values)
-  ElemT<double, double> ef;
-  bool haveElem = false;
-  if constexpr (FLOOR) {
-    const long long gz = gidx(c, i, j);
-    haveElem = torus_floor_zone<COND, VISC>(c, t, q, G, __ldg(geoC + 37LL * c.GZ + gz),
-                                            __ldg(geoC + 38LL * c.GZ + gz), nanReset, POST ? &ef : nullptr);
-  }
-#pragma unroll
-  for (int v = 0; v < DOF; v++) dst[(long long)v * Z + z] = q[v];
-  if constexpr (POST) {
-    if (dtOn && !in_exchange_ghost(c, i, j, k))
-      best = haveElem ? elem_inv_dt<COND, VISC>(c, ef, G) : zone_inv_dt<COND, VISC>(c, q, G);
-    const bool inside = i >= c.g1 && i < c.N1 + c.g1 && j >= c.g2 && j < c.N2 + c.g2 && k >= c.g3 &&
-                        k < c.N3 + c.g3;
-    if (inside)
-#pragma unroll
-      for (int v = 0; v < DOF; v++)
-        if (!isfinite(q[v])) bad = 1;
-  }
-}
-
-// the zone's state as grid::communicate leaves it in the stage's array
-template <int DOF>
-GRIM_D void finish_load(const DevCfg& c, const double* __restrict__ src, int i, int j, int k, double* q) {
-  bool zero;
-  const long long s = comm_source(c, i, j, k, zero);
-#pragma unroll
-  for (int v = 0; v < DOF; v++) q[v] = zero ? 0. : src[(long long)v * c.Z + s];
-}
-
 template <int COND, int VISC, bool FLOOR, bool POST>
 __global__ void __launch_bounds__(128) k_stage_finish(DevCfg c, TorusCfg t, const double* __restrict__ src,
                                                       double* __restrict__ dst, const double* __restrict__ geoC,
                                                       const unsigned long long* nanFlag, int dtOn, DevState* st) {
   constexpr int DOF = 8 + COND + VISC;
   const long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long Z = c.Z;
   double best = 0.;
   int bad = 0;
-  if (z < c.Z) {
+  if (z < Z) {
     int i, j, k;
     zijk(c, z, i, j, k);
+    bool zero;
+    const long long s = comm_source(c, i, j, k, zero);
     double q[DOF];
-    finish_load<DOF>(c, src, i, j, k, q);
+#pragma unroll
+    for (int v = 0; v < DOF; v++) q[v] = zero ? 0. : src[(long long)v * Z + s];
     ZoneGeo<double> G;
     load_geo(G, c, geoC, z, i, j, 0.5, 0.5);
-    stage_finish_zone<COND, VISC, FLOOR, POST>(c, t, q, G, geoC, i, j, k, z, POST && *nanFlag != 0, dtOn, dst,
-                                               best, bad);
-  }
-  if constexpr (POST) {
-    block_max_to(best, &st->maxInvDt);
-    bad = __syncthreads_count(bad);
-    if (threadIdx.x == 0 && bad) atomicAdd(&st->nonFinite, (unsigned long long)bad);
-  }
-}
-
-// The stage finish of the ghost zones only, when the per-zone Newton has
-// finished the interior (k_newton_fast with FIN).  The NaN reset is decided
-// per zone: a ghost zone holds a NaN only as the periodic image of an
-// interior zone that does, in which case the reference's flag is set.
-template <int COND, int VISC, bool FLOOR, bool POST>
-__global__ void __launch_bounds__(128) k_stage_finish_ghosts(DevCfg c, TorusCfg t, const double* __restrict__ src,
-                                                             double* __restrict__ dst,
-                                                             const double* __restrict__ geoC, int dtOn,
-                                                             DevState* st) {
-  constexpr int DOF = 8 + COND + VISC;
-  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  double best = 0.;
-  int bad = 0;
-  if (n < c.Z - c.Zint) {
-    int i, j, k;
-    ghost_ijk(c, n, i, j, k);
-    const long long z = zidx(c, i, j, k);
-    double q[DOF];
-    finish_load<DOF>(c, src, i, j, k, q);
-    ZoneGeo<double> G;
-    load_geo(G, c, geoC, z, i, j, 0.5, 0.5);
-    stage_finish_zone<COND, VISC, FLOOR, POST>(c, t, q, G, geoC, i, j, k, z, POST, dtOn, dst, best, bad);
+    // the floors' last element, when it is that of the final state, serves
+    // the dt speeds below (the same function of the same values)
+    ElemT<double, double> ef;
+    bool haveElem = false;
+    if constexpr (FLOOR) {
+      const long long gz = gidx(c, i, j);
+      haveElem = torus_floor_zone<COND, VISC>(c, t, q, G, __ldg(geoC + 37LL * c.GZ + gz),
+                                              __ldg(geoC + 38LL * c.GZ + gz), POST && *nanFlag != 0,
+                                              POST ? &ef : nullptr);
+    }
+#pragma unroll
+    for (int v = 0; v < DOF; v++) dst[(long long)v * Z + z] = q[v];
+    if constexpr (POST) {
+      if (dtOn && !in_exchange_ghost(c, i, j, k))
+        best = haveElem ? elem_inv_dt<COND, VISC>(c, ef, G) : zone_inv_dt<COND, VISC>(c, q, G);
+      const bool inside = i >= c.g1 && i < c.N1 + c.g1 && j >= c.g2 && j < c.N2 + c.g2 && k >= c.g3 &&
+                          k < c.N3 + c.g3;
+      if (inside)
+#pragma unroll
+        for (int v = 0; v < DOF; v++)
+          if (!isfinite(q[v])) bad = 1;
+    }
   }
   if constexpr (POST) {
     block_max_to(best, &st->maxInvDt);
@@ -1690,18 +1634,12 @@ GRIM_D bool fast_newton_final(const DevCfg& c, const StageConst<5 + COND + VISC>
 }
 
 constexpr int kNewtonMinBlocks = 3;  // blocks per SM of the ideal FP32-Jacobian Newton
-// FIN: the stage finish of the zone fused after its solve (0: none; else
-// 1 + FLOOR + 2 POST): the finished state into b.fin, as k_stage_finish
-// forms it for an interior zone, whose copied state is the solve's result
-template <int COND, int VISC, class T, int FIN = 0>
+template <int COND, int VISC, class T>
 __global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : kNewtonMinBlocks) k_newton_fast(DevCfg c, int stage, StageBufs b,
                                                               const int* __restrict__ list, long long nlist) {
   constexpr int NF = 5 + COND + VISC;
-  constexpr bool FLOOR = FIN > 0 && ((FIN - 1) & 1);
-  constexpr bool POST = FIN > 0 && ((FIN - 1) & 2);
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int unconv = 0, itsMax = 0, finBad = 0;
-  double finBest = 0.;
+  int unconv = 0, itsMax = 0;
   bool nanZone = false;
   if (n < nlist) {
     const long long Z = c.Z;
@@ -1729,23 +1667,6 @@ __global__ void __launch_bounds__(128, (COND || VISC || sizeof(T) == 8) ? 1 : kN
       for (int v = 0; v < NF; v++) nanZone |= isnan(P[v]);
 #pragma unroll
       for (int v = 0; v < 3; v++) nanZone |= isnan(K.B[v]);
-    }
-    if constexpr (FIN > 0) {
-      double q[NF + 3];
-#pragma unroll
-      for (int v = 0; v < NF; v++) q[v] = P[v];
-#pragma unroll
-      for (int v = 0; v < 3; v++) q[NF + v] = K.B[v];
-      stage_finish_zone<COND, VISC, FLOOR, POST>(c, torus_cfg(c), q, G, b.geoC, i, j, k, z, POST, b.finDtOn,
-                                                 b.fin, finBest, finBad);
-    }
-  }
-  if constexpr (POST) {
-    for (int o = 16; o > 0; o >>= 1) finBest = fmax(finBest, __shfl_xor_sync(0xffffffffu, finBest, o));
-    const int nBad = __popc(__ballot_sync(0xffffffffu, finBad != 0));
-    if ((threadIdx.x & 31) == 0) {
-      if (finBest > 0.) atomic_max_pos(&b.st->maxInvDt, finBest);
-      if (nBad) atomicAdd(&b.st->nonFinite, (unsigned long long)nBad);
     }
   }
   hist_add(b.st->itHist[stage], min(itsMax, 15), n < nlist);
@@ -2601,24 +2522,10 @@ template <int C, int V>
 static void newton_fast_t(const DevCfg& c, int stage, const StageBufs& b, int mode, const int* list,
                           long long nlist, cudaStream_t s) {
   if (nlist <= 0) return;
-  const unsigned g = nblk(nlist, 128);
-#ifdef GRIM_FAST_MATH
-  if constexpr (C == 0 && V == 0) {
-    if (b.fin && mode == GRIM_NEWTON_MIXED32 && !list) {
-      // the stage finish fused (runtime: ideal MHD, mixed form, whole interior)
-      const int fin = 1 + (b.finFloor ? 1 : 0) + (b.finPost ? 2 : 0);
-      if (fin == 1) k_newton_fast<0, 0, float, 1><<<g, 128, 0, s>>>(c, stage, b, list, nlist);
-      else if (fin == 2) k_newton_fast<0, 0, float, 2><<<g, 128, 0, s>>>(c, stage, b, list, nlist);
-      else if (fin == 3) k_newton_fast<0, 0, float, 3><<<g, 128, 0, s>>>(c, stage, b, list, nlist);
-      else k_newton_fast<0, 0, float, 4><<<g, 128, 0, s>>>(c, stage, b, list, nlist);
-      return;
-    }
-  }
-#endif
   if (mode == GRIM_NEWTON_MIXED32)
-    k_newton_fast<C, V, float><<<g, 128, 0, s>>>(c, stage, b, list, nlist);
+    k_newton_fast<C, V, float><<<nblk(nlist, 128), 128, 0, s>>>(c, stage, b, list, nlist);
   else
-    k_newton_fast<C, V, double><<<g, 128, 0, s>>>(c, stage, b, list, nlist);
+    k_newton_fast<C, V, double><<<nblk(nlist, 128), 128, 0, s>>>(c, stage, b, list, nlist);
 }
 void newton_fast(const DevCfg& c, int stage, const StageBufs& b, int mode, const int* list, long long nlist,
                  cudaStream_t s) {
@@ -2733,6 +2640,13 @@ int batch_solve(int n, int batch, const double* A, const double* b, double* x, c
     default: return -1;
   }
 }
+static TorusCfg torus_cfg(const DevCfg& c) {
+  TorusCfg t;
+  t.MaxLorentzFactor = c.maxLF; t.RhoFloorAmpl = c.rhoFloorAmpl; t.UFloorAmpl = c.uFloorAmpl;
+  t.RhoFloorSlope = c.rhoFloorSlope; t.UFloorSlope = c.uFloorSlope;
+  t.BsqrOverRhoMax = c.bsqOverRhoMax; t.BsqrOverUMax = c.bsqOverUMax;
+  return t;
+}
 template <int C, int V>
 static void torus_floor_t(const DevCfg& c, double* p, const double* geoC, const unsigned long long* flag,
                           cudaStream_t s) {
@@ -2758,25 +2672,6 @@ static void stage_finish_t(const DevCfg& c, const double* src, double* dst, cons
 void stage_finish(const DevCfg& c, const double* src, double* dst, const double* geoC, bool floors, bool post,
                   const unsigned long long* nanFlag, int dtOn, DevState* st, cudaStream_t s) {
   GRIM_EMHD_DISPATCH(c, stage_finish_t, c, src, dst, geoC, floors, post, nanFlag, dtOn, st, s);
-}
-template <int C, int V>
-static void stage_finish_ghosts_t(const DevCfg& c, const double* src, double* dst, const double* geoC, bool floors,
-                                  bool post, int dtOn, DevState* st, cudaStream_t s) {
-  const TorusCfg t = torus_cfg(c);
-  if (c.Z <= c.Zint) return;
-  const unsigned nb = (unsigned)nblk(c.Z - c.Zint, 128);
-  if (floors && post)
-    k_stage_finish_ghosts<C, V, true, true><<<nb, 128, 0, s>>>(c, t, src, dst, geoC, dtOn, st);
-  else if (floors)
-    k_stage_finish_ghosts<C, V, true, false><<<nb, 128, 0, s>>>(c, t, src, dst, geoC, dtOn, st);
-  else if (post)
-    k_stage_finish_ghosts<C, V, false, true><<<nb, 128, 0, s>>>(c, t, src, dst, geoC, dtOn, st);
-  else
-    k_stage_finish_ghosts<C, V, false, false><<<nb, 128, 0, s>>>(c, t, src, dst, geoC, dtOn, st);
-}
-void stage_finish_ghosts(const DevCfg& c, const double* src, double* dst, const double* geoC, bool floors,
-                         bool post, int dtOn, DevState* st, cudaStream_t s) {
-  GRIM_EMHD_DISPATCH(c, stage_finish_ghosts_t, c, src, dst, geoC, floors, post, dtOn, st, s);
 }
 template <int C, int V>
 static void torus_observe_t(const DevCfg& c, const double* p, const double* geoC, double volElem, double every,

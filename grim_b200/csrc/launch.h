@@ -42,8 +42,6 @@
   void stage_finish(const DevCfg& c, const double* src, double* dst, const double* geoC, bool floors,   \
                     bool post, const unsigned long long* nanFlag, int dtOn, DevState* st,               \
                     cudaStream_t s);                                                                    \
-  void stage_finish_ghosts(const DevCfg& c, const double* src, double* dst, const double* geoC,         \
-                           bool floors, bool post, int dtOn, DevState* st, cudaStream_t s);             \
   void torus_bcs(const DevCfg& c, double* p, const double* geoC, cudaStream_t s);                      \
   }                                                                                                     \
   }

@@ -110,7 +110,6 @@ struct grim_handle {
   cudaStream_t ioUp = nullptr, ioDown = nullptr;
   cudaEvent_t ioEv[8];  // [0,2) upload done, [2,4) input consumed, [4,6) output staged, [6,8) download done
   bool ioReady = false;
-  bool separateFinish = false;  // GRIM_DEBUG_SEPARATE_FINISH
   bool profOn = false;
   std::vector<cudaEvent_t> profEv;
   std::vector<int> profGroup;
@@ -359,29 +358,12 @@ static bool newton_counts_nan(const grim_handle* h) {
   return h->cfg.problem == GRIM_PROBLEM_TORUS && !is_fd(h) && h->cfg.perZoneConvergence != 2;
 }
 
-// the step's per-zone mixed Newton finishes its zones itself (the stage
-// finish then covers the ghost zones only): ideal MHD, one launch over the
-// whole interior
-static bool fused_finish(const grim_handle* h) {
-  return !h->separateFinish && !is_fd(h) && h->cfg.perZoneConvergence == 1 &&
-         h->cfg.newtonMode == GRIM_NEWTON_MIXED32 && !h->dc.conduction && !h->dc.viscosity;
-}
-
 // returns whether the launch counts the NaN zones (countNan asked for it
-// and the Newton form does it); with fuse (the step's stages) and
-// fused_finish, the Newton also finishes the stage's interior zones
-static bool enqueue_newton(grim_handle* h, int stage, bool guessOld = false, bool countNan = false,
-                           bool fuse = false) {
+// and the Newton form does it)
+static bool enqueue_newton(grim_handle* h, int stage, bool guessOld = false, bool countNan = false) {
   const DevCfg& c = h->dc;
   cudaStream_t s = h->stream;
   StageBufs b = stage_bufs(h, stage, guessOld);
-  if (fuse && fused_finish(h)) {
-    b.fin = (stage == GRIM_HALF_STEP) ? h->primHalf : h->primOld;
-    b.finFloor = h->cfg.problem == GRIM_PROBLEM_TORUS ? 1 : 0;
-    b.finPost = (stage == GRIM_FULL_STEP) ? 1 : 0;
-    b.finDtOn = (stage == GRIM_FULL_STEP && h->cfg.elemOldFromFullStep) ? 1 : 0;
-    if (b.finDtOn) cudaMemsetAsync(&h->st->maxInvDt, 0, sizeof(double), s);
-  }
   PROF(GRIM_PROF_NEWTON);
   countNan = countNan && newton_counts_nan(h);
   if (countNan) {
@@ -471,18 +453,13 @@ static void enqueue_pre_half(grim_handle* h, bool timed) {
   if (timed) cudaEventRecord(h->ev[1], s);
 }
 
-// primHalfStep = prim, communicate, halfStepDiagnostics as one pass (the
-// ghost zones only when the Newton finished the interior)
-static void enqueue_mid_finish(grim_handle* h, bool fused = false) {
+// primHalfStep = prim, communicate, halfStepDiagnostics as one pass
+static void enqueue_mid_finish(grim_handle* h) {
   const DevCfg& c = h->dc;
   PROF(GRIM_PROF_COPY);
   const bool torus = h->cfg.problem == GRIM_PROBLEM_TORUS;
   const double* geoC = h->cfg.metric == GRIM_MINKOWSKI ? nullptr : h->geo[GRIM_CENTER];
-  if (fused) {
-    grim::fast::stage_finish_ghosts(c, h->prim, h->primHalf, geoC, torus, false, 0, h->st, h->stream);
-  } else {
-    KNS_CALL(h, stage_finish, c, h->prim, h->primHalf, geoC, torus, false, nullptr, 0, h->st, h->stream);
-  }
+  KNS_CALL(h, stage_finish, c, h->prim, h->primHalf, geoC, torus, false, nullptr, 0, h->st, h->stream);
   g_launch_counter++;
 }
 // the full stage's boundaries on primHalfStep
@@ -494,8 +471,8 @@ static void enqueue_mid_fill(grim_handle* h) {
   }
   enqueue_problem_bcs(h, h->primHalf);
 }
-static void enqueue_mid(grim_handle* h, bool fused = false) {
-  enqueue_mid_finish(h, fused);
+static void enqueue_mid(grim_handle* h) {
+  enqueue_mid_finish(h);
   enqueue_mid_fill(h);
 }
 
@@ -534,21 +511,16 @@ static void enqueue_post_count(grim_handle* h, bool nanCounted) {
     g_launch_counter++;
   }
 }
-static void enqueue_post_finish(grim_handle* h, bool timed, bool fused = false) {
+static void enqueue_post_finish(grim_handle* h, bool timed) {
   const DevCfg& c = h->dc;
   cudaStream_t s = h->stream;
   const bool torus = h->cfg.problem == GRIM_PROBLEM_TORUS;
   {
     PROF(GRIM_PROF_COPY);
     const int dtOn = h->cfg.elemOldFromFullStep ? 1 : 0;
+    if (dtOn) cudaMemsetAsync(&h->st->maxInvDt, 0, sizeof(double), s);
     const double* geoC = h->cfg.metric == GRIM_MINKOWSKI ? nullptr : h->geo[GRIM_CENTER];
-    if (fused) {
-      // the full-stage Newton zeroed maxInvDt and finished the interior
-      grim::fast::stage_finish_ghosts(c, h->prim, h->primOld, geoC, torus, true, dtOn, h->st, s);
-    } else {
-      if (dtOn) cudaMemsetAsync(&h->st->maxInvDt, 0, sizeof(double), s);
-      KNS_CALL(h, stage_finish, c, h->prim, h->primOld, geoC, torus, true, &h->st->nanFlag, dtOn, h->st, s);
-    }
+    KNS_CALL(h, stage_finish, c, h->prim, h->primOld, geoC, torus, true, &h->st->nanFlag, dtOn, h->st, s);
     g_launch_counter++;
   }
   if (h->cfg.ObserveEveryDt > 0.) {
@@ -560,9 +532,9 @@ static void enqueue_post_finish(grim_handle* h, bool timed, bool fused = false) 
   }
   if (timed) cudaEventRecord(h->ev[7], s);
 }
-static void enqueue_post(grim_handle* h, bool timed, bool nanCounted = false, bool fused = false) {
+static void enqueue_post(grim_handle* h, bool timed, bool nanCounted = false) {
   enqueue_post_count(h, nanCounted);
-  enqueue_post_finish(h, timed, fused);
+  enqueue_post_finish(h, timed);
 }
 
 // the step in the four segments of a slab-decomposed run (grim_step_segment)
@@ -585,19 +557,18 @@ static void enqueue_segment(grim_handle* h, int seg) {
 
 static void enqueue_step(grim_handle* h, bool timed) {
   cudaStream_t s = h->stream;
-  const bool fused = fused_finish(h);
   enqueue_pre_half(h, timed);
   enqueue_stencil(h, GRIM_HALF_STEP, step_guess_old(h));
   if (timed) cudaEventRecord(h->ev[2], s);
-  enqueue_newton(h, GRIM_HALF_STEP, step_guess_old(h), false, true);
+  enqueue_newton(h, GRIM_HALF_STEP, step_guess_old(h));
   if (timed) cudaEventRecord(h->ev[3], s);
-  enqueue_mid(h, fused);
+  enqueue_mid(h);
   if (timed) cudaEventRecord(h->ev[4], s);
   enqueue_stencil(h, GRIM_FULL_STEP);
   if (timed) cudaEventRecord(h->ev[5], s);
-  const bool nanCounted = enqueue_newton(h, GRIM_FULL_STEP, false, true, true);
+  const bool nanCounted = enqueue_newton(h, GRIM_FULL_STEP, false, true);
   if (timed) cudaEventRecord(h->ev[6], s);
-  enqueue_post(h, timed, nanCounted, fused);
+  enqueue_post(h, timed, nanCounted);
 }
 
 // ---------------------------------------------------------------------------
@@ -1963,9 +1934,8 @@ int grim_synchronize(grim_handle* h) {
 
 int grim_set_debug(grim_handle* h, int setting, int value) {
   if (!h) return GRIM_EINVAL;
-  if (setting == GRIM_DEBUG_SKIP_BULK_COPIES) h->dc.dbgSkipCopies = value != 0;
-  else if (setting == GRIM_DEBUG_SEPARATE_FINISH) h->separateFinish = value != 0;
-  else { set_err("grim_set_debug: unknown setting %d", setting); return GRIM_EINVAL; }
+  if (setting != GRIM_DEBUG_SKIP_BULK_COPIES) { set_err("grim_set_debug: unknown setting %d", setting); return GRIM_EINVAL; }
+  h->dc.dbgSkipCopies = value != 0;
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
   return GRIM_OK;
 }

@@ -52,12 +52,6 @@ struct StageBufs {
   unsigned long long* nanCount;  // non-null: the per-zone Newton adds the zones whose result (fluid and field
                                  // rows) holds a NaN (fullStepDiagnostics' count of the full stage)
   int* list[2];           // compacted Newton worklists (interior zone indices)
-  // non-null: the per-zone mixed Newton also finishes its zone into fin
-  // (the stage finish: copy, torus floors when finFloor, the next dt term
-  // when finDtOn and the non-finite count when finPost); the ghost zones
-  // are left to stage_finish_ghosts
-  double* fin;
-  int finFloor, finPost, finDtOn;
 };
 
 // one problem of a ragged batch: its configuration, its stage buffers

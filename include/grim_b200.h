@@ -344,11 +344,8 @@ int grim_synchronize(grim_handle* h);
  * still has in flight; if one of those does not land either
  * (grim_stats.drainTimeouts), destroy the handle. */
 enum {
-  GRIM_DEBUG_SKIP_BULK_COPIES = 1, /* value != 0: the TMA-staged face kernels
+  GRIM_DEBUG_SKIP_BULK_COPIES = 1  /* value != 0: the TMA-staged face kernels
                                       issue no copies, so their waits run out */
-  GRIM_DEBUG_SEPARATE_FINISH = 2   /* value != 0: the step finishes each stage
-                                      in a pass of its own instead of in the
-                                      per-zone mixed Newton (same results) */
 };
 /* test hook: set a debug setting; no counterpart in the reference */
 int grim_set_debug(grim_handle* h, int setting, int value);
