@@ -65,7 +65,7 @@ def _worker(rank, world, port, periodic, out):
 def test_halo_wiring_gloo(world, periodic):
     """recv_lo holds the lower neighbour's high interior planes, recv_hi the
     upper neighbour's low ones; physical ends receive nothing."""
-    out = mp.Manager().dict()
+    out = mp.get_context("spawn").Manager().dict()
     mp.start_processes(_worker, args=(world, _free_port(), periodic, out), nprocs=world, start_method="spawn")
     for r in range(world):
         lower, upper = slab.neighbours(r, world, periodic)
@@ -105,7 +105,7 @@ def _obs_worker(rank, world, port, out):
 def test_observer_rows_gathered_over_gloo():
     """Two ranks gather each other's observer records in rank order and
     agree on the combined values."""
-    out = mp.Manager().dict()
+    out = mp.get_context("spawn").Manager().dict()
     mp.start_processes(_obs_worker, args=(2, _free_port(), out), nprocs=2, start_method="spawn")
     for r in range(2):
         got = np.array(out[r])
