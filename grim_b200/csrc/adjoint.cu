@@ -1,27 +1,35 @@
 // adjoint.cu -- reverse (adjoint) sweep of whole implicit timesteps.
 //
 // The forward step (timestep.cpp:3-334) is, per stage with dt' = dt/2 then
-// dt, the implicit system R(P) = (U(P; B) - U(P0)) / dt' + divF(Ps) = 0 for
-// the fluid unknowns, with B = B0 - dt' divF_B(Ps) advanced explicitly and
-// Ps = P0 (half stage) or Ph (full stage).  Given lambda = dL/dP1 at the end
-// of a step, the adjoint of the step is (implicit-function theorem, so the
-// Newton iterations are not differentiated; they are converged):
+// dt, the implicit system R(P) = (U(P; B) - U(P0)) / dt' + divF(Ps) +
+// S(Ps) = 0 for the fluid unknowns (S: the geometric source, zero in
+// Minkowski), with the field advanced explicitly, sqrt(-g) B = sqrt(-g) B0
+// - dt' divF_B(Ps), and Ps = P0 (half stage) or Ph (full stage).  Given
+// lambda = dL/dP1 at the end of a step, the adjoint of the step is
+// (implicit-function theorem, so the Newton iterations are not
+// differentiated; they are converged):
 //
 //   full stage at P1:  mu = (dU/dPf / dt)^-T lambda_f
 //                      beta = lambda_B - (dU/dB / dt)^T mu
-//                      g_h = [-mu ; -dt beta]      (= dL/d divF(Ph))
-//   lambda_h = D(Ph)^T g_h                          (stencil VJP, ghosts folded)
-//   half stage at Ph:  mu_h, beta_h likewise with dt/2, g_0 = [-mu_h ; -dt/2 beta_h]
-//   lambda_0 = D(P0)^T g_0 + dU(P0)/dP^T (mu/dt + mu_h/(dt/2)) + [0 ; beta + beta_h]
+//                      g_h = [-mu ; -dt / sqrt(-g) beta]   (= dL/d divF(Ph))
+//   lambda_h = D(Ph)^T g_h + dS/dP(Ph)^T g_h,fluid   (stencil VJP, ghosts folded)
+//   half stage at Ph:  mu_h, beta_h likewise with dt/2, g_0 = [-mu_h ; -dt/2 / sqrt(-g) beta_h]
+//   lambda_0 = D(P0)^T g_0 + dS/dP(P0)^T g_0,fluid
+//              + dU(P0)/dP^T (mu/dt + mu_h/(dt/2)) + [0 ; beta + beta_h]
 //
 // D^T is the transpose of the stencil: divergence (fvmfluxes.cpp:36-45),
 // flux-CT / EMF (constrainedtransport.cpp:3-83), Riemann solver
-// (riemannsolver.cpp:202-328) and reconstruction, the last two through
-// local Jacobians taken with the forward-tangent scalar on the same
-// templated physics the kernels run.  Scope: ideal MHD, Minkowski, 2D or
-// 3D, periodic in every direction, dt held fixed over the run; the runtime
-// rejects anything else.  Every accumulation is a gather in a fixed order
-// (no atomics), so a gradient is the same bits run to run.
+// (riemannsolver.cpp:202-328) with the face metric, reconstruction, and the
+// ghost fill (boundary.cpp:5-241 and grid::communicate: every ghost zone
+// copies the interior zone that the periodic / outflow / mirror map of each
+// direction selects, so its adjoint goes back to that zone); the Riemann
+// solver, the reconstruction, the conserved variables and the geometric
+// source (physics.cpp:360-420) through local Jacobians taken with the
+// forward-tangent scalar on the same templated physics the kernels run.
+// Scope: ideal MHD, Minkowski or modified Kerr-Schild, 2D or 3D, periodic /
+// outflow / mirror boundaries, no problem hooks, dt held fixed over the
+// run; the runtime rejects anything else.  Every accumulation is a gather
+// in a fixed order (no atomics), so a gradient is the same bits run to run.
 #include <cuda_runtime.h>
 
 #include "launch.h"
@@ -85,16 +93,33 @@ GRIM_D void solve5(double A[5][5], double b[5], double x[5]) {
   }
 }
 
+// the zone's geometry as constants of the tangent scalar
+template <class D>
+GRIM_D void geo_const(ZoneGeo<D>& Gd, const ZoneGeo<double>& G) {
+  for (int m = 0; m < 4; m++)
+    for (int n = 0; n < 4; n++) { Gd.gcov[m][n] = D(G.gcov[m][n]); Gd.gcon[m][n] = D(G.gcon[m][n]); }
+  Gd.g = D(G.g); Gd.alpha = D(G.alpha); Gd.ialpha = D(G.ialpha);
+  Gd.x1 = D(G.x1); Gd.x2 = D(G.x2); Gd.dyn = D(G.dyn);
+}
+
+// the centre geometry of zone z
+GRIM_D void centre_geo(const DevCfg& c, const double* geoC, long long z, ZoneGeo<double>& G) {
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  load_geo(G, c, geoC, z, i, j, 0.5, 0.5);
+}
+
 // conserved fluid rows U (nf = 5) of one zone and their Jacobian with
-// respect to the 8 primitives (5 fluid, then B), Minkowski
-GRIM_D void cons_jacobian(const DevCfg& c, const double* p, long long z, double J[5][8]) {
+// respect to the 8 primitives (5 fluid, then B)
+GRIM_D void cons_jacobian(const DevCfg& c, const double* p, long long z, const ZoneGeo<double>& G0,
+                          double J[5][8]) {
   typedef Dual<double, 8> D;
   const long long Z = c.Z;
   D q[8];
   for (int v = 0; v < 5; v++) q[v] = D::var(p[(long long)v * Z + z], v);
   for (int v = 0; v < 3; v++) q[5 + v] = D::var(p[(long long)(c.B1 + v) * Z + z], 5 + v);
   ZoneGeo<D> G;
-  geo_minkowski<D>(G, D(0.), D(0.));
+  geo_const(G, G0);
   ElemT<D, D> e;
   elem_set<0, 0>(e, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], D(0.), D(0.), G, c);
   D U[5];
@@ -105,14 +130,17 @@ GRIM_D void cons_jacobian(const DevCfg& c, const double* p, long long z, double 
 
 // Stage adjoint at the stage's solution P (interior zones): lam -> g (dL/d
 // divF, dof rows), ubar (+)= mu / dt', bacc (+)= beta
-__global__ void k_stage(DevCfg c, const double* __restrict__ P, double dtp, const double* __restrict__ lam,
-                        double* __restrict__ g, double* __restrict__ ubar, double* __restrict__ bacc, int accumulate) {
+__global__ void k_stage(DevCfg c, const double* __restrict__ geoC, const double* __restrict__ P, double dtp,
+                        const double* __restrict__ lam, double* __restrict__ g, double* __restrict__ ubar,
+                        double* __restrict__ bacc, int accumulate) {
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= c.Zint) return;
   const long long Z = c.Z;
   const long long z = interior_to_z(c, n);
+  ZoneGeo<double> G;
+  centre_geo(c, geoC, z, G);
   double J[5][8];
-  cons_jacobian(c, P, z, J);
+  cons_jacobian(c, P, z, G, J);
   // (J_ff / dt')^T mu = lam_f
   double AT[5][5], b[5], mu[5];
   for (int r = 0; r < 5; r++) {
@@ -128,26 +156,67 @@ __global__ void k_stage(DevCfg c, const double* __restrict__ P, double dtp, cons
   for (int k = 0; k < 3; k++) {
     double beta = lam[(long long)(c.B1 + k) * Z + z];
     for (int r = 0; r < 5; r++) beta -= J[r][5 + k] / dtp * mu[r];
-    g[(long long)(c.B1 + k) * Z + z] = -dtp * beta;
+    g[(long long)(c.B1 + k) * Z + z] = -dtp / G.g * beta;
     bacc[(long long)k * Z + z] = accumulate ? bacc[(long long)k * Z + z] + beta : beta;
   }
 }
 
 // lam_out(P0) += dU/dP(P0)^T ubar + [0 ; bacc]
-__global__ void k_cons(DevCfg c, const double* __restrict__ P, const double* __restrict__ ubar,
-                       const double* __restrict__ bacc, double* __restrict__ lam) {
+__global__ void k_cons(DevCfg c, const double* __restrict__ geoC, const double* __restrict__ P,
+                       const double* __restrict__ ubar, const double* __restrict__ bacc, double* __restrict__ lam) {
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= c.Zint) return;
   const long long Z = c.Z;
   const long long z = interior_to_z(c, n);
+  ZoneGeo<double> G;
+  centre_geo(c, geoC, z, G);
   double J[5][8];
-  cons_jacobian(c, P, z, J);
+  cons_jacobian(c, P, z, G, J);
   for (int k = 0; k < 8; k++) {
     double s = 0.;
     for (int r = 0; r < 5; r++) s += J[r][k] * ubar[(long long)r * Z + z];
     if (k >= 5) s += bacc[(long long)(k - 5) * Z + z];
     const long long row = (k < 5) ? k : c.B1 + (k - 5);
     lam[row * Z + z] += s;
+  }
+}
+
+// The geometric source's transpose (interior zones): out += dS/dP(Ps)^T g
+// over the fluid rows, S^nu = -sqrt(-g) T^ka_la Gamma^la_(ka nu) of the
+// stage element at the centre (physics.cpp:360-420)
+__global__ void k_src_t(DevCfg c, const double* __restrict__ geoC, const double* __restrict__ gamma,
+                        const double* __restrict__ P, const double* __restrict__ g, double* __restrict__ out) {
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= c.Zint) return;
+  typedef Dual<double, 8> D;
+  const long long Z = c.Z;
+  const long long z = interior_to_z(c, n);
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  ZoneGeo<double> G0;
+  load_geo(G0, c, geoC, z, i, j, 0.5, 0.5);
+  ZoneGeo<D> G;
+  geo_const(G, G0);
+  D q[8];
+  for (int v = 0; v < 5; v++) q[v] = D::var(P[(long long)v * Z + z], v);
+  for (int v = 0; v < 3; v++) q[5 + v] = D::var(P[(long long)(c.B1 + v) * Z + z], 5 + v);
+  ElemT<D, D> e;
+  elem_set<0, 0>(e, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], D(0.), D(0.), G, c);
+  D T[4][4];
+  for (int ka = 0; ka < 4; ka++)
+    for (int la = 0; la < 4; la++) T[ka][la] = tmunu<0, 0>(e, ka, la);
+  const double* gam = gamma + gidx(c, i, j);
+  double acc[8] = {0., 0., 0., 0., 0., 0., 0., 0.};
+  for (int nu = 0; nu < 4; nu++) {
+    D s(0.);
+    for (int ka = 0; ka < 4; ka++)
+      for (int la = 0; la < 4; la++) s -= T[ka][la] * (G0.g * __ldg(gam + (long long)(la * 16 + ka * 4 + nu) * c.GZ));
+    const double gb = g[(long long)(UU + nu) * Z + z];
+    for (int m = 0; m < 8; m++) acc[m] += s.d[m] * gb;
+  }
+  for (int m = 0; m < 8; m++) {
+    const long long row = (m < 5) ? m : c.B1 + (m - 5);
+    out[row * Z + z] += acc[m];
   }
 }
 
@@ -247,9 +316,9 @@ __global__ void k_ct_t_raw(DevCfg c, const double* __restrict__ ebar, double* __
 
 // the Riemann flux of one face (riemannsolver.cpp:202-328) on any scalar
 template <class S>
-GRIM_D void riemann_flux(const DevCfg& c, int dir, const S* pl, const S* pr, S* F) {
+GRIM_D void riemann_flux(const DevCfg& c, int dir, const ZoneGeo<double>& G0, const S* pl, const S* pr, S* F) {
   ZoneGeo<S> G;
-  geo_minkowski<S>(G, S(0.), S(0.));
+  geo_const(G, G0);
   const int fd = dir + 1;
   S FL[8], UL[8], FR[8], UR[8], mnL, mxL, mnR, mxR;
   {
@@ -284,8 +353,8 @@ GRIM_D void riemann_flux(const DevCfg& c, int dir, const S* pl, const S* pr, S* 
 // reconstructed states, gl = (dF/dpl)^T Fbar (pl: the right-face state of a)
 // and gr = (dF/dpr)^T Fbar (pr: the left-face state of b), into gface
 // (rows 0..7 gl, 8..15 gr; zero on the faces the stencil does not use)
-__global__ void k_faces_t(DevCfg c, int dir, const double* __restrict__ P, const double* __restrict__ Ft,
-                          double* __restrict__ gface) {
+__global__ void k_faces_t(DevCfg c, int dir, const double* __restrict__ geoF, const double* __restrict__ P,
+                          const double* __restrict__ Ft, double* __restrict__ gface) {
   long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (z >= c.Z) return;
   int i, j, k;
@@ -313,6 +382,9 @@ __global__ void k_faces_t(DevCfg c, int dir, const double* __restrict__ P, const
     pl[v] = ro;
     pr[v] = lo2;
   }
+  // the face metric (the X3 faces of the axisymmetric metrics: the centre's)
+  ZoneGeo<double> G;
+  load_geo(G, c, geoF, z, i, j, dir == 0 ? 0. : 0.5, dir == 1 ? 0. : 0.5);
   // dF/dpl and dF/dpr, 8 tangent lanes each
   typedef Dual<double, 8> D8;
   for (int side = 0; side < 2; side++) {
@@ -321,7 +393,7 @@ __global__ void k_faces_t(DevCfg c, int dir, const double* __restrict__ P, const
       L[v] = side == 0 ? D8::var(pl[v], v) : D8(pl[v]);
       R[v] = side == 1 ? D8::var(pr[v], v) : D8(pr[v]);
     }
-    riemann_flux<D8>(c, dir, L, R, F);
+    riemann_flux<D8>(c, dir, G, L, R, F);
     for (int k2 = 0; k2 < 8; k2++) {
       double acc = 0.;
       for (int r = 0; r < 8; r++) acc += fb[r] * F[r].d[k2];
@@ -368,8 +440,37 @@ __global__ void k_recon_t(DevCfg c, int dir, const double* __restrict__ P, const
   }
 }
 
-// ghosts are periodic images of interior zones: every interior zone
-// gathers the adjoints of itself and of its images
+// The ghost fill's transpose: every ghost zone copies the interior zone
+// that each direction's map selects (periodic: the wrapped image; outflow:
+// the first / last interior zone; mirror: the reflected zone), so every
+// interior zone gathers the adjoints of itself and of the ghost zones that
+// copy it: per direction the positions y with map(y) = x, in a fixed order.
+GRIM_D int preimages(int x, int g, int N, int NT, int lo, int hi, int* ys) {
+  int n = 0;
+  ys[n++] = x;
+  if (NT == 1) return n;
+  // a direction with a periodic side wraps both (grid::communicate's
+  // periodic DMDA; the boundary fill then leaves that direction alone)
+  const bool per = lo == GRIM_PERIODIC || hi == GRIM_PERIODIC;
+  // the lower ghosts y < g
+  if (per) {
+    if (x - N >= 0 && x - N < g) ys[n++] = x - N;
+  } else if (lo == GRIM_MIRROR) {
+    if (x < 2 * g) ys[n++] = 2 * g - 1 - x;
+  } else if (x == g) {
+    for (int y = 0; y < g; y++) ys[n++] = y;
+  }
+  // the upper ghosts y >= N + g
+  if (per) {
+    if (x + N >= N + g && x + N < NT) ys[n++] = x + N;
+  } else if (hi == GRIM_MIRROR) {
+    if (x >= N) ys[n++] = 2 * (N + g) - 1 - x;
+  } else if (x == N + g - 1) {
+    for (int y = N + g; y < NT; y++) ys[n++] = y;
+  }
+  return n;
+}
+
 __global__ void k_fold(DevCfg c, const double* __restrict__ q, double* __restrict__ out) {
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= c.Zint) return;
@@ -377,22 +478,15 @@ __global__ void k_fold(DevCfg c, const double* __restrict__ q, double* __restric
   const long long z = interior_to_z(c, n);
   int i, j, k;
   zijk(c, z, i, j, k);
-  const int kr = c.dim >= 3 ? 1 : 0;
+  int ys1[8], ys2[8], ys3[8];
+  const int n1 = preimages(i, c.g1, c.N1, c.N1T, c.bc[0], c.bc[1], ys1);
+  const int n2 = c.dim >= 2 ? preimages(j, c.g2, c.N2, c.N2T, c.bc[2], c.bc[3], ys2) : (ys2[0] = j, 1);
+  const int n3 = c.dim >= 3 ? preimages(k, c.g3, c.N3, c.N3T, c.bc[4], c.bc[5], ys3) : (ys3[0] = k, 1);
   for (int v = 0; v < c.dof; v++) {
     double s = 0.;
-    for (int a = -1; a <= 1; a++) {
-      const int ii = i + a * c.N1;
-      if (ii < 0 || ii >= c.N1T) continue;
-      for (int b = -1; b <= 1; b++) {
-        const int jj = j + b * c.N2;
-        if (jj < 0 || jj >= c.N2T) continue;
-        for (int m = -kr; m <= kr; m++) {
-          const int kk = k + m * c.N3;
-          if (kk < 0 || kk >= c.N3T) continue;
-          s += q[(long long)v * Z + zidx(c, ii, jj, kk)];
-        }
-      }
-    }
+    for (int a = 0; a < n1; a++)
+      for (int b = 0; b < n2; b++)
+        for (int m = 0; m < n3; m++) s += q[(long long)v * Z + zidx(c, ys1[a], ys2[b], ys3[m])];
     out[(long long)v * Z + z] = s;
   }
 }
@@ -413,8 +507,8 @@ void adjoint_zero_ghosts(const DevCfg& c, double* a, cudaStream_t s) {
   k_zero_ghosts<<<adj::nblk(c.Z, 256), 256, 0, s>>>(c, a);
 }
 
-void adjoint_stencil_t(const DevCfg& c, const double* P, const double* g, double* Ft, double* ebar, double* q,
-                       double* gface, double* out, cudaStream_t s) {
+void adjoint_stencil_t(const DevCfg& c, const AdjointGeo& geo, const double* P, const double* g, double* Ft,
+                       double* ebar, double* q, double* gface, double* out, cudaStream_t s) {
   using namespace adj;
   const size_t bZ = (size_t)c.Z * sizeof(double);
   k_div_t<<<nblk(c.Z, 128), 128, 0, s>>>(c, g, Ft);
@@ -422,22 +516,24 @@ void adjoint_stencil_t(const DevCfg& c, const double* P, const double* g, double
   k_ct_t_raw<<<nblk(c.Z, 256), 256, 0, s>>>(c, ebar, Ft);
   cudaMemsetAsync(q, 0, (size_t)c.dof * bZ, s);
   for (int d = 0; d < c.dim; d++) {
-    k_faces_t<<<nblk(c.Z, 64), 64, 0, s>>>(c, d, P, Ft, gface);
+    k_faces_t<<<nblk(c.Z, 64), 64, 0, s>>>(c, d, geo.geoF[d], P, Ft, gface);
     k_recon_t<<<nblk(c.Z, 64), 64, 0, s>>>(c, d, P, gface, q);
   }
   k_fold<<<nblk(c.Zint, 128), 128, 0, s>>>(c, q, out);
 }
 
-void adjoint_step(const DevCfg& c, double dt, const double* P0, const double* Ph, const double* P1, double* lam,
-                  const AdjointBufs& w, cudaStream_t s) {
+void adjoint_step(const DevCfg& c, const AdjointGeo& geo, double dt, const double* P0, const double* Ph,
+                  const double* P1, double* lam, const AdjointBufs& w, cudaStream_t s) {
   using namespace adj;
   // full stage at P1
-  k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, P1, dt, lam, w.g, w.ubar, w.bacc, 0);
-  adjoint_stencil_t(c, Ph, w.g, w.Ft, w.ebar, w.q, w.gface, w.lamh, s);
+  k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, geo.geoC, P1, dt, lam, w.g, w.ubar, w.bacc, 0);
+  adjoint_stencil_t(c, geo, Ph, w.g, w.Ft, w.ebar, w.q, w.gface, w.lamh, s);
+  if (geo.gamma) k_src_t<<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, geo.gamma, Ph, w.g, w.lamh);
   // half stage at Ph
-  k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, Ph, 0.5 * dt, w.lamh, w.g, w.ubar, w.bacc, 1);
-  adjoint_stencil_t(c, P0, w.g, w.Ft, w.ebar, w.q, w.gface, lam, s);
-  k_cons<<<nblk(c.Zint, 128), 128, 0, s>>>(c, P0, w.ubar, w.bacc, lam);
+  k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, geo.geoC, Ph, 0.5 * dt, w.lamh, w.g, w.ubar, w.bacc, 1);
+  adjoint_stencil_t(c, geo, P0, w.g, w.Ft, w.ebar, w.q, w.gface, lam, s);
+  if (geo.gamma) k_src_t<<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, geo.gamma, P0, w.g, lam);
+  k_cons<<<nblk(c.Zint, 128), 128, 0, s>>>(c, geo.geoC, P0, w.ubar, w.bacc, lam);
 }
 
 }  // namespace grim

@@ -32,17 +32,6 @@ constexpr bool kFastMath = true;   // reassociated arithmetic allowed (fast path
 constexpr bool kFastMath = false;  // the reference's operation order (parity path)
 #endif
 
-GRIM_D double zone_x1(const DevCfg& c, int i, double o) { return c.X1Start + ((double)(i - c.g1) + o) * c.dX[0]; }
-GRIM_D double zone_x2(const DevCfg& c, int j, double o) { return c.X2Start + ((double)(j - c.g2) + o) * c.dX[1]; }
-
-template <class R>
-GRIM_D void load_geo(ZoneGeo<R>& G, const DevCfg& c, const double* geo, long long z, int i, int j, double o1,
-                     double o2) {
-  if (geo == nullptr)
-    geo_minkowski<R>(G, (R)zone_x1(c, i, o1), (R)zone_x2(c, j, o2));
-  else
-    geo_load<R>(G, geo, c.GZ, gidx(c, i, j));
-}
 
 // ---------------------------------------------------------------------------
 // ghost fill: composite gather (every ghost zone reads the interior zone

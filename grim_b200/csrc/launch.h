@@ -61,12 +61,19 @@ struct AdjointBufs {
   double* ubar;  // nf x Z: dL/dU(P0)
   double* bacc;  // 3 x Z: dL/dB0 through the induction
 };
+// the geometry the adjoint reads (all null in Minkowski)
+struct AdjointGeo {
+  const double* geoC;     // centre planes
+  const double* geoF[3];  // face planes per direction (X3: the centre's)
+  const double* gamma;    // centre Christoffel planes
+};
 // lam (dL/dP1, interior) -> dL/dP0 for one step of fixed dt
-void adjoint_step(const DevCfg& c, double dt, const double* P0, const double* Ph, const double* P1, double* lam,
-                  const AdjointBufs& w, cudaStream_t s);
+void adjoint_step(const DevCfg& c, const AdjointGeo& geo, double dt, const double* P0, const double* Ph,
+                  const double* P1, double* lam, const AdjointBufs& w, cudaStream_t s);
 void adjoint_zero_ghosts(const DevCfg& c, double* a, cudaStream_t s);
-void adjoint_stencil_t(const DevCfg& c, const double* P, const double* g, double* Ft, double* ebar, double* q,
-                       double* gface, double* out, cudaStream_t s);
+// out = D(P)^T g: the transpose of the flux divergence with its ghost fill
+void adjoint_stencil_t(const DevCfg& c, const AdjointGeo& geo, const double* P, const double* g, double* Ft,
+                       double* ebar, double* q, double* gface, double* out, cudaStream_t s);
 }  // namespace grim
 
 namespace grim {

@@ -73,6 +73,21 @@ GRIM_D void geo_load(ZoneGeo<R>& G, const double* __restrict__ geo, long long Z,
   G.dyn = (R)__ldg(geo + 36LL * Z + z);
 }
 
+GRIM_D double zone_x1(const DevCfg& c, int i, double o) { return c.X1Start + ((double)(i - c.g1) + o) * c.dX[0]; }
+GRIM_D double zone_x2(const DevCfg& c, int j, double o) { return c.X2Start + ((double)(j - c.g2) + o) * c.dX[1]; }
+
+// the geometry of zone (i, j) (any k) at offsets (o1, o2) in zone widths:
+// Minkowski when geo is null, else the stored plane of that location
+template <class R>
+GRIM_D void load_geo(ZoneGeo<R>& G, const DevCfg& c, const double* geo, long long z, int i, int j, double o1,
+                     double o2) {
+  (void)z;
+  if (geo == nullptr)
+    geo_minkowski<R>(G, (R)zone_x1(c, i, o1), (R)zone_x2(c, j, o2));
+  else
+    geo_load<R>(G, geo, c.GZ, gidx(c, i, j));
+}
+
 template <class S, class R>
 struct ElemT {
   S rho, u, u1, u2, u3, pressure, temperature, soundSpeed, gam;

@@ -1574,15 +1574,27 @@ int grim_set_dt_mode(grim_handle* h, int fixed) {
 
 static int adjoint_scope(grim_handle* h) {
   const grim_config& c = h->cfg;
-  const bool periodic = c.boundaryLeft == GRIM_PERIODIC && c.boundaryRight == GRIM_PERIODIC &&
-                        c.boundaryBottom == GRIM_PERIODIC && c.boundaryTop == GRIM_PERIODIC &&
-                        (c.dim < 3 || (c.boundaryFront == GRIM_PERIODIC && c.boundaryBack == GRIM_PERIODIC));
-  if ((c.dim != 2 && c.dim != 3) || c.metric != GRIM_MINKOWSKI || c.conduction || c.viscosity || !periodic ||
-      c.problem != GRIM_PROBLEM_NONE || c.N3Global > 0) {
-    set_err("adjoint: supported for 2D and 3D ideal MHD in Minkowski with periodic boundaries only");
+  auto ok_bc = [](int b) { return b == GRIM_PERIODIC || b == GRIM_OUTFLOW || b == GRIM_MIRROR; };
+  const bool bcs = ok_bc(c.boundaryLeft) && ok_bc(c.boundaryRight) && ok_bc(c.boundaryBottom) &&
+                   ok_bc(c.boundaryTop) && (c.dim < 3 || (ok_bc(c.boundaryFront) && ok_bc(c.boundaryBack)));
+  if ((c.dim != 2 && c.dim != 3) || c.conduction || c.viscosity || !bcs || c.problem != GRIM_PROBLEM_NONE ||
+      c.N3Global > 0) {
+    set_err("adjoint: supported for 2D and 3D ideal MHD (Minkowski or MKS) with periodic, outflow or mirror "
+            "boundaries and no problem hooks only");
     return GRIM_ENOTSUP;
   }
   return GRIM_OK;
+}
+
+static grim::AdjointGeo adjoint_geo(const grim_handle* h) {
+  grim::AdjointGeo g;
+  const bool mink = h->cfg.metric == GRIM_MINKOWSKI;
+  g.geoC = mink ? nullptr : h->geo[GRIM_CENTER];
+  g.geoF[0] = mink ? nullptr : h->geo[GRIM_LEFT];
+  g.geoF[1] = mink ? nullptr : h->geo[GRIM_BOTTOM];
+  g.geoF[2] = g.geoC;
+  g.gamma = mink ? nullptr : h->gamma;
+  return g;
 }
 
 // work buffers of the reverse sweep: g, Ft (dim x dof), ebar (3), q,
@@ -1624,7 +1636,7 @@ int grim_adjoint_stencil(grim_handle* h, const double* prim, const double* gbar,
   CK(cudaMemcpyAsync(h->scratch, prim, bytes, in, h->stream));
   CK(cudaMemcpyAsync(w.g, gbar, bytes, in, h->stream));
   CK(cudaMemsetAsync(lam, 0, bytes, h->stream));
-  grim::adjoint_stencil_t(c, h->scratch, w.g, w.Ft, w.ebar, w.q, w.gface, lam, h->stream);
+  grim::adjoint_stencil_t(c, adjoint_geo(h), h->scratch, w.g, w.Ft, w.ebar, w.q, w.gface, lam, h->stream);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, lam, bytes, memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                      h->stream));
@@ -1697,13 +1709,18 @@ int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, in
     // recompute the segment, keeping the states each step's adjoint needs
     for (int t = 0; t < m; t++) {
       CK(cudaMemcpyAsync(h->adjSeg[t], h->primOld, bytes, cudaMemcpyDeviceToDevice, h->stream));
+      // the ghosts of the outflow / mirror sides as the step's own boundary
+      // pass forms them before its stencil reads them (the stored state
+      // holds grid::communicate's zeros there)
+      KNS_CALL(h, ghost_fill, c, h->adjSeg[t], c.dof, h->stream);
       rc = run_steps(h, 1);
       if (rc) return rc;
       CK(cudaMemcpyAsync(h->adjSeg[every + 1 + t], h->primHalf, bytes, cudaMemcpyDeviceToDevice, h->stream));
     }
     CK(cudaMemcpyAsync(h->adjSeg[m], h->primOld, bytes, cudaMemcpyDeviceToDevice, h->stream));
     for (int t = m - 1; t >= 0; t--)
-      grim::adjoint_step(c, dt, h->adjSeg[t], h->adjSeg[every + 1 + t], h->adjSeg[t + 1], lam, w, h->stream);
+      grim::adjoint_step(c, adjoint_geo(h), dt, h->adjSeg[t], h->adjSeg[every + 1 + t], h->adjSeg[t + 1], lam, w,
+                         h->stream);
     CK(cudaGetLastError());
   }
   grim::adjoint_zero_ghosts(c, lam, h->stream);

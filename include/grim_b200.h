@@ -421,8 +421,10 @@ int grim_set_face_variant(grim_handle* h, int dir, int variant);
  * interior zones (ghost entries zero; the ghosts are images of interior
  * zones and their share is folded in).  Each segment between checkpoints
  * is recomputed forward once; the stepper is left at the final state.
- * Supported: 2D and 3D ideal MHD, Minkowski, periodic boundaries
- * (GRIM_ENOTSUP otherwise).  Every accumulation is a gather in a fixed
+ * Supported: 2D and 3D ideal MHD, Minkowski or modified Kerr-Schild
+ * (geometric source, face metric), periodic / outflow / mirror boundaries,
+ * no problem hooks (GRIM_ENOTSUP otherwise: EMHD, the torus problem's
+ * floors, inflow check, pole fix and flux filter).  Every accumulation is a gather in a fixed
  * order (no atomics): a gradient is the same bits run to run and for any
  * checkpoint interval. */
 int grim_set_dt_mode(grim_handle* h, int fixed);

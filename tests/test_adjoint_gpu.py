@@ -7,8 +7,10 @@ the same forward map (dt held fixed, Newton converged to roundoff with the
 exact FP64 tangent Jacobian) at a relative tolerance of 1e-6 in FP64.
 The workload is the ideal-MHD linear-mode problem family of the batched
 adjoint configuration: 2D, Minkowski, periodic, minmod / PPM reconstruction,
-LLF / HLL fluxes, flux-CT, random smooth 1e-2 perturbations; and the same
-in 3D (periodic in all three directions, the three edge EMFs of flux-CT).
+LLF / HLL fluxes, flux-CT, random smooth 1e-2 perturbations; the same in
+3D (periodic in all three directions, the three edge EMFs of flux-CT); and
+the torus grid's metric (modified Kerr-Schild) and boundaries (outflow,
+mirror, periodic) without the torus problem hooks.
 """
 import numpy as np
 import pytest
@@ -122,8 +124,8 @@ def test_adjoint_checkpoint_interval_does_not_change_the_gradient():
 
 
 def test_adjoint_refuses_unsupported_configurations():
-    """The torus (MKS, outflow / mirror boundaries, problem hooks) is outside
-    the adjoint's scope."""
+    """The torus problem hooks (floors, inflow check, pole fix, flux
+    filter) are outside the adjoint's scope."""
     from grim_b200.problems import torus as T
     from grim_b200.timestepper import timeStepper
     ts = timeStepper(T.torus_config(N1=32, N2=16, N3=8))
@@ -259,3 +261,124 @@ def test_adjoint_checkpoint_interval_does_not_change_the_gradient_3d():
     a = _adjoint3(cfg, P, 4, every=1)
     b = _adjoint3(cfg, P, 4, every=3)
     assert np.array_equal(a, b)
+
+
+# ---- modified Kerr-Schild, outflow / mirror / periodic ------------------------
+def _mks_cfg(N1=16, N2=16, N3=8, recon=C.PPM, riemann=C.LOCAL_LAX_FRIEDRICH, **kw):
+    """The torus grid's metric and boundaries (spin 0.9375, MKS with the
+    horizon derefinement and cylindrification, outflow in X1, mirror in X2,
+    periodic in X3) on a small grid out to r = 40, without the torus
+    problem hooks (floors, inflow check, pole fix, flux filter)."""
+    import math
+    from grim_b200.problems import torus as T
+    return T.torus_config(N1=N1, N2=N2, N3=N3, problem=C.PROBLEM_NONE, X1End=math.log(40.), reconstruction=recon,
+                          riemannSolver=riemann, dt=2e-3, maxNonLinearIter=8, nonlinearsolve_atol=0.0, **kw)
+
+
+MKS_BG = np.array([1.0, 0.5, 0.0, 0.0, 0.0, 0.05, 0.02, 0.01])
+
+
+def _mks_state(cfg, seed, amp=1e-2):
+    """rho ~ 1, u ~ 0.5, small velocities and field, smooth in X1, X2, X3"""
+    rng = np.random.default_rng(seed)
+    X1, X2, X3 = C.cell_centers(cfg)
+    bg = MKS_BG
+    P = np.zeros((8,) + X1.shape)
+    for v in range(8):
+        k1, k2, k3 = rng.integers(1, 3, 3)
+        ph = rng.uniform(0, 2 * np.pi, 3)
+        P[v] = bg[v] + amp * (np.sin(2 * np.pi * k1 * X1 / 3. + ph[0]) * np.cos(2 * np.pi * k2 * X2 + ph[1])
+                              * np.cos(k3 * X3 + ph[2]))
+    return P
+
+
+def _mks_stepper(cfg, P):
+    from grim_b200.timestepper import timeStepper
+    ts = timeStepper(cfg)
+    ts.setNewtonMode(C.NEWTON_TANGENT64, 1, 0.0)
+    ts.primOld.setVars(P)
+    ts.primOld.communicate()
+    ts.setTime(0.0, cfg["dt"])
+    ts.setFixedDt(True)
+    return ts
+
+
+def _mks_loss(cfg, P, nsteps):
+    """L = 1/2 sum over the interior of (P_final - background)^2, exactly
+    rounded (the screen of fd_check counts two ulps of L per evaluation)"""
+    from tests.adjoint_harness import energy
+    ts = _mks_stepper(cfg, P)
+    for _ in range(nsteps):
+        ts.timeStep()
+    assert ts.stats()["nonFinite"] == 0
+    return energy(cfg, ts.primOld.getVars(), MKS_BG)
+
+
+def test_stencil_transpose_matches_fd_mks():
+    """The stencil transpose with the face metric and the outflow / mirror /
+    periodic ghost fill of the torus grid, against central differences of
+    <gbar, divF(P)> (ghosts from the boundary fill), screened as above."""
+    import math
+    cfg = _mks_cfg(N1=12, N2=12, N3=6)
+    from grim_b200.timestepper import timeStepper
+    ts = timeStepper(cfg)
+    P = _with_images(ts, _mks_state(cfg, 4))
+    g = cfg["numGhost"]
+    rng = np.random.default_rng(2)
+    gbar = np.zeros_like(P)
+    sl = (slice(None),) + tuple(C.interior_slices(cfg))
+    gbar[sl] = rng.standard_normal(gbar[sl].shape)
+    vjp = ts.adjointStencil(P, gbar)
+
+    def f(Q):
+        return math.fsum((gbar * ts.computeDivOfFluxes(Q)[0]).ravel().tolist())
+
+    def shifted(v, k, j, i, h):
+        Q = P.copy()
+        Q[v, k + g, j + g, i + g] += h
+        return f(_with_images(ts, Q))
+
+    # the boundary zones (whose ghosts copy them) are picked on purpose
+    picks = [(n % 8, int(rng.integers(0, 6)), int(rng.choice([0, 1, 5, 10, 11])), int(rng.choice([0, 4, 11])))
+             for n in range(32)]
+    smooth, bad = fd_check(shifted, f(P), interior(cfg, vjp), picks, float(np.max(np.abs(vjp))))
+    assert not bad, bad
+    assert smooth >= 10, smooth
+
+
+def test_adjoint_matches_central_fd_mks():
+    """Whole checkpointed runs on the torus grid's metric and boundaries
+    (12x12x6, 3 steps, checkpoints every 2): the geometric source's
+    transpose, the face metric, the MKS conserved variables and field
+    update, the outflow / mirror ghost fill.  The grid starts at r = 2.5:
+    from the torus grid's inner edge (inside the horizon) this fluid at
+    rest, with no floors or inflow check, turns non-finite in the first
+    three columns within a step (measured), and the check needs a finite
+    forward map."""
+    import math
+    cfg = _mks_cfg(N1=12, N2=12, N3=6, X1Start=math.log(2.5))
+    P = _mks_state(cfg, 6)
+    nsteps = 3
+    ts = _mks_stepper(cfg, P)
+    ts.adjointForward(nsteps, 2)
+    Pf = ts.primOld.getVars()
+    lam = np.zeros_like(Pf)
+    sl = (slice(None),) + tuple(C.interior_slices(cfg))
+    lam[sl] = Pf[sl] - MKS_BG[:, None, None, None]
+    grad = ts.adjointBackward(lam)
+    g = cfg["numGhost"]
+    gi = interior(cfg, grad)
+    L0 = _mks_loss(cfg, P, nsteps)
+
+    def shifted(v, k, j, i, h):
+        Q = P.copy()
+        Q[v, k + g, j + g, i + g] += h
+        return _mks_loss(cfg, Q, nsteps)
+
+    rng = np.random.default_rng(3)
+    picks = [(n % 8, int(rng.integers(0, 6)), int(rng.choice([0, 1, 6, 10, 11])), int(rng.choice([0, 5, 11])))
+             for n in range(32)]
+    smooth, bad = fd_check(shifted, L0, gi, picks, float(np.max(np.abs(gi))))
+    if bad:
+        raise AssertionError("entries off the central differences: %s" % str(bad))
+    assert smooth >= 10, smooth
