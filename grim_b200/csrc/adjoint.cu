@@ -58,12 +58,51 @@ template <class T, int N>
 GRIM_D bool operator>=(const Dual<T, N>& a, T b) { return a.v >= b; }
 template <class T, int N>
 GRIM_D Dual<T, N> fabs(const Dual<T, N>& a) { return a.v < T(0) ? -a : a; }
+// IEEE fmin / fmax: a NaN argument yields the other one, as on doubles
+// (the reconstruction's limiters then discard a NaN neighbour, and so does
+// its derivative)
 template <class T, int N>
-GRIM_D Dual<T, N> fmin(const Dual<T, N>& a, const Dual<T, N>& b) { return (b.v < a.v) ? b : a; }
+GRIM_D Dual<T, N> fmin(const Dual<T, N>& a, const Dual<T, N>& b) {
+  if (isnan(a.v)) return b;
+  if (isnan(b.v)) return a;
+  return (b.v < a.v) ? b : a;
+}
 template <class T, int N>
-GRIM_D Dual<T, N> fmax(const Dual<T, N>& a, const Dual<T, N>& b) { return (b.v > a.v) ? b : a; }
+GRIM_D Dual<T, N> fmax(const Dual<T, N>& a, const Dual<T, N>& b) {
+  if (isnan(a.v)) return b;
+  if (isnan(b.v)) return a;
+  return (b.v > a.v) ? b : a;
+}
 template <class T, int N>
 GRIM_D Dual<T, N> copysign(T a, const Dual<T, N>& b) { return Dual<T, N>(::copysign(a, b.v)); }
+
+// minmod of three slopes (minmod.cpp:3-19) on the tangent scalar: where the
+// smallest magnitude is exactly zero (a flat stretch of data, a zero field)
+// the limited slope stays zero on at least one side of the point, and the
+// sign choices at an exact zero would give a derivative of no side; the
+// derivative taken there is zero
+template <class T, int N>
+GRIM_D Dual<T, N> minmod3(Dual<T, N> x, Dual<T, N> y, Dual<T, N> z) {
+  typedef Dual<T, N> D;
+  D m = fmin(fmin(fabs(x), fabs(y)), fabs(z));
+  if (m.v == T(0)) return D(T(0));
+  const T sx = x.v < T(0) ? T(-1) : T(1), sy = y.v < T(0) ? T(-1) : T(1), sz = z.v < T(0) ? T(-1) : T(1);
+  return m * (T(0.25) * ::fabs(sx + sy) * (sx + sz));
+}
+
+// the overloads on plain doubles stay visible beside the ones above
+using ::fabs;
+using ::fmax;
+using ::fmin;
+
+}  // namespace grim
+
+// the torus problem's floors, on the tangent scalar (their local Jacobian)
+#define GRIM_KNS adjt
+#include "torus.cuh"
+#undef GRIM_KNS
+
+namespace grim {
 
 namespace adj {
 
@@ -137,6 +176,18 @@ __global__ void k_stage(DevCfg c, const double* __restrict__ geoC, const double*
   if (n >= c.Zint) return;
   const long long Z = c.Z;
   const long long z = interior_to_z(c, n);
+  // a zone whose adjoint is zero contributes nothing; its state may be one
+  // the NaN reset discards, where the Jacobian is not finite
+  bool any = false;
+  for (int v = 0; v < c.dof; v++) any |= lam[(long long)v * Z + z] != 0.;
+  if (!any) {
+    for (int v = 0; v < c.dof; v++) g[(long long)v * Z + z] = 0.;
+    if (!accumulate) {
+      for (int v = 0; v < 5; v++) ubar[(long long)v * Z + z] = 0.;
+      for (int k = 0; k < 3; k++) bacc[(long long)k * Z + z] = 0.;
+    }
+    return;
+  }
   ZoneGeo<double> G;
   centre_geo(c, geoC, z, G);
   double J[5][8];
@@ -161,20 +212,25 @@ __global__ void k_stage(DevCfg c, const double* __restrict__ geoC, const double*
   }
 }
 
-// lam_out(P0) += dU/dP(P0)^T ubar + [0 ; bacc]
+// out(P0) += dU/dP(P0)^T ubar + [0 ; bacc] (interior zones)
 __global__ void k_cons(DevCfg c, const double* __restrict__ geoC, const double* __restrict__ P,
                        const double* __restrict__ ubar, const double* __restrict__ bacc, double* __restrict__ lam) {
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= c.Zint) return;
   const long long Z = c.Z;
   const long long z = interior_to_z(c, n);
+  bool any = false;
+  for (int r = 0; r < 5; r++) any |= ubar[(long long)r * Z + z] != 0.;
+  for (int k = 0; k < 3; k++) any |= bacc[(long long)k * Z + z] != 0.;
+  if (!any) return;
   ZoneGeo<double> G;
   centre_geo(c, geoC, z, G);
   double J[5][8];
   cons_jacobian(c, P, z, G, J);
   for (int k = 0; k < 8; k++) {
     double s = 0.;
-    for (int r = 0; r < 5; r++) s += J[r][k] * ubar[(long long)r * Z + z];
+    for (int r = 0; r < 5; r++)
+      if (ubar[(long long)r * Z + z] != 0.) s += J[r][k] * ubar[(long long)r * Z + z];
     if (k >= 5) s += bacc[(long long)(k - 5) * Z + z];
     const long long row = (k < 5) ? k : c.B1 + (k - 5);
     lam[row * Z + z] += s;
@@ -212,7 +268,8 @@ __global__ void k_src_t(DevCfg c, const double* __restrict__ geoC, const double*
     for (int ka = 0; ka < 4; ka++)
       for (int la = 0; la < 4; la++) s -= T[ka][la] * (G0.g * __ldg(gam + (long long)(la * 16 + ka * 4 + nu) * c.GZ));
     const double gb = g[(long long)(UU + nu) * Z + z];
-    for (int m = 0; m < 8; m++) acc[m] += s.d[m] * gb;
+    if (gb != 0.)
+      for (int m = 0; m < 8; m++) acc[m] += s.d[m] * gb;
   }
   for (int m = 0; m < 8; m++) {
     const long long row = (m < 5) ? m : c.B1 + (m - 5);
@@ -239,10 +296,13 @@ __global__ void k_div_t(DevCfg c, const double* __restrict__ g, double* __restri
     const bool in0 = is_interior(c, i, j, k), in1 = is_interior(c, im, jm, km);
     const long long zm = zidx(c, im < 0 ? 0 : im, jm < 0 ? 0 : jm, km < 0 ? 0 : km);
     const double idx = 1. / c.dX[d];
+    // the torus flux filter zeroes every row of the faces at the poles
+    // (problem.cpp:1243-1285): only the zone beside each pole face uses it
+    const bool pole = c.problem == GRIM_PROBLEM_TORUS && d == 1 && (j == c.g2 || j == c.N2 + c.g2);
     for (int v = 0; v < c.dof; v++) {
       const double a = in1 ? g[(long long)v * Z + zm] : 0.;
       const double b = in0 ? g[(long long)v * Z + z] : 0.;
-      Ft[((long long)d * c.dof + v) * Z + z] = (a - b) * idx;
+      Ft[((long long)d * c.dof + v) * Z + z] = pole ? 0. : (a - b) * idx;
     }
   }
 }
@@ -394,9 +454,15 @@ __global__ void k_faces_t(DevCfg c, int dir, const double* __restrict__ geoF, co
       R[v] = side == 1 ? D8::var(pr[v], v) : D8(pr[v]);
     }
     riemann_flux<D8>(c, dir, G, L, R, F);
+    // the torus flux filter on the density flux of the inner / outer X1
+    // faces: min(F, 0) / max(F, 0), so its derivative is 1 or 0
+    double fr0 = fb[0];
+    if (c.problem == GRIM_PROBLEM_TORUS && dir == 0 &&
+        ((x == c.g1 && F[0].v > 0.) || (x == c.N1 + c.g1 && F[0].v < 0.)))
+      fr0 = 0.;
     for (int k2 = 0; k2 < 8; k2++) {
-      double acc = 0.;
-      for (int r = 0; r < 8; r++) acc += fb[r] * F[r].d[k2];
+      double acc = fr0 * F[0].d[k2];
+      for (int r = 1; r < 8; r++) acc += fb[r] * F[r].d[k2];
       gface[(long long)(side * 8 + k2) * Z + z] = acc;
     }
   }
@@ -491,6 +557,164 @@ __global__ void k_fold(DevCfg c, const double* __restrict__ q, double* __restric
   }
 }
 
+// ---- the torus problem's hooks (problem.cpp): floors after each stage,
+// the inflow check and the pole fix at the start of each stage
+GRIM_D adjt::TorusCfg torus_params(const DevCfg& c) {
+  adjt::TorusCfg t;
+  t.MaxLorentzFactor = c.maxLF; t.RhoFloorAmpl = c.rhoFloorAmpl; t.UFloorAmpl = c.uFloorAmpl;
+  t.RhoFloorSlope = c.rhoFloorSlope; t.UFloorSlope = c.uFloorSlope;
+  t.BsqrOverRhoMax = c.bsqOverRhoMax; t.BsqrOverUMax = c.bsqOverUMax;
+  return t;
+}
+GRIM_D long long prow(const DevCfg& c, int v) { return v < 5 ? v : c.B1 + (v - 5); }
+
+// applyFloor's transpose (problem.cpp:542-712), interior zones: lam holds
+// dL/d(floored state); lam <- J^T lam with J the floors' Jacobian at the
+// stage's Newton solution Psol (one forward-tangent pass, 8 lanes)
+__global__ void k_floor_t(DevCfg c, const double* __restrict__ geoC, const double* __restrict__ Psol,
+                          double* __restrict__ lam) {
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= c.Zint) return;
+  typedef Dual<double, 8> D;
+  const long long Z = c.Z;
+  const long long z = interior_to_z(c, n);
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  ZoneGeo<double> G0;
+  load_geo(G0, c, geoC, z, i, j, 0.5, 0.5);
+  ZoneGeo<D> G;
+  geo_const(G, G0);
+  // zero adjoint: nothing to transpose (the local Jacobian need not be
+  // finite where no derivative flows, e.g. at a zero field)
+  bool any = false;
+  for (int v = 0; v < 8; v++) any |= lam[prow(c, v) * Z + z] != 0.;
+  if (!any) return;
+  D q[8];
+  bool nan = false;
+  for (int v = 0; v < 8; v++) {
+    q[v] = D::var(Psol[prow(c, v) * Z + z], v);
+    nan |= isnan(q[v].v);
+  }
+  if (nan) {
+    // fullStepDiagnostics' reset: the zone's state no longer depends on it
+    for (int v = 0; v < 8; v++) lam[prow(c, v) * Z + z] = 0.;
+    return;
+  }
+  const long long gz = gidx(c, i, j);
+  adjt::torus_floor_zone<0, 0>(c, torus_params(c), q, G, __ldg(geoC + 37LL * c.GZ + gz),
+                               __ldg(geoC + 38LL * c.GZ + gz), false);
+  double out[8] = {0., 0., 0., 0., 0., 0., 0., 0.};
+  for (int r = 0; r < 8; r++) {
+    const double lr = lam[prow(c, r) * Z + z];
+    if (lr != 0.)
+      for (int v = 0; v < 8; v++) out[v] += q[r].d[v] * lr;
+  }
+  for (int v = 0; v < 8; v++) lam[prow(c, v) * Z + z] = out[v];
+}
+
+// fixPoles' transpose (problem.cpp:1046-1215) on the full-grid adjoint a,
+// one thread per (i, k) column and pole: the two rows next to the pole take
+// row idx2's fluid values (u2 scaled by theta_row / theta_idx2), the ghost
+// rows mirror the three rows (fluid from row idx2, field from their own
+// row, u2 and B2 negated); every overwritten entry's adjoint goes back to
+// the entry it copies and is cleared
+__global__ void k_poles_t(DevCfg c, const double* __restrict__ geoC, double* __restrict__ a) {
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long cols = (long long)c.N1T * c.N3T;
+  if (n >= 2 * cols) return;
+  const bool top = n >= cols;
+  const long long m = top ? n - cols : n;
+  const int i = (int)(m % c.N1T), k = (int)(m / c.N1T);
+  const long long Z = c.Z;
+  const int ng = c.ng;
+  auto at = [&](int v, int j) -> double& { return a[(long long)v * Z + zidx(c, i, j, k)]; };
+  auto theta = [&](int j) -> double {
+    const double th = __ldg(geoC + 35LL * c.GZ + gidx(c, i, j));
+    return top ? th * (-1.) + M_PI : th;
+  };
+  const int idx0 = top ? c.N2 + ng - 1 : ng;
+  const int row[3] = {idx0, top ? idx0 - 1 : ng + 1, top ? idx0 - 2 : ng + 2};
+  double th[3];
+  for (int g = 0; g < 3; g++) th[g] = theta(row[g]);
+  double acc[5];
+  for (int v = 0; v < 5; v++) acc[v] = at(v, row[2]);
+  // only nonzero adjoints are carried: the ratio of thetas is not finite
+  // in the innermost ghost column of some grids, where the forward's values
+  // are not finite either and nothing downstream reads them
+  for (int g = 0; g < 2; g++)
+    for (int v = 0; v < 5; v++) {
+      const double cf = (v == U2) ? th[g] / th[2] : 1.;
+      if (at(v, row[g]) != 0.) acc[v] += cf * at(v, row[g]);
+      at(v, row[g]) = 0.;
+    }
+  for (int g = 0; g < 3; g++) {
+    const int dst = top ? c.N2 + ng + g : ng - 1 - g;
+    for (int v = 0; v < 5; v++) {
+      const double cf = (v == U2) ? -(g < 2 ? th[g] / th[2] : 1.) : 1.;
+      if (at(v, dst) != 0.) acc[v] += cf * at(v, dst);
+      at(v, dst) = 0.;
+    }
+    for (int b = 0; b < 3; b++) {
+      const double cf = (b == 1) ? -1. : 1.;
+      at(c.B1 + b, row[g]) += cf * at(c.B1 + b, dst);
+      at(c.B1 + b, dst) = 0.;
+    }
+  }
+  for (int v = 0; v < 5; v++) at(v, row[2]) = acc[v];
+}
+
+// inflowCheck's transpose (problem.cpp:941-1044) on the X1 ghost zones of
+// the full-grid adjoint a: the ghost's velocities after the check are a
+// function of its velocities before it (Pfill, the boundary fill's copy):
+// u / gamma, the radial component clamped against inflow, the Lorentz
+// factor capped; a's velocity rows <- J^T a
+__global__ void k_inflow_t(DevCfg c, const double* __restrict__ geoC, const double* __restrict__ Pfill,
+                           double* __restrict__ a) {
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long cols = (long long)2 * c.ng * c.N2T * c.N3T;
+  if (n >= cols) return;
+  typedef Dual<double, 3> D;
+  const int gi = (int)(n % (2 * c.ng));
+  const long long r = n / (2 * c.ng);
+  const int j = (int)(r % c.N2T), k = (int)(r / c.N2T);
+  const bool right = gi >= c.ng;
+  const int i = right ? (c.N1 + c.ng + (gi - c.ng)) : gi;
+  const long long Z = c.Z;
+  const long long z = zidx(c, i, j, k);
+  if (a[(long long)U1 * Z + z] == 0. && a[(long long)U2 * Z + z] == 0. && a[(long long)U3 * Z + z] == 0.) return;
+  ZoneGeo<double> G0;
+  geo_load<double>(G0, geoC, c.GZ, gidx(c, i, j));
+  ZoneGeo<D> G;
+  geo_const(G, G0);
+  D u[3];
+  for (int d = 0; d < 3; d++) u[d] = D::var(Pfill[(long long)(U1 + d) * Z + z], d);
+  ElemT<D, D> e;
+  elem_set<0, 0>(e, D(Pfill[z]), D(Pfill[Z + z]), u[0], u[1], u[2], D(Pfill[(long long)c.B1 * Z + z]),
+                 D(Pfill[(long long)(c.B1 + 1) * Z + z]), D(Pfill[(long long)(c.B1 + 2) * Z + z]), D(0.), D(0.), G,
+                 c);
+  for (int d = 0; d < 3; d++) u[d] = u[d] / e.gam;
+  if (right) {
+    const long long ze = gidx(c, c.N1 + c.ng - 1, j);
+    const double minUr = __ldg(geoC + 17LL * c.GZ + ze) * __ldg(geoC + 33LL * c.GZ + ze);
+    u[0] = fmax(D(minUr), u[0]);
+  } else {
+    u[0] = fmin(D(G0.gcon[0][1] * G0.alpha), u[0]);
+  }
+  D vSqr(0.);
+  for (int p = 0; p < 3; p++)
+    for (int q = 0; q < 3; q++) vSqr += G0.gcov[p + 1][q + 1] * u[p] * u[q];
+  const double vSqrMax = 1. - 1. / c.maxLF / c.maxLF;
+  vSqr = fmax(fmin(vSqr, D(vSqrMax)), D(1.e-13));
+  const D lf = 1. / dsqrt(1. - vSqr);
+  double ab[3], out[3] = {0., 0., 0.};
+  for (int d = 0; d < 3; d++) ab[d] = a[(long long)(U1 + d) * Z + z];
+  for (int d = 0; d < 3; d++) {
+    const D ud = u[d] * lf;
+    for (int m2 = 0; m2 < 3; m2++) out[m2] += ud.d[m2] * ab[d];
+  }
+  for (int d = 0; d < 3; d++) a[(long long)(U1 + d) * Z + z] = out[d];
+}
+
 }  // namespace adj
 
 static __global__ void k_zero_ghosts(DevCfg c, double* __restrict__ a) {
@@ -507,8 +731,10 @@ void adjoint_zero_ghosts(const DevCfg& c, double* a, cudaStream_t s) {
   k_zero_ghosts<<<adj::nblk(c.Z, 256), 256, 0, s>>>(c, a);
 }
 
-void adjoint_stencil_t(const DevCfg& c, const AdjointGeo& geo, const double* P, const double* g, double* Ft,
-                       double* ebar, double* q, double* gface, double* out, cudaStream_t s) {
+// q = the stencil's transpose over the whole grid (ghost entries not yet
+// folded): divergence, flux-CT, Riemann solver, reconstruction
+static void stencil_q(const DevCfg& c, const AdjointGeo& geo, const double* P, const double* g, double* Ft,
+                      double* ebar, double* q, double* gface, cudaStream_t s) {
   using namespace adj;
   const size_t bZ = (size_t)c.Z * sizeof(double);
   k_div_t<<<nblk(c.Z, 128), 128, 0, s>>>(c, g, Ft);
@@ -519,21 +745,39 @@ void adjoint_stencil_t(const DevCfg& c, const AdjointGeo& geo, const double* P, 
     k_faces_t<<<nblk(c.Z, 64), 64, 0, s>>>(c, d, geo.geoF[d], P, Ft, gface);
     k_recon_t<<<nblk(c.Z, 64), 64, 0, s>>>(c, d, P, gface, q);
   }
-  k_fold<<<nblk(c.Zint, 128), 128, 0, s>>>(c, q, out);
 }
 
-void adjoint_step(const DevCfg& c, const AdjointGeo& geo, double dt, const double* P0, const double* Ph,
-                  const double* P1, double* lam, const AdjointBufs& w, cudaStream_t s) {
+void adjoint_stencil_t(const DevCfg& c, const AdjointGeo& geo, const double* P, const double* g, double* Ft,
+                       double* ebar, double* q, double* gface, double* out, cudaStream_t s) {
+  stencil_q(c, geo, P, g, Ft, ebar, q, gface, s);
+  adj::k_fold<<<adj::nblk(c.Zint, 128), 128, 0, s>>>(c, q, out);
+}
+
+void adjoint_step(const DevCfg& c, const AdjointGeo& geo, double dt, const AdjointStates& st, double* lam,
+                  const AdjointBufs& w, cudaStream_t s) {
   using namespace adj;
-  // full stage at P1
-  k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, geo.geoC, P1, dt, lam, w.g, w.ubar, w.bacc, 0);
-  adjoint_stencil_t(c, geo, Ph, w.g, w.Ft, w.ebar, w.q, w.gface, w.lamh, s);
-  if (geo.gamma) k_src_t<<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, geo.gamma, Ph, w.g, w.lamh);
-  // half stage at Ph
-  k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, geo.geoC, Ph, 0.5 * dt, w.lamh, w.g, w.ubar, w.bacc, 1);
-  adjoint_stencil_t(c, geo, P0, w.g, w.Ft, w.ebar, w.q, w.gface, lam, s);
-  if (geo.gamma) k_src_t<<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, geo.gamma, P0, w.g, lam);
-  k_cons<<<nblk(c.Zint, 128), 128, 0, s>>>(c, geo.geoC, P0, w.ubar, w.bacc, lam);
+  const bool torus = c.problem == GRIM_PROBLEM_TORUS;
+  // the start-of-stage hooks' and the ghost fill's transposes: q -> out
+  auto hooks_fold = [&](const double* Pfill, double* out) {
+    if (torus) {
+      k_poles_t<<<nblk(2LL * c.N1T * c.N3T, 128), 128, 0, s>>>(c, geo.geoC, w.q);
+      k_inflow_t<<<nblk(2LL * c.ng * c.N2T * c.N3T, 64), 64, 0, s>>>(c, geo.geoC, Pfill, w.q);
+    }
+    k_fold<<<nblk(c.Zint, 128), 128, 0, s>>>(c, w.q, out);
+  };
+  // full stage: the floors at its finish, then the stage at its Newton solution
+  if (torus) k_floor_t<<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, st.P1Sol, lam);
+  k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, geo.geoC, st.P1Sol, dt, lam, w.g, w.ubar, w.bacc, 0);
+  stencil_q(c, geo, st.PhEff, w.g, w.Ft, w.ebar, w.q, w.gface, s);
+  if (geo.gamma) k_src_t<<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, geo.gamma, st.PhEff, w.g, w.q);
+  hooks_fold(st.PhFill, w.lamh);
+  // half stage
+  if (torus) k_floor_t<<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, st.PhSol, w.lamh);
+  k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, geo.geoC, st.PhSol, 0.5 * dt, w.lamh, w.g, w.ubar, w.bacc, 1);
+  stencil_q(c, geo, st.P0eff, w.g, w.Ft, w.ebar, w.q, w.gface, s);
+  if (geo.gamma) k_src_t<<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, geo.gamma, st.P0eff, w.g, w.q);
+  k_cons<<<nblk(c.Zint, 128), 128, 0, s>>>(c, geo.geoC, st.P0eff, w.ubar, w.bacc, w.q);
+  hooks_fold(st.P0fill, lam);
 }
 
 }  // namespace grim

@@ -190,6 +190,11 @@ GRIM_HD float val(float x) { return x; }
 template <class T, int N>
 GRIM_HD T val(const Dual<T, N>& x) { return x.v; }
 
+// the value of a scalar: a double, or the value part of a tangent scalar
+GRIM_HD double val_of(double x) { return x; }
+template <class T, int N>
+GRIM_HD T val_of(const Dual<T, N>& x) { return x.v; }
+
 GRIM_HD double dsqrt(double x) { return sqrt(x); }
 GRIM_HD float dsqrt(float x) { return sqrtf(x); }
 // 1 / sqrt(x) (the fast path forms gamma and 1 / gamma from one call)

@@ -67,9 +67,18 @@ struct AdjointGeo {
   const double* geoF[3];  // face planes per direction (X3: the centre's)
   const double* gamma;    // centre Christoffel planes
 };
+// the states one step's adjoint reads (dof x Z each)
+struct AdjointStates {
+  const double* P0fill;  // the step's start state, ghosts filled by the boundary pass
+  const double* P0eff;   // the same after the problem's boundary hooks (the half stage's input)
+  const double* PhSol;   // the half stage's Newton solution (before its finish)
+  const double* PhFill;  // primHalfStep after the half stage's finish, ghosts filled
+  const double* PhEff;   // the same after the problem's boundary hooks (the full stage's input)
+  const double* P1Sol;   // the full stage's Newton solution (before its finish)
+};
 // lam (dL/dP1, interior) -> dL/dP0 for one step of fixed dt
-void adjoint_step(const DevCfg& c, const AdjointGeo& geo, double dt, const double* P0, const double* Ph,
-                  const double* P1, double* lam, const AdjointBufs& w, cudaStream_t s);
+void adjoint_step(const DevCfg& c, const AdjointGeo& geo, double dt, const AdjointStates& st, double* lam,
+                  const AdjointBufs& w, cudaStream_t s);
 void adjoint_zero_ghosts(const DevCfg& c, double* a, cudaStream_t s);
 // out = D(P)^T g: the transpose of the flux divergence with its ghost fill
 void adjoint_stencil_t(const DevCfg& c, const AdjointGeo& geo, const double* P, const double* g, double* Ft,

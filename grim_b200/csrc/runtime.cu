@@ -1577,10 +1577,12 @@ static int adjoint_scope(grim_handle* h) {
   auto ok_bc = [](int b) { return b == GRIM_PERIODIC || b == GRIM_OUTFLOW || b == GRIM_MIRROR; };
   const bool bcs = ok_bc(c.boundaryLeft) && ok_bc(c.boundaryRight) && ok_bc(c.boundaryBottom) &&
                    ok_bc(c.boundaryTop) && (c.dim < 3 || (ok_bc(c.boundaryFront) && ok_bc(c.boundaryBack)));
-  if ((c.dim != 2 && c.dim != 3) || c.conduction || c.viscosity || !bcs || c.problem != GRIM_PROBLEM_NONE ||
-      c.N3Global > 0) {
+  const bool torusOk = c.problem == GRIM_PROBLEM_TORUS && c.metric != GRIM_MINKOWSKI && c.numGhost == 3 &&
+                       (c.dim < 2 || c.N2 >= 6);
+  if ((c.dim != 2 && c.dim != 3) || c.conduction || c.viscosity || !bcs ||
+      (c.problem != GRIM_PROBLEM_NONE && !torusOk) || c.N3Global > 0) {
     set_err("adjoint: supported for 2D and 3D ideal MHD (Minkowski or MKS) with periodic, outflow or mirror "
-            "boundaries and no problem hooks only");
+            "boundaries, without problem hooks or with the torus problem's (MKS, N2 >= 6)");
     return GRIM_ENOTSUP;
   }
   return GRIM_OK;
@@ -1681,8 +1683,8 @@ int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, in
   const DevCfg& c = h->dc;
   const size_t bytes = (size_t)c.dof * h->bytesZ;
   const int every = h->adjEvery;
-  // segment states and work buffers
-  while ((int)h->adjSeg.size() < 2 * every + 2) {
+  // segment states (six per step: grim::AdjointStates) and work buffers
+  while ((int)h->adjSeg.size() < 6 * every + 1) {
     double* p = nullptr;
     if (cudaMalloc(&p, bytes) != cudaSuccess) { set_err("adjoint: segment allocation failed"); return GRIM_ENOMEM; }
     h->adjSeg.push_back(p);
@@ -1691,7 +1693,8 @@ int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, in
   double* lam = nullptr;
   int rcw = adjoint_work(h, w, lam);
   if (rcw) return rcw;
-  double* finalState = h->adjSeg[2 * every + 1];
+  double* finalState = h->adjSeg[6 * every];
+  auto state = [&](int kind, int t) { return h->adjSeg[(size_t)kind * every + t]; };
   CK(cudaMemcpyAsync(lam, lambda, bytes, memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                      h->stream));
   grim::adjoint_zero_ghosts(c, lam, h->stream);
@@ -1706,21 +1709,37 @@ int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, in
     CK(cudaMemcpyAsync(h->primOld, h->adjCkpt[seg], bytes, cudaMemcpyDeviceToDevice, h->stream));
     rc = grim_set_time(h, h->adjT0 + (double)seg * every * dt, dt);
     if (rc) return rc;
-    // recompute the segment, keeping the states each step's adjoint needs
+    // recompute the segment step by step, keeping the states each step's
+    // adjoint reads: the start state with its ghosts filled as the step's
+    // boundary pass fills them (the stored state holds grid::communicate's
+    // zeros on the outflow / mirror sides) and after the problem's hooks,
+    // each stage's Newton solution, primHalfStep after its finish (filled,
+    // then after the hooks)
     for (int t = 0; t < m; t++) {
-      CK(cudaMemcpyAsync(h->adjSeg[t], h->primOld, bytes, cudaMemcpyDeviceToDevice, h->stream));
-      // the ghosts of the outflow / mirror sides as the step's own boundary
-      // pass forms them before its stencil reads them (the stored state
-      // holds grid::communicate's zeros there)
-      KNS_CALL(h, ghost_fill, c, h->adjSeg[t], c.dof, h->stream);
-      rc = run_steps(h, 1);
-      if (rc) return rc;
-      CK(cudaMemcpyAsync(h->adjSeg[every + 1 + t], h->primHalf, bytes, cudaMemcpyDeviceToDevice, h->stream));
+      CK(cudaMemcpyAsync(state(0, t), h->primOld, bytes, cudaMemcpyDeviceToDevice, h->stream));
+      KNS_CALL(h, ghost_fill, c, state(0, t), c.dof, h->stream);
+      enqueue_segment(h, GRIM_SEG_PRE);
+      CK(cudaMemcpyAsync(state(1, t), h->primOld, bytes, cudaMemcpyDeviceToDevice, h->stream));
+      enqueue_segment(h, GRIM_SEG_HALF);
+      CK(cudaMemcpyAsync(state(2, t), h->prim, bytes, cudaMemcpyDeviceToDevice, h->stream));
+      CK(cudaMemcpyAsync(state(3, t), h->primHalf, bytes, cudaMemcpyDeviceToDevice, h->stream));
+      KNS_CALL(h, ghost_fill, c, state(3, t), c.dof, h->stream);
+      enqueue_segment(h, GRIM_SEG_FULL);
+      CK(cudaMemcpyAsync(state(4, t), h->primHalf, bytes, cudaMemcpyDeviceToDevice, h->stream));
+      CK(cudaMemcpyAsync(state(5, t), h->prim, bytes, cudaMemcpyDeviceToDevice, h->stream));
+      enqueue_segment(h, GRIM_SEG_POST);
+      CK(cudaGetLastError());
     }
-    CK(cudaMemcpyAsync(h->adjSeg[m], h->primOld, bytes, cudaMemcpyDeviceToDevice, h->stream));
-    for (int t = m - 1; t >= 0; t--)
-      grim::adjoint_step(c, adjoint_geo(h), dt, h->adjSeg[t], h->adjSeg[every + 1 + t], h->adjSeg[t + 1], lam, w,
-                         h->stream);
+    for (int t = m - 1; t >= 0; t--) {
+      grim::AdjointStates st;
+      st.P0fill = state(0, t);
+      st.P0eff = state(1, t);
+      st.PhSol = state(2, t);
+      st.PhFill = state(3, t);
+      st.PhEff = state(4, t);
+      st.P1Sol = state(5, t);
+      grim::adjoint_step(c, adjoint_geo(h), dt, st, lam, w, h->stream);
+    }
     CK(cudaGetLastError());
   }
   grim::adjoint_zero_ghosts(c, lam, h->stream);

@@ -6,6 +6,8 @@
 // (:1243-1285) is applied inside the stage epilogue.  One thread per zone;
 // each is a direct restatement of the reference's array expressions.
 #pragma once
+#include <type_traits>
+
 #include "physics.cuh"
 
 namespace grim {
@@ -25,12 +27,13 @@ GRIM_D void load_elem(ElemT<double, double>& e, const DevCfg& c, const double* p
                        COND ? p[(long long)c.Q * Z + z] : 0., VISC ? p[(long long)c.DP * Z + z] : 0., G, c);
 }
 
-// the element of one zone's primitives q (rows: fluid, then B1..B3)
-template <int COND, int VISC>
-GRIM_D void elem_of(ElemT<double, double>& e, const DevCfg& c, const double* q, const ZoneGeo<double>& G) {
+// the element of one zone's primitives q (rows: fluid, then B1..B3); S is
+// double, or the forward-tangent scalar of the adjoint's local Jacobians
+template <int COND, int VISC, class S>
+GRIM_D void elem_of(ElemT<S, S>& e, const DevCfg& c, const S* q, const ZoneGeo<S>& G) {
   constexpr int NFT = 5 + COND + VISC;
-  elem_set<COND, VISC>(e, q[RHO], q[UU], q[U1], q[U2], q[U3], q[NFT], q[NFT + 1], q[NFT + 2], COND ? q[5] : 0.,
-                       VISC ? q[5 + COND] : 0., G, c);
+  elem_set<COND, VISC>(e, q[RHO], q[UU], q[U1], q[U2], q[U3], q[NFT], q[NFT + 1], q[NFT + 2], COND ? q[5] : S(0.),
+                       VISC ? q[5 + COND] : S(0.), G, c);
 }
 
 // applyFloor (problem.cpp:542-712) on one zone's primitives q, held in
@@ -39,117 +42,120 @@ GRIM_D void elem_of(ElemT<double, double>& e, const DevCfg& c, const double* q, 
 // Returns true when the element left in eOut (if given) is the element of
 // the final q (no change after its last evaluation), so a caller needing
 // that element can use it as is.
-template <int COND, int VISC>
-GRIM_D bool torus_floor_zone(const DevCfg& c, const TorusCfg& t, double* q, const ZoneGeo<double>& G, double minRho,
-                             double minU, bool nanReset, ElemT<double, double>* eOut = nullptr) {
+// S is double on the hot path, or the forward-tangent scalar when the
+// adjoint takes the floors' local Jacobian (branches then follow the values;
+// the zero-weight drift-frame fix is skipped as in the fast path, which
+// leaves the derivative unchanged and keeps a non-finite correction out of
+// it).
+template <int COND, int VISC, class S>
+GRIM_D bool torus_floor_zone(const DevCfg& c, const TorusCfg& t, S* q, const ZoneGeo<S>& G, double minRho,
+                             double minU, bool nanReset, ElemT<S, S>* eOut = nullptr) {
   constexpr int NFT = 5 + COND + VISC, DOFT = NFT + 3;
+#ifdef GRIM_FAST_MATH
+  constexpr bool kSkipNoFix = true;
+#else
+  constexpr bool kSkipNoFix = !std::is_same<S, double>::value;
+#endif
   if (nanReset) {
     bool bad = false;
 #pragma unroll
-    for (int v = 0; v < DOFT; v++) bad |= isnan(q[v]);
+    for (int v = 0; v < DOFT; v++) bad |= isnan(val_of(q[v]));
     if (bad)
 #pragma unroll
-      for (int v = 0; v < DOFT; v++) q[v] = 0.;
+      for (int v = 0; v < DOFT; v++) q[v] = S(0.);
   }
-  const double rho_pre = q[RHO] * 1., u_pre = q[UU] * 1.;
+  const S rho_pre = q[RHO] * 1., u_pre = q[UU] * 1.;
   bool usefloor = false;
   {
-    bool cd = q[RHO] < minRho;
+    bool cd = val_of(q[RHO]) < minRho;
     usefloor = cd;
-    if (cd) q[RHO] = minRho;
-    cd = q[UU] < minU;
+    if (cd) q[RHO] = S(minRho);
+    cd = val_of(q[UU]) < minU;
     usefloor = usefloor || cd;
-    if (cd) q[UU] = minU;
+    if (cd) q[UU] = S(minU);
   }
-  ElemT<double, double> e;
+  ElemT<S, S> e;
   elem_of<COND, VISC>(e, c, q, G);
-  const double bSqr1 = e.bSqr;
+  const S bSqr1 = e.bSqr;
   {
-    bool cd = bSqr1 > t.BsqrOverRhoMax * q[RHO];
+    bool cd = val_of(bSqr1) > t.BsqrOverRhoMax * val_of(q[RHO]);
     usefloor = usefloor || cd;
     if (cd) q[RHO] = bSqr1 / t.BsqrOverRhoMax;
-    cd = bSqr1 > t.BsqrOverUMax * q[UU];
+    cd = val_of(bSqr1) > t.BsqrOverUMax * val_of(q[UU]);
     usefloor = usefloor || cd;
     if (cd) q[UU] = bSqr1 / t.BsqrOverUMax;
   }
-  const double rho = q[RHO], u = q[UU];
-  double trans = fmax(fmin(1., (bSqr1 - 0.1 * rho) / rho), 0.) * (usefloor ? 1. : 0.);
-#ifdef GRIM_FAST_MATH
+  const S rho = q[RHO], u = q[UU];
+  S trans = fmax(fmin(S(1.), (bSqr1 - 0.1 * rho) / rho), S(0.)) * (usefloor ? 1. : 0.);
   // the fix below blends with weight trans: with trans = 0 it returns the
   // velocities unchanged (up to the sign of a zero, or a non-finite
   // correction, which it would propagate), so the fast path skips it
-  if (trans != 0.) {
-#else
-  {
-#endif
+  if (!kSkipNoFix || val_of(trans) != 0.) {
   // drift-frame velocity fix
-  const double betapar = -e.bCon[0] / bSqr1 / e.uCon[0];
-  double betasqr = betapar * betapar * bSqr1;
+  const S betapar = -e.bCon[0] / bSqr1 / e.uCon[0];
+  S betasqr = betapar * betapar * bSqr1;
   const double betasqrmax = 1. - 1. / t.MaxLorentzFactor / t.MaxLorentzFactor;
-  betasqr = fmin(betasqr, betasqrmax);
-  const double gamma = 1. / sqrt(1. - betasqr);
-  double ucondr[4];
+  betasqr = fmin(betasqr, S(betasqrmax));
+  const S gamma = 1. / dsqrt(1. - betasqr);
+  S ucondr[4];
 #pragma unroll
   for (int m = 0; m < 4; m++) ucondr[m] = gamma * (e.uCon[m] + betapar * e.bCon[m]);
-  const double Bcon[4] = {0., q[NFT], q[NFT + 1], q[NFT + 2]};
-  double Bcov[4];
+  const S Bcon[4] = {S(0.), q[NFT], q[NFT + 1], q[NFT + 2]};
+  S Bcov[4];
 #pragma unroll
   for (int m = 0; m < 4; m++) {
-    double s = 0.;
+    S s = S(0.);
 #pragma unroll
     for (int n = 0; n < 4; n++) s += G.gcov[n][m] * Bcon[n];
     Bcov[m] = s;
   }
-  double udotB = 0., bSqr_fl = 0.;
+  S udotB = S(0.), bSqr_fl = S(0.);
 #pragma unroll
   for (int n = 0; n < 4; n++) {
     udotB += Bcov[n] * e.uCon[n];
     bSqr_fl += Bcov[n] * Bcon[n];
   }
-  double bNorm = fmax(sqrt(bSqr_fl), sqrt(c.bSqrFloor));
-  const double wold = rho_pre + u_pre * c.Gam;
-  const double QdotB = udotB * wold * e.uCon[0];
-  const double wnew = rho + u * c.Gam;
-  const double x = 2. * QdotB / (bNorm * wnew * ucondr[0]);
-  const double vpar = x / (ucondr[0] * (1. + sqrt(1. + x * x)));
-  const double inv_ut = 1. / ucondr[0];
-  double vcon[4];
-  vcon[0] = 0. + 1.;
+  S bNorm = fmax(dsqrt(bSqr_fl), S(sqrt(c.bSqrFloor)));
+  const S wold = rho_pre + u_pre * c.Gam;
+  const S QdotB = udotB * wold * e.uCon[0];
+  const S wnew = rho + u * c.Gam;
+  const S x = 2. * QdotB / (bNorm * wnew * ucondr[0]);
+  const S vpar = x / (ucondr[0] * (1. + dsqrt(1. + x * x)));
+  const S inv_ut = 1. / ucondr[0];
+  S vcon[4];
+  vcon[0] = S(0. + 1.);
 #pragma unroll
   for (int m = 1; m < 4; m++) vcon[m] = vpar * Bcon[m] / bNorm + ucondr[m] * inv_ut;
-  double vsqr = 0.;
+  S vsqr = S(0.);
 #pragma unroll
   for (int m = 0; m < 4; m++)
 #pragma unroll
     for (int n = 0; n < 4; n++) vsqr += G.gcov[m][n] * vcon[m] * vcon[n];
-  if (vsqr >= 0. || vsqr < 1. / G.gcon[0][0]) vsqr = 1. / G.gcon[0][0];
-  const double ut = sqrt(-1. / vsqr);
+  if (val_of(vsqr) >= 0. || val_of(vsqr) < val_of(1. / G.gcon[0][0])) vsqr = 1. / G.gcon[0][0];
+  const S ut = dsqrt(-1. / vsqr);
 #pragma unroll
   for (int m = 1; m < 4; m++) {
-    double utcon = ut * (vcon[m] - G.gcon[0][m] / G.gcon[0][0]);
+    S utcon = ut * (vcon[m] - G.gcon[0][m] / G.gcon[0][0]);
     q[UU + m] = q[UU + m] * (1. - trans) + trans * utcon;
   }
   }  // drift-frame fix
   // maximum Lorentz factor
-#ifdef GRIM_FAST_MATH
-  // no floor applied: q is the state the element above was set from (trans
-  // is 0, so the fix was skipped) and that element stands
-  if (usefloor)
-#endif
-    elem_of<COND, VISC>(e, c, q, G);
+  // (no floor applied: q is the state the element above was set from, trans
+  // is 0 so the fix was skipped, and that element stands)
+  if (!kSkipNoFix || usefloor) elem_of<COND, VISC>(e, c, q, G);
   bool current = true;
   {
-    const double lf2 = e.gam * e.gam;
+    const S lf2 = e.gam * e.gam;
     const double gm2 = t.MaxLorentzFactor * t.MaxLorentzFactor;
-    if (lf2 > gm2) {
-      double mf = 1. / sqrt(fmax((lf2 - 1.) / (gm2 - 1.), 1.));
+    if (val_of(lf2) > gm2) {
+      S mf = 1. / dsqrt(fmax((lf2 - 1.) / (gm2 - 1.), S(1.)));
       q[U1] *= mf;
       q[U2] *= mf;
       q[U3] *= mf;
       current = false;
     }
   }
-  if (COND || VISC) {
+  if constexpr (COND || VISC) {
     elem_of<COND, VISC>(e, c, q, G);
     if (COND) {
       const double cs = e.soundSpeed;

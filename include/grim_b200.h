@@ -423,8 +423,10 @@ int grim_set_face_variant(grim_handle* h, int dir, int variant);
  * is recomputed forward once; the stepper is left at the final state.
  * Supported: 2D and 3D ideal MHD, Minkowski or modified Kerr-Schild
  * (geometric source, face metric), periodic / outflow / mirror boundaries,
- * no problem hooks (GRIM_ENOTSUP otherwise: EMHD, the torus problem's
- * floors, inflow check, pole fix and flux filter).  Every accumulation is a gather in a fixed
+ * no problem hooks or the torus problem's (floors after each stage, inflow
+ * check and pole fix at the start of each stage, flux filter; MKS, N2 >= 6);
+ * GRIM_ENOTSUP otherwise (EMHD).  A zone that fullStepDiagnostics' NaN
+ * reset replaces carries no derivative.  Every accumulation is a gather in a fixed
  * order (no atomics): a gradient is the same bits run to run and for any
  * checkpoint interval. */
 int grim_set_dt_mode(grim_handle* h, int fixed);

@@ -124,11 +124,9 @@ def test_adjoint_checkpoint_interval_does_not_change_the_gradient():
 
 
 def test_adjoint_refuses_unsupported_configurations():
-    """The torus problem hooks (floors, inflow check, pole fix, flux
-    filter) are outside the adjoint's scope."""
-    from grim_b200.problems import torus as T
+    """EMHD is outside the adjoint's scope."""
     from grim_b200.timestepper import timeStepper
-    ts = timeStepper(T.torus_config(N1=32, N2=16, N3=8))
+    ts = timeStepper(PR.emhd_stratified_config(N=16))
     with pytest.raises(Exception):
         ts.adjointForward(2, 1)
 
@@ -382,3 +380,82 @@ def test_adjoint_matches_central_fd_mks():
     if bad:
         raise AssertionError("entries off the central differences: %s" % str(bad))
     assert smooth >= 10, smooth
+
+
+# ---- the torus problem: floors, inflow check, pole fix, flux filter ------------
+def test_adjoint_matches_central_fd_torus():
+    """Whole checkpointed runs of the torus problem itself (Fishbone-Moncrief
+    torus in its atmosphere, 16x12x6 from r = 2.5 to 100, 3 steps,
+    checkpoints every 2): the
+    floors after each stage (their local Jacobian at each stage's Newton
+    solution), the inflow check and the pole fix at the start of each stage
+    and the flux filter, on top of the MKS transposes.  The floors make the
+    map piecewise smooth at the atmosphere's floor values; the screen of
+    fd_check skips picks at a switch.  The two rows next to each pole are
+    overwritten from the third by the pole fix before anything reads them,
+    so the gradient of their fluid variables is exactly zero.  From the
+    torus grid's inner edge (inside the horizon) this coarse grid's first
+    columns go non-finite and are reset to the floors every step (measured);
+    the reset's zones carry no derivative, and the central differences need
+    a map without resets, hence r >= 2.5 here."""
+    import math
+    from grim_b200.problems import torus as T
+    from grim_b200.timestepper import timeStepper
+    cfg = T.torus_config(N1=16, N2=12, N3=6, dt=1e-3, maxNonLinearIter=8, nonlinearsolve_atol=0.0,
+                         X1Start=math.log(2.5), X1End=math.log(100.))
+    init = timeStepper(cfg)
+    P, _ = T.torus_prims(cfg, init.getGeometry(C.CENTER))
+    init.primOld.setVars(P)
+    init.problemInit()  # the field loop, the perturbation, the floors
+    P0 = init.primOld.getVars()
+    g = cfg["numGhost"]
+    sl = (slice(None),) + tuple(C.interior_slices(cfg))
+    assert np.isfinite(P0[sl]).all()
+    # the initial torus is exactly axisymmetric, with exactly zero field
+    # outside the loop: every X3 face sits at a switch of the limiters and of
+    # the Riemann solver's speed min / max, where a central difference
+    # averages two branches; a seeded 1e-3 perturbation of every variable
+    # moves the state off those switches
+    rng0 = np.random.default_rng(17)
+    Q = P0[sl]
+    Q[:5] *= 1. + 1e-3 * rng0.uniform(-1., 1., Q[:5].shape)
+    Q[5:] += 1e-6 * rng0.uniform(-1., 1., Q[5:].shape)
+    P0[sl] = Q
+    ref = np.array(P0[sl])
+
+    def stepper(P):
+        ts = _mks_stepper(cfg, P)
+        return ts
+
+    def loss(P):
+        ts = stepper(P)
+        for _ in range(nsteps):
+            ts.timeStep()
+            # no zone went through the NaN reset
+            assert np.isfinite(ts.prim.getVars()[sl]).all()
+        d = (ts.primOld.getVars()[sl] - ref).ravel()
+        return 0.5 * math.fsum((d * d).tolist())
+
+    nsteps = 3
+    ts = stepper(P0)
+    ts.adjointForward(nsteps, 2)
+    Pf = ts.primOld.getVars()
+    lam = np.zeros_like(Pf)
+    lam[sl] = Pf[sl] - ref
+    gi = interior(cfg, ts.adjointBackward(lam))
+    assert np.isfinite(gi).all()
+    assert np.all(gi[:5, :, :2, :] == 0.) and np.all(gi[:5, :, -2:, :] == 0.)
+    L0 = loss(P0)
+
+    def shifted(v, k, j, i, h):
+        Q = P0.copy()
+        Q[v, k + g, j + g, i + g] += h
+        return loss(Q)
+
+    rng = np.random.default_rng(5)
+    picks = [(n % 8, int(rng.integers(0, 6)), int(rng.integers(2, 10)), int(rng.choice([0, 1, 3, 6, 9, 15])))
+             for n in range(40)]
+    smooth, bad = fd_check(shifted, L0, gi, picks, float(np.max(np.abs(gi))))
+    if bad:
+        raise AssertionError("entries off the central differences: %s" % str(bad))
+    assert smooth >= 8, smooth
