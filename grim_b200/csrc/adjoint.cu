@@ -141,6 +141,15 @@ GRIM_D void geo_const(ZoneGeo<D>& Gd, const ZoneGeo<double>& G) {
   Gd.x1 = D(G.x1); Gd.x2 = D(G.x2); Gd.dyn = D(G.dyn);
 }
 
+// the element of one zone's primitives p in grid row order (fluid rows,
+// then B1..B3)
+template <int C, int V, class S>
+GRIM_D void elem_rows(ElemT<S, S>& e, const DevCfg& c, const S* p, const ZoneGeo<S>& G) {
+  constexpr int NF = 5 + C + V;
+  elem_set<C, V>(e, p[0], p[1], p[2], p[3], p[4], p[NF], p[NF + 1], p[NF + 2], C ? p[5] : S(0.),
+                 V ? p[5 + C] : S(0.), G, c);
+}
+
 // the centre geometry of zone z
 GRIM_D void centre_geo(const DevCfg& c, const double* geoC, long long z, ZoneGeo<double>& G) {
   int i, j, k;
@@ -240,11 +249,13 @@ __global__ void k_cons(DevCfg c, const double* __restrict__ geoC, const double* 
 // The geometric source's transpose (interior zones): out += dS/dP(Ps)^T g
 // over the fluid rows, S^nu = -sqrt(-g) T^ka_la Gamma^la_(ka nu) of the
 // stage element at the centre (physics.cpp:360-420)
+template <int C, int V>
 __global__ void k_src_t(DevCfg c, const double* __restrict__ geoC, const double* __restrict__ gamma,
                         const double* __restrict__ P, const double* __restrict__ g, double* __restrict__ out) {
+  constexpr int DOF = 8 + C + V;
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= c.Zint) return;
-  typedef Dual<double, 8> D;
+  typedef Dual<double, DOF> D;
   const long long Z = c.Z;
   const long long z = interior_to_z(c, n);
   int i, j, k;
@@ -253,28 +264,25 @@ __global__ void k_src_t(DevCfg c, const double* __restrict__ geoC, const double*
   load_geo(G0, c, geoC, z, i, j, 0.5, 0.5);
   ZoneGeo<D> G;
   geo_const(G, G0);
-  D q[8];
-  for (int v = 0; v < 5; v++) q[v] = D::var(P[(long long)v * Z + z], v);
-  for (int v = 0; v < 3; v++) q[5 + v] = D::var(P[(long long)(c.B1 + v) * Z + z], 5 + v);
+  D q[DOF];
+  for (int v = 0; v < DOF; v++) q[v] = D::var(P[(long long)v * Z + z], v);
   ElemT<D, D> e;
-  elem_set<0, 0>(e, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], D(0.), D(0.), G, c);
+  elem_rows<C, V>(e, c, q, G);
   D T[4][4];
   for (int ka = 0; ka < 4; ka++)
-    for (int la = 0; la < 4; la++) T[ka][la] = tmunu<0, 0>(e, ka, la);
+    for (int la = 0; la < 4; la++) T[ka][la] = tmunu<C, V>(e, ka, la);
   const double* gam = gamma + gidx(c, i, j);
-  double acc[8] = {0., 0., 0., 0., 0., 0., 0., 0.};
+  double acc[DOF];
+  for (int m = 0; m < DOF; m++) acc[m] = 0.;
   for (int nu = 0; nu < 4; nu++) {
+    const double gb = g[(long long)(UU + nu) * Z + z];
+    if (gb == 0.) continue;
     D s(0.);
     for (int ka = 0; ka < 4; ka++)
       for (int la = 0; la < 4; la++) s -= T[ka][la] * (G0.g * __ldg(gam + (long long)(la * 16 + ka * 4 + nu) * c.GZ));
-    const double gb = g[(long long)(UU + nu) * Z + z];
-    if (gb != 0.)
-      for (int m = 0; m < 8; m++) acc[m] += s.d[m] * gb;
+    for (int m = 0; m < DOF; m++) acc[m] += s.d[m] * gb;
   }
-  for (int m = 0; m < 8; m++) {
-    const long long row = (m < 5) ? m : c.B1 + (m - 5);
-    out[row * Z + z] += acc[m];
-  }
+  for (int m = 0; m < DOF; m++) out[(long long)m * Z + z] += acc[m];
 }
 
 GRIM_D bool is_interior(const DevCfg& c, int i, int j, int k) {
@@ -375,36 +383,37 @@ __global__ void k_ct_t_raw(DevCfg c, const double* __restrict__ ebar, double* __
 }
 
 // the Riemann flux of one face (riemannsolver.cpp:202-328) on any scalar
-template <class S>
+template <int C, int V, class S>
 GRIM_D void riemann_flux(const DevCfg& c, int dir, const ZoneGeo<double>& G0, const S* pl, const S* pr, S* F) {
+  constexpr int NF = 5 + C + V, DOF = NF + 3;
   ZoneGeo<S> G;
   geo_const(G, G0);
   const int fd = dir + 1;
-  S FL[8], UL[8], FR[8], UR[8], mnL, mxL, mnR, mxR;
+  S FL[DOF], UL[DOF], FR[DOF], UR[DOF], mnL, mxL, mnR, mxR;
   {
     ElemT<S, S> e;
-    elem_set<0, 0>(e, pl[0], pl[1], pl[2], pl[3], pl[4], pl[5], pl[6], pl[7], S(0.), S(0.), G, c);
-    fluxes_fluid<0, 0>(e, fd, G.g, FL, 5, 5);
-    fluxes_B(e, fd, G.g, FL + 5);
-    fluxes_fluid<0, 0>(e, 0, G.g, UL, 5, 5);
-    fluxes_B(e, 0, G.g, UL + 5);
-    char_speeds<0, 0>(e, G, dir, c, mnL, mxL);
+    elem_rows<C, V>(e, c, pl, G);
+    fluxes_fluid<C, V>(e, fd, G.g, FL, 5, 5 + C);
+    fluxes_B(e, fd, G.g, FL + NF);
+    fluxes_fluid<C, V>(e, 0, G.g, UL, 5, 5 + C);
+    fluxes_B(e, 0, G.g, UL + NF);
+    char_speeds<C, V>(e, G, dir, c, mnL, mxL);
   }
   {
     ElemT<S, S> e;
-    elem_set<0, 0>(e, pr[0], pr[1], pr[2], pr[3], pr[4], pr[5], pr[6], pr[7], S(0.), S(0.), G, c);
-    fluxes_fluid<0, 0>(e, fd, G.g, FR, 5, 5);
-    fluxes_B(e, fd, G.g, FR + 5);
-    fluxes_fluid<0, 0>(e, 0, G.g, UR, 5, 5);
-    fluxes_B(e, 0, G.g, UR + 5);
-    char_speeds<0, 0>(e, G, dir, c, mnR, mxR);
+    elem_rows<C, V>(e, c, pr, G);
+    fluxes_fluid<C, V>(e, fd, G.g, FR, 5, 5 + C);
+    fluxes_B(e, fd, G.g, FR + NF);
+    fluxes_fluid<C, V>(e, 0, G.g, UR, 5, 5 + C);
+    fluxes_B(e, 0, G.g, UR + NF);
+    char_speeds<C, V>(e, G, dir, c, mnR, mxR);
   }
   const S cmin = dmin2(mnL, mnR), cmax = dmax2(mxL, mxR);
   if (c.riemann == GRIM_HLL) {
-    for (int v = 0; v < 8; v++) F[v] = (cmax * FL[v] - cmin * FR[v] + cmin * cmax * (UR[v] - UL[v])) / (cmax - cmin);
+    for (int v = 0; v < DOF; v++) F[v] = (cmax * FL[v] - cmin * FR[v] + cmin * cmax * (UR[v] - UL[v])) / (cmax - cmin);
   } else {
     const S cm = dmax2(cmax, -cmin);
-    for (int v = 0; v < 8; v++) F[v] = S(0.5) * (FL[v] + FR[v] - cm * (UR[v] - UL[v]));
+    for (int v = 0; v < DOF; v++) F[v] = S(0.5) * (FL[v] + FR[v] - cm * (UR[v] - UL[v]));
   }
 }
 
@@ -412,9 +421,12 @@ GRIM_D void riemann_flux(const DevCfg& c, int dir, const ZoneGeo<double>& G0, co
 // a = z - s and b = z takes Fbar (dof) and forms the adjoints of its two
 // reconstructed states, gl = (dF/dpl)^T Fbar (pl: the right-face state of a)
 // and gr = (dF/dpr)^T Fbar (pr: the left-face state of b), into gface
-// (rows 0..7 gl, 8..15 gr; zero on the faces the stencil does not use)
+// (rows 0..dof-1 gl, dof..2 dof-1 gr; zero on the faces the stencil does
+// not use)
+template <int C, int V>
 __global__ void k_faces_t(DevCfg c, int dir, const double* __restrict__ geoF, const double* __restrict__ P,
                           const double* __restrict__ Ft, double* __restrict__ gface) {
+  constexpr int DOF = 8 + C + V;
   long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (z >= c.Z) return;
   int i, j, k;
@@ -422,19 +434,19 @@ __global__ void k_faces_t(DevCfg c, int dir, const double* __restrict__ geoF, co
   const int x = dir == 0 ? i : (dir == 1 ? j : k);
   const int NT = dir == 0 ? c.N1T : (dir == 1 ? c.N2T : c.N3T);
   const long long Z = c.Z, s = stride_of(c, dir);
-  double fb[8];
+  double fb[DOF];
   bool any = false;
-  for (int v = 0; v < 8; v++) {
+  for (int v = 0; v < DOF; v++) {
     fb[v] = (x < 3 || x > NT - 3) ? 0. : Ft[((long long)dir * c.dof + v) * Z + z];
     any |= fb[v] != 0.;
   }
   if (!any) {
-    for (int v = 0; v < 16; v++) gface[(long long)v * Z + z] = 0.;
+    for (int v = 0; v < 2 * DOF; v++) gface[(long long)v * Z + z] = 0.;
     return;
   }
   // the face states
-  double pl[8], pr[8];
-  for (int v = 0; v < 8; v++) {
+  double pl[DOF], pr[DOF];
+  for (int v = 0; v < DOF; v++) {
     const double* a = P + (long long)v * Z;
     double lo, ro, lo2, ro2;
     recon_faces<double>(c.reconstruction, c.theta, a[z - 3 * s], a[z - 2 * s], a[z - s], a[z], a[z + s], lo, ro);
@@ -445,25 +457,26 @@ __global__ void k_faces_t(DevCfg c, int dir, const double* __restrict__ geoF, co
   // the face metric (the X3 faces of the axisymmetric metrics: the centre's)
   ZoneGeo<double> G;
   load_geo(G, c, geoF, z, i, j, dir == 0 ? 0. : 0.5, dir == 1 ? 0. : 0.5);
-  // dF/dpl and dF/dpr, 8 tangent lanes each
-  typedef Dual<double, 8> D8;
+  // dF/dpl and dF/dpr, dof tangent lanes each
+  typedef Dual<double, DOF> D8;
   for (int side = 0; side < 2; side++) {
-    D8 L[8], R[8], F[8];
-    for (int v = 0; v < 8; v++) {
+    D8 L[DOF], R[DOF], F[DOF];
+    for (int v = 0; v < DOF; v++) {
       L[v] = side == 0 ? D8::var(pl[v], v) : D8(pl[v]);
       R[v] = side == 1 ? D8::var(pr[v], v) : D8(pr[v]);
     }
-    riemann_flux<D8>(c, dir, G, L, R, F);
+    riemann_flux<C, V, D8>(c, dir, G, L, R, F);
     // the torus flux filter on the density flux of the inner / outer X1
     // faces: min(F, 0) / max(F, 0), so its derivative is 1 or 0
     double fr0 = fb[0];
     if (c.problem == GRIM_PROBLEM_TORUS && dir == 0 &&
         ((x == c.g1 && F[0].v > 0.) || (x == c.N1 + c.g1 && F[0].v < 0.)))
       fr0 = 0.;
-    for (int k2 = 0; k2 < 8; k2++) {
+    for (int k2 = 0; k2 < DOF; k2++) {
       double acc = fr0 * F[0].d[k2];
-      for (int r = 1; r < 8; r++) acc += fb[r] * F[r].d[k2];
-      gface[(long long)(side * 8 + k2) * Z + z] = acc;
+      for (int r = 1; r < DOF; r++)
+        if (fb[r] != 0.) acc += fb[r] * F[r].d[k2];
+      gface[(long long)(side * DOF + k2) * Z + z] = acc;
     }
   }
 }
@@ -485,7 +498,7 @@ __global__ void k_recon_t(DevCfg c, int dir, const double* __restrict__ P, const
   const int NT = dir == 0 ? c.N1T : (dir == 1 ? c.N2T : c.N3T);
   const long long Z = c.Z, s = stride_of(c, dir);
   typedef Dual<double, 5> D5;
-  for (int v = 0; v < 8; v++) {
+  for (int v = 0; v < c.dof; v++) {
     const double* a = P + (long long)v * Z;
     double acc = 0.;
     for (int m = 4; m >= 0; m--) {
@@ -494,7 +507,7 @@ __global__ void k_recon_t(DevCfg c, int dir, const double* __restrict__ P, const
       if (y < 2 || y > NT - 3) continue;
       const long long zy = z + (long long)(2 - m) * s;
       const double gl = (y + 1 <= NT - 1) ? gface[(long long)v * Z + zy + s] : 0.;
-      const double gr = gface[(long long)(8 + v) * Z + zy];
+      const double gr = gface[(long long)(c.dof + v) * Z + zy];
       if (gl == 0. && gr == 0.) continue;
       D5 yb[5];
       for (int mm = 0; mm < 5; mm++) yb[mm] = D5::var(a[zy + (mm - 2) * s], mm);
@@ -555,6 +568,361 @@ __global__ void k_fold(DevCfg c, const double* __restrict__ q, double* __restric
         for (int m = 0; m < n3; m++) s += q[(long long)v * Z + zidx(c, ys1[a], ys2[b], ys3[m])];
     out[(long long)v * Z + z] = s;
   }
+}
+
+
+// ---- extended MHD (conduction, viscosity) -----------------------------------
+// The EMHD stage residual of one zone (residual.cpp with the stage
+// constants of timestep.cpp: elemOld from P0, the reference element from
+// Ps, elemOld itself on the half stage) on the tangent scalar, for the
+// three seeds the adjoint needs: the unknowns and the new field, P0, Ps.
+// divF and Sexp are the stage's values (their rows enter additively, times
+// the row normalisation of q and deltaP).  normQ / normDP are returned for
+// those rows' dR / d divF.
+template <int C, int V, class D>
+GRIM_D void emhd_residual(const DevCfg& c, int stage, double dtp, const D* Pf, const D* Bn, const D* p0,
+                          const D* ps, const double* divF, const double* Sexp, const ZoneGeo<D>& G, D* R, D& normQ,
+                          D& normDP) {
+  constexpr int NF = 5 + C + V, Q = 5, DP = 5 + C;
+  ElemT<D, D> eo, er;
+  elem_rows<C, V>(eo, c, p0, G);
+  if (stage == GRIM_HALF_STEP) er = eo;
+  else elem_rows<C, V>(er, c, ps, G);
+  D Uold[NF];
+  fluxes_fluid<C, V>(eo, 0, G.g, Uold, 5, 5 + C);
+  ElemT<D, D> e;
+  elem_set<C, V>(e, Pf[0], Pf[1], Pf[2], Pf[3], Pf[4], Bn[0], Bn[1], Bn[2], C ? Pf[Q] : D(0.), V ? Pf[DP] : D(0.),
+                 G, c);
+  D U[NF];
+  fluxes_fluid<C, V>(e, 0, G.g, U, 5, 5 + C);
+  for (int v = 0; v < NF; v++) R[v] = (U[v] - Uold[v]) / dtp + divF[v] + Sexp[v];
+  D dtuCov[4];
+  for (int mu = 0; mu < 4; mu++) dtuCov[mu] = (e.uCov[mu] - eo.uCov[mu]) / dtp;
+  D div(0.);
+  for (int mu = 0; mu < 4; mu++) div += G.gcon[0][mu] * dtuCov[mu];
+  const D rr = er.rho, rtau = er.tau, rT = er.temperature;
+  normQ = D(1.);
+  normDP = D(1.);
+  if (V) {
+    const D rnu = er.nu;
+    D d0 = -div * rr * rnu;
+    for (int mu = 0; mu < 4; mu++) d0 += 3. * rr * rnu * er.bCon[0] * er.bCon[mu] / er.bSqr * dtuCov[mu];
+    if (c.hoVisc == 1) d0 = d0 * dsqrt(rtau / rr / rnu / rT);
+    D sdt = -G.g * d0 / rtau;
+    if (c.hoVisc == 1) sdt = sdt - 0.5 * G.g * div * er.deltaPTilde;
+    const D simp = G.g * Pf[DP] / rtau;
+    const D sOld = G.g * eo.deltaPTilde / rtau;
+    normDP = c.hoVisc ? dsqrt(rr * rnu * rT * rtau) : rtau;
+    R[DP] = (R[DP] + 0.5 * (sOld + simp) + sdt) * normDP;
+  }
+  if (C) {
+    const D rchi = er.chi;
+    D qq = -rr * rchi * er.bCon[0] / er.bNorm * (e.temperature - eo.temperature) / dtp;
+    for (int nu = 0; nu < 4; nu++) qq -= rr * rchi * rT * er.bCon[nu] / er.bNorm * er.uCon[0] * dtuCov[nu];
+    if (c.hoCond == 1) qq = qq * (dsqrt(rtau / rr / rchi) / rT);
+    D sdt = -G.g * qq / rtau;
+    if (c.hoCond == 1) sdt = sdt - 0.5 * G.g * div * er.qTilde;
+    const D simp = G.g * Pf[Q] / rtau;
+    const D sOld = G.g * eo.qTilde / rtau;
+    normQ = c.hoCond ? rT * dsqrt(rr * rchi * rtau) : rtau;
+    R[Q] = (R[Q] + 0.5 * (sOld + simp) + sdt) * normQ;
+  }
+}
+
+// Gaussian elimination with partial pivoting, n x n
+template <int N>
+GRIM_D void solveN(double A[N][N], double b[N], double x[N]) {
+  for (int kk = 0; kk < N; kk++) {
+    int p = kk;
+    double best = ::fabs(A[kk][kk]);
+    for (int r = kk + 1; r < N; r++)
+      if (::fabs(A[r][kk]) > best) { best = ::fabs(A[r][kk]); p = r; }
+    if (p != kk) {
+      for (int cc = 0; cc < N; cc++) { const double t = A[kk][cc]; A[kk][cc] = A[p][cc]; A[p][cc] = t; }
+      const double t = b[kk]; b[kk] = b[p]; b[p] = t;
+    }
+    for (int r = kk + 1; r < N; r++) {
+      const double f = A[r][kk] / A[kk][kk];
+      for (int cc = kk; cc < N; cc++) A[r][cc] -= f * A[kk][cc];
+      b[r] -= f * b[kk];
+    }
+  }
+  for (int r = N - 1; r >= 0; r--) {
+    double s = b[r];
+    for (int cc = r + 1; cc < N; cc++) s -= A[r][cc] * x[cc];
+    x[r] = s / A[r][r];
+  }
+}
+
+// EMHD stage adjoint at the stage's solution P (interior zones): lam ->
+// g (dL/d divF = dL/d Sexp, dof rows), p0bar (+)= dL/dP0 through the stage
+// constants and the induction, psl = dL/dPs through the reference element
+// (full stage; zero on the half stage, whose reference element is elemOld)
+template <int C, int V>
+__global__ void k_stage_emhd(DevCfg c, const double* __restrict__ geoC, int stage, double dtp,
+                             const double* __restrict__ P, const double* __restrict__ P0,
+                             const double* __restrict__ Ps, const double* __restrict__ divF,
+                             const double* __restrict__ Sexp, const double* __restrict__ lam, double* __restrict__ g,
+                             double* __restrict__ p0bar, double* __restrict__ psl) {
+  constexpr int NF = 5 + C + V, DOF = NF + 3, Q = 5, DP = 5 + C;
+  typedef Dual<double, DOF> D;
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= c.Zint) return;
+  const long long Z = c.Z;
+  const long long z = interior_to_z(c, n);
+  double lv[DOF];
+  bool any = false;
+  for (int v = 0; v < DOF; v++) {
+    lv[v] = lam[(long long)v * Z + z];
+    any |= lv[v] != 0.;
+  }
+  if (!any) {
+    for (int v = 0; v < DOF; v++) { g[(long long)v * Z + z] = 0.; psl[(long long)v * Z + z] = 0.; }
+    return;
+  }
+  ZoneGeo<double> G0;
+  centre_geo(c, geoC, z, G0);
+  ZoneGeo<D> G;
+  geo_const(G, G0);
+  double pv[DOF], p0v[DOF], psv[DOF], dF[NF], sE[NF];
+  for (int v = 0; v < DOF; v++) {
+    pv[v] = P[(long long)v * Z + z];
+    p0v[v] = P0[(long long)v * Z + z];
+    psv[v] = Ps[(long long)v * Z + z];
+  }
+  for (int v = 0; v < NF; v++) { dF[v] = divF[(long long)v * Z + z]; sE[v] = Sexp[(long long)v * Z + z]; }
+  D Pf[NF], Bn[3], a0[DOF], as[DOF], R[NF], nQ, nDP;
+  // seed 1: the unknowns and the new field
+  for (int v = 0; v < NF; v++) Pf[v] = D::var(pv[v], v);
+  for (int k = 0; k < 3; k++) Bn[k] = D::var(pv[NF + k], NF + k);
+  for (int v = 0; v < DOF; v++) { a0[v] = D(p0v[v]); as[v] = D(psv[v]); }
+  emhd_residual<C, V, D>(c, stage, dtp, Pf, Bn, a0, as, dF, sE, G, R, nQ, nDP);
+  double AT[NF][NF], b[NF], mu[NF];
+  for (int r = 0; r < NF; r++) {
+    b[r] = lv[r];
+    for (int k = 0; k < NF; k++) AT[r][k] = R[k].d[r];
+  }
+  solveN<NF>(AT, b, mu);
+  double beta[3];
+  for (int k = 0; k < 3; k++) {
+    beta[k] = lv[NF + k];
+    for (int r = 0; r < NF; r++) beta[k] -= R[r].d[NF + k] * mu[r];
+  }
+  for (int v = 0; v < NF; v++) {
+    const double sc = (C && v == Q) ? nQ.v : ((V && v == DP) ? nDP.v : 1.);
+    g[(long long)v * Z + z] = -mu[v] * sc;
+  }
+  for (int k = 0; k < 3; k++) g[(long long)(NF + k) * Z + z] = -dtp / G0.g * beta[k];
+  // seed 2: P0 (elemOld, the old conserved variables, and on the half
+  // stage the reference element); the induction adds beta to B0
+  for (int v = 0; v < NF; v++) Pf[v] = D(pv[v]);
+  for (int k = 0; k < 3; k++) Bn[k] = D(pv[NF + k]);
+  for (int v = 0; v < DOF; v++) a0[v] = D::var(p0v[v], v);
+  emhd_residual<C, V, D>(c, stage, dtp, Pf, Bn, a0, as, dF, sE, G, R, nQ, nDP);
+  for (int v = 0; v < DOF; v++) {
+    double s = (v >= NF) ? beta[v - NF] : 0.;
+    for (int r = 0; r < NF; r++) s -= R[r].d[v] * mu[r];
+    p0bar[(long long)v * Z + z] += s;
+  }
+  // seed 3: Ps (the full stage's reference element)
+  if (stage == GRIM_HALF_STEP) {
+    for (int v = 0; v < DOF; v++) psl[(long long)v * Z + z] = 0.;
+    return;
+  }
+  for (int v = 0; v < DOF; v++) { a0[v] = D(p0v[v]); as[v] = D::var(psv[v], v); }
+  emhd_residual<C, V, D>(c, stage, dtp, Pf, Bn, a0, as, dF, sE, G, R, nQ, nDP);
+  for (int v = 0; v < DOF; v++) {
+    double s = 0.;
+    for (int r = 0; r < NF; r++) s -= R[r].d[v] * mu[r];
+    psl[(long long)v * Z + z] = s;
+  }
+}
+
+// The EMHD explicit source of one zone (computeEMHDGradients and the
+// sources of physics.cpp:502-586): the q and deltaP rows from the stage
+// element e and the limited slopes sl[d][m] of u_mu (m < 4) and T (m = 4)
+template <int C, int V, class S>
+GRIM_D void emhd_source(const DevCfg& c, const ElemT<S, S>& e, const ZoneGeo<S>& G, const double* gam, S sl[3][5],
+                        S& SQ, S& SDP) {
+  S gu[4][4], gT[4];
+  for (int mu = 0; mu < 4; mu++) {
+    gu[0][mu] = S(0.);
+    gu[1][mu] = sl[0][mu];
+    gu[2][mu] = (c.dim > 1) ? sl[1][mu] : S(0.);
+    gu[3][mu] = (c.dim > 2) ? sl[2][mu] : S(0.);
+    if (gam)
+      for (int nu = 0; nu < 4; nu++)
+        for (int la = 0; la < 4; la++) gu[nu][mu] -= __ldg(gam + (long long)(la * 16 + nu * 4 + mu) * c.GZ) * e.uCov[la];
+  }
+  gT[0] = S(0.);
+  gT[1] = sl[0][4];
+  gT[2] = (c.dim > 1) ? sl[1][4] : S(0.);
+  gT[3] = (c.dim > 2) ? sl[2][4] : S(0.);
+  S dv(0.);
+  for (int mu = 0; mu < 4; mu++)
+    for (int nu = 0; nu < 4; nu++) dv += G.gcon[mu][nu] * gu[mu][nu];
+  SQ = S(0.);
+  SDP = S(0.);
+  if (V) {
+    S d0 = -dv * e.rho * e.nu;
+    for (int mu = 0; mu < 4; mu++)
+      for (int nu = 0; nu < 4; nu++) d0 += 3. * e.rho * e.nu * e.bCon[mu] * e.bCon[nu] / e.bSqr * gu[mu][nu];
+    const S d0t = (c.hoVisc == 1) ? d0 * dsqrt(e.tau / e.rho / e.nu / e.temperature) : d0;
+    S s = -G.g * d0t / e.tau;
+    if (c.hoVisc == 1) s = s - 0.5 * G.g * dv * e.deltaPTilde;
+    SDP = s;
+  }
+  if (C) {
+    S qq(0.);
+    for (int mu = 0; mu < 4; mu++) {
+      qq -= e.rho * e.chi * e.bCon[mu] / e.bNorm * gT[mu];
+      for (int nu = 0; nu < 4; nu++) qq -= e.rho * e.chi * e.temperature * e.bCon[nu] / e.bNorm * e.uCon[mu] * gu[mu][nu];
+    }
+    const S qt = (c.hoCond == 1) ? qq * dsqrt(e.tau / e.rho / e.chi) / e.temperature : qq;
+    S s = -G.g * qt / e.tau;
+    if (c.hoCond == 1) s = s - 0.5 * G.g * dv * e.qTilde;
+    SQ = s;
+  }
+}
+
+// the limited slope of u_mu / T along d at zone z (the forward's st())
+GRIM_D double uT_slope(const DevCfg& c, const double* uT, long long z, int d, int m) {
+  const long long sd = stride_of(c, d);
+  const double* a = uT + (long long)m * c.Z + z;
+  return recon_slope(c.reconstruction, c.theta, a[-2 * sd], a[-sd], a[0], a[sd], a[2 * sd], c.dX[d]);
+}
+
+// The EMHD source's transpose, step 1 (interior zones): its dependence on
+// the zone's own stage element into out, and the adjoints of the slopes it
+// reads (sbar, dim x 5 per zone)
+template <int C, int V>
+__global__ void k_emhd_src_t(DevCfg c, const double* __restrict__ geoC, const double* __restrict__ gamma,
+                             const double* __restrict__ Ps, const double* __restrict__ uT,
+                             const double* __restrict__ g, double* __restrict__ out, double* __restrict__ sbar) {
+  constexpr int DOF = 8 + C + V, Q = 5, DP = 5 + C;
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= c.Zint) return;
+  const long long Z = c.Z;
+  const long long z = interior_to_z(c, n);
+  const double gQ = C ? g[(long long)Q * Z + z] : 0., gD = V ? g[(long long)DP * Z + z] : 0.;
+  if (gQ == 0. && gD == 0.) {
+    for (int m = 0; m < 15; m++) sbar[(long long)m * Z + z] = 0.;
+    return;
+  }
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  ZoneGeo<double> G0;
+  load_geo(G0, c, geoC, z, i, j, 0.5, 0.5);
+  const double* gam = gamma ? gamma + gidx(c, i, j) : nullptr;
+  double slv[3][5];
+  for (int d = 0; d < 3; d++)
+    for (int m = 0; m < 5; m++) slv[d][m] = d < c.dim ? uT_slope(c, uT, z, d, m) : 0.;
+  {
+    // the zone's element, slopes fixed
+    typedef Dual<double, DOF> D;
+    ZoneGeo<D> G;
+    geo_const(G, G0);
+    D q[DOF], sl[3][5], SQ, SD;
+    for (int v = 0; v < DOF; v++) q[v] = D::var(Ps[(long long)v * Z + z], v);
+    for (int d = 0; d < 3; d++)
+      for (int m = 0; m < 5; m++) sl[d][m] = D(slv[d][m]);
+    ElemT<D, D> e;
+    elem_rows<C, V>(e, c, q, G);
+    emhd_source<C, V, D>(c, e, G, gam, sl, SQ, SD);
+    for (int v = 0; v < DOF; v++) out[(long long)v * Z + z] += SQ.d[v] * gQ + SD.d[v] * gD;
+  }
+  {
+    // the slopes, element fixed
+    typedef Dual<double, 15> D;
+    ZoneGeo<D> G;
+    geo_const(G, G0);
+    D q[DOF], sl[3][5], SQ, SD;
+    for (int v = 0; v < DOF; v++) q[v] = D(Ps[(long long)v * Z + z]);
+    for (int d = 0; d < 3; d++)
+      for (int m = 0; m < 5; m++) sl[d][m] = D::var(slv[d][m], d * 5 + m);
+    ElemT<D, D> e;
+    elem_rows<C, V>(e, c, q, G);
+    emhd_source<C, V, D>(c, e, G, gam, sl, SQ, SD);
+    for (int m = 0; m < 15; m++) sbar[(long long)m * Z + z] = SQ.d[m] * gQ + SD.d[m] * gD;
+  }
+}
+
+// step 2 (every zone): the adjoint of its u_mu, T from the slopes of the
+// interior zones whose 5-point stencils hold it, gathered in a fixed order
+__global__ void k_emhd_slope_t(DevCfg c, const double* __restrict__ uT, const double* __restrict__ sbar,
+                               double* __restrict__ uTbar) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  typedef Dual<double, 5> D5;
+  double acc[5] = {0., 0., 0., 0., 0.};
+  for (int d = 0; d < c.dim; d++) {
+    const long long sd = stride_of(c, d);
+    const int x = d == 0 ? i : (d == 1 ? j : k);
+    const int g0 = d == 0 ? c.g1 : (d == 1 ? c.g2 : c.g3);
+    const int N = d == 0 ? c.N1 : (d == 1 ? c.N2 : c.N3);
+    for (int p = 0; p < 5; p++) {
+      // this zone is point p of the stencil of zone y = x + 2 - p
+      const int y = x + 2 - p;
+      if (y < g0 || y >= g0 + N) continue;
+      const long long zy = z + (long long)(2 - p) * sd;
+      int iy, jy, ky;
+      zijk(c, zy, iy, jy, ky);
+      const bool inside = iy >= c.g1 && iy < c.N1 + c.g1 && (c.dim < 2 || (jy >= c.g2 && jy < c.N2 + c.g2)) &&
+                          (c.dim < 3 || (ky >= c.g3 && ky < c.N3 + c.g3));
+      if (!inside) continue;
+      for (int m = 0; m < 5; m++) {
+        const double sb = sbar[(long long)(d * 5 + m) * c.Z + zy];
+        if (sb == 0.) continue;
+        const double* a = uT + (long long)m * c.Z + zy;
+        D5 yb[5];
+        for (int mm = 0; mm < 5; mm++) yb[mm] = D5::var(a[(mm - 2) * sd], mm);
+        const D5 sl = recon_slope<D5>(c.reconstruction, c.theta, yb[0], yb[1], yb[2], yb[3], yb[4], c.dX[d]);
+        acc[m] += sb * sl.d[p];
+      }
+    }
+  }
+  for (int m = 0; m < 5; m++) uTbar[(long long)m * c.Z + z] = acc[m];
+}
+
+// step 3 (every zone): u_mu, T of the zone's element back to its primitives
+template <int C, int V>
+__global__ void k_emhd_uT_t(DevCfg c, const double* __restrict__ geoC, const double* __restrict__ Ps,
+                            const double* __restrict__ uTbar, double* __restrict__ out) {
+  constexpr int DOF = 8 + C + V;
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  const long long Z = c.Z;
+  double ub[5];
+  bool any = false;
+  for (int m = 0; m < 5; m++) { ub[m] = uTbar[(long long)m * Z + z]; any |= ub[m] != 0.; }
+  if (!any) return;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  ZoneGeo<double> G0;
+  load_geo(G0, c, geoC, z, i, j, 0.5, 0.5);
+  typedef Dual<double, DOF> D;
+  ZoneGeo<D> G;
+  geo_const(G, G0);
+  D q[DOF];
+  for (int v = 0; v < DOF; v++) q[v] = D::var(Ps[(long long)v * Z + z], v);
+  ElemT<D, D> e;
+  elem_rows<C, V>(e, c, q, G);
+  for (int v = 0; v < DOF; v++) {
+    double s = 0.;
+    for (int m = 0; m < 4; m++) s += e.uCov[m].d[v] * ub[m];
+    s += e.temperature.d[v] * ub[4];
+    out[(long long)v * Z + z] += s;
+  }
+}
+
+// out[interior] += a[interior] (dof rows)
+__global__ void k_add_interior(DevCfg c, const double* __restrict__ a, double* __restrict__ out) {
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= c.Zint) return;
+  const long long z = interior_to_z(c, n);
+  for (int v = 0; v < c.dof; v++) out[(long long)v * c.Z + z] += a[(long long)v * c.Z + z];
 }
 
 // ---- the torus problem's hooks (problem.cpp): floors after each stage,
@@ -742,7 +1110,10 @@ static void stencil_q(const DevCfg& c, const AdjointGeo& geo, const double* P, c
   k_ct_t_raw<<<nblk(c.Z, 256), 256, 0, s>>>(c, ebar, Ft);
   cudaMemsetAsync(q, 0, (size_t)c.dof * bZ, s);
   for (int d = 0; d < c.dim; d++) {
-    k_faces_t<<<nblk(c.Z, 64), 64, 0, s>>>(c, d, geo.geoF[d], P, Ft, gface);
+    if (c.conduction && c.viscosity) k_faces_t<1, 1><<<nblk(c.Z, 32), 32, 0, s>>>(c, d, geo.geoF[d], P, Ft, gface);
+    else if (c.conduction) k_faces_t<1, 0><<<nblk(c.Z, 32), 32, 0, s>>>(c, d, geo.geoF[d], P, Ft, gface);
+    else if (c.viscosity) k_faces_t<0, 1><<<nblk(c.Z, 32), 32, 0, s>>>(c, d, geo.geoF[d], P, Ft, gface);
+    else k_faces_t<0, 0><<<nblk(c.Z, 64), 64, 0, s>>>(c, d, geo.geoF[d], P, Ft, gface);
     k_recon_t<<<nblk(c.Z, 64), 64, 0, s>>>(c, d, P, gface, q);
   }
 }
@@ -753,10 +1124,13 @@ void adjoint_stencil_t(const DevCfg& c, const AdjointGeo& geo, const double* P, 
   adj::k_fold<<<adj::nblk(c.Zint, 128), 128, 0, s>>>(c, q, out);
 }
 
-void adjoint_step(const DevCfg& c, const AdjointGeo& geo, double dt, const AdjointStates& st, double* lam,
-                  const AdjointBufs& w, cudaStream_t s) {
+template <int C, int V>
+static void adjoint_step_t(const DevCfg& c, const AdjointGeo& geo, double dt, const AdjointStates& st, double* lam,
+                           const AdjointBufs& w, cudaStream_t s) {
   using namespace adj;
+  constexpr bool emhd = C || V;
   const bool torus = c.problem == GRIM_PROBLEM_TORUS;
+  const size_t rows = (size_t)c.dof * c.Z * sizeof(double);
   // the start-of-stage hooks' and the ghost fill's transposes: q -> out
   auto hooks_fold = [&](const double* Pfill, double* out) {
     if (torus) {
@@ -765,19 +1139,50 @@ void adjoint_step(const DevCfg& c, const AdjointGeo& geo, double dt, const Adjoi
     }
     k_fold<<<nblk(c.Zint, 128), 128, 0, s>>>(c, w.q, out);
   };
+  // the explicit sources' transposes at the stage input Ps, into q
+  auto sources = [&](const double* Ps) {
+    if (geo.gamma) k_src_t<C, V><<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, geo.gamma, Ps, w.g, w.q);
+    if constexpr (emhd) {
+      fast::emhd_prepass(c, Ps, geo.geoC, w.uTs, s);
+      k_emhd_src_t<C, V><<<nblk(c.Zint, 32), 32, 0, s>>>(c, geo.geoC, geo.gamma, Ps, w.uTs, w.g, w.q, w.sbar);
+      k_emhd_slope_t<<<nblk(c.Z, 64), 64, 0, s>>>(c, w.uTs, w.sbar, w.uTbar);
+      k_emhd_uT_t<C, V><<<nblk(c.Z, 64), 64, 0, s>>>(c, geo.geoC, Ps, w.uTbar, w.q);
+    }
+  };
   // full stage: the floors at its finish, then the stage at its Newton solution
   if (torus) k_floor_t<<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, st.P1Sol, lam);
-  k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, geo.geoC, st.P1Sol, dt, lam, w.g, w.ubar, w.bacc, 0);
+  if constexpr (emhd) {
+    cudaMemsetAsync(w.p0bar, 0, rows, s);
+    k_stage_emhd<C, V><<<nblk(c.Zint, 32), 32, 0, s>>>(c, geo.geoC, GRIM_FULL_STEP, dt, st.P1Sol, st.P0eff, st.PhEff,
+                                                      st.divF1, st.Sexp1, lam, w.g, w.p0bar, w.psl);
+  } else {
+    k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, geo.geoC, st.P1Sol, dt, lam, w.g, w.ubar, w.bacc, 0);
+  }
   stencil_q(c, geo, st.PhEff, w.g, w.Ft, w.ebar, w.q, w.gface, s);
-  if (geo.gamma) k_src_t<<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, geo.gamma, st.PhEff, w.g, w.q);
+  sources(st.PhEff);
+  if constexpr (emhd) k_add_interior<<<nblk(c.Zint, 128), 128, 0, s>>>(c, w.psl, w.q);
   hooks_fold(st.PhFill, w.lamh);
   // half stage
   if (torus) k_floor_t<<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, st.PhSol, w.lamh);
-  k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, geo.geoC, st.PhSol, 0.5 * dt, w.lamh, w.g, w.ubar, w.bacc, 1);
+  if constexpr (emhd) {
+    k_stage_emhd<C, V><<<nblk(c.Zint, 32), 32, 0, s>>>(c, geo.geoC, GRIM_HALF_STEP, 0.5 * dt, st.PhSol, st.P0eff,
+                                                      st.P0eff, st.divFh, st.Sexph, w.lamh, w.g, w.p0bar, w.psl);
+  } else {
+    k_stage<<<nblk(c.Zint, 128), 128, 0, s>>>(c, geo.geoC, st.PhSol, 0.5 * dt, w.lamh, w.g, w.ubar, w.bacc, 1);
+  }
   stencil_q(c, geo, st.P0eff, w.g, w.Ft, w.ebar, w.q, w.gface, s);
-  if (geo.gamma) k_src_t<<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, geo.gamma, st.P0eff, w.g, w.q);
-  k_cons<<<nblk(c.Zint, 128), 128, 0, s>>>(c, geo.geoC, st.P0eff, w.ubar, w.bacc, w.q);
+  sources(st.P0eff);
+  if constexpr (emhd) k_add_interior<<<nblk(c.Zint, 128), 128, 0, s>>>(c, w.p0bar, w.q);
+  else k_cons<<<nblk(c.Zint, 128), 128, 0, s>>>(c, geo.geoC, st.P0eff, w.ubar, w.bacc, w.q);
   hooks_fold(st.P0fill, lam);
+}
+
+void adjoint_step(const DevCfg& c, const AdjointGeo& geo, double dt, const AdjointStates& st, double* lam,
+                  const AdjointBufs& w, cudaStream_t s) {
+  if (c.conduction && c.viscosity) adjoint_step_t<1, 1>(c, geo, dt, st, lam, w, s);
+  else if (c.conduction) adjoint_step_t<1, 0>(c, geo, dt, st, lam, w, s);
+  else if (c.viscosity) adjoint_step_t<0, 1>(c, geo, dt, st, lam, w, s);
+  else adjoint_step_t<0, 0>(c, geo, dt, st, lam, w, s);
 }
 
 }  // namespace grim

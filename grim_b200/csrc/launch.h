@@ -60,6 +60,14 @@ struct AdjointBufs {
   double* lamh;  // dL/dPh
   double* ubar;  // nf x Z: dL/dU(P0)
   double* bacc;  // 3 x Z: dL/dB0 through the induction
+  // EMHD: dL/dP0 through both stages' constants (dof x Z), dL/dPs through
+  // the full stage's reference element (dof x Z), the source's slope
+  // adjoints (15 x Z), the u_mu, T adjoints (5 x Z), u_mu, T of Ps (5 x Z)
+  double* p0bar;
+  double* psl;
+  double* sbar;
+  double* uTbar;
+  double* uTs;
 };
 // the geometry the adjoint reads (all null in Minkowski)
 struct AdjointGeo {
@@ -75,6 +83,12 @@ struct AdjointStates {
   const double* PhFill;  // primHalfStep after the half stage's finish, ghosts filled
   const double* PhEff;   // the same after the problem's boundary hooks (the full stage's input)
   const double* P1Sol;   // the full stage's Newton solution (before its finish)
+  // EMHD: each stage's divF and Sexp (nf x Z; the row normalisation of q
+  // and deltaP multiplies them)
+  const double* divFh;
+  const double* Sexph;
+  const double* divF1;
+  const double* Sexp1;
 };
 // lam (dL/dP1, interior) -> dL/dP0 for one step of fixed dt
 void adjoint_step(const DevCfg& c, const AdjointGeo& geo, double dt, const AdjointStates& st, double* lam,

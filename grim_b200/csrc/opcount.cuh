@@ -60,6 +60,10 @@ struct Cnt {
   friend GRIM_D bool isfinite(Cnt a) { return ::isfinite((double)a.v); }
 };
 
+// the value of a counted scalar (the closures read the geometry's values)
+template <class B>
+GRIM_HD double val_of(const Cnt<B>& x) { return (double)x.v; }
+
 template <class B>
 struct Lift<Cnt<B>> {
   GRIM_HD static Cnt<B> of(double x) { return Cnt<B>(x); }

@@ -134,13 +134,13 @@ GRIM_D void closure(ElemT<S, R>& e, const ZoneGeo<R>& G, const DevCfg& c) {
     e.nu = cs * cs * e.tau;
   } else if (c.closure == GRIM_CLOSURE_TAU_PROFILE) {
     R s = (G.x2 - (R)c.X2Start) / ((R)c.X2End - (R)c.X2Start);
-    e.tau = Lift<S>::of((double)((R)c.tau0 + ((R)c.tau1 - (R)c.tau0) * s));
+    e.tau = Lift<S>::of((double)val_of((R)c.tau0 + ((R)c.tau1 - (R)c.tau0) * s));
     e.chi = cs * cs * e.tau;
     e.nu = cs * cs * e.tau;
   } else {
     // torus/problem.cpp:7-55
     typedef typename Real<S>::type T;
-    const T Dyn = (T)G.dyn;
+    const T Dyn = (T)val_of(G.dyn);
     S t = Lift<S>::of((double)Dyn);
     if (c.conduction) {
       S Qmax = (T)c.CondClosure * e.rho * dcube(cs);

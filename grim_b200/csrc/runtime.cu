@@ -1577,12 +1577,12 @@ static int adjoint_scope(grim_handle* h) {
   auto ok_bc = [](int b) { return b == GRIM_PERIODIC || b == GRIM_OUTFLOW || b == GRIM_MIRROR; };
   const bool bcs = ok_bc(c.boundaryLeft) && ok_bc(c.boundaryRight) && ok_bc(c.boundaryBottom) &&
                    ok_bc(c.boundaryTop) && (c.dim < 3 || (ok_bc(c.boundaryFront) && ok_bc(c.boundaryBack)));
-  const bool torusOk = c.problem == GRIM_PROBLEM_TORUS && c.metric != GRIM_MINKOWSKI && c.numGhost == 3 &&
-                       (c.dim < 2 || c.N2 >= 6);
-  if ((c.dim != 2 && c.dim != 3) || c.conduction || c.viscosity || !bcs ||
-      (c.problem != GRIM_PROBLEM_NONE && !torusOk) || c.N3Global > 0) {
-    set_err("adjoint: supported for 2D and 3D ideal MHD (Minkowski or MKS) with periodic, outflow or mirror "
-            "boundaries, without problem hooks or with the torus problem's (MKS, N2 >= 6)");
+  const bool emhd = c.conduction || c.viscosity;
+  const bool torusOk = c.problem == GRIM_PROBLEM_TORUS && !emhd && c.metric != GRIM_MINKOWSKI &&
+                       c.numGhost == 3 && (c.dim < 2 || c.N2 >= 6);
+  if ((c.dim != 2 && c.dim != 3) || !bcs || (c.problem != GRIM_PROBLEM_NONE && !torusOk) || c.N3Global > 0) {
+    set_err("adjoint: supported for 2D and 3D ideal or extended MHD (Minkowski or MKS) with periodic, outflow or "
+            "mirror boundaries, without problem hooks, or ideal MHD with the torus problem's (MKS, N2 >= 6)");
     return GRIM_ENOTSUP;
   }
   return GRIM_OK;
@@ -1604,7 +1604,8 @@ static grim::AdjointGeo adjoint_geo(const grim_handle* h) {
 static int adjoint_work(grim_handle* h, AdjointBufs& w, double*& lam) {
   const DevCfg& c = h->dc;
   if (!h->adjWork) {
-    const size_t words = (size_t)c.Z * (c.dof * (6 + c.dim) + 3 + c.nf + 3);
+    const bool emhd = c.conduction || c.viscosity;
+    const size_t words = (size_t)c.Z * (c.dof * (6 + c.dim) + 3 + c.nf + 3 + (emhd ? 2 * c.dof + 25 : 0));
     if (cudaMalloc(&h->adjWork, words * sizeof(double)) != cudaSuccess) {
       set_err("adjoint: work allocation failed");
       return GRIM_ENOMEM;
@@ -1619,7 +1620,15 @@ static int adjoint_work(grim_handle* h, AdjointBufs& w, double*& lam) {
   w.lamh = wp; wp += (size_t)c.dof * c.Z;
   w.ubar = wp; wp += (size_t)c.nf * c.Z;
   w.bacc = wp; wp += (size_t)3 * c.Z;
-  lam = wp;
+  lam = wp; wp += (size_t)c.dof * c.Z;
+  w.p0bar = w.psl = w.sbar = w.uTbar = w.uTs = nullptr;
+  if (c.conduction || c.viscosity) {
+    w.p0bar = wp; wp += (size_t)c.dof * c.Z;
+    w.psl = wp; wp += (size_t)c.dof * c.Z;
+    w.sbar = wp; wp += (size_t)15 * c.Z;
+    w.uTbar = wp; wp += (size_t)5 * c.Z;
+    w.uTs = wp;
+  }
   return GRIM_OK;
 }
 
@@ -1683,8 +1692,10 @@ int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, in
   const DevCfg& c = h->dc;
   const size_t bytes = (size_t)c.dof * h->bytesZ;
   const int every = h->adjEvery;
-  // segment states (six per step: grim::AdjointStates) and work buffers
-  while ((int)h->adjSeg.size() < 6 * every + 1) {
+  // segment states (six per step: grim::AdjointStates, four more with EMHD)
+  // and work buffers
+  const int kinds = (c.conduction || c.viscosity) ? 10 : 6;
+  while ((int)h->adjSeg.size() < kinds * every + 1) {
     double* p = nullptr;
     if (cudaMalloc(&p, bytes) != cudaSuccess) { set_err("adjoint: segment allocation failed"); return GRIM_ENOMEM; }
     h->adjSeg.push_back(p);
@@ -1693,7 +1704,7 @@ int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, in
   double* lam = nullptr;
   int rcw = adjoint_work(h, w, lam);
   if (rcw) return rcw;
-  double* finalState = h->adjSeg[6 * every];
+  double* finalState = h->adjSeg[(size_t)kinds * every];
   auto state = [&](int kind, int t) { return h->adjSeg[(size_t)kind * every + t]; };
   CK(cudaMemcpyAsync(lam, lambda, bytes, memKind == GRIM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                      h->stream));
@@ -1721,10 +1732,20 @@ int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, in
       enqueue_segment(h, GRIM_SEG_PRE);
       CK(cudaMemcpyAsync(state(1, t), h->primOld, bytes, cudaMemcpyDeviceToDevice, h->stream));
       enqueue_segment(h, GRIM_SEG_HALF);
+      if (kinds > 6) {
+        const size_t nfBytes = (size_t)c.nf * h->bytesZ;
+        CK(cudaMemcpyAsync(state(6, t), h->divF, nfBytes, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(state(7, t), h->Sexp, nfBytes, cudaMemcpyDeviceToDevice, h->stream));
+      }
       CK(cudaMemcpyAsync(state(2, t), h->prim, bytes, cudaMemcpyDeviceToDevice, h->stream));
       CK(cudaMemcpyAsync(state(3, t), h->primHalf, bytes, cudaMemcpyDeviceToDevice, h->stream));
       KNS_CALL(h, ghost_fill, c, state(3, t), c.dof, h->stream);
       enqueue_segment(h, GRIM_SEG_FULL);
+      if (kinds > 6) {
+        const size_t nfBytes = (size_t)c.nf * h->bytesZ;
+        CK(cudaMemcpyAsync(state(8, t), h->divF, nfBytes, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(state(9, t), h->Sexp, nfBytes, cudaMemcpyDeviceToDevice, h->stream));
+      }
       CK(cudaMemcpyAsync(state(4, t), h->primHalf, bytes, cudaMemcpyDeviceToDevice, h->stream));
       CK(cudaMemcpyAsync(state(5, t), h->prim, bytes, cudaMemcpyDeviceToDevice, h->stream));
       enqueue_segment(h, GRIM_SEG_POST);
@@ -1738,6 +1759,13 @@ int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, in
       st.PhFill = state(3, t);
       st.PhEff = state(4, t);
       st.P1Sol = state(5, t);
+      st.divFh = st.Sexph = st.divF1 = st.Sexp1 = nullptr;
+      if (kinds > 6) {
+        st.divFh = state(6, t);
+        st.Sexph = state(7, t);
+        st.divF1 = state(8, t);
+        st.Sexp1 = state(9, t);
+      }
       grim::adjoint_step(c, adjoint_geo(h), dt, st, lam, w, h->stream);
     }
     CK(cudaGetLastError());

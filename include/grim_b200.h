@@ -421,12 +421,13 @@ int grim_set_face_variant(grim_handle* h, int dir, int variant);
  * interior zones (ghost entries zero; the ghosts are images of interior
  * zones and their share is folded in).  Each segment between checkpoints
  * is recomputed forward once; the stepper is left at the final state.
- * Supported: 2D and 3D ideal MHD, Minkowski or modified Kerr-Schild
- * (geometric source, face metric), periodic / outflow / mirror boundaries,
- * no problem hooks or the torus problem's (floors after each stage, inflow
- * check and pole fix at the start of each stage, flux filter; MKS, N2 >= 6);
- * GRIM_ENOTSUP otherwise (EMHD).  A zone that fullStepDiagnostics' NaN
- * reset replaces carries no derivative.  Every accumulation is a gather in a fixed
+ * Supported: 2D and 3D, ideal or extended MHD (conduction and / or
+ * viscosity), Minkowski or modified Kerr-Schild (geometric source, face
+ * metric), periodic / outflow / mirror boundaries, no problem hooks; or
+ * ideal MHD with the torus problem's (floors after each stage, inflow check
+ * and pole fix at the start of each stage, flux filter; MKS, N2 >= 6).
+ * GRIM_ENOTSUP otherwise (the torus problem with EMHD).  A zone that
+ * fullStepDiagnostics' NaN reset replaces carries no derivative.  Every accumulation is a gather in a fixed
  * order (no atomics): a gradient is the same bits run to run and for any
  * checkpoint interval. */
 int grim_set_dt_mode(grim_handle* h, int fixed);
