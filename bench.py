@@ -402,10 +402,11 @@ def run_batch(args, local_rank):
     ts.primOld.setVars(P)
     ts.primOld.communicate()
     ts.setFixedDt(True)
-    # one untimed forward / backward pair first: the adjoint's buffers are
-    # allocated and its kernels loaded on the first call
+    # one untimed forward / backward pair of the same shape first: the
+    # adjoint's checkpoint and segment buffers are allocated and its kernels
+    # loaded on the first call
     time0, dt0 = ts.time, ts.dt
-    ts.adjointForward(2, 1)
+    ts.adjointForward(20, 10)
     ts.adjointBackward(ts.primOld.getVars())
     ts.setTime(time0, dt0)
     ts.primOld.setVars(P)
