@@ -578,3 +578,33 @@ def test_timestep_parity_1d():
     assert change > 0
     assert np.max(np.abs(f - g)) <= 1e-6 * change
     assert fast.stats()["nonFinite"] == 0
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_flux_ct_divergence_is_the_field_update(dim):
+    """timeStepperPy.fluxCT: the divergence of the constrained-transport
+    fluxes' field rows over the interior equals computeDivOfFluxes' field
+    rows (the induction's input) to rounding."""
+    if dim == 2:
+        cfg = PR.fast_mode_config(N=32)
+    else:
+        cfg = PR.fast_mode_config(N=16, N3=16, dim=3)
+    P = _smooth_random(cfg, 7)
+    from grim_b200.timestepper import timeStepper
+    ts = timeStepper(cfg)
+    divF, _ = ts.computeDivOfFluxes(P)
+    fl = ts.fluxCT(P)
+    g = cfg["numGhost"]
+    dX = [(cfg["X%dEnd" % d] - cfg["X%dStart" % d]) / cfg["N%d" % d] for d in (1, 2, 3)]
+    b1 = ts.dof - 3
+    s3, s2, s1 = C.interior_slices(cfg)
+    for b in range(3):
+        div = np.zeros_like(divF[0])
+        for d in range(dim):
+            axis = 2 - d
+            f = fl[d, b1 + b]
+            div += (np.roll(f, -1, axis=axis) - f) / dX[d]
+        got = div[s3, s2, s1]
+        ref = divF[b1 + b][s3, s2, s1]
+        scale = max(np.max(np.abs(ref)), 1e-30)
+        assert np.max(np.abs(got - ref)) <= 1e-12 * scale, (b, np.max(np.abs(got - ref)) / scale)
