@@ -945,7 +945,10 @@ int grim_time_steps_host(grim_handle* h, int nsteps, const double* const* hostIn
   cudaEvent_t* inFree = h->ioEv + 2;
   cudaEvent_t* outStaged = h->ioEv + 4;
   cudaEvent_t* outFree = h->ioEv + 6;
-  for (int k = 0; k < nsteps; k++) {
+  // one step of the pipeline; an error ends the loop below, which still
+  // waits for every copy already issued (they read or write the caller's
+  // buffers)
+  auto pipeline_step = [&](int k) -> int {
     const int s = k & 1;
     if (hostIn && hostIn[k]) {
       // staging buffer s is free once the step of k - 2 has copied it in
@@ -963,7 +966,7 @@ int grim_time_steps_host(grim_handle* h, int nsteps, const double* const* hostIn
       }
       CK(cudaEventRecord(inFree[s], h->stream));
     }
-    int rc = run_steps(h, 1);
+    const int rc = run_steps(h, 1);
     if (rc) return rc;
     if (hostOut && hostOut[k]) {
       // staging buffer s is free once the download of k - 2 has finished
@@ -975,10 +978,19 @@ int grim_time_steps_host(grim_handle* h, int nsteps, const double* const* hostIn
       CK(cudaMemcpyAsync(hostOut[k], h->ioOut[s], hostBytes, cudaMemcpyDeviceToHost, h->ioDown));
       CK(cudaEventRecord(outFree[s], h->ioDown));
     }
+    return GRIM_OK;
+  };
+  int rc = GRIM_OK;
+  for (int k = 0; k < nsteps && rc == GRIM_OK; k++) rc = pipeline_step(k);
+  const cudaError_t e1 = cudaStreamSynchronize(h->ioUp);
+  const cudaError_t e2 = cudaStreamSynchronize(h->stream);
+  const cudaError_t e3 = cudaStreamSynchronize(h->ioDown);
+  if (rc) return rc;
+  if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+    set_err("grim_time_steps_host: %s",
+            cudaGetErrorString(e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3)));
+    return GRIM_ECUDA;
   }
-  CK(cudaStreamSynchronize(h->ioUp));
-  CK(cudaStreamSynchronize(h->stream));
-  CK(cudaStreamSynchronize(h->ioDown));
   return take_async_error(h);
 }
 

@@ -140,3 +140,36 @@ def test_interior_layout_matches_the_ghosted_calls(problem):
         e = seq.primOld.getVars()[sl]
         assert np.array_equal(outs[step].numpy(), e), step
     assert piped.time == seq.time and piped.dt == seq.dt
+
+
+def test_timeout_inside_the_pipeline_is_reported():
+    """A bounded device wait that runs out during the pipelined steps (the
+    debug setting that makes the TMA-staged face kernels issue no copies)
+    ends the call with GRIM_ETIMEOUT after every issued copy has finished;
+    with the setting cleared and the state set again the handle steps as a
+    fresh one does."""
+    import torch
+    from grim_b200 import _lib
+    from grim_b200.timestepper import timeStepper
+    cfg = PR.fast_mode_config(N=64)
+    P = PR.fast_mode_prims(cfg)
+    ts, ref = timeStepper(cfg), timeStepper(cfg)
+    for h in (ts, ref):
+        h.setFaceVariant(0, 2)  # the TMA-staged X1 kernel
+        h.setFixedDt(True)
+        h.primOld.setVars(P)
+    t0, dt0 = ts.time, ts.dt
+    inp = torch.from_numpy(np.ascontiguousarray(P)).pin_memory()
+    out = torch.zeros_like(inp).pin_memory()
+    ts.setDebug(_lib.DEBUG_SKIP_BULK_COPIES, 1)
+    with pytest.raises(_lib.GrimError) as err:
+        ts.timeStepsHost([inp.data_ptr()] * 3, [out.data_ptr()] * 3)
+    assert err.value.status == _lib.GRIM_ETIMEOUT
+    ts.setDebug(_lib.DEBUG_SKIP_BULK_COPIES, 0)
+    ts.synchronize()
+    for h in (ts, ref):
+        h.primOld.setVars(P)
+        h.setTime(t0, dt0)
+    ts.timeStepsHost([inp.data_ptr(), None], [None, out.data_ptr()])
+    ref.timeSteps(2)
+    assert np.array_equal(out.numpy(), ref.primOld.getVars())
