@@ -97,12 +97,23 @@ def torus_state(cfg, ts):
 
 
 def cpu_sample_config(name, cfg):
-    """The workload for the CPU baseline: the full grid, except the torus,
-    whose oracle run is bounded to a 64x32x16 sample of the same set-up."""
+    """The workload of the one-core CPU figure: the full grid, except the
+    torus, whose one-core run is bounded to a 64x32x16 sample of the same
+    set-up (a full 256x128x64 step takes minutes on one core)."""
     if name == "torus":
         from grim_b200.problems import torus as T
         return T.torus_config(N1=64, N2=32, N3=16, nonlinearsolve_atol=ATOL, nonlinearsolve_rtol=RTOL, nonlinearsolve_ulps=ULPS)
     return cfg
+
+
+def workload_config(name, desc, cfg):
+    """The `config` of a bench line: what the workload is, the same for the
+    GPU arm and the CPU reference arm (how each arm computes it goes under
+    `method`)."""
+    return {"workload": name, "description": desc, "zones": cfg["N1"] * cfg["N2"] * cfg["N3"],
+            "rel_residual_tol": RTOL, "abs_residual_floor": ATOL, "maxNonLinearIter": cfg["maxNonLinearIter"],
+            "l2": "working set above the L2 size in both arms; the GPU arm also flushes L2 between timed steps "
+                  "(256 MB write, untimed)"}
 
 
 class Clocks:
@@ -166,10 +177,13 @@ class Clocks:
 
 
 def cpu_reference(cfg, P, seconds=15.0, threads=None):
-    """Time the CPU oracle on a bounded sample of the workload."""
+    """Time the CPU oracle on the workload's grid: set-up and one warm-up
+    step untimed, then whole steps until `seconds` have passed (at least
+    one, at most 50).  Returns (zone-cycles/s, threads, sample text)."""
     from oracle import oracle as O
     n = threads or os.cpu_count()
     O.set_threads(n)
+    t_setup = time.perf_counter()
     o = O.Oracle(cfg)
     if P is None:  # torus: initial conditions from the oracle's geometry
         from grim_b200.problems import torus as T
@@ -179,6 +193,7 @@ def cpu_reference(cfg, P, seconds=15.0, threads=None):
     else:
         o.set_prims(P)
     o.time_step(1)  # warm-up (page faults, first dt)
+    t_setup = time.perf_counter() - t_setup
     steps, t0 = 0, time.perf_counter()
     while True:
         o.time_step(1)
@@ -187,8 +202,8 @@ def cpu_reference(cfg, P, seconds=15.0, threads=None):
         if el >= seconds or steps >= 50:
             break
     zones = cfg["N1"] * cfg["N2"] * cfg["N3"]
-    return zones * steps / el, n, "%d step(s) of the full %dx%dx%d grid after 1 warm-up step, %.1f s" % (
-        steps, cfg["N1"], cfg["N2"], cfg["N3"], el)
+    return zones * steps / el, n, ("%d timed step(s) of the full %dx%dx%d grid, %.1f s, after %.1f s of set-up "
+                                   "and 1 warm-up step (untimed)" % (steps, cfg["N1"], cfg["N2"], cfg["N3"], el, t_setup))
 
 
 def profile_path(ts, steps, flush):
@@ -508,9 +523,9 @@ def run_decomposed(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f64 residual / f32 Jacobian+solve",
         "data": "synthetic (seeded initial conditions of the named workload)",
-        "config": {"workload": args.workload, "description": desc, "zones": zones,
-                   "parallelism": "X3 slabs of %d planes on %d GPUs (NCCL halos)" % (cfg["N3"] // world, world),
-                   "l2": "flushed between timed steps (256 MB write, untimed)", "face_kernel_variants": tuned},
+        "config": workload_config(args.workload, desc, cfg),
+        "method": {"parallelism": "X3 slabs of %d planes on %d GPUs (NCCL halos)" % (cfg["N3"] // world, world),
+                   "face_kernel_variants": tuned},
         "e2e": {"value": zones * e2e_steps / e2e_s, "unit": "zone-cycles/s",
                 "h2d_bytes_per_step": host_in.numel() * 8 * world, "d2h_bytes_per_step": host_in.numel() * 8 * world},
         "gpu_launches": None, "clocks": clocks_info, "roofline": None, "cpu_baseline": None,
@@ -643,11 +658,9 @@ def run_gpu(args, rank, world, local_rank):
         "vs_baseline": None,
         "dtype": "f64 residual / f32 Jacobian+solve",
         "data": "synthetic (seeded initial conditions of the named workload)",
-        "config": {"workload": args.workload, "description": desc, "zones": zones,
-                   "newton": "tangent Jacobian, FP32 solve, FP64 residual, per-zone convergence",
-                   "rel_residual_tol": RTOL, "abs_residual_floor": ATOL, "rounding_floor_ulps": ULPS,
-                   "maxNonLinearIter": cfg["maxNonLinearIter"],
-                   "l2": "flushed between timed steps (256 MB write, untimed)",
+        "config": workload_config(args.workload, desc, cfg),
+        "method": {"newton": "tangent Jacobian, FP32 solve, FP64 residual, per-zone convergence",
+                   "rounding_floor_ulps": ULPS,
                    "parallelism": "replicas" if world > 1 else "single GPU", "cuda_graph": True,
                    "face_kernel_variants": state.get("tuned", {})},
         "fd64": {"value": fd, "ms_per_step": ms_fd / args.steps, "newton_iters": st_fd["newtonIters"],
@@ -740,18 +753,17 @@ def main():
         if rank != 0:
             return
         cfg, P, desc = workload(args.workload, args.grid)
-        cfg = cpu_sample_config(args.workload, cfg)
-        vals = []
-        for _ in range(max(1, args.steps // 10)):
-            v, n, sample = cpu_reference(cfg, P, seconds=10.0)
-            vals.append(v)
-        v = float(np.median(vals))
+        # the whole workload grid, whole steps for about 20 s after an
+        # untimed set-up and warm-up step
+        v, n, sample = cpu_reference(cfg, P, seconds=20.0)
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": v, "unit": "zone-cycles/s", "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "description": desc,
-                       "newton": "FD Jacobian (reference method), FP64"},
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded initial conditions of the named workload)",
+            "config": workload_config(args.workload, desc, cfg),
+            "method": {"newton": "FD Jacobian (reference method), FP64, global break",
+                       "runs_on": "host cores: the CPU restatement of the reference's step (oracle/grim_oracle.cpp), "
+                                  "OpenMP over zones"},
             "cpu_baseline": {"value": v, "unit": "zone-cycles/s", "cores": n, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "zone-cycles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }))
@@ -786,11 +798,12 @@ def main():
         return
     out, cfg, P = run_gpu(args, rank, world, local_rank)
     if rank == 0 and not args.no_cpu:
-        ccfg = cpu_sample_config(args.workload, cfg)
-        v, n, sample = cpu_reference(ccfg, P if ccfg is cfg else None, seconds=10.0)
+        v, n, sample = cpu_reference(cfg, P, seconds=20.0)
         out["cpu_baseline"] = {"value": v, "unit": "zone-cycles/s", "cores": n, "kind": "port",
                                "sample": sample, "host_nproc": os.cpu_count()}
-        # the same sample on one core (the oracle's OpenMP loops on one thread)
+        # one core (the oracle's OpenMP loops on one thread), on a smaller
+        # sample of the torus set-up
+        ccfg = cpu_sample_config(args.workload, cfg)
         v1, n1, sample1 = cpu_reference(ccfg, P if ccfg is cfg else None, seconds=10.0, threads=1)
         out["cpu_baseline_1core"] = {"value": v1, "unit": "zone-cycles/s", "cores": n1, "kind": "port",
                                      "sample": sample1}
