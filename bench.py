@@ -775,7 +775,7 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     if args.workload == "batch":
         out = run_batch(args, local_rank)
-        if rank == 0 and not args.no_cpu:
+        if rank == 0 and world == 1 and not args.no_cpu:
             cfg, P = batch_problems()[0]
             v, n, sample = cpu_reference(cfg, P, seconds=10.0)
             out["cpu_baseline"] = {"value": v, "unit": "zone-cycles/s", "cores": n, "kind": "port",
@@ -797,7 +797,7 @@ def main():
             print(json.dumps(out))
         return
     out, cfg, P = run_gpu(args, rank, world, local_rank)
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:
         v, n, sample = cpu_reference(cfg, P, seconds=20.0)
         out["cpu_baseline"] = {"value": v, "unit": "zone-cycles/s", "cores": n, "kind": "port",
                                "sample": sample, "host_nproc": os.cpu_count()}
@@ -807,6 +807,9 @@ def main():
         v1, n1, sample1 = cpu_reference(ccfg, P if ccfg is cfg else None, seconds=10.0, threads=1)
         out["cpu_baseline_1core"] = {"value": v1, "unit": "zone-cycles/s", "cores": n1, "kind": "port",
                                      "sample": sample1}
+    elif world > 1:
+        # timed at N=1 only: the other ranks would wait for it in the barrier
+        out["cpu_baseline"] = None
     if world > 1:
         import torch
         torch.distributed.barrier()
