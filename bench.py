@@ -290,15 +290,15 @@ def rooflines(cfg, prof, prof_fd, device):
     n64 = f64 / (newton_ms * 1e-3) / 1e12
     n32 = f32 / (newton_ms * 1e-3) / 1e12
     pipe_frac = (n64 / fp64_peak) + (n32 / fp32_peak)
-    traffic = _ncu_traffic(cfg)
+    traffic, traffic_src = _ncu_traffic(cfg)
     newton = {"bound": "fp64", "achieved": n64, "peak": fp64_peak, "unit": "TFLOP/s", "frac": n64 / fp64_peak,
               "fp32_achieved": n32, "fp32_peak": fp32_peak, "fp32_frac": n32 / fp32_peak,
               "pipe_time_frac": pipe_frac,
-              "traffic": traffic.get("newton"),
+              "traffic": traffic.get("newton"), "traffic_source": traffic_src,
               "kernel": "newton (one launch per stage)", "ms_per_launch": newton_ms / newton_launches,
               "flops_per_zone": prof["flops"],
               "peak_source": "measured: FMA-chain self-test of this GPU (grim_measure_peaks)"}
-    common = {"traffic": traffic.get("stencil"),
+    common = {"traffic": traffic.get("stencil"), "traffic_source": traffic_src,
               "kernel": "stencil (face fluxes x%d + epilogue, per stage)" % cfg["dim"],
               "ms_per_launch": t_st * 1e3, "bytes_per_zone": B, "flops_per_zone": F,
               "hbm_achieved_gbs": st_gbs, "hbm_peak_gbs": hbm_peak, "hbm_frac": st_gbs / hbm_peak,
@@ -330,18 +330,40 @@ def rooflines(cfg, prof, prof_fd, device):
     return out
 
 
+# the sources that define the step's kernels: a DRAM capture describes the
+# kernels these files built
+KERNEL_SOURCES = ("kernels.cuh", "physics.cuh", "recon.cuh", "stage.cuh", "common.cuh", "torus.cuh",
+                  "launch.h", "kernels_fast.cu", "faces_fast.cu")
+
+
+def kernel_sources_sha16():
+    import hashlib
+    h = hashlib.sha256()
+    for n in KERNEL_SOURCES:
+        with open(os.path.join(ROOT, "grim_b200", "csrc", n), "rb") as fh:
+            h.update(n.encode() + b"\0" + fh.read())
+    return h.hexdigest()[:16]
+
+
 def _ncu_traffic(cfg):
     """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
     of the workload's kernel groups from the committed ncu summary, when
-    one exists for this grid."""
+    one exists for this grid and was taken on the current kernel sources
+    (else {} and the line's traffic is null), and what was found."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as fh:
             table = json.load(fh)
     except (OSError, ValueError):
-        return {}
+        return {}, "no profiles/traffic.json"
     key = "%dx%dx%d" % (cfg["N1"], cfg["N2"], cfg["N3"])
-    return table.get(key, {})
+    entry = table.get(key)
+    if entry is None:
+        return {}, "no capture of the %s grid" % key
+    if entry.get("sources_sha16") != kernel_sources_sha16():
+        return {}, "stale: the kernel sources changed since the capture of the %s grid" % key
+    return entry, "profiles/traffic.json, %s grid, captured on these kernel sources (%s)" % (
+        key, entry["sources_sha16"])
 
 
 def batch_problems(seed=5, count=16):
