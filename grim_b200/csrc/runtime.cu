@@ -181,6 +181,22 @@ static int make_devcfg(const grim_config& c, DevCfg& d) {
   if (c.reconstruction < 0 || c.reconstruction > 3) { set_err("bad reconstruction"); return GRIM_EINVAL; }
   if (c.maxNonLinearIter < 1 || c.maxNonLinearIter > 15) { set_err("maxNonLinearIter must be 1..15"); return GRIM_EINVAL; }
   if (c.maxLineSearchIters < 1 || c.maxLineSearchIters > 32) { set_err("maxLineSearchIters must be 1..32"); return GRIM_EINVAL; }
+  if (c.metric != GRIM_MINKOWSKI && c.metric != GRIM_MODIFIED_KERR_SCHILD) { set_err("bad metric %d", c.metric); return GRIM_EINVAL; }
+  if (c.riemannSolver != GRIM_HLL && c.riemannSolver != GRIM_LOCAL_LAX_FRIEDRICH) {
+    set_err("bad riemannSolver %d", c.riemannSolver); return GRIM_EINVAL;
+  }
+  if (c.closure < GRIM_CLOSURE_CONST_TAU || c.closure > GRIM_CLOSURE_TAU_PROFILE) { set_err("bad closure %d", c.closure); return GRIM_EINVAL; }
+  if (c.problem != GRIM_PROBLEM_NONE && c.problem != GRIM_PROBLEM_TORUS) { set_err("bad problem %d", c.problem); return GRIM_EINVAL; }
+  if (c.newtonMode < GRIM_NEWTON_PARITY_FD64 || c.newtonMode > GRIM_NEWTON_FD64_FAST) {
+    set_err("bad newtonMode %d", c.newtonMode); return GRIM_EINVAL;
+  }
+  if (c.perZoneConvergence < 0 || c.perZoneConvergence > 3) {
+    set_err("perZoneConvergence must be 0..3"); return GRIM_EINVAL;
+  }
+  // coordinatesGrid (grid.cpp:142-146) divides each active extent by N
+  if (!(c.X1End > c.X1Start) || (c.dim >= 2 && !(c.X2End > c.X2Start)) || (c.dim >= 3 && !(c.X3End > c.X3Start))) {
+    set_err("each active direction needs XEnd > XStart"); return GRIM_EINVAL;
+  }
   memset(&d, 0, sizeof(d));
   d.dim = c.dim; d.ng = c.numGhost;
   d.N1 = c.N1; d.N2 = c.dim >= 2 ? c.N2 : 1; d.N3 = c.dim >= 3 ? c.N3 : 1;
@@ -195,7 +211,9 @@ static int make_devcfg(const grim_config& c, DevCfg& d) {
   d.Z = (long long)d.N1T * d.N2T * d.N3T;
   d.Zint = (long long)d.N1 * d.N2 * d.N3;
   d.GZ = (long long)d.N1T * d.N2T;
-  if (d.Z >= (1LL << 31)) return GRIM_EINVAL;  // 32-bit zone indices in the kernels
+  if (d.Z >= (1LL << 31)) {  // 32-bit zone indices in the kernels
+    set_err("grid of %lld zones with ghosts: at most 2^31 - 1", d.Z); return GRIM_EINVAL;
+  }
   d.conduction = c.conduction ? 1 : 0; d.viscosity = c.viscosity ? 1 : 0;
   d.nf = 5 + d.conduction + d.viscosity; d.dof = d.nf + 3;
   d.Q = 5; d.DP = 5 + d.conduction; d.B1 = d.nf;
@@ -1435,7 +1453,10 @@ int grim_problem_init(grim_handle* h) {
 }
 
 int grim_set_newton_mode(grim_handle* h, int mode, int perZone, double rtol) {
-  if (!h || mode < 0 || mode > 3 || perZone < 0 || perZone > 3) return GRIM_EINVAL;
+  if (!h || mode < 0 || mode > 3 || perZone < 0 || perZone > 3) {
+    set_err("grim_set_newton_mode: null handle, or mode outside 0..3 or perZone outside 0..3");
+    return GRIM_EINVAL;
+  }
   h->cfg.newtonMode = mode;
   h->cfg.perZoneConvergence = perZone;
   h->cfg.nonlinearsolve_rtol = rtol;

@@ -130,7 +130,16 @@ typedef struct grim_stats {
 } grim_stats;
 
 /* ---- lifecycle: timeStepper::timeStepper / ~timeStepper
- *      (timestepper.cpp:4-470) ------------------------------------------ */
+ *      (timestepper.cpp:4-470) ------------------------------------------
+ * The configuration is checked before any CUDA call; GRIM_EINVAL, with
+ * grim_last_error() naming the field, for: dim outside 1..3, numGhost != 3,
+ * fewer than 4 zones in an active direction, more than 2^31 - 1 zones with
+ * ghosts, an enum field outside its GRIM_* values (metric, reconstruction,
+ * riemannSolver, closure, problem, newtonMode, the six boundaries),
+ * perZoneConvergence outside 0..3, maxNonLinearIter outside 1..15,
+ * maxLineSearchIters outside 1..32, XEnd <= XStart in an active direction,
+ * a negative or NaN nonlinearsolve_ulps, an N3Global that is not a 3D slab
+ * count >= N3, and the torus problem or closure without the MKS metric. */
 int grim_create(const grim_config* cfg, int device, grim_handle** out);
 int grim_destroy(grim_handle* h);
 int grim_dims(const grim_handle* h, int* N1T, int* N2T, int* N3T, int* dof, int* numFluidVars);
