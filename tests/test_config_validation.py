@@ -1,4 +1,5 @@
-"""grim_create's configuration checks (include/grim_b200.h, grim_create).
+"""grim_create's configuration checks (include/grim_b200.h, grim_create),
+and the NULL-handle refusal of every entry point that takes a handle.
 
 The checks run before any CUDA call, so these run on the CPU: each invalid
 configuration is refused with GRIM_EINVAL and grim_last_error() naming
@@ -90,3 +91,36 @@ def test_null_arguments_are_refused():
     assert L.grim_create(None, 0, ctypes.byref(h)) == EINVAL
     s = C.to_struct(_base())
     assert L.grim_create(ctypes.byref(s), 0, None) == EINVAL
+
+
+# entry points whose first argument is a handle; grim_destroy and
+# grim_batch_destroy accept NULL as a no-op and grim_batch_size(NULL) is 0
+_NO_OP_ON_NULL = {"grim_destroy": 0, "grim_batch_destroy": 0, "grim_batch_size": 0}
+
+
+def _handle_entry_points():
+    import re
+    import inspect
+    src = inspect.getsource(_lib.lib)
+    return re.findall(r'"(grim_[a-z0-9_]+)": \[vp', src)
+
+
+def test_every_handle_entry_point_refuses_a_null_handle():
+    """Each call taking a grim_handle / grim_batch first returns GRIM_EINVAL
+    (nothing runs, no CUDA call) when that handle is NULL, with every other
+    pointer NULL and every number zero."""
+    L = _lib.lib()
+    names = _handle_entry_points()
+    assert len(names) > 50
+    for n in names:
+        f = getattr(L, n)
+        args = [None]
+        for t in f.argtypes[1:]:
+            if t in (ctypes.c_int, ctypes.c_longlong):
+                args.append(0)
+            elif t is ctypes.c_double:
+                args.append(0.)
+            else:
+                args.append(None)
+        want = _NO_OP_ON_NULL.get(n, EINVAL)
+        assert f(*args) == want, n
