@@ -589,6 +589,13 @@ static void enqueue_step(grim_handle* h, bool timed) {
   enqueue_post(h, timed, nanCounted);
 }
 
+// the memory kind of a caller's pointer: GRIM_HOST or GRIM_DEVICE, nothing else
+static bool mem_kind_ok(int memKind) {
+  if (memKind == GRIM_HOST || memKind == GRIM_DEVICE) return true;
+  set_err("memKind %d: GRIM_HOST or GRIM_DEVICE", memKind);
+  return false;
+}
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
@@ -720,6 +727,7 @@ static double* pick(grim_handle* h, int which) {
 }
 
 int grim_set_prims(grim_handle* h, int which, const double* src, int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   if (!h || !src) { set_err("null argument"); return GRIM_EINVAL; }
   double* dst = pick(h, which);
   if (!dst) { set_err("bad state selector %d", which); return GRIM_EINVAL; }
@@ -732,6 +740,7 @@ int grim_set_prims(grim_handle* h, int which, const double* src, int memKind) {
 }
 
 int grim_get_prims(grim_handle* h, int which, double* dst, int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   if (!h || !dst) { set_err("null argument"); return GRIM_EINVAL; }
   double* src = pick(h, which);
   if (!src) { set_err("bad state selector %d", which); return GRIM_EINVAL; }
@@ -895,7 +904,7 @@ int grim_time_step(grim_handle* h, int* numReads, int* numWrites) {
 }
 
 int grim_time_steps(grim_handle* h, int nsteps) {
-  if (!h || nsteps < 0) return GRIM_EINVAL;
+  if (!h || nsteps < 0) { set_err("grim_time_steps: null handle or nsteps < 0"); return GRIM_EINVAL; }
   return run_steps(h, nsteps);
 }
 
@@ -1043,9 +1052,9 @@ int grim_compute_dt(grim_handle* h) {
 }
 
 int grim_apply_boundaries(grim_handle* h, int which) {
-  if (!h) return GRIM_EINVAL;
+  if (!h) { set_err("null argument"); return GRIM_EINVAL; }
   double* p = pick(h, which);
-  if (!p) return GRIM_EINVAL;
+  if (!p) { set_err("bad state selector %d", which); return GRIM_EINVAL; }
   CK(cudaSetDevice(h->device));
   KNS_CALL(h, communicate, h->dc, p, h->dc.dof, h->stream);
   KNS_CALL(h, ghost_fill, h->dc, p, h->dc.dof, h->stream);
@@ -1054,9 +1063,9 @@ int grim_apply_boundaries(grim_handle* h, int which) {
 }
 
 int grim_communicate(grim_handle* h, int which) {
-  if (!h) return GRIM_EINVAL;
+  if (!h) { set_err("null argument"); return GRIM_EINVAL; }
   double* p = pick(h, which);
-  if (!p) return GRIM_EINVAL;
+  if (!p) { set_err("bad state selector %d", which); return GRIM_EINVAL; }
   CK(cudaSetDevice(h->device));
   KNS_CALL(h, communicate, h->dc, p, h->dc.dof, h->stream);
   CK(cudaGetLastError());
@@ -1078,6 +1087,7 @@ static int stage_out(grim_handle* h, double* dst, const double* src, size_t byte
 
 int grim_compute_div_fluxes(grim_handle* h, const double* prim, double* divF, double* fluxes, double* emf,
                             int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   if (!h || !prim) return GRIM_EINVAL;
   CK(cudaSetDevice(h->device));
   const DevCfg& c = h->dc;
@@ -1124,6 +1134,7 @@ int grim_compute_div_fluxes(grim_handle* h, const double* prim, double* divF, do
 }
 
 int grim_reconstruct(grim_handle* h, const double* prim, int dir, double* pl, double* pr, int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   if (!h || !prim || !pl || !pr || dir < 0 || dir >= h->dc.dim) return GRIM_EINVAL;
   CK(cudaSetDevice(h->device));
   const DevCfg& c = h->dc;
@@ -1201,7 +1212,9 @@ int grim_torus_observers(grim_handle* h, double* out) {
 }
 
 int grim_get_observations(grim_handle* h, double* out, int maxRecords, int* nRecords) {
-  if (!h || !nRecords || maxRecords < 0 || (maxRecords > 0 && !out)) return GRIM_EINVAL;
+  if (!h || !nRecords || maxRecords < 0 || (maxRecords > 0 && !out)) {
+    set_err("grim_get_observations: bad argument"); return GRIM_EINVAL;
+  }
   CK(cudaSetDevice(h->device));
   unsigned long long count = 0;
   CK(cudaMemcpyAsync(&count, &h->st->obsCount, sizeof(count), cudaMemcpyDeviceToHost, h->stream));
@@ -1224,6 +1237,7 @@ int grim_get_observations(grim_handle* h, double* out, int maxRecords, int* nRec
 }
 
 int grim_compute_divb(grim_handle* h, const double* prim, double* divB, int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   if (!h || !prim || !divB) return GRIM_EINVAL;
   CK(cudaSetDevice(h->device));
   const DevCfg& c = h->dc;
@@ -1236,6 +1250,7 @@ int grim_compute_divb(grim_handle* h, const double* prim, double* divB, int memK
 }
 
 int grim_conserved(grim_handle* h, const double* prim, double* cons, int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   if (!h || !prim || !cons) return GRIM_EINVAL;
   CK(cudaSetDevice(h->device));
   const DevCfg& c = h->dc;
@@ -1249,6 +1264,7 @@ int grim_conserved(grim_handle* h, const double* prim, double* cons, int memKind
 }
 
 int grim_char_speeds(grim_handle* h, const double* prim, int dir, double* mn, double* mx, int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   if (!h || !prim || !mn || !mx || dir < 0 || dir > 2) return GRIM_EINVAL;
   CK(cudaSetDevice(h->device));
   const DevCfg& c = h->dc;
@@ -1279,6 +1295,7 @@ int grim_stage_setup(grim_handle* h, int stage) {
 }
 
 int grim_residual(grim_handle* h, const double* pg, double* res, int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   if (!h || !pg || !res) return GRIM_EINVAL;
   CK(cudaSetDevice(h->device));
   const DevCfg& c = h->dc;
@@ -1311,12 +1328,15 @@ static int jac_common(grim_handle* h, const double* pg, double* jac, int memKind
   return rc;
 }
 int grim_jacobian_fd(grim_handle* h, const double* pg, double* jac, int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   return jac_common(h, pg, jac, memKind, 0);
 }
 int grim_jacobian_tangent(grim_handle* h, const double* pg, double* jac, int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   return jac_common(h, pg, jac, memKind, 1);
 }
 int grim_jacobian_form(grim_handle* h, const double* pg, double* jac, int form, int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   if (form < GRIM_JAC_FD64 || form > GRIM_JAC_FAST32) {
     set_err("grim_jacobian_form: unknown form %d", form);
     return GRIM_EINVAL;
@@ -1339,6 +1359,7 @@ int grim_newton_solve(grim_handle* h, int* iters) {
 }
 
 int grim_batch_solve(int n, int batch, const double* A, const double* b, double* x, int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   if (n < 1 || n > 8 || batch < 0 || !A || !b || !x) return GRIM_EINVAL;
   if (batch == 0) return GRIM_OK;
   cudaStream_t s = 0;
@@ -1387,7 +1408,8 @@ static int full_to_plane(grim_handle* h, double* dst, const double* src, int row
 }
 
 int grim_get_geometry(grim_handle* h, int location, double* out, double* gamma, double* xc, int memKind) {
-  if (!h || location < 0 || location > 4) return GRIM_EINVAL;
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
+  if (!h || location < 0 || location > 4) { set_err("grim_get_geometry: null handle or bad location"); return GRIM_EINVAL; }
   CK(cudaSetDevice(h->device));
   const DevCfg& c = h->dc;
   if (h->cfg.metric == GRIM_MINKOWSKI) {
@@ -1421,6 +1443,7 @@ int grim_get_geometry(grim_handle* h, int location, double* out, double* gamma, 
 
 int grim_set_geometry(grim_handle* h, int location, const double* in, const double* gamma, const double* xc,
                       int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   if (!h || location < 0 || location > 4) return GRIM_EINVAL;
   if (h->cfg.metric == GRIM_MINKOWSKI) { set_err("Minkowski geometry is compile-time"); return GRIM_ENOTSUP; }
   CK(cudaSetDevice(h->device));
@@ -1666,6 +1689,7 @@ static int adjoint_work(grim_handle* h, AdjointBufs& w, double*& lam) {
 }
 
 int grim_adjoint_stencil(grim_handle* h, const double* prim, const double* gbar, double* out, int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   if (!h || !prim || !gbar || !out) { set_err("grim_adjoint_stencil: null argument"); return GRIM_EINVAL; }
   int rc = adjoint_scope(h);
   if (rc) return rc;
@@ -1719,6 +1743,7 @@ int grim_adjoint_forward(grim_handle* h, int nsteps, int every) {
 }
 
 int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   if (!h || !lambda || !grad) { set_err("grim_adjoint_backward: null argument"); return GRIM_EINVAL; }
   if (h->adjSteps <= 0) { set_err("grim_adjoint_backward: no grim_adjoint_forward run to reverse"); return GRIM_EINVAL; }
   CK(cudaSetDevice(h->device));
