@@ -8,14 +8,17 @@
  *
  * Conventions
  *  - Every call returns an int status: 0 = OK, < 0 = error (GRIM_E*).
- *    No exceptions cross the ABI.
+ *    No exceptions cross the ABI.  A refused argument (NULL handle or
+ *    buffer, a selector, kind or count outside its range) returns
+ *    GRIM_EINVAL before any work is enqueued, and grim_last_error() says
+ *    which; grim_destroy(NULL) and grim_batch_destroy(NULL) do nothing.
  *  - Primitive arrays are FP64 in [var][k][j][i] order including ghost
  *    zones (i fastest), the layout of the reference's grid::vars and of
  *    gridPy.getVars (src/grid/gridPy.pyx:185-221).  N1T = N1 + 2*numGhost,
  *    N2T/N3T likewise for active dimensions (1 otherwise).
  *  - Pointers passed with GRIM_HOST are host memory (pageable or pinned),
- *    GRIM_DEVICE pointers are device memory on the handle's GPU.  The library
- *    copies; the caller keeps ownership.
+ *    GRIM_DEVICE pointers are device memory on the handle's GPU (any other
+ *    memKind is GRIM_EINVAL).  The library copies; the caller keeps ownership.
  *  - All work is asynchronous on the handle's stream except the getters of
  *    scalars and statistics, which synchronise.  Calls on one handle are not
  *    thread-safe; different handles are independent.
