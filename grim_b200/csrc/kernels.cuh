@@ -43,7 +43,7 @@ GRIM_D int bc_map(int x, int g, int N, int lo, int hi) {
   if (x < g) {
     if (lo == GRIM_PERIODIC) return g + ((x - g) % N + N) % N;
     if (lo == GRIM_MIRROR) return 2 * g - 1 - x;
-    return g;  // outflow (and Dirichlet: left to the problem hook)
+    return g;  // outflow
   }
   if (hi == GRIM_PERIODIC) return g + ((x - g) % N + N) % N;
   if (hi == GRIM_MIRROR) return 2 * (N + g) - 1 - x;

@@ -225,6 +225,13 @@ static int make_devcfg(const grim_config& c, DevCfg& d) {
   d.bc[4] = c.boundaryBack; d.bc[5] = c.boundaryFront;
   for (int q = 0; q < 6; q++)
     if (d.bc[q] < GRIM_PERIODIC || d.bc[q] > GRIM_EXCHANGE) { set_err("bad boundary condition %d", d.bc[q]); return GRIM_EINVAL; }
+  // boundary.cpp fills OUTFLOW and MIRROR sides only; a DIRICHLET side is
+  // the problem's own boundary hook, which none of the supported problems has
+  for (int q = 0; q < 6; q++)
+    if (d.bc[q] == GRIM_DIRICHLET) {
+      set_err("GRIM_DIRICHLET sides are a problem hook's; give the side GRIM_EXCHANGE and set its ghosts instead");
+      return GRIM_ENOTSUP;
+    }
   if (c.N3Global < 0 || (c.N3Global > 0 && (c.dim < 3 || c.N3Global < c.N3))) {
     set_err("N3Global: a slab of a 3D grid with N3 <= N3Global"); return GRIM_EINVAL;
   }

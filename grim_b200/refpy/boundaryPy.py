@@ -16,11 +16,14 @@ _handles = {}
 
 def _handle(prim, bcs):
     """A library handle of prim's shape with these boundary kinds (cached);
-    ideal MHD (8 variables per zone)."""
+    ideal MHD (8 variables per zone).  boundary.cpp:5-241 fills OUTFLOW and
+    MIRROR sides only and leaves PERIODIC (grid::communicate's) and
+    DIRICHLET (a problem hook's) sides as they are: those sides are
+    GRIM_EXCHANGE here, the library's "keep these ghosts"."""
     key = (prim.N1, prim.N2, prim.N3, prim.dim, prim.numGhostX1, bcs)
     if key not in _handles:
         from ..timestepper import timeStepper
-        left, right, top, bottom, front, back = bcs
+        left, right, top, bottom, front, back = (C.EXCHANGE if b in (PERIODIC, DIRICHLET) else b for b in bcs)
         cfg = C.make_config(N1=prim.N1, N2=prim.N2, N3=prim.N3, dim=prim.dim, numGhost=prim.numGhostX1,
                             boundaryLeft=left, boundaryRight=right, boundaryTop=top, boundaryBottom=bottom,
                             boundaryFront=front, boundaryBack=back)
@@ -30,8 +33,9 @@ def _handle(prim, bcs):
 
 def applyBoundaryConditionsPy(boundaryLeft, boundaryRight, boundaryTop, boundaryBottom, boundaryFront,
                               boundaryBack, prim):
-    """The ghost fill of every side, in place on prim's variables: they pass
-    through the library's state grid eight at a time."""
+    """The ghost fill of the OUTFLOW and MIRROR sides, in place on prim's
+    variables (the other sides keep their ghosts): they pass through the
+    library's state grid eight at a time."""
     bcs = tuple(int(b) for b in (boundaryLeft, boundaryRight, boundaryTop, boundaryBottom, boundaryFront,
                                  boundaryBack))
     ts = _handle(prim, bcs)

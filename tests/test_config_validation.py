@@ -72,6 +72,14 @@ def test_invalid_configuration_is_refused(name, overrides, words):
     assert words in msg, (name, msg)
 
 
+def test_dirichlet_sides_are_not_supported():
+    """boundary.cpp:5-241 leaves DIRICHLET sides to the problem's hook; no
+    supported problem has one, so such a side is refused, not filled."""
+    cfg = _base(boundaryRight=C.DIRICHLET)
+    rc, h, msg = _create(cfg)
+    assert rc == -5 and h is None and "GRIM_DIRICHLET" in msg
+
+
 def test_slab_count_below_the_slab_is_refused():
     cfg = C.make_config(dim=3, N1=8, N2=8, N3=8, N3Global=4)
     rc, h, msg = _create(cfg)

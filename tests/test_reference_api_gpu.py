@@ -87,6 +87,49 @@ def test_mirror(prim, side, axis, lower):
             np.testing.assert_equal(_plane(v, axis, n + NUM_GHOST + q), _plane(v, axis, n + NUM_GHOST - 1 - q))
 
 
+def _reference_fill(v, bcs, n, g):
+    """boundary.cpp:5-241 on a [var][k][j][i] array: the X1 sides over all
+    j, k, then the X2 sides over all i, k, then the X3 sides over all i, j;
+    only OUTFLOW and MIRROR sides are written."""
+    v = v.copy()
+    for axis in range(3):
+        lo, hi = bcs[2 * axis], bcs[2 * axis + 1]
+        N = n[axis]
+        for q in range(g):
+            dst_lo, dst_hi = q, N + g + q
+            src = {boundaryPy.OUTFLOW: (g, N + g - 1), boundaryPy.MIRROR: (2 * g - 1 - q, N + g - 1 - q)}
+            if lo in src:
+                _plane(v, axis, dst_lo)[...] = _plane(v, axis, src[lo][0])
+            if hi in src:
+                _plane(v, axis, dst_hi)[...] = _plane(v, axis, src[hi][1])
+    return v
+
+
+MIXED = [
+    # (left, right, bottom, top, back, front)
+    (boundaryPy.OUTFLOW, boundaryPy.PERIODIC, boundaryPy.MIRROR, boundaryPy.DIRICHLET,
+     boundaryPy.OUTFLOW, boundaryPy.PERIODIC),
+    (boundaryPy.PERIODIC, boundaryPy.MIRROR, boundaryPy.DIRICHLET, boundaryPy.OUTFLOW,
+     boundaryPy.MIRROR, boundaryPy.DIRICHLET),
+    (boundaryPy.PERIODIC,) * 6,
+]
+
+
+@pytest.mark.parametrize("bcs", MIXED)
+def test_mixed_sides_follow_the_reference_fill(bcs):
+    """With PERIODIC and DIRICHLET sides among OUTFLOW and MIRROR ones the
+    result is boundary.cpp's, corners included: the PERIODIC and DIRICHLET
+    sides keep their ghosts (boundary.cpp has no case for them), and each
+    later direction copies the earlier directions' ghost zones."""
+    g0 = gridPy.gridPy(N1, N2, N3, DIM, 10, NUM_GHOST, False, False, False)
+    g0.setVars(np.random.default_rng(3).random(g0.shape))
+    before = g0.getVars()
+    left, right, bottom, top, back, front = bcs
+    boundaryPy.applyBoundaryConditionsPy(left, right, top, bottom, front, back, g0)
+    want = _reference_fill(before, bcs, (g0.N1Local, g0.N2Local, g0.N3Local), NUM_GHOST)
+    np.testing.assert_array_equal(g0.getVars(), want)
+
+
 # ---- geometry (test_geometry.py) ---------------------------------------------
 @pytest.fixture(scope="module")
 def coords():
