@@ -337,11 +337,18 @@ KERNEL_SOURCES = ("kernels.cuh", "physics.cuh", "recon.cuh", "stage.cuh", "commo
 
 
 def kernel_sources_sha16():
+    """Fingerprint of the kernel sources' code: comments and blank space
+    removed, so that only a change of code makes a capture stale."""
     import hashlib
+    import re
     h = hashlib.sha256()
     for n in KERNEL_SOURCES:
-        with open(os.path.join(ROOT, "grim_b200", "csrc", n), "rb") as fh:
-            h.update(n.encode() + b"\0" + fh.read())
+        with open(os.path.join(ROOT, "grim_b200", "csrc", n)) as fh:
+            t = fh.read()
+        t = re.sub(r"/\*.*?\*/", " ", t, flags=re.S)
+        t = re.sub(r"//[^\n]*", " ", t)
+        t = " ".join(t.split())
+        h.update(n.encode() + b"\0" + t.encode())
     return h.hexdigest()[:16]
 
 
