@@ -21,6 +21,7 @@ DEBUG_SKIP_BULK_COPIES = 1
 LAYOUT_GHOSTED, LAYOUT_INTERIOR = 0, 1
 HOST, DEVICE = 0, 1
 PRIM_OLD, PRIM, PRIM_HALF = 0, 1, 2
+STAGE_CONS_OLD, STAGE_DIV_FLUXES, STAGE_SOURCES_EXPLICIT = 0, 1, 2
 
 
 class GrimStats(ctypes.Structure):
@@ -95,8 +96,10 @@ def lib():
         "grim_prims_from_natural": [P(GrimConfig), vp, vp],
         "grim_get_observations": [vp, P(d), i, P(i)],
         "grim_conserved": [vp, vp, vp, i],
+        "grim_element_fluxes": [vp, vp, i, vp, i],
         "grim_char_speeds": [vp, vp, i, vp, vp, i],
         "grim_stage_setup": [vp, i],
+        "grim_get_stage_grid": [vp, i, vp, i],
         "grim_residual": [vp, vp, vp, i],
         "grim_jacobian_fd": [vp, vp, vp, i],
         "grim_jacobian_tangent": [vp, vp, vp, i],

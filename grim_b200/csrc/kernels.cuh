@@ -2140,10 +2140,13 @@ __global__ void k_jacobian(DevCfg c, int stage, StageBufs b, const double* __res
     for (int q = 0; q < NF; q++) jac[(z * NF + a) * NF + q] = J[a][q];
 }
 
-// conserved variables / characteristic speeds of a prim array
+// the centre element of a prim array: its fluxes along X^fdir into out
+// (fluidElement::computeFluxes, physics.cpp:185-217; fdir 0 gives the
+// conserved variables) and / or its characteristic speeds along the
+// spatial direction dir into mn, mx
 template <int COND, int VISC>
 __global__ void k_conserved(DevCfg c, const double* __restrict__ p, const double* __restrict__ geoC,
-                                     double* __restrict__ out, int dir, double* mn, double* mx) {
+                                     double* __restrict__ out, int fdir, int dir, double* mn, double* mx) {
   constexpr int NF = 5 + COND + VISC;
   long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (z >= c.Z) return;
@@ -2158,8 +2161,8 @@ __global__ void k_conserved(DevCfg c, const double* __restrict__ p, const double
                        COND ? p[(long long)c.Q * Z + z] : 0., VISC ? p[(long long)c.DP * Z + z] : 0., G, c);
   if (out) {
     double U[NF], UB[3];
-    fluxes_fluid<COND, VISC>(e, 0, G.g, U, 5, 5 + COND);
-    fluxes_B(e, 0, G.g, UB);
+    fluxes_fluid<COND, VISC>(e, fdir, G.g, U, 5, 5 + COND);
+    fluxes_B(e, fdir, G.g, UB);
 #pragma unroll
     for (int v = 0; v < NF; v++) out[(long long)v * Z + z] = U[v];
 #pragma unroll
@@ -2604,13 +2607,13 @@ void jacobian(const DevCfg& c, int stage, const StageBufs& b, const double* pg, 
   GRIM_EMHD_DISPATCH(c, jacobian_t, c, stage, b, pg, jac, tangent, s);
 }
 template <int C, int V>
-static void conserved_t(const DevCfg& c, const double* p, const double* geoC, double* out, int dir, double* mn,
-                        double* mx, cudaStream_t s) {
-  k_conserved<C, V><<<nblk(c.Z, 128), 128, 0, s>>>(c, p, geoC, out, dir, mn, mx);
+static void conserved_t(const DevCfg& c, const double* p, const double* geoC, double* out, int fdir, int dir,
+                        double* mn, double* mx, cudaStream_t s) {
+  k_conserved<C, V><<<nblk(c.Z, 128), 128, 0, s>>>(c, p, geoC, out, fdir, dir, mn, mx);
 }
-void conserved(const DevCfg& c, const double* p, const double* geoC, double* out, int dir, double* mn, double* mx,
-               cudaStream_t s) {
-  GRIM_EMHD_DISPATCH(c, conserved_t, c, p, geoC, out, dir, mn, mx, s);
+void conserved(const DevCfg& c, const double* p, const double* geoC, double* out, int fdir, int dir, double* mn,
+               double* mx, cudaStream_t s) {
+  GRIM_EMHD_DISPATCH(c, conserved_t, c, p, geoC, out, fdir, dir, mn, mx, s);
 }
 void reconstruct(const DevCfg& c, int dir, const double* p, double* pl, double* pr, cudaStream_t s) {
   k_reconstruct<<<nblk(c.Z, 128), 128, 0, s>>>(c, dir, p, pl, pr);

@@ -27,7 +27,7 @@
                 cudaStream_t s);                                                                        \
   void jacobian(const DevCfg& c, int stage, const StageBufs& b, const double* pg, double* jac,         \
                 int tangent, cudaStream_t s);                                                           \
-  void conserved(const DevCfg& c, const double* p, const double* geoC, double* out, int dir,           \
+  void conserved(const DevCfg& c, const double* p, const double* geoC, double* out, int fdir, int dir, \
                  double* mn, double* mx, cudaStream_t s);                                               \
   void reconstruct(const DevCfg& c, int dir, const double* p, double* pl, double* pr, cudaStream_t s); \
   int batch_solve(int n, int batch, const double* A, const double* b, double* x, cudaStream_t s);      \

@@ -1256,18 +1256,23 @@ int grim_compute_divb(grim_handle* h, const double* prim, double* divB, int memK
   return stage_out(h, divB, h->scratch2, h->bytesZ, memKind);
 }
 
-int grim_conserved(grim_handle* h, const double* prim, double* cons, int memKind) {
+int grim_element_fluxes(grim_handle* h, const double* prim, int dir, double* out, int memKind) {
   if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
-  if (!h || !prim || !cons) return GRIM_EINVAL;
+  if (!h || !prim || !out) { set_err("null argument"); return GRIM_EINVAL; }
+  if (dir < 0 || dir > 3) { set_err("grim_element_fluxes: direction %d outside 0..3", dir); return GRIM_EINVAL; }
   CK(cudaSetDevice(h->device));
   const DevCfg& c = h->dc;
   int rc = stage_in(h, h->scratch, prim, c.dof, memKind);
   if (rc) return rc;
   const bool mink = h->cfg.metric == GRIM_MINKOWSKI;
-  KNS_CALL(h, conserved, c, h->scratch, mink ? nullptr : h->geo[GRIM_CENTER], h->scratch2, 0, nullptr, nullptr,
-           h->stream);
+  KNS_CALL(h, conserved, c, h->scratch, mink ? nullptr : h->geo[GRIM_CENTER], h->scratch2, dir, 0, nullptr,
+           nullptr, h->stream);
   CK(cudaGetLastError());
-  return stage_out(h, cons, h->scratch2, (size_t)c.dof * h->bytesZ, memKind);
+  return stage_out(h, out, h->scratch2, (size_t)c.dof * h->bytesZ, memKind);
+}
+
+int grim_conserved(grim_handle* h, const double* prim, double* cons, int memKind) {
+  return grim_element_fluxes(h, prim, 0, cons, memKind);
 }
 
 int grim_char_speeds(grim_handle* h, const double* prim, int dir, double* mn, double* mx, int memKind) {
@@ -1280,7 +1285,7 @@ int grim_char_speeds(grim_handle* h, const double* prim, int dir, double* mn, do
   const bool mink = h->cfg.metric == GRIM_MINKOWSKI;
   double* a = h->scratch2;
   double* b = h->scratch2 + c.Z;
-  KNS_CALL(h, conserved, c, h->scratch, mink ? nullptr : h->geo[GRIM_CENTER], nullptr, dir, a, b, h->stream);
+  KNS_CALL(h, conserved, c, h->scratch, mink ? nullptr : h->geo[GRIM_CENTER], nullptr, 0, dir, a, b, h->stream);
   CK(cudaGetLastError());
   rc = stage_out(h, mn, a, h->bytesZ, memKind);
   if (rc) return rc;
@@ -1299,6 +1304,19 @@ int grim_stage_setup(grim_handle* h, int stage) {
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(h->stream));
   return GRIM_OK;
+}
+
+int grim_get_stage_grid(grim_handle* h, int which, double* out, int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
+  if (!h || !out) { set_err("null argument"); return GRIM_EINVAL; }
+  const DevCfg& c = h->dc;
+  const double* src = which == GRIM_STAGE_CONS_OLD ? h->consOld
+                      : which == GRIM_STAGE_DIV_FLUXES ? h->divF
+                      : which == GRIM_STAGE_SOURCES_EXPLICIT ? h->Sexp : nullptr;
+  if (!src) { set_err("bad stage grid %d", which); return GRIM_EINVAL; }
+  CK(cudaSetDevice(h->device));
+  const int rows = which == GRIM_STAGE_CONS_OLD ? c.dof : c.nf;
+  return stage_out(h, out, src, (size_t)rows * h->bytesZ, memKind);
 }
 
 int grim_residual(grim_handle* h, const double* pg, double* res, int memKind) {

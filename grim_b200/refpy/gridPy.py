@@ -7,6 +7,8 @@ from .. import config as C
 # locations::CENTER ... BACK (src/params.hpp:34-37); the first five are the
 # library's GRIM_CENTER .. GRIM_BOTTOM
 CENTER, LEFT, RIGHT, TOP, BOTTOM, FRONT, BACK = range(7)
+# directions:: (src/params.hpp:40-46)
+X1, X2, X3 = 0, 1, 2
 
 
 def _totals(N1, N2, N3, dim, numGhost):

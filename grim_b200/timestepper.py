@@ -384,12 +384,30 @@ class timeStepper:
         _lib.check(_lib.lib().grim_conserved(self._h, _ptr(p), _ptr(out), _lib.HOST), "conserved")
         return out
 
+    def elementFluxes(self, prim, direction):
+        """fluidElement::computeFluxes(direction) at the zone centres
+        (physics.cpp:185-217): dof x Z; direction 0 gives the conserved
+        variables."""
+        p = np.ascontiguousarray(prim, dtype=np.float64)
+        out = self._zeros(self.dof)
+        _lib.check(_lib.lib().grim_element_fluxes(self._h, _ptr(p), int(direction), _ptr(out), _lib.HOST),
+                   "elementFluxes")
+        return out
+
     def charSpeeds(self, prim, direction):
         p = np.ascontiguousarray(prim, dtype=np.float64)
         mn, mx = np.zeros(self.zshape), np.zeros(self.zshape)
         _lib.check(_lib.lib().grim_char_speeds(self._h, _ptr(p), int(direction), _ptr(mn), _ptr(mx),
                                                _lib.HOST), "charSpeeds")
         return mn, mx
+
+    def stageGrid(self, which):
+        """consOld (STAGE_CONS_OLD, dof rows), divFluxes or sourcesExplicit
+        (nf fluid rows) as the last stage left them; interior zones."""
+        rows = self.dof if which == _lib.STAGE_CONS_OLD else self.numFluidVars
+        out = self._zeros(rows)
+        _lib.check(_lib.lib().grim_get_stage_grid(self._h, int(which), _ptr(out), _lib.HOST), "stageGrid")
+        return out
 
     def stageSetup(self, stage):
         _lib.check(_lib.lib().grim_stage_setup(self._h, int(stage)), "stage_setup")

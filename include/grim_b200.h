@@ -283,6 +283,11 @@ int grim_compute_divb(grim_handle* h, const double* prim, double* divB, int memK
 /* conserved variables and characteristic speeds of a prim array at the
  * zone centres (physics.cpp:185-217, riemannsolver.cpp:54-200) */
 int grim_conserved(grim_handle* h, const double* prim, double* cons, int memKind);
+/* fluidElement::set then computeFluxes(dir) (physics.cpp:53-217) at the zone
+ * centres with the centre geometry: out (dof x Z) = the fluxes along X^dir,
+ * dir 0..3 (0: the conserved variables, as grim_conserved); the reference's
+ * fluidElementPy.computeFluxes (physicsPy.pyx:31-42) */
+int grim_element_fluxes(grim_handle* h, const double* prim, int dir, double* out, int memKind);
 int grim_char_speeds(grim_handle* h, const double* prim, int dir,
                      double* minSpeed, double* maxSpeed, int memKind);
 
@@ -290,6 +295,18 @@ int grim_char_speeds(grim_handle* h, const double* prim, int dir,
 /* Stage set-up of timeStep (BCs, elemOld, consOld, sources, divF,
  * induction) on the current state, leaving the Newton guess in GRIM_PRIM. */
 int grim_stage_setup(grim_handle* h, int stage);
+/* The stage grids the last stage left (grim_stage_setup, or the full stage
+ * of a step), timeStepperPy's consOld, divFluxes and sourcesExplicit
+ * (timestep.cpp:26-79, 180-237): GRIM_STAGE_CONS_OLD is dof x Z (the
+ * conserved variables of primOld, formed on the half stage);
+ * GRIM_STAGE_DIV_FLUXES and GRIM_STAGE_SOURCES_EXPLICIT are nf x Z, the
+ * fluid rows (the field rows of the divergence go straight into the
+ * induction update and are not kept; the explicit sources have none).
+ * Interior zones only: the ghost entries of out are unspecified.  With the
+ * Minkowski metric and ideal MHD the explicit sources are zero and never
+ * written. */
+enum { GRIM_STAGE_CONS_OLD = 0, GRIM_STAGE_DIV_FLUXES = 1, GRIM_STAGE_SOURCES_EXPLICIT = 2 };
+int grim_get_stage_grid(grim_handle* h, int which, double* out, int memKind);
 /* computeResidual (residual.cpp:3-180) of a guess: nf x Z */
 int grim_residual(grim_handle* h, const double* primGuess, double* residual, int memKind);
 /* FD Jacobian (solve.cpp:82-109): [Z][nf][nf], J[z][i][j] = dR_i/dP_j */

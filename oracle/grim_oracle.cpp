@@ -1728,6 +1728,28 @@ int orc_conserved(orc_handle* h, const double* prim, double* cons) {
   std::memcpy(cons, c.d.data(), sizeof(double) * c.d.size());
   return 0;
 }
+/* fluidElement::set then computeFluxes(dir) (physics.cpp:53-217) at the
+ * zone centres, dir = 0 (the conserved variables), 1, 2, 3 */
+int orc_element_fluxes(orc_handle* h, const double* prim, int dir, double* out) {
+  if (dir < 0 || dir > 3) return -1;
+  Stepper& s = h->s;
+  const long Z = s.L.Z; const int dof = s.P.dof;
+  Grid p; p.init(dof, Z); std::memcpy(p.d.data(), prim, sizeof(double) * p.d.size());
+  Elem e; e.alloc(s.L, s.P); e.set(p, s.geomCenter);
+  Grid f; f.init(dof, Z); e.computeFluxes(dir, f);
+  std::memcpy(out, f.d.data(), sizeof(double) * f.d.size());
+  return 0;
+}
+/* the stage grids stageSetup left (timestep.cpp:26-79 / 180-237):
+ * 0 consOld (dof rows), 1 divFluxes and 2 sourcesExplicit (the nf fluid rows) */
+int orc_get_stage_grid(const orc_handle* h, int which, double* out) {
+  const Stepper& s = h->s;
+  const Grid* g = which == 0 ? &s.consOld : which == 1 ? &s.divFluxes : which == 2 ? &s.sourcesExplicit : nullptr;
+  if (!g) return -1;
+  const int rows = which == 0 ? s.P.dof : s.P.nf;
+  std::memcpy(out, g->d.data(), sizeof(double) * (size_t)rows * s.L.Z);
+  return 0;
+}
 /* computeDivB (constrainedtransport.cpp:85-110), 2D */
 int orc_compute_divb(orc_handle* h, const double* prim, double* divB) {
   Stepper& s = h->s;

@@ -94,6 +94,8 @@ int  orc_reconstruct(orc_handle* h, const double* prim, int dir,
                      double* primLeft, double* primRight);
 /* conserved variables U = computeFluxes(0) of prim, dof x Z */
 int  orc_conserved(orc_handle* h, const double* prim, double* cons);
+int  orc_element_fluxes(orc_handle* h, const double* prim, int dir, double* out);
+int  orc_get_stage_grid(const orc_handle* h, int which, double* out);
 int  orc_compute_divb(orc_handle* h, const double* prim, double* divB);
 /* torus observers on primOld: mass, EMag, ETh, rhoMax, betaMin, MdotIn,
  * MdotOut, unbound and relativistic unbound MdotOut (9 values) */

@@ -83,6 +83,8 @@ def lib():
         L.orc_div_fluxes.argtypes = [vp, P(d), P(d), P(d), P(d)]
         L.orc_reconstruct.argtypes = [vp, P(d), i, P(d), P(d)]
         L.orc_conserved.argtypes = [vp, P(d), P(d)]
+        L.orc_element_fluxes.argtypes = [vp, P(d), ctypes.c_int, P(d)]
+        L.orc_get_stage_grid.argtypes = [vp, ctypes.c_int, P(d)]
         L.orc_compute_divb.argtypes = [vp, P(d), P(d)]
         L.orc_torus_observers.argtypes = [vp, P(d)]
         L.orc_char_speeds.argtypes = [vp, P(d), i, P(d), P(d)]
@@ -226,6 +228,21 @@ class Oracle:
         c = self._arr()
         lib().orc_conserved(self._h, _ptr(p), _ptr(c))
         return c
+
+    def element_fluxes(self, prim, direction):
+        """fluidElement::computeFluxes(direction) at the zone centres
+        (physics.cpp:185-217); direction 0 gives the conserved variables."""
+        p = np.ascontiguousarray(prim, dtype=np.float64)
+        out = self._arr()
+        assert lib().orc_element_fluxes(self._h, _ptr(p), int(direction), _ptr(out)) == 0
+        return out
+
+    def stage_grid(self, which):
+        """consOld (0, dof rows), divFluxes (1) or sourcesExplicit (2, the
+        fluid rows) as the last stage_setup left them."""
+        out = self._arr(self.dof if which == 0 else self.nf)
+        assert lib().orc_get_stage_grid(self._h, int(which), _ptr(out)) == 0
+        return out
 
     def compute_divb(self, prim):
         p = np.ascontiguousarray(prim, dtype=np.float64)
