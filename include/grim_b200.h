@@ -41,7 +41,9 @@ extern "C" {
 #define GRIM_ESTATE       -4   /* call not valid in the current state */
 #define GRIM_ENOTSUP      -5   /* configuration not supported */
 #define GRIM_ETIMEOUT     -6   /* a bounded device wait gave up */
-#define GRIM_ENONFINITE   -7   /* NaN/Inf detected in a result */
+/* Non-finite primitives are not an error status: a step counts them
+ * (grim_stats.nonFinite) and the torus problem resets them, as the
+ * reference's fullStepDiagnostics does (torus/problem.cpp:719-878). */
 
 /* ---- enums (src/params.hpp:32-94; MP5, closures, Newton modes are new) -- */
 enum { GRIM_PERIODIC = 0, GRIM_OUTFLOW = 1, GRIM_MIRROR = 2, GRIM_DIRICHLET = 3,
