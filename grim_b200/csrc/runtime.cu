@@ -85,6 +85,9 @@ struct grim_handle {
   long long launchesPerStep = 0;
   size_t bytesZ = 0;
   int lastStage = GRIM_HALF_STEP;
+  // the stage constants (consOld, divF, Sexp, the field guess) are those
+  // grim_stage_setup formed, not yet replaced by a step or a stencil call
+  bool stageReady = false;
   // per-kernel-group device timing (grim_profile_steps): event pairs
   // recorded around each launch on the handle's stream
   // TMA descriptors of the arrays the X1 face kernel reads (primOld,
@@ -872,6 +875,7 @@ static int run_steps(grim_handle* h, int nsteps) {
     const int rc = take_async_error(h);
     if (rc) return rc;
   }
+  h->stageReady = false;
   CK(cudaSetDevice(h->device));
   for (int n = 0; n < nsteps; n++) {
     const bool last = (n == nsteps - 1);
@@ -950,6 +954,7 @@ int grim_time_steps_host(grim_handle* h, int nsteps, const double* const* hostIn
     const int rc = take_async_error(h);
     if (rc) return rc;
   }
+  h->stageReady = false;
   CK(cudaSetDevice(h->device));
   const bool interior = layout == GRIM_LAYOUT_INTERIOR;
   const size_t bytes = (size_t)h->dc.dof * h->bytesZ;
@@ -1098,6 +1103,7 @@ int grim_compute_div_fluxes(grim_handle* h, const double* prim, double* divF, do
   if (!h || !prim) return GRIM_EINVAL;
   CK(cudaSetDevice(h->device));
   const DevCfg& c = h->dc;
+  h->stageReady = false;  // the pass below replaces divF and the field guess
   int rc = stage_in(h, h->scratch, prim, c.dof, memKind);
   if (rc) return rc;
   // a stencil pass on the scratch prims as a half stage with dt = 0 keeps
@@ -1159,6 +1165,7 @@ int grim_reconstruct(grim_handle* h, const double* prim, int dir, double* pl, do
 int grim_step_segment(grim_handle* h, int segment) {
   if (!h || segment < GRIM_SEG_PRE || segment > GRIM_SEG_POST) { set_err("bad segment"); return GRIM_EINVAL; }
   CK(cudaSetDevice(h->device));
+  h->stageReady = false;
   enqueue_segment(h, segment);
   CK(cudaGetLastError());
   return GRIM_OK;
@@ -1301,6 +1308,7 @@ int grim_stage_setup(grim_handle* h, int stage) {
   enqueue_problem_bcs(h, ps);
   enqueue_stencil(h, stage);
   h->lastStage = stage;
+  h->stageReady = true;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(h->stream));
   return GRIM_OK;
@@ -1319,9 +1327,17 @@ int grim_get_stage_grid(grim_handle* h, int which, double* out, int memKind) {
   return stage_out(h, out, src, (size_t)rows * h->bytesZ, memKind);
 }
 
+// the Newton pieces read the constants of the stage grim_stage_setup formed
+static int stage_ready(grim_handle* h, const char* what) {
+  if (h->stageReady) return GRIM_OK;
+  set_err("%s: no stage set up (grim_stage_setup), or a step or stencil call has replaced it since", what);
+  return GRIM_ESTATE;
+}
+
 int grim_residual(grim_handle* h, const double* pg, double* res, int memKind) {
   if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   if (!h || !pg || !res) return GRIM_EINVAL;
+  if (const int rc = stage_ready(h, "grim_residual")) return rc;
   CK(cudaSetDevice(h->device));
   const DevCfg& c = h->dc;
   int rc = stage_in(h, h->scratch, pg, c.dof, memKind);
@@ -1334,6 +1350,7 @@ int grim_residual(grim_handle* h, const double* pg, double* res, int memKind) {
 
 static int jac_common(grim_handle* h, const double* pg, double* jac, int memKind, int tangent) {
   if (!h || !pg || !jac) return GRIM_EINVAL;
+  if (const int rc = stage_ready(h, "Jacobian")) return rc;
   CK(cudaSetDevice(h->device));
   const DevCfg& c = h->dc;
   int rc = stage_in(h, h->scratch, pg, c.dof, memKind);
@@ -1371,6 +1388,7 @@ int grim_jacobian_form(grim_handle* h, const double* pg, double* jac, int form, 
 
 int grim_newton_solve(grim_handle* h, int* iters) {
   if (!h) return GRIM_EINVAL;
+  if (const int rc = stage_ready(h, "grim_newton_solve")) return rc;
   CK(cudaSetDevice(h->device));
   cudaMemsetAsync(h->st->count, 0, sizeof(h->st->count), h->stream);
   cudaMemsetAsync(h->st->itersDone, 0, sizeof(h->st->itersDone), h->stream);
@@ -1741,6 +1759,7 @@ int grim_adjoint_forward(grim_handle* h, int nsteps, int every) {
   if (!h || nsteps <= 0 || every <= 0) { set_err("grim_adjoint_forward: bad argument"); return GRIM_EINVAL; }
   int rc = adjoint_scope(h);
   if (rc) return rc;
+  h->stageReady = false;
   CK(cudaSetDevice(h->device));
   const size_t bytes = (size_t)h->dc.dof * h->bytesZ;
   const int nck = (nsteps + every - 1) / every;
@@ -1770,7 +1789,8 @@ int grim_adjoint_forward(grim_handle* h, int nsteps, int every) {
 int grim_adjoint_backward(grim_handle* h, const double* lambda, double* grad, int memKind) {
   if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
   if (!h || !lambda || !grad) { set_err("grim_adjoint_backward: null argument"); return GRIM_EINVAL; }
-  if (h->adjSteps <= 0) { set_err("grim_adjoint_backward: no grim_adjoint_forward run to reverse"); return GRIM_EINVAL; }
+  if (h->adjSteps <= 0) { set_err("grim_adjoint_backward: no grim_adjoint_forward run to reverse"); return GRIM_ESTATE; }
+  h->stageReady = false;
   CK(cudaSetDevice(h->device));
   const DevCfg& c = h->dc;
   const size_t bytes = (size_t)c.dof * h->bytesZ;

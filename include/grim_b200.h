@@ -326,7 +326,11 @@ enum {
   GRIM_JAC_FAST32 = 3    /* the mixed Newton's Jacobian: FAST64's form on FP32 geometry, in FP32 */
 };
 int grim_jacobian_form(grim_handle* h, const double* primGuess, double* jac, int form, int memKind);
-/* solve() on GRIM_PRIM with the configured newtonMode */
+/* solve() on GRIM_PRIM with the configured newtonMode.
+ * grim_residual, the grim_jacobian_* calls and grim_newton_solve read the
+ * stage grim_stage_setup formed: they return GRIM_ESTATE before the first
+ * grim_stage_setup and after any call that replaces its constants (a step,
+ * a step segment, grim_compute_div_fluxes, the adjoint calls). */
 int grim_newton_solve(grim_handle* h, int* itersDone);
 /* batched pivoted solve of nf x nf systems (the af::solve of solve.cpp:220)
  * A: [batch][n][n] row-major, b: [batch][n] */
@@ -452,6 +456,7 @@ int grim_set_face_variant(grim_handle* h, int dir, int variant);
  * interior zones (ghost entries zero; the ghosts are images of interior
  * zones and their share is folded in).  Each segment between checkpoints
  * is recomputed forward once; the stepper is left at the final state.
+ * Without a grim_adjoint_forward run to reverse it returns GRIM_ESTATE.
  * Supported: 2D and 3D, ideal or extended MHD (conduction and / or
  * viscosity), Minkowski or modified Kerr-Schild (geometric source, face
  * metric), periodic / outflow / mirror boundaries, no problem hooks; or

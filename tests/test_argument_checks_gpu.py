@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 from grim_b200 import _lib
+from grim_b200 import config as C
 from grim_b200 import problems as PR
 
 pytestmark = pytest.mark.gpu
@@ -69,3 +70,37 @@ def test_bad_arguments_are_refused_and_leave_the_handle_as_it_was():
             s.timeStep()
     np.testing.assert_array_equal(ts.primOld.getVars(), ref.primOld.getVars())
     assert (ts.time, ts.dt) == (ref.time, ref.dt)
+
+
+ESTATE = -4
+
+
+def test_calls_out_of_order_are_refused_with_estate():
+    """The Newton pieces read the stage grim_stage_setup formed: before it,
+    and after a step has replaced its constants, they return GRIM_ESTATE;
+    the adjoint's backward sweep needs a forward run first."""
+    cfg = PR.fast_mode_config(N=16)
+    P = PR.fast_mode_prims(cfg)
+    ts = _stepper(cfg, P)
+    L, h = _lib.lib(), ts._h
+    host = np.zeros(ts.prim.getVars().shape)
+    hp = ctypes.c_void_p(host.ctypes.data)
+    it = ctypes.c_int()
+
+    def refused(rc):
+        assert rc == ESTATE, rc
+        assert "grim_stage_setup" in L.grim_last_error().decode()
+
+    refused(L.grim_residual(h, hp, hp, _lib.HOST))
+    refused(L.grim_jacobian_fd(h, hp, hp, _lib.HOST))
+    refused(L.grim_newton_solve(h, ctypes.byref(it)))
+    ts.stageSetup(C.HALF_STEP)
+    r = ts.computeResidual(P)
+    assert np.isfinite(r).all()
+    ts.timeStep()
+    refused(L.grim_jacobian_tangent(h, hp, hp, _lib.HOST))
+    ts.stageSetup(C.HALF_STEP)
+    assert np.isfinite(ts.computeResidual(ts.primOld.getVars())).all()
+
+    rc = L.grim_adjoint_backward(h, hp, hp, _lib.HOST)
+    assert rc == ESTATE and "grim_adjoint_forward" in L.grim_last_error().decode()
