@@ -4,6 +4,18 @@ of a grid of primitives (fluidElement, physics.cpp:53-183) and its fluxes
 element kernel on the GPU (grim_element_fluxes)."""
 from .gridPy import CENTER
 
+_handles = {}
+
+
+def _handle(cfg):
+    """A library handle of this configuration (cached: an element holds
+    only its primitives, the handle's grids are scratch)."""
+    from ..timestepper import timeStepper
+    key = tuple(sorted(cfg.items()))
+    if key not in _handles:
+        _handles[key] = timeStepper(cfg)
+    return _handles[key]
+
 
 class fluidElementPy:
     """fluidElement(prim, geom): the element is set from prim when it is
@@ -13,7 +25,6 @@ class fluidElementPy:
     zone centres (geom set to CENTER)."""
 
     def __init__(self, prim, geom, conduction=None, viscosity=None):
-        from ..timestepper import timeStepper
         if conduction is None and viscosity is None:
             if prim.numVars not in (8, 10):
                 raise ValueError("numVars %d: give conduction and viscosity" % prim.numVars)
@@ -22,7 +33,7 @@ class fluidElementPy:
             raise ValueError("the element is set with the geometry at the zone centres")
         cfg = dict(geom._ts.cfg)
         cfg.update(conduction=int(bool(conduction)), viscosity=int(bool(viscosity)))
-        self._ts = timeStepper(cfg)
+        self._ts = _handle(cfg)
         if self._ts.dof != prim.numVars:
             raise ValueError("numVars %d, but the element has %d variables" % (prim.numVars, self._ts.dof))
         self._prim = prim.getVars().copy()
