@@ -96,6 +96,20 @@ class timeStepper {
     check(grim_compute_div_fluxes(h_, primHost, divFluxesHost, nullptr, nullptr, GRIM_HOST),
           "computeDivOfFluxes");
   }
+  // timeStepper::computeDivB (constrainedtransport.cpp:85-110), 1 x Z
+  void computeDivB(const double* primHost, double* divBHost) {
+    check(grim_compute_divb(h_, primHost, divBHost, GRIM_HOST), "computeDivB");
+  }
+  // fluidElement::set + computeFluxes(dir) (physics.cpp:53-217) at the zone
+  // centres, dof x Z; dir 0 gives the conserved variables
+  void computeFluxes(const double* primHost, int dir, double* fluxHost) {
+    check(grim_element_fluxes(h_, primHost, dir, fluxHost, GRIM_HOST), "computeFluxes");
+  }
+  // consOld / divFluxes / sourcesExplicit of the last stage
+  // (GRIM_STAGE_*; grim_get_stage_grid)
+  void stageGrid(int which, double* outHost) {
+    check(grim_get_stage_grid(h_, which, outHost, GRIM_HOST), "stageGrid");
+  }
   void setNewtonMode(int mode, int perZone, double rtol) {
     check(grim_set_newton_mode(h_, mode, perZone, rtol), "setNewtonMode");
   }

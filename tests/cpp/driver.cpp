@@ -1,6 +1,7 @@
 // A C++ driver written against the reference-shaped facade
 // (include/grim_b200_timestepper.hpp): 2D ideal fast mode 32^2, a few
-// timesteps, prints time and a checksum of the primitives.  The GPU test
+// timesteps, prints time and checksums of the primitives, of the element
+// fluxes along X1 and X0 and of |div B| of the final state.  The GPU test
 // compares its output with the Python binding of the same library.
 #include <cmath>
 #include <cstdio>
@@ -47,6 +48,21 @@ int main(int argc, char** argv) {
   for (int v = 0; v < 8; v++)
     for (int j = 3; j < 3 + N; j++)
       for (int i = 3; i < 3 + N; i++) sum += Q[(size_t)v * n1 * n2 + (size_t)j * n1 + i];
-  printf("%.17g %.17g\n", ts.time, sum);
+  // the element's X1 fluxes and the conserved variables of the final state,
+  // and the corner divergence of its field
+  std::vector<double> F(Q.size()), U(Q.size()), D((size_t)n1 * n2);
+  ts.computeFluxes(Q.data(), 1, F.data());
+  ts.computeFluxes(Q.data(), 0, U.data());
+  ts.computeDivB(Q.data(), D.data());
+  double sumF = 0., sumU = 0., sumD = 0.;
+  for (int v = 0; v < 8; v++)
+    for (int j = 3; j < 3 + N; j++)
+      for (int i = 3; i < 3 + N; i++) {
+        sumF += F[(size_t)v * n1 * n2 + (size_t)j * n1 + i];
+        sumU += U[(size_t)v * n1 * n2 + (size_t)j * n1 + i];
+      }
+  for (int j = 3; j < 3 + N; j++)
+    for (int i = 3; i < 3 + N; i++) sumD += fabs(D[(size_t)j * n1 + i]);
+  printf("%.17g %.17g %.17g %.17g %.17g\n", ts.time, sum, sumF, sumU, sumD);
   return 0;
 }

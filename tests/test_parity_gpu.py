@@ -361,7 +361,7 @@ def test_cpp_driver_matches_python_binding(tmp_path):
     from tests.test_abi import _build_cpp_driver
     exe = _build_cpp_driver(tmp_path)
     out = subprocess.check_output([exe, "3"]).decode().split()
-    t_cpp, sum_cpp = float(out[0]), float(out[1])
+    t_cpp, sum_cpp, sumF_cpp, sumU_cpp, sumD_cpp = (float(x) for x in out)
     cfg = PR.fast_mode_config(N=32, CourantFactor=0.5)
     X1, X2, _ = C.cell_centers(cfg)
     base = [1., 2., 0., 0., 0., 0.1, 0.3, 0.]
@@ -371,9 +371,15 @@ def test_cpp_driver_matches_python_binding(tmp_path):
     ts.primOld.setVars(P)
     for _ in range(3):
         ts.timeStep()
-    Q = interior(cfg, ts.primOld.getVars())
+    Qg = ts.primOld.getVars()
+    Q = interior(cfg, Qg)
     assert t_cpp == ts.time
     assert abs(sum_cpp - float(np.sum(Q))) <= 1e-12 * abs(sum_cpp)
+    # the facade's computeFluxes / computeDivB: the same calls as the binding's
+    for got, want in ((sumF_cpp, np.sum(interior(cfg, ts.elementFluxes(Qg, 1)))),
+                      (sumU_cpp, np.sum(interior(cfg, ts.elementFluxes(Qg, 0)))),
+                      (sumD_cpp, np.sum(np.abs(interior(cfg, ts.computeDivB(Qg)[None]))))):
+        assert abs(got - float(want)) <= 1e-12 * max(abs(got), 1e-300), (got, want)
 
 
 def test_profile_steps_and_flop_counts():
