@@ -79,6 +79,9 @@ def lib():
         "grim_apply_boundaries": [vp, i],
         "grim_communicate": [vp, i],
         "grim_compute_div_fluxes": [vp, vp, vp, vp, vp, i],
+        "grim_compute_emf": [vp, vp, vp, i],
+        "grim_flux_ct": [vp, vp, vp, i],
+        "grim_capture_graph": [vp, i],
         "grim_reconstruct": [vp, vp, i, vp, vp, i],
         "grim_compute_divb": [vp, vp, vp, i],
         "grim_torus_observers": [vp, P(d)],

@@ -937,6 +937,37 @@ static void interior_copy(const DevCfg& c, const double* src, double* dst, bool 
   k_interior_copy<<<grid, 256, 0, s>>>(c, src, dst, toGrid ? 1 : 0);
 }
 
+// fluxCT (constrainedtransport.cpp:3-51) on the face fluxes f[0..dim): the
+// field rows replaced by averages of the edge EMFs emf = [E1 | E2 | E3] x Z,
+// each with its neighbour one zone up along the other direction taken by
+// circular shift over the whole array, as af::shift takes it; a
+// direction's own field row is zero.  One thread per zone, dim >= 2.
+__global__ void k_flux_ct(DevCfg c, double* __restrict__ f1, double* __restrict__ f2, double* __restrict__ f3,
+                          const double* __restrict__ emf) {
+  const long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= c.Z) return;
+  const long long Z = c.Z;
+  int i, j, k;
+  zijk(c, z, i, j, k);
+  const long long zi = zidx(c, (i + 1) % c.N1T, j, k), zj = zidx(c, i, (j + 1) % c.N2T, k);
+  const long long b1 = (long long)c.B1 * Z + z, b2 = b1 + Z, b3 = b2 + Z;
+  const double* e1 = emf;
+  const double* e2 = emf + Z;
+  const double* e3 = emf + 2 * Z;
+  f1[b1] = 0.;
+  f1[b2] = 0.5 * (e3[z] + e3[zj]);
+  f2[b1] = -0.5 * (e3[z] + e3[zi]);
+  f2[b2] = 0.;
+  if (c.dim == 3) {
+    const long long zk = zidx(c, i, j, (k + 1) % c.N3T);
+    f1[b3] = -0.5 * (e2[z] + e2[zk]);
+    f2[b3] = 0.5 * (e1[z] + e1[zk]);
+    f3[b1] = 0.5 * (e2[z] + e2[zi]);
+    f3[b2] = -0.5 * (e1[z] + e1[zj]);
+    f3[b3] = 0.;
+  }
+}
+
 extern "C" {
 
 // nsteps of (primOld <- hostIn[k]; timeStep; hostOut[k] <- primOld) with the
@@ -1145,6 +1176,34 @@ int grim_compute_div_fluxes(grim_handle* h, const double* prim, double* divF, do
   CK(cudaStreamSynchronize(h->stream));
   return GRIM_OK;
 }
+
+int grim_compute_emf(grim_handle* h, const double* prim, double* emf, int memKind) {
+  if (!emf) { set_err("null argument"); return GRIM_EINVAL; }
+  return grim_compute_div_fluxes(h, prim, nullptr, nullptr, emf, memKind);
+}
+
+int grim_flux_ct(grim_handle* h, const double* prim, double* fluxes, int memKind) {
+  if (!mem_kind_ok(memKind)) return GRIM_EINVAL;
+  if (!h || !prim || !fluxes) { set_err("null argument"); return GRIM_EINVAL; }
+  // the Riemann fluxes of prim into the handle's face-flux buffers
+  int rc = grim_compute_div_fluxes(h, prim, nullptr, nullptr, nullptr, memKind);
+  if (rc) return rc;
+  const DevCfg& c = h->dc;
+  if (c.dim >= 2) {
+    const double* fl[3] = {h->flux[0], h->flux[1], h->flux[2]};
+    grim::exact::emf(c, fl, h->scratch, h->stream);
+    k_flux_ct<<<(unsigned)((c.Z + 255) / 256), 256, 0, h->stream>>>(c, h->flux[0], h->flux[1],
+                                                                     c.dim == 3 ? h->flux[2] : nullptr, h->scratch);
+    CK(cudaGetLastError());
+  }
+  for (int d = 0; d < c.dim; d++) {
+    rc = stage_out(h, fluxes + (size_t)d * c.dof * c.Z, h->flux[d], (size_t)c.dof * h->bytesZ, memKind);
+    if (rc) return rc;
+  }
+  return GRIM_OK;
+}
+
+int grim_capture_graph(grim_handle* h, int enable) { return grim_enable_graph(h, enable); }
 
 int grim_reconstruct(grim_handle* h, const double* prim, int dir, double* pl, double* pr, int memKind) {
   if (!mem_kind_ok(memKind)) return GRIM_EINVAL;

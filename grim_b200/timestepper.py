@@ -281,39 +281,21 @@ class timeStepper:
         (3 x Z) from the Riemann fluxes of prim."""
         p = np.ascontiguousarray(prim, dtype=np.float64)
         out = np.zeros((3,) + self.zshape)
-        _lib.check(_lib.lib().grim_compute_div_fluxes(self._h, _ptr(p), None, None, _ptr(out), _lib.HOST),
-                   "computeEMF")
+        _lib.check(_lib.lib().grim_compute_emf(self._h, _ptr(p), _ptr(out), _lib.HOST), "computeEMF")
         return out
 
     def fluxCT(self, prim):
         """timeStepperPy.fluxCT (constrainedtransport.cpp:3-51) on a prim
         array: the face fluxes (3 x dof x Z) with the field rows replaced by
-        the constrained-transport values formed from the edge EMFs,
-        neighbours by circular shift as in the reference: F1_B2 = (E3 +
-        E3[j+1]) / 2, F2_B1 = -(E3 + E3[i+1]) / 2 and, in 3D, F1_B3 = -(E2 +
-        E2[k+1]) / 2, F3_B1 = (E2 + E2[i+1]) / 2, F2_B3 = (E1 + E1[k+1]) / 2,
-        F3_B2 = -(E1 + E1[j+1]) / 2; a direction's own field row is zero.
-        In 1D the fluxes are returned as they are."""
-        _, fl = self.computeDivOfFluxes(prim)
-        dim = int(self.cfg["dim"])
-        if dim < 2:
-            return fl
-        e1, e2, e3 = self.computeEMF(prim)
-        b1 = self.dof - 3
-
-        def up(a, axis):  # a[index + 1] along axis (k, j, i) = (0, 1, 2)
-            return np.roll(a, -1, axis=axis)
-
-        fl[0, b1] = 0.
-        fl[0, b1 + 1] = 0.5 * (e3 + up(e3, 1))
-        fl[1, b1] = -0.5 * (e3 + up(e3, 2))
-        fl[1, b1 + 1] = 0.
-        if dim == 3:
-            fl[0, b1 + 2] = -0.5 * (e2 + up(e2, 0))
-            fl[1, b1 + 2] = 0.5 * (e1 + up(e1, 0))
-            fl[2, b1] = 0.5 * (e2 + up(e2, 2))
-            fl[2, b1 + 1] = -0.5 * (e1 + up(e1, 1))
-            fl[2, b1 + 2] = 0.
+        the constrained-transport values formed from the edge EMFs on the
+        GPU (grim_flux_ct), neighbours by circular shift as in the
+        reference: F1_B2 = (E3 + E3[j+1]) / 2, F2_B1 = -(E3 + E3[i+1]) / 2
+        and, in 3D, F1_B3 = -(E2 + E2[k+1]) / 2, F3_B1 = (E2 + E2[i+1]) / 2,
+        F2_B3 = (E1 + E1[k+1]) / 2, F3_B2 = -(E1 + E1[j+1]) / 2; a
+        direction's own field row is zero.  In 1D the Riemann fluxes."""
+        p = np.ascontiguousarray(prim, dtype=np.float64)
+        fl = np.zeros((3, self.dof) + self.zshape)
+        _lib.check(_lib.lib().grim_flux_ct(self._h, _ptr(p), _ptr(fl), _lib.HOST), "fluxCT")
         return fl
 
     def computeDivB(self, prim):

@@ -272,9 +272,20 @@ int grim_apply_boundaries(grim_handle* h, int which);
 int grim_communicate(grim_handle* h, int which);
 /* computeDivOfFluxes (fvmfluxes.cpp:3-183) incl. fluxCT/computeEMF
  * (constrainedtransport.cpp:3-83) on a caller's prim array; outputs may be
- * NULL.  divF: dof x Z, fluxes: 3 x dof x Z, emf: 3 x Z (X1, X2, X3). */
+ * NULL.  divF: dof x Z (the field rows from the constrained-transport
+ * fluxes), fluxes: 3 x dof x Z (the Riemann fluxes, before flux-CT), emf:
+ * 3 x Z (X1, X2, X3). */
 int grim_compute_div_fluxes(grim_handle* h, const double* prim, double* divF,
                             double* fluxes, double* emf, int memKind);
+/* computeEMF (constrainedtransport.cpp:53-83) from the Riemann fluxes of a
+ * caller's prim array: emf = [emfX1 | emfX2 | emfX3] x Z (emfX3 from 2D on,
+ * emfX1 and emfX2 in 3D, zero otherwise) */
+int grim_compute_emf(grim_handle* h, const double* prim, double* emf, int memKind);
+/* fluxCT (constrainedtransport.cpp:3-51): the Riemann fluxes of a caller's
+ * prim array with the field rows replaced by the averages of the edge EMFs
+ * (neighbours by circular shift over the whole array, as af::shift takes
+ * them), on the GPU: fluxes = dim x dof x Z; in 1D the Riemann fluxes */
+int grim_flux_ct(grim_handle* h, const double* prim, double* fluxes, int memKind);
 /* reconstruction of one direction (reconstruction.cpp:3-36) */
 int grim_reconstruct(grim_handle* h, const double* prim, int dir,
                      double* primLeft, double* primRight, int memKind);
@@ -363,8 +374,10 @@ int grim_set_newton_mode(grim_handle* h, int mode, int perZoneConvergence, doubl
  * (tangent / mixed modes) */
 int grim_get_newton_histogram(grim_handle* h, long long* out);
 int grim_get_stats(grim_handle* h, grim_stats* out);
-/* capture timeStep into a CUDA graph and replay it from grim_time_step */
+/* capture timeStep into a CUDA graph and replay it from grim_time_step
+ * (grim_capture_graph is the same call) */
 int grim_enable_graph(grim_handle* h, int enable);
+int grim_capture_graph(grim_handle* h, int enable);
 int grim_synchronize(grim_handle* h);
 
 /* Bounded waits.  The TMA-staged face kernels wait on their copies for at

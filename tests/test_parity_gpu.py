@@ -587,6 +587,24 @@ def test_timestep_parity_1d():
 
 
 @pytest.mark.parametrize("dim", [2, 3])
+def test_flux_ct_matches_oracle(dim):
+    """grim_flux_ct (constrainedtransport.cpp:3-51 on the GPU): the face
+    fluxes with constrained-transport field rows equal the oracle's fluxes
+    after its fluxCT on every interior face, all rows."""
+    if dim == 2:
+        cfg = PR.fast_mode_config(N=32)
+    else:
+        cfg = PR.fast_mode_config(N=16, N3=16, dim=3)
+    P = _smooth_random(cfg, 11)
+    ts, orc = pair(cfg)
+    fl = ts.fluxCT(P)
+    of = orc.div_fluxes(P)[1]
+    for d in range(dim):
+        assert scaled_err(interior(cfg, fl[d]), interior(cfg, of[d])) <= 1e-14, d
+        assert np.max(np.abs(interior(cfg, fl[d][ts.dof - 3 + d]))) == 0.  # own field row
+
+
+@pytest.mark.parametrize("dim", [2, 3])
 def test_flux_ct_divergence_is_the_field_update(dim):
     """timeStepperPy.fluxCT: the divergence of the constrained-transport
     fluxes' field rows over the interior equals computeDivOfFluxes' field
