@@ -96,6 +96,14 @@ class timeStepper {
     check(grim_compute_div_fluxes(h_, primHost, divFluxesHost, nullptr, nullptr, GRIM_HOST),
           "computeDivOfFluxes");
   }
+  // timeStepper::computeEMF / fluxCT (constrainedtransport.cpp:3-83) on
+  // the Riemann fluxes of a host array: 3 x Z EMFs; dim x dof x Z fluxes
+  void computeEMF(const double* primHost, double* emfHost) {
+    check(grim_compute_emf(h_, primHost, emfHost, GRIM_HOST), "computeEMF");
+  }
+  void fluxCT(const double* primHost, double* fluxesHost) {
+    check(grim_flux_ct(h_, primHost, fluxesHost, GRIM_HOST), "fluxCT");
+  }
   // timeStepper::computeDivB (constrainedtransport.cpp:85-110), 1 x Z
   void computeDivB(const double* primHost, double* divBHost) {
     check(grim_compute_divb(h_, primHost, divBHost, GRIM_HOST), "computeDivB");
