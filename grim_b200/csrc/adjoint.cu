@@ -26,10 +26,13 @@
 // solver, the reconstruction, the conserved variables and the geometric
 // source (physics.cpp:360-420) through local Jacobians taken with the
 // forward-tangent scalar on the same templated physics the kernels run.
-// Scope: ideal MHD, Minkowski or modified Kerr-Schild, 2D or 3D, periodic /
-// outflow / mirror boundaries, no problem hooks, dt held fixed over the
-// run; the runtime rejects anything else.  Every accumulation is a gather
-// in a fixed order (no atomics), so a gradient is the same bits run to run.
+// Scope: ideal or extended MHD (conduction and / or viscosity: the EMHD
+// residual's tangents, its source's gradient gathers), Minkowski or
+// modified Kerr-Schild, 2D or 3D, periodic / outflow / mirror boundaries,
+// without problem hooks or with the torus problem's (floors, inflow check,
+// pole fix, flux filter), dt held fixed over the run; the runtime rejects
+// anything else.  Every accumulation is a gather in a fixed order (no
+// atomics), so a gradient is the same bits run to run.
 #include <cuda_runtime.h>
 
 #include "launch.h"
@@ -934,16 +937,18 @@ GRIM_D adjt::TorusCfg torus_params(const DevCfg& c) {
   t.BsqrOverRhoMax = c.bsqOverRhoMax; t.BsqrOverUMax = c.bsqOverUMax;
   return t;
 }
-GRIM_D long long prow(const DevCfg& c, int v) { return v < 5 ? v : c.B1 + (v - 5); }
-
 // applyFloor's transpose (problem.cpp:542-712), interior zones: lam holds
 // dL/d(floored state); lam <- J^T lam with J the floors' Jacobian at the
-// stage's Newton solution Psol (one forward-tangent pass, 8 lanes)
+// stage's Newton solution Psol (one forward-tangent pass, one lane per
+// primitive: the fluid rows, then the field)
+template <int C, int V>
 __global__ void k_floor_t(DevCfg c, const double* __restrict__ geoC, const double* __restrict__ Psol,
                           double* __restrict__ lam) {
+  constexpr int NF = 5 + C + V, DOF = NF + 3;
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= c.Zint) return;
-  typedef Dual<double, 8> D;
+  typedef Dual<double, DOF> D;
+  auto prow = [&](int v) -> long long { return v; };  // [fluid | field] rows, B1 = NF
   const long long Z = c.Z;
   const long long z = interior_to_z(c, n);
   int i, j, k;
@@ -955,29 +960,30 @@ __global__ void k_floor_t(DevCfg c, const double* __restrict__ geoC, const doubl
   // zero adjoint: nothing to transpose (the local Jacobian need not be
   // finite where no derivative flows, e.g. at a zero field)
   bool any = false;
-  for (int v = 0; v < 8; v++) any |= lam[prow(c, v) * Z + z] != 0.;
+  for (int v = 0; v < DOF; v++) any |= lam[prow(v) * Z + z] != 0.;
   if (!any) return;
-  D q[8];
+  D q[DOF];
   bool nan = false;
-  for (int v = 0; v < 8; v++) {
-    q[v] = D::var(Psol[prow(c, v) * Z + z], v);
+  for (int v = 0; v < DOF; v++) {
+    q[v] = D::var(Psol[prow(v) * Z + z], v);
     nan |= isnan(q[v].v);
   }
   if (nan) {
     // fullStepDiagnostics' reset: the zone's state no longer depends on it
-    for (int v = 0; v < 8; v++) lam[prow(c, v) * Z + z] = 0.;
+    for (int v = 0; v < DOF; v++) lam[prow(v) * Z + z] = 0.;
     return;
   }
   const long long gz = gidx(c, i, j);
-  adjt::torus_floor_zone<0, 0>(c, torus_params(c), q, G, __ldg(geoC + 37LL * c.GZ + gz),
+  adjt::torus_floor_zone<C, V>(c, torus_params(c), q, G, __ldg(geoC + 37LL * c.GZ + gz),
                                __ldg(geoC + 38LL * c.GZ + gz), false);
-  double out[8] = {0., 0., 0., 0., 0., 0., 0., 0.};
-  for (int r = 0; r < 8; r++) {
-    const double lr = lam[prow(c, r) * Z + z];
+  double out[DOF];
+  for (int v = 0; v < DOF; v++) out[v] = 0.;
+  for (int r = 0; r < DOF; r++) {
+    const double lr = lam[prow(r) * Z + z];
     if (lr != 0.)
-      for (int v = 0; v < 8; v++) out[v] += q[r].d[v] * lr;
+      for (int v = 0; v < DOF; v++) out[v] += q[r].d[v] * lr;
   }
-  for (int v = 0; v < 8; v++) lam[prow(c, v) * Z + z] = out[v];
+  for (int v = 0; v < DOF; v++) lam[prow(v) * Z + z] = out[v];
 }
 
 // fixPoles' transpose (problem.cpp:1046-1215) on the full-grid adjoint a,
@@ -1004,21 +1010,25 @@ __global__ void k_poles_t(DevCfg c, const double* __restrict__ geoC, double* __r
   const int row[3] = {idx0, top ? idx0 - 1 : ng + 1, top ? idx0 - 2 : ng + 2};
   double th[3];
   for (int g = 0; g < 3; g++) th[g] = theta(row[g]);
-  double acc[5];
-  for (int v = 0; v < 5; v++) acc[v] = at(v, row[2]);
+  // the fluid rows (with EMHD q and deltaP, which fixPoles scales and
+  // mirrors as it does u2)
+  const int nf = c.nf;
+  auto scaled = [&](int v) { return v == U2 || (c.conduction && v == c.Q) || (c.viscosity && v == c.DP); };
+  double acc[7];
+  for (int v = 0; v < nf; v++) acc[v] = at(v, row[2]);
   // only nonzero adjoints are carried: the ratio of thetas is not finite
   // in the innermost ghost column of some grids, where the forward's values
   // are not finite either and nothing downstream reads them
   for (int g = 0; g < 2; g++)
-    for (int v = 0; v < 5; v++) {
-      const double cf = (v == U2) ? th[g] / th[2] : 1.;
+    for (int v = 0; v < nf; v++) {
+      const double cf = scaled(v) ? th[g] / th[2] : 1.;
       if (at(v, row[g]) != 0.) acc[v] += cf * at(v, row[g]);
       at(v, row[g]) = 0.;
     }
   for (int g = 0; g < 3; g++) {
     const int dst = top ? c.N2 + ng + g : ng - 1 - g;
-    for (int v = 0; v < 5; v++) {
-      const double cf = (v == U2) ? -(g < 2 ? th[g] / th[2] : 1.) : 1.;
+    for (int v = 0; v < nf; v++) {
+      const double cf = scaled(v) ? -(g < 2 ? th[g] / th[2] : 1.) : 1.;
       if (at(v, dst) != 0.) acc[v] += cf * at(v, dst);
       at(v, dst) = 0.;
     }
@@ -1028,7 +1038,7 @@ __global__ void k_poles_t(DevCfg c, const double* __restrict__ geoC, double* __r
       at(c.B1 + b, dst) = 0.;
     }
   }
-  for (int v = 0; v < 5; v++) at(v, row[2]) = acc[v];
+  for (int v = 0; v < nf; v++) at(v, row[2]) = acc[v];
 }
 
 // inflowCheck's transpose (problem.cpp:941-1044) on the X1 ghost zones of
@@ -1150,7 +1160,7 @@ static void adjoint_step_t(const DevCfg& c, const AdjointGeo& geo, double dt, co
     }
   };
   // full stage: the floors at its finish, then the stage at its Newton solution
-  if (torus) k_floor_t<<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, st.P1Sol, lam);
+  if (torus) k_floor_t<C, V><<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, st.P1Sol, lam);
   if constexpr (emhd) {
     cudaMemsetAsync(w.p0bar, 0, rows, s);
     k_stage_emhd<C, V><<<nblk(c.Zint, 32), 32, 0, s>>>(c, geo.geoC, GRIM_FULL_STEP, dt, st.P1Sol, st.P0eff, st.PhEff,
@@ -1163,7 +1173,7 @@ static void adjoint_step_t(const DevCfg& c, const AdjointGeo& geo, double dt, co
   if constexpr (emhd) k_add_interior<<<nblk(c.Zint, 128), 128, 0, s>>>(c, w.psl, w.q);
   hooks_fold(st.PhFill, w.lamh);
   // half stage
-  if (torus) k_floor_t<<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, st.PhSol, w.lamh);
+  if (torus) k_floor_t<C, V><<<nblk(c.Zint, 64), 64, 0, s>>>(c, geo.geoC, st.PhSol, w.lamh);
   if constexpr (emhd) {
     k_stage_emhd<C, V><<<nblk(c.Zint, 32), 32, 0, s>>>(c, geo.geoC, GRIM_HALF_STEP, 0.5 * dt, st.PhSol, st.P0eff,
                                                       st.P0eff, st.divFh, st.Sexph, w.lamh, w.g, w.p0bar, w.psl);

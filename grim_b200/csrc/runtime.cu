@@ -1736,11 +1736,12 @@ static int adjoint_scope(grim_handle* h) {
   const bool bcs = ok_bc(c.boundaryLeft) && ok_bc(c.boundaryRight) && ok_bc(c.boundaryBottom) &&
                    ok_bc(c.boundaryTop) && (c.dim < 3 || (ok_bc(c.boundaryFront) && ok_bc(c.boundaryBack)));
   const bool emhd = c.conduction || c.viscosity;
-  const bool torusOk = c.problem == GRIM_PROBLEM_TORUS && !emhd && c.metric != GRIM_MINKOWSKI &&
-                       c.numGhost == 3 && (c.dim < 2 || c.N2 >= 6);
+  (void)emhd;
+  const bool torusOk = c.problem == GRIM_PROBLEM_TORUS && c.metric != GRIM_MINKOWSKI && c.numGhost == 3 &&
+                       (c.dim < 2 || c.N2 >= 6);
   if ((c.dim != 2 && c.dim != 3) || !bcs || (c.problem != GRIM_PROBLEM_NONE && !torusOk) || c.N3Global > 0) {
     set_err("adjoint: supported for 2D and 3D ideal or extended MHD (Minkowski or MKS) with periodic, outflow or "
-            "mirror boundaries, without problem hooks, or ideal MHD with the torus problem's (MKS, N2 >= 6)");
+            "mirror boundaries, without problem hooks or with the torus problem's (MKS, N2 >= 6)");
     return GRIM_ENOTSUP;
   }
   return GRIM_OK;

@@ -156,19 +156,21 @@ GRIM_D bool torus_floor_zone(const DevCfg& c, const TorusCfg& t, S* q, const Zon
     }
   }
   if constexpr (COND || VISC) {
+    // the EMHD limiters, on the scalar type (the adjoint takes their local
+    // Jacobian); on doubles the same operations in the same order
     elem_of<COND, VISC>(e, c, q, G);
     if (COND) {
-      const double cs = e.soundSpeed;
-      const double Qmax = 1.07 * c.CondClosure * q[RHO] * pow(cs, 3.);
-      const double lim = fmax(fabs(e.q) / Qmax, 1.);
+      const S cs = e.soundSpeed;
+      const S Qmax = 1.07 * c.CondClosure * q[RHO] * dcube(cs);
+      const S lim = fmax(fabs(e.q) / Qmax, S(1.));
       q[5] = q[5] / lim;
     }
     if (VISC) {
-      const double pr = e.pressure, dP = e.deltaP, bs = e.bSqr;
-      const double dPmod = fmax(pr - 2. / 3. * dP, 0.01 * c.bSqrFloor) / fmax(pr + 1. / 3. * dP, c.bSqrFloor);
-      const double dPmaxPlus = fmin(1.07 * c.ViscClosure * bs * 0.5 * dPmod, 1.49 * pr);
-      const double dPmaxMinus = fmax(-1.07 * c.ViscClosure * bs, -2.99 * pr);
-      const double f = (dP > 0.) ? 1. / fmax(dP / dPmaxPlus, 1.) : 1. / fmax(dP / dPmaxMinus, 1.);
+      const S pr = e.pressure, dP = e.deltaP, bs = e.bSqr;
+      const S dPmod = fmax(pr - 2. / 3. * dP, S(0.01 * c.bSqrFloor)) / fmax(pr + 1. / 3. * dP, S(c.bSqrFloor));
+      const S dPmaxPlus = fmin(1.07 * c.ViscClosure * bs * 0.5 * dPmod, 1.49 * pr);
+      const S dPmaxMinus = fmax(-1.07 * c.ViscClosure * bs, -2.99 * pr);
+      const S f = (val_of(dP) > 0.) ? 1. / fmax(dP / dPmaxPlus, S(1.)) : 1. / fmax(dP / dPmaxMinus, S(1.));
       q[5 + COND] = q[5 + COND] * f;
     }
     current = false;

@@ -472,10 +472,10 @@ int grim_set_face_variant(grim_handle* h, int dir, int variant);
  * Without a grim_adjoint_forward run to reverse it returns GRIM_ESTATE.
  * Supported: 2D and 3D, ideal or extended MHD (conduction and / or
  * viscosity), Minkowski or modified Kerr-Schild (geometric source, face
- * metric), periodic / outflow / mirror boundaries, no problem hooks; or
- * ideal MHD with the torus problem's (floors after each stage, inflow check
- * and pole fix at the start of each stage, flux filter; MKS, N2 >= 6).
- * GRIM_ENOTSUP otherwise (the torus problem with EMHD).  A zone that
+ * metric), periodic / outflow / mirror boundaries, no problem hooks or the
+ * torus problem's (floors after each stage, inflow check and pole fix at
+ * the start of each stage, flux filter; MKS, N2 >= 6), ideal or extended
+ * MHD.  GRIM_ENOTSUP otherwise (1D, a slab of a decomposed grid).  A zone that
  * fullStepDiagnostics' NaN reset replaces carries no derivative.  Every accumulation is a gather in a fixed
  * order (no atomics): a gradient is the same bits run to run and for any
  * checkpoint interval. */

@@ -146,6 +146,8 @@ def fd_check_richardson(loss_of, L0, adjoint, picks, scale, rtol=1e-6, h=1e-6):
         D = {}
         for k in (1, 2, 4):
             D[k] = (loss_of(*pick, k * h) - loss_of(*pick, -k * h)) / (2 * k * h)
+        if not all(math.isfinite(d) for d in D.values()):
+            continue  # a perturbed run left the map (a non-finite loss)
         r1 = (4 * D[1] - D[2]) / 3
         r2 = (4 * D[2] - D[4]) / 3
         spread = abs(r1 - r2)
